@@ -1,0 +1,348 @@
+"""Unstructured 2-D meshes for the DNDS hot path.
+
+A mesh is a set of flat arrays, the same ones the C-ABI takes
+(``dndsg_mesh_desc`` in include/dndsg.h):
+
+* ``node_xy``    float64 [n_nodes, 2]
+* ``cell_nodes`` int32   [n_cells, 4], counter-clockwise, -1 in slot 3 for a triangle
+* ``face_nodes`` int32   [n_faces, 2], ordered so that the right-hand normal of
+  node0->node1 points out of the left cell
+* ``face_cells`` int32   [n_faces, 2], (left, right); right = -1 on a boundary
+* ``face_bc``    int32   [n_faces], DNDS ``BoundaryType`` (DNDS_Mesh.hpp:21-35):
+  -1 inner, 1 Wall, 2 Farfield, 3 Wall_Euler, 4 Wall_NoSlip,
+  -4 Special_IVFar, -5 Special_2DRiemannFar
+* ``face_shift`` float64 [n_faces, 2], the translation that brings the right
+  cell next to the face (non-zero only on periodic faces)
+
+The reference builds this topology from Gmsh files
+(``CompactFacedMeshSerialRW``, DNDS_Mesh.hpp:634-1906).  The reference has no
+periodic boundary; periodic faces are interior faces whose right cell is seen
+through ``face_shift``.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+BC_INNER = -1
+BC_WALL = 1
+BC_FARFIELD = 2
+BC_WALL_EULER = 3
+BC_WALL_NOSLIP = 4
+BC_DMR_FAR = -2
+BC_RT_FAR = -3
+BC_IV_FAR = -4
+BC_2DRIEMANN_FAR = -5
+
+# Gmsh physical-group names -> BoundaryType (DNDS_Mesh.hpp:801-829)
+GMSH_BC_NAMES = {
+    "bc-1": BC_WALL,
+    "bc-2": BC_FARFIELD,
+    "bc-3": BC_WALL_EULER,
+    "bc-4": BC_WALL_NOSLIP,
+    "bc-DMRFar": BC_DMR_FAR,
+    "bc-RTFar": BC_RT_FAR,
+    "bc-IVFar": BC_IV_FAR,
+    "bc-2DRiemannFar": BC_2DRIEMANN_FAR,
+}
+
+
+@dataclass
+class Mesh:
+    node_xy: np.ndarray
+    cell_nodes: np.ndarray
+    face_nodes: np.ndarray
+    face_cells: np.ndarray
+    face_bc: np.ndarray
+    face_shift: np.ndarray
+    name: str = "mesh"
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def n_nodes(self) -> int:
+        return int(self.node_xy.shape[0])
+
+    @property
+    def n_cells(self) -> int:
+        return int(self.cell_nodes.shape[0])
+
+    @property
+    def n_faces(self) -> int:
+        return int(self.face_nodes.shape[0])
+
+    def validate(self) -> None:
+        """Host-side checks the kernels rely on (they do no bounds checks of their own)."""
+        n, f = self.n_cells, self.n_faces
+        assert self.node_xy.dtype == np.float64 and self.node_xy.shape == (self.n_nodes, 2)
+        assert self.cell_nodes.dtype == np.int32 and self.cell_nodes.shape == (n, 4)
+        assert self.face_nodes.dtype == np.int32 and self.face_nodes.shape == (f, 2)
+        assert self.face_cells.dtype == np.int32 and self.face_cells.shape == (f, 2)
+        assert self.face_bc.dtype == np.int32 and self.face_bc.shape == (f,)
+        assert self.face_shift.dtype == np.float64 and self.face_shift.shape == (f, 2)
+        cn = self.cell_nodes
+        assert cn[:, :3].min() >= 0 and cn.max() < self.n_nodes
+        assert self.face_nodes.min() >= 0 and self.face_nodes.max() < self.n_nodes
+        L, R = self.face_cells[:, 0], self.face_cells[:, 1]
+        assert L.min() >= 0 and L.max() < n and R.max() < n and R.min() >= -1
+        assert np.all((R >= 0) == (self.face_bc == BC_INNER)), "inner faces need a right cell"
+        deg = np.bincount(L, minlength=n) + np.bincount(R[R >= 0], minlength=n)
+        nn = np.where(cn[:, 3] < 0, 3, 4)
+        assert np.array_equal(deg, nn), "every cell needs one face per edge"
+
+
+def _as_mesh(node_xy, cell_nodes, faces, name, meta) -> Mesh:
+    fn, fc, fb, fs = faces
+    m = Mesh(
+        node_xy=np.ascontiguousarray(node_xy, dtype=np.float64),
+        cell_nodes=np.ascontiguousarray(cell_nodes, dtype=np.int32),
+        face_nodes=np.ascontiguousarray(fn, dtype=np.int32),
+        face_cells=np.ascontiguousarray(fc, dtype=np.int32),
+        face_bc=np.ascontiguousarray(fb, dtype=np.int32),
+        face_shift=np.ascontiguousarray(fs, dtype=np.float64),
+        name=name,
+        meta=meta,
+    )
+    m.validate()
+    return m
+
+
+def structured_grid(
+    nx: int,
+    ny: int,
+    lx: float = 10.0,
+    ly: float = 10.0,
+    x0: float = 0.0,
+    y0: float = 0.0,
+    triangles: bool = False,
+    jitter: float = 0.0,
+    seed: int = 1234,
+    periodic: bool = True,
+    bc: int = BC_FARFIELD,
+    name: str | None = None,
+) -> Mesh:
+    """An nx x ny grid of quads (or 2 triangles per quad) stored as an unstructured mesh.
+
+    ``jitter`` moves every interior node by U(-jitter*h, jitter*h) in x and in y
+    (h = grid spacing per direction), drawn from numpy's PCG64 seeded with
+    ``seed``; boundary nodes stay put, so periodic faces pair exactly.
+    Triangles alternate their diagonal with the parity of (i + j).
+    ``periodic`` pairs opposite sides; otherwise every side gets ``bc``.
+    """
+    hx, hy = lx / nx, ly / ny
+    I, J = np.meshgrid(np.arange(nx + 1), np.arange(ny + 1), indexing="xy")  # [ny+1, nx+1]
+    X = x0 + I * hx
+    Y = y0 + J * hy
+    if jitter > 0.0:
+        rng = np.random.Generator(np.random.PCG64(seed))
+        d = rng.uniform(-jitter, jitter, size=(ny + 1, nx + 1, 2))
+        inner = (I > 0) & (I < nx) & (J > 0) & (J < ny)
+        X = X + np.where(inner, d[..., 0] * hx, 0.0)
+        Y = Y + np.where(inner, d[..., 1] * hy, 0.0)
+    node_xy = np.stack([X.ravel(), Y.ravel()], axis=1)
+
+    def nid(i, j):
+        return (j * (nx + 1) + i).astype(np.int64)
+
+    ii, jj = np.meshgrid(np.arange(nx), np.arange(ny), indexing="xy")
+    ii = ii.ravel()
+    jj = jj.ravel()
+    q = jj * nx + ii  # quad id, row-major
+    n00, n10, n11, n01 = nid(ii, jj), nid(ii + 1, jj), nid(ii + 1, jj + 1), nid(ii, jj + 1)
+    nq = nx * ny
+
+    fnodes, fcells, fbc, fshift = [], [], [], []
+
+    def add(nodes, cells, bcs, shifts):
+        fnodes.append(nodes)
+        fcells.append(cells)
+        fbc.append(bcs)
+        fshift.append(shifts)
+
+    if not triangles:
+        cell_nodes = np.stack([n00, n10, n11, n01], axis=1)
+        cid = q
+        # bottom edge of quad (i,j): left = this quad (above), right = quad (i, j-1)
+        below = jj > 0
+        rb = np.where(below, (jj - 1) * nx + ii, (ny - 1) * nx + ii)
+        # left edge of quad (i,j): left = this quad, right = quad (i-1, j)
+        lft = ii > 0
+        rl = np.where(lft, jj * nx + ii - 1, jj * nx + nx - 1)
+        cb_b = cid
+        cl_l = cid
+        cell_of_top = lambda i, j: j * nx + i  # noqa: E731
+        cell_of_right = lambda i, j: j * nx + i  # noqa: E731
+    else:
+        even = ((ii + jj) % 2) == 0
+        t0 = 2 * q
+        t1 = 2 * q + 1
+        tri0 = np.where(even[:, None], np.stack([n00, n10, n11], 1), np.stack([n00, n10, n01], 1))
+        tri1 = np.where(even[:, None], np.stack([n00, n11, n01], 1), np.stack([n10, n11, n01], 1))
+        cell_nodes = np.full((2 * nq, 4), -1, dtype=np.int64)
+        cell_nodes[0::2, :3] = tri0
+        cell_nodes[1::2, :3] = tri1
+        cb_b = t0  # the bottom edge always belongs to triangle 0
+        cl_l = np.where(even, t1, t0)  # left edge: even -> T1, odd -> T0
+
+        def cell_of_top(i, j):  # top edge of quad (i,j) belongs to triangle 1
+            return 2 * (j * nx + i) + 1
+
+        def cell_of_right(i, j):  # right edge: even -> T0, odd -> T1
+            return 2 * (j * nx + i) + np.where(((i + j) % 2) == 0, 0, 1)
+
+        rb = None
+        rl = None
+
+    # --- bottom faces
+    jb = jj - 1
+    wrap_b = jj == 0
+    if periodic:
+        rbc = np.where(wrap_b, cell_of_top(ii, np.full_like(jj, ny - 1)), cell_of_top(ii, np.maximum(jb, 0)))
+        sh = np.stack([np.zeros(nq), np.where(wrap_b, -ly, 0.0)], 1)
+        add(np.stack([n00, n10], 1), np.stack([cb_b, rbc], 1), np.full(nq, BC_INNER), sh)
+    else:
+        rbc = np.where(wrap_b, -1, cell_of_top(ii, np.maximum(jb, 0)))
+        add(np.stack([n00, n10], 1), np.stack([cb_b, rbc], 1), np.where(wrap_b, bc, BC_INNER), np.zeros((nq, 2)))
+    # --- left faces
+    il = ii - 1
+    wrap_l = ii == 0
+    if periodic:
+        rlc = np.where(wrap_l, cell_of_right(np.full_like(ii, nx - 1), jj), cell_of_right(np.maximum(il, 0), jj))
+        sh = np.stack([np.where(wrap_l, -lx, 0.0), np.zeros(nq)], 1)
+        add(np.stack([n01, n00], 1), np.stack([cl_l, rlc], 1), np.full(nq, BC_INNER), sh)
+    else:
+        rlc = np.where(wrap_l, -1, cell_of_right(np.maximum(il, 0), jj))
+        add(np.stack([n01, n00], 1), np.stack([cl_l, rlc], 1), np.where(wrap_l, bc, BC_INNER), np.zeros((nq, 2)))
+    # --- diagonals
+    if triangles:
+        even = ((ii + jj) % 2) == 0
+        dn = np.where(even[:, None], np.stack([n00, n11], 1), np.stack([n01, n10], 1))
+        add(dn, np.stack([2 * q + 1, 2 * q], 1), np.full(nq, BC_INNER), np.zeros((nq, 2)))
+    if not periodic:
+        # top row and right column boundary faces
+        it = np.arange(nx)
+        add(
+            np.stack([nid(it + 1, np.full(nx, ny)), nid(it, np.full(nx, ny))], 1),
+            np.stack([cell_of_top(it, np.full(nx, ny - 1)), np.full(nx, -1)], 1),
+            np.full(nx, bc),
+            np.zeros((nx, 2)),
+        )
+        jt = np.arange(ny)
+        add(
+            np.stack([nid(np.full(ny, nx), jt), nid(np.full(ny, nx), jt + 1)], 1),
+            np.stack([cell_of_right(np.full(ny, nx - 1), jt), np.full(ny, -1)], 1),
+            np.full(ny, bc),
+            np.zeros((ny, 2)),
+        )
+    # interleave the per-quad faces so that faces of nearby cells are nearby in memory
+    nper = 3 if triangles else 2
+    fn = np.stack([a for a in fnodes[:nper]], 1).reshape(-1, 2)
+    fc = np.stack([a for a in fcells[:nper]], 1).reshape(-1, 2)
+    fb = np.stack([a for a in fbc[:nper]], 1).reshape(-1)
+    fs = np.stack([a for a in fshift[:nper]], 1).reshape(-1, 2)
+    if len(fnodes) > nper:
+        fn = np.concatenate([fn] + fnodes[nper:], 0)
+        fc = np.concatenate([fc] + fcells[nper:], 0)
+        fb = np.concatenate([fb] + fbc[nper:], 0)
+        fs = np.concatenate([fs] + fshift[nper:], 0)
+    # a periodic face's right cell is the cell on the opposite side: its shift
+    # moves that cell next to the face (bottom: R lies at the top -> -ly)
+    meta = dict(nx=nx, ny=ny, lx=lx, ly=ly, x0=x0, y0=y0, triangles=triangles, jitter=jitter, seed=seed,
+                periodic=periodic)
+    nm = name or f"{'tri' if triangles else 'quad'}{nx}x{ny}{'_per' if periodic else ''}"
+    return _as_mesh(node_xy, cell_nodes, (fn, fc, fb, fs), nm, meta)
+
+
+def vortex_mesh(n: int, triangles: bool, jitter: float = 0.0, seed: int = 1234) -> Mesh:
+    """Periodic [0,10]^2 isentropic-vortex mesh (n x n quads, optionally split)."""
+    return structured_grid(n, n, 10.0, 10.0, triangles=triangles, jitter=jitter, seed=seed, periodic=True)
+
+
+def riemann_mesh(n: int, jitter: float = 0.15, seed: int = 4321) -> Mesh:
+    """[0,1]^2 four-quadrant Riemann mesh, triangles, Special_2DRiemannFar on all sides."""
+    return structured_grid(n, n, 1.0, 1.0, triangles=True, jitter=jitter, seed=seed, periodic=False,
+                           bc=BC_2DRIEMANN_FAR)
+
+
+def read_gmsh2(path: str) -> Mesh:
+    """Gmsh 2.2 ASCII reader for 2-D meshes (SerialGmshReader2d, DNDS_Mesh.hpp:87-236).
+
+    Cells are Tri3 (type 2) and Quad4 (type 3); boundary lines (type 1) carry
+    the physical-group names of ``GMSH_BC_NAMES``.  Faces are extracted from
+    the cell edges; cells are made counter-clockwise.
+    """
+    with open(path) as fh:
+        lines = [ln.strip() for ln in fh]
+    k = 0
+    names = {}
+    nodes = None
+    cells = []
+    bnd = []
+    while k < len(lines):
+        ln = lines[k]
+        if ln == "$PhysicalNames":
+            cnt = int(lines[k + 1])
+            for t in range(cnt):
+                parts = lines[k + 2 + t].split()
+                names[int(parts[1])] = parts[2].strip('"')
+            k += cnt + 3
+        elif ln == "$Nodes":
+            cnt = int(lines[k + 1])
+            arr = np.array([lines[k + 2 + t].split() for t in range(cnt)], dtype=np.float64)
+            ids = arr[:, 0].astype(np.int64)
+            nodes = np.zeros((int(ids.max()) + 1, 2))
+            nodes[ids] = arr[:, 1:3]
+            k += cnt + 3
+        elif ln == "$Elements":
+            cnt = int(lines[k + 1])
+            for t in range(cnt):
+                p = [int(v) for v in lines[k + 2 + t].split()]
+                et, ntag = p[1], p[2]
+                phys = p[3] if ntag > 0 else -1
+                conn = p[3 + ntag:]
+                if et == 1:
+                    bnd.append((conn[0], conn[1], phys))
+                elif et == 2:
+                    cells.append(conn[:3] + [-1])
+                elif et == 3:
+                    cells.append(conn[:4])
+            k += cnt + 3
+        else:
+            k += 1
+    assert nodes is not None
+    used = np.unique(np.array([c for cc in cells for c in cc if c >= 0] + [b[0] for b in bnd] + [b[1] for b in bnd]))
+    remap = -np.ones(nodes.shape[0], dtype=np.int64)
+    remap[used] = np.arange(used.size)
+    node_xy = nodes[used]
+    cn = np.array(cells, dtype=np.int64)
+    cn = np.where(cn >= 0, remap[np.maximum(cn, 0)], -1)
+    # orient counter-clockwise
+    for i in range(cn.shape[0]):
+        nn = 3 if cn[i, 3] < 0 else 4
+        p = node_xy[cn[i, :nn]]
+        a = 0.5 * np.sum(p[:, 0] * np.roll(p[:, 1], -1) - np.roll(p[:, 0], -1) * p[:, 1])
+        if a < 0:
+            cn[i, :nn] = cn[i, :nn][::-1]
+    bmap = {}
+    for a, b, phys in bnd:
+        key = (min(remap[a], remap[b]), max(remap[a], remap[b]))
+        nm = names.get(phys, "")
+        bmap[key] = GMSH_BC_NAMES.get(nm, BC_FARFIELD)
+    edges = {}
+    fn, fc, fb = [], [], []
+    for i in range(cn.shape[0]):
+        nn = 3 if cn[i, 3] < 0 else 4
+        for e in range(nn):
+            a, b = int(cn[i, e]), int(cn[i, (e + 1) % nn])
+            key = (min(a, b), max(a, b))
+            if key in edges:
+                fc[edges[key]][1] = i
+            else:
+                edges[key] = len(fn)
+                fn.append([a, b])
+                fc.append([i, -1])
+    for f, (a, b) in enumerate(fn):
+        key = (min(a, b), max(a, b))
+        fb.append(BC_INNER if fc[f][1] >= 0 else bmap.get(key, BC_FARFIELD))
+    nf = len(fn)
+    return _as_mesh(node_xy, cn, (np.array(fn), np.array(fc), np.array(fb), np.zeros((nf, 2))), path, {})
