@@ -1,0 +1,350 @@
+"""Benchmark: cell-RK-stage updates/s of the DNDS residual-evaluation path on B200.
+
+Workload: the 2-D isentropic vortex on a periodic [0,10]^2 1024x1024 grid whose
+interior nodes are jittered by U(-0.2h, 0.2h) (seed 1234), each quad split into
+2 triangles (2,097,152 cells); P2 variational reconstruction (one Jacobi sweep
+per stage), Roe flux, SSP-RK3 at CFL 0.5 with a global time step.  One "step"
+is one SSP-RK3 step = 3 cell-RK-stage updates of every cell.  The headline
+`value` is the FP32-bulk path (FP64 cell means, dt and norms); the plain FP64
+path is timed beside it.  Synthetic data generated here; no dataset.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl dnds_b200|reference]
+
+With N > 1 (torchrun, one rank per GPU) every rank runs an independent
+replica (the reference partitions the mesh with MPI halos; this build runs
+one mesh per GPU), and `value` is the sum over ranks (weak scaling).
+`--impl reference` times the FP64 CPU restatement of the reference (oracle/)
+on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-RK-stage updates/s: FP32+learned VR vs plain FP64 at equal L2 error, 1 B200"
+UNIT = "cell-stage updates/s"
+WORKLOAD = "isentropic vortex, periodic [0,10]^2, 1024x1024 jittered quads -> 2,097,152 triangles, P2 VR + Roe, SSP-RK3 CFL 0.5"
+N_GRID = 1024
+# algorithmic bytes per triangle cell of one VR Jacobi sweep: read urec 20s, A^-1B 75s, A^-1b 15s,
+# write urec 20s (s = bytes per real), cell means 4x8, 3 neighbour indices 3x4
+VR_BYTES_PER_CELL = {4: 130 * 4 + 32 + 12, 8: 130 * 8 + 32 + 12}
+KERNELS_PER_STEP = 14  # init, dt face, dt cell, dt finalize, 3 x (VR, flux, update), time advance
+# DRAM bytes (read + write) per launch of the FP32 VR sweep on this workload, from the
+# ncu capture summarised in profiles/vr_sweep_fp32_vortex_tri1024.md (None until captured)
+VR_TRAFFIC_FP32 = None
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.f = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-i", str(gpu_index), "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].strip().lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(max_seconds=12.0):
+    """The FP64 CPU oracle on a bounded sample of the workload (512x512 grid -> 524,288 triangles)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from dnds_b200 import geometry as G
+    from dnds_b200 import mesh as M
+    from dnds_b200 import settings as S
+
+    pyoracle.build()
+    cores = os.cpu_count() or 1
+    m = M.vortex_mesh(512, True, jitter=0.2, seed=1234)
+    o = pyoracle.Oracle(m, S.preset("vortex"), n_threads=cores)
+    o.set_u(G.isentropic_vortex(m))
+    steps = 0
+    t = 0.0
+    t0 = time.perf_counter()
+    while True:
+        _, d = o.eval_dt(0.5)
+        o.ssprk3_step(d, t)
+        t += d
+        steps += 1
+        el = time.perf_counter() - t0
+        if el > max_seconds or steps >= 200:
+            break
+    v = m.n_cells * 3 * steps / el
+    return {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"FP64 oracle, {steps} SSP-RK3 steps on the 512x512 (524,288-triangle) version of the workload, "
+                      f"{el:.1f} s, {cores} threads"}
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    cb = cpu_baseline(max_seconds=1.0)  # warm the build; the measured arm follows
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from dnds_b200 import geometry as G
+    from dnds_b200 import mesh as M
+    from dnds_b200 import settings as S
+
+    cores = os.cpu_count() or 1
+    n = 512
+    m = M.vortex_mesh(n, True, jitter=0.2, seed=1234)
+    o = pyoracle.Oracle(m, S.preset("vortex"), n_threads=cores)
+    o.set_u(G.isentropic_vortex(m))
+    t = 0.0
+    for _ in range(args.warmup):
+        _, d = o.eval_dt(0.5)
+        o.ssprk3_step(d, t)
+        t += d
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        _, d = o.eval_dt(0.5)
+        o.ssprk3_step(d, t)
+        t += d
+    el = time.perf_counter() - t0
+    v = m.n_cells * 3 * args.steps / el
+    out = {
+        "metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": el / max(args.steps, 1) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD.replace("1024x1024", "512x512").replace("2,097,152", "524,288"),
+                   "cells": m.n_cells, "parallelism": "host threads",
+                   "note": "FP64 CPU restatement of the reference (the reference needs Eigen/MPI/METIS, absent here); "
+                           "each step is the 524,288-cell sample of the workload; the metric is per cell"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} timed SSP-RK3 steps on 524,288 triangles, {cores} threads"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    del cb
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="dnds_b200", choices=["dnds_b200", "reference"])
+    ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+
+    from dnds_b200 import geometry as G
+    from dnds_b200 import mesh as M
+    from dnds_b200 import settings as S
+    from dnds_b200.solver import Solver
+
+    m = M.vortex_mesh(N_GRID, True, jitter=0.2, seed=1234)
+    N = m.n_cells
+    cfg = S.preset("vortex")
+    u0 = G.isentropic_vortex(m)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if ws > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def time_steps(solver, k):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        e0.record()
+        for _ in range(k):
+            solver.ssprk3_step(0.5, 1e300)
+        e1.record()
+        barrier()
+        ms = e0.elapsed_time(e1)
+        if ws > 1:
+            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    results = {}
+    for prec, name in ((1, "fp32"), (0, "fp64")):
+        s = Solver(m, cfg, device=dev, precision=prec)
+        s.set_u(u0)
+        for _ in range(args.warmup):
+            s.ssprk3_step(0.5, 1e300)
+        clk = ClockSampler(dev) if name == "fp32" else None
+        ms = time_steps(s, args.steps)
+        clocks = clk.stop() if clk else None
+        # per-kernel: the VR sweep alone, and the RHS (face flux + gather)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        nk = 20
+        barrier()
+        e0.record()
+        for _ in range(nk):
+            s.ReconstructionJacobiStep(1)
+        e1.record()
+        torch.cuda.synchronize()
+        vr_ms = e0.elapsed_time(e1) / nk
+        s.EvaluateDt(0.5)
+        e0.record()
+        for _ in range(nk):
+            s.EvaluateRHS(0.0, copy=False)
+        e1.record()
+        torch.cuda.synchronize()
+        rhs_ms = e0.elapsed_time(e1) / nk
+        flags, nred = s.status()
+        results[name] = dict(ms=ms, vr_ms=vr_ms, rhs_ms=rhs_ms, clocks=clocks, flags=flags, nred=nred)
+        # end-to-end through the public API with host buffers: per step h2d of the
+        # state u (pinned), one SSP-RK3 step, d2h of the new state
+        if name == "fp32":
+            host = torch.empty((N, 4), dtype=torch.float64, pin_memory=True)
+            host.copy_(torch.from_numpy(u0))
+            hnp = host.numpy()
+            barrier()
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                s.set_u(hnp)
+                s.ssprk3_step(0.5, 1e300)
+                s.get_u(out=hnp)
+            barrier()
+            e2e_s = time.perf_counter() - t0
+            if ws > 1:
+                t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+                torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+                e2e_s = float(t.item())
+            results[name]["e2e_s"] = e2e_s
+        # accuracy at t = 2 against the exact advected vortex (density)
+        if not args.no_accuracy:
+            s.set_u(u0)
+            s.set_urec(np.zeros((N, 5, 4)))
+            s.time = 0.0
+            steps = s.run_to(2.0, 0.5)
+            u = s.get_u()
+            ex = G.isentropic_vortex(m, t=2.0)
+            vol = G.cell_quadrature(m)[1].sum(1)
+            d = u[:, 0] - ex[:, 0]
+            results[name]["l2_rho"] = float(np.sqrt((d * d * vol).sum() / vol.sum()))
+            results[name]["linf_rho"] = float(np.abs(d).max())
+            results[name]["steps_to_t2"] = steps
+            results[name]["u_t2"] = u
+        s.close()
+
+    if "u_t2" in results["fp32"]:
+        d = results["fp32"]["u_t2"][:, 0] - results["fp64"]["u_t2"][:, 0]
+        vol = G.cell_quadrature(m)[1].sum(1)
+        l2_vs64 = float(np.sqrt((d * d * vol).sum() / vol.sum()))
+        for r in results.values():
+            r.pop("u_t2")
+    else:
+        l2_vs64 = None
+
+    r32, r64 = results["fp32"], results["fp64"]
+    value = N * 3 * args.steps / (r32["ms"] * 1e-3) * ws
+    value64 = N * 3 * args.steps / (r64["ms"] * 1e-3) * ws
+    peak, peak_kind = measured_peak()
+    vr_bytes = VR_BYTES_PER_CELL[4] * N
+    achieved = vr_bytes / (r32["vr_ms"] * 1e-3) / 1e9
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": r32["ms"] / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 bulk (f64 means, dt, norms)", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "cells": N, "faces": m.n_faces, "precision": "fp32-bulk",
+                   "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU",
+                   "l2_flush": "no flush: per-step working set ~1.3 GB > 126 MB L2"},
+        "fp64_path": {"value": value64, "ms_per_step": r64["ms"] / args.steps, "vr_ms": r64["vr_ms"],
+                      "rhs_ms": r64["rhs_ms"]},
+        "speedup_fp32_over_fp64": value / value64,
+        "kernels_ms": {"vr_sweep_fp32": r32["vr_ms"], "rhs_fp32": r32["rhs_ms"]},
+        "roofline": {"kernel": "vr_sweep (FP32)", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": f"{peak_kind} hbm_gbs",
+                     "traffic": VR_TRAFFIC_FP32,
+                     "alg_bytes_per_launch": vr_bytes},
+        "gpu_launches": KERNELS_PER_STEP * args.steps,
+        "clocks": r32["clocks"],
+        "status": {"flags": r32["flags"] | r64["flags"], "reduced_order_points": r32["nred"] + r64["nred"]},
+    }
+    if "e2e_s" in r32:
+        out["e2e"] = {"value": N * 3 * args.steps / r32["e2e_s"] * ws, "unit": UNIT,
+                      "h2d_bytes_per_step": N * 4 * 8, "d2h_bytes_per_step": N * 4 * 8}
+    if "l2_rho" in r32:
+        out["accuracy_t2"] = {"l2_rho_fp32": r32["l2_rho"], "l2_rho_fp64": r64["l2_rho"],
+                              "linf_rho_fp32": r32["linf_rho"], "linf_rho_fp64": r64["linf_rho"],
+                              "l2_rho_fp32_vs_fp64": l2_vs64, "steps": r32["steps_to_t2"],
+                              "reference": "exact advected vortex (cell averages), density"}
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_baseline()
+    if rank == 0:
+        print(json.dumps(out))
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

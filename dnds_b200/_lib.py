@@ -1,0 +1,72 @@
+"""ctypes binding of libdndsg.so (include/dndsg.h).  No fallback: if the
+library is missing or a call fails, an exception says so."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from .build import LIB
+
+_lib = None
+
+# every symbol include/dndsg.h declares
+EXPORTS = [
+    "dndsg_create", "dndsg_destroy", "dndsg_last_error", "dndsg_n_cells", "dndsg_n_faces",
+    "dndsg_set_u", "dndsg_get_u", "dndsg_set_urec", "dndsg_get_urec", "dndsg_get_dt",
+    "dndsg_device_buffer", "dndsg_get_time", "dndsg_set_time", "dndsg_vr_jacobi_step",
+    "dndsg_limiter_wbap", "dndsg_eval_dt", "dndsg_eval_rhs", "dndsg_ssprk3_step",
+    "dndsg_residual", "dndsg_face_values", "dndsg_get_status",
+]
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [
+        ("n_nodes", C.c_int64),
+        ("n_cells", C.c_int64),
+        ("n_faces", C.c_int64),
+        ("node_xy", C.c_void_p),
+        ("cell_nodes", C.c_void_p),
+        ("face_nodes", C.c_void_p),
+        ("face_cells", C.c_void_p),
+        ("face_bc", C.c_void_p),
+        ("face_shift", C.c_void_p),
+    ]
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB):
+        raise RuntimeError(f"{LIB} is not built; run `python -m dnds_b200.build` (nvcc, sm_100a)")
+    L = C.CDLL(LIB)
+    vp, i32, dbl, i64 = C.c_void_p, C.c_int, C.c_double, C.c_int64
+    from .settings import Settings
+
+    L.dndsg_create.argtypes = [C.POINTER(MeshDesc), C.POINTER(Settings), i32, C.POINTER(vp)]
+    L.dndsg_destroy.argtypes = [vp]
+    L.dndsg_destroy.restype = None
+    L.dndsg_last_error.argtypes = [vp]
+    L.dndsg_last_error.restype = C.c_char_p
+    L.dndsg_n_cells.argtypes = [vp]
+    L.dndsg_n_cells.restype = i64
+    L.dndsg_n_faces.argtypes = [vp]
+    L.dndsg_n_faces.restype = i64
+    for nm in ["dndsg_set_u", "dndsg_get_u", "dndsg_set_urec", "dndsg_get_urec", "dndsg_get_dt"]:
+        getattr(L, nm).argtypes = [vp, vp, vp]
+    L.dndsg_device_buffer.argtypes = [vp, i32, C.POINTER(vp), C.POINTER(i64)]
+    L.dndsg_get_time.argtypes = [vp, C.POINTER(dbl), vp]
+    L.dndsg_set_time.argtypes = [vp, dbl, vp]
+    L.dndsg_vr_jacobi_step.argtypes = [vp, i32, C.POINTER(dbl), vp]
+    L.dndsg_limiter_wbap.argtypes = [vp, i32, vp, vp]
+    L.dndsg_eval_dt.argtypes = [vp, dbl, dbl, i32, C.POINTER(dbl), vp]
+    L.dndsg_eval_rhs.argtypes = [vp, dbl, vp, vp]
+    L.dndsg_ssprk3_step.argtypes = [vp, dbl, dbl, vp]
+    L.dndsg_residual.argtypes = [vp, i32, i32, vp, vp]
+    L.dndsg_face_values.argtypes = [vp, dbl, vp, vp]
+    L.dndsg_get_status.argtypes = [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), vp]
+    for nm in EXPORTS:
+        if nm not in ("dndsg_destroy", "dndsg_last_error", "dndsg_n_cells", "dndsg_n_faces"):
+            getattr(L, nm).restype = i32
+    _lib = L
+    return L

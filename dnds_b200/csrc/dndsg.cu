@@ -1,0 +1,760 @@
+// dndsg.cu -- context, kernels and C ABI of the B200 DNDS hot path.
+//
+// Build: nvcc -gencode arch=compute_100a,code=sm_100a -O3 -lineinfo -shared
+// (see dnds_b200/build.py).  One thread per cell / face around the bodies of
+// dndsg_bodies.cuh; block-level reductions use warp shuffles.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/dndsg.h"
+#include "dndsg_bodies.cuh"
+
+using namespace dg;
+
+namespace {
+constexpr int kBlock = 256;
+inline unsigned grid_for(int64_t n) { return (unsigned)((n + kBlock - 1) / kBlock); }
+
+// device scalar slots
+enum { S_T = 0, S_DT = 1, S_DTMIN = 2, S_TEVAL = 3, S_ZERO = 4, S_INC = 5, S_NSLOT = 8 };
+}  // namespace
+
+struct dndsg_ctx {
+  int device = 0;
+  dndsg_settings s{};
+  int64_t N = 0, F = 0;
+  int nfmax = 3;
+  bool fp32 = false;
+  bool hasWallCorr = false;
+  std::string err;
+  // mesh / geometry
+  int32_t *faceL = nullptr, *faceR = nullptr, *faceBC = nullptr;
+  double *vol = nullptr, *closure = nullptr, *faceNormal = nullptr, *faceArea = nullptr, *faceCenter = nullptr,
+         *faceW0 = nullptr;
+  int32_t *cellFace = nullptr, *vrNbr = nullptr, *vrMode = nullptr, *vrFace = nullptr;
+  void* vrOp = nullptr;       // T
+  void* faceBasis = nullptr;  // T
+  double* Ainv = nullptr;
+  // state
+  double *u = nullptr, *uLast = nullptr, *rhs = nullptr, *dt = nullptr, *flux = nullptr, *lamA = nullptr,
+         *dLam = nullptr, *scal = nullptr, *partial = nullptr;
+  void *urec = nullptr, *urecNew = nullptr;  // T
+  unsigned* flags = nullptr;
+  unsigned long long* nreduced = nullptr;
+  std::vector<void*> allocs;
+
+  size_t tsize() const { return fp32 ? sizeof(float) : sizeof(double); }
+};
+
+namespace {
+
+int fail(dndsg_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+#define DG_CUDA(ctx, call)                                                                          \
+  do {                                                                                              \
+    cudaError_t e_ = (call);                                                                        \
+    if (e_ != cudaSuccess)                                                                          \
+      return fail(ctx, DNDSG_CUDA_ERROR, std::string(#call) + ": " + cudaGetErrorString(e_));      \
+  } while (0)
+
+template <class P>
+int dalloc(dndsg_ctx* c, P*& p, size_t bytes) {
+  void* q = nullptr;
+  cudaError_t e = cudaMalloc(&q, bytes > 0 ? bytes : 16);
+  if (e != cudaSuccess) return fail(c, DNDSG_CUDA_ERROR, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  c->allocs.push_back(q);
+  p = (P*)q;
+  return 0;
+}
+
+// ------------------------------------------------------------------ warp/block reductions
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_min(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// ------------------------------------------------------------------ setup kernels
+__global__ void k_setup_cell(MeshView m, SetupParams p, CellSetup* cells, double* vol, double* bary, int* bad) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= m.N) return;
+  CellSetup c;
+  if (!setup_cell(i, m, p, c)) atomicOr(bad, 1);
+  cells[i] = c;
+  vol[i] = c.vol;
+  bary[2 * i] = c.bary[0];
+  bary[2 * i + 1] = c.bary[1];
+}
+
+template <class T>
+__global__ void k_setup_face(MeshView m, SetupParams p, const CellSetup* cells, double* faceW, double* normal,
+                             double* area, double* center, double* w0, T* basis) {
+  int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (f >= m.F) return;
+  setup_face<T>(f, m, p, cells, faceW, normal, area, center, w0, basis, nullptr);
+}
+
+template <class T>
+__global__ void k_setup_matrices(MeshView m, SetupParams p, const CellSetup* cells, const double* faceW,
+                                 const int32_t* cellFace, int nfmax, T* vrOp, int32_t* vrNbr, int32_t* vrMode,
+                                 int32_t* vrFace, double* Ainv, int* bad) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= m.N) return;
+  if (!setup_cell_matrices<T>(i, m, p, cells, faceW, cellFace, nfmax, vrOp, nullptr, vrNbr, vrMode, vrFace, Ainv))
+    atomicOr(bad, 2);
+}
+
+// ------------------------------------------------------------------ hot kernels
+template <class T, bool RELAX1, bool INC>
+__global__ void __launch_bounds__(kBlock) k_vr(HotView<T> h, double* incAcc) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  double d2 = 0;
+  if (i < h.N) {
+    vr_cell<T, RELAX1>(i, h);
+    if (INC) {
+      for (int k = 0; k < 20; k++) {
+        double d = (double)h.urecNew[i * 20 + k] - (double)h.urec[i * 20 + k];
+        d2 += d * d;
+      }
+    }
+  }
+  if (INC) {
+    d2 = warp_sum(d2);
+    if ((threadIdx.x & 31) == 0 && d2 != 0.0) atomicAdd(incAcc, d2);
+  }
+}
+
+__device__ __forceinline__ double stage_time(const double* scal, int useDev, double tHost, double c) {
+  return useDev ? scal[S_T] + c * scal[S_DT] : tHost;
+}
+
+template <class T, int RIEMANN>
+__global__ void __launch_bounds__(kBlock) k_face_flux(HotView<T> h, const double* scal, int useDev, double tHost,
+                                                      double c, unsigned* flags, unsigned long long* nred) {
+  int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int r = 0;
+  bool bad = false;
+  if (f < h.F) {
+    double out[4];
+    double t = stage_time(scal, useDev, tHost, c);
+    r = face_flux<T, RIEMANN>(f, h, t, out, bad);
+    double* o = &h.flux[f * 4];
+    *reinterpret_cast<double2*>(o) = make_double2(out[0], out[1]);
+    *reinterpret_cast<double2*>(o + 2) = make_double2(out[2], out[3]);
+  }
+  unsigned anyBad = __ballot_sync(0xffffffffu, bad);
+  int rs = __reduce_add_sync(0xffffffffu, r);
+  if ((threadIdx.x & 31) == 0) {
+    if (anyBad) atomicOr(flags, 1u);
+    if (rs) atomicAdd(nred, (unsigned long long)rs);
+  }
+}
+
+template <class T>
+__global__ void k_face_values(HotView<T> h, double t, double* out) {
+  int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (f >= h.F) return;
+  double UL[3][4], UR[3][4], nx, ny, area;
+  face_states(f, h, t, UL, UR, nx, ny, area);
+  for (int g = 0; g < 3; g++)
+    for (int v = 0; v < 4; v++) {
+      out[((f * 3 + g) * 2 + 0) * 4 + v] = UL[g][v];
+      out[((f * 3 + g) * 2 + 1) * 4 + v] = UR[g][v];
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_dt_face(HotView<T> h) {
+  int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (f < h.F) dt_face<T>(f, h);
+}
+
+__global__ void k_init_dtmin(double* scal) {
+  unsigned long long inf = 0x7ff0000000000000ull;
+  reinterpret_cast<unsigned long long*>(scal)[S_DTMIN] = inf;
+  scal[S_INC] = 0.0;
+}
+
+// per-cell dt, global min, and (for a step) the copy u -> uLast
+template <class T, bool COPY_LAST>
+__global__ void __launch_bounds__(kBlock) k_dt_cell(HotView<T> h, double cfl, double maxDt, double* scal) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  double d = 1e300;
+  if (i < h.N) {
+    d = dt_cell<T>(i, h, cfl, maxDt);
+    h.dt[i] = d;
+    if (COPY_LAST) {
+      const double2* s = reinterpret_cast<const double2*>(&h.u[i * 4]);
+      double2* o = reinterpret_cast<double2*>(&h.uLast[i * 4]);
+      o[0] = s[0];
+      o[1] = s[1];
+    }
+  }
+  d = warp_min(d);
+  __shared__ double sm[kBlock / 32];
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = d;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = threadIdx.x < kBlock / 32 ? sm[threadIdx.x] : 1e300;
+    v = warp_min(v);
+    if (threadIdx.x == 0 && v >= 0)
+      atomicMin(reinterpret_cast<unsigned long long*>(scal) + S_DTMIN, (unsigned long long)__double_as_longlong(v));
+  }
+}
+
+// step dt = min(dt_min, t_end - t)
+__global__ void k_dt_finalize(double* scal, double tEnd) {
+  double dmin = __longlong_as_double((long long)reinterpret_cast<unsigned long long*>(scal)[S_DTMIN]);
+  double rem = tEnd - scal[S_T];
+  scal[S_DT] = fmax(0.0, fmin(dmin, rem));
+}
+__global__ void k_advance_time(double* scal) { scal[S_T] += scal[S_DT]; }
+
+__global__ void k_fill_dt(double* dt, int64_t n, const double* scal) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) dt[i] = __longlong_as_double((long long)reinterpret_cast<const unsigned long long*>(scal)[S_DTMIN]);
+}
+
+// rhs gather + (optionally) SSP-RK3 stage update (ExplicitSSPRK3LocalDt::Step, DNDS_ODE.hpp:140-163)
+template <class T, int STAGE>
+__global__ void __launch_bounds__(kBlock) k_cell_update(HotView<T> h, const double* scal) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= h.N) return;
+  double r[4];
+  cell_rhs<T>(i, h, r);
+  if (STAGE < 0) {
+    double2* o = reinterpret_cast<double2*>(&h.rhs[i * 4]);
+    o[0] = make_double2(r[0], r[1]);
+    o[1] = make_double2(r[2], r[3]);
+    return;
+  }
+  const double dt = scal[S_DT];
+  double x[4];
+  load4<T>(&h.u[i * 4], x);
+  for (int v = 0; v < 4; v++) x[v] += r[v] * dt;
+  if (STAGE > 0) {
+    const double cf = STAGE == 1 ? 0.25 : 2.0 / 3.0;
+    double xl[4];
+    load4<T>(&h.uLast[i * 4], xl);
+    for (int v = 0; v < 4; v++) {
+      double a = x[v] * (cf / (1 - cf));
+      a += xl[v];
+      x[v] = a * (1 - cf);
+    }
+  }
+  double2* o = reinterpret_cast<double2*>(&h.u[i * 4]);
+  o[0] = make_double2(x[0], x[1]);
+  o[1] = make_double2(x[2], x[3]);
+}
+
+// per-block partial sums / maxima of |rhs|^p (EvaluateResidual)
+__global__ void k_residual(const double* rhs, const double* vol, int64_t n, int p, int volWise, double* partial) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  double a[4] = {0, 0, 0, 0};
+  if (i < n)
+    for (int v = 0; v < 4; v++) {
+      double x = fabs(rhs[i * 4 + v]);
+      if (p < 3) {
+        x = p == 1 ? x : (p == 2 ? x * x : pow(x, (double)p));
+        if (volWise) x *= vol[i];
+      }
+      a[v] = x;
+    }
+  __shared__ double sm[4][kBlock / 32];
+  for (int v = 0; v < 4; v++) {
+    double w = p < 3 ? warp_sum(a[v]) : warp_max(a[v]);
+    if ((threadIdx.x & 31) == 0) sm[v][threadIdx.x >> 5] = w;
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    double acc = 0;
+    for (int k = 0; k < kBlock / 32; k++) acc = p < 3 ? acc + sm[threadIdx.x][k] : fmax(acc, sm[threadIdx.x][k]);
+    partial[blockIdx.x * 4 + threadIdx.x] = acc;
+  }
+}
+
+template <class T>
+__global__ void k_cvt_to(const double* src, T* dst, int64_t n) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = (T)src[i];
+}
+template <class T>
+__global__ void k_cvt_from(const T* src, double* dst, int64_t n) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = (double)src[i];
+}
+
+template <class T>
+HotView<T> view(dndsg_ctx* c) {
+  HotView<T> h;
+  h.N = c->N; h.F = c->F; h.nfmax = c->nfmax;
+  h.vol = c->vol; h.closure = c->closure; h.cellFace = c->cellFace;
+  h.vrOp = (const T*)c->vrOp; h.vrNbr = c->vrNbr; h.vrMode = c->vrMode; h.vrFace = c->vrFace; h.Ainv = c->Ainv;
+  h.faceL = c->faceL; h.faceR = c->faceR; h.faceBC = c->faceBC;
+  h.faceBasis = (const T*)c->faceBasis; h.faceNormal = c->faceNormal; h.faceArea = c->faceArea;
+  h.faceCenter = c->faceCenter; h.faceW0 = c->faceW0;
+  h.u = c->u; h.uLast = c->uLast; h.rhs = c->rhs; h.dt = c->dt;
+  h.urec = (const T*)c->urec; h.urecNew = (T*)c->urecNew;
+  h.flux = c->flux; h.lamA = c->lamA; h.dLam = c->dLam;
+  h.gamma = c->s.gamma;
+  for (int k = 0; k < 4; k++) h.farU[k] = c->s.far_field[k];
+  h.relax = c->s.jacobi_relax;
+  return h;
+}
+
+inline cudaStream_t st(void* s) { return (cudaStream_t)s; }
+
+// ------------------------------------------------------------------ hot-path drivers (templated on T)
+template <class T>
+int run_vr(dndsg_ctx* c, bool inc, cudaStream_t s) {
+  HotView<T> h = view<T>(c);
+  bool r1 = c->s.jacobi_relax == 1.0;
+  if (inc) {
+    if (r1) k_vr<T, true, true><<<grid_for(c->N), kBlock, 0, s>>>(h, c->scal + S_INC);
+    else k_vr<T, false, true><<<grid_for(c->N), kBlock, 0, s>>>(h, c->scal + S_INC);
+  } else {
+    if (r1) k_vr<T, true, false><<<grid_for(c->N), kBlock, 0, s>>>(h, nullptr);
+    else k_vr<T, false, false><<<grid_for(c->N), kBlock, 0, s>>>(h, nullptr);
+  }
+  std::swap(c->urec, c->urecNew);
+  return 0;
+}
+
+template <class T>
+void launch_flux(dndsg_ctx* c, int useDev, double tHost, double cst, cudaStream_t s) {
+  HotView<T> h = view<T>(c);
+  if (c->s.riemann == 2)
+    k_face_flux<T, 2><<<grid_for(c->F), kBlock, 0, s>>>(h, c->scal, useDev, tHost, cst, c->flags, c->nreduced);
+  else
+    k_face_flux<T, 1><<<grid_for(c->F), kBlock, 0, s>>>(h, c->scal, useDev, tHost, cst, c->flags, c->nreduced);
+}
+
+template <class T>
+int run_dt(dndsg_ctx* c, double cfl, double maxDt, bool copyLast, cudaStream_t s) {
+  HotView<T> h = view<T>(c);
+  k_init_dtmin<<<1, 1, 0, s>>>(c->scal);
+  k_dt_face<T><<<grid_for(c->F), kBlock, 0, s>>>(h);
+  if (copyLast) k_dt_cell<T, true><<<grid_for(c->N), kBlock, 0, s>>>(h, cfl, maxDt, c->scal);
+  else k_dt_cell<T, false><<<grid_for(c->N), kBlock, 0, s>>>(h, cfl, maxDt, c->scal);
+  return 0;
+}
+
+template <class T>
+int run_step(dndsg_ctx* c, double cfl, double tEnd, cudaStream_t s) {
+  run_dt<T>(c, cfl, 1e100, true, s);
+  k_dt_finalize<<<1, 1, 0, s>>>(c->scal, tEnd);
+  const double cst[3] = {0.0, 1.0, 0.5};
+  for (int stg = 0; stg < 3; stg++) {
+    run_vr<T>(c, false, s);
+    if (c->s.limiter) { /* limiter kernels come with the CWBAP path */ }
+    launch_flux<T>(c, 1, 0.0, cst[stg], s);
+    HotView<T> h = view<T>(c);
+    if (stg == 0) k_cell_update<T, 0><<<grid_for(c->N), kBlock, 0, s>>>(h, c->scal);
+    else if (stg == 1) k_cell_update<T, 1><<<grid_for(c->N), kBlock, 0, s>>>(h, c->scal);
+    else k_cell_update<T, 2><<<grid_for(c->N), kBlock, 0, s>>>(h, c->scal);
+  }
+  k_advance_time<<<1, 1, 0, s>>>(c->scal);
+  return 0;
+}
+
+template <class T>
+int run_rhs(dndsg_ctx* c, double t, cudaStream_t s) {
+  launch_flux<T>(c, 0, t, 0.0, s);
+  HotView<T> h = view<T>(c);
+  k_cell_update<T, -1><<<grid_for(c->N), kBlock, 0, s>>>(h, c->scal);
+  return 0;
+}
+
+int check_launch(dndsg_ctx* c) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(c, DNDSG_CUDA_ERROR, std::string("kernel launch: ") + cudaGetErrorString(e));
+  return 0;
+}
+
+int set_device(dndsg_ctx* c) {
+  cudaError_t e = cudaSetDevice(c->device);
+  if (e != cudaSuccess) return fail(c, DNDSG_CUDA_ERROR, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+  return 0;
+}
+
+template <class T>
+int setup_run(dndsg_ctx* c, const dndsg_mesh_desc* md) {
+  const int64_t N = c->N, F = c->F;
+  // ---- host-side topology: per-cell face slots, closure vectors, checks
+  std::vector<int32_t> slots((size_t)aos_size(N, c->nfmax), kEmptySlot);
+  std::vector<int> cnt(N, 0);
+  std::vector<double> closure(2 * N, 0.0);
+  bool hasWallCorr = false;
+  for (int64_t f = 0; f < F; f++) {
+    int32_t L = md->face_cells[2 * f], R = md->face_cells[2 * f + 1];
+    if (L < 0 || L >= N || R >= N || R < -1) return fail(c, DNDSG_BAD_ARGUMENT, "face_cells out of range");
+    int32_t a = md->face_nodes[2 * f], b = md->face_nodes[2 * f + 1];
+    if (a < 0 || b < 0 || a >= md->n_nodes || b >= md->n_nodes) return fail(c, DNDSG_BAD_ARGUMENT, "face_nodes out of range");
+    int bc = md->face_bc[f];
+    if (R < 0 && !(bc == BC_WALL || bc == BC_FAR || bc == BC_WALL_EULER || bc == BC_WALL_NOSLIP || bc == BC_IV_FAR ||
+                   bc == BC_RIEMANN_FAR))
+      return fail(c, DNDSG_UNSUPPORTED, "boundary face with an unsupported BoundaryType");
+    if (R >= 0 && bc != BC_INNER) return fail(c, DNDSG_BAD_ARGUMENT, "interior face with a boundary type");
+    if (bc == BC_WALL_EULER || bc == BC_WALL_NOSLIP) hasWallCorr = true;
+    double dx = md->node_xy[2 * b] - md->node_xy[2 * a], dy = md->node_xy[2 * b + 1] - md->node_xy[2 * a + 1];
+    if (cnt[L] >= c->nfmax) return fail(c, DNDSG_BAD_ARGUMENT, "cell with more faces than nodes");
+    slots[aos(L, cnt[L]++, c->nfmax)] = (int32_t)f;
+    closure[2 * L] += dy; closure[2 * L + 1] += -dx;
+    if (R >= 0) {
+      if (cnt[R] >= c->nfmax) return fail(c, DNDSG_BAD_ARGUMENT, "cell with more faces than nodes");
+      slots[aos(R, cnt[R]++, c->nfmax)] = ~(int32_t)f;
+      closure[2 * R] -= dy; closure[2 * R + 1] -= -dx;
+    }
+  }
+  for (int64_t i = 0; i < N; i++) {
+    int nn = md->cell_nodes[4 * i + 3] < 0 ? 3 : 4;
+    for (int k = 0; k < nn; k++) {
+      int32_t nd = md->cell_nodes[4 * i + k];
+      if (nd < 0 || nd >= md->n_nodes) return fail(c, DNDSG_BAD_ARGUMENT, "cell_nodes out of range");
+    }
+    if (cnt[i] != nn) return fail(c, DNDSG_BAD_ARGUMENT, "cell face count differs from its node count");
+  }
+  c->hasWallCorr = hasWallCorr;
+  // ---- device mesh
+  double* dNode; int32_t *dCellNodes, *dFaceNodes, *dFaceCells; double* dShift = nullptr;
+  int rc = 0;
+  if ((rc = dalloc(c, dNode, sizeof(double) * 2 * md->n_nodes))) return rc;
+  if ((rc = dalloc(c, dCellNodes, sizeof(int32_t) * 4 * N))) return rc;
+  if ((rc = dalloc(c, dFaceNodes, sizeof(int32_t) * 2 * F))) return rc;
+  if ((rc = dalloc(c, dFaceCells, sizeof(int32_t) * 2 * F))) return rc;
+  if ((rc = dalloc(c, c->faceBC, sizeof(int32_t) * F))) return rc;
+  if ((rc = dalloc(c, c->faceL, sizeof(int32_t) * F))) return rc;
+  if ((rc = dalloc(c, c->faceR, sizeof(int32_t) * F))) return rc;
+  DG_CUDA(c, cudaMemcpy(dNode, md->node_xy, sizeof(double) * 2 * md->n_nodes, cudaMemcpyHostToDevice));
+  DG_CUDA(c, cudaMemcpy(dCellNodes, md->cell_nodes, sizeof(int32_t) * 4 * N, cudaMemcpyHostToDevice));
+  DG_CUDA(c, cudaMemcpy(dFaceNodes, md->face_nodes, sizeof(int32_t) * 2 * F, cudaMemcpyHostToDevice));
+  DG_CUDA(c, cudaMemcpy(dFaceCells, md->face_cells, sizeof(int32_t) * 2 * F, cudaMemcpyHostToDevice));
+  DG_CUDA(c, cudaMemcpy(c->faceBC, md->face_bc, sizeof(int32_t) * F, cudaMemcpyHostToDevice));
+  {
+    std::vector<int32_t> l(F), r(F);
+    for (int64_t f = 0; f < F; f++) { l[f] = md->face_cells[2 * f]; r[f] = md->face_cells[2 * f + 1]; }
+    DG_CUDA(c, cudaMemcpy(c->faceL, l.data(), sizeof(int32_t) * F, cudaMemcpyHostToDevice));
+    DG_CUDA(c, cudaMemcpy(c->faceR, r.data(), sizeof(int32_t) * F, cudaMemcpyHostToDevice));
+  }
+  if (md->face_shift) {
+    if ((rc = dalloc(c, dShift, sizeof(double) * 2 * F))) return rc;
+    DG_CUDA(c, cudaMemcpy(dShift, md->face_shift, sizeof(double) * 2 * F, cudaMemcpyHostToDevice));
+  }
+  MeshView m{N, F, dNode, dCellNodes, dFaceNodes, dFaceCells, c->faceBC, dShift};
+  SetupParams p;
+  p.use_local_coord = c->s.use_local_coord; p.anisotropic_lengths = c->s.anisotropic_lengths;
+  p.base_center_type = c->s.base_center_type; p.weight_scheme_geom = c->s.weight_scheme_geom;
+  p.weight_scheme_dir = c->s.weight_scheme_dir; p.tang_weight_direction = c->s.tang_weight_direction;
+  p.tang_weight_mod_loc = c->s.tang_weight_mod_loc; p.weight_len_scale = c->s.weight_len_scale;
+  p.wall_weight = c->s.wall_weight; p.far_weight = c->s.far_weight; p.tang_weight = c->s.tang_weight;
+  p.tang_weight_mod_min = c->s.tang_weight_mod_min; p.tang_weight_mod_power = c->s.tang_weight_mod_power;
+  // ---- per-cell geometry
+  CellSetup* cells;
+  double* bary;
+  int* dBad;
+  if ((rc = dalloc(c, cells, sizeof(CellSetup) * N))) return rc;
+  if ((rc = dalloc(c, c->vol, sizeof(double) * N))) return rc;
+  if ((rc = dalloc(c, bary, sizeof(double) * 2 * N))) return rc;
+  if ((rc = dalloc(c, dBad, sizeof(int)))) return rc;
+  DG_CUDA(c, cudaMemset(dBad, 0, sizeof(int)));
+  k_setup_cell<<<grid_for(N), kBlock>>>(m, p, cells, c->vol, bary, dBad);
+  if ((rc = check_launch(c))) return rc;
+  // ---- faces
+  double* faceW;
+  if ((rc = dalloc(c, faceW, sizeof(double) * 6 * F))) return rc;
+  if ((rc = dalloc(c, c->faceNormal, sizeof(double) * 2 * F))) return rc;
+  if ((rc = dalloc(c, c->faceArea, sizeof(double) * F))) return rc;
+  if ((rc = dalloc(c, c->faceCenter, sizeof(double) * 2 * F))) return rc;
+  if ((rc = dalloc(c, c->faceW0, sizeof(double) * F))) return rc;
+  if ((rc = dalloc(c, c->faceBasis, sizeof(T) * aos_size(F, 30)))) return rc;
+  k_setup_face<T><<<grid_for(F), kBlock>>>(m, p, cells, faceW, c->faceNormal, c->faceArea, c->faceCenter, c->faceW0,
+                                           (T*)c->faceBasis);
+  if ((rc = check_launch(c))) return rc;
+  // ---- VR matrices
+  if ((rc = dalloc(c, c->cellFace, sizeof(int32_t) * slots.size()))) return rc;
+  DG_CUDA(c, cudaMemcpy(c->cellFace, slots.data(), sizeof(int32_t) * slots.size(), cudaMemcpyHostToDevice));
+  if ((rc = dalloc(c, c->vrNbr, sizeof(int32_t) * slots.size()))) return rc;
+  if ((rc = dalloc(c, c->vrMode, sizeof(int32_t) * slots.size()))) return rc;
+  if ((rc = dalloc(c, c->vrFace, sizeof(int32_t) * slots.size()))) return rc;
+  if ((rc = dalloc(c, c->vrOp, sizeof(T) * aos_size(N, c->nfmax * 30)))) return rc;
+  if (hasWallCorr)
+    if ((rc = dalloc(c, c->Ainv, sizeof(double) * 25 * N))) return rc;
+  k_setup_matrices<T><<<grid_for(N), kBlock>>>(m, p, cells, faceW, c->cellFace, c->nfmax, (T*)c->vrOp, c->vrNbr,
+                                               c->vrMode, c->vrFace, c->Ainv, dBad);
+  if ((rc = check_launch(c))) return rc;
+  DG_CUDA(c, cudaDeviceSynchronize());
+  int bad = 0;
+  DG_CUDA(c, cudaMemcpy(&bad, dBad, sizeof(int), cudaMemcpyDeviceToHost));
+  if (bad & 1) return fail(c, DNDSG_SETUP_ERROR, "non-positive cell jacobian (cell not counter-clockwise?)");
+  if (bad & 2) return fail(c, DNDSG_SETUP_ERROR, "VR matrix A_ii is not positive definite");
+  if ((rc = dalloc(c, c->closure, sizeof(double) * 2 * N))) return rc;
+  DG_CUDA(c, cudaMemcpy(c->closure, closure.data(), sizeof(double) * 2 * N, cudaMemcpyHostToDevice));
+  // setup-only buffers are released here
+  for (void* q : {(void*)dNode, (void*)dCellNodes, (void*)dFaceNodes, (void*)dFaceCells, (void*)dShift, (void*)cells,
+                  (void*)bary, (void*)faceW, (void*)dBad}) {
+    if (!q) continue;
+    auto it = std::find(c->allocs.begin(), c->allocs.end(), q);
+    if (it != c->allocs.end()) { cudaFree(q); c->allocs.erase(it); }
+  }
+  // ---- state
+  if ((rc = dalloc(c, c->u, sizeof(double) * 4 * N))) return rc;
+  if ((rc = dalloc(c, c->uLast, sizeof(double) * 4 * N))) return rc;
+  if ((rc = dalloc(c, c->rhs, sizeof(double) * 4 * N))) return rc;
+  if ((rc = dalloc(c, c->dt, sizeof(double) * N))) return rc;
+  if ((rc = dalloc(c, c->urec, sizeof(T) * 20 * N))) return rc;
+  if ((rc = dalloc(c, c->urecNew, sizeof(T) * 20 * N))) return rc;
+  if ((rc = dalloc(c, c->flux, sizeof(double) * 4 * F))) return rc;
+  if ((rc = dalloc(c, c->lamA, sizeof(double) * F))) return rc;
+  if ((rc = dalloc(c, c->dLam, sizeof(double) * F))) return rc;
+  if ((rc = dalloc(c, c->scal, sizeof(double) * S_NSLOT))) return rc;
+  if ((rc = dalloc(c, c->partial, sizeof(double) * 4 * grid_for(N)))) return rc;
+  if ((rc = dalloc(c, c->flags, sizeof(unsigned)))) return rc;
+  if ((rc = dalloc(c, c->nreduced, sizeof(unsigned long long)))) return rc;
+  DG_CUDA(c, cudaMemset(c->u, 0, sizeof(double) * 4 * N));
+  DG_CUDA(c, cudaMemset(c->urec, 0, sizeof(T) * 20 * N));
+  DG_CUDA(c, cudaMemset(c->urecNew, 0, sizeof(T) * 20 * N));
+  DG_CUDA(c, cudaMemset(c->dLam, 0, sizeof(double) * F));
+  DG_CUDA(c, cudaMemset(c->scal, 0, sizeof(double) * S_NSLOT));
+  DG_CUDA(c, cudaMemset(c->flags, 0, sizeof(unsigned)));
+  DG_CUDA(c, cudaMemset(c->nreduced, 0, sizeof(unsigned long long)));
+  DG_CUDA(c, cudaDeviceSynchronize());
+  return 0;
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+extern "C" {
+
+int dndsg_create(const dndsg_mesh_desc* mesh, const dndsg_settings* settings, int device, dndsg_ctx** out) {
+  if (!out) return DNDSG_BAD_ARGUMENT;
+  *out = nullptr;
+  dndsg_ctx* c = new dndsg_ctx();
+  *out = c;
+  if (!mesh || !settings) return fail(c, DNDSG_BAD_ARGUMENT, "null mesh or settings");
+  c->s = *settings;
+  c->device = device;
+  if (c->s.nvars != 4) return fail(c, DNDSG_UNSUPPORTED, "nvars must be 4 (NS_2D)");
+  if (c->s.rec_order != 2) return fail(c, DNDSG_UNSUPPORTED, "rec_order must be 2 (P2)");
+  if (c->s.sor_instead) return fail(c, DNDSG_UNSUPPORTED, "the GPU VR sweep is Jacobi (sor_instead must be 0)");
+  if (c->s.riemann != 1 && c->s.riemann != 2) return fail(c, DNDSG_UNSUPPORTED, "riemann must be 1 (Roe) or 2 (HLLC)");
+  if (c->s.limiter) return fail(c, DNDSG_UNSUPPORTED, "limiter not available in this build");
+  if (mesh->n_cells <= 0 || mesh->n_faces <= 0 || mesh->n_cells > INT32_MAX || mesh->n_faces > INT32_MAX)
+    return fail(c, DNDSG_BAD_ARGUMENT, "mesh sizes out of range");
+  c->N = mesh->n_cells;
+  c->F = mesh->n_faces;
+  c->fp32 = c->s.precision == 1;
+  bool anyQuad = false;
+  for (int64_t i = 0; i < c->N; i++) if (mesh->cell_nodes[4 * i + 3] >= 0) { anyQuad = true; break; }
+  c->nfmax = anyQuad ? 4 : 3;
+  int rc = set_device(c);
+  if (rc) return rc;
+  rc = c->fp32 ? setup_run<float>(c, mesh) : setup_run<double>(c, mesh);
+  return rc;
+}
+
+void dndsg_destroy(dndsg_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  for (void* p : c->allocs) cudaFree(p);
+  delete c;
+}
+
+const char* dndsg_last_error(dndsg_ctx* c) { return c ? c->err.c_str() : "null context"; }
+int64_t dndsg_n_cells(dndsg_ctx* c) { return c ? c->N : -1; }
+int64_t dndsg_n_faces(dndsg_ctx* c) { return c ? c->F : -1; }
+
+int dndsg_set_u(dndsg_ctx* c, const double* u, void* s) {
+  if (!c || !u) return DNDSG_BAD_ARGUMENT;
+  DG_CUDA(c, cudaMemcpyAsync(c->u, u, sizeof(double) * 4 * c->N, cudaMemcpyHostToDevice, st(s)));
+  DG_CUDA(c, cudaStreamSynchronize(st(s)));
+  return 0;
+}
+int dndsg_get_u(dndsg_ctx* c, double* u, void* s) {
+  if (!c || !u) return DNDSG_BAD_ARGUMENT;
+  DG_CUDA(c, cudaMemcpyAsync(u, c->u, sizeof(double) * 4 * c->N, cudaMemcpyDeviceToHost, st(s)));
+  DG_CUDA(c, cudaStreamSynchronize(st(s)));
+  return 0;
+}
+int dndsg_get_dt(dndsg_ctx* c, double* dt, void* s) {
+  if (!c || !dt) return DNDSG_BAD_ARGUMENT;
+  DG_CUDA(c, cudaMemcpyAsync(dt, c->dt, sizeof(double) * c->N, cudaMemcpyDeviceToHost, st(s)));
+  DG_CUDA(c, cudaStreamSynchronize(st(s)));
+  return 0;
+}
+
+int dndsg_set_urec(dndsg_ctx* c, const double* r, void* s) {
+  if (!c || !r) return DNDSG_BAD_ARGUMENT;
+  const int64_t n = 20 * c->N;
+  if (!c->fp32) {
+    DG_CUDA(c, cudaMemcpyAsync(c->urec, r, sizeof(double) * n, cudaMemcpyHostToDevice, st(s)));
+  } else {
+    double* tmp;
+    DG_CUDA(c, cudaMallocAsync((void**)&tmp, sizeof(double) * n, st(s)));
+    DG_CUDA(c, cudaMemcpyAsync(tmp, r, sizeof(double) * n, cudaMemcpyHostToDevice, st(s)));
+    k_cvt_to<float><<<grid_for(n), kBlock, 0, st(s)>>>(tmp, (float*)c->urec, n);
+    DG_CUDA(c, cudaFreeAsync(tmp, st(s)));
+  }
+  DG_CUDA(c, cudaStreamSynchronize(st(s)));
+  return check_launch(c);
+}
+int dndsg_get_urec(dndsg_ctx* c, double* r, void* s) {
+  if (!c || !r) return DNDSG_BAD_ARGUMENT;
+  const int64_t n = 20 * c->N;
+  if (!c->fp32) {
+    DG_CUDA(c, cudaMemcpyAsync(r, c->urec, sizeof(double) * n, cudaMemcpyDeviceToHost, st(s)));
+  } else {
+    double* tmp;
+    DG_CUDA(c, cudaMallocAsync((void**)&tmp, sizeof(double) * n, st(s)));
+    k_cvt_from<float><<<grid_for(n), kBlock, 0, st(s)>>>((const float*)c->urec, tmp, n);
+    DG_CUDA(c, cudaMemcpyAsync(r, tmp, sizeof(double) * n, cudaMemcpyDeviceToHost, st(s)));
+    DG_CUDA(c, cudaFreeAsync(tmp, st(s)));
+  }
+  DG_CUDA(c, cudaStreamSynchronize(st(s)));
+  return check_launch(c);
+}
+
+int dndsg_device_buffer(dndsg_ctx* c, int which, void** ptr, int64_t* bytes) {
+  if (!c || !ptr) return DNDSG_BAD_ARGUMENT;
+  switch (which) {
+    case DNDSG_BUF_U: *ptr = c->u; if (bytes) *bytes = sizeof(double) * 4 * c->N; return 0;
+    case DNDSG_BUF_UREC: *ptr = c->urec; if (bytes) *bytes = (int64_t)c->tsize() * 20 * c->N; return 0;
+    case DNDSG_BUF_RHS: *ptr = c->rhs; if (bytes) *bytes = sizeof(double) * 4 * c->N; return 0;
+    case DNDSG_BUF_DT: *ptr = c->dt; if (bytes) *bytes = sizeof(double) * c->N; return 0;
+  }
+  return fail(c, DNDSG_BAD_ARGUMENT, "unknown buffer id");
+}
+
+int dndsg_get_time(dndsg_ctx* c, double* t, void* s) {
+  if (!c || !t) return DNDSG_BAD_ARGUMENT;
+  DG_CUDA(c, cudaMemcpyAsync(t, c->scal + S_T, sizeof(double), cudaMemcpyDeviceToHost, st(s)));
+  DG_CUDA(c, cudaStreamSynchronize(st(s)));
+  return 0;
+}
+int dndsg_set_time(dndsg_ctx* c, double t, void* s) {
+  if (!c) return DNDSG_BAD_ARGUMENT;
+  DG_CUDA(c, cudaMemcpyAsync(c->scal + S_T, &t, sizeof(double), cudaMemcpyHostToDevice, st(s)));
+  DG_CUDA(c, cudaStreamSynchronize(st(s)));
+  return 0;
+}
+
+int dndsg_vr_jacobi_step(dndsg_ctx* c, int nsweeps, double* inc_out, void* s) {
+  if (!c || nsweeps < 0) return DNDSG_BAD_ARGUMENT;
+  for (int k = 0; k < nsweeps; k++) {
+    bool last = inc_out && k == nsweeps - 1;
+    if (last) k_init_dtmin<<<1, 1, 0, st(s)>>>(c->scal);
+    if (c->fp32) run_vr<float>(c, last, st(s));
+    else run_vr<double>(c, last, st(s));
+  }
+  int rc = check_launch(c);
+  if (rc) return rc;
+  if (inc_out) {
+    double v = 0;
+    DG_CUDA(c, cudaMemcpyAsync(&v, c->scal + S_INC, sizeof(double), cudaMemcpyDeviceToHost, st(s)));
+    DG_CUDA(c, cudaStreamSynchronize(st(s)));
+    *inc_out = v / double(c->N);
+  }
+  return 0;
+}
+
+int dndsg_limiter_wbap(dndsg_ctx* c, int if_all, double* indicator_out, void* s) {
+  return fail(c, DNDSG_UNSUPPORTED, "limiter not available in this build");
+}
+
+int dndsg_eval_dt(dndsg_ctx* c, double cfl, double max_dt, int use_local_dt, double* dt_min_out, void* s) {
+  if (!c) return DNDSG_BAD_ARGUMENT;
+  if (c->fp32) run_dt<float>(c, cfl, max_dt, false, st(s));
+  else run_dt<double>(c, cfl, max_dt, false, st(s));
+  if (!use_local_dt) k_fill_dt<<<grid_for(c->N), kBlock, 0, st(s)>>>(c->dt, c->N, c->scal);
+  int rc = check_launch(c);
+  if (rc) return rc;
+  if (dt_min_out) {
+    unsigned long long bits = 0;
+    DG_CUDA(c, cudaMemcpyAsync(&bits, c->scal + S_DTMIN, sizeof(bits), cudaMemcpyDeviceToHost, st(s)));
+    DG_CUDA(c, cudaStreamSynchronize(st(s)));
+    std::memcpy(dt_min_out, &bits, sizeof(double));
+  }
+  return 0;
+}
+
+int dndsg_eval_rhs(dndsg_ctx* c, double t, double* rhs_out, void* s) {
+  if (!c) return DNDSG_BAD_ARGUMENT;
+  if (c->fp32) run_rhs<float>(c, t, st(s));
+  else run_rhs<double>(c, t, st(s));
+  int rc = check_launch(c);
+  if (rc) return rc;
+  if (rhs_out) {
+    DG_CUDA(c, cudaMemcpyAsync(rhs_out, c->rhs, sizeof(double) * 4 * c->N, cudaMemcpyDeviceToHost, st(s)));
+    DG_CUDA(c, cudaStreamSynchronize(st(s)));
+  }
+  return 0;
+}
+
+int dndsg_ssprk3_step(dndsg_ctx* c, double cfl, double t_end, void* s) {
+  if (!c) return DNDSG_BAD_ARGUMENT;
+  if (c->fp32) run_step<float>(c, cfl, t_end, st(s));
+  else run_step<double>(c, cfl, t_end, st(s));
+  return check_launch(c);
+}
+
+int dndsg_residual(dndsg_ctx* c, int p, int vol_wise, double* out, void* s) {
+  if (!c || !out) return DNDSG_BAD_ARGUMENT;
+  unsigned nb = grid_for(c->N);
+  k_residual<<<nb, kBlock, 0, st(s)>>>(c->rhs, c->vol, c->N, p, vol_wise, c->partial);
+  int rc = check_launch(c);
+  if (rc) return rc;
+  std::vector<double> part(4 * (size_t)nb);
+  DG_CUDA(c, cudaMemcpyAsync(part.data(), c->partial, sizeof(double) * 4 * nb, cudaMemcpyDeviceToHost, st(s)));
+  DG_CUDA(c, cudaStreamSynchronize(st(s)));
+  for (int v = 0; v < 4; v++) {
+    double a = 0;
+    for (unsigned b = 0; b < nb; b++) a = p < 3 ? a + part[4 * b + v] : std::max(a, part[4 * b + v]);
+    out[v] = p < 3 ? std::pow(a, 1.0 / p) : a;
+  }
+  return 0;
+}
+
+int dndsg_face_values(dndsg_ctx* c, double t, double* out, void* s) {
+  if (!c || !out) return DNDSG_BAD_ARGUMENT;
+  double* d;
+  size_t bytes = sizeof(double) * 24 * c->F;
+  DG_CUDA(c, cudaMallocAsync((void**)&d, bytes, st(s)));
+  if (c->fp32) k_face_values<float><<<grid_for(c->F), kBlock, 0, st(s)>>>(view<float>(c), t, d);
+  else k_face_values<double><<<grid_for(c->F), kBlock, 0, st(s)>>>(view<double>(c), t, d);
+  int rc = check_launch(c);
+  if (rc) return rc;
+  DG_CUDA(c, cudaMemcpyAsync(out, d, bytes, cudaMemcpyDeviceToHost, st(s)));
+  DG_CUDA(c, cudaFreeAsync(d, st(s)));
+  DG_CUDA(c, cudaStreamSynchronize(st(s)));
+  return 0;
+}
+
+int dndsg_get_status(dndsg_ctx* c, uint32_t* flags, uint64_t* n_reduced, void* s) {
+  if (!c) return DNDSG_BAD_ARGUMENT;
+  unsigned f = 0;
+  unsigned long long r = 0;
+  DG_CUDA(c, cudaMemcpyAsync(&f, c->flags, sizeof(f), cudaMemcpyDeviceToHost, st(s)));
+  DG_CUDA(c, cudaMemcpyAsync(&r, c->nreduced, sizeof(r), cudaMemcpyDeviceToHost, st(s)));
+  DG_CUDA(c, cudaMemsetAsync(c->flags, 0, sizeof(unsigned), st(s)));
+  DG_CUDA(c, cudaMemsetAsync(c->nreduced, 0, sizeof(unsigned long long), st(s)));
+  DG_CUDA(c, cudaStreamSynchronize(st(s)));
+  if (flags) *flags = f;
+  if (n_reduced) *n_reduced = r;
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,628 @@
+// dndsg_bodies.cuh -- per-cell / per-face bodies of the setup and hot kernels.
+//
+// Each body processes one cell or one face and touches only its own outputs,
+// so a kernel is "one thread per item" around a body.  Data layouts:
+//   * per-cell and per-face operator data: tile-major AoSoA, element e of item
+//     i at ((i/32)*E + e)*32 + i%32 -> a warp reads one contiguous 32-wide row
+//     per element (fully coalesced without shared-memory staging);
+//   * u  [N][4] double, urec [N][5][4] (T), flux [F][4] double: one item's
+//     values are contiguous, so neighbour gathers use whole 16-byte vectors.
+#pragma once
+#include "dndsg_math.cuh"
+
+namespace dg {
+
+DG_HD int64_t aos(int64_t i, int e, int E) { return ((i >> 5) * (int64_t)E + e) * 32 + (i & 31); }
+DG_HD int64_t aos_size(int64_t n, int E) { return ((n + 31) / 32) * 32 * (int64_t)E; }
+
+// VR slot modes (what a cell's face contributes to its Jacobi update,
+// DNDS_FV_VR.hpp:1520-1665)
+enum : int32_t { VR_INNER = 0, VR_FAR = 1, VR_WALL = 2, VR_WALLCORR = 3, VR_EMPTY = 4 };
+constexpr int32_t kEmptySlot = INT32_MIN;  // cellFace slot without a face
+
+// LINE_3 Gauss-Legendre on [-1, 1]
+DG_HD double l3_point(int g) { return g == 0 ? -0.7745966692414834 : (g == 1 ? 0.0 : 0.7745966692414834); }
+DG_HD double l3_weight(int g) { return g == 1 ? 8.0 / 9.0 : 5.0 / 9.0; }
+
+// ---------------------------------------------------------------- setup
+struct SetupParams {
+  int use_local_coord, anisotropic_lengths, base_center_type;
+  int weight_scheme_geom, weight_scheme_dir, tang_weight_direction, tang_weight_mod_loc;
+  double weight_len_scale, wall_weight, far_weight, tang_weight, tang_weight_mod_min, tang_weight_mod_power;
+};
+
+struct CellSetup {
+  int nn;
+  double xy[4][2];
+  double vol;
+  double bary[2];
+  CellFrame fr;
+};
+
+struct MeshView {
+  int64_t N, F;
+  const double* node_xy;
+  const int32_t* cell_nodes;
+  const int32_t* face_nodes;
+  const int32_t* face_cells;
+  const int32_t* face_bc;
+  const double* face_shift;  // may be null
+};
+
+// Tri3 / Quad4 map at parametric (a, b): point and jacobian determinant
+DG_HD void elem_map(const CellSetup& c, double a, double b, double& x, double& y, double& det) {
+  if (c.nn == 3) {
+    x = c.xy[0][0] * (1 - a - b) + c.xy[1][0] * a + c.xy[2][0] * b;
+    y = c.xy[0][1] * (1 - a - b) + c.xy[1][1] * a + c.xy[2][1] * b;
+    det = (c.xy[1][0] - c.xy[0][0]) * (c.xy[2][1] - c.xy[0][1]) - (c.xy[1][1] - c.xy[0][1]) * (c.xy[2][0] - c.xy[0][0]);
+  } else {
+    double N[4] = {(1 - a) * (1 - b) * 0.25, (1 + a) * (1 - b) * 0.25, (1 + a) * (1 + b) * 0.25, (1 - a) * (1 + b) * 0.25};
+    double da[4] = {-(1 - b) * 0.25, (1 - b) * 0.25, (1 + b) * 0.25, -(1 + b) * 0.25};
+    double db[4] = {-(1 - a) * 0.25, -(1 + a) * 0.25, (1 + a) * 0.25, (1 - a) * 0.25};
+    x = y = 0;
+    double xa = 0, ya = 0, xb = 0, yb = 0;
+    for (int k = 0; k < 4; k++) {
+      x += N[k] * c.xy[k][0]; y += N[k] * c.xy[k][1];
+      xa += da[k] * c.xy[k][0]; ya += da[k] * c.xy[k][1];
+      xb += db[k] * c.xy[k][0]; yb += db[k] * c.xy[k][1];
+    }
+    det = xa * yb - ya * xb;
+  }
+}
+// cell quadrature: TRI_4 (Hammer) / QUAD_9 (Gauss) -- the reconstruction's cell schemes
+DG_HD int cell_nq(int nn) { return nn == 3 ? 4 : 9; }
+DG_HD void cell_qp(int nn, int g, double& a, double& b, double& w) {
+  if (nn == 3) {
+    const double P[4][2] = {{1. / 3., 1. / 3.}, {0.6, 0.2}, {0.2, 0.6}, {0.2, 0.2}};
+    a = P[g][0]; b = P[g][1]; w = g == 0 ? -27. / 96. : 25. / 96.;
+  } else {
+    int i = g % 3, j = g / 3;
+    a = l3_point(i); b = l3_point(j); w = l3_weight(i) * l3_weight(j);
+  }
+}
+
+// initMoment (DNDS_FV_VR.cpp:82-181) + the basis frame of FDiffBaseValue
+DG_HD bool setup_cell(int64_t i, const MeshView& m, const SetupParams& p, CellSetup& c) {
+  c.nn = m.cell_nodes[4 * i + 3] < 0 ? 3 : 4;
+  for (int k = 0; k < c.nn; k++) {
+    int32_t nd = m.cell_nodes[4 * i + k];
+    c.xy[k][0] = m.node_xy[2 * nd]; c.xy[k][1] = m.node_xy[2 * nd + 1];
+  }
+  int nq = cell_nq(c.nn);
+  double vol = 0, bx = 0, by = 0;
+  bool ok = true;
+  for (int g = 0; g < nq; g++) {
+    double a, b, w, x, y, det;
+    cell_qp(c.nn, g, a, b, w);
+    elem_map(c, a, b, x, y, det);
+    if (!(det > 0)) ok = false;
+    vol += det * w; bx += x * det * w; by += y * det * w;
+  }
+  c.vol = vol;
+  c.bary[0] = bx / vol; c.bary[1] = by / vol;
+  double ixx = 0, ixy = 0, iyy = 0;
+  for (int g = 0; g < nq; g++) {
+    double a, b, w, x, y, det;
+    cell_qp(c.nn, g, a, b, w);
+    elem_map(c, a, b, x, y, det);
+    double rx = x - c.bary[0], ry = y - c.bary[1];
+    ixx += rx * rx * det * w; ixy += rx * ry * det * w; iyy += ry * ry * det * w;
+  }
+  ixx /= vol; ixy /= vol; iyy /= vol;
+  // basis centre
+  if (p.base_center_type == 0) { c.fr.c[0] = c.bary[0]; c.fr.c[1] = c.bary[1]; }
+  else {
+    double x, y, det;
+    elem_map(c, c.nn == 3 ? 1. / 3. : 0., c.nn == 3 ? 1. / 3. : 0., x, y, det);
+    c.fr.c[0] = x; c.fr.c[1] = y;
+  }
+  if (!p.use_local_coord) {
+    // CoordMinMaxScale: half extents
+    double mnx = c.xy[0][0], mxx = mnx, mny = c.xy[0][1], mxy = mny;
+    for (int k = 1; k < c.nn; k++) {
+      mnx = dmin(mnx, c.xy[k][0]); mxx = dmax(mxx, c.xy[k][0]);
+      mny = dmin(mny, c.xy[k][1]); mxy = dmax(mxy, c.xy[k][1]);
+    }
+    double sx = (mxx - mnx) * 0.5, sy = (mxy - mny) * 0.5;
+    if (!p.anisotropic_lengths) { double s = sqrt(sx * sx + sy * sy); sx = sy = s; }
+    c.fr.Pinv[0][0] = 1.0 / sx; c.fr.Pinv[0][1] = 0; c.fr.Pinv[1][0] = 0; c.fr.Pinv[1][1] = 1.0 / sy;
+  } else {
+    // principal axes of the inertia (largest first), then scale each axis by
+    // the cell's half extent along it (DNDS_FV_VR.hpp:358-410)
+    double hm = 0.5 * (ixx + iyy), hd = 0.5 * (ixx - iyy);
+    double rr = sqrt(hd * hd + ixy * ixy);
+    double e0x = 1, e0y = 0;
+    if (rr > 1e-14 * fabs(hm)) {
+      double lmax = hm + rr;
+      double vx, vy;
+      if (ixx >= iyy) { vx = lmax - iyy; vy = ixy; } else { vx = ixy; vy = lmax - ixx; }
+      double nr = sqrt(vx * vx + vy * vy);
+      e0x = vx / nr; e0y = vy / nr;
+    }
+    double e1x = -e0y, e1y = e0x;
+    // coordinates along e0, e1 are projections (orthonormal frame)
+    double mn0 = 1e300, mx0 = -1e300, mn1 = 1e300, mx1 = -1e300;
+    for (int k = 0; k < c.nn; k++) {
+      double rx = c.xy[k][0] - c.fr.c[0], ry = c.xy[k][1] - c.fr.c[1];
+      double s0 = e0x * rx + e0y * ry, s1 = e1x * rx + e1y * ry;
+      mn0 = dmin(mn0, s0); mx0 = dmax(mx0, s0); mn1 = dmin(mn1, s1); mx1 = dmax(mx1, s1);
+    }
+    double a0 = (mx0 - mn0) * 0.5, a1 = (mx1 - mn1) * 0.5;
+    if (!p.anisotropic_lengths) { double s = sqrt(a0 * a0 + a1 * a1); a0 = a1 = s; }
+    // P = [e0*a0, e1*a1]; Pinv rows = e_k^T / a_k
+    c.fr.Pinv[0][0] = e0x / a0; c.fr.Pinv[0][1] = e0y / a0;
+    c.fr.Pinv[1][0] = e1x / a1; c.fr.Pinv[1][1] = e1y / a1;
+  }
+  for (int k = 0; k < 5; k++) c.fr.moment[k] = 0;
+  double mom[5] = {0, 0, 0, 0, 0};
+  for (int g = 0; g < nq; g++) {
+    double a, b, w, x, y, det, v[5];
+    cell_qp(c.nn, g, a, b, w);
+    elem_map(c, a, b, x, y, det);
+    p2_values(c.fr, x, y, v);
+    for (int k = 0; k < 5; k++) mom[k] += v[k] * det * w;
+  }
+  for (int k = 0; k < 5; k++) c.fr.moment[k] = mom[k] / vol;
+  return ok;
+}
+
+// face geometry: nodes -> unit normal (out of L), length, centre, gauss points
+struct FaceGeom {
+  double nx, ny, area, cx, cy;
+  double gx[3], gy[3];
+};
+DG_HD FaceGeom face_geom(int64_t f, const MeshView& m) {
+  FaceGeom g;
+  int32_t a = m.face_nodes[2 * f], b = m.face_nodes[2 * f + 1];
+  double x0 = m.node_xy[2 * a], y0 = m.node_xy[2 * a + 1], x1 = m.node_xy[2 * b], y1 = m.node_xy[2 * b + 1];
+  double dx = x1 - x0, dy = y1 - y0;
+  g.area = sqrt(dx * dx + dy * dy);
+  g.nx = dy / g.area; g.ny = -dx / g.area;
+  g.cx = 0.5 * (x0 + x1); g.cy = 0.5 * (y0 + y1);
+  for (int q = 0; q < 3; q++) {
+    double s = l3_point(q);
+    g.gx[q] = x0 * (1 - s) * 0.5 + x1 * (1 + s) * 0.5;
+    g.gy[q] = y0 * (1 - s) * 0.5 + y1 * (1 + s) * 0.5;
+  }
+  return g;
+}
+
+// faceWeights (DNDS_FV_VR.cpp:716-888) for P2
+DG_HD void face_weights(int64_t f, const MeshView& m, const SetupParams& p, const FaceGeom& g, const CellSetup* cells,
+                        double W[6]) {
+  int32_t L = m.face_cells[2 * f], R = m.face_cells[2 * f + 1];
+  int bc = m.face_bc[f];
+  double dx, dy;
+  for (int k = 0; k < 6; k++) W[k] = 1.0;
+  if (R >= 0) {
+    double sx = m.face_shift ? m.face_shift[2 * f] : 0.0, sy = m.face_shift ? m.face_shift[2 * f + 1] : 0.0;
+    dx = cells[R].bary[0] + sx - cells[L].bary[0];
+    dy = cells[R].bary[1] + sy - cells[L].bary[1];
+  } else {
+    for (int k = 0; k < 6; k++) W[k] = 0.0;
+    dx = g.cx - cells[L].bary[0];
+    dy = g.cy - cells[L].bary[1];
+    if (bc == BC_WALL || bc == BC_WALL_EULER) W[0] = p.wall_weight;
+    else if (is_far_type(bc)) W[0] = p.far_weight;
+    else if (bc == BC_WALL_NOSLIP) {
+      W[0] = p.wall_weight;
+      double d = g.nx * dx + g.ny * dy;  // first-order wall delta
+      dx = g.nx * d; dy = g.ny * d;
+    }
+  }
+  double D = sqrt(dx * dx + dy * dy), S = g.area, GW = 1;
+  if (p.weight_scheme_geom == 1) GW = pow(1.0 / D, 0.5);
+  else if (p.weight_scheme_geom == 2) GW = pow(1.0 / S, 0.5);
+  else if (p.weight_scheme_geom == 3) GW = pow(S / D, 0.25);
+  if (p.tang_weight_direction == 0) { dx = g.nx * D; dy = g.ny * D; }
+  dx *= p.weight_len_scale; dy *= p.weight_len_scale;
+  // diffs {1, x, y, xx, xy, yy}
+  const int ox[6] = {0, 1, 0, 2, 1, 0}, oy[6] = {0, 0, 1, 0, 1, 2};
+  const double fac[3] = {1, 1, 2}, ncomb[6] = {1, 1, 1, 1, 2, 1}, hqm[3] = {1, 0.4643, 0.1559};
+  for (int k = 0; k < 6; k++) {
+    double pw = pow(dx, ox[k]) * pow(dy, oy[k]);
+    if (p.weight_scheme_dir == 0) W[k] *= GW * pw * ncomb[k] / fac[ox[k] + oy[k]];
+    else W[k] *= GW * pw * hqm[ox[k] + oy[k]];
+  }
+}
+
+DG_HD double tang_modifier(const SetupParams& p, double volL, double volR, double area) {
+  double sL = sqrt(volL) / area, sR = sqrt(volR) / area;
+  double arMax = dmax(1.0, dmax(sL, sR));
+  return pow((1.0 / arMax) * (1 - p.tang_weight_mod_min) + p.tang_weight_mod_min, p.tang_weight_mod_power);
+}
+
+// ---------------------------------------------------------------- hot path
+template <class T>
+struct HotView {
+  int64_t N, F;
+  int nfmax;
+  // cells
+  const double* vol;
+  const double* closure;    // [N][2]
+  const int32_t* cellFace;  // AoSoA E = nfmax: f (cell is left) or ~f (cell is right)
+  const T* vrOp;            // AoSoA E = nfmax*30: per slot 25 A^-1B (row-major) + 5 A^-1b
+  const int32_t* vrNbr;     // AoSoA E = nfmax
+  const int32_t* vrMode;    // AoSoA E = nfmax
+  const int32_t* vrFace;    // AoSoA E = nfmax (face id of the slot)
+  const double* Ainv;       // [N][25] or null
+  // faces
+  const int32_t* faceL;
+  const int32_t* faceR;
+  const int32_t* faceBC;
+  const T* faceBasis;       // AoSoA E = 30: [side][gp][5] value-row basis at face gauss points
+  const double* faceNormal; // [F][2] unit, out of L
+  const double* faceArea;   // [F]
+  const double* faceCenter; // [F][2]
+  const double* faceW0;     // [F] weight 0 (wall corrections)
+  // state
+  double* u;
+  double* uLast;
+  double* rhs;
+  double* dt;
+  const T* urec;
+  T* urecNew;
+  double* flux;             // [F][4]
+  double* lamA;             // [F]
+  double* dLam;             // [F]
+  double gamma;
+  double farU[4];
+  double relax;
+};
+
+template <class T>
+DG_HD void load4(const double* p, double* v) { for (int k = 0; k < 4; k++) v[k] = p[k]; }
+template <class T>
+DG_HD void load_rec(const T* p, T r[5][4]) {
+  for (int q = 0; q < 5; q++)
+    for (int v = 0; v < 4; v++) r[q][v] = p[q * 4 + v];
+}
+
+// one cell of ReconstructionJacobiStep (Jacobi form, DNDS_FV_VR.hpp:1500-1712)
+template <class T, bool RELAX1>
+DG_HD void vr_cell(int64_t i, const HotView<T>& h) {
+  const int64_t E = (int64_t)h.nfmax * 30;
+  double ui[4];
+  load4<T>(&h.u[i * 4], ui);
+  T acc[5][4];
+  if (RELAX1) {
+    for (int q = 0; q < 5; q++) for (int v = 0; v < 4; v++) acc[q][v] = T(0);
+  } else {
+    T r0[5][4];
+    load_rec(&h.urec[i * 20], r0);
+    for (int q = 0; q < 5; q++) for (int v = 0; v < 4; v++) acc[q][v] = T(1 - h.relax) * r0[q][v];
+  }
+  const T relax = T(h.relax);
+  for (int k = 0; k < h.nfmax; k++) {
+    int mode = h.vrMode[aos(i, k, h.nfmax)];
+    if (mode == VR_EMPTY) continue;
+    int32_t j = h.vrNbr[aos(i, k, h.nfmax)];
+    T b[5];
+    for (int r = 0; r < 5; r++) b[r] = h.vrOp[aos(i, k * 30 + 25 + r, (int)E)];
+    if (mode == VR_INNER || mode == VR_FAR) {
+      T rj[5][4];
+      load_rec(&h.urec[(int64_t)j * 20], rj);
+      for (int r = 0; r < 5; r++) {
+        T M[5];
+        for (int q = 0; q < 5; q++) M[q] = h.vrOp[aos(i, k * 30 + r * 5 + q, (int)E)];
+        for (int v = 0; v < 4; v++) {
+          T s = M[0] * rj[0][v] + M[1] * rj[1][v] + M[2] * rj[2][v] + M[3] * rj[3][v] + M[4] * rj[4][v];
+          acc[r][v] += relax * s;
+        }
+      }
+    }
+    if (mode == VR_INNER || mode == VR_WALL) {
+      T du[4];
+      if (mode == VR_INNER) {
+        double uj[4];
+        load4<T>(&h.u[(int64_t)j * 4], uj);
+        for (int v = 0; v < 4; v++) du[v] = T(uj[v] - ui[v]);
+      } else {
+        for (int v = 0; v < 4; v++) du[v] = T(0.0 - ui[v]);
+      }
+      for (int r = 0; r < 5; r++)
+        for (int v = 0; v < 4; v++) acc[r][v] += relax * (du[v] * b[r]);
+    }
+    if (mode == VR_WALLCORR) {
+      // Wall_Euler / Wall_NoSlip: A^-1 * integral of the weighted jump to the wall state
+      int32_t f = h.vrFace[aos(i, k, h.nfmax)];
+      double nx = h.faceNormal[2 * f], ny = h.faceNormal[2 * f + 1];
+      double w0 = h.faceW0[f], area = h.faceArea[f];
+      int bc = h.faceBC[f];
+      T ri[5][4];
+      load_rec(&h.urec[i * 20], ri);
+      double corr[5][4];
+      for (int q = 0; q < 5; q++) for (int v = 0; v < 4; v++) corr[q][v] = 0;
+      for (int g = 0; g < 3; g++) {
+        double phi[5];
+        for (int q = 0; q < 5; q++) phi[q] = (double)h.faceBasis[aos(f, g * 5 + q, 30)];
+        double uBL[4], uBV[4];
+        for (int v = 0; v < 4; v++) {
+          double s = 0;
+          for (int q = 0; q < 5; q++) s += phi[q] * (double)ri[q][v];
+          uBL[v] = s + ui[v];
+        }
+        if (bc == BC_WALL_EULER) {
+          double d = nx * uBL[1] + ny * uBL[2];
+          uBV[0] = uBL[0]; uBV[1] = uBL[1] - nx * d; uBV[2] = uBL[2] - ny * d; uBV[3] = uBL[3];
+        } else {
+          uBV[0] = uBL[0]; uBV[1] = -uBL[1]; uBV[2] = -uBL[2]; uBV[3] = uBL[3];
+        }
+        double jw = 0.5 * area * l3_weight(g);
+        for (int q = 0; q < 5; q++)
+          for (int v = 0; v < 4; v++) corr[q][v] += phi[q] * w0 * w0 * (uBV[v] - ui[v]) * jw;
+      }
+      const double* Ai = &h.Ainv[i * 25];
+      for (int r = 0; r < 5; r++)
+        for (int v = 0; v < 4; v++) {
+          double s = 0;
+          for (int q = 0; q < 5; q++) s += Ai[r * 5 + q] * corr[q][v];
+          acc[r][v] += relax * T(s);
+        }
+    }
+  }
+  T* out = &h.urecNew[i * 20];
+  for (int q = 0; q < 5; q++) for (int v = 0; v < 4; v++) out[q * 4 + v] = acc[q][v];
+}
+
+// reconstructed states at the 3 gauss points of face f (EvaluateRHS, DNDS_FV_EulerEvaluator.cpp:250-360)
+template <class T>
+DG_HD int face_states(int64_t f, const HotView<T>& h, double t, double UL[3][4], double UR[3][4], double& nx,
+                      double& ny, double& area) {
+  int32_t L = h.faceL[f], R = h.faceR[f];
+  nx = h.faceNormal[2 * f]; ny = h.faceNormal[2 * f + 1]; area = h.faceArea[f];
+  double uL[4], uR[4];
+  load4<T>(&h.u[(int64_t)L * 4], uL);
+  T rL[5][4], rR[5][4];
+  load_rec(&h.urec[(int64_t)L * 20], rL);
+  int nred = 0;
+  if (R >= 0) {
+    load4<T>(&h.u[(int64_t)R * 4], uR);
+    load_rec(&h.urec[(int64_t)R * 20], rR);
+  }
+  int bc = h.faceBC[f];
+  for (int g = 0; g < 3; g++) {
+    T phi[5];
+    for (int q = 0; q < 5; q++) phi[q] = h.faceBasis[aos(f, g * 5 + q, 30)];
+    double inc[4];
+    for (int v = 0; v < 4; v++) {
+      T s = phi[0] * rL[0][v] + phi[1] * rL[1][v] + phi[2] * rL[2][v] + phi[3] * rL[3][v] + phi[4] * rL[4][v];
+      inc[v] = (double)s;
+    }
+    nred += compress_rec_part(uL, inc, UL[g]) ? 1 : 0;
+    if (R >= 0) {
+      for (int q = 0; q < 5; q++) phi[q] = h.faceBasis[aos(f, 15 + g * 5 + q, 30)];
+      for (int v = 0; v < 4; v++) {
+        T s = phi[0] * rR[0][v] + phi[1] * rR[1][v] + phi[2] * rR[2][v] + phi[3] * rR[3][v] + phi[4] * rR[4][v];
+        inc[v] = (double)s;
+      }
+      nred += compress_rec_part(uR, inc, UR[g]) ? 1 : 0;
+    } else {
+      boundary_value(bc, UL[g], nx, ny, h.faceCenter[2 * f], h.faceCenter[2 * f + 1], t, h.gamma, h.farU, UR[g]);
+    }
+  }
+  return nred;
+}
+
+// face flux: sum over gauss points of -F(UL,UR).n |n| w (fluxFace, DNDS_FV_EulerEvaluator.hpp:371-591)
+// returns the reduced-order count; bit 0 of *bad is set on non-physical input
+template <class T, int RIEMANN>
+DG_HD int face_flux(int64_t f, const HotView<T>& h, double t, double out[4], bool& bad) {
+  double UL[3][4], UR[3][4], nx, ny, area;
+  int nred = face_states(f, h, t, UL, UR, nx, ny, area);
+  double dl = h.dLam[f];
+  double acc[4] = {0, 0, 0, 0};
+  for (int g = 0; g < 3; g++) {
+    double a[4], b[4], F[4];
+    to_normal_frame(UL[g], nx, ny, a);
+    to_normal_frame(UR[g], nx, ny, b);
+    if (!(a[0] > 0 && b[0] > 0)) bad = true;
+    if (RIEMANN == 2) hllc_flux(a, b, h.gamma, F);
+    else roe_flux(a, b, h.gamma, dl, F);
+    from_normal_frame(F, nx, ny);
+    double jw = 0.5 * area * l3_weight(g);
+    for (int k = 0; k < 4; k++) acc[k] -= F[k] * jw;
+  }
+  for (int k = 0; k < 4; k++) {
+    if (!(acc[k] == acc[k])) bad = true;
+    out[k] = acc[k];
+  }
+  return nred;
+}
+
+// EvaluateDt face part (DNDS_FV_EulerEvaluator.cpp:25-137): lambda_f * area, deltaLambdaFace
+template <class T>
+DG_HD void dt_face(int64_t f, const HotView<T>& h) {
+  int32_t L = h.faceL[f], R = h.faceR[f];
+  double nx = h.faceNormal[2 * f], ny = h.faceNormal[2 * f + 1], area = h.faceArea[f];
+  double UL[4];
+  load4<T>(&h.u[(int64_t)L * 4], UL);
+  double pL, aL2, HL, pR, aR2, HR;
+  double uL = UL[1] / UL[0], vL = UL[2] / UL[0], uR = uL, vR = vL;
+  thermal(UL[3], UL[0], uL * uL + vL * vL, h.gamma, pL, aL2, HL);
+  pR = pL; aR2 = aL2;
+  double rhoMean = UL[0];
+  if (R >= 0) {
+    double UR[4];
+    load4<T>(&h.u[(int64_t)R * 4], UR);
+    rhoMean = (UL[0] + UR[0]) * 0.5;
+    uR = UR[1] / UR[0]; vR = UR[2] / UR[0];
+    thermal(UR[3], UR[0], uR * uR + vR * vR, h.gamma, pR, aR2, HR);
+  }
+  double vn = 0.5 * ((uL + uR) * nx + (vL + vR) * ny);
+  double pMean = (pL + pR) * 0.5;
+  double lam = fabs(vn) + sqrt(h.gamma * pMean / rhoMean);
+  h.lamA[f] = lam * area;
+  h.dLam[f] = fabs((uR - uL) * nx + (vR - vL) * ny) + sqrt(fabs(aR2 - aL2)) * 0.7071;
+}
+
+// EvaluateDt cell part: dt_i = min(CFL V / sum lambda_f A_f, MaxDt)
+template <class T>
+DG_HD double dt_cell(int64_t i, const HotView<T>& h, double cfl, double maxDt) {
+  double lam = 0;
+  for (int k = 0; k < h.nfmax; k++) {
+    int32_t sf = h.cellFace[aos(i, k, h.nfmax)];
+    if (sf == kEmptySlot) continue;
+    int32_t f = sf >= 0 ? sf : ~sf;
+    lam += h.lamA[f];
+  }
+  return dmin(cfl * h.vol[i] / (lam + 1e-100), maxDt);
+}
+
+// rhs of cell i: gather of face fluxes plus the flux-balance term
+// (DNDS_FV_EulerEvaluator.cpp:501-508): -F(u_i) . sum_f n_f A_f / V_i
+template <class T>
+DG_HD void cell_rhs(int64_t i, const HotView<T>& h, double r[4]) {
+  double s[4] = {0, 0, 0, 0};
+  for (int k = 0; k < h.nfmax; k++) {
+    int32_t sf = h.cellFace[aos(i, k, h.nfmax)];
+    if (sf == kEmptySlot) continue;
+    int32_t f = sf >= 0 ? sf : ~sf;
+    const double* fl = &h.flux[(int64_t)f * 4];
+    if (sf >= 0) { for (int v = 0; v < 4; v++) s[v] += fl[v]; }
+    else { for (int v = 0; v < 4; v++) s[v] -= fl[v]; }
+  }
+  double U[4];
+  load4<T>(&h.u[i * 4], U);
+  double ir = 1.0 / U[0];
+  double vx = U[1] * ir, vy = U[2] * ir;
+  double p = (h.gamma - 1) * (U[3] - U[0] * 0.5 * (vx * vx + vy * vy));
+  double cx = h.closure[2 * i], cy = h.closure[2 * i + 1];
+  double Fn[4] = {U[1] * cx + U[2] * cy, (U[1] * vx + p) * cx + U[1] * vy * cy, U[2] * vx * cx + (U[2] * vy + p) * cy,
+                  (U[3] + p) * (vx * cx + vy * cy)};
+  double iv = 1.0 / h.vol[i];
+  for (int v = 0; v < 4; v++) r[v] = (s[v] - Fn[v]) * iv;
+}
+
+}  // namespace dg
+
+namespace dg {
+
+// ---------------------------------------------------------------- setup bodies
+// face part of initBaseDiffCache (DNDS_FV_VR.cpp:367-890): weights, geometry
+// and the value-row basis of both cells at the face gauss points
+template <class T>
+DG_HD void setup_face(int64_t f, const MeshView& m, const SetupParams& p, const CellSetup* cells, double* faceW,
+                      double* normal, double* area, double* center, double* w0, T* basis, double* basisD) {
+  FaceGeom g = face_geom(f, m);
+  double W[6];
+  face_weights(f, m, p, g, cells, W);
+  for (int k = 0; k < 6; k++) faceW[f * 6 + k] = W[k];
+  normal[2 * f] = g.nx; normal[2 * f + 1] = g.ny;
+  area[f] = g.area;
+  center[2 * f] = g.cx; center[2 * f + 1] = g.cy;
+  w0[f] = W[0];
+  int32_t L = m.face_cells[2 * f], R = m.face_cells[2 * f + 1];
+  double sx = m.face_shift ? m.face_shift[2 * f] : 0.0, sy = m.face_shift ? m.face_shift[2 * f + 1] : 0.0;
+  for (int q = 0; q < 3; q++) {
+    double v[5];
+    p2_values(cells[L].fr, g.gx[q], g.gy[q], v);
+    for (int k = 0; k < 5; k++) {
+      basis[aos(f, q * 5 + k, 30)] = (T)v[k];
+      if (basisD) basisD[aos(f, q * 5 + k, 30)] = v[k];
+    }
+    if (R >= 0) p2_values(cells[R].fr, g.gx[q] - sx, g.gy[q] - sy, v);
+    else for (int k = 0; k < 5; k++) v[k] = 0;
+    for (int k = 0; k < 5; k++) {
+      basis[aos(f, 15 + q * 5 + k, 30)] = (T)v[k];
+      if (basisD) basisD[aos(f, 15 + q * 5 + k, 30)] = v[k];
+    }
+  }
+}
+
+// initReconstructionMatVec (DNDS_FV_VR.cpp:892-1154) for one cell:
+// A = sum_faces sum_gp |n| w F(D_i, D_i), B_k = ... F(D_i, D_j), b_k = w0^2 D_i[0];
+// stores A^-1 B_k and A^-1 b_k per face slot.  Returns false if A is not SPD.
+template <class T>
+DG_HD bool setup_cell_matrices(int64_t i, const MeshView& m, const SetupParams& p, const CellSetup* cells,
+                               const double* faceW, const int32_t* cellFace, int nfmax, T* vrOp, double* vrOpD,
+                               int32_t* vrNbr, int32_t* vrMode, int32_t* vrFace, double* Ainv) {
+  const int E = nfmax * 30;
+  double A[5][5];
+  double B[4][5][5], bv[4][5];
+  int mode[4], nbr[4], face[4];
+  for (int r = 0; r < 5; r++) for (int q = 0; q < 5; q++) A[r][q] = 0;
+  for (int k = 0; k < nfmax; k++) {
+    mode[k] = VR_EMPTY; nbr[k] = -1; face[k] = -1;
+    for (int r = 0; r < 5; r++) { bv[k][r] = 0; for (int q = 0; q < 5; q++) B[k][r][q] = 0; }
+    int32_t sf = cellFace[aos(i, k, nfmax)];
+    if (sf == kEmptySlot) continue;
+    int32_t f = sf >= 0 ? sf : ~sf;
+    int side = sf >= 0 ? 0 : 1;
+    int32_t L = m.face_cells[2 * f], R = m.face_cells[2 * f + 1];
+    int32_t j = side == 0 ? R : L;
+    int bc = m.face_bc[f];
+    FaceGeom g = face_geom(f, m);
+    const double* W = &faceW[f * 6];
+    double sx = m.face_shift ? m.face_shift[2 * f] : 0.0, sy = m.face_shift ? m.face_shift[2 * f + 1] : 0.0;
+    // own points: the cell on the right of a periodic face sees the face shifted back
+    double ox = side == 1 ? -sx : 0.0, oy = side == 1 ? -sy : 0.0;
+    double jx = side == 0 ? -sx : 0.0, jy = side == 0 ? -sy : 0.0;
+    double tm = tang_modifier(p, cells[L].vol, cells[R >= 0 ? R : L].vol, g.area);
+    FaceFunctional Fn = make_functional(W, g.nx, g.ny, p.tang_weight, tm, p.tang_weight_mod_loc);
+    bool far = R < 0 && is_far_type(bc);
+    for (int q = 0; q < 3; q++) {
+      double jw = 0.5 * g.area * l3_weight(q);
+      double D[6][5], P[6][5];
+      p2_diffs(cells[i].fr, g.gx[q] + ox, g.gy[q] + oy, D);
+      functional_proj(Fn, D, P);
+      for (int r = 0; r < 5; r++)
+        for (int c = 0; c < 5; c++) {
+          double s = 0;
+          for (int a = 0; a < 6; a++) s += P[a][r] * P[a][c];
+          A[r][c] += s * jw;
+          if (far) B[k][r][c] += s * jw;
+        }
+      if (j >= 0) {
+        double Dj[6][5], Pj[6][5];
+        p2_diffs(cells[j].fr, g.gx[q] + jx, g.gy[q] + jy, Dj);
+        functional_proj(Fn, Dj, Pj);
+        for (int r = 0; r < 5; r++)
+          for (int c = 0; c < 5; c++) {
+            double s = 0;
+            for (int a = 0; a < 6; a++) s += P[a][r] * Pj[a][c];
+            B[k][r][c] += s * jw;
+          }
+      }
+      for (int r = 0; r < 5; r++) bv[k][r] += W[0] * W[0] * D[0][r] * jw;
+    }
+    face[k] = f;
+    if (j >= 0) { mode[k] = VR_INNER; nbr[k] = j; }
+    else if (far) { mode[k] = VR_FAR; nbr[k] = (int32_t)i; }
+    else if (bc == BC_WALL) { mode[k] = VR_WALL; nbr[k] = -1; }
+    else if (bc == BC_WALL_EULER || bc == BC_WALL_NOSLIP) { mode[k] = VR_WALLCORR; nbr[k] = -1; }
+    else { mode[k] = VR_EMPTY; }
+  }
+  double Lc[5][5];
+  for (int r = 0; r < 5; r++) for (int q = 0; q < 5; q++) Lc[r][q] = A[r][q];
+  if (!chol5(Lc)) return false;
+  double Ai[5][5];
+  for (int c = 0; c < 5; c++) {
+    double col[5];
+    for (int r = 0; r < 5; r++) col[r] = r == c ? 1.0 : 0.0;
+    chol5_solve_vec(Lc, col);
+    for (int r = 0; r < 5; r++) Ai[r][c] = col[r];
+  }
+  if (Ainv)
+    for (int r = 0; r < 5; r++) for (int q = 0; q < 5; q++) Ainv[i * 25 + r * 5 + q] = Ai[r][q];
+  for (int k = 0; k < nfmax; k++) {
+    vrNbr[aos(i, k, nfmax)] = nbr[k];
+    vrMode[aos(i, k, nfmax)] = mode[k];
+    vrFace[aos(i, k, nfmax)] = face[k];
+    for (int r = 0; r < 5; r++) {
+      for (int c = 0; c < 5; c++) {
+        double s = 0;
+        for (int t = 0; t < 5; t++) s += Ai[r][t] * B[k][t][c];
+        vrOp[aos(i, k * 30 + r * 5 + c, E)] = (T)s;
+        if (vrOpD) vrOpD[aos(i, k * 30 + r * 5 + c, E)] = s;
+      }
+      double s = 0;
+      for (int t = 0; t < 5; t++) s += Ai[r][t] * bv[k][t];
+      vrOp[aos(i, k * 30 + 25 + r, E)] = (T)s;
+      if (vrOpD) vrOpD[aos(i, k * 30 + 25 + r, E)] = s;
+    }
+  }
+  return true;
+}
+
+}  // namespace dg

@@ -1,0 +1,169 @@
+"""Host-side mirror of DNDS's solver/evaluator call surface over the C ABI.
+
+``Solver`` owns one ``dndsg_ctx``: the mesh, the FP64 VR setup and the
+resident state on one GPU.  Its methods carry the reference's member-function
+names and argument meanings:
+
+* ``ReconstructionJacobiStep``      VRFiniteVolume2D, DNDS_FV_VR.hpp:1474-1713
+* ``ReconstructionWBAPLimitFacialV3`` VRFiniteVolume2D, DNDS_FV_VR.hpp:2053-2329
+* ``EvaluateDt``                    EulerEvaluator, DNDS_FV_EulerEvaluator.cpp:14-183
+* ``EvaluateRHS``                   EulerEvaluator, DNDS_FV_EulerEvaluator.cpp:198-640
+* ``EvaluateResidual``              EulerEvaluator, DNDS_FV_EulerEvaluator.cpp:1557-1592
+* ``ssprk3_step``                   ExplicitSSPRK3LocalDt::Step with the EulerSolver stage body
+
+Where the reference aborts (``DNDS_assert``), these raise ``DndsgError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .mesh import Mesh
+from .settings import make_settings
+
+BUF_U, BUF_UREC, BUF_RHS, BUF_DT = 0, 1, 2, 3
+
+
+class DndsgError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"dndsg error {code}: {msg}")
+        self.code = code
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class Solver:
+    def __init__(self, mesh: Mesh, cfg: dict, device: int = 0, precision: int | None = None, stream=None):
+        self.L = _lib.lib()
+        s = make_settings(cfg)
+        if precision is not None:
+            s.precision = int(precision)
+        s.sor_instead = 0
+        self.settings = s
+        self.mesh = mesh
+        self.stream = C.c_void_p(stream) if stream else None
+        self._keep = [mesh.node_xy, mesh.cell_nodes, mesh.face_nodes, mesh.face_cells, mesh.face_bc, mesh.face_shift]
+        md = _lib.MeshDesc(mesh.n_nodes, mesh.n_cells, mesh.n_faces, *[_p(a) for a in self._keep])
+        h = C.c_void_p()
+        rc = self.L.dndsg_create(C.byref(md), C.byref(s), device, C.byref(h))
+        self.h = h
+        if rc != 0:
+            msg = self.L.dndsg_last_error(h).decode() if h else "no context"
+            if h:
+                self.L.dndsg_destroy(h)
+            self.h = None
+            raise DndsgError(rc, msg)
+        self.N = mesh.n_cells
+        self.F = mesh.n_faces
+        self.nv = 4
+
+    # ------------------------------------------------------------------ lifetime
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.dndsg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def _check(self, rc: int):
+        if rc != 0:
+            raise DndsgError(rc, self.L.dndsg_last_error(self.h).decode())
+
+    # ------------------------------------------------------------------ state
+    def set_u(self, u):
+        u = np.ascontiguousarray(u, dtype=np.float64).reshape(self.N, 4)
+        self._check(self.L.dndsg_set_u(self.h, _p(u), self.stream))
+
+    def get_u(self, out: np.ndarray | None = None) -> np.ndarray:
+        u = np.empty((self.N, 4)) if out is None else out
+        assert u.dtype == np.float64 and u.flags.c_contiguous and u.size == self.N * 4
+        self._check(self.L.dndsg_get_u(self.h, _p(u), self.stream))
+        return u
+
+    def set_urec(self, r):
+        r = np.ascontiguousarray(r, dtype=np.float64).reshape(self.N, 5, 4)
+        self._check(self.L.dndsg_set_urec(self.h, _p(r), self.stream))
+
+    def get_urec(self) -> np.ndarray:
+        r = np.empty((self.N, 5, 4))
+        self._check(self.L.dndsg_get_urec(self.h, _p(r), self.stream))
+        return r
+
+    def get_dt(self) -> np.ndarray:
+        d = np.empty(self.N)
+        self._check(self.L.dndsg_get_dt(self.h, _p(d), self.stream))
+        return d
+
+    @property
+    def time(self) -> float:
+        t = C.c_double()
+        self._check(self.L.dndsg_get_time(self.h, C.byref(t), self.stream))
+        return t.value
+
+    @time.setter
+    def time(self, t: float):
+        self._check(self.L.dndsg_set_time(self.h, float(t), self.stream))
+
+    def device_buffer(self, which: int):
+        p = C.c_void_p()
+        n = C.c_int64()
+        self._check(self.L.dndsg_device_buffer(self.h, which, C.byref(p), C.byref(n)))
+        return p.value, n.value
+
+    # ------------------------------------------------------------------ reference-named operations
+    def ReconstructionJacobiStep(self, nsweeps: int = 1, with_increment: bool = False):
+        inc = C.c_double()
+        self._check(self.L.dndsg_vr_jacobi_step(self.h, nsweeps, C.byref(inc) if with_increment else None,
+                                                self.stream))
+        return inc.value if with_increment else None
+
+    def ReconstructionWBAPLimitFacialV3(self, if_all: bool = False, indicator: bool = False):
+        ind = np.empty(self.N) if indicator else None
+        self._check(self.L.dndsg_limiter_wbap(self.h, int(if_all), _p(ind) if indicator else None, self.stream))
+        return ind
+
+    def EvaluateDt(self, cfl: float, max_dt: float = 1e100, use_local_dt: bool = False) -> float:
+        dmin = C.c_double()
+        self._check(self.L.dndsg_eval_dt(self.h, cfl, max_dt, int(use_local_dt), C.byref(dmin), self.stream))
+        return dmin.value
+
+    def EvaluateRHS(self, t: float = 0.0, copy: bool = True):
+        rhs = np.empty((self.N, 4)) if copy else None
+        self._check(self.L.dndsg_eval_rhs(self.h, float(t), _p(rhs) if copy else None, self.stream))
+        return rhs
+
+    def EvaluateResidual(self, p: int = 1, vol_wise: bool = False) -> np.ndarray:
+        out = np.empty(4)
+        self._check(self.L.dndsg_residual(self.h, int(p), int(vol_wise), _p(out), self.stream))
+        return out
+
+    def ssprk3_step(self, cfl: float, t_end: float = 1e300):
+        self._check(self.L.dndsg_ssprk3_step(self.h, cfl, t_end, self.stream))
+
+    def face_values(self, t: float = 0.0) -> np.ndarray:
+        out = np.empty((self.F, 3, 2, 4))
+        self._check(self.L.dndsg_face_values(self.h, float(t), _p(out), self.stream))
+        return out
+
+    def status(self):
+        f = C.c_uint32()
+        n = C.c_uint64()
+        self._check(self.L.dndsg_get_status(self.h, C.byref(f), C.byref(n), self.stream))
+        return f.value, n.value
+
+    def run_to(self, t_end: float, cfl: float, max_steps: int = 10**9) -> int:
+        """SSP-RK3 steps until the device clock reaches t_end (last step clipped)."""
+        steps = 0
+        chunk = 16
+        while steps < max_steps:
+            for _ in range(min(chunk, max_steps - steps)):
+                self.ssprk3_step(cfl, t_end)
+                steps += 1
+            if self.time >= t_end - 1e-12:
+                break
+        return steps

@@ -1,0 +1,167 @@
+/*
+ * dndsg.h -- C ABI of the B200 (sm_100a) implementation of the DNDS
+ * residual-evaluation hot path: the variational-reconstruction (VR) Jacobi
+ * sweep, the CWBAP limiter and the face Gauss-point Riemann flux with scatter
+ * to cells, plus the SSP-RK3 stage composition that drives them.
+ *
+ * Every entry point returns 0 on success and a non-zero dndsg_status code on
+ * failure; nothing throws or aborts.  dndsg_last_error() gives the message.
+ * Arrays passed as host pointers are plain C arrays in the layouts stated
+ * below; the state itself stays resident on the GPU inside the context.
+ *
+ * The reference exposes this path as C++ templates, not a plugin ABI; each
+ * function below names the reference member function it replaces
+ * (file:line inside the DNDS repository).
+ */
+#ifndef DNDSG_H
+#define DNDSG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum dndsg_status {
+  DNDSG_OK = 0,
+  DNDSG_BAD_ARGUMENT = 1,
+  DNDSG_CUDA_ERROR = 2,
+  DNDSG_UNSUPPORTED = 3,
+  DNDSG_NUMERIC_ERROR = 4, /* NaN / non-positive state seen by a kernel */
+  DNDSG_SETUP_ERROR = 5    /* degenerate mesh or singular VR matrix */
+};
+
+/* Mesh topology and geometry.  Replaces CompactFacedMeshSerialRW
+ * (DNDS_Mesh.hpp:634-1906) as the input of the solver.
+ *   node_xy    [n_nodes][2]
+ *   cell_nodes [n_cells][4]  counter-clockwise, slot 3 = -1 for a triangle
+ *   face_nodes [n_faces][2]  right-hand normal of node0->node1 points out of the left cell
+ *   face_cells [n_faces][2]  (left, right), right = -1 on a boundary face
+ *   face_bc    [n_faces]     BoundaryType (DNDS_Mesh.hpp:21-35): -1 inner, 1 Wall,
+ *                            2 Farfield, 3 Wall_Euler, 4 Wall_NoSlip,
+ *                            -4 Special_IVFar, -5 Special_2DRiemannFar
+ *   face_shift [n_faces][2]  translation that brings the right cell next to a
+ *                            periodic face (NULL: no periodic faces)
+ * Indices are int32 (meshes up to 2^31-1 cells / faces). */
+typedef struct {
+  int64_t n_nodes, n_cells, n_faces;
+  const double* node_xy;
+  const int32_t* cell_nodes;
+  const int32_t* face_nodes;
+  const int32_t* face_cells;
+  const int32_t* face_bc;
+  const double* face_shift;
+} dndsg_mesh_desc;
+
+/* The subset of the reference's JSON settings the path reads:
+ * VRFiniteVolume2D::Setting (DNDS_FV_VR.hpp:170-230) and
+ * EulerEvaluator::Setting (DNDS_FV_EulerEvaluator.hpp:138-194). */
+typedef struct {
+  int32_t nvars;                 /* 4 = NS_2D */
+  int32_t rec_order;             /* 2 = P2 (5 coefficients per variable) */
+  int32_t riemann;               /* 1 Roe (Harten-Yee), 2 HLLC */
+  int32_t sor_instead;           /* must be 0: the GPU sweep is a Jacobi sweep */
+  double jacobi_relax;
+  double tang_weight;
+  double tang_weight_mod_min;
+  double tang_weight_mod_power;
+  int32_t tang_weight_mod_loc;
+  int32_t tang_weight_direction; /* 0 Norm, 1 Bary */
+  int32_t base_center_type;      /* 0 Bary, 1 Param */
+  int32_t use_local_coord;
+  int32_t anisotropic_lengths;
+  int32_t weight_scheme_geom;    /* 0 None, 1 D, 2 S, 3 SDHQM */
+  int32_t weight_scheme_dir;     /* 0 None, 1 optHQM */
+  int32_t limiter;               /* 0 none, 1 CWBAP limiter in every stage */
+  double weight_len_scale;
+  double wall_weight;
+  double far_weight;
+  double wbap_smooth_indicator_scale;
+  double wbap_n_std;
+  double gamma;
+  double far_field[6];           /* farFieldStaticValue (conservative) */
+  int32_t n_threads;             /* unused by the GPU path */
+  int32_t precision;             /* 0 FP64 throughout, 1 FP32 bulk (FP64 means/norms) */
+} dndsg_settings;
+
+typedef struct dndsg_ctx dndsg_ctx;
+
+/* device buffers reachable through dndsg_device_buffer */
+enum dndsg_buffer {
+  DNDSG_BUF_U = 0,    /* double [n_cells][nvars] cell means */
+  DNDSG_BUF_UREC = 1, /* double or float [n_cells][5][nvars] VR coefficients */
+  DNDSG_BUF_RHS = 2,  /* double [n_cells][nvars] */
+  DNDSG_BUF_DT = 3    /* double [n_cells] */
+};
+
+/* Build the context on CUDA device `device`: uploads the mesh and runs the
+ * FP64 VR setup on the GPU.  Replaces ImplicitFiniteVolume2D's constructor
+ * (DNDS_FV_VR.hpp:29-102), VRFiniteVolume2D::Initialization
+ * (DNDS_FV_VR.cpp:3-13) and the EulerEvaluator constructor
+ * (DNDS_FV_EulerEvaluator.hpp:196-365).  On failure *out may still hold a
+ * context that carries the error message; destroy it. */
+int dndsg_create(const dndsg_mesh_desc* mesh, const dndsg_settings* settings, int device, dndsg_ctx** out);
+void dndsg_destroy(dndsg_ctx* ctx);
+const char* dndsg_last_error(dndsg_ctx* ctx);
+int64_t dndsg_n_cells(dndsg_ctx* ctx);
+int64_t dndsg_n_faces(dndsg_ctx* ctx);
+
+/* State transfer between host arrays and the resident device state.  `stream`
+ * is a cudaStream_t (NULL = legacy default stream); the call returns after the
+ * copy has completed.  u is [n_cells][nvars] (ArrayDOFV order); urec is
+ * [n_cells][5][nvars] (coefficient-major per cell), in the context's basis. */
+int dndsg_set_u(dndsg_ctx* ctx, const double* u, void* stream);
+int dndsg_get_u(dndsg_ctx* ctx, double* u, void* stream);
+int dndsg_set_urec(dndsg_ctx* ctx, const double* urec, void* stream);
+int dndsg_get_urec(dndsg_ctx* ctx, double* urec, void* stream);
+int dndsg_get_dt(dndsg_ctx* ctx, double* dt, void* stream);
+int dndsg_device_buffer(dndsg_ctx* ctx, int which, void** ptr, int64_t* bytes);
+int dndsg_get_time(dndsg_ctx* ctx, double* t, void* stream);
+int dndsg_set_time(dndsg_ctx* ctx, double t, void* stream);
+
+/* VRFiniteVolume2D::ReconstructionJacobiStep (DNDS_FV_VR.hpp:1474-1713):
+ * nsweeps Jacobi sweeps on the resident u / urec.  If inc_out is not NULL it
+ * receives sum ||urec_new - urec||^2 / n_cells of the last sweep (FP64). */
+int dndsg_vr_jacobi_step(dndsg_ctx* ctx, int nsweeps, double* inc_out, void* stream);
+
+/* VRFiniteVolume2D::ReconstructionWBAPLimitFacialV3 (DNDS_FV_VR.hpp:2053-2329):
+ * CWBAP limiting of the resident urec in place.  indicator_out (nullable) gets
+ * the smoothness indicator per cell [n_cells]. */
+int dndsg_limiter_wbap(dndsg_ctx* ctx, int if_all, double* indicator_out, void* stream);
+
+/* EulerEvaluator::EvaluateDt (DNDS_FV_EulerEvaluator.cpp:14-183): per-cell dt
+ * into DNDSG_BUF_DT and the face spectral data used by the Roe entropy fix.
+ * dt_min_out (nullable) receives the global minimum. */
+int dndsg_eval_dt(dndsg_ctx* ctx, double cfl, double max_dt, int use_local_dt, double* dt_min_out, void* stream);
+
+/* EulerEvaluator::EvaluateRHS (DNDS_FV_EulerEvaluator.cpp:198-640) on the
+ * resident u / urec at time t, into DNDSG_BUF_RHS; rhs_out (nullable) gets a
+ * host copy [n_cells][nvars]. */
+int dndsg_eval_rhs(dndsg_ctx* ctx, double t, double* rhs_out, void* stream);
+
+/* One explicit SSP-RK3 step: ExplicitSSPRK3LocalDt::Step (DNDS_ODE.hpp:131-177)
+ * with the EulerSolver stage body frhs (DNDS_FV_EulerSolver.hpp:713-837):
+ * EvaluateDt (global dt, clipped so that t does not pass t_end), then per
+ * stage one VR Jacobi sweep, the limiter when enabled, EvaluateRHS and the
+ * stage update.  Time lives on the device and advances by the step's dt, so
+ * the call is asynchronous and can be captured in a CUDA graph. */
+int dndsg_ssprk3_step(dndsg_ctx* ctx, double cfl, double t_end, void* stream);
+
+/* EulerEvaluator::EvaluateResidual (DNDS_FV_EulerEvaluator.cpp:1557-1592) of
+ * DNDSG_BUF_RHS: p < 3 gives the p-norm (volume-weighted when vol_wise), else
+ * the max norm; out [nvars] (host), FP64. */
+int dndsg_residual(dndsg_ctx* ctx, int p, int vol_wise, double* out, void* stream);
+
+/* Diagnostic: reconstructed, positivity-compressed states at every face Gauss
+ * point, out [n_faces][3][2][nvars] (side 1 of a boundary face = boundary
+ * state), evaluated as in EvaluateRHS (DNDS_FV_EulerEvaluator.cpp:250-360). */
+int dndsg_face_values(dndsg_ctx* ctx, double t, double* out, void* stream);
+
+/* Error flags raised by kernels since the last call (bit 0: NaN or
+ * non-positive density/pressure in a flux; bit 1: reduced-order face point). */
+int dndsg_get_status(dndsg_ctx* ctx, uint32_t* flags, uint64_t* n_reduced, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DNDSG_H */

@@ -1,0 +1,148 @@
+"""GPU parity of the CUDA path (through the C ABI) against the FP64 oracle.
+
+Tolerances: FP64 GPU path vs FP64 oracle, relative to the field's max
+magnitude, 1e-11 for one evaluation and 1e-10 after a few RK steps (the two
+differ only in summation order, FMA contraction and the 5x5 solver).  The
+FP32-bulk path is held to 2e-6 (relative) on single evaluations.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from dnds_b200 import geometry as G
+from dnds_b200 import mesh as M
+from dnds_b200 import settings as S
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+pytestmark = pytest.mark.gpu
+
+
+def _solver(m, cfg, precision=0):
+    from dnds_b200.solver import Solver
+
+    return Solver(m, cfg, precision=precision)
+
+
+def _golden_case(name):
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLDEN, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    mk, pre, _ = mg.CASES[name]
+    return mk(), S.preset(pre, useLimiter=False), np.load(os.path.join(GOLDEN, f"{name}.npz"))
+
+
+def _rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+CASES = ["vortex_quad10", "vortex_tri8_jitter", "riemann_tri8", "eulerwall_quad6x5", "farfield_tri6x5"]
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_fp64_matches_golden(name):
+    m, cfg, ref = _golden_case(name)
+    s = _solver(m, cfg, 0)
+    s.set_u(ref["u0"])
+    s.ReconstructionJacobiStep(3)
+    assert _rel(s.face_values(0.1), ref["face_values"]) < 1e-11
+    dtmin = s.EvaluateDt(0.5, use_local_dt=False)
+    assert abs(dtmin - float(ref["dtmin"])) < 1e-13 * float(ref["dtmin"])
+    assert _rel(s.get_dt(), ref["dt"]) < 1e-13
+    rhs = s.EvaluateRHS(0.1)
+    assert _rel(rhs, ref["rhs"]) < 1e-11
+    flags, _ = s.status()
+    assert flags == 0
+    # two SSP-RK3 steps from u0 and a zero reconstruction
+    s.set_u(ref["u0"])
+    s.set_urec(np.zeros((m.n_cells, 5, 4)))
+    s.time = 0.0
+    for _ in range(2):
+        s.ssprk3_step(0.5, 1e300)
+    assert _rel(s.get_u(), ref["u_rk2"]) < 1e-12
+    assert abs(s.time - float(ref["t_rk2"])) < 1e-14
+
+
+@pytest.mark.parametrize("name", ["vortex_tri8_jitter", "riemann_tri8", "eulerwall_quad6x5"])
+def test_fp32_bulk_close_to_golden(name):
+    m, cfg, ref = _golden_case(name)
+    s = _solver(m, cfg, 1)
+    s.set_u(ref["u0"])
+    s.ReconstructionJacobiStep(3)
+    assert _rel(s.face_values(0.1), ref["face_values"]) < 2e-6
+    s.EvaluateDt(0.5, use_local_dt=True)
+    rhs = s.EvaluateRHS(0.1)
+    assert _rel(rhs, ref["rhs"]) < 2e-5
+
+
+def test_vortex_c1_against_oracle(oracle_lib):
+    """40x40 periodic quads, P2 VR + Roe, SSP-RK3 CFL 0.5: 20 steps GPU vs oracle."""
+    m = M.vortex_mesh(40, False)
+    cfg = S.preset("vortex")
+    u0 = G.isentropic_vortex(m)
+    o = oracle_lib.Oracle(m, cfg)
+    o.set_u(u0)
+    s = _solver(m, cfg, 0)
+    s.set_u(u0)
+    t = 0.0
+    for _ in range(20):
+        _, d = o.eval_dt(0.5)
+        o.ssprk3_step(d, t)
+        t += d
+        s.ssprk3_step(0.5, 1e300)
+    assert abs(s.time - t) < 1e-13 * t
+    assert _rel(s.get_u(), o.get_u()) < 1e-10
+    s.EvaluateRHS(s.time)
+    ro, _ = o.eval_rhs(t)
+    for p in (1, 2, 3):
+        np.testing.assert_allclose(s.EvaluateResidual(p, p == 2), o.residual(ro, p, p == 2), rtol=1e-9)
+
+
+def test_vr_increment_and_buffers():
+    m = M.vortex_mesh(16, True, jitter=0.2)
+    s = _solver(m, S.preset("vortex"), 0)
+    s.set_u(G.isentropic_vortex(m))
+    inc = [s.ReconstructionJacobiStep(1, with_increment=True) for _ in range(30)]
+    assert inc[0] > 0 and inc[-1] < inc[0] * 1e-2
+    p, nbytes = s.device_buffer(0)
+    assert p and nbytes == m.n_cells * 32
+
+
+def test_full_size_vortex_properties():
+    """The 2,097,152-triangle jittered periodic vortex mesh: free-stream
+    preservation and discrete conservation of one RHS evaluation, both precisions."""
+    m = M.vortex_mesh(1024, True, jitter=0.2, seed=1234)
+    for prec in (0, 1):
+        s = _solver(m, S.preset("vortex"), prec)
+        s.set_u(np.tile([1.0, 1.0, 1.0, 3.5], (m.n_cells, 1)))
+        s.ReconstructionJacobiStep(2)
+        s.EvaluateDt(0.5)
+        rhs = s.EvaluateRHS(0.0)
+        assert np.abs(rhs).max() < (1e-9 if prec == 0 else 2e-3)
+        s.set_u(G.isentropic_vortex(m))
+        s.ReconstructionJacobiStep(2)
+        s.EvaluateDt(0.5)
+        rhs = s.EvaluateRHS(0.0)
+        vol = np.zeros(m.n_cells)
+        pts, wts = G.cell_quadrature(m)
+        vol = wts.sum(1)
+        tot = (rhs * vol[:, None]).sum(0)
+        assert np.abs(tot).max() < 1e-10 * np.abs(rhs * vol[:, None]).sum()
+        flags, nred = s.status()
+        assert flags == 0 and nred == 0
+        s.close()
+
+
+def test_bad_arguments_fail_loudly():
+    from dnds_b200.solver import DndsgError
+
+    m = M.vortex_mesh(4, False)
+    cfg = S.preset("vortex")
+    bad = M.Mesh(m.node_xy, m.cell_nodes, m.face_nodes, m.face_cells.copy(), m.face_bc, m.face_shift)
+    bad.face_cells[0, 0] = m.n_cells + 5
+    with pytest.raises(DndsgError):
+        _solver(bad, cfg)
+    with pytest.raises(DndsgError):
+        _solver(m, S.preset("vortex", recOrder=3))
