@@ -28,6 +28,8 @@ struct dndsg_ctx {
   int device = 0;
   dndsg_settings s{};
   int64_t N = 0, F = 0;
+  int64_t Fi = 0;                // faces [0, Fi) are interior, [Fi, F) boundary (internal order)
+  std::vector<int64_t> facePerm; // internal face id -> caller's face id
   int nfmax = 3;
   bool fp32 = false;
   bool hasWallCorr = false;
@@ -120,7 +122,7 @@ __global__ void k_setup_matrices(MeshView m, SetupParams p, const CellSetup* cel
 
 // ------------------------------------------------------------------ hot kernels
 template <class T, bool RELAX1, bool INC>
-__global__ void __launch_bounds__(kBlock) k_vr(HotView<T> h, double* incAcc) {
+__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 2 : 1) k_vr(HotView<T> h, double* incAcc) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   double d2 = 0;
   if (i < h.N) {
@@ -142,16 +144,18 @@ __device__ __forceinline__ double stage_time(const double* scal, int useDev, dou
   return useDev ? scal[S_T] + c * scal[S_DT] : tHost;
 }
 
-template <class T, int RIEMANN>
-__global__ void __launch_bounds__(kBlock) k_face_flux(HotView<T> h, const double* scal, int useDev, double tHost,
-                                                      double c, unsigned* flags, unsigned long long* nred) {
-  int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+// faces [f0, f1): interior faces first (BND = false), then boundary faces
+template <class T, int RIEMANN, bool BND>
+__global__ void __launch_bounds__(kBlock, 2) k_face_flux(HotView<T> h, int64_t f0, int64_t f1, const double* scal,
+                                                         int useDev, double tHost, double c, unsigned* flags,
+                                                         unsigned long long* nred) {
+  int64_t f = f0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   int r = 0;
   bool bad = false;
-  if (f < h.F) {
+  if (f < f1) {
     double out[4];
     double t = stage_time(scal, useDev, tHost, c);
-    r = face_flux<T, RIEMANN>(f, h, t, out, bad);
+    r = face_flux<T, RIEMANN, BND>(f, h, t, out, bad);
     double* o = &h.flux[f * 4];
     *reinterpret_cast<double2*>(o) = make_double2(out[0], out[1]);
     *reinterpret_cast<double2*>(o + 2) = make_double2(out[2], out[3]);
@@ -337,10 +341,18 @@ int run_vr(dndsg_ctx* c, bool inc, cudaStream_t s) {
 template <class T>
 void launch_flux(dndsg_ctx* c, int useDev, double tHost, double cst, cudaStream_t s) {
   HotView<T> h = view<T>(c);
-  if (c->s.riemann == 2)
-    k_face_flux<T, 2><<<grid_for(c->F), kBlock, 0, s>>>(h, c->scal, useDev, tHost, cst, c->flags, c->nreduced);
-  else
-    k_face_flux<T, 1><<<grid_for(c->F), kBlock, 0, s>>>(h, c->scal, useDev, tHost, cst, c->flags, c->nreduced);
+  const int64_t Fi = c->Fi, F = c->F;
+  if (c->s.riemann == 2) {
+    if (Fi > 0)
+      k_face_flux<T, 2, false><<<grid_for(Fi), kBlock, 0, s>>>(h, 0, Fi, c->scal, useDev, tHost, cst, c->flags, c->nreduced);
+    if (F > Fi)
+      k_face_flux<T, 2, true><<<grid_for(F - Fi), kBlock, 0, s>>>(h, Fi, F, c->scal, useDev, tHost, cst, c->flags, c->nreduced);
+  } else {
+    if (Fi > 0)
+      k_face_flux<T, 1, false><<<grid_for(Fi), kBlock, 0, s>>>(h, 0, Fi, c->scal, useDev, tHost, cst, c->flags, c->nreduced);
+    if (F > Fi)
+      k_face_flux<T, 1, true><<<grid_for(F - Fi), kBlock, 0, s>>>(h, Fi, F, c->scal, useDev, tHost, cst, c->flags, c->nreduced);
+  }
 }
 
 template <class T>
@@ -563,7 +575,26 @@ int dndsg_create(const dndsg_mesh_desc* mesh, const dndsg_settings* settings, in
   c->nfmax = anyQuad ? 4 : 3;
   int rc = set_device(c);
   if (rc) return rc;
-  rc = c->fp32 ? setup_run<float>(c, mesh) : setup_run<double>(c, mesh);
+  // internal face order: interior faces first, then boundary faces, so the hot
+  // flux kernel carries no boundary-condition code
+  const int64_t F = c->F;
+  c->facePerm.reserve(F);
+  for (int64_t f = 0; f < F; f++) if (mesh->face_cells[2 * f + 1] >= 0) c->facePerm.push_back(f);
+  c->Fi = (int64_t)c->facePerm.size();
+  for (int64_t f = 0; f < F; f++) if (mesh->face_cells[2 * f + 1] < 0) c->facePerm.push_back(f);
+  std::vector<int32_t> fn(2 * F), fc(2 * F), fb(F);
+  std::vector<double> fs(mesh->face_shift ? 2 * F : 0);
+  for (int64_t k = 0; k < F; k++) {
+    int64_t f = c->facePerm[k];
+    fn[2 * k] = mesh->face_nodes[2 * f]; fn[2 * k + 1] = mesh->face_nodes[2 * f + 1];
+    fc[2 * k] = mesh->face_cells[2 * f]; fc[2 * k + 1] = mesh->face_cells[2 * f + 1];
+    fb[k] = mesh->face_bc[f];
+    if (mesh->face_shift) { fs[2 * k] = mesh->face_shift[2 * f]; fs[2 * k + 1] = mesh->face_shift[2 * f + 1]; }
+  }
+  dndsg_mesh_desc pm = *mesh;
+  pm.face_nodes = fn.data(); pm.face_cells = fc.data(); pm.face_bc = fb.data();
+  pm.face_shift = mesh->face_shift ? fs.data() : nullptr;
+  rc = c->fp32 ? setup_run<float>(c, &pm) : setup_run<double>(c, &pm);
   return rc;
 }
 
@@ -737,9 +768,11 @@ int dndsg_face_values(dndsg_ctx* c, double t, double* out, void* s) {
   else k_face_values<double><<<grid_for(c->F), kBlock, 0, st(s)>>>(view<double>(c), t, d);
   int rc = check_launch(c);
   if (rc) return rc;
-  DG_CUDA(c, cudaMemcpyAsync(out, d, bytes, cudaMemcpyDeviceToHost, st(s)));
+  std::vector<double> tmp(24 * (size_t)c->F);
+  DG_CUDA(c, cudaMemcpyAsync(tmp.data(), d, bytes, cudaMemcpyDeviceToHost, st(s)));
   DG_CUDA(c, cudaFreeAsync(d, st(s)));
   DG_CUDA(c, cudaStreamSynchronize(st(s)));
+  for (int64_t k = 0; k < c->F; k++) std::memcpy(out + 24 * c->facePerm[k], tmp.data() + 24 * k, 24 * sizeof(double));
   return 0;
 }
 

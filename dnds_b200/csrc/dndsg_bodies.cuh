@@ -271,11 +271,42 @@ struct HotView {
 };
 
 template <class T>
-DG_HD void load4(const double* p, double* v) { for (int k = 0; k < 4; k++) v[k] = p[k]; }
+DG_HD void load4(const double* p, double* v) {
+#if defined(__CUDA_ARCH__)
+  const double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
+  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+#else
+  for (int k = 0; k < 4; k++) v[k] = p[k];
+#endif
+}
+// one 4-variable row of a cell's coefficient block (16 B for float, 32 B for double)
+DG_HD void load_row(const float* p, float r[4]) {
+#if defined(__CUDA_ARCH__)
+  const float4 a = *reinterpret_cast<const float4*>(p);
+  r[0] = a.x; r[1] = a.y; r[2] = a.z; r[3] = a.w;
+#else
+  for (int k = 0; k < 4; k++) r[k] = p[k];
+#endif
+}
+DG_HD void load_row(const double* p, double r[4]) { load4<double>(p, r); }
+DG_HD void store_row(float* p, const float r[4]) {
+#if defined(__CUDA_ARCH__)
+  *reinterpret_cast<float4*>(p) = make_float4(r[0], r[1], r[2], r[3]);
+#else
+  for (int k = 0; k < 4; k++) p[k] = r[k];
+#endif
+}
+DG_HD void store_row(double* p, const double r[4]) {
+#if defined(__CUDA_ARCH__)
+  reinterpret_cast<double2*>(p)[0] = make_double2(r[0], r[1]);
+  reinterpret_cast<double2*>(p)[1] = make_double2(r[2], r[3]);
+#else
+  for (int k = 0; k < 4; k++) p[k] = r[k];
+#endif
+}
 template <class T>
 DG_HD void load_rec(const T* p, T r[5][4]) {
-  for (int q = 0; q < 5; q++)
-    for (int v = 0; v < 4; v++) r[q][v] = p[q * 4 + v];
+  for (int q = 0; q < 5; q++) load_row(p + 4 * q, r[q]);
 }
 
 // one cell of ReconstructionJacobiStep (Jacobi form, DNDS_FV_VR.hpp:1500-1712)
@@ -300,15 +331,14 @@ DG_HD void vr_cell(int64_t i, const HotView<T>& h) {
     T b[5];
     for (int r = 0; r < 5; r++) b[r] = h.vrOp[aos(i, k * 30 + 25 + r, (int)E)];
     if (mode == VR_INNER || mode == VR_FAR) {
-      T rj[5][4];
-      load_rec(&h.urec[(int64_t)j * 20], rj);
-      for (int r = 0; r < 5; r++) {
-        T M[5];
-        for (int q = 0; q < 5; q++) M[q] = h.vrOp[aos(i, k * 30 + r * 5 + q, (int)E)];
-        for (int v = 0; v < 4; v++) {
-          T s = M[0] * rj[0][v] + M[1] * rj[1][v] + M[2] * rj[2][v] + M[3] * rj[3][v] + M[4] * rj[4][v];
-          acc[r][v] += relax * s;
-        }
+      // stream the neighbour's coefficient rows: acc[r][:] += sum_q (A^-1B)[r][q] * urec_j[q][:]
+      const T* rj = &h.urec[(int64_t)j * 20];
+      for (int q = 0; q < 5; q++) {
+        T row[4], col[5];
+        load_row(rj + 4 * q, row);
+        for (int r = 0; r < 5; r++) col[r] = relax * h.vrOp[aos(i, k * 30 + r * 5 + q, (int)E)];
+        for (int r = 0; r < 5; r++)
+          for (int v = 0; v < 4; v++) acc[r][v] += col[r] * row[v];
       }
     }
     if (mode == VR_INNER || mode == VR_WALL) {
@@ -362,60 +392,91 @@ DG_HD void vr_cell(int64_t i, const HotView<T>& h) {
     }
   }
   T* out = &h.urecNew[i * 20];
-  for (int q = 0; q < 5; q++) for (int v = 0; v < 4; v++) out[q * 4 + v] = acc[q][v];
+  for (int q = 0; q < 5; q++) store_row(out + 4 * q, acc[q]);
 }
 
-// reconstructed states at the 3 gauss points of face f (EvaluateRHS, DNDS_FV_EulerEvaluator.cpp:250-360)
+// reconstruction increments phi(gp) . urec of both cells at the 3 gauss points of
+// face f; the coefficient rows are streamed once (EvaluateRHS, DNDS_FV_EulerEvaluator.cpp:250-360)
+template <class T>
+DG_HD void face_increments(int64_t f, int32_t L, int32_t R, const HotView<T>& h, T incL[3][4], T incR[3][4]) {
+  T phi[3][5];
+  for (int g = 0; g < 3; g++)
+    for (int q = 0; q < 5; q++) phi[g][q] = h.faceBasis[aos(f, g * 5 + q, 30)];
+  for (int g = 0; g < 3; g++) for (int v = 0; v < 4; v++) incL[g][v] = T(0);
+  const T* rl = &h.urec[(int64_t)L * 20];
+  for (int q = 0; q < 5; q++) {
+    T row[4];
+    load_row(rl + 4 * q, row);
+    for (int g = 0; g < 3; g++)
+      for (int v = 0; v < 4; v++) incL[g][v] += phi[g][q] * row[v];
+  }
+  for (int g = 0; g < 3; g++) for (int v = 0; v < 4; v++) incR[g][v] = T(0);
+  if (R >= 0) {
+    for (int g = 0; g < 3; g++)
+      for (int q = 0; q < 5; q++) phi[g][q] = h.faceBasis[aos(f, 15 + g * 5 + q, 30)];
+    const T* rr = &h.urec[(int64_t)R * 20];
+    for (int q = 0; q < 5; q++) {
+      T row[4];
+      load_row(rr + 4 * q, row);
+      for (int g = 0; g < 3; g++)
+        for (int v = 0; v < 4; v++) incR[g][v] += phi[g][q] * row[v];
+    }
+  }
+}
+
+// positivity-compressed states at gauss point g (CompressRecPart, boundary state on a boundary face)
+template <class T, bool BND = true>
+DG_HD int gp_states(int64_t f, int32_t R, const HotView<T>& h, double t, double nx, double ny, const double uL[4],
+                    const double uR[4], const T incL[4], const T incR[4], double UL[4], double UR[4]) {
+  double inc[4];
+  for (int v = 0; v < 4; v++) inc[v] = (double)incL[v];
+  int nred = compress_rec_part(uL, inc, UL) ? 1 : 0;
+  if (!BND || R >= 0) {
+    for (int v = 0; v < 4; v++) inc[v] = (double)incR[v];
+    nred += compress_rec_part(uR, inc, UR) ? 1 : 0;
+  } else {
+    const double far[4] = {h.farU[0], h.farU[1], h.farU[2], h.farU[3]};  // keeps the view out of local memory
+    boundary_value(h.faceBC[f], UL, nx, ny, h.faceCenter[2 * f], h.faceCenter[2 * f + 1], t, h.gamma, far, UR);
+  }
+  return nred;
+}
+
+// all gauss-point states of face f (diagnostic)
 template <class T>
 DG_HD int face_states(int64_t f, const HotView<T>& h, double t, double UL[3][4], double UR[3][4], double& nx,
                       double& ny, double& area) {
   int32_t L = h.faceL[f], R = h.faceR[f];
   nx = h.faceNormal[2 * f]; ny = h.faceNormal[2 * f + 1]; area = h.faceArea[f];
-  double uL[4], uR[4];
+  double uL[4], uR[4] = {0, 0, 0, 0};
   load4<T>(&h.u[(int64_t)L * 4], uL);
-  T rL[5][4], rR[5][4];
-  load_rec(&h.urec[(int64_t)L * 20], rL);
+  if (R >= 0) load4<T>(&h.u[(int64_t)R * 4], uR);
+  T incL[3][4], incR[3][4];
+  face_increments(f, L, R, h, incL, incR);
   int nred = 0;
-  if (R >= 0) {
-    load4<T>(&h.u[(int64_t)R * 4], uR);
-    load_rec(&h.urec[(int64_t)R * 20], rR);
-  }
-  int bc = h.faceBC[f];
-  for (int g = 0; g < 3; g++) {
-    T phi[5];
-    for (int q = 0; q < 5; q++) phi[q] = h.faceBasis[aos(f, g * 5 + q, 30)];
-    double inc[4];
-    for (int v = 0; v < 4; v++) {
-      T s = phi[0] * rL[0][v] + phi[1] * rL[1][v] + phi[2] * rL[2][v] + phi[3] * rL[3][v] + phi[4] * rL[4][v];
-      inc[v] = (double)s;
-    }
-    nred += compress_rec_part(uL, inc, UL[g]) ? 1 : 0;
-    if (R >= 0) {
-      for (int q = 0; q < 5; q++) phi[q] = h.faceBasis[aos(f, 15 + g * 5 + q, 30)];
-      for (int v = 0; v < 4; v++) {
-        T s = phi[0] * rR[0][v] + phi[1] * rR[1][v] + phi[2] * rR[2][v] + phi[3] * rR[3][v] + phi[4] * rR[4][v];
-        inc[v] = (double)s;
-      }
-      nred += compress_rec_part(uR, inc, UR[g]) ? 1 : 0;
-    } else {
-      boundary_value(bc, UL[g], nx, ny, h.faceCenter[2 * f], h.faceCenter[2 * f + 1], t, h.gamma, h.farU, UR[g]);
-    }
-  }
+  for (int g = 0; g < 3; g++) nred += gp_states(f, R, h, t, nx, ny, uL, uR, incL[g], incR[g], UL[g], UR[g]);
   return nred;
 }
 
 // face flux: sum over gauss points of -F(UL,UR).n |n| w (fluxFace, DNDS_FV_EulerEvaluator.hpp:371-591)
-// returns the reduced-order count; bit 0 of *bad is set on non-physical input
-template <class T, int RIEMANN>
+// returns the reduced-order count; *bad is set on non-physical input
+// BND = false: an interior (or periodic) face, so no boundary-state code is compiled in
+template <class T, int RIEMANN, bool BND>
 DG_HD int face_flux(int64_t f, const HotView<T>& h, double t, double out[4], bool& bad) {
-  double UL[3][4], UR[3][4], nx, ny, area;
-  int nred = face_states(f, h, t, UL, UR, nx, ny, area);
+  int32_t L = h.faceL[f], R = h.faceR[f];
+  double nx = h.faceNormal[2 * f], ny = h.faceNormal[2 * f + 1], area = h.faceArea[f];
+  double uL[4], uR[4] = {0, 0, 0, 0};
+  load4<T>(&h.u[(int64_t)L * 4], uL);
+  if (!BND || R >= 0) load4<T>(&h.u[(int64_t)R * 4], uR);
   double dl = h.dLam[f];
+  T incL[3][4], incR[3][4];
+  face_increments(f, L, R, h, incL, incR);
+  int nred = 0;
   double acc[4] = {0, 0, 0, 0};
   for (int g = 0; g < 3; g++) {
-    double a[4], b[4], F[4];
-    to_normal_frame(UL[g], nx, ny, a);
-    to_normal_frame(UR[g], nx, ny, b);
+    double UL[4], UR[4], a[4], b[4], F[4];
+    nred += gp_states<T, BND>(f, R, h, t, nx, ny, uL, uR, incL[g], incR[g], UL, UR);
+    to_normal_frame(UL, nx, ny, a);
+    to_normal_frame(UR, nx, ny, b);
     if (!(a[0] > 0 && b[0] > 0)) bad = true;
     if (RIEMANN == 2) hllc_flux(a, b, h.gamma, F);
     else roe_flux(a, b, h.gamma, dl, F);
