@@ -140,6 +140,81 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 2 : 1) k_vr(HotView<T
   }
 }
 
+// ------------------------------------------------------------------ bulk-copy (TMA) helpers
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+// one contiguous global -> shared bulk copy completing on an mbarrier (no multicast)
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+// bounded wait for an mbarrier phase; false if the limit ran out
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint32_t limit) {
+  uint32_t done = 0;
+  for (uint32_t it = 0; it < limit && !done; ++it) {
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+  }
+  return done != 0;
+}
+constexpr uint32_t kWaitLimit = 1u << 22;
+constexpr unsigned kFlagTimeout = 4u;
+
+// VR operator of the CTA's tile in shared memory, same AoSoA order as in global memory
+template <class T>
+struct VrOpSmem {
+  const T* p;  // &tile[(sub * E) * 32 + lane]
+  __device__ __forceinline__ T operator()(int k, int e) const { return p[(k * 30 + e) * 32]; }
+};
+
+// VR Jacobi sweep with the per-cell operator blocks staged by one bulk async copy
+// per CTA (TILE cells = TILE*E values, contiguous in the AoSoA layout); relax = 1.
+template <class T, int TILE>
+__global__ void __launch_bounds__(TILE, 4) k_vr_tma(HotView<T> h, unsigned* flags) {
+  extern __shared__ __align__(128) unsigned char dsm[];
+  __shared__ __align__(8) unsigned long long bar;
+  const int E = h.nfmax * 30;
+  const int tid = threadIdx.x;
+  const int64_t c0 = (int64_t)blockIdx.x * TILE;
+  const uint32_t bytes = (uint32_t)(TILE * E * sizeof(T));
+  const uint32_t b = smem_u32(&bar);
+  if (tid == 0) {
+    mbar_init(b, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (tid == 0) {
+    mbar_expect_tx(b, bytes);
+    bulk_g2s(smem_u32(dsm), h.vrOp + c0 * E, bytes, b);
+  }
+  const bool ok = mbar_wait(b, 0, kWaitLimit);
+  if (__syncthreads_or(!ok)) {
+    // the copy did not land in time: flag it, let the copy drain (bounded) and leave
+    if (tid == 0) {
+      atomicOr(flags, kFlagTimeout);
+      mbar_wait(b, 0, kWaitLimit);
+    }
+    return;
+  }
+  const int64_t i = c0 + tid;
+  if (i < h.N) {
+    const T* sm = reinterpret_cast<const T*>(dsm);
+    vr_cell_op<T, true>(i, h, VrOpSmem<T>{sm + (tid >> 5) * E * 32 + (tid & 31)});
+  }
+}
+template <class T>
+constexpr int vr_tile() { return sizeof(T) == 4 ? 128 : 64; }
+
 __device__ __forceinline__ double stage_time(const double* scal, int useDev, double tHost, double c) {
   return useDev ? scal[S_T] + c * scal[S_DT] : tHost;
 }
@@ -155,7 +230,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_face_flux(HotView<T> h, int64_t f
   if (f < f1) {
     double out[4];
     double t = stage_time(scal, useDev, tHost, c);
-    r = face_flux<T, RIEMANN, BND>(f, h, t, out, bad);
+    if constexpr (sizeof(T) == 4 && RIEMANN == 1 && !BND)
+      r = face_flux_roe_delta32(f, h, out, bad);
+    else
+      r = face_flux<T, RIEMANN, BND>(f, h, t, out, bad);
     double* o = &h.flux[f * 4];
     *reinterpret_cast<double2*>(o) = make_double2(out[0], out[1]);
     *reinterpret_cast<double2*>(o + 2) = make_double2(out[2], out[3]);
@@ -330,9 +408,12 @@ int run_vr(dndsg_ctx* c, bool inc, cudaStream_t s) {
   if (inc) {
     if (r1) k_vr<T, true, true><<<grid_for(c->N), kBlock, 0, s>>>(h, c->scal + S_INC);
     else k_vr<T, false, true><<<grid_for(c->N), kBlock, 0, s>>>(h, c->scal + S_INC);
+  } else if (r1) {
+    constexpr int TILE = vr_tile<T>();
+    const size_t smem = (size_t)TILE * c->nfmax * 30 * sizeof(T);
+    k_vr_tma<T, TILE><<<(unsigned)((c->N + TILE - 1) / TILE), TILE, smem, s>>>(h, c->flags);
   } else {
-    if (r1) k_vr<T, true, false><<<grid_for(c->N), kBlock, 0, s>>>(h, nullptr);
-    else k_vr<T, false, false><<<grid_for(c->N), kBlock, 0, s>>>(h, nullptr);
+    k_vr<T, false, false><<<grid_for(c->N), kBlock, 0, s>>>(h, nullptr);
   }
   std::swap(c->urec, c->urecNew);
   return 0;
@@ -502,7 +583,13 @@ int setup_run(dndsg_ctx* c, const dndsg_mesh_desc* md) {
   if ((rc = dalloc(c, c->vrNbr, sizeof(int32_t) * slots.size()))) return rc;
   if ((rc = dalloc(c, c->vrMode, sizeof(int32_t) * slots.size()))) return rc;
   if ((rc = dalloc(c, c->vrFace, sizeof(int32_t) * slots.size()))) return rc;
-  if ((rc = dalloc(c, c->vrOp, sizeof(T) * aos_size(N, c->nfmax * 30)))) return rc;
+  // padded to whole bulk-copy tiles (128 cells) so every tile copy stays inside the allocation
+  if ((rc = dalloc(c, c->vrOp, sizeof(T) * aos_size(((N + 127) / 128) * 128, c->nfmax * 30)))) return rc;
+  {
+    constexpr int TILE = vr_tile<T>();
+    DG_CUDA(c, cudaFuncSetAttribute(k_vr_tma<T, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(TILE * c->nfmax * 30 * sizeof(T))));
+  }
   if (hasWallCorr)
     if ((rc = dalloc(c, c->Ainv, sizeof(double) * 25 * N))) return rc;
   k_setup_matrices<T><<<grid_for(N), kBlock>>>(m, p, cells, faceW, c->cellFace, c->nfmax, (T*)c->vrOp, c->vrNbr,

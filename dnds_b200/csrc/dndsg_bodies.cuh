@@ -309,10 +309,20 @@ DG_HD void load_rec(const T* p, T r[5][4]) {
   for (int q = 0; q < 5; q++) load_row(p + 4 * q, r[q]);
 }
 
+// accessor of the per-slot VR operator (25 A^-1B entries then 5 A^-1b entries) in global memory
+template <class T>
+struct VrOpGlobal {
+  const T* op;
+  int64_t i;
+  int E;
+  DG_HD T operator()(int k, int e) const { return op[aos(i, k * 30 + e, E)]; }
+};
+
 // one cell of ReconstructionJacobiStep (Jacobi form, DNDS_FV_VR.hpp:1500-1712)
 template <class T, bool RELAX1>
-DG_HD void vr_cell(int64_t i, const HotView<T>& h) {
-  const int64_t E = (int64_t)h.nfmax * 30;
+DG_HD void vr_cell(int64_t i, const HotView<T>& h);
+template <class T, bool RELAX1, class Op>
+DG_HD void vr_cell_op(int64_t i, const HotView<T>& h, const Op& opk) {
   double ui[4];
   load4<T>(&h.u[i * 4], ui);
   T acc[5][4];
@@ -329,14 +339,14 @@ DG_HD void vr_cell(int64_t i, const HotView<T>& h) {
     if (mode == VR_EMPTY) continue;
     int32_t j = h.vrNbr[aos(i, k, h.nfmax)];
     T b[5];
-    for (int r = 0; r < 5; r++) b[r] = h.vrOp[aos(i, k * 30 + 25 + r, (int)E)];
+    for (int r = 0; r < 5; r++) b[r] = opk(k, 25 + r);
     if (mode == VR_INNER || mode == VR_FAR) {
       // stream the neighbour's coefficient rows: acc[r][:] += sum_q (A^-1B)[r][q] * urec_j[q][:]
       const T* rj = &h.urec[(int64_t)j * 20];
       for (int q = 0; q < 5; q++) {
         T row[4], col[5];
         load_row(rj + 4 * q, row);
-        for (int r = 0; r < 5; r++) col[r] = relax * h.vrOp[aos(i, k * 30 + r * 5 + q, (int)E)];
+        for (int r = 0; r < 5; r++) col[r] = relax * opk(k, r * 5 + q);
         for (int r = 0; r < 5; r++)
           for (int v = 0; v < 4; v++) acc[r][v] += col[r] * row[v];
       }
@@ -393,6 +403,10 @@ DG_HD void vr_cell(int64_t i, const HotView<T>& h) {
   }
   T* out = &h.urecNew[i * 20];
   for (int q = 0; q < 5; q++) store_row(out + 4 * q, acc[q]);
+}
+template <class T, bool RELAX1>
+DG_HD void vr_cell(int64_t i, const HotView<T>& h) {
+  vr_cell_op<T, RELAX1>(i, h, VrOpGlobal<T>{h.vrOp, i, h.nfmax * 30});
 }
 
 // reconstruction increments phi(gp) . urec of both cells at the 3 gauss points of
@@ -487,6 +501,125 @@ DG_HD int face_flux(int64_t f, const HotView<T>& h, double t, double out[4], boo
   for (int k = 0; k < 4; k++) {
     if (!(acc[k] == acc[k])) bad = true;
     out[k] = acc[k];
+  }
+  return nred;
+}
+
+// F(U0 + d) - F(U0) of the normal-frame Euler flux, evaluated from the
+// increments so that FP32 rounding scales with |d|, not with |F|
+DG_HD void flux_delta_f32(const float U[4], const float d[4], float gamma, float D[4]) {
+  const float rho = U[0], m = U[1], k = U[2], E = U[3];
+  const float ir = 1.0f / rho, u = m * ir, v = k * ir;
+  const float p = (gamma - 1.0f) * (E - 0.5f * (m * u + k * v));
+  const float irn = 1.0f / (rho + d[0]);
+  const float du = (d[1] - u * d[0]) * irn, dv = (d[2] - v * d[0]) * irn;
+  const float un = u + du, vn = v + dv;
+  const float dp = (gamma - 1.0f) * (d[3] - 0.5f * (m * du + d[1] * un + k * dv + d[2] * vn));
+  D[0] = d[1];
+  D[1] = m * du + d[1] * un + dp;
+  D[2] = k * du + d[2] * un;
+  D[3] = (E + p) * du + (d[3] + dp) * un;
+}
+
+// physical flux F(U).n of a cell mean in the x-y frame, FP64
+DG_HD void flux_n_f64(const double U[4], double nx, double ny, double gamma, double F[4]) {
+  const double ir = 1.0 / U[0];
+  const double u = U[1] * ir, v = U[2] * ir;
+  const double p = (gamma - 1) * (U[3] - 0.5 * (U[1] * u + U[2] * v));
+  const double un = u * nx + v * ny;
+  F[0] = U[0] * un;
+  F[1] = U[1] * un + p * nx;
+  F[2] = U[2] * un + p * ny;
+  F[3] = (U[3] + p) * un;
+}
+
+// Roe flux of an interior face for the FP32-bulk path, in flux-difference form:
+//   F(UL,UR) = 1/2 (F(uL) + F(uR))                      FP64, once per face
+//            + 1/2 (F(UL) - F(uL) + F(UR) - F(uR))      FP32 from the increments
+//            - 1/2 R |Lambda| L (UR - UL)               FP32, UR - UL formed from an FP64 mean difference
+// uL/uR are the cell means, UL = uL + phi_L . urec_L at each gauss point.  The
+// algebra is that of Gas::RoeFlux_IdealGas_HartenYee<2,0> (DNDS_Gas.hpp:406-654).
+DG_HD int face_flux_roe_delta32(int64_t f, const HotView<float>& h, double out[4], bool& bad) {
+  const int32_t L = h.faceL[f], R = h.faceR[f];
+  const double nxd = h.faceNormal[2 * f], nyd = h.faceNormal[2 * f + 1], area = h.faceArea[f];
+  double uL[4], uR[4];
+  load4<float>(&h.u[(int64_t)L * 4], uL);
+  load4<float>(&h.u[(int64_t)R * 4], uR);
+  float incL[3][4], incR[3][4];
+  face_increments(f, L, R, h, incL, incR);
+  const float gamma = (float)h.gamma, dl = (float)h.dLam[f];
+  const float nx = (float)nxd, ny = (float)nyd;
+  // FP64 part: area * (F(uL) + F(uR)) / 2
+  double FL[4], FR[4];
+  flux_n_f64(uL, nxd, nyd, h.gamma, FL);
+  flux_n_f64(uR, nxd, nyd, h.gamma, FR);
+  // normal-frame FP32 bases and the mean jump
+  float bL[4], bR[4], dmean[4];
+  {
+    float tL[4] = {(float)uL[0], (float)uL[1], (float)uL[2], (float)uL[3]};
+    float tR[4] = {(float)uR[0], (float)uR[1], (float)uR[2], (float)uR[3]};
+    float tD[4] = {(float)(uR[0] - uL[0]), (float)(uR[1] - uL[1]), (float)(uR[2] - uL[2]), (float)(uR[3] - uL[3])};
+    to_normal_frame(tL, nx, ny, bL);
+    to_normal_frame(tR, nx, ny, bR);
+    to_normal_frame(tD, nx, ny, dmean);
+  }
+  int nred = 0;
+  float acc[4] = {0.f, 0.f, 0.f, 0.f};
+  for (int g = 0; g < 3; g++) {
+    float dL[4], dR[4];
+    to_normal_frame(incL[g], nx, ny, dL);
+    to_normal_frame(incR[g], nx, ny, dR);
+    // CompressRecPart: fall back to the mean where density or internal energy would be negative
+    float UL[4], UR[4];
+    for (int v = 0; v < 4; v++) { UL[v] = bL[v] + dL[v]; UR[v] = bR[v] + dR[v]; }
+    if (UL[0] < 0.f || UL[3] - (UL[1] * UL[1] + UL[2] * UL[2]) * 0.5f / UL[0] < 0.f) {
+      for (int v = 0; v < 4; v++) { dL[v] = 0.f; UL[v] = bL[v]; }
+      nred++;
+    }
+    if (UR[0] < 0.f || UR[3] - (UR[1] * UR[1] + UR[2] * UR[2]) * 0.5f / UR[0] < 0.f) {
+      for (int v = 0; v < 4; v++) { dR[v] = 0.f; UR[v] = bR[v]; }
+      nred++;
+    }
+    if (!(UL[0] > 0.f && UR[0] > 0.f)) bad = true;
+    float DL[4], DR[4];
+    flux_delta_f32(bL, dL, gamma, DL);
+    flux_delta_f32(bR, dR, gamma, DR);
+    // Roe average and wave strengths of dU = (uR - uL) + (dR - dL)
+    const float irL = 1.0f / UL[0], irR = 1.0f / UR[0];
+    const float u1 = UL[1] * irL, v1 = UL[2] * irL, u2 = UR[1] * irR, v2 = UR[2] * irR;
+    const float pL = (gamma - 1.0f) * (UL[3] - 0.5f * (UL[1] * u1 + UL[2] * v1));
+    const float pR = (gamma - 1.0f) * (UR[3] - 0.5f * (UR[1] * u2 + UR[2] * v2));
+    const float HL = (UL[3] + pL) * irL, HR = (UR[3] + pR) * irR;
+    const float sL = sqrtf(UL[0]), sR = sqrtf(UR[0]), isum = 1.0f / (sL + sR);
+    const float u = (sL * u1 + sR * u2) * isum, v = (sL * v1 + sR * v2) * isum;
+    const float vs = u * u + v * v;
+    const float H = (sL * HL + sR * HR) * isum;
+    const float a2 = (gamma - 1.0f) * (H - 0.5f * vs);
+    const float a = sqrtf(a2);
+    float lam0 = fabsf(u - a), lam1 = fabsf(u), lam3 = fabsf(u + a);
+    const float thr = fmaxf(0.05f * (sqrtf(vs) + a), dl), thrS = thr * thr;
+    if (lam0 < thr) lam0 = (lam0 * lam0 + thrS) / (2.0f * thr);
+    if (lam3 < thr) lam3 = (lam3 * lam3 + thrS) / (2.0f * thr);
+    const float d0 = dmean[0] + (dR[0] - dL[0]), d1 = dmean[1] + (dR[1] - dL[1]);
+    const float d2 = dmean[2] + (dR[2] - dL[2]), d3 = dmean[3] + (dR[3] - dL[3]);
+    const float al2 = d2 - v * d0;
+    const float d3b = d3 - al2 * v;
+    const float al1 = (gamma - 1.0f) / a2 * (d0 * (H - u * u) + u * d1 - d3b);
+    const float al0 = (d0 * (u + a) - d1 - a * al1) / (2.0f * a);
+    const float al3 = d0 - (al0 + al1);
+    const float w0 = lam0 * al0, w1 = lam1 * al1, w2 = lam1 * al2, w3 = lam3 * al3;
+    float G[4];
+    G[0] = 0.5f * (DL[0] + DR[0]) - 0.5f * (w0 + w1 + w3);
+    G[1] = 0.5f * (DL[1] + DR[1]) - 0.5f * ((u - a) * w0 + u * w1 + (u + a) * w3);
+    G[2] = 0.5f * (DL[2] + DR[2]) - 0.5f * (v * (w0 + w1 + w3) + w2);
+    G[3] = 0.5f * (DL[3] + DR[3]) - 0.5f * ((H - u * a) * w0 + 0.5f * vs * w1 + v * w2 + (H + u * a) * w3);
+    from_normal_frame(G, nx, ny);
+    const float jw = (float)(0.5 * area * l3_weight(g));
+    for (int k = 0; k < 4; k++) acc[k] += G[k] * jw;
+  }
+  for (int k = 0; k < 4; k++) {
+    out[k] = -(area * 0.5 * (FL[k] + FR[k]) + (double)acc[k]);
+    if (!(out[k] == out[k])) bad = true;
   }
   return nred;
 }
