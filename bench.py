@@ -40,9 +40,10 @@ N_GRID = 1024
 # write urec 20s (s = bytes per real), cell means 4x8, 3 neighbour indices 3x4
 VR_BYTES_PER_CELL = {4: 130 * 4 + 32 + 12, 8: 130 * 8 + 32 + 12}
 KERNELS_PER_STEP = 14  # init, dt face, dt cell, dt finalize, 3 x (VR, flux, update), time advance
-# DRAM bytes (read + write) per launch of the FP32 VR sweep on this workload, from the
-# ncu capture summarised in profiles/vr_sweep_fp32_vortex_tri1024.md (None until captured)
-VR_TRAFFIC_FP32 = None
+# DRAM bytes (read + write) per launch of the FP32 VR sweep: ncu dram__bytes_read.sum +
+# dram__bytes_write.sum on the 512x512 mesh (292.25 MB for 524,288 cells, see
+# profiles/vr_sweep_fp32_vortex_tri512.md) scaled by the cell count (x4) to this workload
+VR_TRAFFIC_FP32 = 292.249e6 * 4
 
 
 def dist_env():
@@ -50,6 +51,23 @@ def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return ws, rank, local
+
+
+def max_over_ranks(x: float, device=None) -> float:
+    """Max of a per-rank scalar over all ranks (identity without torch.distributed)."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(n_cells: int, steps: int, ms_max: float, world: int) -> float:
+    """Whole-job cell-stage updates/s of `world` independent replicas timed by the slowest rank."""
+    return n_cells * 3 * steps / (ms_max * 1e-3) * world
 
 
 def measured_peak():
@@ -230,12 +248,7 @@ def main():
             solver.ssprk3_step(0.5, 1e300)
         e1.record()
         barrier()
-        ms = e0.elapsed_time(e1)
-        if ws > 1:
-            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return max_over_ranks(e0.elapsed_time(e1), device="cuda")
 
     results = {}
     wanted = args.precisions.split(",")
@@ -281,12 +294,7 @@ def main():
                 s.ssprk3_step(0.5, 1e300)
                 s.get_u(out=hnp)
             barrier()
-            e2e_s = time.perf_counter() - t0
-            if ws > 1:
-                t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-                torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-                e2e_s = float(t.item())
-            results[name]["e2e_s"] = e2e_s
+            results[name]["e2e_s"] = max_over_ranks(time.perf_counter() - t0, device="cuda")
         # accuracy at t = 2 against the exact advected vortex (density)
         if not args.no_accuracy:
             s.set_u(u0)
@@ -314,8 +322,8 @@ def main():
 
     r32 = results.get("fp32") or results["fp64"]
     r64 = results.get("fp64") or r32
-    value = N * 3 * args.steps / (r32["ms"] * 1e-3) * ws
-    value64 = N * 3 * args.steps / (r64["ms"] * 1e-3) * ws
+    value = replica_throughput(N, args.steps, r32["ms"], ws)
+    value64 = replica_throughput(N, args.steps, r64["ms"], ws)
     peak, peak_kind = measured_peak()
     vr_bytes = VR_BYTES_PER_CELL[4] * N
     achieved = vr_bytes / (r32["vr_ms"] * 1e-3) / 1e9
@@ -339,7 +347,7 @@ def main():
         "status": {"flags": r32["flags"] | r64["flags"], "reduced_order_points": r32["nred"] + r64["nred"]},
     }
     if "e2e_s" in r32:
-        out["e2e"] = {"value": N * 3 * args.steps / r32["e2e_s"] * ws, "unit": UNIT,
+        out["e2e"] = {"value": replica_throughput(N, args.steps, r32["e2e_s"] * 1e3, ws), "unit": UNIT,
                       "h2d_bytes_per_step": N * 4 * 8, "d2h_bytes_per_step": N * 4 * 8}
     if "l2_rho" in r32:
         out["accuracy"] = {"t_end": args.accuracy_t, "l2_rho_fp32": r32["l2_rho"], "l2_rho_fp64": r64["l2_rho"],
