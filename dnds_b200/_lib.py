@@ -15,7 +15,7 @@ EXPORTS = [
     "dndsg_set_u", "dndsg_get_u", "dndsg_set_urec", "dndsg_get_urec", "dndsg_get_dt",
     "dndsg_device_buffer", "dndsg_get_time", "dndsg_set_time", "dndsg_vr_jacobi_step",
     "dndsg_limiter_wbap", "dndsg_eval_dt", "dndsg_eval_rhs", "dndsg_ssprk3_step",
-    "dndsg_residual", "dndsg_face_values", "dndsg_get_status",
+    "dndsg_residual", "dndsg_face_values", "dndsg_get_status", "dndsg_eval_rhs_noalloc",
 ]
 
 
@@ -65,6 +65,7 @@ def lib():
     L.dndsg_residual.argtypes = [vp, i32, i32, vp, vp]
     L.dndsg_face_values.argtypes = [vp, dbl, vp, vp]
     L.dndsg_get_status.argtypes = [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), vp]
+    L.dndsg_eval_rhs_noalloc.argtypes = [vp, vp, vp, vp, dbl, vp]
     for nm in EXPORTS:
         if nm not in ("dndsg_destroy", "dndsg_last_error", "dndsg_n_cells", "dndsg_n_faces"):
             getattr(L, nm).restype = i32

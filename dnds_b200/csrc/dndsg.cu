@@ -878,3 +878,72 @@ int dndsg_get_status(dndsg_ctx* c, uint32_t* flags, uint64_t* n_reduced, void* s
 }
 
 }  // extern "C"
+
+// ====================================================================== allocation-free RHS
+// Some callers cannot call cudaMalloc at the point where they need a residual:
+// real-time loops where the implicit device synchronisation of cudaMalloc is
+// not acceptable, host frameworks that own all device memory and forbid
+// allocations after start-up, and code running inside another library's
+// callback where allocating is not allowed.
+// dndsg_eval_rhs_noalloc serves them: it allocates nothing and keeps its only
+// scratch -- the per-face flux buffer between the face kernel and the cell
+// gather -- in the file-scope array below, sized for at most
+// DNDSG_NOALLOC_MAX_FACES faces (8 MiB; every GPU that loads this library holds
+// it until the process exits).
+namespace {
+constexpr int64_t kNoAllocMaxFaces = DNDSG_NOALLOC_MAX_FACES;
+static __device__ __align__(256) double g_noalloc_flux[kNoAllocMaxFaces * 4];
+constexpr int kMaxDevices = 64;
+double* g_noalloc_ptr[kMaxDevices] = {nullptr};
+
+// Host code must not pass g_noalloc_flux itself to a kernel (on the host it is
+// only a stand-in symbol); the device address comes from cudaGetSymbolAddress,
+// once per device, with that device current.
+int noalloc_scratch(dndsg_ctx* c, double** out) {
+  if (c->device < 0 || c->device >= kMaxDevices) return fail(c, DNDSG_BAD_ARGUMENT, "device index out of range");
+  if (!g_noalloc_ptr[c->device]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_flux);
+    if (e != cudaSuccess)
+      return fail(c, DNDSG_CUDA_ERROR, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    g_noalloc_ptr[c->device] = (double*)p;
+  }
+  *out = g_noalloc_ptr[c->device];
+  return 0;
+}
+
+template <class T>
+void run_rhs_noalloc(dndsg_ctx* c, const double* u, const void* urec, double* rhs, double* scratch, double t,
+                     cudaStream_t s) {
+  HotView<T> h = view<T>(c);
+  h.u = const_cast<double*>(u);
+  h.urec = (const T*)urec;
+  h.rhs = rhs;
+  h.flux = scratch;
+  const int64_t Fi = c->Fi, F = c->F;
+  if (c->s.riemann == 2) {
+    if (Fi > 0) k_face_flux<T, 2, false><<<grid_for(Fi), kBlock, 0, s>>>(h, 0, Fi, c->scal, 0, t, 0.0, c->flags, c->nreduced);
+    if (F > Fi) k_face_flux<T, 2, true><<<grid_for(F - Fi), kBlock, 0, s>>>(h, Fi, F, c->scal, 0, t, 0.0, c->flags, c->nreduced);
+  } else {
+    if (Fi > 0) k_face_flux<T, 1, false><<<grid_for(Fi), kBlock, 0, s>>>(h, 0, Fi, c->scal, 0, t, 0.0, c->flags, c->nreduced);
+    if (F > Fi) k_face_flux<T, 1, true><<<grid_for(F - Fi), kBlock, 0, s>>>(h, Fi, F, c->scal, 0, t, 0.0, c->flags, c->nreduced);
+  }
+  k_cell_update<T, -1><<<grid_for(c->N), kBlock, 0, s>>>(h, c->scal);
+}
+}  // namespace
+
+extern "C" int dndsg_eval_rhs_noalloc(dndsg_ctx* c, const double* u, const void* urec, double* rhs, double t,
+                                      void* s) {
+  if (!c || !u || !urec || !rhs) return DNDSG_BAD_ARGUMENT;
+  if (c->F > kNoAllocMaxFaces)
+    return fail(c, DNDSG_BAD_ARGUMENT,
+                "dndsg_eval_rhs_noalloc: mesh has " + std::to_string(c->F) + " faces, more than its scratch limit of " +
+                    std::to_string(kNoAllocMaxFaces));
+  int rc = set_device(c);
+  if (rc) return rc;
+  double* scratch = nullptr;
+  if ((rc = noalloc_scratch(c, &scratch))) return rc;
+  if (c->fp32) run_rhs_noalloc<float>(c, u, urec, rhs, scratch, t, st(s));
+  else run_rhs_noalloc<double>(c, u, urec, rhs, scratch, t, st(s));
+  return check_launch(c);
+}

@@ -137,6 +137,14 @@ class Solver:
         self._check(self.L.dndsg_eval_rhs(self.h, float(t), _p(rhs) if copy else None, self.stream))
         return rhs
 
+    def EvaluateRHS_noalloc(self, u_ptr: int, urec_ptr: int, rhs_ptr: int, t: float = 0.0):
+        """EvaluateRHS from caller-owned device arrays without any device allocation
+        (dndsg_eval_rhs_noalloc): for callers that cannot allocate device memory
+        when they need a residual.  Meshes are limited to DNDSG_NOALLOC_MAX_FACES
+        faces; concurrent calls on the GPU share one scratch array and race."""
+        self._check(self.L.dndsg_eval_rhs_noalloc(self.h, C.c_void_p(u_ptr), C.c_void_p(urec_ptr),
+                                                  C.c_void_p(rhs_ptr), float(t), self.stream))
+
     def EvaluateResidual(self, p: int = 1, vol_wise: bool = False) -> np.ndarray:
         out = np.empty(4)
         self._check(self.L.dndsg_residual(self.h, int(p), int(vol_wise), _p(out), self.stream))

@@ -157,6 +157,26 @@ int dndsg_residual(dndsg_ctx* ctx, int p, int vol_wise, double* out, void* strea
  * state), evaluated as in EvaluateRHS (DNDS_FV_EulerEvaluator.cpp:250-360). */
 int dndsg_face_values(dndsg_ctx* ctx, double t, double* out, void* stream);
 
+/* Allocation-free EvaluateRHS.  No counterpart in the reference: it is for
+ * callers that cannot allocate device memory when they need a residual -- a
+ * real-time loop that cannot afford cudaMalloc's implicit device
+ * synchronisation, a host framework that owns all device memory and forbids
+ * allocations after start-up, or code running inside another library's
+ * callback where allocating is not allowed.  It computes what dndsg_eval_rhs computes, but
+ * from caller-owned device arrays -- u [n_cells][4] double, urec
+ * [n_cells][5][4] in the context's precision (double, or float when
+ * precision = 1), rhs [n_cells][4] double (output) -- and it allocates
+ * nothing: its face-flux scratch is a fixed array inside the library of
+ * DNDSG_NOALLOC_MAX_FACES faces (8 MiB per GPU, held until exit); larger
+ * meshes are rejected with DNDSG_BAD_ARGUMENT.  The first call on a device
+ * looks up the scratch address (cudaGetSymbolAddress), so make that first call
+ * before any stream capture.  All calls share the one scratch array: calls
+ * that overlap on the GPU (different streams or contexts at the same time)
+ * race and must be serialised by the caller.  The Roe entropy fix uses the
+ * face data of the context's last dndsg_eval_dt, as dndsg_eval_rhs does. */
+#define DNDSG_NOALLOC_MAX_FACES 262144
+int dndsg_eval_rhs_noalloc(dndsg_ctx* ctx, const double* u, const void* urec, double* rhs, double t, void* stream);
+
 /* Error flags raised by kernels since the last call (bit 0: NaN or
  * non-positive density/pressure in a flux; bit 1: reduced-order face point). */
 int dndsg_get_status(dndsg_ctx* ctx, uint32_t* flags, uint64_t* n_reduced, void* stream);
