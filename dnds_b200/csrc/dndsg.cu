@@ -13,6 +13,7 @@
 
 #include "../../include/dndsg.h"
 #include "dndsg_bodies.cuh"
+#include "dndsg_limiter.cuh"
 
 using namespace dg;
 
@@ -42,6 +43,9 @@ struct dndsg_ctx {
   void* vrOp = nullptr;       // T
   void* faceBasis = nullptr;  // T
   double* Ainv = nullptr;
+  double *limFace = nullptr, *faceInd = nullptr, *indicator = nullptr;  // CWBAP limiter data
+  int32_t* wallCells = nullptr;  // cells with a Wall_Euler / Wall_NoSlip face
+  int64_t nWallCells = 0;
   // state
   double *u = nullptr, *uLast = nullptr, *rhs = nullptr, *dt = nullptr, *flux = nullptr, *lamA = nullptr,
          *dLam = nullptr, *scal = nullptr, *partial = nullptr;
@@ -177,10 +181,15 @@ struct VrOpSmem {
   __device__ __forceinline__ T operator()(int k, int e) const { return p[(k * 30 + e) * 32]; }
 };
 
-// VR Jacobi sweep with the per-cell operator blocks staged by one bulk async copy
-// per CTA (TILE cells = TILE*E values, contiguous in the AoSoA layout); relax = 1.
+template <class T>
+constexpr int vr_tile() { return sizeof(T) == 4 ? 128 : 64; }
+
+// VR Jacobi sweep, 4 threads per cell (one per conserved variable): the CTA's
+// TILE-cell operator tile is bulk-copied into shared memory as above; the 4
+// threads of a cell read the same shared words (broadcast), so each thread
+// keeps only its 5 accumulators and the warp keeps 8 cells' gathers in flight.
 template <class T, int TILE>
-__global__ void __launch_bounds__(TILE, 4) k_vr_tma(HotView<T> h, unsigned* flags) {
+__global__ void __launch_bounds__(TILE * 4) k_vr_tma4(HotView<T> h, unsigned* flags) {
   extern __shared__ __align__(128) unsigned char dsm[];
   __shared__ __align__(8) unsigned long long bar;
   const int E = h.nfmax * 30;
@@ -199,21 +208,97 @@ __global__ void __launch_bounds__(TILE, 4) k_vr_tma(HotView<T> h, unsigned* flag
   }
   const bool ok = mbar_wait(b, 0, kWaitLimit);
   if (__syncthreads_or(!ok)) {
-    // the copy did not land in time: flag it, let the copy drain (bounded) and leave
     if (tid == 0) {
       atomicOr(flags, kFlagTimeout);
       mbar_wait(b, 0, kWaitLimit);
     }
     return;
   }
-  const int64_t i = c0 + tid;
+  const int cl = tid >> 2, v = tid & 3;
+  const int64_t i = c0 + cl;
   if (i < h.N) {
     const T* sm = reinterpret_cast<const T*>(dsm);
-    vr_cell_op<T, true>(i, h, VrOpSmem<T>{sm + (tid >> 5) * E * 32 + (tid & 31)});
+    vr_cell_var<T>(i, v, h, VrOpSmem<T>{sm + (cl >> 5) * E * 32 + (cl & 31)});
+  }
+}
+
+// interior faces, 3 threads per face (one per gauss point, lanes 30 and 31 idle):
+// each thread forms its gauss point's flux, the three are summed with shuffles
+template <class T, int RIEMANN>
+__global__ void __launch_bounds__(192) k_face_flux_gp(HotView<T> h, int64_t nf, unsigned* flags,
+                                                      unsigned long long* nredAcc) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int fl = lane / 3, g = lane - 3 * (lane / 3);
+  const int64_t f = warp * 10 + fl;
+  const bool active = fl < 10 && f < nf;
+  bool bad = false;
+  int nred = 0;
+  double part[4] = {0, 0, 0, 0};
+  double uL[4] = {0, 0, 0, 0}, uR[4] = {0, 0, 0, 0}, nx = 0, ny = 0, area = 0;
+  if (active) {
+    load4<T>(&h.u[(int64_t)h.faceL[f] * 4], uL);
+    load4<T>(&h.u[(int64_t)h.faceR[f] * 4], uR);
+    nx = h.faceNormal[2 * f]; ny = h.faceNormal[2 * f + 1]; area = h.faceArea[f];
+    if constexpr (sizeof(T) == 4 && RIEMANN == 1) {
+      float o[4];
+      nred = gp_flux_delta32(f, g, h, uL, uR, nx, ny, area, o, bad);
+      for (int k = 0; k < 4; k++) part[k] = (double)o[k];
+    } else {
+      nred = gp_flux_full<T, RIEMANN>(f, g, h, uL, uR, nx, ny, area, part, bad);
+    }
+  }
+  for (int k = 0; k < 4; k++) {
+    double a = __shfl_down_sync(0xffffffffu, part[k], 1);
+    double c = __shfl_down_sync(0xffffffffu, part[k], 2);
+    part[k] += a + c;
+  }
+  if (active && g == 0) {
+    if constexpr (sizeof(T) == 4 && RIEMANN == 1) {
+      double m[4];
+      face_mean_flux(f, uL, uR, nx, ny, area, h.gamma, m);
+      for (int k = 0; k < 4; k++) part[k] += m[k];
+    }
+    for (int k = 0; k < 4; k++)
+      if (!(part[k] == part[k])) bad = true;
+    double* o = &h.flux[f * 4];
+    *reinterpret_cast<double2*>(o) = make_double2(part[0], part[1]);
+    *reinterpret_cast<double2*>(o + 2) = make_double2(part[2], part[3]);
+  }
+  const unsigned anyBad = __ballot_sync(0xffffffffu, bad);
+  const int rs = __reduce_add_sync(0xffffffffu, nred);
+  if (lane == 0) {
+    if (anyBad) atomicOr(flags, 1u);
+    if (rs) atomicAdd(nredAcc, (unsigned long long)rs);
   }
 }
 template <class T>
-constexpr int vr_tile() { return sizeof(T) == 4 ? 128 : 64; }
+__global__ void k_vr_wall_fixup(HotView<T> h, const int32_t* cells, int64_t n) {
+  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k < n) vr_wall_fixup<T>(cells[k], h);
+}
+// ---- CWBAP limiter: face indicator integrals, cell indicator, limiting pass
+__global__ void k_setup_limiter(MeshView m, SetupParams p, const CellSetup* cells, const double* faceW, double* lim,
+                                int* bad) {
+  int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (f < m.F && !setup_limiter_face(f, m, p, cells, faceW, lim)) atomicOr(bad, 4);
+}
+template <class T>
+__global__ void k_lim_face(LimView v, const T* urec) {
+  int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (f < v.F) limiter_face_indicator<T>(f, v, urec);
+}
+__global__ void k_lim_cell_indicator(LimView v) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < v.N) v.indicator[i] = limiter_cell_indicator(i, v);
+}
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_lim_apply(LimView v, const T* urec, T* out) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < v.N) limiter_cell<T>(i, v, urec, out);
+}
+
+inline unsigned gp_grid(int64_t nf) { return (unsigned)(((nf + 9) / 10 + 5) / 6); }
 
 __device__ __forceinline__ double stage_time(const double* scal, int useDev, double tHost, double c) {
   return useDev ? scal[S_T] + c * scal[S_DT] : tHost;
@@ -411,7 +496,8 @@ int run_vr(dndsg_ctx* c, bool inc, cudaStream_t s) {
   } else if (r1) {
     constexpr int TILE = vr_tile<T>();
     const size_t smem = (size_t)TILE * c->nfmax * 30 * sizeof(T);
-    k_vr_tma<T, TILE><<<(unsigned)((c->N + TILE - 1) / TILE), TILE, smem, s>>>(h, c->flags);
+    k_vr_tma4<T, TILE><<<(unsigned)((c->N + TILE - 1) / TILE), TILE * 4, smem, s>>>(h, c->flags);
+    if (c->nWallCells > 0) k_vr_wall_fixup<T><<<grid_for(c->nWallCells), kBlock, 0, s>>>(h, c->wallCells, c->nWallCells);
   } else {
     k_vr<T, false, false><<<grid_for(c->N), kBlock, 0, s>>>(h, nullptr);
   }
@@ -419,18 +505,39 @@ int run_vr(dndsg_ctx* c, bool inc, cudaStream_t s) {
   return 0;
 }
 
+LimView lim_view(dndsg_ctx* c, int ifAll) {
+  LimView v;
+  v.N = c->N; v.F = c->F; v.Fi = c->Fi; v.nfmax = c->nfmax;
+  v.cellFace = c->cellFace; v.faceL = c->faceL; v.faceR = c->faceR;
+  v.faceNormal = c->faceNormal; v.faceArea = c->faceArea; v.limFace = c->limFace;
+  v.u = c->u; v.faceInd = c->faceInd; v.indicator = c->indicator;
+  v.gamma = c->s.gamma; v.tangWeight = c->s.tang_weight; v.tangModMin = c->s.tang_weight_mod_min;
+  v.tangModPower = c->s.tang_weight_mod_power; v.tangModLoc = c->s.tang_weight_mod_loc; v.vol = c->vol;
+  v.porder2 = (double)(c->s.rec_order * c->s.rec_order);
+  v.scale = c->s.wbap_smooth_indicator_scale; v.nStd = c->s.wbap_n_std; v.ifAll = ifAll;
+  return v;
+}
+
+// ReconstructionWBAPLimitFacialV3 on the resident urec (result swapped into urec)
+template <class T>
+void run_limiter(dndsg_ctx* c, int ifAll, cudaStream_t s) {
+  LimView v = lim_view(c, ifAll);
+  k_lim_face<T><<<grid_for(c->F), kBlock, 0, s>>>(v, (const T*)c->urec);
+  k_lim_cell_indicator<<<grid_for(c->N), kBlock, 0, s>>>(v);
+  k_lim_apply<T><<<grid_for(c->N), kBlock, 0, s>>>(v, (const T*)c->urec, (T*)c->urecNew);
+  std::swap(c->urec, c->urecNew);
+}
+
 template <class T>
 void launch_flux(dndsg_ctx* c, int useDev, double tHost, double cst, cudaStream_t s) {
   HotView<T> h = view<T>(c);
   const int64_t Fi = c->Fi, F = c->F;
   if (c->s.riemann == 2) {
-    if (Fi > 0)
-      k_face_flux<T, 2, false><<<grid_for(Fi), kBlock, 0, s>>>(h, 0, Fi, c->scal, useDev, tHost, cst, c->flags, c->nreduced);
+    if (Fi > 0) k_face_flux_gp<T, 2><<<gp_grid(Fi), 192, 0, s>>>(h, Fi, c->flags, c->nreduced);
     if (F > Fi)
       k_face_flux<T, 2, true><<<grid_for(F - Fi), kBlock, 0, s>>>(h, Fi, F, c->scal, useDev, tHost, cst, c->flags, c->nreduced);
   } else {
-    if (Fi > 0)
-      k_face_flux<T, 1, false><<<grid_for(Fi), kBlock, 0, s>>>(h, 0, Fi, c->scal, useDev, tHost, cst, c->flags, c->nreduced);
+    if (Fi > 0) k_face_flux_gp<T, 1><<<gp_grid(Fi), 192, 0, s>>>(h, Fi, c->flags, c->nreduced);
     if (F > Fi)
       k_face_flux<T, 1, true><<<grid_for(F - Fi), kBlock, 0, s>>>(h, Fi, F, c->scal, useDev, tHost, cst, c->flags, c->nreduced);
   }
@@ -453,7 +560,7 @@ int run_step(dndsg_ctx* c, double cfl, double tEnd, cudaStream_t s) {
   const double cst[3] = {0.0, 1.0, 0.5};
   for (int stg = 0; stg < 3; stg++) {
     run_vr<T>(c, false, s);
-    if (c->s.limiter) { /* limiter kernels come with the CWBAP path */ }
+    if (c->s.limiter) run_limiter<T>(c, 0, s);
     launch_flux<T>(c, 1, 0.0, cst[stg], s);
     HotView<T> h = view<T>(c);
     if (stg == 0) k_cell_update<T, 0><<<grid_for(c->N), kBlock, 0, s>>>(h, c->scal);
@@ -587,7 +694,7 @@ int setup_run(dndsg_ctx* c, const dndsg_mesh_desc* md) {
   if ((rc = dalloc(c, c->vrOp, sizeof(T) * aos_size(((N + 127) / 128) * 128, c->nfmax * 30)))) return rc;
   {
     constexpr int TILE = vr_tile<T>();
-    DG_CUDA(c, cudaFuncSetAttribute(k_vr_tma<T, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    DG_CUDA(c, cudaFuncSetAttribute(k_vr_tma4<T, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)(TILE * c->nfmax * 30 * sizeof(T))));
   }
   if (hasWallCorr)
@@ -595,11 +702,33 @@ int setup_run(dndsg_ctx* c, const dndsg_mesh_desc* md) {
   k_setup_matrices<T><<<grid_for(N), kBlock>>>(m, p, cells, faceW, c->cellFace, c->nfmax, (T*)c->vrOp, c->vrNbr,
                                                c->vrMode, c->vrFace, c->Ainv, dBad);
   if ((rc = check_launch(c))) return rc;
+  if (c->s.limiter) {
+    if ((rc = dalloc(c, c->limFace, sizeof(double) * aos_size(F, kLimE)))) return rc;
+    if ((rc = dalloc(c, c->faceInd, sizeof(double) * 4 * F))) return rc;
+    if ((rc = dalloc(c, c->indicator, sizeof(double) * N))) return rc;
+    k_setup_limiter<<<grid_for(F), kBlock>>>(m, p, cells, faceW, c->limFace, dBad);
+    if ((rc = check_launch(c))) return rc;
+  }
   DG_CUDA(c, cudaDeviceSynchronize());
   int bad = 0;
   DG_CUDA(c, cudaMemcpy(&bad, dBad, sizeof(int), cudaMemcpyDeviceToHost));
   if (bad & 1) return fail(c, DNDSG_SETUP_ERROR, "non-positive cell jacobian (cell not counter-clockwise?)");
   if (bad & 2) return fail(c, DNDSG_SETUP_ERROR, "VR matrix A_ii is not positive definite");
+  if (bad & 4) return fail(c, DNDSG_SETUP_ERROR, "singular secondary-reconstruction matrix at a face");
+  {
+    std::vector<char> isWall(N, 0);
+    for (int64_t f = 0; f < F; f++) {
+      int bc = md->face_bc[f];
+      if (md->face_cells[2 * f + 1] < 0 && (bc == BC_WALL_EULER || bc == BC_WALL_NOSLIP)) isWall[md->face_cells[2 * f]] = 1;
+    }
+    std::vector<int32_t> wc;
+    for (int64_t i = 0; i < N; i++) if (isWall[i]) wc.push_back((int32_t)i);
+    c->nWallCells = (int64_t)wc.size();
+    if (!wc.empty()) {
+      if ((rc = dalloc(c, c->wallCells, sizeof(int32_t) * wc.size()))) return rc;
+      DG_CUDA(c, cudaMemcpy(c->wallCells, wc.data(), sizeof(int32_t) * wc.size(), cudaMemcpyHostToDevice));
+    }
+  }
   if ((rc = dalloc(c, c->closure, sizeof(double) * 2 * N))) return rc;
   DG_CUDA(c, cudaMemcpy(c->closure, closure.data(), sizeof(double) * 2 * N, cudaMemcpyHostToDevice));
   // setup-only buffers are released here
@@ -651,7 +780,6 @@ int dndsg_create(const dndsg_mesh_desc* mesh, const dndsg_settings* settings, in
   if (c->s.rec_order != 2) return fail(c, DNDSG_UNSUPPORTED, "rec_order must be 2 (P2)");
   if (c->s.sor_instead) return fail(c, DNDSG_UNSUPPORTED, "the GPU VR sweep is Jacobi (sor_instead must be 0)");
   if (c->s.riemann != 1 && c->s.riemann != 2) return fail(c, DNDSG_UNSUPPORTED, "riemann must be 1 (Roe) or 2 (HLLC)");
-  if (c->s.limiter) return fail(c, DNDSG_UNSUPPORTED, "limiter not available in this build");
   if (mesh->n_cells <= 0 || mesh->n_faces <= 0 || mesh->n_cells > INT32_MAX || mesh->n_faces > INT32_MAX)
     return fail(c, DNDSG_BAD_ARGUMENT, "mesh sizes out of range");
   c->N = mesh->n_cells;
@@ -790,7 +918,17 @@ int dndsg_vr_jacobi_step(dndsg_ctx* c, int nsweeps, double* inc_out, void* s) {
 }
 
 int dndsg_limiter_wbap(dndsg_ctx* c, int if_all, double* indicator_out, void* s) {
-  return fail(c, DNDSG_UNSUPPORTED, "limiter not available in this build");
+  if (!c) return DNDSG_BAD_ARGUMENT;
+  if (!c->limFace) return fail(c, DNDSG_UNSUPPORTED, "context was created without the limiter (settings.limiter = 0)");
+  if (c->fp32) run_limiter<float>(c, if_all, st(s));
+  else run_limiter<double>(c, if_all, st(s));
+  int rc = check_launch(c);
+  if (rc) return rc;
+  if (indicator_out) {
+    DG_CUDA(c, cudaMemcpyAsync(indicator_out, c->indicator, sizeof(double) * c->N, cudaMemcpyDeviceToHost, st(s)));
+    DG_CUDA(c, cudaStreamSynchronize(st(s)));
+  }
+  return 0;
 }
 
 int dndsg_eval_dt(dndsg_ctx* c, double cfl, double max_dt, int use_local_dt, double* dt_min_out, void* s) {

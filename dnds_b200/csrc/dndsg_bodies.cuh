@@ -825,16 +825,17 @@ namespace dg {
 
 // ---------------------------------------------------------------- thread-per-(item, sub-item) bodies
 // VR sweep of one variable v of cell i: acc[r] = sum_k (A^-1B_k urec_j(k))[r][v] + (A^-1b_k)[r] du_k[v]
-// (relax = 1).  Four threads (v = 0..3) cooperate on a cell.
+// (relax = 1).  Four threads (v = 0..3) cooperate on a cell.  Wall_Euler / Wall_NoSlip
+// slots are skipped here and added by vr_wall_fixup.
 template <class T, class Op>
 DG_HD void vr_cell_var(int64_t i, int v, const HotView<T>& h, const Op& opk) {
   T acc[5] = {T(0), T(0), T(0), T(0), T(0)};
   const double uiv = h.u[i * 4 + v];
   for (int k = 0; k < h.nfmax; k++) {
     const int mode = h.vrMode[aos(i, k, h.nfmax)];
-    if (mode == VR_EMPTY) continue;
+    if (mode == VR_EMPTY || mode == VR_WALLCORR) continue;
     const int32_t j = h.vrNbr[aos(i, k, h.nfmax)];
-    if (mode == VR_INNER || mode == VR_FAR) {
+    if (mode != VR_WALL) {
       const T* rj = &h.urec[(int64_t)j * 20 + v];
       T rv[5];
       for (int q = 0; q < 5; q++) rv[q] = rj[4 * q];
@@ -844,48 +845,59 @@ DG_HD void vr_cell_var(int64_t i, int v, const HotView<T>& h, const Op& opk) {
         acc[r] = s;
       }
     }
-    if (mode == VR_INNER || mode == VR_WALL) {
+    if (mode != VR_FAR) {
       const T du = mode == VR_INNER ? T(h.u[(int64_t)j * 4 + v] - uiv) : T(0.0 - uiv);
       for (int r = 0; r < 5; r++) acc[r] += opk(k, 25 + r) * du;
-    }
-    if (mode == VR_WALLCORR) {
-      // the wall state couples the velocity components: every thread forms the full correction
-      int32_t f = h.vrFace[aos(i, k, h.nfmax)];
-      double nx = h.faceNormal[2 * f], ny = h.faceNormal[2 * f + 1];
-      double w0 = h.faceW0[f], area = h.faceArea[f];
-      int bc = h.faceBC[f];
-      double ui[4];
-      for (int c = 0; c < 4; c++) ui[c] = h.u[i * 4 + c];
-      double corr[5] = {0, 0, 0, 0, 0};
-      for (int g = 0; g < 3; g++) {
-        double phi[5], uBL[4];
-        for (int q = 0; q < 5; q++) phi[q] = (double)h.faceBasis[aos(f, g * 5 + q, 30)];
-        for (int c = 0; c < 4; c++) {
-          double s = 0;
-          for (int q = 0; q < 5; q++) s += phi[q] * (double)h.urec[i * 20 + q * 4 + c];
-          uBL[c] = s + ui[c];
-        }
-        double uBV;
-        if (v == 0 || v == 3) uBV = uBL[v];
-        else if (bc == BC_WALL_EULER) {
-          double d = nx * uBL[1] + ny * uBL[2];
-          uBV = uBL[v] - (v == 1 ? nx : ny) * d;
-        } else {
-          uBV = -uBL[v];
-        }
-        double jw = 0.5 * area * l3_weight(g);
-        for (int q = 0; q < 5; q++) corr[q] += phi[q] * w0 * w0 * (uBV - ui[v]) * jw;
-      }
-      const double* Ai = &h.Ainv[i * 25];
-      for (int r = 0; r < 5; r++) {
-        double s = 0;
-        for (int q = 0; q < 5; q++) s += Ai[r * 5 + q] * corr[q];
-        acc[r] += T(s);
-      }
     }
   }
   T* out = &h.urecNew[i * 20 + v];
   for (int q = 0; q < 5; q++) out[4 * q] = acc[q];
+}
+
+// Wall_Euler / Wall_NoSlip slots of cell i (DNDS_FV_VR.hpp:1577-1665): adds
+// relax * A^-1 * (integral of the weighted jump to the wall state) to urecNew
+template <class T>
+DG_HD void vr_wall_fixup(int64_t i, const HotView<T>& h) {
+  double ui[4];
+  for (int c = 0; c < 4; c++) ui[c] = h.u[i * 4 + c];
+  double add[5][4];
+  for (int r = 0; r < 5; r++) for (int c = 0; c < 4; c++) add[r][c] = 0;
+  for (int k = 0; k < h.nfmax; k++) {
+    if (h.vrMode[aos(i, k, h.nfmax)] != VR_WALLCORR) continue;
+    int32_t f = h.vrFace[aos(i, k, h.nfmax)];
+    double nx = h.faceNormal[2 * f], ny = h.faceNormal[2 * f + 1];
+    double w0 = h.faceW0[f], area = h.faceArea[f];
+    int bc = h.faceBC[f];
+    double corr[5][4];
+    for (int q = 0; q < 5; q++) for (int c = 0; c < 4; c++) corr[q][c] = 0;
+    for (int g = 0; g < 3; g++) {
+      double phi[5], uBL[4], uBV[4];
+      for (int q = 0; q < 5; q++) phi[q] = (double)h.faceBasis[aos(f, g * 5 + q, 30)];
+      for (int c = 0; c < 4; c++) {
+        double s = 0;
+        for (int q = 0; q < 5; q++) s += phi[q] * (double)h.urec[i * 20 + q * 4 + c];
+        uBL[c] = s + ui[c];
+      }
+      if (bc == BC_WALL_EULER) {
+        double d = nx * uBL[1] + ny * uBL[2];
+        uBV[0] = uBL[0]; uBV[1] = uBL[1] - nx * d; uBV[2] = uBL[2] - ny * d; uBV[3] = uBL[3];
+      } else {
+        uBV[0] = uBL[0]; uBV[1] = -uBL[1]; uBV[2] = -uBL[2]; uBV[3] = uBL[3];
+      }
+      double jw = 0.5 * area * l3_weight(g);
+      for (int q = 0; q < 5; q++)
+        for (int c = 0; c < 4; c++) corr[q][c] += phi[q] * w0 * w0 * (uBV[c] - ui[c]) * jw;
+    }
+    const double* Ai = &h.Ainv[i * 25];
+    for (int r = 0; r < 5; r++)
+      for (int c = 0; c < 4; c++) {
+        double s = 0;
+        for (int q = 0; q < 5; q++) s += Ai[r * 5 + q] * corr[q][c];
+        add[r][c] += s;
+      }
+  }
+  for (int r = 0; r < 5; r++)
+    for (int c = 0; c < 4; c++) h.urecNew[i * 20 + r * 4 + c] += T(h.relax * add[r][c]);
 }
 
 // -area (F(uL) + F(uR)) . n / 2 of an interior face: the FP64 part of the flux-difference form

@@ -39,7 +39,32 @@ CASES = {
 }
 
 
+def make_limiter_case():
+    """2-D Riemann mesh with the CWBAP limiter: indicator and limited face states
+    after 3 VR sweeps, then 2 SSP-RK3 steps with the limiter in every stage."""
+    m = M.riemann_mesh(16, jitter=0.15, seed=4321)
+    cfg = S.preset("riemann")
+    o = pyoracle.Oracle(m, cfg, n_threads=1)
+    u0 = G.quadrant_states(m, S.RIEMANN_2D_STATES)
+    o.set_u(u0)
+    o.vr_step(3)
+    ind = o.limiter(False)
+    fv = o.face_values(0.0)
+    o.limiter(True)
+    fv_all = o.face_values(0.0)
+    o.set_u(u0)
+    o.set_urec(np.zeros((m.n_cells, 5, 4)))
+    t = 0.0
+    for _ in range(2):
+        _, d = o.eval_dt(0.4)
+        o.ssprk3_step(d, t)
+        t += d
+    return dict(u0=u0, indicator=ind, face_values_lim=fv, face_values_limall=fv_all, u_rk2=o.get_u(), t_rk2=t)
+
+
 def make_case(name):
+    if name == "riemann_tri16_limiter":
+        return make_limiter_case()
     mk, pre, init = CASES[name]
     m = mk()
     cfg = S.preset(pre, useLimiter=False)
@@ -62,9 +87,11 @@ def make_case(name):
     return dict(u0=u0, face_values=fv, dt=dt, dtmin=dtmin, rhs=rhs, u_rk2=u2, t_rk2=t)
 
 
+LIMITER_CASES = ["riemann_tri16_limiter"]
+
 if __name__ == "__main__":
     pyoracle.build()
-    for name in CASES:
+    for name in list(CASES) + LIMITER_CASES:
         d = make_case(name)
         np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **d)
         print(name, {k: np.shape(v) for k, v in d.items()})

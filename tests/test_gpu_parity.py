@@ -77,6 +77,29 @@ def test_fp32_bulk_close_to_golden(name):
     assert _rel(rhs, ref["rhs"]) < 2e-5
 
 
+@pytest.mark.parametrize("precision,tol", [(0, 1e-10), (1, 1e-4)])
+def test_limiter_matches_golden(precision, tol):
+    """CWBAP limiter (ReconstructionWBAPLimitFacialV3) and SSP-RK3 with the limiter, 2-D Riemann mesh."""
+    m = M.riemann_mesh(16, jitter=0.15, seed=4321)
+    ref = np.load(os.path.join(GOLDEN, "riemann_tri16_limiter.npz"))
+    s = _solver(m, S.preset("riemann"), precision)
+    s.set_u(ref["u0"])
+    s.ReconstructionJacobiStep(3)
+    ind = s.ReconstructionWBAPLimitFacialV3(False, indicator=True)
+    assert _rel(ind, ref["indicator"]) < tol
+    assert _rel(s.face_values(0.0), ref["face_values_lim"]) < tol
+    s.ReconstructionWBAPLimitFacialV3(True)
+    assert _rel(s.face_values(0.0), ref["face_values_limall"]) < tol
+    s.set_u(ref["u0"])
+    s.set_urec(np.zeros((m.n_cells, 5, 4)))
+    s.time = 0.0
+    for _ in range(2):
+        s.ssprk3_step(0.4, 1e300)
+    assert _rel(s.get_u(), ref["u_rk2"]) < (1e-11 if precision == 0 else 1e-5)
+    flags, _ = s.status()
+    assert flags == 0
+
+
 def test_vortex_c1_against_oracle(oracle_lib):
     """40x40 periodic quads, P2 VR + Roe, SSP-RK3 CFL 0.5: 20 steps GPU vs oracle."""
     m = M.vortex_mesh(40, False)

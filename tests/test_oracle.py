@@ -123,7 +123,7 @@ def test_freestream_and_conservation(oracle_lib):
 
 
 @pytest.mark.parametrize("name", ["vortex_quad10", "vortex_tri8_jitter", "riemann_tri8", "eulerwall_quad6x5",
-                                  "farfield_tri6x5"])
+                                  "farfield_tri6x5", "riemann_tri16_limiter"])
 def test_oracle_matches_golden(oracle_lib, name):
     import importlib.util
 
@@ -132,6 +132,8 @@ def test_oracle_matches_golden(oracle_lib, name):
     spec.loader.exec_module(mg)
     ref = np.load(os.path.join(GOLDEN, f"{name}.npz"))
     d = mg.make_case(name)
-    for k in ("face_values", "dt", "rhs", "u_rk2"):
+    keys = ("indicator", "face_values_lim", "face_values_limall", "u_rk2") if "limiter" in name else \
+        ("face_values", "dt", "rhs", "u_rk2")
+    for k in keys:
         sc = max(np.abs(ref[k]).max(), 1e-300)
         assert np.abs(d[k] - ref[k]).max() <= 1e-12 * sc, k
