@@ -8,11 +8,14 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libdndsg.so")
-SOURCES = [os.path.join(HERE, "csrc", f) for f in ("dndsg.cu", "dndsg_bodies.cuh", "dndsg_math.cuh")]
+SOURCES = [os.path.join(HERE, "csrc", f) for f in ("dndsg.cu", "dndsg_bodies.cuh", "dndsg_math.cuh", "dndsg_limiter.cuh")]
 HEADERS = [os.path.join(ROOT, "include", "dndsg.h")]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "-shared", "--expt-relaxed-constexpr"]
+# --prec-div/--prec-sqrt=false relax single-precision division and square root only
+# (the FP32-bulk flux); double precision is unaffected
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "-shared", "--expt-relaxed-constexpr",
+         "--prec-div=false", "--prec-sqrt=false"]
 
 
 def needs_build() -> bool:

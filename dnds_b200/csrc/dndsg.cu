@@ -184,18 +184,19 @@ struct VrOpSmem {
 template <class T>
 constexpr int vr_tile() { return sizeof(T) == 4 ? 128 : 64; }
 
-// VR Jacobi sweep, 4 threads per cell (one per conserved variable): the CTA's
-// TILE-cell operator tile is bulk-copied into shared memory as above; the 4
-// threads of a cell read the same shared words (broadcast), so each thread
-// keeps only its 5 accumulators and the warp keeps 8 cells' gathers in flight.
-template <class T, int TILE>
+// VR Jacobi sweep, 4 threads per cell (one per conserved variable).  One
+// elected thread bulk-copies the CTA's TILE-cell operator tile (contiguous in the
+// AoSoA layout) into shared memory on an mbarrier; meanwhile every thread issues
+// its neighbour gathers; then the 4 threads of a cell read the same shared words
+// (broadcast) and keep only 5 accumulators each.
+template <class T, int TILE, int NF>
 __global__ void __launch_bounds__(TILE * 4) k_vr_tma4(HotView<T> h, unsigned* flags) {
   extern __shared__ __align__(128) unsigned char dsm[];
   __shared__ __align__(8) unsigned long long bar;
-  const int E = h.nfmax * 30;
+  constexpr int E = NF * 30;
   const int tid = threadIdx.x;
   const int64_t c0 = (int64_t)blockIdx.x * TILE;
-  const uint32_t bytes = (uint32_t)(TILE * E * sizeof(T));
+  constexpr uint32_t bytes = (uint32_t)(TILE * E * sizeof(T));
   const uint32_t b = smem_u32(&bar);
   if (tid == 0) {
     mbar_init(b, 1);
@@ -206,6 +207,10 @@ __global__ void __launch_bounds__(TILE * 4) k_vr_tma4(HotView<T> h, unsigned* fl
     mbar_expect_tx(b, bytes);
     bulk_g2s(smem_u32(dsm), h.vrOp + c0 * E, bytes, b);
   }
+  const int cl = tid >> 2, v = tid & 3;
+  const int64_t i = c0 + cl;
+  VrPre<T, NF> pre;
+  if (i < h.N) vr_var_prefetch<T, NF>(i, v, h, pre);
   const bool ok = mbar_wait(b, 0, kWaitLimit);
   if (__syncthreads_or(!ok)) {
     if (tid == 0) {
@@ -214,64 +219,12 @@ __global__ void __launch_bounds__(TILE * 4) k_vr_tma4(HotView<T> h, unsigned* fl
     }
     return;
   }
-  const int cl = tid >> 2, v = tid & 3;
-  const int64_t i = c0 + cl;
   if (i < h.N) {
     const T* sm = reinterpret_cast<const T*>(dsm);
-    vr_cell_var<T>(i, v, h, VrOpSmem<T>{sm + (cl >> 5) * E * 32 + (cl & 31)});
+    vr_var_compute<T, NF>(i, v, h, pre, VrOpSmem<T>{sm + (cl >> 5) * E * 32 + (cl & 31)});
   }
 }
 
-// interior faces, 3 threads per face (one per gauss point, lanes 30 and 31 idle):
-// each thread forms its gauss point's flux, the three are summed with shuffles
-template <class T, int RIEMANN>
-__global__ void __launch_bounds__(192) k_face_flux_gp(HotView<T> h, int64_t nf, unsigned* flags,
-                                                      unsigned long long* nredAcc) {
-  const int lane = threadIdx.x & 31;
-  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  const int fl = lane / 3, g = lane - 3 * (lane / 3);
-  const int64_t f = warp * 10 + fl;
-  const bool active = fl < 10 && f < nf;
-  bool bad = false;
-  int nred = 0;
-  double part[4] = {0, 0, 0, 0};
-  double uL[4] = {0, 0, 0, 0}, uR[4] = {0, 0, 0, 0}, nx = 0, ny = 0, area = 0;
-  if (active) {
-    load4<T>(&h.u[(int64_t)h.faceL[f] * 4], uL);
-    load4<T>(&h.u[(int64_t)h.faceR[f] * 4], uR);
-    nx = h.faceNormal[2 * f]; ny = h.faceNormal[2 * f + 1]; area = h.faceArea[f];
-    if constexpr (sizeof(T) == 4 && RIEMANN == 1) {
-      float o[4];
-      nred = gp_flux_delta32(f, g, h, uL, uR, nx, ny, area, o, bad);
-      for (int k = 0; k < 4; k++) part[k] = (double)o[k];
-    } else {
-      nred = gp_flux_full<T, RIEMANN>(f, g, h, uL, uR, nx, ny, area, part, bad);
-    }
-  }
-  for (int k = 0; k < 4; k++) {
-    double a = __shfl_down_sync(0xffffffffu, part[k], 1);
-    double c = __shfl_down_sync(0xffffffffu, part[k], 2);
-    part[k] += a + c;
-  }
-  if (active && g == 0) {
-    if constexpr (sizeof(T) == 4 && RIEMANN == 1) {
-      double m[4];
-      face_mean_flux(f, uL, uR, nx, ny, area, h.gamma, m);
-      for (int k = 0; k < 4; k++) part[k] += m[k];
-    }
-    for (int k = 0; k < 4; k++)
-      if (!(part[k] == part[k])) bad = true;
-    double* o = &h.flux[f * 4];
-    *reinterpret_cast<double2*>(o) = make_double2(part[0], part[1]);
-    *reinterpret_cast<double2*>(o + 2) = make_double2(part[2], part[3]);
-  }
-  const unsigned anyBad = __ballot_sync(0xffffffffu, bad);
-  const int rs = __reduce_add_sync(0xffffffffu, nred);
-  if (lane == 0) {
-    if (anyBad) atomicOr(flags, 1u);
-    if (rs) atomicAdd(nredAcc, (unsigned long long)rs);
-  }
-}
 template <class T>
 __global__ void k_vr_wall_fixup(HotView<T> h, const int32_t* cells, int64_t n) {
   int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -298,7 +251,6 @@ __global__ void __launch_bounds__(kBlock) k_lim_apply(LimView v, const T* urec, 
   if (i < v.N) limiter_cell<T>(i, v, urec, out);
 }
 
-inline unsigned gp_grid(int64_t nf) { return (unsigned)(((nf + 9) / 10 + 5) / 6); }
 
 __device__ __forceinline__ double stage_time(const double* scal, int useDev, double tHost, double c) {
   return useDev ? scal[S_T] + c * scal[S_DT] : tHost;
@@ -496,7 +448,10 @@ int run_vr(dndsg_ctx* c, bool inc, cudaStream_t s) {
   } else if (r1) {
     constexpr int TILE = vr_tile<T>();
     const size_t smem = (size_t)TILE * c->nfmax * 30 * sizeof(T);
-    k_vr_tma4<T, TILE><<<(unsigned)((c->N + TILE - 1) / TILE), TILE * 4, smem, s>>>(h, c->flags);
+    if (c->nfmax == 3)
+      k_vr_tma4<T, TILE, 3><<<(unsigned)((c->N + TILE - 1) / TILE), TILE * 4, smem, s>>>(h, c->flags);
+    else
+      k_vr_tma4<T, TILE, 4><<<(unsigned)((c->N + TILE - 1) / TILE), TILE * 4, smem, s>>>(h, c->flags);
     if (c->nWallCells > 0) k_vr_wall_fixup<T><<<grid_for(c->nWallCells), kBlock, 0, s>>>(h, c->wallCells, c->nWallCells);
   } else {
     k_vr<T, false, false><<<grid_for(c->N), kBlock, 0, s>>>(h, nullptr);
@@ -533,11 +488,13 @@ void launch_flux(dndsg_ctx* c, int useDev, double tHost, double cst, cudaStream_
   HotView<T> h = view<T>(c);
   const int64_t Fi = c->Fi, F = c->F;
   if (c->s.riemann == 2) {
-    if (Fi > 0) k_face_flux_gp<T, 2><<<gp_grid(Fi), 192, 0, s>>>(h, Fi, c->flags, c->nreduced);
+    if (Fi > 0)
+      k_face_flux<T, 2, false><<<grid_for(Fi), kBlock, 0, s>>>(h, 0, Fi, c->scal, useDev, tHost, cst, c->flags, c->nreduced);
     if (F > Fi)
       k_face_flux<T, 2, true><<<grid_for(F - Fi), kBlock, 0, s>>>(h, Fi, F, c->scal, useDev, tHost, cst, c->flags, c->nreduced);
   } else {
-    if (Fi > 0) k_face_flux_gp<T, 1><<<gp_grid(Fi), 192, 0, s>>>(h, Fi, c->flags, c->nreduced);
+    if (Fi > 0)
+      k_face_flux<T, 1, false><<<grid_for(Fi), kBlock, 0, s>>>(h, 0, Fi, c->scal, useDev, tHost, cst, c->flags, c->nreduced);
     if (F > Fi)
       k_face_flux<T, 1, true><<<grid_for(F - Fi), kBlock, 0, s>>>(h, Fi, F, c->scal, useDev, tHost, cst, c->flags, c->nreduced);
   }
@@ -694,8 +651,10 @@ int setup_run(dndsg_ctx* c, const dndsg_mesh_desc* md) {
   if ((rc = dalloc(c, c->vrOp, sizeof(T) * aos_size(((N + 127) / 128) * 128, c->nfmax * 30)))) return rc;
   {
     constexpr int TILE = vr_tile<T>();
-    DG_CUDA(c, cudaFuncSetAttribute(k_vr_tma4<T, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)(TILE * c->nfmax * 30 * sizeof(T))));
+    DG_CUDA(c, cudaFuncSetAttribute(k_vr_tma4<T, TILE, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(TILE * 3 * 30 * sizeof(T))));
+    DG_CUDA(c, cudaFuncSetAttribute(k_vr_tma4<T, TILE, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(TILE * 4 * 30 * sizeof(T))));
   }
   if (hasWallCorr)
     if ((rc = dalloc(c, c->Ainv, sizeof(double) * 25 * N))) return rc;

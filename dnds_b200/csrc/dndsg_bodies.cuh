@@ -572,11 +572,12 @@ DG_HD int face_flux_roe_delta32(int64_t f, const HotView<float>& h, double out[4
     // CompressRecPart: fall back to the mean where density or internal energy would be negative
     float UL[4], UR[4];
     for (int v = 0; v < 4; v++) { UL[v] = bL[v] + dL[v]; UR[v] = bR[v] + dR[v]; }
-    if (UL[0] < 0.f || UL[3] - (UL[1] * UL[1] + UL[2] * UL[2]) * 0.5f / UL[0] < 0.f) {
+    // rho < 0 or internal energy E - |m|^2 / (2 rho) < 0, i.e. 2 rho E < |m|^2 for rho > 0
+    if (UL[0] < 0.f || 2.f * UL[0] * UL[3] < UL[1] * UL[1] + UL[2] * UL[2]) {
       for (int v = 0; v < 4; v++) { dL[v] = 0.f; UL[v] = bL[v]; }
       nred++;
     }
-    if (UR[0] < 0.f || UR[3] - (UR[1] * UR[1] + UR[2] * UR[2]) * 0.5f / UR[0] < 0.f) {
+    if (UR[0] < 0.f || 2.f * UR[0] * UR[3] < UR[1] * UR[1] + UR[2] * UR[2]) {
       for (int v = 0; v < 4; v++) { dR[v] = 0.f; UR[v] = bR[v]; }
       nred++;
     }
@@ -824,34 +825,59 @@ DG_HD bool setup_cell_matrices(int64_t i, const MeshView& m, const SetupParams& 
 namespace dg {
 
 // ---------------------------------------------------------------- thread-per-(item, sub-item) bodies
-// VR sweep of one variable v of cell i: acc[r] = sum_k (A^-1B_k urec_j(k))[r][v] + (A^-1b_k)[r] du_k[v]
-// (relax = 1).  Four threads (v = 0..3) cooperate on a cell.  Wall_Euler / Wall_NoSlip
-// slots are skipped here and added by vr_wall_fixup.
-template <class T, class Op>
-DG_HD void vr_cell_var(int64_t i, int v, const HotView<T>& h, const Op& opk) {
-  T acc[5] = {T(0), T(0), T(0), T(0), T(0)};
+// VR sweep of one variable v of cell i, relax = 1, split in two phases so a
+// kernel can issue every neighbour gather before it waits for its operator tile:
+//   vr_var_prefetch: slot modes, the neighbours' coefficients of variable v and
+//                    the mean differences du (NF = faces per cell, compile time);
+//   vr_var_compute:  acc[r] = sum_k (A^-1B_k urec_j(k))[r][v] + (A^-1b_k)[r] du_k[v].
+// Four threads (v = 0..3) cooperate on a cell.  Wall_Euler / Wall_NoSlip slots
+// are skipped here and added by vr_wall_fixup.
+template <class T, int NF>
+struct VrPre {
+  int mode[NF];
+  T rv[NF][5];
+  T du[NF];
+};
+template <class T, int NF>
+DG_HD void vr_var_prefetch(int64_t i, int v, const HotView<T>& h, VrPre<T, NF>& p) {
   const double uiv = h.u[i * 4 + v];
-  for (int k = 0; k < h.nfmax; k++) {
-    const int mode = h.vrMode[aos(i, k, h.nfmax)];
+  for (int k = 0; k < NF; k++) {
+    const int mode = h.vrMode[aos(i, k, NF)];
+    const int32_t j = h.vrNbr[aos(i, k, NF)];
+    p.mode[k] = mode;
+    const bool rec = mode == VR_INNER || mode == VR_FAR;
+    const T* rj = &h.urec[(int64_t)(rec ? j : i) * 20 + v];
+    for (int q = 0; q < 5; q++) p.rv[k][q] = rec ? rj[4 * q] : T(0);
+    const double uj = mode == VR_INNER ? h.u[(int64_t)j * 4 + v] : 0.0;
+    p.du[k] = (mode == VR_INNER || mode == VR_WALL) ? T(uj - uiv) : T(0);
+  }
+}
+template <class T, int NF, class Op>
+DG_HD void vr_var_compute(int64_t i, int v, const HotView<T>& h, const VrPre<T, NF>& p, const Op& opk) {
+  T acc[5] = {T(0), T(0), T(0), T(0), T(0)};
+  for (int k = 0; k < NF; k++) {
+    const int mode = p.mode[k];
     if (mode == VR_EMPTY || mode == VR_WALLCORR) continue;
-    const int32_t j = h.vrNbr[aos(i, k, h.nfmax)];
-    if (mode != VR_WALL) {
-      const T* rj = &h.urec[(int64_t)j * 20 + v];
-      T rv[5];
-      for (int q = 0; q < 5; q++) rv[q] = rj[4 * q];
-      for (int r = 0; r < 5; r++) {
-        T s = acc[r];
-        for (int q = 0; q < 5; q++) s += opk(k, r * 5 + q) * rv[q];
-        acc[r] = s;
-      }
-    }
-    if (mode != VR_FAR) {
-      const T du = mode == VR_INNER ? T(h.u[(int64_t)j * 4 + v] - uiv) : T(0.0 - uiv);
-      for (int r = 0; r < 5; r++) acc[r] += opk(k, 25 + r) * du;
+    for (int r = 0; r < 5; r++) {
+      T s = acc[r] + opk(k, 25 + r) * p.du[k];
+      for (int q = 0; q < 5; q++) s += opk(k, r * 5 + q) * p.rv[k][q];
+      acc[r] = s;
     }
   }
   T* out = &h.urecNew[i * 20 + v];
   for (int q = 0; q < 5; q++) out[4 * q] = acc[q];
+}
+template <class T, class Op>
+DG_HD void vr_cell_var(int64_t i, int v, const HotView<T>& h, const Op& opk) {
+  if (h.nfmax == 3) {
+    VrPre<T, 3> p;
+    vr_var_prefetch<T, 3>(i, v, h, p);
+    vr_var_compute<T, 3>(i, v, h, p, opk);
+  } else {
+    VrPre<T, 4> p;
+    vr_var_prefetch<T, 4>(i, v, h, p);
+    vr_var_compute<T, 4>(i, v, h, p, opk);
+  }
 }
 
 // Wall_Euler / Wall_NoSlip slots of cell i (DNDS_FV_VR.hpp:1577-1665): adds

@@ -39,6 +39,22 @@ CASES = {
 }
 
 
+def perturbed_quadrants(m):
+    """Four-quadrant Riemann states times a smooth perturbation, so that no
+    reconstruction coefficient is zero up to rounding: the WBAP biway of the
+    reference uses sign(u2), which jumps at u2 = 0, so on exactly constant
+    regions the limiter's decision depends on rounding noise."""
+    q = np.array(S.RIEMANN_2D_STATES)
+
+    def f(x, y):
+        k = np.where(x > 0.8, np.where(y > 0.8, 0, 3), np.where(y > 0.8, 1, 2))
+        pert = 1.0 + 0.05 * np.sin(6.3 * x + 1.1) * np.cos(5.1 * y + 0.3)
+        rho, u, v, p = q[k, 0] * pert, q[k, 1] + 0.02 * pert, q[k, 2] - 0.01 * pert, q[k, 3] * pert
+        return np.stack([rho, rho * u, rho * v, p / 0.4 + 0.5 * rho * (u * u + v * v)], -1)
+
+    return G.cell_average(m, f)
+
+
 def make_limiter_case():
     """2-D Riemann mesh with the CWBAP limiter: indicator and limited face states
     after 3 VR sweeps, then 2 SSP-RK3 steps with the limiter in every stage."""
@@ -52,14 +68,16 @@ def make_limiter_case():
     fv = o.face_values(0.0)
     o.limiter(True)
     fv_all = o.face_values(0.0)
-    o.set_u(u0)
+    up = perturbed_quadrants(m)
+    o.set_u(up)
     o.set_urec(np.zeros((m.n_cells, 5, 4)))
     t = 0.0
     for _ in range(2):
         _, d = o.eval_dt(0.4)
         o.ssprk3_step(d, t)
         t += d
-    return dict(u0=u0, indicator=ind, face_values_lim=fv, face_values_limall=fv_all, u_rk2=o.get_u(), t_rk2=t)
+    return dict(u0=u0, indicator=ind, face_values_lim=fv, face_values_limall=fv_all, u0_perturbed=up,
+                u_rk2=o.get_u(), t_rk2=t)
 
 
 def make_case(name):
