@@ -16,7 +16,14 @@ EXPORTS = [
     "dndsg_device_buffer", "dndsg_get_time", "dndsg_set_time", "dndsg_vr_jacobi_step",
     "dndsg_limiter_wbap", "dndsg_eval_dt", "dndsg_eval_rhs", "dndsg_ssprk3_step",
     "dndsg_residual", "dndsg_face_values", "dndsg_get_status", "dndsg_eval_rhs_noalloc",
+    "dndsg_mlp_create", "dndsg_mlp_destroy", "dndsg_mlp_last_error", "dndsg_mlp_set_params",
+    "dndsg_mlp_get_params", "dndsg_mlp_forward", "dndsg_mlp_gradient", "dndsg_mlp_train_step",
+    "dndsg_mlp_features", "dndsg_vr_to_tolerance", "dndsg_ssprk3_step_tol",
 ]
+_NO_STATUS = ("dndsg_destroy", "dndsg_last_error", "dndsg_n_cells", "dndsg_n_faces", "dndsg_mlp_destroy",
+              "dndsg_mlp_last_error")
+
+MLP_IN, MLP_OUT, MLP_NPARAM = 64, 20, 14560
 
 
 class MeshDesc(C.Structure):
@@ -66,8 +73,21 @@ def lib():
     L.dndsg_face_values.argtypes = [vp, dbl, vp, vp]
     L.dndsg_get_status.argtypes = [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), vp]
     L.dndsg_eval_rhs_noalloc.argtypes = [vp, vp, vp, vp, dbl, vp]
+    L.dndsg_mlp_create.argtypes = [i32, C.c_uint64, C.POINTER(vp)]
+    L.dndsg_mlp_destroy.argtypes = [vp]
+    L.dndsg_mlp_destroy.restype = None
+    L.dndsg_mlp_last_error.argtypes = [vp]
+    L.dndsg_mlp_last_error.restype = C.c_char_p
+    L.dndsg_mlp_set_params.argtypes = [vp, vp]
+    L.dndsg_mlp_get_params.argtypes = [vp, vp]
+    L.dndsg_mlp_forward.argtypes = [vp, vp, i64, vp, vp]
+    L.dndsg_mlp_gradient.argtypes = [vp, vp, vp, i64, C.POINTER(dbl), vp, vp]
+    L.dndsg_mlp_train_step.argtypes = [vp, vp, vp, i64, C.c_float, C.POINTER(dbl), vp]
+    L.dndsg_mlp_features.argtypes = [vp, vp, vp, vp]
+    L.dndsg_vr_to_tolerance.argtypes = [vp, vp, dbl, i32, C.POINTER(i32), C.POINTER(i64), vp, vp, vp]
+    L.dndsg_ssprk3_step_tol.argtypes = [vp, vp, dbl, dbl, dbl, i32, C.POINTER(i32), vp, vp, vp]
     for nm in EXPORTS:
-        if nm not in ("dndsg_destroy", "dndsg_last_error", "dndsg_n_cells", "dndsg_n_faces"):
+        if nm not in _NO_STATUS:
             getattr(L, nm).restype = i32
     _lib = L
     return L

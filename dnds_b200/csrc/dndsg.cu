@@ -14,6 +14,7 @@
 #include "../../include/dndsg.h"
 #include "dndsg_bodies.cuh"
 #include "dndsg_limiter.cuh"
+#include "dndsg_mlp.cuh"
 
 using namespace dg;
 
@@ -45,6 +46,10 @@ struct dndsg_ctx {
   double* Ainv = nullptr;
   double *limFace = nullptr, *faceInd = nullptr, *indicator = nullptr;  // CWBAP limiter data
   int32_t* wallCells = nullptr;  // cells with a Wall_Euler / Wall_NoSlip face
+  float* mlpGeom = nullptr;  // [N][8] slot face centres in each cell's polynomial frame
+  void *mlpM = nullptr, *mlpA = nullptr, *mlpB = nullptr, *mlpH = nullptr;  // learned warm start work (T)
+  float* mlpSc = nullptr;                                                     // [N][4] output scales
+  unsigned long long* accCount = nullptr;
   int64_t nWallCells = 0;
   // state
   double *u = nullptr, *uLast = nullptr, *rhs = nullptr, *dt = nullptr, *flux = nullptr, *lamA = nullptr,
@@ -122,6 +127,30 @@ __global__ void k_setup_matrices(MeshView m, SetupParams p, const CellSetup* cel
   if (i >= m.N) return;
   if (!setup_cell_matrices<T>(i, m, p, cells, faceW, cellFace, nfmax, vrOp, nullptr, vrNbr, vrMode, vrFace, Ainv))
     atomicOr(bad, 2);
+}
+
+// slot face centres in the cell's polynomial frame, the geometric inputs of the learned warm start
+__global__ void k_setup_mlp_geom(MeshView m, const CellSetup* cells, const int32_t* cellFace, int nfmax,
+                                 const double* faceCenter, float* geom) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= m.N) return;
+  const CellFrame& fr = cells[i].fr;
+  for (int k = 0; k < 4; k++) {
+    double g0 = 0, g1 = 0;
+    if (k < nfmax) {
+      int32_t sf = cellFace[aos(i, k, nfmax)];
+      if (sf != kEmptySlot) {
+        const int64_t f = sf >= 0 ? sf : ~sf;
+        double x = faceCenter[2 * f], y = faceCenter[2 * f + 1];
+        if (sf < 0 && m.face_shift) { x -= m.face_shift[2 * f]; y -= m.face_shift[2 * f + 1]; }
+        const double dx = x - fr.c[0], dy = y - fr.c[1];
+        g0 = fr.Pinv[0][0] * dx + fr.Pinv[0][1] * dy;
+        g1 = fr.Pinv[1][0] * dx + fr.Pinv[1][1] * dy;
+      }
+    }
+    geom[i * 8 + 2 * k] = (float)g0;
+    geom[i * 8 + 2 * k + 1] = (float)g1;
+  }
 }
 
 // ------------------------------------------------------------------ hot kernels
@@ -661,6 +690,9 @@ int setup_run(dndsg_ctx* c, const dndsg_mesh_desc* md) {
   k_setup_matrices<T><<<grid_for(N), kBlock>>>(m, p, cells, faceW, c->cellFace, c->nfmax, (T*)c->vrOp, c->vrNbr,
                                                c->vrMode, c->vrFace, c->Ainv, dBad);
   if ((rc = check_launch(c))) return rc;
+  if ((rc = dalloc(c, c->mlpGeom, sizeof(float) * 8 * N))) return rc;
+  k_setup_mlp_geom<<<grid_for(N), kBlock>>>(m, cells, c->cellFace, c->nfmax, c->faceCenter, c->mlpGeom);
+  if ((rc = check_launch(c))) return rc;
   if (c->s.limiter) {
     if ((rc = dalloc(c, c->limFace, sizeof(double) * aos_size(F, kLimE)))) return rc;
     if ((rc = dalloc(c, c->faceInd, sizeof(double) * 4 * F))) return rc;
@@ -1044,3 +1076,397 @@ extern "C" int dndsg_eval_rhs_noalloc(dndsg_ctx* c, const double* u, const void*
   else run_rhs_noalloc<double>(c, u, urec, rhs, scratch, t, st(s));
   return check_launch(c);
 }
+
+// ====================================================================== learned VR warm start
+struct dndsg_mlp {
+  int device = 0;
+  float *P = nullptr, *M = nullptr, *V = nullptr, *G = nullptr;
+  __nv_bfloat16* W = nullptr;
+  double* loss = nullptr;
+  int64_t step = 0;
+  bool attrFwd = false, attrTrain = false;
+  std::string err;
+};
+
+namespace {
+int mfail(dndsg_mlp* m, int code, const std::string& msg) {
+  if (m) m->err = msg;
+  return code;
+}
+#define DG_MCUDA(m, call)                                                                                 \
+  do {                                                                                                    \
+    cudaError_t e_ = (call);                                                                              \
+    if (e_ != cudaSuccess) return mfail(m, DNDSG_CUDA_ERROR, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+static_assert(kIn == DNDSG_MLP_IN && kOut == DNDSG_MLP_OUT && kNParam == DNDSG_MLP_NPARAM, "header constants");
+MlpDev mlp_dev(const dndsg_mlp* m) { return MlpDev{m->P, m->W}; }
+
+template <class T>
+__global__ void k_mlp_features(HotView<T> h, MlpIters<T> it, float* X, float* Sc) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= h.N) return;
+  float x[kInP], sc[4];
+  mlp_cell_features<T>(i, h, it, x, sc);
+  if (X)
+    for (int k = 0; k < kIn; k++) X[i * kIn + k] = x[k];
+  for (int v = 0; v < 4; v++) Sc[i * 4 + v] = sc[v];
+}
+
+template <class T>
+__global__ void k_mlp_target(int64_t n, const T* start, const T* conv, const float* Sc, float* Tg) {
+  int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= n * 20) return;
+  const int64_t i = e / 20;
+  const int v = (int)(e - i * 20) & 3;
+  const double t = ((double)conv[e] - (double)start[e]) / (double)Sc[i * 4 + v];
+  Tg[e] = (float)(t > 1e3 ? 1e3 : (t < -1e3 ? -1e3 : t));  // clamped like the features
+}
+
+// per cell: keep the sweep from the learned start where its Jacobi increment is the smaller one
+template <class T>
+__global__ void k_vr_gate(int64_t n, const T* x0, const T* y0, const T* xm, const T* ym, T* out, double* incAcc,
+                          unsigned long long* accepted) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  double inc = 0;
+  int acc = 0;
+  if (i < n) {
+    double d0 = 0, dm = 0;
+    for (int k = 0; k < 20; k++) {
+      double a = (double)y0[i * 20 + k] - (double)x0[i * 20 + k], b = (double)ym[i * 20 + k] - (double)xm[i * 20 + k];
+      d0 += a * a;
+      dm += b * b;
+    }
+    acc = dm < d0;  // false for a NaN increment
+    const T* src = acc ? ym : y0;
+    for (int k = 0; k < 20; k++) out[i * 20 + k] = src[i * 20 + k];
+    inc = acc ? dm : d0;
+  }
+  inc = warp_sum(inc);
+  unsigned na = __popc(__ballot_sync(0xffffffffu, acc != 0));
+  if ((threadIdx.x & 31) == 0) {
+    if (inc != 0.0) atomicAdd(incAcc, inc);
+    if (na) atomicAdd(accepted, (unsigned long long)na);
+  }
+}
+
+__global__ void k_zero_scalar(double* p) { *p = 0.0; }
+
+// one Jacobi sweep from src into dst (the kernels of run_vr); with inc the increment norm
+// accumulates into scal[S_INC]
+template <class T>
+void launch_vr_from(dndsg_ctx* c, const void* src, void* dst, bool inc, cudaStream_t s) {
+  HotView<T> h = view<T>(c);
+  h.urec = (const T*)src;
+  h.urecNew = (T*)dst;
+  const bool r1 = c->s.jacobi_relax == 1.0;
+  if (inc) {
+    if (r1) k_vr<T, true, true><<<grid_for(c->N), kBlock, 0, s>>>(h, c->scal + S_INC);
+    else k_vr<T, false, true><<<grid_for(c->N), kBlock, 0, s>>>(h, c->scal + S_INC);
+  } else if (r1) {
+    constexpr int TILE = vr_tile<T>();
+    const unsigned grid = (unsigned)((c->N + TILE - 1) / TILE);
+    if (c->nfmax == 3) k_vr_tma4<T, TILE, 3><<<grid, TILE * 4, (size_t)TILE * 3 * 30 * sizeof(T), s>>>(h, c->flags);
+    else k_vr_tma4<T, TILE, 4><<<grid, TILE * 4, (size_t)TILE * 4 * 30 * sizeof(T), s>>>(h, c->flags);
+    if (c->nWallCells > 0) k_vr_wall_fixup<T><<<grid_for(c->nWallCells), kBlock, 0, s>>>(h, c->wallCells, c->nWallCells);
+  } else {
+    k_vr<T, false, false><<<grid_for(c->N), kBlock, 0, s>>>(h, nullptr);
+  }
+}
+
+int read_scalar(dndsg_ctx* c, const double* dsrc, double* out, cudaStream_t s) {
+  DG_CUDA(c, cudaMemcpyAsync(out, dsrc, sizeof(double), cudaMemcpyDeviceToHost, s));
+  DG_CUDA(c, cudaStreamSynchronize(s));
+  return 0;
+}
+
+template <class T>
+int ensure_mlp_buffers(dndsg_ctx* c) {
+  if (c->mlpM) return 0;
+  const size_t bytes = sizeof(T) * 20 * c->N;
+  int rc;
+  if ((rc = dalloc(c, c->mlpM, bytes)) || (rc = dalloc(c, c->mlpA, bytes)) || (rc = dalloc(c, c->mlpB, bytes)) ||
+      (rc = dalloc(c, c->mlpH, bytes)) || (rc = dalloc(c, c->mlpSc, sizeof(float) * 4 * c->N)) ||
+      (rc = dalloc(c, c->accCount, sizeof(unsigned long long))))
+    return rc;
+  DG_CUDA(c, cudaFuncSetAttribute(k_mlp_warm_start<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sizeof(InfSmem)));
+  return 0;
+}
+
+template <class T>
+MlpIters<T> iters(dndsg_ctx* c, const void* x0, const void* x1, const void* x2) {
+  return MlpIters<T>{(const T*)x0, (const T*)x1, (const T*)x2, c->mlpGeom};
+}
+
+// Jacobi sweeps until the rms coefficient increment sqrt(sum |dx|^2 / N) <= tol (or max_sweeps).
+// With a network: two plain sweeps x0 -> x1 -> x2, the learned start xm from (x0, x1, x2), then
+// J(x2) (the plain path's third sweep) and J(xm) gated per cell, then plain sweeps to tol.
+// hX / hT (device, may be null) receive the features after the first two sweeps and the
+// training targets (converged - x2) / r at the end (harvesting runs without a network).
+template <class T>
+int vr_to_tol(dndsg_ctx* c, const dndsg_mlp* m, double tol, int maxSweeps, int* sweepsOut, int64_t* accOut,
+              float* hX, float* hT, cudaStream_t s) {
+  int rc = 0, sweeps = 0;
+  double inc = 0;
+  const bool harvest = hX || hT;
+  if (m && harvest) return fail(c, DNDSG_BAD_ARGUMENT, "harvesting runs without a network");
+  if (accOut) *accOut = 0;
+  auto converged = [&]() { return sweeps > 0 && std::sqrt(inc / double(c->N)) <= tol; };
+  if ((m || harvest) && maxSweeps >= (m ? 4 : 2)) {
+    if ((rc = ensure_mlp_buffers<T>(c))) return rc;
+    // x1 = J(x0) into A, x2 = J(x1) into B (with its increment)
+    launch_vr_from<T>(c, c->urec, c->mlpA, false, s);
+    k_zero_scalar<<<1, 1, 0, s>>>(c->scal + S_INC);
+    launch_vr_from<T>(c, c->mlpA, c->mlpB, true, s);
+    sweeps = 2;
+    k_mlp_features<T><<<grid_for(c->N), kBlock, 0, s>>>(view<T>(c), iters<T>(c, c->urec, c->mlpA, c->mlpB), hX,
+                                                         c->mlpSc);
+    if ((rc = check_launch(c))) return rc;
+    if (m) {
+      DG_CUDA(c, cudaMemsetAsync(c->accCount, 0, sizeof(unsigned long long), s));
+      int sms = 148;
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+      k_mlp_warm_start<T><<<sms * 2, kInfWarps * 32, sizeof(InfSmem), s>>>(
+          view<T>(c), iters<T>(c, c->urec, c->mlpA, c->mlpB), mlp_dev(m), (T*)c->mlpM);
+      launch_vr_from<T>(c, c->mlpB, c->urecNew, false, s);  // J(x2)
+      launch_vr_from<T>(c, c->mlpM, c->mlpH, false, s);     // J(xm)
+      k_zero_scalar<<<1, 1, 0, s>>>(c->scal + S_INC);
+      k_vr_gate<T><<<grid_for(c->N), kBlock, 0, s>>>(c->N, (const T*)c->mlpB, (const T*)c->urecNew,
+                                                     (const T*)c->mlpM, (const T*)c->mlpH, (T*)c->mlpA,
+                                                     c->scal + S_INC, c->accCount);
+      std::swap(c->urec, c->mlpA);
+      sweeps = 4;
+      if ((rc = check_launch(c))) return rc;
+      if (accOut) {
+        unsigned long long a = 0;
+        DG_CUDA(c, cudaMemcpyAsync(&a, c->accCount, sizeof(a), cudaMemcpyDeviceToHost, s));
+        DG_CUDA(c, cudaStreamSynchronize(s));
+        *accOut = (int64_t)a;
+      }
+    } else {
+      if (hT) DG_CUDA(c, cudaMemcpyAsync(c->mlpH, c->mlpB, sizeof(T) * 20 * c->N, cudaMemcpyDeviceToDevice, s));
+      std::swap(c->urec, c->mlpB);
+    }
+    if ((rc = read_scalar(c, c->scal + S_INC, &inc, s))) return rc;
+  }
+  while (sweeps < maxSweeps && !converged()) {
+    k_zero_scalar<<<1, 1, 0, s>>>(c->scal + S_INC);
+    launch_vr_from<T>(c, c->urec, c->urecNew, true, s);
+    std::swap(c->urec, c->urecNew);
+    if ((rc = check_launch(c))) return rc;
+    sweeps++;
+    if ((rc = read_scalar(c, c->scal + S_INC, &inc, s))) return rc;
+  }
+  if (hT && c->mlpH) {
+    const int64_t n20 = c->N * 20;
+    k_mlp_target<T><<<(unsigned)((n20 + kBlock - 1) / kBlock), kBlock, 0, s>>>(c->N, (const T*)c->mlpH,
+                                                                               (const T*)c->urec, c->mlpSc, hT);
+    if ((rc = check_launch(c))) return rc;
+  }
+  if (sweepsOut) *sweepsOut = sweeps;
+  return 0;
+}
+
+template <class T>
+int run_step_tol(dndsg_ctx* c, const dndsg_mlp* m, double cfl, double tEnd, double tol, int maxSweeps,
+                 int* sweepsOut, float* hX, float* hT, cudaStream_t s) {
+  run_dt<T>(c, cfl, 1e100, true, s);
+  k_dt_finalize<<<1, 1, 0, s>>>(c->scal, tEnd);
+  const double cst[3] = {0.0, 1.0, 0.5};
+  int total = 0, rc = 0;
+  const size_t xs = (size_t)c->N * kIn, ts = (size_t)c->N * 20;
+  for (int stg = 0; stg < 3; stg++) {
+    int sw = 0;
+    if ((rc = vr_to_tol<T>(c, m, tol, maxSweeps, &sw, nullptr, hX ? hX + stg * xs : nullptr,
+                           hT ? hT + stg * ts : nullptr, s)))
+      return rc;
+    total += sw;
+    if (c->s.limiter) run_limiter<T>(c, 0, s);
+    launch_flux<T>(c, 1, 0.0, cst[stg], s);
+    HotView<T> h = view<T>(c);
+    if (stg == 0) k_cell_update<T, 0><<<grid_for(c->N), kBlock, 0, s>>>(h, c->scal);
+    else if (stg == 1) k_cell_update<T, 1><<<grid_for(c->N), kBlock, 0, s>>>(h, c->scal);
+    else k_cell_update<T, 2><<<grid_for(c->N), kBlock, 0, s>>>(h, c->scal);
+  }
+  k_advance_time<<<1, 1, 0, s>>>(c->scal);
+  if (sweepsOut) *sweepsOut = total;
+  return check_launch(c);
+}
+}  // namespace
+
+extern "C" {
+
+int dndsg_mlp_set_params(dndsg_mlp* m, const float* params) {
+  if (!m || !params) return DNDSG_BAD_ARGUMENT;
+  DG_MCUDA(m, cudaSetDevice(m->device));
+  DG_MCUDA(m, cudaMemcpy(m->P, params, sizeof(float) * kNParam, cudaMemcpyHostToDevice));
+  DG_MCUDA(m, cudaMemset(m->M, 0, sizeof(float) * kNParam));
+  DG_MCUDA(m, cudaMemset(m->V, 0, sizeof(float) * kNParam));
+  k_mlp_to_bf16<<<(kNParam + 255) / 256, 256>>>(m->P, m->W);
+  DG_MCUDA(m, cudaGetLastError());
+  DG_MCUDA(m, cudaDeviceSynchronize());
+  m->step = 0;
+  return 0;
+}
+
+int dndsg_mlp_create(int device, uint64_t seed, dndsg_mlp** out) {
+  if (!out) return DNDSG_BAD_ARGUMENT;
+  *out = nullptr;
+  dndsg_mlp* m = new dndsg_mlp();
+  m->device = device;
+  auto bail = [&](int code) { dndsg_mlp_destroy(m); return code; };
+  if (cudaSetDevice(device) != cudaSuccess) return bail(DNDSG_CUDA_ERROR);
+  if (cudaMalloc(&m->P, sizeof(float) * kNParam) != cudaSuccess ||
+      cudaMalloc(&m->M, sizeof(float) * kNParam) != cudaSuccess ||
+      cudaMalloc(&m->V, sizeof(float) * kNParam) != cudaSuccess ||
+      cudaMalloc(&m->G, sizeof(float) * kNParam) != cudaSuccess ||
+      cudaMalloc(&m->W, sizeof(__nv_bfloat16) * kNW) != cudaSuccess || cudaMalloc(&m->loss, sizeof(double)) != cudaSuccess)
+    return bail(DNDSG_CUDA_ERROR);
+  // Glorot-uniform weights from a 64-bit LCG, zero biases and padding
+  std::vector<float> p(kNParam, 0.f);
+  uint64_t st = seed * 6364136223846793005ull + 1442695040888963407ull;
+  auto uni = [&]() {
+    st = st * 6364136223846793005ull + 1442695040888963407ull;
+    return (double)(st >> 11) * (1.0 / 9007199254740992.0);
+  };
+  auto fill = [&](int off, int rows, int ld, int rowsReal, int colsReal) {
+    const double a = std::sqrt(6.0 / (colsReal + rowsReal));
+    for (int n = 0; n < rows; n++)
+      for (int k = 0; k < ld; k++) p[off + n * ld + k] = (n < rowsReal && k < colsReal) ? (float)((2 * uni() - 1) * a) : 0.f;
+  };
+  fill(kOffW1, kHid, kInP, kHid, kIn);
+  fill(kOffW2, kHid, kHid, kHid, kHid);
+  fill(kOffW3, kHid, kHid, kHid, kHid);
+  fill(kOffW4, kOutP, kHid, kOut, kHid);
+  int rc = dndsg_mlp_set_params(m, p.data());
+  if (rc) return bail(rc);
+  *out = m;
+  return 0;
+}
+
+void dndsg_mlp_destroy(dndsg_mlp* m) {
+  if (!m) return;
+  cudaSetDevice(m->device);
+  for (void* q : {(void*)m->P, (void*)m->M, (void*)m->V, (void*)m->G, (void*)m->W, (void*)m->loss})
+    if (q) cudaFree(q);
+  delete m;
+}
+
+const char* dndsg_mlp_last_error(dndsg_mlp* m) { return m ? m->err.c_str() : "null network"; }
+
+int dndsg_mlp_get_params(dndsg_mlp* m, float* params) {
+  if (!m || !params) return DNDSG_BAD_ARGUMENT;
+  DG_MCUDA(m, cudaSetDevice(m->device));
+  DG_MCUDA(m, cudaMemcpy(params, m->P, sizeof(float) * kNParam, cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int dndsg_mlp_forward(dndsg_mlp* m, const float* X, int64_t n, float* Y, void* s) {
+  if (!m || !X || !Y || n < 0) return DNDSG_BAD_ARGUMENT;
+  DG_MCUDA(m, cudaSetDevice(m->device));
+  if (!m->attrFwd) {
+    DG_MCUDA(m, cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(FwdSmem)));
+    m->attrFwd = true;
+  }
+  if (n == 0) return 0;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m->device);
+  k_mlp_forward<<<sms * 2, kInfWarps * 32, sizeof(FwdSmem), st(s)>>>(mlp_dev(m), X, n, Y);
+  DG_MCUDA(m, cudaGetLastError());
+  return 0;
+}
+
+}  // extern "C"
+
+namespace {
+int mlp_grad(dndsg_mlp* m, const float* X, const float* Tg, int64_t n, cudaStream_t s) {
+  if (!m->attrTrain) {
+    DG_MCUDA(m, cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TrSmem)));
+    m->attrTrain = true;
+  }
+  DG_MCUDA(m, cudaMemsetAsync(m->G, 0, sizeof(float) * kNParam, s));
+  DG_MCUDA(m, cudaMemsetAsync(m->loss, 0, sizeof(double), s));
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m->device);
+  const int64_t tiles = (n + 63) / 64;
+  const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(tiles, sms));
+  k_mlp_train<<<grid, kTrWarps * 32, sizeof(TrSmem), s>>>(mlp_dev(m), X, Tg, n, 1.0f / (float)(n * kOut), m->G,
+                                                          m->loss);
+  DG_MCUDA(m, cudaGetLastError());
+  return 0;
+}
+}  // namespace
+
+extern "C" {
+
+int dndsg_mlp_gradient(dndsg_mlp* m, const float* X, const float* Tg, int64_t n, double* loss, float* grad, void* s) {
+  if (!m || !X || !Tg || n <= 0) return DNDSG_BAD_ARGUMENT;
+  DG_MCUDA(m, cudaSetDevice(m->device));
+  int rc = mlp_grad(m, X, Tg, n, st(s));
+  if (rc) return rc;
+  double l = 0;
+  DG_MCUDA(m, cudaMemcpyAsync(&l, m->loss, sizeof(double), cudaMemcpyDeviceToHost, st(s)));
+  if (grad) DG_MCUDA(m, cudaMemcpyAsync(grad, m->G, sizeof(float) * kNParam, cudaMemcpyDeviceToHost, st(s)));
+  DG_MCUDA(m, cudaStreamSynchronize(st(s)));
+  if (loss) *loss = l / (double)(n * kOut);
+  return 0;
+}
+
+int dndsg_mlp_train_step(dndsg_mlp* m, const float* X, const float* Tg, int64_t n, float lr, double* loss, void* s) {
+  if (!m || !X || !Tg || n <= 0 || !(lr > 0)) return DNDSG_BAD_ARGUMENT;
+  DG_MCUDA(m, cudaSetDevice(m->device));
+  int rc = mlp_grad(m, X, Tg, n, st(s));
+  if (rc) return rc;
+  m->step++;
+  const double b1 = 0.9, b2 = 0.999;
+  const float c1 = (float)(1.0 / (1.0 - std::pow(b1, (double)m->step)));
+  const float c2 = (float)(1.0 / (1.0 - std::pow(b2, (double)m->step)));
+  k_mlp_adam<<<(kNParam + 255) / 256, 256, 0, st(s)>>>(m->P, m->M, m->V, m->G, m->W, lr, (float)b1, (float)b2, 1e-8f,
+                                                        c1, c2);
+  DG_MCUDA(m, cudaGetLastError());
+  if (loss) {
+    double l = 0;
+    DG_MCUDA(m, cudaMemcpyAsync(&l, m->loss, sizeof(double), cudaMemcpyDeviceToHost, st(s)));
+    DG_MCUDA(m, cudaStreamSynchronize(st(s)));
+    *loss = l / (double)(n * kOut);
+  }
+  return 0;
+}
+
+int dndsg_mlp_features(dndsg_ctx* c, float* X, float* scales, void* s) {
+  if (!c || !X || !scales) return DNDSG_BAD_ARGUMENT;
+  int rc = c->fp32 ? ensure_mlp_buffers<float>(c) : ensure_mlp_buffers<double>(c);
+  if (rc) return rc;
+  // x1 = J(x0), x2 = J(x1) into work buffers; the context's coefficients are left as they are
+  if (c->fp32) {
+    launch_vr_from<float>(c, c->urec, c->mlpA, false, st(s));
+    launch_vr_from<float>(c, c->mlpA, c->mlpB, false, st(s));
+    k_mlp_features<float><<<grid_for(c->N), kBlock, 0, st(s)>>>(view<float>(c), iters<float>(c, c->urec, c->mlpA, c->mlpB),
+                                                                 X, scales);
+  } else {
+    launch_vr_from<double>(c, c->urec, c->mlpA, false, st(s));
+    launch_vr_from<double>(c, c->mlpA, c->mlpB, false, st(s));
+    k_mlp_features<double><<<grid_for(c->N), kBlock, 0, st(s)>>>(view<double>(c),
+                                                                  iters<double>(c, c->urec, c->mlpA, c->mlpB), X, scales);
+  }
+  return check_launch(c);
+}
+
+int dndsg_vr_to_tolerance(dndsg_ctx* c, const dndsg_mlp* m, double tol, int max_sweeps, int* sweeps_out,
+                          int64_t* accepted_out, float* harvest_x, float* harvest_t, void* s) {
+  if (!c || max_sweeps < 1 || !(tol >= 0)) return DNDSG_BAD_ARGUMENT;
+  if (m && m->device != c->device) return fail(c, DNDSG_BAD_ARGUMENT, "network and context on different devices");
+  return c->fp32 ? vr_to_tol<float>(c, m, tol, max_sweeps, sweeps_out, accepted_out, harvest_x, harvest_t, st(s))
+                 : vr_to_tol<double>(c, m, tol, max_sweeps, sweeps_out, accepted_out, harvest_x, harvest_t, st(s));
+}
+
+int dndsg_ssprk3_step_tol(dndsg_ctx* c, const dndsg_mlp* m, double cfl, double t_end, double tol, int max_sweeps,
+                          int* sweeps_out, float* harvest_x, float* harvest_t, void* s) {
+  if (!c || max_sweeps < 1 || !(tol >= 0)) return DNDSG_BAD_ARGUMENT;
+  if (m && m->device != c->device) return fail(c, DNDSG_BAD_ARGUMENT, "network and context on different devices");
+  return c->fp32 ? run_step_tol<float>(c, m, cfl, t_end, tol, max_sweeps, sweeps_out, harvest_x, harvest_t, st(s))
+                 : run_step_tol<double>(c, m, cfl, t_end, tol, max_sweeps, sweeps_out, harvest_x, harvest_t, st(s));
+}
+
+}  // extern "C"

@@ -1,0 +1,469 @@
+// dndsg_mlp.cuh -- learned warm start for the VR coefficients (no counterpart in
+// the reference): a per-cell MLP 64 -> 64 -> 64 -> 64 -> 20 (SiLU), BF16 weights
+// and activations, FP32 accumulation, on the tensor cores through warp-level
+// 16x16x16 BF16 MMA (wmma), for inference and for training (forward, backward,
+// Adam).
+//
+// The network extrapolates the Jacobi sequence: from the starting coefficients
+// x0 and two plain sweeps x1 = J(x0), x2 = J(x1) it proposes the converged
+// coefficients x* (for an error dominated by one slow mode of eigenvalue l,
+// x* - x2 = (x2 - x1) l / (1 - l); the network learns the local, many-mode
+// version of that from the solver's own iterations).
+// Features of cell i (d1 = x1 - x0, d2 = x2 - x1):
+//   x[4k + v]      = du_k[v] / s_v,  du_k = u_j(k) - u_i over the face slots k < 4
+//                    (zero for boundary or absent slots), s_v = max_k |du_k[v]|
+//   x[16 + 4q + v] = d1[q][v] / r_v,  r_v = max_q |d1[q][v]|
+//   x[36 + 4q + v] = d2[q][v] / r_v
+//   x[56 + 2k + d] = slot k's face centre in the cell's own polynomial frame,
+//                    (xi, eta) = Pinv (x_f - c_i)
+// Output y[4q + v] = (x* - x2)[q][v] / r_v.  Increments and the remaining error
+// are linear in the error of x0 and the sweep acts on each variable alike, so
+// this scaling makes the learned map homogeneous of degree one per variable.
+// Scales are floored so that a converged or uniform region gives finite features.
+#pragma once
+#include <cuda_bf16.h>
+#include <mma.h>
+
+#include "dndsg_bodies.cuh"
+
+namespace dg {
+
+constexpr int kIn = 64, kInP = 64, kHid = 64, kOut = 20, kOutP = 32;
+// FP32 master parameters, contiguous: W1[64][64] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] W4[32][64] b4[32]
+// (W[n][k]: output unit n, input k; padded rows/columns are kept at zero)
+constexpr int kOffW1 = 0, kOffB1 = kOffW1 + kHid * kInP, kOffW2 = kOffB1 + kHid, kOffB2 = kOffW2 + kHid * kHid,
+              kOffW3 = kOffB2 + kHid, kOffB3 = kOffW3 + kHid * kHid, kOffW4 = kOffB3 + kHid,
+              kOffB4 = kOffW4 + kOutP * kHid, kNParam = kOffB4 + kOutP;
+// BF16 weight copy (the matrices only), same order without biases
+constexpr int kWOff1 = 0, kWOff2 = kWOff1 + kHid * kInP, kWOff3 = kWOff2 + kHid * kHid, kWOff4 = kWOff3 + kHid * kHid,
+              kNW = kWOff4 + kOutP * kHid;
+
+DG_HD float sigm(float z) {
+#if defined(__CUDA_ARCH__)
+  return 1.0f / (1.0f + __expf(-z));
+#else
+  return 1.0f / (1.0f + expf(-z));
+#endif
+}
+DG_HD float silu(float z) { return z * sigm(z); }
+DG_HD float silu_grad(float z) {
+  float s = sigm(z);
+  return s * (1.0f + z * (1.0f - s));
+}
+
+// the coefficient iterates the features are taken from
+template <class T>
+struct MlpIters {
+  const T* x0;
+  const T* x1;
+  const T* x2;
+  const float* geom;  // [N][8] slot face centres in each cell's own frame
+};
+
+// features of one cell into x[64] and the output scales r[4]
+template <class T>
+DG_HD void mlp_cell_features(int64_t i, const HotView<T>& h, const MlpIters<T>& it, float x[kInP], float r[4]) {
+  double du[4][4], ui[4];
+  for (int v = 0; v < 4; v++) ui[v] = h.u[i * 4 + v];
+  for (int k = 0; k < 4; k++)
+    for (int v = 0; v < 4; v++) du[k][v] = 0.0;
+  for (int k = 0; k < h.nfmax && k < 4; k++) {
+    if (h.vrMode[aos(i, k, h.nfmax)] != VR_INNER) continue;
+    const int64_t j = h.vrNbr[aos(i, k, h.nfmax)];
+    for (int v = 0; v < 4; v++) du[k][v] = h.u[j * 4 + v] - ui[v];
+  }
+  double d1[20], d2[20];
+  for (int e = 0; e < 20; e++) {
+    const double a = it.x0[i * 20 + e], b = it.x1[i * 20 + e], c = it.x2[i * 20 + e];
+    d1[e] = b - a;
+    d2[e] = c - b;
+  }
+  auto clampf = [](double a) { return (float)(a > 1e3 ? 1e3 : (a < -1e3 ? -1e3 : a)); };
+  for (int v = 0; v < 4; v++) {
+    double m = 0, md = 0;
+    for (int k = 0; k < 4; k++) m = dmax(m, fabs(du[k][v]));
+    for (int q = 0; q < 5; q++) md = dmax(md, fabs(d1[4 * q + v]));
+    const double s = dmax(m, dmax(1e-12 * fabs(ui[v]), 1e-30));
+    const double rv = dmax(md, 1e-30);
+    r[v] = (float)rv;
+    for (int k = 0; k < 4; k++) x[4 * k + v] = clampf(du[k][v] / s);
+    for (int q = 0; q < 5; q++) {
+      x[16 + 4 * q + v] = clampf(d1[4 * q + v] / (double)r[v]);
+      x[36 + 4 * q + v] = clampf(d2[4 * q + v] / (double)r[v]);
+    }
+  }
+  for (int k = 0; k < 8; k++) x[56 + k] = it.geom[i * 8 + k];
+}
+
+}  // namespace dg
+
+#if defined(__CUDACC__)
+namespace dg {
+namespace wm = nvcuda::wmma;
+typedef __nv_bfloat16 bf16;
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// out[16][N] (FP32, ld 64) = in[16][K] (BF16, ld ldin) . W^T, W [N][K] BF16 row-major (ld K)
+template <int K, int N>
+__device__ __forceinline__ void warp_gemm_xwT(const bf16* in, int ldin, const bf16* W, float* out) {
+  for (int nt = 0; nt < N / 16; nt++) {
+    wm::fragment<wm::accumulator, 16, 16, 16, float> acc;
+    wm::fill_fragment(acc, 0.0f);
+    for (int kt = 0; kt < K / 16; kt++) {
+      wm::fragment<wm::matrix_a, 16, 16, 16, bf16, wm::row_major> a;
+      wm::fragment<wm::matrix_b, 16, 16, 16, bf16, wm::col_major> b;
+      wm::load_matrix_sync(a, in + kt * 16, ldin);
+      wm::load_matrix_sync(b, W + nt * 16 * K + kt * 16, K);
+      wm::mma_sync(acc, a, b, acc);
+    }
+    wm::store_matrix_sync(out + nt * 16, acc, 64, wm::mem_row_major);
+  }
+}
+
+// out[16][K] (FP32, ld 64) = dz[16][N] (BF16, ld 64) . W, W [N][K] BF16 row-major (ld K)
+template <int N, int K>
+__device__ __forceinline__ void warp_gemm_dzW(const bf16* dz, const bf16* W, float* out) {
+  for (int kt = 0; kt < K / 16; kt++) {
+    wm::fragment<wm::accumulator, 16, 16, 16, float> acc;
+    wm::fill_fragment(acc, 0.0f);
+    for (int nt = 0; nt < N / 16; nt++) {
+      wm::fragment<wm::matrix_a, 16, 16, 16, bf16, wm::row_major> a;
+      wm::fragment<wm::matrix_b, 16, 16, 16, bf16, wm::row_major> b;
+      wm::load_matrix_sync(a, dz + nt * 16, 64);
+      wm::load_matrix_sync(b, W + nt * 16 * K + kt * 16, K);
+      wm::mma_sync(acc, a, b, acc);
+    }
+    wm::store_matrix_sync(out + kt * 16, acc, 64, wm::mem_row_major);
+  }
+}
+
+// one 16x16 tile (n-tile nt, k-tile kt) of dW[N][K] += dz^T . x over 64 rows;
+// dz [64][*] BF16 ld 64, x [64][*] BF16 ld ldx; result added into g (FP32, ld K)
+template <int K>
+__device__ __forceinline__ void cta_tile_dW(const bf16* dz, const bf16* x, int ldx, int nt, int kt, float* scratch,
+                                            float* g) {
+  wm::fragment<wm::accumulator, 16, 16, 16, float> acc;
+  wm::fill_fragment(acc, 0.0f);
+  for (int rt = 0; rt < 4; rt++) {
+    wm::fragment<wm::matrix_a, 16, 16, 16, bf16, wm::col_major> a;
+    wm::fragment<wm::matrix_b, 16, 16, 16, bf16, wm::row_major> b;
+    wm::load_matrix_sync(a, dz + rt * 16 * 64 + nt * 16, 64);
+    wm::load_matrix_sync(b, x + rt * 16 * ldx + kt * 16, ldx);
+    wm::mma_sync(acc, a, b, acc);
+  }
+  wm::store_matrix_sync(scratch, acc, 16, wm::mem_row_major);
+  __syncwarp();
+  const int lane = threadIdx.x & 31;
+  for (int e = lane; e < 256; e += 32) g[(nt * 16 + e / 16) * K + kt * 16 + (e & 15)] += scratch[e];
+  __syncwarp();
+}
+
+struct MlpDev {
+  const float* P;   // FP32 master parameters [kNParam]
+  const bf16* W;    // BF16 weight matrices [kNW]
+};
+
+// ---------------------------------------------------------------- inference: features + MLP + warm start
+// dst[i] = x2[i] + y(features_i) * r, for cells i; 8 warps x 16 cells per CTA
+constexpr int kInfWarps = 8;
+struct InfSmem {
+  bf16 W[kNW];
+  float b[3 * kHid + kOutP];
+  bf16 x[kInfWarps][16 * kInP];
+  float z[kInfWarps][16 * 64];
+  bf16 hA[kInfWarps][16 * 64];
+  float sc[kInfWarps][16 * 4];
+};
+
+template <class T>
+__global__ void __launch_bounds__(kInfWarps * 32) k_mlp_warm_start(HotView<T> h, MlpIters<T> it, MlpDev m, T* dst) {
+  extern __shared__ __align__(128) unsigned char raw[];
+  InfSmem& S = *reinterpret_cast<InfSmem*>(raw);
+  for (int e = threadIdx.x; e < kNW; e += blockDim.x) S.W[e] = m.W[e];
+  for (int e = threadIdx.x; e < 3 * kHid + kOutP; e += blockDim.x) {
+    int off = e < kHid ? kOffB1 + e : e < 2 * kHid ? kOffB2 + e - kHid : e < 3 * kHid ? kOffB3 + e - 2 * kHid
+                                                                                    : kOffB4 + e - 3 * kHid;
+    S.b[e] = m.P[off];
+  }
+  __syncthreads();
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t tiles = (h.N + 15) / 16;
+  for (int64_t tile = (int64_t)blockIdx.x * kInfWarps + w; tile < tiles; tile += (int64_t)gridDim.x * kInfWarps) {
+    const int64_t i0 = tile * 16;
+    if (lane < 16) {
+      const int64_t i = i0 + lane;
+      float x[kInP], sc[4];
+      if (i < h.N) mlp_cell_features<T>(i, h, it, x, sc);
+      else { for (int k = 0; k < kInP; k++) x[k] = 0.f; for (int v = 0; v < 4; v++) sc[v] = 0.f; }
+      for (int k = 0; k < kInP; k++) S.x[w][lane * kInP + k] = __float2bfloat16(x[k]);
+      for (int v = 0; v < 4; v++) S.sc[w][lane * 4 + v] = sc[v];
+    }
+    __syncwarp();
+    const bf16* in = S.x[w];
+    int ldin = kInP;
+    for (int layer = 0; layer < 4; layer++) {
+      if (layer == 0) warp_gemm_xwT<kInP, kHid>(in, ldin, S.W + kWOff1, S.z[w]);
+      else if (layer == 1) warp_gemm_xwT<kHid, kHid>(in, ldin, S.W + kWOff2, S.z[w]);
+      else if (layer == 2) warp_gemm_xwT<kHid, kHid>(in, ldin, S.W + kWOff3, S.z[w]);
+      else warp_gemm_xwT<kHid, kOutP>(in, ldin, S.W + kWOff4, S.z[w]);
+      __syncwarp();
+      if (layer < 3) {
+        for (int e = lane; e < 16 * 64; e += 32) {
+          float zz = S.z[w][e] + S.b[layer * kHid + (e & 63)];
+          S.hA[w][e] = __float2bfloat16(silu(zz));
+        }
+        __syncwarp();
+        in = S.hA[w];
+        ldin = 64;
+      }
+    }
+    // y = z + b4; dst = x2 + y * r
+    for (int e = lane; e < 16 * kOut; e += 32) {
+      const int r = e / kOut, o = e - r * kOut;
+      const int64_t i = i0 + r;
+      if (i < h.N) {
+        const float y = S.z[w][r * 64 + o] + S.b[3 * kHid + o];
+        const int v = o & 3;
+        dst[i * 20 + o] = (T)((double)it.x2[i * 20 + o] + (double)y * (double)S.sc[w][r * 4 + v]);
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// plain forward on given features X [n][36] -> Y [n][20] (FP32), for tests
+struct FwdSmem {
+  bf16 W[kNW];
+  float b[3 * kHid + kOutP];
+  bf16 x[kInfWarps][16 * kInP];
+  float z[kInfWarps][16 * 64];
+  bf16 hA[kInfWarps][16 * 64];
+};
+__global__ void __launch_bounds__(kInfWarps * 32) k_mlp_forward(MlpDev m, const float* X, int64_t n, float* Y) {
+  extern __shared__ __align__(128) unsigned char raw[];
+  FwdSmem& S = *reinterpret_cast<FwdSmem*>(raw);
+  for (int e = threadIdx.x; e < kNW; e += blockDim.x) S.W[e] = m.W[e];
+  for (int e = threadIdx.x; e < 3 * kHid + kOutP; e += blockDim.x) {
+    int off = e < kHid ? kOffB1 + e : e < 2 * kHid ? kOffB2 + e - kHid : e < 3 * kHid ? kOffB3 + e - 2 * kHid
+                                                                                    : kOffB4 + e - 3 * kHid;
+    S.b[e] = m.P[off];
+  }
+  __syncthreads();
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t tiles = (n + 15) / 16;
+  for (int64_t tile = (int64_t)blockIdx.x * kInfWarps + w; tile < tiles; tile += (int64_t)gridDim.x * kInfWarps) {
+    const int64_t r0 = tile * 16;
+    for (int e = lane; e < 16 * kInP; e += 32) {
+      const int r = e / kInP, k = e - r * kInP;
+      const float v = (r0 + r < n && k < kIn) ? X[(r0 + r) * kIn + k] : 0.f;
+      S.x[w][e] = __float2bfloat16(v);
+    }
+    __syncwarp();
+    const bf16* in = S.x[w];
+    int ldin = kInP;
+    for (int layer = 0; layer < 4; layer++) {
+      if (layer == 0) warp_gemm_xwT<kInP, kHid>(in, ldin, S.W + kWOff1, S.z[w]);
+      else if (layer == 1) warp_gemm_xwT<kHid, kHid>(in, ldin, S.W + kWOff2, S.z[w]);
+      else if (layer == 2) warp_gemm_xwT<kHid, kHid>(in, ldin, S.W + kWOff3, S.z[w]);
+      else warp_gemm_xwT<kHid, kOutP>(in, ldin, S.W + kWOff4, S.z[w]);
+      __syncwarp();
+      if (layer < 3) {
+        for (int e = lane; e < 16 * 64; e += 32) {
+          float zz = S.z[w][e] + S.b[layer * kHid + (e & 63)];
+          S.hA[w][e] = __float2bfloat16(silu(zz));
+        }
+        __syncwarp();
+        in = S.hA[w];
+        ldin = 64;
+      }
+    }
+    for (int e = lane; e < 16 * kOut; e += 32) {
+      const int r = e / kOut, o = e - r * kOut;
+      if (r0 + r < n) Y[(r0 + r) * kOut + o] = S.z[w][r * 64 + o] + S.b[3 * kHid + o];
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------- training: forward + backward
+// loss = mean over rows and the 20 outputs of (y - t)^2; gradients accumulate into G
+constexpr int kTrWarps = 4;
+struct TrSmem {
+  bf16 W[kNW];
+  float b[3 * kHid + kOutP];
+  bf16 x[64 * kInP];
+  bf16 h1[64 * 64], h2[64 * 64], h3[64 * 64];
+  float z1[64 * 64], z2[64 * 64], z3[64 * 64];
+  float dy[64 * 64];  // y, then dy (first 32 columns), then dH scratch
+  bf16 dz[64 * 64];
+  float g[kNParam];
+  float scratch[kTrWarps][256];
+};
+
+__global__ void __launch_bounds__(kTrWarps * 32) k_mlp_train(MlpDev m, const float* X, const float* Tg, int64_t n,
+                                                             float invCount, float* G, double* lossAcc) {
+  extern __shared__ __align__(128) unsigned char raw[];
+  TrSmem& S = *reinterpret_cast<TrSmem*>(raw);
+  const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+  for (int e = tid; e < kNW; e += blockDim.x) S.W[e] = m.W[e];
+  for (int e = tid; e < 3 * kHid + kOutP; e += blockDim.x) {
+    int off = e < kHid ? kOffB1 + e : e < 2 * kHid ? kOffB2 + e - kHid : e < 3 * kHid ? kOffB3 + e - 2 * kHid
+                                                                                    : kOffB4 + e - 3 * kHid;
+    S.b[e] = m.P[off];
+  }
+  for (int e = tid; e < kNParam; e += blockDim.x) S.g[e] = 0.f;
+  __syncthreads();
+  double lossLocal = 0.0;
+  const int64_t tiles = (n + 63) / 64;
+  for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const int64_t r0 = tile * 64;
+    for (int e = tid; e < 64 * kInP; e += blockDim.x) {
+      const int r = e / kInP, k = e - r * kInP;
+      const float v = (r0 + r < n && k < kIn) ? X[(r0 + r) * kIn + k] : 0.f;
+      S.x[e] = __float2bfloat16(v);
+    }
+    __syncthreads();
+    // ---- forward, warp w on rows 16w..16w+15
+    const int rw = 16 * w;
+    warp_gemm_xwT<kInP, kHid>(S.x + rw * kInP, kInP, S.W + kWOff1, S.z1 + rw * 64);
+    __syncwarp();
+    for (int e = lane; e < 16 * 64; e += 32) {
+      float zz = S.z1[rw * 64 + e] + S.b[e & 63];
+      S.z1[rw * 64 + e] = zz;
+      S.h1[rw * 64 + e] = __float2bfloat16(silu(zz));
+    }
+    __syncwarp();
+    warp_gemm_xwT<kHid, kHid>(S.h1 + rw * 64, 64, S.W + kWOff2, S.z2 + rw * 64);
+    __syncwarp();
+    for (int e = lane; e < 16 * 64; e += 32) {
+      float zz = S.z2[rw * 64 + e] + S.b[kHid + (e & 63)];
+      S.z2[rw * 64 + e] = zz;
+      S.h2[rw * 64 + e] = __float2bfloat16(silu(zz));
+    }
+    __syncwarp();
+    warp_gemm_xwT<kHid, kHid>(S.h2 + rw * 64, 64, S.W + kWOff3, S.z3 + rw * 64);
+    __syncwarp();
+    for (int e = lane; e < 16 * 64; e += 32) {
+      float zz = S.z3[rw * 64 + e] + S.b[2 * kHid + (e & 63)];
+      S.z3[rw * 64 + e] = zz;
+      S.h3[rw * 64 + e] = __float2bfloat16(silu(zz));
+    }
+    __syncwarp();
+    warp_gemm_xwT<kHid, kOutP>(S.h3 + rw * 64, 64, S.W + kWOff4, S.dy + rw * 64);
+    __syncwarp();
+    // loss and dy = 2 (y - t) / count on the 20 real outputs
+    for (int e = lane; e < 16 * 64; e += 32) {
+      const int r = e >> 6, o = e & 63;
+      const int64_t row = r0 + rw + r;
+      float d = 0.f;
+      if (o < kOut && row < n) {
+        const float y = S.dy[rw * 64 + e] + S.b[3 * kHid + o];
+        const float dd = y - Tg[row * kOut + o];
+        lossLocal += (double)dd * dd;
+        d = 2.f * dd * invCount;
+      }
+      S.dy[rw * 64 + e] = d;
+      S.dz[rw * 64 + e] = __float2bfloat16(d);
+    }
+    __syncthreads();
+    // ---- layer 4: dW4 [32][64] (8 tiles), db4, dH3 = dz4 . W4
+    for (int t = w; t < 8; t += kTrWarps) cta_tile_dW<kHid>(S.dz, S.h3, 64, t >> 2, t & 3, S.scratch[w], S.g + kOffW4);
+    if (tid < kOutP) {
+      float a = 0.f;
+      for (int r = 0; r < 64; r++) a += S.dy[r * 64 + tid];
+      S.g[kOffB4 + tid] += a;
+    }
+    __syncthreads();  // dy is read whole above and overwritten row-wise below
+    warp_gemm_dzW<kOutP, kHid>(S.dz + rw * 64, S.W + kWOff4, S.dy + rw * 64);
+    __syncthreads();
+    for (int e = lane; e < 16 * 64; e += 32) {
+      const float dz = S.dy[rw * 64 + e] * silu_grad(S.z3[rw * 64 + e]);
+      S.z3[rw * 64 + e] = dz;  // FP32 dz3 for the bias gradient
+      S.dz[rw * 64 + e] = __float2bfloat16(dz);
+    }
+    __syncthreads();
+    // ---- layer 3
+    for (int t = w; t < 16; t += kTrWarps) cta_tile_dW<kHid>(S.dz, S.h2, 64, t >> 2, t & 3, S.scratch[w], S.g + kOffW3);
+    for (int c = tid; c < kHid; c += blockDim.x) {
+      float a = 0.f;
+      for (int r = 0; r < 64; r++) a += S.z3[r * 64 + c];
+      S.g[kOffB3 + c] += a;
+    }
+    warp_gemm_dzW<kHid, kHid>(S.dz + rw * 64, S.W + kWOff3, S.dy + rw * 64);
+    __syncthreads();
+    for (int e = lane; e < 16 * 64; e += 32) {
+      const float dz = S.dy[rw * 64 + e] * silu_grad(S.z2[rw * 64 + e]);
+      S.z2[rw * 64 + e] = dz;
+      S.dz[rw * 64 + e] = __float2bfloat16(dz);
+    }
+    __syncthreads();
+    // ---- layer 2
+    for (int t = w; t < 16; t += kTrWarps) cta_tile_dW<kHid>(S.dz, S.h1, 64, t >> 2, t & 3, S.scratch[w], S.g + kOffW2);
+    for (int c = tid; c < kHid; c += blockDim.x) {
+      float a = 0.f;
+      for (int r = 0; r < 64; r++) a += S.z2[r * 64 + c];
+      S.g[kOffB2 + c] += a;
+    }
+    warp_gemm_dzW<kHid, kHid>(S.dz + rw * 64, S.W + kWOff2, S.dy + rw * 64);
+    __syncthreads();
+    for (int e = lane; e < 16 * 64; e += 32) {
+      const float dz = S.dy[rw * 64 + e] * silu_grad(S.z1[rw * 64 + e]);
+      S.z1[rw * 64 + e] = dz;
+      S.dz[rw * 64 + e] = __float2bfloat16(dz);
+    }
+    __syncthreads();
+    // ---- layer 1: dW1 [64][kInP], db1
+    constexpr int kT1 = kInP / 16;
+    for (int t = w; t < 4 * kT1; t += kTrWarps)
+      cta_tile_dW<kInP>(S.dz, S.x, kInP, t / kT1, t % kT1, S.scratch[w], S.g + kOffW1);
+    for (int c = tid; c < kHid; c += blockDim.x) {
+      float a = 0.f;
+      for (int r = 0; r < 64; r++) a += S.z1[r * 64 + c];
+      S.g[kOffB1 + c] += a;
+    }
+    __syncthreads();
+  }
+  for (int e = tid; e < kNParam; e += blockDim.x)
+    if (S.g[e] != 0.f) atomicAdd(&G[e], S.g[e]);
+  lossLocal = warp_sum_d(lossLocal);
+  if (lane == 0 && lossLocal != 0.0) atomicAdd(lossAcc, lossLocal);
+}
+
+// Adam (Kingma & Ba) on the FP32 master parameters; padded entries stay zero; refreshes the BF16 copy
+__global__ void k_mlp_adam(float* P, float* Mo, float* V, const float* G, bf16* W, float lr, float b1, float b2,
+                           float eps, float c1, float c2) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= kNParam) return;
+  bool pad = false;
+  int wi = -1;
+  if (e < kOffB1) { pad = (e % kInP) >= kIn; wi = kWOff1 + e; }
+  else if (e >= kOffW2 && e < kOffB2) wi = kWOff2 + (e - kOffW2);
+  else if (e >= kOffW3 && e < kOffB3) wi = kWOff3 + (e - kOffW3);
+  else if (e >= kOffW4 && e < kOffB4) { pad = (e - kOffW4) / kHid >= kOut; wi = kWOff4 + (e - kOffW4); }
+  else if (e >= kOffB4) pad = (e - kOffB4) >= kOut;
+  if (pad) { P[e] = 0.f; if (wi >= 0) W[wi] = __float2bfloat16(0.f); return; }
+  const float g = G[e];
+  const float m = b1 * Mo[e] + (1.f - b1) * g, v = b2 * V[e] + (1.f - b2) * g * g;
+  Mo[e] = m;
+  V[e] = v;
+  const float p = P[e] - lr * (m * c1) / (sqrtf(v * c2) + eps);
+  P[e] = p;
+  if (wi >= 0) W[wi] = __float2bfloat16(p);
+}
+__global__ void k_mlp_to_bf16(const float* P, bf16* W) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= kNParam) return;
+  int wi = -1;
+  if (e < kOffB1) wi = kWOff1 + e;
+  else if (e >= kOffW2 && e < kOffB2) wi = kWOff2 + (e - kOffW2);
+  else if (e >= kOffW3 && e < kOffB3) wi = kWOff3 + (e - kOffW3);
+  else if (e >= kOffW4 && e < kOffB4) wi = kWOff4 + (e - kOffW4);
+  if (wi >= 0) W[wi] = __float2bfloat16(P[e]);
+}
+
+}  // namespace dg
+#endif

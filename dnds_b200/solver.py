@@ -153,6 +153,32 @@ class Solver:
     def ssprk3_step(self, cfl: float, t_end: float = 1e300):
         self._check(self.L.dndsg_ssprk3_step(self.h, cfl, t_end, self.stream))
 
+    # ------------------------------------------------------------------ learned warm start
+    def mlp_features(self, X_ptr: int, scales_ptr: int):
+        """Features [N][44] and scales [N][4] of the current state into device arrays."""
+        self._check(self.L.dndsg_mlp_features(self.h, C.c_void_p(X_ptr), C.c_void_p(scales_ptr), self.stream))
+
+    def vr_to_tolerance(self, tol: float, max_sweeps: int = 200, mlp=None, harvest_x: int = 0,
+                        harvest_t: int = 0):
+        """Jacobi sweeps until the rms coefficient increment <= tol; returns (sweeps, cells on the learned start)."""
+        sw = C.c_int()
+        acc = C.c_int64()
+        self._check(self.L.dndsg_vr_to_tolerance(self.h, mlp.h if mlp is not None else None, float(tol),
+                                                  int(max_sweeps), C.byref(sw), C.byref(acc),
+                                                  C.c_void_p(harvest_x or None), C.c_void_p(harvest_t or None),
+                                                  self.stream))
+        return sw.value, acc.value
+
+    def ssprk3_step_tol(self, cfl: float, tol: float, max_sweeps: int = 200, mlp=None, t_end: float = 1e300,
+                        harvest_x: int = 0, harvest_t: int = 0) -> int:
+        """One SSP-RK3 step with every stage's reconstruction iterated to tol; returns the sweeps taken."""
+        sw = C.c_int()
+        self._check(self.L.dndsg_ssprk3_step_tol(self.h, mlp.h if mlp is not None else None, float(cfl),
+                                                  float(t_end), float(tol), int(max_sweeps), C.byref(sw),
+                                                  C.c_void_p(harvest_x or None), C.c_void_p(harvest_t or None),
+                                                  self.stream))
+        return sw.value
+
     def face_values(self, t: float = 0.0) -> np.ndarray:
         out = np.empty((self.F, 3, 2, 4))
         self._check(self.L.dndsg_face_values(self.h, float(t), _p(out), self.stream))

@@ -181,6 +181,63 @@ int dndsg_eval_rhs_noalloc(dndsg_ctx* ctx, const double* u, const void* urec, do
  * non-positive density/pressure in a flux; bit 1: reduced-order face point). */
 int dndsg_get_status(dndsg_ctx* ctx, uint32_t* flags, uint64_t* n_reduced, void* stream);
 
+/* ---------------------------------------------------------------------------
+ * Learned warm start for the VR coefficients.  No counterpart in the
+ * reference: a per-cell network 64 -> 64 -> 64 -> 64 -> 20 (SiLU), BF16
+ * weights and activations with FP32 accumulation on the tensor cores, trained
+ * on pairs the solver itself produces.  From the starting coefficients x0 and
+ * two plain Jacobi sweeps x1, x2 (ReconstructionJacobiStep,
+ * DNDS_FV_VR.hpp:1474-1479) it proposes the converged coefficients.  Its output
+ * is only a starting point: the plain sweep still iterates to the same
+ * tolerance, and per cell the learned start is kept only where the Jacobi
+ * increment from it is smaller than from x2.
+ * Features per cell [DNDSG_MLP_IN] (float): neighbour mean differences (16)
+ * divided per variable by their largest magnitude; the two sweep increments
+ * x1 - x0 and x2 - x1 (20 + 20) divided per variable by r_v, the largest
+ * |x1 - x0| of that variable; the slot face centres in the cell's own
+ * polynomial frame (8).  Targets [20]: (converged - x2) / r_v.
+ * ------------------------------------------------------------------------ */
+#define DNDSG_MLP_IN 64
+#define DNDSG_MLP_OUT 20
+#define DNDSG_MLP_NPARAM 14560 /* FP32 parameters, W1[64][64] b1 W2[64][64] b2 W3[64][64] b3 W4[32][64] b4[32] */
+typedef struct dndsg_mlp dndsg_mlp;
+
+/* new network on a device: Glorot-uniform weights from seed, zero biases */
+int dndsg_mlp_create(int device, uint64_t seed, dndsg_mlp** out);
+void dndsg_mlp_destroy(dndsg_mlp* mlp);
+const char* dndsg_mlp_last_error(dndsg_mlp* mlp);
+/* host FP32 parameters [DNDSG_MLP_NPARAM] (padded rows/columns are zero);
+ * set_params also resets the Adam moments */
+int dndsg_mlp_set_params(dndsg_mlp* mlp, const float* params);
+int dndsg_mlp_get_params(dndsg_mlp* mlp, float* params);
+/* Y [n][20] = network(X [n][64]), device arrays */
+int dndsg_mlp_forward(dndsg_mlp* mlp, const float* X, int64_t n, float* Y, void* stream);
+/* mean-square loss over n rows x 20 outputs against targets T [n][20] (device)
+ * and its gradient (host [DNDSG_MLP_NPARAM], may be NULL); synchronous */
+int dndsg_mlp_gradient(dndsg_mlp* mlp, const float* X, const float* T, int64_t n, double* loss, float* grad,
+                       void* stream);
+/* one Adam step (b1 0.9, b2 0.999, eps 1e-8) on the batch X, T (device);
+ * loss (host, may be NULL) is the batch loss before the step */
+int dndsg_mlp_train_step(dndsg_mlp* mlp, const float* X, const float* T, int64_t n, float lr, double* loss,
+                         void* stream);
+/* features of the context's current coefficients, X [n_cells][64], and the
+ * output scales r [n_cells][4] (device); runs two sweeps into work buffers
+ * and leaves the context's coefficients unchanged */
+int dndsg_mlp_features(dndsg_ctx* ctx, float* X, float* scales, void* stream);
+/* Jacobi sweeps on the context's coefficients until the rms increment
+ * sqrt(sum |dx|^2 / n_cells) <= tol or max_sweeps.  With mlp (may be NULL,
+ * needs max_sweeps >= 4): sweeps x0 -> x1 -> x2, the learned start xm, then
+ * J(x2) and J(xm) gated per cell (accepted_out: cells that kept the learned
+ * start); the four count as sweeps.  harvest_x [n_cells][64], harvest_t
+ * [n_cells][20] (device, may be NULL; only without mlp) receive the features
+ * after the first two sweeps and the targets (converged - x2) / r_v. */
+int dndsg_vr_to_tolerance(dndsg_ctx* ctx, const dndsg_mlp* mlp, double tol, int max_sweeps, int* sweeps_out,
+                          int64_t* accepted_out, float* harvest_x, float* harvest_t, void* stream);
+/* dndsg_ssprk3_step with the reconstruction of every stage iterated to tol
+ * (above); harvest arrays, when given, hold 3 stages back to back */
+int dndsg_ssprk3_step_tol(dndsg_ctx* ctx, const dndsg_mlp* mlp, double cfl, double t_end, double tol,
+                          int max_sweeps, int* sweeps_out, float* harvest_x, float* harvest_t, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
