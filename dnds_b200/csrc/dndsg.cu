@@ -51,6 +51,10 @@ struct dndsg_ctx {
   float* mlpSc = nullptr;                                                     // [N][4] output scales
   unsigned long long* accCount = nullptr;
   int64_t nWallCells = 0;
+  // implicit path: distance-1 colouring, LU-SGS diagonal, increment, residual accumulator
+  int32_t *colourOf = nullptr, *colourCells = nullptr;
+  std::vector<int64_t> colourOff;
+  double *Dinv = nullptr, *inc = nullptr, *resAcc = nullptr;
   // state
   double *u = nullptr, *uLast = nullptr, *rhs = nullptr, *dt = nullptr, *flux = nullptr, *lamA = nullptr,
          *dLam = nullptr, *scal = nullptr, *partial = nullptr;
@@ -1467,6 +1471,286 @@ int dndsg_ssprk3_step_tol(dndsg_ctx* c, const dndsg_mlp* m, double cfl, double t
   if (m && m->device != c->device) return fail(c, DNDSG_BAD_ARGUMENT, "network and context on different devices");
   return c->fp32 ? run_step_tol<float>(c, m, cfl, t_end, tol, max_sweeps, sweeps_out, harvest_x, harvest_t, st(s))
                  : run_step_tol<double>(c, m, cfl, t_end, tol, max_sweeps, sweeps_out, harvest_x, harvest_t, st(s));
+}
+
+}  // extern "C"
+
+// ====================================================================== implicit path (LU-SGS, BDF1)
+namespace {
+
+// fluxJacobian0_Right_Times_du (DNDS_FV_EulerEvaluator.hpp:928-956) for 2-D Euler:
+// the inviscid flux increment of dU about U through the unit normal n
+// (IdealGasUIncrement, GasInviscidFluxFacialIncrement, DNDS_Gas.hpp:122-146) minus lam dU
+__device__ __forceinline__ void flux_jac_times_du(const double U[4], double nx, double ny, const double dU[4],
+                                                  double lam, double gamma, double dF[4]) {
+  const double ir = 1.0 / U[0];
+  const double vx = U[1] * ir, vy = U[2] * ir;
+  const double p = (gamma - 1) * (U[3] - 0.5 * U[0] * (vx * vx + vy * vy));
+  const double dvx = (dU[1] - vx * dU[0]) * ir, dvy = (dU[2] - vy * dU[0]) * ir;
+  const double dp = (gamma - 1) * (dU[3] - 0.5 * (dU[1] * vx + dU[2] * vy + U[1] * dvx + U[2] * dvy));
+  const double vn = vx * nx + vy * ny, dvn = dvx * nx + dvy * ny;
+  dF[0] = dU[1] * nx + dU[2] * ny - lam * dU[0];
+  dF[1] = dU[1] * vn + U[1] * dvn + nx * dp - lam * dU[1];
+  dF[2] = dU[2] * vn + U[2] * dvn + ny * dp - lam * dU[2];
+  dF[3] = (dU[3] + dp) * vn + (U[3] + p) * dvn - lam * dU[3];
+}
+
+// LUSGSMatrixInit (DNDS_FV_EulerEvaluator.cpp:995-1047), no source term: the diagonal is one
+// scalar per cell, D_i = alpha/dt_i + 1/dtPhys + sum_f (alpha/2) lambda_f A_f / V_i, where dt_i is
+// the EvaluateDt step (dTau = dt_i / alpha) and lamA holds lambda_f A_f
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_lusgs_init(HotView<T> h, double dtPhysInv, double alpha, double* Dinv) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= h.N) return;
+  double sum = 0;
+  for (int k = 0; k < h.nfmax; k++) {
+    const int32_t sf = h.cellFace[aos(i, k, h.nfmax)];
+    if (sf == kEmptySlot) continue;
+    sum += h.lamA[sf >= 0 ? sf : ~sf];
+  }
+  const double d = alpha / h.dt[i] + dtPhysInv + 0.5 * alpha * sum / h.vol[i];
+  Dinv[i] = 1.0 / d;
+}
+
+// rhs of the first-order BDF pseudo-time system (ImplicitBDFDualTimeStep::Step,
+// DNDS_ODE.hpp:455-465): alpha R(u) - (u - uLast) / dtPhys, in place on rhs
+__global__ void k_bdf_rhs(int64_t n4, const double* u, const double* uLast, double alpha, double dtPhysInv,
+                          double* rhs) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= n4) return;
+  rhs[e] = alpha * rhs[e] - u[e] * dtPhysInv + uLast[e] * dtPhysInv;
+}
+
+// one colour of UpdateLUSGSForward (FWD) or UpdateLUSGSBackward (DNDS_FV_EulerEvaluator.cpp:
+// 1149-1357).  Cells of one colour share no face, so sweeping the colours in order is the
+// reference's sweep in the colour-sorted scan order: a neighbour is "before" a cell exactly
+// when its colour is smaller.  inc is updated in place, as the reference calls both sweeps.
+template <class T, bool FWD>
+__global__ void __launch_bounds__(kBlock) k_lusgs_colour(HotView<T> h, const int32_t* colourOf,
+                                                         const int32_t* cells, int64_t n, double alpha,
+                                                         const double* Dinv, const double* rhs, double* inc) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int64_t i = cells[t];
+  const int ci = colourOf[i];
+  double buf[4];
+  if (FWD) load4<T>(&rhs[i * 4], buf);
+  else buf[0] = buf[1] = buf[2] = buf[3] = 0.0;
+  const double scale = -0.5 * alpha / h.vol[i];
+  for (int k = 0; k < h.nfmax; k++) {
+    const int32_t sf = h.cellFace[aos(i, k, h.nfmax)];
+    if (sf == kEmptySlot) continue;
+    const int32_t f = sf >= 0 ? sf : ~sf;
+    const int32_t j = sf >= 0 ? h.faceR[f] : h.faceL[f];
+    if (j < 0) continue;
+    const int cj = colourOf[j];
+    if (FWD ? !(cj < ci) : !(cj > ci)) continue;
+    const double sg = sf >= 0 ? 1.0 : -1.0;
+    const double area = h.faceArea[f];
+    double U[4], dU[4], dF[4];
+    load4<T>(&h.u[(int64_t)j * 4], U);
+    load4<T>(&inc[(int64_t)j * 4], dU);
+    flux_jac_times_du(U, sg * h.faceNormal[2 * f], sg * h.faceNormal[2 * f + 1], dU, h.lamA[f] / area, h.gamma, dF);
+    for (int v = 0; v < 4; v++) buf[v] += scale * area * dF[v];
+  }
+  const double di = Dinv[i];
+  double* o = &inc[i * 4];
+  if (FWD) {
+    for (int v = 0; v < 4; v++) o[v] = di * buf[v];
+  } else {
+    for (int v = 0; v < 4; v++) o[v] += di * buf[v];
+  }
+}
+
+// x += inc, with the L1 norm of inc per variable (volume-weighted on request) into acc[4]
+__global__ void __launch_bounds__(kBlock) k_add_inc(int64_t N, double* u, const double* inc, const double* vol,
+                                                    int volWise, double* acc) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  double a[4] = {0, 0, 0, 0};
+  if (i < N) {
+    const double w = volWise ? vol[i] : 1.0;
+    for (int v = 0; v < 4; v++) {
+      const double d = inc[i * 4 + v];
+      u[i * 4 + v] += d;
+      a[v] = fabs(d) * w;
+    }
+  }
+  for (int v = 0; v < 4; v++) {
+    const double r = warp_sum(a[v]);
+    if ((threadIdx.x & 31) == 0 && r != 0.0) atomicAdd(&acc[v], r);
+  }
+}
+
+// the wall force: minus the sum of the Riemann fluxes of the Wall_Euler / Wall_NoSlip faces
+// (fluxWallSum, DNDS_FV_EulerEvaluator.cpp:510-516), from the last flux evaluation
+__global__ void __launch_bounds__(kBlock) k_wall_flux(int64_t Fi, int64_t F, const int32_t* faceBC,
+                                                      const double* flux, double* acc) {
+  const int64_t f = Fi + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  double a[4] = {0, 0, 0, 0};
+  if (f < F) {
+    const int bc = faceBC[f];
+    if (bc == BC_WALL_NOSLIP || bc == BC_WALL_EULER)
+      for (int v = 0; v < 4; v++) a[v] = -flux[f * 4 + v];
+  }
+  for (int v = 0; v < 4; v++) {
+    const double r = warp_sum(a[v]);
+    if ((threadIdx.x & 31) == 0 && r != 0.0) atomicAdd(&acc[v], r);
+  }
+}
+
+// greedy distance-1 colouring over the interior faces, in cell order; cells sorted by colour
+int ensure_lusgs(dndsg_ctx* c) {
+  if (c->colourOf) return 0;
+  const int64_t N = c->N, F = c->F;
+  std::vector<int32_t> L(F), R(F);
+  DG_CUDA(c, cudaMemcpy(L.data(), c->faceL, sizeof(int32_t) * F, cudaMemcpyDeviceToHost));
+  DG_CUDA(c, cudaMemcpy(R.data(), c->faceR, sizeof(int32_t) * F, cudaMemcpyDeviceToHost));
+  std::vector<int64_t> deg(N + 1, 0);
+  for (int64_t f = 0; f < F; f++)
+    if (R[f] >= 0) { deg[L[f] + 1]++; deg[R[f] + 1]++; }
+  for (int64_t i = 0; i < N; i++) deg[i + 1] += deg[i];
+  std::vector<int32_t> adj(deg[N]);
+  std::vector<int64_t> fill(deg.begin(), deg.end() - 1);
+  for (int64_t f = 0; f < F; f++)
+    if (R[f] >= 0) { adj[fill[L[f]]++] = R[f]; adj[fill[R[f]]++] = L[f]; }
+  std::vector<int32_t> col(N, -1);
+  int ncol = 0;
+  for (int64_t i = 0; i < N; i++) {
+    uint64_t used = 0;
+    for (int64_t k = deg[i]; k < deg[i + 1]; k++) {
+      const int cj = col[adj[k]];
+      if (cj >= 0 && cj < 64) used |= 1ull << cj;
+    }
+    int cc = 0;
+    while (cc < 64 && (used >> cc & 1)) cc++;
+    if (cc >= 64) return fail(c, DNDSG_SETUP_ERROR, "colouring needs more than 64 colours");
+    col[i] = cc;
+    ncol = std::max(ncol, cc + 1);
+  }
+  c->colourOff.assign(ncol + 1, 0);
+  for (int64_t i = 0; i < N; i++) c->colourOff[col[i] + 1]++;
+  for (int k = 0; k < ncol; k++) c->colourOff[k + 1] += c->colourOff[k];
+  std::vector<int32_t> cells(N);
+  std::vector<int64_t> pos(c->colourOff.begin(), c->colourOff.end() - 1);
+  for (int64_t i = 0; i < N; i++) cells[pos[col[i]]++] = (int32_t)i;
+  int rc;
+  if ((rc = dalloc(c, c->colourOf, sizeof(int32_t) * N)) || (rc = dalloc(c, c->colourCells, sizeof(int32_t) * N)) ||
+      (rc = dalloc(c, c->Dinv, sizeof(double) * N)) || (rc = dalloc(c, c->inc, sizeof(double) * 4 * N)) ||
+      (rc = dalloc(c, c->resAcc, sizeof(double) * 8)))
+    return rc;
+  DG_CUDA(c, cudaMemcpy(c->colourOf, col.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice));
+  DG_CUDA(c, cudaMemcpy(c->colourCells, cells.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice));
+  DG_CUDA(c, cudaMemset(c->inc, 0, sizeof(double) * 4 * N));
+  return 0;
+}
+
+template <class T>
+void launch_lusgs_sweep(dndsg_ctx* c, bool forward, double alpha, const double* rhs, double* inc, cudaStream_t s) {
+  HotView<T> h = view<T>(c);
+  const int nc = (int)c->colourOff.size() - 1;
+  for (int q = 0; q < nc; q++) {
+    const int k = forward ? q : nc - 1 - q;
+    const int64_t b = c->colourOff[k], n = c->colourOff[k + 1] - b;
+    if (n == 0) continue;
+    if (forward)
+      k_lusgs_colour<T, true><<<grid_for(n), kBlock, 0, s>>>(h, c->colourOf, c->colourCells + b, n, alpha, c->Dinv,
+                                                              rhs, inc);
+    else
+      k_lusgs_colour<T, false><<<grid_for(n), kBlock, 0, s>>>(h, c->colourOf, c->colourCells + b, n, alpha, c->Dinv,
+                                                               rhs, inc);
+  }
+}
+
+// ImplicitBDFDualTimeStep::Step (DNDS_ODE.hpp:444-486), one pseudo-time iteration at order 1, with
+// the EulerSolver lambdas (DNDS_FV_EulerSolver.hpp:713-925): fdtau (local EvaluateDt), frhs
+// (n_rec Jacobi sweeps, limiter, EvaluateRHS), fsolve (LUSGSMatrixInit, forward, backward from a
+// zero increment), then x += inc and the L1 norm of inc (the fstop residual) into resAcc
+template <class T>
+int run_implicit(dndsg_ctx* c, double cfl, double dtPhys, double alpha, int nRec, int volWise, double t,
+                 cudaStream_t s) {
+  int rc;
+  if ((rc = ensure_lusgs(c))) return rc;
+  run_dt<T>(c, cfl, 1e100, false, s);
+  for (int k = 0; k < nRec; k++) run_vr<T>(c, false, s);
+  if (c->s.limiter) run_limiter<T>(c, 0, s);
+  run_rhs<T>(c, t, s);
+  const double dtInv = 1.0 / dtPhys;
+  const int64_t n4 = c->N * 4;
+  k_bdf_rhs<<<(unsigned)((n4 + kBlock - 1) / kBlock), kBlock, 0, s>>>(n4, c->u, c->uLast, alpha, dtInv, c->rhs);
+  HotView<T> h = view<T>(c);
+  k_lusgs_init<T><<<grid_for(c->N), kBlock, 0, s>>>(h, dtInv, alpha, c->Dinv);
+  launch_lusgs_sweep<T>(c, true, alpha, c->rhs, c->inc, s);
+  launch_lusgs_sweep<T>(c, false, alpha, c->rhs, c->inc, s);
+  DG_CUDA(c, cudaMemsetAsync(c->resAcc, 0, sizeof(double) * 8, s));
+  k_add_inc<<<grid_for(c->N), kBlock, 0, s>>>(c->N, c->u, c->inc, c->vol, volWise, c->resAcc);
+  if (c->F > c->Fi)
+    k_wall_flux<<<grid_for(c->F - c->Fi), kBlock, 0, s>>>(c->Fi, c->F, c->faceBC, c->flux, c->resAcc + 4);
+  return check_launch(c);
+}
+}  // namespace
+
+extern "C" {
+
+int dndsg_lusgs_colours(dndsg_ctx* c, int32_t* colour_out, int* n_colours) {
+  if (!c) return DNDSG_BAD_ARGUMENT;
+  int rc;
+  if ((rc = set_device(c)) || (rc = ensure_lusgs(c))) return rc;
+  if (colour_out) DG_CUDA(c, cudaMemcpy(colour_out, c->colourOf, sizeof(int32_t) * c->N, cudaMemcpyDeviceToHost));
+  if (n_colours) *n_colours = (int)c->colourOff.size() - 1;
+  return 0;
+}
+
+int dndsg_lusgs_matrix_init(dndsg_ctx* c, double dt_phys, double alpha, void* s) {
+  if (!c || !(dt_phys > 0) || !(alpha > 0)) return DNDSG_BAD_ARGUMENT;
+  int rc;
+  if ((rc = set_device(c)) || (rc = ensure_lusgs(c))) return rc;
+  if (c->fp32) k_lusgs_init<float><<<grid_for(c->N), kBlock, 0, st(s)>>>(view<float>(c), 1.0 / dt_phys, alpha, c->Dinv);
+  else k_lusgs_init<double><<<grid_for(c->N), kBlock, 0, st(s)>>>(view<double>(c), 1.0 / dt_phys, alpha, c->Dinv);
+  return check_launch(c);
+}
+
+static int lusgs_sweep_api(dndsg_ctx* c, bool fwd, double alpha, const double* rhs, double* inc, void* s) {
+  if (!c || !rhs || !inc) return DNDSG_BAD_ARGUMENT;
+  if (!c->colourOf) return fail(c, DNDSG_BAD_ARGUMENT, "dndsg_lusgs_matrix_init first");
+  int rc;
+  if ((rc = set_device(c))) return rc;
+  if (c->fp32) launch_lusgs_sweep<float>(c, fwd, alpha, rhs, inc, st(s));
+  else launch_lusgs_sweep<double>(c, fwd, alpha, rhs, inc, st(s));
+  return check_launch(c);
+}
+
+int dndsg_lusgs_forward(dndsg_ctx* c, double alpha, const double* rhs, double* inc, void* s) {
+  return lusgs_sweep_api(c, true, alpha, rhs, inc, s);
+}
+
+int dndsg_lusgs_backward(dndsg_ctx* c, double alpha, const double* rhs, double* inc, void* s) {
+  return lusgs_sweep_api(c, false, alpha, rhs, inc, s);
+}
+
+int dndsg_bdf_begin(dndsg_ctx* c, void* s) {
+  if (!c) return DNDSG_BAD_ARGUMENT;
+  int rc;
+  if ((rc = set_device(c))) return rc;
+  DG_CUDA(c, cudaMemcpyAsync(c->uLast, c->u, sizeof(double) * 4 * c->N, cudaMemcpyDeviceToDevice, st(s)));
+  return 0;
+}
+
+int dndsg_implicit_iteration(dndsg_ctx* c, double cfl, double dt_phys, double alpha, int n_rec, int vol_wise,
+                             double t, double* inc_res_out, double* wall_flux_out, void* s) {
+  if (!c || !(cfl > 0) || !(dt_phys > 0) || !(alpha > 0) || n_rec < 0) return DNDSG_BAD_ARGUMENT;
+  int rc;
+  if ((rc = set_device(c))) return rc;
+  rc = c->fp32 ? run_implicit<float>(c, cfl, dt_phys, alpha, n_rec, vol_wise, t, st(s))
+               : run_implicit<double>(c, cfl, dt_phys, alpha, n_rec, vol_wise, t, st(s));
+  if (rc) return rc;
+  if (inc_res_out || wall_flux_out) {
+    double acc[8];
+    DG_CUDA(c, cudaMemcpyAsync(acc, c->resAcc, sizeof(acc), cudaMemcpyDeviceToHost, st(s)));
+    DG_CUDA(c, cudaStreamSynchronize(st(s)));
+    if (inc_res_out) for (int v = 0; v < 4; v++) inc_res_out[v] = acc[v];
+    if (wall_flux_out) for (int v = 0; v < 4; v++) wall_flux_out[v] = acc[4 + v];
+  }
+  return 0;
 }
 
 }  // extern "C"

@@ -264,6 +264,112 @@ def riemann_mesh(n: int, jitter: float = 0.15, seed: int = 4321) -> Mesh:
                            bc=BC_2DRIEMANN_FAR)
 
 
+def faces_from_cells(node_xy, cell_nodes, boundary_bc):
+    """Faces of a conforming mesh of counter-clockwise cells.  An edge a->b of a cell
+    has its right-hand normal out of that cell, so the first cell met owns the face as
+    its left cell and the cell that runs the edge b->a becomes the right cell.
+    boundary_bc(a, b) gives the BoundaryType of an edge with one cell."""
+    cell_nodes = np.asarray(cell_nodes)
+    key_face = {}
+    fn, fc = [], []
+    for c in range(cell_nodes.shape[0]):
+        nodes = [int(v) for v in cell_nodes[c] if v >= 0]
+        for k in range(len(nodes)):
+            a, b = nodes[k], nodes[(k + 1) % len(nodes)]
+            key = (a, b) if a < b else (b, a)
+            f = key_face.get(key)
+            if f is None:
+                key_face[key] = len(fn)
+                fn.append((a, b))
+                fc.append([c, -1])
+            else:
+                assert fc[f][1] < 0 and fn[f] == (b, a), "non-conforming or mis-oriented cells"
+                fc[f][1] = c
+    fb = [BC_INNER if r >= 0 else int(boundary_bc(a, b)) for (a, b), (_, r) in zip(fn, fc)]
+    return np.array(fn), np.array(fc), np.array(fb), np.zeros((len(fn), 2))
+
+
+def _geometric_ratio(d0: float, n: int, total: float) -> float:
+    """The ratio q > 1 with d0 (q^n - 1) / (q - 1) = total (bisection; needs n d0 < total)."""
+    assert n * d0 < total
+    lo, hi = 1.0 + 1e-12, 2.0
+    while d0 * (hi ** n - 1) / (hi - 1) < total:
+        hi *= 2
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        if d0 * (mid ** n - 1) / (mid - 1) < total:
+            lo = mid
+        else:
+            hi = mid
+    return 0.5 * (lo + hi)
+
+
+def naca0012_cmesh(n_airfoil: int = 256, n_wake: int = 128, nj: int = 128, first: float = 1e-6,
+                   far: float = 20.0, wall_bc: int = BC_WALL_NOSLIP, far_bc: int = BC_FARFIELD) -> Mesh:
+    """C-mesh of quadrilaterals around the NACA 0012 (4-digit thickness formula, closed trailing
+    edge, chord 1 from (0,0) to (1,0)): n_airfoil cells along the surface (cosine-clustered at both
+    edges), n_wake cells on each wake branch out to x = 1 + far, nj cells from the wall to the outer
+    boundary at distance `far`, the first one `first` (times the line length over `far`) thick and
+    the rest growing geometrically at the ratio that reaches `far` in nj cells.  The wake cut is a
+    line of interior faces.  Cells run (n_wake + n_airfoil + n_wake) x nj; faces on the airfoil get
+    wall_bc, the outer C and the two outflow lines far_bc."""
+    assert n_airfoil % 2 == 0
+    ni = 2 * n_wake + n_airfoil
+
+    def yt(x):
+        return 0.6 * (0.2969 * np.sqrt(x) - 0.1260 * x - 0.3516 * x ** 2 + 0.2843 * x ** 3 - 0.1036 * x ** 4)
+
+    h = n_airfoil // 2
+    xs = 0.5 * (1 - np.cos(np.pi * np.arange(h + 1) / h))          # LE (0) -> TE (1)
+    lower = np.stack([xs[::-1], -yt(xs[::-1])], 1)                   # TE -> LE
+    upper = np.stack([xs[1:], yt(xs[1:])], 1)                        # after LE -> TE
+    surf = np.concatenate([lower, upper])                            # n_airfoil + 1 points
+    # wake: geometric from the trailing-edge spacing to x = 1 + far
+    d0 = xs[-1] - xs[-2]
+    r = _geometric_ratio(d0, n_wake, far)
+    xw = 1.0 + d0 * (r ** np.arange(n_wake + 1) - 1) / (r - 1)
+    xw[-1] = 1.0 + far
+    wl = np.stack([xw[::-1], np.zeros(n_wake + 1)], 1)[:-1]          # far -> TE (TE excluded)
+    wu = np.stack([xw, np.zeros(n_wake + 1)], 1)[1:]                 # after TE -> far
+    inner = np.concatenate([wl, surf, wu])                           # ni + 1 points
+    # outer C: straight lines below/above the wake, half circle of radius far about (1, 0).
+    # Surface point x maps to the circle point straight above/below it (phi = asin((1 - x)/far)),
+    # fanning out towards the leading edge ((pi/2) s^8, s = 0 at the trailing edge, 1 at the
+    # leading edge); grid lines are straight from the surface to the outer boundary.
+    sfrac = np.arange(h + 1) / h                                      # TE (0) -> LE (1)
+    phi = np.maximum(np.arcsin(np.minimum(1.0, (1 - xs[::-1]) / far)), 0.5 * np.pi * sfrac ** 8)
+    lo_out = np.stack([1 - far * np.sin(phi), -far * np.cos(phi)], 1)            # TE -> LE
+    up_out = np.stack([1 - far * np.sin(phi[::-1]), far * np.cos(phi[::-1])], 1)[1:]  # after LE -> TE
+    outer = np.concatenate([np.stack([xw[::-1][:-1], -far * np.ones(n_wake)], 1), lo_out, up_out,
+                            np.stack([xw[1:], far * np.ones(n_wake)], 1)])
+    # distances: first cell `first`, geometric ratio q reaching `far` in nj cells
+    q = _geometric_ratio(first, nj, far)
+    dist = first * (q ** np.arange(nj + 1) - 1) / (q - 1)
+    frac = dist / dist[-1]
+    P = inner[:, None, :] + frac[None, :, None] * (outer - inner)[:, None, :]  # [ni+1, nj+1, 2]
+    # node numbering; upper-wake wall nodes are the lower-wake ones (the cut)
+    nid = np.arange((ni + 1) * (nj + 1)).reshape(ni + 1, nj + 1)
+    for i in range(n_wake + 1):
+        nid[ni - i, 0] = nid[i, 0]
+    used = np.unique(nid)
+    remap = -np.ones(nid.size, dtype=np.int64)
+    remap[used] = np.arange(used.size)
+    nid = remap[nid]
+    xy = np.zeros((used.size, 2))
+    xy[nid.ravel()] = P.reshape(-1, 2)
+    ii, jj = np.meshgrid(np.arange(ni), np.arange(nj), indexing="ij")
+    cells = np.stack([nid[ii, jj], nid[ii + 1, jj], nid[ii + 1, jj + 1], nid[ii, jj + 1]], -1).reshape(-1, 4)
+    wall_nodes = set(int(v) for v in nid[n_wake:n_wake + n_airfoil + 1, 0])
+
+    def bc(a, b):
+        return wall_bc if (a in wall_nodes and b in wall_nodes) else far_bc
+
+    faces = faces_from_cells(xy, cells, bc)
+    meta = dict(kind="naca0012_cmesh", n_airfoil=n_airfoil, n_wake=n_wake, nj=nj, first=first, far=far,
+                normal_ratio=float(q), wake_ratio=float(r))
+    return _as_mesh(xy, cells, faces, f"naca0012_c{ni}x{nj}", meta)
+
+
 def read_gmsh2(path: str) -> Mesh:
     """Gmsh 2.2 ASCII reader for 2-D meshes (SerialGmshReader2d, DNDS_Mesh.hpp:87-236).
 

@@ -147,10 +147,42 @@ RIEMANN_2D_STATES = [
 ]
 
 
+def free_stream(mach: float, alpha_deg: float, gamma: float = 1.4):
+    """Conservative free stream (rho, rho u, rho v, E) with rho = 1 and |V| = 1 at the given Mach
+    number and angle of attack."""
+    import math
+
+    a = math.radians(alpha_deg)
+    p = 1.0 / (gamma * mach * mach)
+    return [1.0, math.cos(a), math.sin(a), p / (gamma - 1) + 0.5]
+
+
+# vfvSetting of data/eulerSA_config_BenchSA.json:61-77 (Jacobi sweep instead of SOR), Roe flux,
+# free stream at M 0.15, alpha 10 degrees; the steady inviscid case of the implicit path
+NACA0012 = {
+    "recOrder": 2,
+    "vfvSetting": {
+        "SOR_Instead": False,
+        "JacobiRelax": 1.0,
+        "anisotropicLengths": False,
+        "tangWeight": 0.1,
+        "wallWeight": 1.5,
+        "farWeight": 1.0,
+        "weightSchemeGeom": "None",
+        "baseCenterType": "Bary",
+    },
+    "eulerSetting": {
+        "riemannSolverType": "Roe",
+        "idealGasProperty": {"gamma": 1.4},
+        "farFieldStaticValue": free_stream(0.15, 10.0),
+    },
+}
+
+
 def preset(name: str, **overrides) -> dict:
     import copy
 
-    base = {"vortex": ISENTROPIC_VORTEX, "riemann": RIEMANN_2D}[name]
+    base = {"vortex": ISENTROPIC_VORTEX, "riemann": RIEMANN_2D, "naca0012": NACA0012}[name]
     cfg = copy.deepcopy(base)
     for k, v in overrides.items():
         if isinstance(v, dict) and isinstance(cfg.get(k), dict):

@@ -153,6 +153,60 @@ class Solver:
     def ssprk3_step(self, cfl: float, t_end: float = 1e300):
         self._check(self.L.dndsg_ssprk3_step(self.h, cfl, t_end, self.stream))
 
+    # ------------------------------------------------------------------ implicit steady path
+    def lusgs_colours(self):
+        """(colour of every cell, number of colours) of the LU-SGS colouring."""
+        col = np.empty(self.N, dtype=np.int32)
+        n = C.c_int()
+        self._check(self.L.dndsg_lusgs_colours(self.h, _p(col), C.byref(n)))
+        return col, n.value
+
+    def LUSGSMatrixInit(self, dt: float = 1e100, alpha_diag: float = 1.0):
+        """LUSGSMatrixInit (DNDS_FV_EulerEvaluator.cpp:995-1047) from the last EvaluateDt."""
+        self._check(self.L.dndsg_lusgs_matrix_init(self.h, float(dt), float(alpha_diag), self.stream))
+
+    def UpdateLUSGSForward(self, alpha_diag: float, rhs_ptr: int, inc_ptr: int):
+        """In place on the device array inc [N][4] (DNDS_FV_EulerEvaluator.cpp:1149-1276)."""
+        self._check(self.L.dndsg_lusgs_forward(self.h, float(alpha_diag), C.c_void_p(rhs_ptr), C.c_void_p(inc_ptr),
+                                               self.stream))
+
+    def UpdateLUSGSBackward(self, alpha_diag: float, rhs_ptr: int, inc_ptr: int):
+        """In place on the device array inc [N][4] (DNDS_FV_EulerEvaluator.cpp:1285-1357)."""
+        self._check(self.L.dndsg_lusgs_backward(self.h, float(alpha_diag), C.c_void_p(rhs_ptr), C.c_void_p(inc_ptr),
+                                                self.stream))
+
+    def bdf_begin(self):
+        self._check(self.L.dndsg_bdf_begin(self.h, self.stream))
+
+    def implicit_iteration(self, cfl: float, dt: float = 1e100, alpha_diag: float = 1.0, n_rec: int = 1,
+                           vol_wise: bool = False, t: float = 0.0):
+        """One first-order BDF pseudo-time iteration; returns (L1 norm of the increment, wall flux)."""
+        res = np.empty(4)
+        wf = np.empty(4)
+        self._check(self.L.dndsg_implicit_iteration(self.h, float(cfl), float(dt), float(alpha_diag), int(n_rec),
+                                                    int(vol_wise), float(t), _p(res), _p(wf), self.stream))
+        return res, wf
+
+    def steady_solve(self, cfl: float, threshold: float = 1e-8, max_iter: int = 10000, dt: float = 1e100,
+                     n_rec: int = 1, vol_wise: bool = False, history: list | None = None):
+        """Pseudo-time iterations until the density component of the increment norm, relative to its
+        largest value so far, drops below threshold (fstop, DNDS_FV_EulerSolver.hpp:984-994).
+        Returns (iterations, relative residual, wall flux of the last iteration)."""
+        self.bdf_begin()
+        base = None
+        rel = np.ones(4)
+        wf = np.zeros(4)
+        it = 0
+        for it in range(1, max_iter + 1):
+            res, wf = self.implicit_iteration(cfl, dt, 1.0, n_rec, vol_wise)
+            base = res.copy() if base is None else np.maximum(base, res)
+            rel = res / np.where(base > 0, base, 1.0)
+            if history is not None:
+                history.append(res.copy())
+            if rel[0] < threshold:
+                break
+        return it, rel, wf
+
     # ------------------------------------------------------------------ learned warm start
     def mlp_features(self, X_ptr: int, scales_ptr: int):
         """Features [N][44] and scales [N][4] of the current state into device arrays."""

@@ -182,6 +182,39 @@ int dndsg_eval_rhs_noalloc(dndsg_ctx* ctx, const double* u, const void* urec, do
 int dndsg_get_status(dndsg_ctx* ctx, uint32_t* flags, uint64_t* n_reduced, void* stream);
 
 /* ---------------------------------------------------------------------------
+ * Implicit steady path: colour-batched LU-SGS and first-order BDF pseudo time.
+ * The reference sweeps cells one at a time in a scan order
+ * (UpdateLUSGSForward / Backward, DNDS_FV_EulerEvaluator.cpp:1149-1357).  Here
+ * the cells get a greedy distance-1 colouring and each colour is one parallel
+ * step; that is exactly the reference's sweep in the colour-sorted scan order
+ * (a neighbour is "before" a cell when its colour is smaller).  The diagonal
+ * is one scalar per cell, as in the reference without source terms.
+ * ------------------------------------------------------------------------ */
+/* the colouring: colour_out [n_cells] (host, may be NULL), n_colours */
+int dndsg_lusgs_colours(dndsg_ctx* ctx, int32_t* colour_out, int* n_colours);
+/* LUSGSMatrixInit (DNDS_FV_EulerEvaluator.cpp:995-1047): D_i = 1/dTau_i + 1/dt
+ * + sum_f (alpha/2) lambda_f A_f / V_i with dTau = (the DNDSG_BUF_DT of the last
+ * dndsg_eval_dt) / alpha, and lambda_f from that same call */
+int dndsg_lusgs_matrix_init(dndsg_ctx* ctx, double dt_phys, double alpha, void* stream);
+/* UpdateLUSGSForward / UpdateLUSGSBackward (DNDS_FV_EulerEvaluator.cpp:1149-1357)
+ * in place on inc [n_cells][nvars] (device) with rhs [n_cells][nvars] (device),
+ * about the context's u; forward expects inc zero where the reference does */
+int dndsg_lusgs_forward(dndsg_ctx* ctx, double alpha, const double* rhs, double* inc, void* stream);
+int dndsg_lusgs_backward(dndsg_ctx* ctx, double alpha, const double* rhs, double* inc, void* stream);
+/* start of a physical BDF step: xLast = u */
+int dndsg_bdf_begin(dndsg_ctx* ctx, void* stream);
+/* one pseudo-time iteration of ImplicitBDFDualTimeStep::Step at order 1
+ * (DNDS_ODE.hpp:444-486) with the EulerSolver fdtau / frhs / fsolve lambdas
+ * (DNDS_FV_EulerSolver.hpp:713-925): local EvaluateDt at cfl, n_rec Jacobi
+ * sweeps, [limiter], EvaluateRHS at t, rhs = alpha R - (u - xLast)/dt_phys,
+ * LU-SGS forward + backward from zero, u += inc.  inc_res_out [nvars] (host,
+ * may be NULL): the L1 norm of inc (volume-weighted when vol_wise), the
+ * quantity the reference's fstop tests; wall_flux_out [nvars] (host, may be
+ * NULL): fluxWallSum of this iteration's RHS. */
+int dndsg_implicit_iteration(dndsg_ctx* ctx, double cfl, double dt_phys, double alpha, int n_rec, int vol_wise,
+                             double t, double* inc_res_out, double* wall_flux_out, void* stream);
+
+/* ---------------------------------------------------------------------------
  * Learned warm start for the VR coefficients.  No counterpart in the
  * reference: a per-cell network 64 -> 64 -> 64 -> 64 -> 20 (SiLU), BF16
  * weights and activations with FP32 accumulation on the tensor cores, trained

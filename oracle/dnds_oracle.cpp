@@ -142,6 +142,7 @@ struct orc_ctx {
   std::vector<double> u, urec, urecNew, urec1;
   std::vector<double> dtFace, lambdaFace, deltaLambdaFace, lambdaCell;
   std::vector<double> dtCell;
+  std::vector<double> Dinv;  // LU-SGS diagonal inverse (scalar per cell: NS_2D has no source term)
   double lastInc = 0;
   std::string err;
 };
@@ -1196,6 +1197,90 @@ void eval_rhs(orc_ctx& c, double t, double* rhs, double* wallFlux, int* nreduced
   if (nreduced) *nreduced = red.load();
 }
 
+// ------------------------------------------------------------------ implicit path
+// EulerEvaluator::fluxJacobian0_Right_Times_du (DNDS_FV_EulerEvaluator.hpp:928-956) for NS_2D:
+// the inviscid flux increment of dU about U through the unit normal n
+// (Gas::IdealGasUIncrement, GasInviscidFluxFacialIncrement, DNDS_Gas.hpp:122-146),
+// minus lambdaMain * dU
+void flux_jac_times_du(const double* U, const double* n, const double* dU, double lam, double gamma, double* dF) {
+  const double vx = U[1] / U[0], vy = U[2] / U[0];
+  double p, a2, H;
+  thermal(U[3], U[0], vx * vx + vy * vy, gamma, p, a2, H);
+  const double dvx = (dU[1] - U[1] / U[0] * dU[0]) / U[0], dvy = (dU[2] - U[2] / U[0] * dU[0]) / U[0];
+  const double dp = (gamma - 1) * (dU[3] - 0.5 * (dU[1] * vx + dU[2] * vy + U[1] * dvx + U[2] * dvy));
+  const double vn = vx * n[0] + vy * n[1], dvn = dvx * n[0] + dvy * n[1];
+  dF[0] = dU[1] * n[0] + dU[2] * n[1];
+  dF[1] = dU[1] * vn + U[1] * dvn + n[0] * dp;
+  dF[2] = dU[2] * vn + U[2] * dvn + n[1] * dp;
+  dF[3] = (dU[3] + dp) * vn + (U[3] + p) * dvn;
+  for (int k = 0; k < 4; k++) dF[k] -= lam * dU[k];
+}
+
+// LUSGSMatrixInit (DNDS_FV_EulerEvaluator.cpp:995-1047), jacobianCode 0, no source term:
+// D_i = 1/dTau_i + 1/dt + sum_f (alpha/2) A_f lambdaFace_f / V_i, kept as its inverse
+void lusgs_matrix_init(orc_ctx& c, const double* dTau, double dt, double alpha) {
+  c.Dinv.assign(c.N, 0.0);
+  for (int64_t i = 0; i < c.N; i++) {
+    const CellGeo& g = c.cg[i];
+    double d = 1.0 / dTau[i] + 1.0 / dt;
+    for (int k = 0; k < g.nface; k++) {
+      const int f = g.faces[k];
+      d += (0.5 * alpha) * c.fg[f].area * c.lambdaFace[f] / g.vol;
+    }
+    c.Dinv[i] = 1.0 / d;
+  }
+}
+
+// the off-diagonal sum of UpdateLUSGSForward / Backward (DNDS_FV_EulerEvaluator.cpp:1149-1357)
+// over the neighbours j with scan position before (forward) or after (backward) cell i
+void lusgs_offdiag(const orc_ctx& c, int64_t i, int64_t si, const std::vector<int64_t>& pos, bool forward,
+                   double alpha, const double* inc, double* buf) {
+  const CellGeo& g = c.cg[i];
+  for (int k = 0; k < g.nface; k++) {
+    const int f = g.faces[k];
+    const FaceGeo& fg = c.fg[f];
+    const int64_t j = fg.L == i ? fg.R : fg.L;
+    if (j < 0) continue;
+    if (forward ? !(pos[j] < si) : !(pos[j] > si)) continue;
+    const double nn = std::sqrt(sqr(fg.ncenter[0]) + sqr(fg.ncenter[1]));
+    const double sg = fg.L == i ? 1.0 : -1.0;  // faces out of i
+    const double n[2] = {sg * fg.ncenter[0] / nn, sg * fg.ncenter[1] / nn};
+    double dF[4];
+    flux_jac_times_du(&c.u[j * 4], n, &inc[j * 4], c.lambdaFace[f], c.s.gamma, dF);
+    for (int v = 0; v < 4; v++) buf[v] -= (0.5 * alpha) * fg.area / g.vol * dF[v];
+  }
+}
+
+void scan_positions(const orc_ctx& c, const int64_t* scan2cell, std::vector<int64_t>& order,
+                    std::vector<int64_t>& pos) {
+  order.resize(c.N);
+  pos.resize(c.N);
+  for (int64_t s = 0; s < c.N; s++) order[s] = scan2cell ? scan2cell[s] : s;
+  for (int64_t s = 0; s < c.N; s++) pos[order[s]] = s;
+}
+
+// forward then backward sweep in place on inc (the reference calls both with uInc == uIncNew)
+void lusgs_sweeps(const orc_ctx& c, double alpha, const double* rhs, double* inc, const int64_t* scan2cell,
+                  bool doForward, bool doBackward) {
+  std::vector<int64_t> order, pos;
+  scan_positions(c, scan2cell, order, pos);
+  if (doForward)
+    for (int64_t s = 0; s < c.N; s++) {
+      const int64_t i = order[s];
+      double buf[4];
+      for (int v = 0; v < 4; v++) buf[v] = rhs[i * 4 + v];
+      lusgs_offdiag(c, i, s, pos, true, alpha, inc, buf);
+      for (int v = 0; v < 4; v++) inc[i * 4 + v] = c.Dinv[i] * buf[v];
+    }
+  if (doBackward)
+    for (int64_t s = c.N - 1; s >= 0; s--) {
+      const int64_t i = order[s];
+      double buf[4] = {0, 0, 0, 0};
+      lusgs_offdiag(c, i, s, pos, false, alpha, inc, buf);
+      for (int v = 0; v < 4; v++) inc[i * 4 + v] += c.Dinv[i] * buf[v];
+    }
+}
+
 }  // namespace
 
 // ====================================================================== C ABI
@@ -1365,6 +1450,51 @@ int orc_residual(orc_ctx* c, const double* rhs, int p, int vol_wise, double* out
     for (int64_t i = 0; i < c->N; i++)
       for (int k = 0; k < nv; k++) out[k] = std::max(out[k], std::fabs(rhs[i * nv + k]));
   }
+  return 0;
+}
+
+int orc_lusgs_matrix_init(orc_ctx* c, const double* dtau, double dt, double alpha) {
+  std::vector<double> d(c->N);
+  for (int64_t i = 0; i < c->N; i++) d[i] = dtau ? dtau[i] : c->dtCell[i] / alpha;
+  lusgs_matrix_init(*c, d.data(), dt, alpha);
+  return 0;
+}
+
+int orc_lusgs_forward(orc_ctx* c, double alpha, const double* rhs, double* inc, const int64_t* scan2cell) {
+  if (c->Dinv.size() != (size_t)c->N) return 1;
+  lusgs_sweeps(*c, alpha, rhs, inc, scan2cell, true, false);
+  return 0;
+}
+
+int orc_lusgs_backward(orc_ctx* c, double alpha, const double* rhs, double* inc, const int64_t* scan2cell) {
+  if (c->Dinv.size() != (size_t)c->N) return 1;
+  lusgs_sweeps(*c, alpha, rhs, inc, scan2cell, false, true);
+  return 0;
+}
+
+// one pseudo-time iteration of ImplicitBDFDualTimeStep::Step (DNDS_ODE.hpp:444-486) at BDF order 1
+// with the EulerSolver lambdas fdtau / frhs / fsolve (DNDS_FV_EulerSolver.hpp:713-925):
+// dTau = EvaluateDt(CFL, local)/alpha; nInternalRecStep Jacobi sweeps; [limiter]; EvaluateRHS;
+// rhs = alpha R - (x - xLast)/dt; LU-SGS forward + backward from zero; x += inc
+int orc_implicit_iteration(orc_ctx* c, double cfl, double dt, double alpha, const double* x_last,
+                           const int64_t* scan2cell, double t, int n_rec, double* inc_out) {
+  const int64_t n = c->N * 4;
+  double dtMin;
+  eval_dt(*c, cfl, 1e100, true, &dtMin);
+  std::vector<double> dTau(c->N), rhs(n), inc(n, 0.0);
+  for (int64_t i = 0; i < c->N; i++) dTau[i] = c->dtCell[i] / alpha;
+  for (int k = 0; k < n_rec; k++) vr_sweep(*c);
+  if (c->s.limiter) limiter_wbap(*c, false, nullptr);
+  eval_rhs(*c, t, rhs.data(), nullptr, nullptr);
+  for (int64_t k = 0; k < n; k++) {
+    rhs[k] *= alpha;
+    rhs[k] += -c->u[k] / dt;
+    rhs[k] += x_last[k] / dt;
+  }
+  lusgs_matrix_init(*c, dTau.data(), dt, alpha);
+  lusgs_sweeps(*c, alpha, rhs.data(), inc.data(), scan2cell, true, true);
+  for (int64_t k = 0; k < n; k++) c->u[k] += inc[k];
+  if (inc_out) std::memcpy(inc_out, inc.data(), sizeof(double) * n);
   return 0;
 }
 

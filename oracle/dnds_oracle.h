@@ -13,6 +13,10 @@
  *   - EulerEvaluator::EvaluateRHS   DNDS_FV_EulerEvaluator.cpp:198-640
  *   - Roe / HLLC fluxes             DNDS_Gas.hpp:312-654
  *   - ExplicitSSPRK3LocalDt::Step   DNDS_ODE.hpp:131-177
+ *   - LU-SGS (LUSGSMatrixInit, UpdateLUSGSForward/Backward,
+ *     fluxJacobian0_Right_Times_du)  DNDS_FV_EulerEvaluator.cpp:995-1357,
+ *                                   DNDS_FV_EulerEvaluator.hpp:928-956
+ *   - ImplicitBDFDualTimeStep::Step DNDS_ODE.hpp:420-497 (order 1)
  *   - EvaluateResidual              DNDS_FV_EulerEvaluator.cpp:1557-1592
  * Deviations (documented where they occur): no Eigen (the 5x5 inverse is a
  * pivoted Gauss-Jordan instead of JacobiSVD; A_ii is SPD so both give A^-1),
@@ -114,6 +118,19 @@ int orc_face_values(orc_ctx* c, double t, double* out);
 int orc_ssprk3_step(orc_ctx* c, double dt, double t);
 /* EvaluateResidual */
 int orc_residual(orc_ctx* c, const double* rhs, int p, int vol_wise, double* out);
+
+/* LUSGSMatrixInit (DNDS_FV_EulerEvaluator.cpp:995-1047): dtau [n] (NULL: the
+ * dt of the last orc_eval_dt divided by alpha), physical dt, alphaDiag */
+int orc_lusgs_matrix_init(orc_ctx* c, const double* dtau, double dt, double alpha);
+/* UpdateLUSGSForward / Backward (DNDS_FV_EulerEvaluator.cpp:1149-1357) in place
+ * on inc [n][nvars]; scan2cell [n] is the sweep order (NULL: natural order) */
+int orc_lusgs_forward(orc_ctx* c, double alpha, const double* rhs, double* inc, const int64_t* scan2cell);
+int orc_lusgs_backward(orc_ctx* c, double alpha, const double* rhs, double* inc, const int64_t* scan2cell);
+/* one BDF pseudo-time iteration (ImplicitBDFDualTimeStep::Step, DNDS_ODE.hpp:444-486,
+ * first order) with the EulerSolver fdtau/frhs/fsolve lambdas; x_last [n][nvars]
+ * is the state at the start of the physical step; inc_out [n][nvars] may be NULL */
+int orc_implicit_iteration(orc_ctx* c, double cfl, double dt, double alpha, const double* x_last,
+                           const int64_t* scan2cell, double t, int n_rec, double* inc_out);
 
 /* setup products, for cross-checks: [n][5][5], [n][4][5][5], [n][4][5] */
 int orc_get_vr_blocks(orc_ctx* c, double* ainv, double* ainvb, double* ainv_b);

@@ -92,6 +92,10 @@ def lib():
         L.orc_residual.argtypes = [vp, vp, i32, i32, vp]
         L.orc_get_vr_blocks.argtypes = [vp, vp, vp, vp]
         L.orc_get_face_dibj.argtypes = [vp, vp]
+        L.orc_lusgs_matrix_init.argtypes = [vp, vp, dbl, dbl]
+        L.orc_lusgs_forward.argtypes = [vp, dbl, vp, vp, vp]
+        L.orc_lusgs_backward.argtypes = [vp, dbl, vp, vp, vp]
+        L.orc_implicit_iteration.argtypes = [vp, dbl, dbl, dbl, vp, vp, dbl, i32, vp]
         L.orc_riemann_flux.argtypes = [i32, vp, vp, dbl, dbl, vp]
         L.orc_riemann_flux.restype = None
         _lib = L
@@ -215,6 +219,39 @@ class Oracle:
 
     def ssprk3_step(self, dt, t):
         lib().orc_ssprk3_step(self.h, dt, t)
+
+    # ---------------------------------------------------------------- implicit path
+    @staticmethod
+    def _order(scan2cell):
+        if scan2cell is None:
+            return None, None
+        o = np.ascontiguousarray(scan2cell, dtype=np.int64)
+        return o, _p(o)
+
+    def lusgs_matrix_init(self, dt, alpha=1.0, dtau=None):
+        d = None if dtau is None else np.ascontiguousarray(dtau, dtype=np.float64)
+        lib().orc_lusgs_matrix_init(self.h, _p(d) if d is not None else None, dt, alpha)
+
+    def lusgs_forward(self, rhs, inc, alpha=1.0, scan2cell=None):
+        """In place on inc (float64 [N][nv])."""
+        rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+        o, op = self._order(scan2cell)
+        if lib().orc_lusgs_forward(self.h, alpha, _p(rhs), _p(inc), op):
+            raise RuntimeError("lusgs_matrix_init first")
+
+    def lusgs_backward(self, rhs, inc, alpha=1.0, scan2cell=None):
+        rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+        o, op = self._order(scan2cell)
+        if lib().orc_lusgs_backward(self.h, alpha, _p(rhs), _p(inc), op):
+            raise RuntimeError("lusgs_matrix_init first")
+
+    def implicit_iteration(self, cfl, x_last, dt=1e100, alpha=1.0, scan2cell=None, t=0.0, n_rec=1):
+        """One first-order BDF pseudo-time iteration; returns the increment [N][nv]."""
+        xl = np.ascontiguousarray(x_last, dtype=np.float64)
+        inc = np.empty((self.N, self.nv))
+        o, op = self._order(scan2cell)
+        lib().orc_implicit_iteration(self.h, cfl, dt, alpha, _p(xl), op, t, n_rec, _p(inc))
+        return inc
 
     def residual(self, rhs, p=1, vol_wise=False):
         rhs = np.ascontiguousarray(rhs, dtype=np.float64)
