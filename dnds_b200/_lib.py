@@ -19,7 +19,7 @@ EXPORTS = [
     "dndsg_mlp_create", "dndsg_mlp_destroy", "dndsg_mlp_last_error", "dndsg_mlp_set_params",
     "dndsg_mlp_get_params", "dndsg_mlp_forward", "dndsg_mlp_gradient", "dndsg_mlp_train_step",
     "dndsg_mlp_features", "dndsg_vr_to_tolerance", "dndsg_ssprk3_step_tol",
-    "dndsg_lusgs_colours", "dndsg_lusgs_matrix_init", "dndsg_lusgs_forward", "dndsg_lusgs_backward",
+    "dndsg_lusgs_colours", "dndsg_lusgs_set_order", "dndsg_lusgs_matrix_init", "dndsg_lusgs_forward", "dndsg_lusgs_backward",
     "dndsg_bdf_begin", "dndsg_implicit_iteration",
 ]
 _NO_STATUS = ("dndsg_destroy", "dndsg_last_error", "dndsg_n_cells", "dndsg_n_faces", "dndsg_mlp_destroy",
@@ -89,6 +89,7 @@ def lib():
     L.dndsg_vr_to_tolerance.argtypes = [vp, vp, dbl, i32, C.POINTER(i32), C.POINTER(i64), vp, vp, vp]
     L.dndsg_ssprk3_step_tol.argtypes = [vp, vp, dbl, dbl, dbl, i32, C.POINTER(i32), vp, vp, vp]
     L.dndsg_lusgs_colours.argtypes = [vp, vp, C.POINTER(i32)]
+    L.dndsg_lusgs_set_order.argtypes = [vp, i32, vp, C.POINTER(i32)]
     L.dndsg_lusgs_matrix_init.argtypes = [vp, dbl, dbl, vp]
     L.dndsg_lusgs_forward.argtypes = [vp, dbl, vp, vp, vp]
     L.dndsg_lusgs_backward.argtypes = [vp, dbl, vp, vp, vp]

@@ -51,9 +51,15 @@ struct dndsg_ctx {
   float* mlpSc = nullptr;                                                     // [N][4] output scales
   unsigned long long* accCount = nullptr;
   int64_t nWallCells = 0;
-  // implicit path: distance-1 colouring, LU-SGS diagonal, increment, residual accumulator
-  int32_t *colourOf = nullptr, *colourCells = nullptr;
-  std::vector<int64_t> colourOff;
+  // implicit path: the sweep order as a rank per cell (a neighbour of lower rank is "before"),
+  // the forward / backward schedules (batches of independent cells), LU-SGS diagonal,
+  // increment, residual accumulator
+  int32_t *rankOf = nullptr, *fwdCells = nullptr, *bwdCells = nullptr;
+  std::vector<int64_t> fwdOff, bwdOff;
+  int64_t *fwdOffDev = nullptr, *bwdOffDev = nullptr;  // level offsets on the device (scan-order mode)
+  int64_t maxLevelWidth = 0;
+  std::vector<int32_t> colourHost;  // greedy colouring, kept for dndsg_lusgs_colours
+  int lusgsOrder = 0;               // 0 colour batches, 1 level-scheduled scan order
   double *Dinv = nullptr, *inc = nullptr, *resAcc = nullptr;
   // state
   double *u = nullptr, *uLast = nullptr, *rhs = nullptr, *dt = nullptr, *flux = nullptr, *lamA = nullptr,
@@ -1521,18 +1527,17 @@ __global__ void k_bdf_rhs(int64_t n4, const double* u, const double* uLast, doub
   rhs[e] = alpha * rhs[e] - u[e] * dtPhysInv + uLast[e] * dtPhysInv;
 }
 
-// one colour of UpdateLUSGSForward (FWD) or UpdateLUSGSBackward (DNDS_FV_EulerEvaluator.cpp:
-// 1149-1357).  Cells of one colour share no face, so sweeping the colours in order is the
-// reference's sweep in the colour-sorted scan order: a neighbour is "before" a cell exactly
-// when its colour is smaller.  inc is updated in place, as the reference calls both sweeps.
+// one batch of UpdateLUSGSForward (FWD) or UpdateLUSGSBackward (DNDS_FV_EulerEvaluator.cpp:
+// 1149-1357): a neighbour j is "before" cell i when rank[j] < rank[i].  With rank = colour and
+// one batch per colour this is the reference's sweep in the colour-sorted scan order; with
+// rank = scan position and one batch per dependency level it is the reference's sequential
+// sweep in that scan order, level by level.  No two cells of a batch are neighbours and every
+// neighbour a cell reads was finished in an earlier batch, so the result does not depend on the
+// order within a batch.  inc is updated in place, as the reference calls both sweeps.
 template <class T, bool FWD>
-__global__ void __launch_bounds__(kBlock) k_lusgs_colour(HotView<T> h, const int32_t* colourOf,
-                                                         const int32_t* cells, int64_t n, double alpha,
-                                                         const double* Dinv, const double* rhs, double* inc) {
-  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  const int64_t i = cells[t];
-  const int ci = colourOf[i];
+__device__ __forceinline__ void lusgs_cell(const HotView<T>& h, const int32_t* rankOf, int64_t i, double alpha,
+                                           const double* Dinv, const double* rhs, double* inc) {
+  const int ci = rankOf[i];
   double buf[4];
   if (FWD) load4<T>(&rhs[i * 4], buf);
   else buf[0] = buf[1] = buf[2] = buf[3] = 0.0;
@@ -1543,7 +1548,7 @@ __global__ void __launch_bounds__(kBlock) k_lusgs_colour(HotView<T> h, const int
     const int32_t f = sf >= 0 ? sf : ~sf;
     const int32_t j = sf >= 0 ? h.faceR[f] : h.faceL[f];
     if (j < 0) continue;
-    const int cj = colourOf[j];
+    const int cj = rankOf[j];
     if (FWD ? !(cj < ci) : !(cj > ci)) continue;
     const double sg = sf >= 0 ? 1.0 : -1.0;
     const double area = h.faceArea[f];
@@ -1559,6 +1564,30 @@ __global__ void __launch_bounds__(kBlock) k_lusgs_colour(HotView<T> h, const int
     for (int v = 0; v < 4; v++) o[v] = di * buf[v];
   } else {
     for (int v = 0; v < 4; v++) o[v] += di * buf[v];
+  }
+}
+
+template <class T, bool FWD>
+__global__ void __launch_bounds__(kBlock) k_lusgs_batch(HotView<T> h, const int32_t* rankOf,
+                                                        const int32_t* cells, int64_t n, double alpha,
+                                                        const double* Dinv, const double* rhs, double* inc) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t < n) lusgs_cell<T, FWD>(h, rankOf, cells[t], alpha, Dinv, rhs, inc);
+}
+
+// a whole sweep of narrow batches (dependency levels) in one thread block: the levels run one
+// after another with a block barrier between them, which makes a level's increments visible to
+// the next; no grid-wide synchronisation and no waiting on flags
+constexpr int kLevelBlock = 512;
+template <class T, bool FWD>
+__global__ void __launch_bounds__(kLevelBlock) k_lusgs_levels(HotView<T> h, const int32_t* rankOf,
+                                                              const int32_t* cells, const int64_t* off, int nlev,
+                                                              double alpha, const double* Dinv, const double* rhs,
+                                                              double* inc) {
+  for (int l = 0; l < nlev; l++) {
+    const int64_t b = off[l], e = off[l + 1];
+    for (int64_t t = b + threadIdx.x; t < e; t += blockDim.x) lusgs_cell<T, FWD>(h, rankOf, cells[t], alpha, Dinv, rhs, inc);
+    __syncthreads();
   }
 }
 
@@ -1598,21 +1627,52 @@ __global__ void __launch_bounds__(kBlock) k_wall_flux(int64_t Fi, int64_t F, con
   }
 }
 
-// greedy distance-1 colouring over the interior faces, in cell order; cells sorted by colour
-int ensure_lusgs(dndsg_ctx* c) {
-  if (c->colourOf) return 0;
+// cell adjacency over the interior faces (CSR), from the device face table
+int lusgs_adjacency(dndsg_ctx* c, std::vector<int64_t>& deg, std::vector<int32_t>& adj) {
   const int64_t N = c->N, F = c->F;
   std::vector<int32_t> L(F), R(F);
   DG_CUDA(c, cudaMemcpy(L.data(), c->faceL, sizeof(int32_t) * F, cudaMemcpyDeviceToHost));
   DG_CUDA(c, cudaMemcpy(R.data(), c->faceR, sizeof(int32_t) * F, cudaMemcpyDeviceToHost));
-  std::vector<int64_t> deg(N + 1, 0);
+  deg.assign(N + 1, 0);
   for (int64_t f = 0; f < F; f++)
     if (R[f] >= 0) { deg[L[f] + 1]++; deg[R[f] + 1]++; }
   for (int64_t i = 0; i < N; i++) deg[i + 1] += deg[i];
-  std::vector<int32_t> adj(deg[N]);
+  adj.assign(deg[N], 0);
   std::vector<int64_t> fill(deg.begin(), deg.end() - 1);
   for (int64_t f = 0; f < F; f++)
     if (R[f] >= 0) { adj[fill[L[f]]++] = R[f]; adj[fill[R[f]]++] = L[f]; }
+  return 0;
+}
+
+// cells grouped by key (0..nkey-1), in cell order within a group
+void group_by(const std::vector<int32_t>& key, int nkey, std::vector<int32_t>& cells, std::vector<int64_t>& off) {
+  const int64_t N = (int64_t)key.size();
+  off.assign(nkey + 1, 0);
+  for (int64_t i = 0; i < N; i++) off[key[i] + 1]++;
+  for (int k = 0; k < nkey; k++) off[k + 1] += off[k];
+  cells.assign(N, 0);
+  std::vector<int64_t> pos(off.begin(), off.end() - 1);
+  for (int64_t i = 0; i < N; i++) cells[pos[key[i]]++] = (int32_t)i;
+}
+
+int upload_schedule(dndsg_ctx* c, const std::vector<int32_t>& rank, const std::vector<int32_t>& fwd,
+                    const std::vector<int32_t>& bwd) {
+  const int64_t N = c->N;
+  DG_CUDA(c, cudaMemcpy(c->rankOf, rank.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice));
+  DG_CUDA(c, cudaMemcpy(c->fwdCells, fwd.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice));
+  DG_CUDA(c, cudaMemcpy(c->bwdCells, bwd.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice));
+  return 0;
+}
+
+// default schedule: greedy distance-1 colouring in cell order; forward runs the colours up,
+// backward down
+int ensure_lusgs(dndsg_ctx* c) {
+  if (c->rankOf) return 0;
+  const int64_t N = c->N;
+  std::vector<int64_t> deg;
+  std::vector<int32_t> adj;
+  int rc;
+  if ((rc = lusgs_adjacency(c, deg, adj))) return rc;
   std::vector<int32_t> col(N, -1);
   int ncol = 0;
   for (int64_t i = 0; i < N; i++) {
@@ -1627,37 +1687,98 @@ int ensure_lusgs(dndsg_ctx* c) {
     col[i] = cc;
     ncol = std::max(ncol, cc + 1);
   }
-  c->colourOff.assign(ncol + 1, 0);
-  for (int64_t i = 0; i < N; i++) c->colourOff[col[i] + 1]++;
-  for (int k = 0; k < ncol; k++) c->colourOff[k + 1] += c->colourOff[k];
-  std::vector<int32_t> cells(N);
-  std::vector<int64_t> pos(c->colourOff.begin(), c->colourOff.end() - 1);
-  for (int64_t i = 0; i < N; i++) cells[pos[col[i]]++] = (int32_t)i;
-  int rc;
-  if ((rc = dalloc(c, c->colourOf, sizeof(int32_t) * N)) || (rc = dalloc(c, c->colourCells, sizeof(int32_t) * N)) ||
-      (rc = dalloc(c, c->Dinv, sizeof(double) * N)) || (rc = dalloc(c, c->inc, sizeof(double) * 4 * N)) ||
-      (rc = dalloc(c, c->resAcc, sizeof(double) * 8)))
+  std::vector<int32_t> fwd, bwd;
+  group_by(col, ncol, fwd, c->fwdOff);
+  std::vector<int32_t> rev(N);
+  for (int64_t i = 0; i < N; i++) rev[i] = ncol - 1 - col[i];
+  group_by(rev, ncol, bwd, c->bwdOff);
+  if ((rc = dalloc(c, c->rankOf, sizeof(int32_t) * N)) || (rc = dalloc(c, c->fwdCells, sizeof(int32_t) * N)) ||
+      (rc = dalloc(c, c->bwdCells, sizeof(int32_t) * N)) || (rc = dalloc(c, c->Dinv, sizeof(double) * N)) ||
+      (rc = dalloc(c, c->inc, sizeof(double) * 4 * N)) || (rc = dalloc(c, c->resAcc, sizeof(double) * 8)))
     return rc;
-  DG_CUDA(c, cudaMemcpy(c->colourOf, col.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice));
-  DG_CUDA(c, cudaMemcpy(c->colourCells, cells.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice));
+  c->colourHost = col;
+  c->lusgsOrder = 0;
   DG_CUDA(c, cudaMemset(c->inc, 0, sizeof(double) * 4 * N));
-  return 0;
+  return upload_schedule(c, col, fwd, bwd);
+}
+
+// the reference's sequential sweep in a given scan order, level-scheduled: the forward level of a
+// cell is one more than the largest forward level of its neighbours earlier in the scan (the
+// backward level likewise over the later ones), and each level is one batch
+int set_scan_order(dndsg_ctx* c, const int64_t* scan2cell) {
+  int rc;
+  if ((rc = ensure_lusgs(c))) return rc;
+  const int64_t N = c->N;
+  std::vector<int32_t> pos(N, -1), order(N);
+  for (int64_t s = 0; s < N; s++) {
+    const int64_t i = scan2cell ? scan2cell[s] : s;
+    if (i < 0 || i >= N || pos[i] >= 0) return fail(c, DNDSG_BAD_ARGUMENT, "scan order is not a permutation");
+    pos[i] = (int32_t)s;
+    order[s] = (int32_t)i;
+  }
+  std::vector<int64_t> deg;
+  std::vector<int32_t> adj;
+  if ((rc = lusgs_adjacency(c, deg, adj))) return rc;
+  std::vector<int32_t> lf(N, 0), lb(N, 0);
+  int nf = 0, nb = 0;
+  for (int64_t s = 0; s < N; s++) {
+    const int32_t i = order[s];
+    int l = 0;
+    for (int64_t k = deg[i]; k < deg[i + 1]; k++)
+      if (pos[adj[k]] < s) l = std::max(l, lf[adj[k]] + 1);
+    lf[i] = l;
+    nf = std::max(nf, l + 1);
+  }
+  for (int64_t s = N - 1; s >= 0; s--) {
+    const int32_t i = order[s];
+    int l = 0;
+    for (int64_t k = deg[i]; k < deg[i + 1]; k++)
+      if (pos[adj[k]] > s) l = std::max(l, lb[adj[k]] + 1);
+    lb[i] = l;
+    nb = std::max(nb, l + 1);
+  }
+  std::vector<int32_t> fwd, bwd;
+  group_by(lf, nf, fwd, c->fwdOff);
+  group_by(lb, nb, bwd, c->bwdOff);
+  c->maxLevelWidth = 0;
+  for (int k = 0; k < nf; k++) c->maxLevelWidth = std::max(c->maxLevelWidth, c->fwdOff[k + 1] - c->fwdOff[k]);
+  for (int k = 0; k < nb; k++) c->maxLevelWidth = std::max(c->maxLevelWidth, c->bwdOff[k + 1] - c->bwdOff[k]);
+  for (int64_t** d : {&c->fwdOffDev, &c->bwdOffDev}) {
+    if (*d) {
+      auto it = std::find(c->allocs.begin(), c->allocs.end(), (void*)*d);
+      if (it != c->allocs.end()) c->allocs.erase(it);
+      cudaFree(*d);
+      *d = nullptr;
+    }
+  }
+  if ((rc = dalloc(c, c->fwdOffDev, sizeof(int64_t) * (nf + 1))) || (rc = dalloc(c, c->bwdOffDev, sizeof(int64_t) * (nb + 1))))
+    return rc;
+  DG_CUDA(c, cudaMemcpy(c->fwdOffDev, c->fwdOff.data(), sizeof(int64_t) * (nf + 1), cudaMemcpyHostToDevice));
+  DG_CUDA(c, cudaMemcpy(c->bwdOffDev, c->bwdOff.data(), sizeof(int64_t) * (nb + 1), cudaMemcpyHostToDevice));
+  c->lusgsOrder = 1;
+  return upload_schedule(c, pos, fwd, bwd);
 }
 
 template <class T>
 void launch_lusgs_sweep(dndsg_ctx* c, bool forward, double alpha, const double* rhs, double* inc, cudaStream_t s) {
   HotView<T> h = view<T>(c);
-  const int nc = (int)c->colourOff.size() - 1;
-  for (int q = 0; q < nc; q++) {
-    const int k = forward ? q : nc - 1 - q;
-    const int64_t b = c->colourOff[k], n = c->colourOff[k + 1] - b;
+  const std::vector<int64_t>& off = forward ? c->fwdOff : c->bwdOff;
+  const int32_t* cells = forward ? c->fwdCells : c->bwdCells;
+  const int nb = (int)off.size() - 1;
+  // many narrow levels: one block walks them all (a launch per level would cost more than the work)
+  if (c->lusgsOrder == 1 && c->maxLevelWidth <= 8 * kLevelBlock) {
+    const int64_t* od = forward ? c->fwdOffDev : c->bwdOffDev;
+    if (forward) k_lusgs_levels<T, true><<<1, kLevelBlock, 0, s>>>(h, c->rankOf, cells, od, nb, alpha, c->Dinv, rhs, inc);
+    else k_lusgs_levels<T, false><<<1, kLevelBlock, 0, s>>>(h, c->rankOf, cells, od, nb, alpha, c->Dinv, rhs, inc);
+    return;
+  }
+  for (int k = 0; k < nb; k++) {
+    const int64_t b = off[k], n = off[k + 1] - b;
     if (n == 0) continue;
     if (forward)
-      k_lusgs_colour<T, true><<<grid_for(n), kBlock, 0, s>>>(h, c->colourOf, c->colourCells + b, n, alpha, c->Dinv,
-                                                              rhs, inc);
+      k_lusgs_batch<T, true><<<grid_for(n), kBlock, 0, s>>>(h, c->rankOf, cells + b, n, alpha, c->Dinv, rhs, inc);
     else
-      k_lusgs_colour<T, false><<<grid_for(n), kBlock, 0, s>>>(h, c->colourOf, c->colourCells + b, n, alpha, c->Dinv,
-                                                               rhs, inc);
+      k_lusgs_batch<T, false><<<grid_for(n), kBlock, 0, s>>>(h, c->rankOf, cells + b, n, alpha, c->Dinv, rhs, inc);
   }
 }
 
@@ -1695,8 +1816,29 @@ int dndsg_lusgs_colours(dndsg_ctx* c, int32_t* colour_out, int* n_colours) {
   if (!c) return DNDSG_BAD_ARGUMENT;
   int rc;
   if ((rc = set_device(c)) || (rc = ensure_lusgs(c))) return rc;
-  if (colour_out) DG_CUDA(c, cudaMemcpy(colour_out, c->colourOf, sizeof(int32_t) * c->N, cudaMemcpyDeviceToHost));
-  if (n_colours) *n_colours = (int)c->colourOff.size() - 1;
+  if (colour_out) std::memcpy(colour_out, c->colourHost.data(), sizeof(int32_t) * c->N);
+  if (n_colours) *n_colours = 1 + *std::max_element(c->colourHost.begin(), c->colourHost.end());
+  return 0;
+}
+
+int dndsg_lusgs_set_order(dndsg_ctx* c, int mode, const int64_t* scan2cell, int* n_batches) {
+  if (!c || (mode != 0 && mode != 1)) return DNDSG_BAD_ARGUMENT;
+  int rc;
+  if ((rc = set_device(c)) || (rc = ensure_lusgs(c))) return rc;
+  if (mode == 1) {
+    if ((rc = set_scan_order(c, scan2cell))) return rc;
+  } else if (c->lusgsOrder != 0) {
+    const int64_t N = c->N;
+    const std::vector<int32_t>& col = c->colourHost;
+    const int ncol = 1 + *std::max_element(col.begin(), col.end());
+    std::vector<int32_t> fwd, bwd, rev(N);
+    group_by(col, ncol, fwd, c->fwdOff);
+    for (int64_t i = 0; i < N; i++) rev[i] = ncol - 1 - col[i];
+    group_by(rev, ncol, bwd, c->bwdOff);
+    c->lusgsOrder = 0;
+    if ((rc = upload_schedule(c, col, fwd, bwd))) return rc;
+  }
+  if (n_batches) *n_batches = (int)(c->fwdOff.size() - 1 + c->bwdOff.size() - 1);
   return 0;
 }
 
@@ -1711,7 +1853,7 @@ int dndsg_lusgs_matrix_init(dndsg_ctx* c, double dt_phys, double alpha, void* s)
 
 static int lusgs_sweep_api(dndsg_ctx* c, bool fwd, double alpha, const double* rhs, double* inc, void* s) {
   if (!c || !rhs || !inc) return DNDSG_BAD_ARGUMENT;
-  if (!c->colourOf) return fail(c, DNDSG_BAD_ARGUMENT, "dndsg_lusgs_matrix_init first");
+  if (!c->rankOf) return fail(c, DNDSG_BAD_ARGUMENT, "dndsg_lusgs_matrix_init first");
   int rc;
   if ((rc = set_device(c))) return rc;
   if (c->fp32) launch_lusgs_sweep<float>(c, fwd, alpha, rhs, inc, st(s));

@@ -161,6 +161,14 @@ class Solver:
         self._check(self.L.dndsg_lusgs_colours(self.h, _p(col), C.byref(n)))
         return col, n.value
 
+    def lusgs_set_order(self, mode: int = 0, scan2cell=None) -> int:
+        """LU-SGS schedule: 0 colour batches; 1 the sequential sweep in scan2cell (None: natural
+        cell order), level-scheduled.  Returns the forward plus backward batches per iteration."""
+        nb = C.c_int()
+        o = None if scan2cell is None else np.ascontiguousarray(scan2cell, dtype=np.int64)
+        self._check(self.L.dndsg_lusgs_set_order(self.h, int(mode), _p(o) if o is not None else None, C.byref(nb)))
+        return nb.value
+
     def LUSGSMatrixInit(self, dt: float = 1e100, alpha_diag: float = 1.0):
         """LUSGSMatrixInit (DNDS_FV_EulerEvaluator.cpp:995-1047) from the last EvaluateDt."""
         self._check(self.L.dndsg_lusgs_matrix_init(self.h, float(dt), float(alpha_diag), self.stream))

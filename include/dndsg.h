@@ -192,6 +192,15 @@ int dndsg_get_status(dndsg_ctx* ctx, uint32_t* flags, uint64_t* n_reduced, void*
  * ------------------------------------------------------------------------ */
 /* the colouring: colour_out [n_cells] (host, may be NULL), n_colours */
 int dndsg_lusgs_colours(dndsg_ctx* ctx, int32_t* colour_out, int* n_colours);
+/* the sweep schedule.  mode 0 (default): colour batches, the reference's sweep
+ * in the colour-sorted order (few batches; on meshes with strongly coupled
+ * cell lines, such as stretched boundary-layer cells, it converges more slowly
+ * than a line-following order).  mode 1: the reference's sequential sweep in
+ * the scan order scan2cell [n_cells] (host; NULL = natural cell order, the
+ * reference's SOR_iScan2iCell default), run as dependency levels (one batch
+ * per level) so that it computes what the sequential sweep computes.
+ * n_batches (may be NULL): forward plus backward batches per iteration. */
+int dndsg_lusgs_set_order(dndsg_ctx* ctx, int mode, const int64_t* scan2cell, int* n_batches);
 /* LUSGSMatrixInit (DNDS_FV_EulerEvaluator.cpp:995-1047): D_i = 1/dTau_i + 1/dt
  * + sum_f (alpha/2) lambda_f A_f / V_i with dTau = (the DNDSG_BUF_DT of the last
  * dndsg_eval_dt) / alpha, and lambda_f from that same call */
