@@ -57,6 +57,7 @@ struct dndsg_ctx {
   int32_t *rankOf = nullptr, *fwdCells = nullptr, *bwdCells = nullptr;
   std::vector<int64_t> fwdOff, bwdOff;
   int64_t *fwdOffDev = nullptr, *bwdOffDev = nullptr;  // level offsets on the device (scan-order mode)
+  int32_t *fwdNbF = nullptr, *fwdNbJ = nullptr, *bwdNbF = nullptr, *bwdNbJ = nullptr;  // [pos][4] records
   int64_t maxLevelWidth = 0;
   std::vector<int32_t> colourHost;  // greedy colouring, kept for dndsg_lusgs_colours
   int lusgsOrder = 0;               // 0 colour batches, 1 level-scheduled scan order
@@ -1575,6 +1576,105 @@ __global__ void __launch_bounds__(kBlock) k_lusgs_batch(HotView<T> h, const int3
   if (t < n) lusgs_cell<T, FWD>(h, rankOf, cells[t], alpha, Dinv, rhs, inc);
 }
 
+// the parts of one LU-SGS cell update that do not depend on the increments of earlier cells
+struct LusgsPre {
+  int64_t i;
+  bool use[4];  // slot k holds a neighbour that enters this sweep (static slot index: registers)
+  int32_t j[4];
+  double U[4][4], nx[4], ny[4], lam[4], w[4];
+  double base[4], di;
+};
+
+// everything of the cell at schedule position t that does not depend on this sweep's increments.
+// nbF / nbJ [t][4] hold, per face slot, the slot's face (cellFace encoding) and the neighbour when
+// that neighbour enters this sweep (-1 otherwise), so every load here is independent of the others
+template <class T, bool FWD>
+__device__ __forceinline__ void lusgs_prefetch(const HotView<T>& h, const int32_t* cells, const int32_t* nbF,
+                                               const int32_t* nbJ, int64_t t, double alpha, const double* Dinv,
+                                               const double* rhs, LusgsPre& p) {
+  const int64_t i = cells[t];
+  const int4 sf4 = reinterpret_cast<const int4*>(nbF)[t];
+  const int4 j4 = reinterpret_cast<const int4*>(nbJ)[t];
+  const int32_t sfa[4] = {sf4.x, sf4.y, sf4.z, sf4.w}, ja[4] = {j4.x, j4.y, j4.z, j4.w};
+  p.i = i;
+  if (FWD) load4<T>(&rhs[i * 4], p.base);
+  p.di = Dinv[i];
+  const double scale = -0.5 * alpha / h.vol[i];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const bool use = ja[k] >= 0;
+    const int32_t sf = sfa[k];
+    const int32_t f = use ? (sf >= 0 ? sf : ~sf) : 0;   // index 0 is a valid face: loads stay unconditional
+    const int64_t j = use ? ja[k] : i;
+    const double sg = sf >= 0 ? 1.0 : -1.0;
+    const double area = h.faceArea[f];
+    p.use[k] = use;
+    p.j[k] = (int32_t)j;
+    load4<T>(&h.u[j * 4], p.U[k]);
+    p.nx[k] = sg * h.faceNormal[2 * f];
+    p.ny[k] = sg * h.faceNormal[2 * f + 1];
+    p.lam[k] = h.lamA[f] / area;
+    p.w[k] = scale * area;
+  }
+}
+
+template <class T, bool FWD>
+__device__ __forceinline__ void lusgs_finish(const HotView<T>& h, const LusgsPre& p, double* inc) {
+  double buf[4];
+  for (int v = 0; v < 4; v++) buf[v] = FWD ? p.base[v] : 0.0;
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    if (!p.use[q]) continue;
+    double dU[4], dF[4];
+    load4<T>(&inc[(int64_t)p.j[q] * 4], dU);
+    flux_jac_times_du(p.U[q], p.nx[q], p.ny[q], dU, p.lam[q], h.gamma, dF);
+    for (int v = 0; v < 4; v++) buf[v] += p.w[q] * dF[v];
+  }
+  double* o = &inc[p.i * 4];
+  if (FWD) {
+    for (int v = 0; v < 4; v++) o[v] = p.di * buf[v];
+  } else {
+    for (int v = 0; v < 4; v++) o[v] += p.di * buf[v];
+  }
+}
+
+// a whole sweep of narrow dependency levels in one thread block, software-pipelined: before the
+// barrier that ends a level, each thread requests what its cell of the next level needs (all but
+// the neighbours' fresh increments), so after the barrier one dependent load per neighbour is
+// left.  Level offsets sit in shared memory.
+constexpr int kPipeBlock = 256, kPipeMaxLevels = 4095;
+template <class T, bool FWD>
+__global__ void __launch_bounds__(kPipeBlock) k_lusgs_levels_pipe(HotView<T> h, const int32_t* nbF,
+                                                                  const int32_t* nbJ, const int32_t* cells,
+                                                                  const int64_t* off,
+                                                                  int nlev, double alpha, const double* Dinv,
+                                                                  const double* rhs, double* inc) {
+  __shared__ int64_t so[kPipeMaxLevels + 1];
+  for (int l = threadIdx.x; l <= nlev; l += blockDim.x) so[l] = off[l];
+  __syncthreads();
+  LusgsPre p;
+  bool have = false;
+  if (nlev > 0 && so[0] + threadIdx.x < so[1]) {
+    lusgs_prefetch<T, FWD>(h, cells, nbF, nbJ, so[0] + threadIdx.x, alpha, Dinv, rhs, p);
+    have = true;
+  }
+  for (int l = 0; l < nlev; l++) {
+    if (have) lusgs_finish<T, FWD>(h, p, inc);
+    for (int64_t t = so[l] + threadIdx.x + blockDim.x; t < so[l + 1]; t += blockDim.x) {
+      LusgsPre q;
+      lusgs_prefetch<T, FWD>(h, cells, nbF, nbJ, t, alpha, Dinv, rhs, q);
+      lusgs_finish<T, FWD>(h, q, inc);
+    }
+    // the next level's static data, requested before the barrier
+    have = false;
+    if (l + 1 < nlev && so[l + 1] + threadIdx.x < so[l + 2]) {
+      lusgs_prefetch<T, FWD>(h, cells, nbF, nbJ, so[l + 1] + threadIdx.x, alpha, Dinv, rhs, p);
+      have = true;
+    }
+    __syncthreads();
+  }
+}
+
 // a whole sweep of narrow batches (dependency levels) in one thread block: the levels run one
 // after another with a block barrier between them, which makes a level's increments visible to
 // the next; no grid-wide synchronisation and no waiting on flags
@@ -1755,6 +1855,39 @@ int set_scan_order(dndsg_ctx* c, const int64_t* scan2cell) {
     return rc;
   DG_CUDA(c, cudaMemcpy(c->fwdOffDev, c->fwdOff.data(), sizeof(int64_t) * (nf + 1), cudaMemcpyHostToDevice));
   DG_CUDA(c, cudaMemcpy(c->bwdOffDev, c->bwdOff.data(), sizeof(int64_t) * (nb + 1), cudaMemcpyHostToDevice));
+  // per schedule position: the face slots and the neighbours that enter each sweep
+  std::vector<int32_t> slots((size_t)aos_size(N, c->nfmax)), L(c->F), R(c->F);
+  DG_CUDA(c, cudaMemcpy(slots.data(), c->cellFace, sizeof(int32_t) * slots.size(), cudaMemcpyDeviceToHost));
+  DG_CUDA(c, cudaMemcpy(L.data(), c->faceL, sizeof(int32_t) * c->F, cudaMemcpyDeviceToHost));
+  DG_CUDA(c, cudaMemcpy(R.data(), c->faceR, sizeof(int32_t) * c->F, cudaMemcpyDeviceToHost));
+  auto records = [&](const std::vector<int32_t>& cellsOf, bool forward, std::vector<int32_t>& nf,
+                     std::vector<int32_t>& nj) {
+    nf.assign(4 * N, kEmptySlot);
+    nj.assign(4 * N, -1);
+    for (int64_t t = 0; t < N; t++) {
+      const int64_t i = cellsOf[t];
+      for (int k = 0; k < c->nfmax && k < 4; k++) {
+        const int32_t sf = slots[aos(i, k, c->nfmax)];
+        nf[4 * t + k] = sf;
+        if (sf == kEmptySlot) continue;
+        const int32_t f = sf >= 0 ? sf : ~sf;
+        const int32_t j = sf >= 0 ? R[f] : L[f];
+        if (j < 0) continue;
+        if (forward ? pos[j] < pos[i] : pos[j] > pos[i]) nj[4 * t + k] = j;
+      }
+    }
+  };
+  std::vector<int32_t> ff, fj, bf, bj;
+  records(fwd, true, ff, fj);
+  records(bwd, false, bf, bj);
+  if (!c->fwdNbF)
+    if ((rc = dalloc(c, c->fwdNbF, sizeof(int32_t) * 4 * N)) || (rc = dalloc(c, c->fwdNbJ, sizeof(int32_t) * 4 * N)) ||
+        (rc = dalloc(c, c->bwdNbF, sizeof(int32_t) * 4 * N)) || (rc = dalloc(c, c->bwdNbJ, sizeof(int32_t) * 4 * N)))
+      return rc;
+  DG_CUDA(c, cudaMemcpy(c->fwdNbF, ff.data(), sizeof(int32_t) * 4 * N, cudaMemcpyHostToDevice));
+  DG_CUDA(c, cudaMemcpy(c->fwdNbJ, fj.data(), sizeof(int32_t) * 4 * N, cudaMemcpyHostToDevice));
+  DG_CUDA(c, cudaMemcpy(c->bwdNbF, bf.data(), sizeof(int32_t) * 4 * N, cudaMemcpyHostToDevice));
+  DG_CUDA(c, cudaMemcpy(c->bwdNbJ, bj.data(), sizeof(int32_t) * 4 * N, cudaMemcpyHostToDevice));
   c->lusgsOrder = 1;
   return upload_schedule(c, pos, fwd, bwd);
 }
@@ -1766,6 +1899,16 @@ void launch_lusgs_sweep(dndsg_ctx* c, bool forward, double alpha, const double* 
   const int32_t* cells = forward ? c->fwdCells : c->bwdCells;
   const int nb = (int)off.size() - 1;
   // many narrow levels: one block walks them all (a launch per level would cost more than the work)
+  if (c->lusgsOrder == 1 && nb <= kPipeMaxLevels && c->maxLevelWidth <= 8 * kPipeBlock && c->nfmax <= 4) {
+    const int64_t* od = forward ? c->fwdOffDev : c->bwdOffDev;
+    if (forward)
+      k_lusgs_levels_pipe<T, true><<<1, kPipeBlock, 0, s>>>(h, c->fwdNbF, c->fwdNbJ, cells, od, nb, alpha, c->Dinv,
+                                                            rhs, inc);
+    else
+      k_lusgs_levels_pipe<T, false><<<1, kPipeBlock, 0, s>>>(h, c->bwdNbF, c->bwdNbJ, cells, od, nb, alpha, c->Dinv,
+                                                             rhs, inc);
+    return;
+  }
   if (c->lusgsOrder == 1 && c->maxLevelWidth <= 8 * kLevelBlock) {
     const int64_t* od = forward ? c->fwdOffDev : c->bwdOffDev;
     if (forward) k_lusgs_levels<T, true><<<1, kLevelBlock, 0, s>>>(h, c->rankOf, cells, od, nb, alpha, c->Dinv, rhs, inc);
