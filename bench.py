@@ -192,6 +192,136 @@ def run_reference(args):
     print(json.dumps(out))
 
 
+def steady_leg(dev, iters=1000, log=None):
+    """The implicit steady path on the 512 x 128 NACA 0012 C-mesh (first spacing 1e-6 chord, far field
+    20 chords), inviscid, M 0.15, alpha 10 deg, CFL 100, LU-SGS in the reference's natural scan order
+    and in wall-normal line order (both level-scheduled) and in colour batches (which, at this CFL on
+    these stretched cells, does not converge): ms per pseudo-time iteration (CUDA events), the increment
+    residual after `iters` iterations, and CL / CD from the wall force.  Timed outside the headline."""
+    import math
+
+    import torch
+
+    from dnds_b200 import mesh as M
+    from dnds_b200 import settings as S
+    from dnds_b200.solver import Solver
+
+    m = M.naca0012_cmesh(wall_bc=M.BC_WALL_EULER)
+    cfg = S.preset("naca0012")
+    u0 = np.tile(np.array(cfg["eulerSetting"]["farFieldStaticValue"]), (m.n_cells, 1))
+    a = math.radians(10.0)
+    out = {"workload": "NACA 0012 C-mesh 512x128 (65,536 quads), Euler wall, M 0.15, alpha 10, CFL 100, BDF1 pseudo time",
+           "cells": m.n_cells}
+    lines = M.line_scan_order(m)
+    for prec, name in ((0, "fp64"), (1, "fp32")):
+        for mode, mname, scan in ((1, "natural_order", None), (1, "line_order", lines), (0, "colour_batches", None)):
+            s = Solver(m, cfg, device=dev, precision=prec)
+            nb = s.lusgs_set_order(mode, scan)
+            s.set_u(u0)
+            s.bdf_begin()
+            for _ in range(5):
+                s.implicit_iteration(100.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            k = 50
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(k):
+                s._check(s.L.dndsg_implicit_iteration(s.h, 100.0, 1e100, 1.0, 1, 0, 0.0, None, None, s.stream))
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / k
+            r = {"batches_per_iteration": nb, "ms_per_iteration": ms, "cell_iterations_per_s": m.n_cells / (ms * 1e-3)}
+            if mode == 1:
+                s.set_u(u0)
+                hist = []
+                t0 = time.perf_counter()
+                it, rel, wf = s.steady_solve(100.0, 1e-8, iters, history=hist)
+                r["iterations"] = it
+                r["wall_s"] = time.perf_counter() - t0
+                r["rel_residual_rho"] = float(rel[0])
+                q = 0.5
+                r["CL"] = float((-wf[1] * math.sin(a) + wf[2] * math.cos(a)) / q)
+                r["CD"] = float((wf[1] * math.cos(a) + wf[2] * math.sin(a)) / q)
+            out[f"{name}_{mname}"] = r
+            s.close()
+            if log:
+                log(name, mname, r)
+    # the oracle's sequential sweep on the host cores, a bounded sample of iterations
+    try:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle
+
+        pyoracle.build()
+        o = pyoracle.Oracle(m, cfg, n_threads=0)
+        o.set_u(u0)
+        o.implicit_iteration(100.0, u0)
+        t0 = time.perf_counter()
+        n = 10
+        for _ in range(n):
+            o.implicit_iteration(100.0, u0)
+        dt = (time.perf_counter() - t0) / n
+        out["cpu_oracle"] = {"ms_per_iteration": dt * 1e3, "cores": os.cpu_count(), "kind": "port",
+                             "sample": "10 pseudo-time iterations, natural order"}
+    except Exception as e:  # the CPU figure is a side report
+        out["cpu_oracle"] = {"error": str(e)[:200]}
+    return out
+
+
+def learned_leg(dev, grid, tol=1e-7, log=None):
+    """The learned VR warm start: harvest on two 256 x 256 x 2 vortex meshes, train on the GPU,
+    then Jacobi sweeps per SSP-RK3 step to the same rms-increment tolerance, with and without the
+    network, on a fresh seed of the headline mesh.  Timed outside the headline."""
+    import torch
+
+    from dnds_b200 import geometry as G
+    from dnds_b200 import mesh as M
+    from dnds_b200 import settings as S
+    from dnds_b200.learned import WarmStartNet, harvest, train
+    from dnds_b200.solver import Solver
+
+    cfg = S.preset("vortex")
+    Xs, Ts = [], []
+    t0 = time.perf_counter()
+    for seed in (11, 12):
+        m = M.vortex_mesh(256, True, jitter=0.2, seed=seed)
+        s = Solver(m, cfg, device=dev, precision=1)
+        s.set_u(G.isentropic_vortex(m))
+        s.vr_to_tolerance(tol, 2000)
+        X, T, _ = harvest(s, 8, 0.5, tol, 2000)
+        Xs.append(X)
+        Ts.append(T)
+        s.close()
+    X, T = torch.cat(Xs), torch.cat(Ts)
+    torch.cuda.synchronize()
+    t_harvest = time.perf_counter() - t0
+    net = WarmStartNet(dev, seed=7)
+    t0 = time.perf_counter()
+    _, val = train(net, X, T, epochs=20)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    out = {"pairs": int(X.shape[0]), "harvest_s": t_harvest, "train_s": t_train,
+           "train_samples_per_s": 20 * X.shape[0] / t_train, "val_loss": val,
+           "target_mean_square": float((T ** 2).mean()), "tolerance_rms_increment": tol}
+    del X, T, Xs, Ts
+    m = M.vortex_mesh(grid, True, jitter=0.2, seed=9999)
+    for name, use in (("plain", None), ("learned", net)):
+        s = Solver(m, cfg, device=dev, precision=1)
+        s.set_u(G.isentropic_vortex(m))
+        s.vr_to_tolerance(tol, 2000)
+        s.ssprk3_step_tol(0.5, tol, 2000, use)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sw = [s.ssprk3_step_tol(0.5, tol, 2000, use) for _ in range(3)]
+        torch.cuda.synchronize()
+        out[name] = {"sweeps_per_step": sw, "ms_per_step": (time.perf_counter() - t0) / 3 * 1e3}
+        s.close()
+    out["sweeps_saved_per_step"] = float(np.mean(out["plain"]["sweeps_per_step"]) -
+                                         np.mean(out["learned"]["sweeps_per_step"]))
+    if log:
+        log(out)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -204,6 +334,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--grid", type=int, default=N_GRID, help="grid size n (n x n quads -> 2 n^2 triangles)")
     ap.add_argument("--precisions", default="fp32,fp64")
+    ap.add_argument("--no-steady", action="store_true", help="skip the implicit steady NACA 0012 report")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start report")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -356,6 +488,10 @@ def main():
                            "reference": "exact advected vortex (cell averages), density"}
     if rank == 0 and ws == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline()
+    if rank == 0 and ws == 1 and not args.no_steady:
+        out["steady_naca0012"] = steady_leg(dev)
+    if rank == 0 and ws == 1 and not args.no_learned:
+        out["learned_vr"] = learned_leg(dev, args.grid)
     if rank == 0:
         print(json.dumps(out))
     if ws > 1:

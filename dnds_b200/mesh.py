@@ -370,6 +370,20 @@ def naca0012_cmesh(n_airfoil: int = 256, n_wake: int = 128, nj: int = 128, first
     return _as_mesh(xy, cells, faces, f"naca0012_c{ni}x{nj}", meta)
 
 
+def line_scan_order(m: Mesh) -> np.ndarray:
+    """LU-SGS scan order for a C-mesh from naca0012_cmesh: the wall-normal grid lines, even ones
+    first, then odd ones, each from the wall outwards.  Like the natural cell order (which also runs
+    along the wall-normal lines fastest) it sweeps the strongly coupled stretched cells of a line in
+    sequence, but lines of one parity share no face (the wake cut pairs line i with line
+    2 n_wake + n_airfoil - 1 - i, of the other parity), so a level-scheduled sweep has 2 nj levels
+    instead of the natural order's ni + nj - 1."""
+    assert m.meta.get("kind") == "naca0012_cmesh", "line_scan_order needs a naca0012_cmesh"
+    nj = m.meta["nj"]
+    ni = m.n_cells // nj
+    idx = np.arange(ni * nj).reshape(ni, nj)
+    return np.concatenate([idx[0::2].ravel(), idx[1::2].ravel()]).astype(np.int64)
+
+
 def read_gmsh2(path: str) -> Mesh:
     """Gmsh 2.2 ASCII reader for 2-D meshes (SerialGmshReader2d, DNDS_Mesh.hpp:87-236).
 

@@ -69,6 +69,19 @@ def test_naca_cmesh_topology():
     assert 0.9e-4 < h < 1.5e-4
 
 
+def test_line_scan_order_is_a_permutation_with_independent_lines():
+    m = _naca_small()
+    scan = M.line_scan_order(m)
+    assert np.array_equal(np.sort(scan), np.arange(m.n_cells))
+    nj = m.meta["nj"]
+    line = np.arange(m.n_cells) // nj
+    L, R = m.face_cells[:, 0], m.face_cells[:, 1]
+    inner = R >= 0
+    cross = line[L[inner]] != line[R[inner]]
+    # faces between different lines always join lines of opposite parity
+    assert np.all((line[L[inner]][cross] - line[R[inner]][cross]) % 2 == 1)
+
+
 def test_oracle_free_stream_is_a_fixed_point(oracle_lib):
     m = M.vortex_mesh(8, True, jitter=0.2)
     cfg = S.preset("vortex")
@@ -224,6 +237,26 @@ def test_level_scheduled_natural_order_matches_sequential_oracle(oracle_lib):
     assert np.abs(inc.cpu().numpy() - nat).max() < 1e-12 * np.abs(nat).max()
     # back to colour batches
     assert s.lusgs_set_order(0) == 2 * s.lusgs_colours()[1]
+
+
+@pytest.mark.gpu
+def test_line_scan_order_matches_oracle(oracle_lib):
+    """A caller-given scan order (wall-normal lines, even then odd) runs as 2 nj levels and
+    computes what the oracle's sequential sweep in that order computes."""
+    m, cfg = _naca_small(), _cfg()
+    scan = M.line_scan_order(m)
+    u0 = _free_stream(m, cfg)
+    s = _gpu(m, cfg)
+    assert s.lusgs_set_order(1, scan) == 2 * 2 * 16
+    s.set_u(u0)
+    s.bdf_begin()
+    o = _oracle(oracle_lib, m, cfg)
+    o.set_u(u0)
+    for it in range(10):
+        s.implicit_iteration(100.0)
+        o.implicit_iteration(100.0, u0, scan2cell=scan)
+    ref = o.get_u()
+    assert np.abs(s.get_u() - ref).max() < 1e-10 * np.abs(ref).max()
 
 
 @pytest.mark.gpu
