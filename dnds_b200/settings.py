@@ -46,6 +46,11 @@ class Settings(C.Structure):
         ("far_field", C.c_double * 6),
         ("n_threads", C.c_int32),
         ("precision", C.c_int32),
+        ("mu_gas", C.c_double),
+        ("cp_gas", C.c_double),
+        ("pr_gas", C.c_double),
+        ("t_ref", C.c_double),
+        ("c_sutherland", C.c_double),
     ]
 
 
@@ -82,6 +87,14 @@ def make_settings(cfg: dict) -> Settings:
         s.far_field[k] = float(ff[k]) if k < len(ff) else 0.0
     s.n_threads = int(cfg.get("nThreads", 0))
     s.precision = int(cfg.get("precision", PRECISION_FP64))
+    # idealGasProperty defaults of EulerEvaluator::Setting (DNDS_FV_EulerEvaluator.hpp:150-160); without
+    # muGas the model is inviscid
+    rgas = float(gas.get("Rgas", 1.0))
+    s.mu_gas = float(gas.get("muGas", 0.0))
+    s.cp_gas = float(gas.get("CpGas", rgas * s.gamma / (s.gamma - 1)))
+    s.pr_gas = float(gas.get("prGas", 0.72))
+    s.t_ref = float(gas.get("TRef", 273.15))
+    s.c_sutherland = float(gas.get("CSutherland", 110.4))
     return s
 
 
@@ -179,10 +192,33 @@ NACA0012 = {
 }
 
 
+def laminar_gas(mach: float, reynolds: float, gamma: float = 1.4) -> dict:
+    """idealGasProperty for a laminar case with rho = 1, |V| = 1, chord 1 and Rgas = 1: the reference
+    temperature is the free-stream one (T = p / rho), Sutherland's constant scaled from 110.4 K at
+    288.15 K, and muGas = 1 / Re, so that the free-stream viscosity is 1 / Re."""
+    t_inf = 1.0 / (gamma * mach * mach)
+    return {"gamma": gamma, "Rgas": 1.0, "muGas": 1.0 / reynolds, "prGas": 0.72, "TRef": t_inf,
+            "CSutherland": 110.4 / 288.15 * t_inf}
+
+
+# the laminar NACA 0012 at M 0.5, Re 5000, alpha 0 (no-slip wall): the Navier-Stokes case of the
+# implicit path, with the NACA0012 vfvSetting
+NACA0012_LAMINAR = {
+    "recOrder": 2,
+    "vfvSetting": dict(NACA0012["vfvSetting"]),
+    "eulerSetting": {
+        "riemannSolverType": "Roe",
+        "idealGasProperty": laminar_gas(0.5, 5000.0),
+        "farFieldStaticValue": free_stream(0.5, 0.0),
+    },
+}
+
+
 def preset(name: str, **overrides) -> dict:
     import copy
 
-    base = {"vortex": ISENTROPIC_VORTEX, "riemann": RIEMANN_2D, "naca0012": NACA0012}[name]
+    base = {"vortex": ISENTROPIC_VORTEX, "riemann": RIEMANN_2D, "naca0012": NACA0012,
+            "naca0012_laminar": NACA0012_LAMINAR}[name]
     cfg = copy.deepcopy(base)
     for k, v in overrides.items():
         if isinstance(v, dict) and isinstance(cfg.get(k), dict):

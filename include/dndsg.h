@@ -82,6 +82,14 @@ typedef struct {
   double far_field[6];           /* farFieldStaticValue (conservative) */
   int32_t n_threads;             /* unused by the GPU path */
   int32_t precision;             /* 0 FP64 throughout, 1 FP32 bulk (FP64 means/norms) */
+  /* idealGasProperty (DNDS_FV_EulerEvaluator.hpp:150-160): mu_gas = 0 is the
+   * inviscid Euler model (the reference's Euler runs use 1e-200); mu_gas > 0
+   * adds the Navier-Stokes viscous flux with Sutherland's law */
+  double mu_gas;
+  double cp_gas;                 /* Rgas * gamma / (gamma - 1) */
+  double pr_gas;
+  double t_ref;
+  double c_sutherland;
 } dndsg_settings;
 
 typedef struct dndsg_ctx dndsg_ctx;

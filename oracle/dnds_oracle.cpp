@@ -1041,6 +1041,13 @@ void limiter_wbap(orc_ctx& c, bool ifAll, double* indicator_out) {
 }
 
 // ------------------------------------------------------------------ dt
+// Sutherland's law at the mean state (fluxFace, DNDS_FV_EulerEvaluator.hpp:405-412):
+// T = p / ((gamma - 1) / gamma * Cp * rho)
+double sutherland_mu(const orc_settings& s, double p, double rho) {
+  const double T = p / ((s.gamma - 1) / s.gamma * s.cp_gas * rho);
+  return s.mu_gas * std::pow(T / s.t_ref, 1.5) * (s.t_ref + s.c_sutherland) / (T + s.c_sutherland);
+}
+
 void eval_dt(orc_ctx& c, double cfl, double maxDt, bool useLocal, double* dtMinOut) {
   const int nv = c.nv;
   const double gamma = c.s.gamma;
@@ -1069,8 +1076,12 @@ void eval_dt(orc_ctx& c, double cfl, double maxDt, bool useLocal, double* dtMinO
       double pMean = (pL + pR) * 0.5;
       double aMean = std::sqrt(gamma * pMean / uMean[0]);
       double lamConv = std::fabs(vnMean) + aMean;
-      // viscous part: Euler model has mu = 0 here (reference runs use mu = 1e-200)
+      // viscous part (DNDS_FV_EulerEvaluator.cpp:80-99): muf at the mean state
       double lamVis = 0.0;
+      if (c.s.mu_gas > 0) {
+        const double muf = sutherland_mu(c.s, pMean, uMean[0]);
+        lamVis = muf / uMean[0] * std::max(4. / 3., gamma / c.s.pr_gas);
+      }
       double area = fg.area;
       c.lambdaFace[f] = lamConv + lamVis * area * (1. / c.cg[fg.L].vol + 1. / volR);
       c.deltaLambdaFace[f] = std::fabs((vR[0] - vL[0]) * un[0] + (vR[1] - vL[1]) * un[1]) +
@@ -1094,6 +1105,34 @@ void eval_dt(orc_ctx& c, double cfl, double maxDt, bool useLocal, double* dtMinO
 
 // ------------------------------------------------------------------ RHS
 // one face: fluxEs (3 columns: flux, FLfix, FRfix) integrated over the 3 GPs
+// Gas::ViscousFlux_IdealGas (DNDS_Gas.hpp:795-826) for dim 2, contracted with the unit normal:
+// Fn[k] = sum_i n_i Flux(i, k).  G[i][v] = d U_v / d x_i (conservative gradients).
+void viscous_flux_n(const double* U, const double G[2][4], const double* n, bool adiabatic, double gamma,
+                    double mu, double k, double cp, double* Fn) {
+  const double v[2] = {U[1] / U[0], U[2] / U[0]};
+  double S[2][2];  // strainRate(i, j) = d u_j / d x_i
+  for (int i = 0; i < 2; i++)
+    for (int j = 0; j < 2; j++) S[i][j] = (U[0] * G[i][1 + j] - G[i][0] * U[1 + j]) / (U[0] * U[0]);
+  double gradP[2], gradT[2];
+  for (int i = 0; i < 2; i++)
+    gradP[i] = (gamma - 1) * (G[i][3] - 0.5 * (G[i][1] * v[0] + G[i][2] * v[1] + S[i][0] * U[1] + S[i][1] * U[2]));
+  const double p = (gamma - 1) * (U[3] - U[0] * 0.5 * (v[0] * v[0] + v[1] * v[1]));
+  for (int i = 0; i < 2; i++) gradT[i] = gamma / ((gamma - 1) * cp * U[0] * U[0]) * (U[0] * gradP[i] - p * G[i][0]);
+  if (adiabatic) {
+    const double d = gradT[0] * n[0] + gradT[1] * n[1];
+    gradT[0] -= d * n[0];
+    gradT[1] -= d * n[1];
+  }
+  const double lambda = -2. / 3., tr = S[0][0] + S[1][1];
+  double F[2][4];
+  for (int i = 0; i < 2; i++) {
+    F[i][0] = 0;
+    for (int j = 0; j < 2; j++) F[i][1 + j] = (S[i][j] + S[j][i]) * mu + (i == j ? lambda * mu * tr : 0.0);
+    F[i][3] = F[i][1] * v[0] + F[i][2] * v[1] + k * gradT[i];
+  }
+  for (int q = 0; q < 4; q++) Fn[q] = n[0] * F[0][q] + n[1] * F[1][q];
+}
+
 void face_flux(const orc_ctx& c, int64_t f, double t, double fl[3][4], double* gpvals /*[3][2][4] or null*/,
                int* reduced) {
   const int nv = c.nv;
@@ -1151,6 +1190,37 @@ void face_flux(const orc_ctx& c, int64_t f, double t, double fl[3][4], double* g
     else roe_flux(UL, UR, gamma, F, c.deltaLambdaFace[f]);
     double a1 = F[1], a2 = F[2];
     F[1] = nb[0][0] * a1 + nb[0][1] * a2; F[2] = nb[1][0] * a1 + nb[1][1] * a2;
+    if (c.s.mu_gas > 0) {
+      // the viscous flux at the mean state with the face gradient of EvaluateRHS
+      // (DNDS_FV_EulerEvaluator.cpp:279-370): the mean of both sides' reconstructed gradients
+      // (the inner one's on a boundary) plus the jump (UR - UL) n / distGRP, distGRP =
+      // 2 min(V_L, V_R) / A, made effectively infinite at walls
+      double GL[2][4], GR[2][4], G[2][4];
+      for (int d = 0; d < 2; d++)
+        for (int v = 0; v < 4; v++) {
+          double sL = 0, sR = 0;
+          for (int q = 0; q < 5; q++) sL += fg.D[ig][0][1 + d][q + 1] * c.urec[(fg.L * 5 + q) * nv + v];
+          if (fg.R >= 0)
+            for (int q = 0; q < 5; q++) sR += fg.D[ig][1][1 + d][q + 1] * c.urec[(fg.R * 5 + q) * nv + v];
+          GL[d][v] = sL;
+          GR[d][v] = fg.R >= 0 ? sR : sL;
+        }
+      double minVol = c.cg[fg.L].vol;
+      if (fg.R >= 0) minVol = std::min(minVol, c.cg[fg.R].vol);
+      double distGRP = minVol / fg.area * 2;
+      if (fg.bc == kWallEuler || fg.bc == kWallNoSlip) distGRP += 3e200;
+      for (int d = 0; d < 2; d++)
+        for (int v = 0; v < 4; v++) G[d][v] = (GR[d][v] + GL[d][v]) * 0.5 + (1.0 / distGRP) * un[d] * (URxy[v] - ULxy[v]);
+      double Um[4];
+      for (int v = 0; v < 4; v++) Um[v] = 0.5 * (ULxy[v] + URxy[v]);
+      double pm, am, Hm;
+      thermal(Um[3], Um[0], sqr(Um[1] / Um[0]) + sqr(Um[2] / Um[0]), gamma, pm, am, Hm);
+      const double mu = sutherland_mu(c.s, pm, Um[0]);
+      const double kc = c.s.cp_gas * mu / c.s.pr_gas;
+      double Fv[4];
+      viscous_flux_n(Um, G, un, fg.bc == kWallNoSlip, gamma, mu, kc, c.s.cp_gas, Fv);
+      for (int k = 0; k < 4; k++) F[k] -= Fv[k];
+    }
     double w = nn * fg.wq[ig];
     for (int k = 0; k < 4; k++) {
       fl[0][k] += -F[k] * w;

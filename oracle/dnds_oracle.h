@@ -78,6 +78,14 @@ typedef struct {
   double far_field[6];
   int32_t n_threads;             /* 0 = hardware concurrency */
   int32_t pad0;
+  /* idealGasProperty (DNDS_FV_EulerEvaluator.hpp:150-160): mu_gas = 0 is the
+   * inviscid Euler model (the reference's Euler runs use 1e-200); mu_gas > 0
+   * adds the Navier-Stokes viscous flux with Sutherland's law */
+  double mu_gas;
+  double cp_gas;                 /* Rgas * gamma / (gamma - 1) */
+  double pr_gas;
+  double t_ref;
+  double c_sutherland;
 } orc_settings;
 
 typedef struct orc_ctx orc_ctx;

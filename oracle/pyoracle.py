@@ -56,6 +56,11 @@ class OrcSettings(C.Structure):
         ("far_field", C.c_double * 6),
         ("n_threads", C.c_int32),
         ("pad0", C.c_int32),
+        ("mu_gas", C.c_double),
+        ("cp_gas", C.c_double),
+        ("pr_gas", C.c_double),
+        ("t_ref", C.c_double),
+        ("c_sutherland", C.c_double),
     ]
 
 
