@@ -43,6 +43,7 @@ struct dndsg_ctx {
   int32_t *cellFace = nullptr, *vrNbr = nullptr, *vrMode = nullptr, *vrFace = nullptr;
   void* vrOp = nullptr;       // T
   void* faceBasis = nullptr;  // T
+  void* faceGrad = nullptr;   // T, viscous contexts only
   double* Ainv = nullptr;
   double *limFace = nullptr, *faceInd = nullptr, *indicator = nullptr;  // CWBAP limiter data
   int32_t* wallCells = nullptr;  // cells with a Wall_Euler / Wall_NoSlip face
@@ -128,6 +129,12 @@ __global__ void k_setup_face(MeshView m, SetupParams p, const CellSetup* cells, 
   int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (f >= m.F) return;
   setup_face<T>(f, m, p, cells, faceW, normal, area, center, w0, basis, nullptr);
+}
+
+template <class T>
+__global__ void k_setup_face_grad(MeshView m, const CellSetup* cells, T* grad) {
+  int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (f < m.F) setup_face_grad<T>(f, m, cells, grad);
 }
 
 template <class T>
@@ -323,6 +330,29 @@ __global__ void __launch_bounds__(kBlock, 2) k_face_flux(HotView<T> h, int64_t f
   }
 }
 
+// the same with the Navier-Stokes viscous term (contexts with mu_gas > 0)
+template <class T, int RIEMANN, bool BND>
+__global__ void __launch_bounds__(kBlock) k_face_flux_vis(HotView<T> h, int64_t f0, int64_t f1, const double* scal,
+                                                          int useDev, double tHost, double c, unsigned* flags,
+                                                          unsigned long long* nred) {
+  int64_t f = f0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int r = 0;
+  bool bad = false;
+  if (f < f1) {
+    double out[4];
+    r = face_flux_vis<T, RIEMANN, BND>(f, h, stage_time(scal, useDev, tHost, c), out, bad);
+    double* o = &h.flux[f * 4];
+    *reinterpret_cast<double2*>(o) = make_double2(out[0], out[1]);
+    *reinterpret_cast<double2*>(o + 2) = make_double2(out[2], out[3]);
+  }
+  unsigned anyBad = __ballot_sync(0xffffffffu, bad);
+  int rs = __reduce_add_sync(0xffffffffu, r);
+  if ((threadIdx.x & 31) == 0) {
+    if (anyBad) atomicOr(flags, 1u);
+    if (rs) atomicAdd(nred, (unsigned long long)rs);
+  }
+}
+
 template <class T>
 __global__ void k_face_values(HotView<T> h, double t, double* out) {
   int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -472,6 +502,8 @@ HotView<T> view(dndsg_ctx* c) {
   h.gamma = c->s.gamma;
   for (int k = 0; k < 4; k++) h.farU[k] = c->s.far_field[k];
   h.relax = c->s.jacobi_relax;
+  h.faceGrad = (const T*)c->faceGrad;
+  h.mu = c->s.mu_gas; h.cp = c->s.cp_gas; h.pr = c->s.pr_gas; h.tRef = c->s.t_ref; h.cSuth = c->s.c_sutherland;
   return h;
 }
 
@@ -527,6 +559,20 @@ template <class T>
 void launch_flux(dndsg_ctx* c, int useDev, double tHost, double cst, cudaStream_t s) {
   HotView<T> h = view<T>(c);
   const int64_t Fi = c->Fi, F = c->F;
+  if (c->s.mu_gas > 0) {
+    if (c->s.riemann == 2) {
+      if (Fi > 0)
+        k_face_flux_vis<T, 2, false><<<grid_for(Fi), kBlock, 0, s>>>(h, 0, Fi, c->scal, useDev, tHost, cst, c->flags, c->nreduced);
+      if (F > Fi)
+        k_face_flux_vis<T, 2, true><<<grid_for(F - Fi), kBlock, 0, s>>>(h, Fi, F, c->scal, useDev, tHost, cst, c->flags, c->nreduced);
+    } else {
+      if (Fi > 0)
+        k_face_flux_vis<T, 1, false><<<grid_for(Fi), kBlock, 0, s>>>(h, 0, Fi, c->scal, useDev, tHost, cst, c->flags, c->nreduced);
+      if (F > Fi)
+        k_face_flux_vis<T, 1, true><<<grid_for(F - Fi), kBlock, 0, s>>>(h, Fi, F, c->scal, useDev, tHost, cst, c->flags, c->nreduced);
+    }
+    return;
+  }
   if (c->s.riemann == 2) {
     if (Fi > 0)
       k_face_flux<T, 2, false><<<grid_for(Fi), kBlock, 0, s>>>(h, 0, Fi, c->scal, useDev, tHost, cst, c->flags, c->nreduced);
@@ -681,6 +727,11 @@ int setup_run(dndsg_ctx* c, const dndsg_mesh_desc* md) {
   k_setup_face<T><<<grid_for(F), kBlock>>>(m, p, cells, faceW, c->faceNormal, c->faceArea, c->faceCenter, c->faceW0,
                                            (T*)c->faceBasis);
   if ((rc = check_launch(c))) return rc;
+  if (c->s.mu_gas > 0) {
+    if ((rc = dalloc(c, c->faceGrad, sizeof(T) * aos_size(F, 60)))) return rc;
+    k_setup_face_grad<T><<<grid_for(F), kBlock>>>(m, cells, (T*)c->faceGrad);
+    if ((rc = check_launch(c))) return rc;
+  }
   // ---- VR matrices
   if ((rc = dalloc(c, c->cellFace, sizeof(int32_t) * slots.size()))) return rc;
   DG_CUDA(c, cudaMemcpy(c->cellFace, slots.data(), sizeof(int32_t) * slots.size(), cudaMemcpyHostToDevice));
@@ -1074,6 +1125,8 @@ void run_rhs_noalloc(dndsg_ctx* c, const double* u, const void* urec, double* rh
 
 extern "C" int dndsg_eval_rhs_noalloc(dndsg_ctx* c, const double* u, const void* urec, double* rhs, double t,
                                       void* s) {
+  if (c && c->s.mu_gas > 0)
+    return fail(c, DNDSG_UNSUPPORTED, "the allocation-free RHS covers the inviscid model only (mu_gas = 0)");
   if (!c || !u || !urec || !rhs) return DNDSG_BAD_ARGUMENT;
   if (c->F > kNoAllocMaxFaces)
     return fail(c, DNDSG_BAD_ARGUMENT,

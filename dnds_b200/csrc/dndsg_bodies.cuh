@@ -268,6 +268,10 @@ struct HotView {
   double gamma;
   double farU[4];
   double relax;
+  // Navier-Stokes (mu > 0): gradient rows of both cells' basis at the face gauss points,
+  // AoSoA E = 60: [side][gp][d/dx, d/dy][5], and the gas properties
+  const T* faceGrad;
+  double mu, cp, pr, tRef, cSuth;
 };
 
 template <class T>
@@ -505,6 +509,109 @@ DG_HD int face_flux(int64_t f, const HotView<T>& h, double t, double out[4], boo
   return nred;
 }
 
+// Sutherland's law at a state (fluxFace, DNDS_FV_EulerEvaluator.hpp:405-412): T = p / ((gamma-1)/gamma Cp rho)
+template <class T>
+DG_HD double sutherland_mu(const HotView<T>& h, double p, double rho) {
+  const double Tm = p / ((h.gamma - 1) / h.gamma * h.cp * rho);
+  return h.mu * pow(Tm / h.tRef, 1.5) * (h.tRef + h.cSuth) / (Tm + h.cSuth);
+}
+
+// Gas::ViscousFlux_IdealGas (DNDS_Gas.hpp:795-826), 2-D, contracted with the unit normal;
+// G[i][v] = d U_v / d x_i of the conservative variables
+DG_HD void viscous_flux_n(const double U[4], const double G[2][4], double nx, double ny, bool adiabatic,
+                          double gamma, double mu, double k, double cp, double Fn[4]) {
+  const double ir = 1.0 / U[0];
+  const double v0 = U[1] * ir, v1 = U[2] * ir;
+  double S[2][2];  // d u_j / d x_i
+  for (int i = 0; i < 2; i++)
+    for (int j = 0; j < 2; j++) S[i][j] = (U[0] * G[i][1 + j] - G[i][0] * U[1 + j]) * ir * ir;
+  const double p = (gamma - 1) * (U[3] - U[0] * 0.5 * (v0 * v0 + v1 * v1));
+  double gT[2];
+  for (int i = 0; i < 2; i++) {
+    const double gP = (gamma - 1) * (G[i][3] - 0.5 * (G[i][1] * v0 + G[i][2] * v1 + S[i][0] * U[1] + S[i][1] * U[2]));
+    gT[i] = gamma / ((gamma - 1) * cp * U[0] * U[0]) * (U[0] * gP - p * G[i][0]);
+  }
+  if (adiabatic) {
+    const double d = gT[0] * nx + gT[1] * ny;
+    gT[0] -= d * nx;
+    gT[1] -= d * ny;
+  }
+  const double tr = S[0][0] + S[1][1];
+  const double txx = 2 * S[0][0] * mu - 2.0 / 3.0 * mu * tr, tyy = 2 * S[1][1] * mu - 2.0 / 3.0 * mu * tr;
+  const double txy = (S[0][1] + S[1][0]) * mu;
+  Fn[0] = 0;
+  Fn[1] = nx * txx + ny * txy;
+  Fn[2] = nx * txy + ny * tyy;
+  Fn[3] = nx * (txx * v0 + txy * v1 + k * gT[0]) + ny * (txy * v0 + tyy * v1 + k * gT[1]);
+}
+
+// reconstructed gradient of cell `cell` (side 0 = left, 1 = right) at gauss point g of face f
+template <class T>
+DG_HD void face_grad(int64_t f, int side, int g, int64_t cell, const HotView<T>& h, double G[2][4]) {
+  const T* rc = &h.urec[cell * 20];
+  for (int d = 0; d < 2; d++) {
+    for (int v = 0; v < 4; v++) G[d][v] = 0.0;
+    for (int q = 0; q < 5; q++) {
+      const double b = (double)h.faceGrad[aos(f, ((side * 3 + g) * 2 + d) * 5 + q, 60)];
+      for (int v = 0; v < 4; v++) G[d][v] += b * (double)rc[4 * q + v];
+    }
+  }
+}
+
+// face flux with the Navier-Stokes viscous term (fluxFace, DNDS_FV_EulerEvaluator.hpp:371-591, and
+// the face gradient of EvaluateRHS, DNDS_FV_EulerEvaluator.cpp:279-370): the mean of both sides'
+// reconstructed gradients (the inner one's on a boundary face) plus (UR - UL) n / distGRP with
+// distGRP = 2 min(V_L, V_R) / A, no jump term at walls; viscous flux at the mean state, Sutherland
+// viscosity, k = Cp mu / Pr, adiabatic at a no-slip wall
+template <class T, int RIEMANN, bool BND>
+DG_HD int face_flux_vis(int64_t f, const HotView<T>& h, double t, double out[4], bool& bad) {
+  const int32_t L = h.faceL[f], R = h.faceR[f];
+  const double nx = h.faceNormal[2 * f], ny = h.faceNormal[2 * f + 1], area = h.faceArea[f];
+  double uL[4], uR[4] = {0, 0, 0, 0};
+  load4<T>(&h.u[(int64_t)L * 4], uL);
+  const bool inner = !BND || R >= 0;
+  if (inner) load4<T>(&h.u[(int64_t)R * 4], uR);
+  const int bc = BND ? h.faceBC[f] : BC_INNER;
+  const bool wall = bc == BC_WALL_EULER || bc == BC_WALL_NOSLIP;
+  double minVol = h.vol[L];
+  if (inner) minVol = dmin(minVol, h.vol[R]);
+  const double invD = wall ? 0.0 : area / (2.0 * minVol);
+  const double dl = h.dLam[f];
+  T incL[3][4], incR[3][4];
+  face_increments(f, L, R, h, incL, incR);
+  int nred = 0;
+  double acc[4] = {0, 0, 0, 0};
+  for (int g = 0; g < 3; g++) {
+    double UL[4], UR[4], a[4], b[4], F[4];
+    nred += gp_states<T, BND>(f, R, h, t, nx, ny, uL, uR, incL[g], incR[g], UL, UR);
+    to_normal_frame(UL, nx, ny, a);
+    to_normal_frame(UR, nx, ny, b);
+    if (!(a[0] > 0 && b[0] > 0)) bad = true;
+    if (RIEMANN == 2) hllc_flux(a, b, h.gamma, F);
+    else roe_flux(a, b, h.gamma, dl, F);
+    from_normal_frame(F, nx, ny);
+    double GL[2][4], GR[2][4], G[2][4], Um[4], Fv[4];
+    face_grad(f, 0, g, L, h, GL);
+    if (inner) face_grad(f, 1, g, R, h, GR);
+    for (int v = 0; v < 4; v++) {
+      const double jump = invD * (UR[v] - UL[v]);
+      G[0][v] = 0.5 * (GL[0][v] + (inner ? GR[0][v] : GL[0][v])) + jump * nx;
+      G[1][v] = 0.5 * (GL[1][v] + (inner ? GR[1][v] : GL[1][v])) + jump * ny;
+      Um[v] = 0.5 * (UL[v] + UR[v]);
+    }
+    const double pm = (h.gamma - 1) * (Um[3] - 0.5 * (Um[1] * Um[1] + Um[2] * Um[2]) / Um[0]);
+    const double mu = sutherland_mu(h, pm, Um[0]);
+    viscous_flux_n(Um, G, nx, ny, bc == BC_WALL_NOSLIP, h.gamma, mu, h.cp * mu / h.pr, h.cp, Fv);
+    const double jw = 0.5 * area * l3_weight(g);
+    for (int k = 0; k < 4; k++) acc[k] -= (F[k] - Fv[k]) * jw;
+  }
+  for (int k = 0; k < 4; k++) {
+    if (!(acc[k] == acc[k])) bad = true;
+    out[k] = acc[k];
+  }
+  return nred;
+}
+
 // F(U0 + d) - F(U0) of the normal-frame Euler flux, evaluated from the
 // increments so that FP32 rounding scales with |d|, not with |F|
 DG_HD void flux_delta_f32(const float U[4], const float d[4], float gamma, float D[4]) {
@@ -647,6 +754,10 @@ DG_HD void dt_face(int64_t f, const HotView<T>& h) {
   double vn = 0.5 * ((uL + uR) * nx + (vL + vR) * ny);
   double pMean = (pL + pR) * 0.5;
   double lam = fabs(vn) + sqrt(h.gamma * pMean / rhoMean);
+  if (h.mu > 0) {  // viscous part (DNDS_FV_EulerEvaluator.cpp:80-99)
+    const double lamVis = sutherland_mu(h, pMean, rhoMean) / rhoMean * dmax(4. / 3., h.gamma / h.pr);
+    lam += lamVis * area * (1.0 / h.vol[L] + 1.0 / (R >= 0 ? h.vol[R] : h.vol[L]));
+  }
   h.lamA[f] = lam * area;
   h.dLam[f] = fabs((uR - uL) * nx + (vR - vL) * ny) + sqrt(fabs(aR2 - aL2)) * 0.7071;
 }
@@ -696,6 +807,23 @@ namespace dg {
 // ---------------------------------------------------------------- setup bodies
 // face part of initBaseDiffCache (DNDS_FV_VR.cpp:367-890): weights, geometry
 // and the value-row basis of both cells at the face gauss points
+// gradient rows (d/dx, d/dy) of both cells' basis at the face gauss points, for the viscous flux
+template <class T>
+DG_HD void setup_face_grad(int64_t f, const MeshView& m, const CellSetup* cells, T* grad) {
+  const FaceGeom g = face_geom(f, m);
+  const int32_t L = m.face_cells[2 * f], R = m.face_cells[2 * f + 1];
+  const double sx = m.face_shift ? m.face_shift[2 * f] : 0.0, sy = m.face_shift ? m.face_shift[2 * f + 1] : 0.0;
+  for (int side = 0; side < 2; side++)
+    for (int q = 0; q < 3; q++) {
+      double D[6][5];
+      if (side == 0) p2_diffs(cells[L].fr, g.gx[q], g.gy[q], D);
+      else if (R >= 0) p2_diffs(cells[R].fr, g.gx[q] - sx, g.gy[q] - sy, D);
+      else for (int r = 0; r < 6; r++) for (int k = 0; k < 5; k++) D[r][k] = 0;
+      for (int d = 0; d < 2; d++)
+        for (int k = 0; k < 5; k++) grad[aos(f, ((side * 3 + q) * 2 + d) * 5 + k, 60)] = (T)D[1 + d][k];
+    }
+}
+
 template <class T>
 DG_HD void setup_face(int64_t f, const MeshView& m, const SetupParams& p, const CellSetup* cells, double* faceW,
                       double* normal, double* area, double* center, double* w0, T* basis, double* basisD) {
