@@ -375,8 +375,8 @@ def line_scan_order(m: Mesh) -> np.ndarray:
     first, then odd ones, each from the wall outwards.  Like the natural cell order (which also runs
     along the wall-normal lines fastest) it sweeps the strongly coupled stretched cells of a line in
     sequence, but lines of one parity share no face (the wake cut pairs line i with line
-    2 n_wake + n_airfoil - 1 - i, of the other parity), so a level-scheduled sweep has 2 nj levels
-    instead of the natural order's ni + nj - 1."""
+    2 n_wake + n_airfoil - 1 - i, of the other parity), so a level-scheduled sweep has nj + 1 levels
+    (the odd lines run one level behind the even ones) instead of the natural order's ni + nj - 1."""
     assert m.meta.get("kind") == "naca0012_cmesh", "line_scan_order needs a naca0012_cmesh"
     nj = m.meta["nj"]
     ni = m.n_cells // nj

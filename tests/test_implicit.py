@@ -241,13 +241,14 @@ def test_level_scheduled_natural_order_matches_sequential_oracle(oracle_lib):
 
 @pytest.mark.gpu
 def test_line_scan_order_matches_oracle(oracle_lib):
-    """A caller-given scan order (wall-normal lines, even then odd) runs as 2 nj levels and
-    computes what the oracle's sequential sweep in that order computes."""
+    """A caller-given scan order (wall-normal lines, even then odd) runs as nj + 1 levels per
+    sweep (the odd lines follow the even ones one level behind) and computes what the oracle's
+    sequential sweep in that order computes."""
     m, cfg = _naca_small(), _cfg()
     scan = M.line_scan_order(m)
     u0 = _free_stream(m, cfg)
     s = _gpu(m, cfg)
-    assert s.lusgs_set_order(1, scan) == 2 * 2 * 16
+    assert s.lusgs_set_order(1, scan) == 2 * (16 + 1)
     s.set_u(u0)
     s.bdf_begin()
     o = _oracle(oracle_lib, m, cfg)
