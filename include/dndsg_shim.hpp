@@ -6,6 +6,11 @@
 //   EulerEvaluatorGPU::EvaluateDt                       EulerEvaluator, DNDS_FV_EulerEvaluator.hpp:1408-1411
 //   EulerEvaluatorGPU::EvaluateRHS                      DNDS_FV_EulerEvaluator.hpp:1412-1418
 //   EulerEvaluatorGPU::EvaluateResidual                 DNDS_FV_EulerEvaluator.hpp:1455-1461
+//   EulerEvaluatorGPU::LUSGSMatrixInit                  DNDS_FV_EulerEvaluator.cpp:995-1047
+//   EulerEvaluatorGPU::UpdateLUSGSForward / Backward    DNDS_FV_EulerEvaluator.cpp:1149-1357
+//   ImplicitSteadyGPU::Step                             ImplicitBDFDualTimeStep::Step (order 1) with the
+//                                                       EulerSolver lambdas, DNDS_ODE.hpp:444-486 and
+//                                                       DNDS_FV_EulerSolver.hpp:713-994
 //
 // The reference's ArrayDOFV / ArrayRecV live in host memory and are passed to
 // every call; here the state is resident on the GPU, and the shim moves it
@@ -103,6 +108,49 @@ class EulerEvaluatorGPU {
   void EvaluateResidual(std::vector<double>& res, int P = 1, bool volWise = false, void* stream = nullptr) {
     res.resize(4);
     c_.check(dndsg_residual(c_.get(), P, volWise ? 1 : 0, res.data(), stream));
+  }
+  // the diagonal from the dTau of the last EvaluateDt (called with UseLocaldt) divided by alphaDiag
+  void LUSGSMatrixInit(double dt, double alphaDiag, void* stream = nullptr) {
+    c_.check(dndsg_lusgs_matrix_init(c_.get(), dt, alphaDiag, stream));
+  }
+  // rhs / uInc are device arrays [nCells][nVars]; uInc is updated in place (uInc == uIncNew in the reference)
+  void UpdateLUSGSForward(double alphaDiag, const double* rhs, double* uInc, void* stream = nullptr) {
+    c_.check(dndsg_lusgs_forward(c_.get(), alphaDiag, rhs, uInc, stream));
+  }
+  void UpdateLUSGSBackward(double alphaDiag, const double* rhs, double* uInc, void* stream = nullptr) {
+    c_.check(dndsg_lusgs_backward(c_.get(), alphaDiag, rhs, uInc, stream));
+  }
+  // sweep order: mode 0 colour batches, 1 the sequential order scan2cell (nullptr: natural), level-scheduled
+  int SetLUSGSOrder(int mode, const int64_t* scan2cell = nullptr) {
+    int nb = 0;
+    c_.check(dndsg_lusgs_set_order(c_.get(), mode, scan2cell, &nb));
+    return nb;
+  }
+
+ private:
+  Context& c_;
+};
+
+// the steady path: pseudo-time iterations of a first-order BDF step until the density increment,
+// relative to its largest value so far, drops below rhsThresholdInternal (fstop)
+class ImplicitSteadyGPU {
+ public:
+  explicit ImplicitSteadyGPU(Context& c) : c_(c) {}
+  // returns the iterations taken; wallFlux (may be null) receives fluxWallSum of the last iteration
+  int Step(double CFL, double rhsThresholdInternal, int nTimeStepInternal, double dtImplicit = 1e100,
+           int nInternalRecStep = 1, bool useVolWiseResidual = false, std::vector<double>* wallFlux = nullptr,
+           void* stream = nullptr) {
+    c_.check(dndsg_bdf_begin(c_.get(), stream));
+    double base = 0, res[4], wf[4];
+    int iter = 1;
+    for (; iter <= nTimeStepInternal; iter++) {
+      c_.check(dndsg_implicit_iteration(c_.get(), CFL, dtImplicit, 1.0, nInternalRecStep, useVolWiseResidual ? 1 : 0,
+                                        0.0, res, wf, stream));
+      base = iter == 1 ? res[0] : (res[0] > base ? res[0] : base);
+      if (res[0] < rhsThresholdInternal * base) break;
+    }
+    if (wallFlux) wallFlux->assign(wf, wf + 4);
+    return iter > nTimeStepInternal ? nTimeStepInternal : iter;
   }
 
  private:
