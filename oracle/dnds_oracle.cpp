@@ -7,6 +7,7 @@
 #include "dnds_oracle.h"
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <cmath>
 #include <cstring>
@@ -142,7 +143,9 @@ struct orc_ctx {
   std::vector<double> u, urec, urecNew, urec1;
   std::vector<double> dtFace, lambdaFace, deltaLambdaFace, lambdaCell;
   std::vector<double> dtCell;
-  std::vector<double> Dinv;  // LU-SGS diagonal inverse (scalar per cell: NS_2D has no source term)
+  std::vector<double> Dinv;      // LU-SGS diagonal inverse [N][nv] (diagonal per variable)
+  std::vector<double> dWall;     // SA: wall distance per cell (first-order, from the cell barycentre)
+  std::vector<double> srcJac;    // SA: jacobianCellSourceDiag [N][nv] of the last RHS
   double lastInc = 0;
   std::string err;
 };
@@ -419,10 +422,14 @@ void vortex_state(double x, double y, double xc, double yc, double gamma, bool t
 }
 
 // EulerEvaluator::generateBoundaryValue (DNDS_FV_EulerEvaluator.hpp:958-1275)
-// for the 2-D Euler model; un = unit normal, pc = face centre
-void boundary_value(const orc_ctx& c, const double* UL, const double* un, const double* pc, double t,
-                    int bc, double* UR) {
+// for the 2-D Euler model and, with c.nv = 5, the SA variable (a passive scalar: its primitive is
+// U5 / rho, DNDS_Gas.hpp:82-107); un = unit normal, pc = face centre.  fixUL: at a no-slip wall the
+// SA variable of both states is set to zero, UL included (USE_FIX_ZERO_SA_NUT_AT_WALL)
+void boundary_value(const orc_ctx& c, double* UL, const double* un, const double* pc, double t,
+                    int bc, double* UR, bool fixUL = false) {
   const double gamma = c.s.gamma;
+  const int nv = c.nv;
+  for (int k = 4; k < nv; k++) UR[k] = UL[k];
   if (bc == kFar) {
     const double* far = c.s.far_field;
     double vn = (UL[1] * un[0] + UL[2] * un[1]) / UL[0];
@@ -430,7 +437,7 @@ void boundary_value(const orc_ctx& c, const double* UL, const double* un, const 
     double p, a2, H;
     thermal(UL[3], UL[0], vs, gamma, p, a2, H);
     double a = std::sqrt(a2);
-    if (vn - a > 0) { for (int k = 0; k < 4; k++) UR[k] = UL[k]; }
+    if (vn - a > 0) { for (int k = 0; k < nv; k++) UR[k] = UL[k]; }
     else if (vn > 0) {
       double fp[4], lp[4];
       cons2prim(far, fp, gamma); cons2prim(UL, lp, gamma);
@@ -441,8 +448,9 @@ void boundary_value(const orc_ctx& c, const double* UL, const double* un, const 
       cons2prim(far, fp, gamma); cons2prim(UL, lp, gamma);
       fp[3] = lp[3];
       prim2cons(fp, UR, gamma);
+      for (int k = 4; k < nv; k++) UR[k] = far[k];  // far primitive U5/rho times the far density
     } else {
-      for (int k = 0; k < 4; k++) UR[k] = far[k];
+      for (int k = 0; k < nv; k++) UR[k] = far[k];
     }
   } else if (bc == kIVFar) {
     vortex_state(pc[0], pc[1], 5 + t, 5 + t, gamma, false, UR);
@@ -474,18 +482,22 @@ void boundary_value(const orc_ctx& c, const double* UL, const double* un, const 
     UR[1] -= d * un[0]; UR[2] -= d * un[1];
   } else if (bc == kWallNoSlip) {
     UR[0] = UL[0]; UR[1] = -UL[1]; UR[2] = -UL[2]; UR[3] = UL[3];
+    if (nv > 4) {
+      UR[4] = -UL[4];
+      if (fixUL) UL[4] = UR[4] = 0;
+    }
   } else {
     for (int k = 0; k < 4; k++) UR[k] = std::nan("");
   }
 }
 
 // EulerEvaluator::CompressRecPart (DNDS_FV_EulerEvaluator.hpp:1277-1360)
-inline void compress_rec_part(const double* umean, const double* inc, double* ret, bool& compressed) {
-  for (int k = 0; k < 4; k++) ret[k] = umean[k] + inc[k];
-  if (ret[0] < 0) { for (int k = 0; k < 4; k++) ret[k] = umean[k]; compressed = true; }
+inline void compress_rec_part(const double* umean, const double* inc, double* ret, bool& compressed, int nv = 4) {
+  for (int k = 0; k < nv; k++) ret[k] = umean[k] + inc[k];
+  if (ret[0] < 0) { for (int k = 0; k < nv; k++) ret[k] = umean[k]; compressed = true; }
   double eK = (ret[1] * ret[1] + ret[2] * ret[2]) * 0.5 / (kVerySmall + ret[0]);
   double e = ret[3] - eK;
-  if (e < 0) { for (int k = 0; k < 4; k++) ret[k] = umean[k]; compressed = true; }
+  if (e < 0) { for (int k = 0; k < nv; k++) ret[k] = umean[k]; compressed = true; }
 }
 
 // ------------------------------------------------------------------ setup
@@ -826,7 +838,7 @@ void cell_vr_update(orc_ctx& c, int64_t i, const double* src, double* dst) {
           double d = un[0] * uBV[1] + un[1] * uBV[2];
           uBV[1] = uBL[1] - un[0] * d; uBV[2] = uBL[2] - un[1] * d;
         } else {
-          boundary_value(c, uBL, un, f.gp[ig], 0.0, f.bc, uBV);
+          boundary_value(c, uBL, un, f.gp[ig], 0.0, f.bc, uBV, true);
         }
         double w0 = f.weights[0];
         for (int r = 0; r < 5; r++)
@@ -1048,6 +1060,17 @@ double sutherland_mu(const orc_settings& s, double p, double rho) {
   return s.mu_gas * std::pow(T / s.t_ref, 1.5) * (s.t_ref + s.c_sutherland) / (T + s.c_sutherland);
 }
 
+// SA eddy-viscosity factor of fluxFace / EvaluateDt (DNDS_FV_EulerEvaluator.hpp:413-425,
+// USE_NS_SA_NEGATIVE_MODEL): muf = mu (1 + Chi fnu1), Chi = U5 muRef / mu softened below 10
+double sa_mu_factor(const orc_settings& s, double U5, double mufPhy) {
+  const double cnu1 = 7.1;
+  double Chi = U5 * s.mu_gas / mufPhy;
+  if (Chi < 10) Chi = 0.05 * std::log(1 + std::exp(20 * Chi));
+  const double Chi3 = Chi * Chi * Chi;
+  const double fnu1 = Chi3 / (Chi3 + cnu1 * cnu1 * cnu1);
+  return std::max(1 + Chi * fnu1, 1.0);
+}
+
 void eval_dt(orc_ctx& c, double cfl, double maxDt, bool useLocal, double* dtMinOut) {
   const int nv = c.nv;
   const double gamma = c.s.gamma;
@@ -1058,8 +1081,8 @@ void eval_dt(orc_ctx& c, double cfl, double maxDt, bool useLocal, double* dtMinO
       double nn = std::sqrt(sqr(fg.ncenter[0]) + sqr(fg.ncenter[1]));
       double un[2] = {fg.ncenter[0] / nn, fg.ncenter[1] / nn};
       const double* UL = &c.u[fg.L * nv];
-      double uMean[4];
-      for (int k = 0; k < 4; k++) uMean[k] = UL[k];
+      double uMean[kMaxV];
+      for (int k = 0; k < nv; k++) uMean[k] = UL[k];
       double vL[2] = {UL[1] / UL[0], UL[2] / UL[0]}, vR[2] = {vL[0], vL[1]};
       double pL, aL2, HL, pR, aR2, HR;
       thermal(UL[3], UL[0], vL[0] * vL[0] + vL[1] * vL[1], gamma, pL, aL2, HL);
@@ -1067,7 +1090,7 @@ void eval_dt(orc_ctx& c, double cfl, double maxDt, bool useLocal, double* dtMinO
       double volR = c.cg[fg.L].vol;
       if (fg.R >= 0) {
         const double* UR = &c.u[fg.R * nv];
-        for (int k = 0; k < 4; k++) uMean[k] = (uMean[k] + UR[k]) * 0.5;
+        for (int k = 0; k < nv; k++) uMean[k] = (uMean[k] + UR[k]) * 0.5;
         vR[0] = UR[1] / UR[0]; vR[1] = UR[2] / UR[0];
         thermal(UR[3], UR[0], vR[0] * vR[0] + vR[1] * vR[1], gamma, pR, aR2, HR);
         volR = c.cg[fg.R].vol;
@@ -1079,7 +1102,8 @@ void eval_dt(orc_ctx& c, double cfl, double maxDt, bool useLocal, double* dtMinO
       // viscous part (DNDS_FV_EulerEvaluator.cpp:80-99): muf at the mean state
       double lamVis = 0.0;
       if (c.s.mu_gas > 0) {
-        const double muf = sutherland_mu(c.s, pMean, uMean[0]);
+        double muf = sutherland_mu(c.s, pMean, uMean[0]);
+        if (nv > 4) muf *= sa_mu_factor(c.s, uMean[4], muf);
         lamVis = muf / uMean[0] * std::max(4. / 3., gamma / c.s.pr_gas);
       }
       double area = fg.area;
@@ -1104,7 +1128,6 @@ void eval_dt(orc_ctx& c, double cfl, double maxDt, bool useLocal, double* dtMinO
 }
 
 // ------------------------------------------------------------------ RHS
-// one face: fluxEs (3 columns: flux, FLfix, FRfix) integrated over the 3 GPs
 // Gas::ViscousFlux_IdealGas (DNDS_Gas.hpp:795-826) for dim 2, contracted with the unit normal:
 // Fn[k] = sum_i n_i Flux(i, k).  G[i][v] = d U_v / d x_i (conservative gradients).
 void viscous_flux_n(const double* U, const double G[2][4], const double* n, bool adiabatic, double gamma,
@@ -1133,46 +1156,50 @@ void viscous_flux_n(const double* U, const double G[2][4], const double* n, bool
   for (int q = 0; q < 4; q++) Fn[q] = n[0] * F[0][q] + n[1] * F[1][q];
 }
 
-void face_flux(const orc_ctx& c, int64_t f, double t, double fl[3][4], double* gpvals /*[3][2][4] or null*/,
+// one face: fluxEs (3 columns: flux, FLfix, FRfix) integrated over the 3 GPs
+// (EvaluateRHS face loop, DNDS_FV_EulerEvaluator.cpp:215-514, and fluxFace,
+// DNDS_FV_EulerEvaluator.hpp:371-591); nv = 4 (NS_2D) or 5 (SA, the last variable rho nu~ / muRef)
+void face_flux(const orc_ctx& c, int64_t f, double t, double fl[3][kMaxV], double* gpvals /*[3][2][nv] or null*/,
                int* reduced) {
   const int nv = c.nv;
   const FaceGeo& fg = c.fg[f];
   const double gamma = c.s.gamma;
-  for (int a = 0; a < 3; a++) for (int k = 0; k < 4; k++) fl[a][k] = 0;
+  for (int a = 0; a < 3; a++) for (int k = 0; k < kMaxV; k++) fl[a][k] = 0;
   const double* uL = &c.u[fg.L * nv];
   const double* uR = fg.R >= 0 ? &c.u[fg.R * nv] : nullptr;
   for (int ig = 0; ig < 3; ig++) {
     double nn = std::sqrt(sqr(fg.n[ig][0]) + sqr(fg.n[ig][1]));
     double un[2] = {fg.n[ig][0] / nn, fg.n[ig][1] / nn};
-    double inc[4], ULxy[4], URxy[4], ULm[4], URm[4];
+    double inc[kMaxV], ULxy[kMaxV], URxy[kMaxV], ULm[kMaxV], URm[kMaxV];
     bool redL = false, redR = false;
-    for (int v = 0; v < 4; v++) {
+    for (int v = 0; v < nv; v++) {
       double s = 0;
       for (int q = 0; q < 5; q++) s += fg.D[ig][0][0][q + 1] * c.urec[(fg.L * 5 + q) * nv + v];
       inc[v] = s;
     }
-    compress_rec_part(uL, inc, ULxy, redL);
-    for (int v = 0; v < 4; v++) ULm[v] = uL[v];
+    compress_rec_part(uL, inc, ULxy, redL, nv);
+    for (int v = 0; v < nv; v++) ULm[v] = uL[v];
     if (fg.R >= 0) {
-      for (int v = 0; v < 4; v++) {
+      for (int v = 0; v < nv; v++) {
         double s = 0;
         for (int q = 0; q < 5; q++) s += fg.D[ig][1][0][q + 1] * c.urec[(fg.R * 5 + q) * nv + v];
         inc[v] = s;
       }
-      compress_rec_part(uR, inc, URxy, redR);
-      for (int v = 0; v < 4; v++) URm[v] = uR[v];
+      compress_rec_part(uR, inc, URxy, redR, nv);
+      for (int v = 0; v < nv; v++) URm[v] = uR[v];
     } else {
-      boundary_value(c, ULxy, un, fg.center, t, fg.bc, URxy);
-      boundary_value(c, ULm, un, fg.center, t, fg.bc, URm);
+      boundary_value(c, ULxy, un, fg.center, t, fg.bc, URxy, true);
+      boundary_value(c, ULm, un, fg.center, t, fg.bc, URm, false);
     }
     if (reduced) *reduced += int(redL) + int(redR);
     if (gpvals)
-      for (int v = 0; v < 4; v++) { gpvals[(ig * 2 + 0) * 4 + v] = ULxy[v]; gpvals[(ig * 2 + 1) * 4 + v] = URxy[v]; }
-    // fluxFace (DNDS_FV_EulerEvaluator.hpp:371-591), Euler part
+      for (int v = 0; v < nv; v++) { gpvals[(ig * 2 + 0) * nv + v] = ULxy[v]; gpvals[(ig * 2 + 1) * nv + v] = URxy[v]; }
+    // fluxFace (DNDS_FV_EulerEvaluator.hpp:371-591)
     double nb[2][2] = {{un[0], -un[1]}, {un[1], un[0]}};
-    double UL[4] = {ULxy[0], nb[0][0] * ULxy[1] + nb[1][0] * ULxy[2], nb[0][1] * ULxy[1] + nb[1][1] * ULxy[2], ULxy[3]};
-    double UR[4] = {URxy[0], nb[0][0] * URxy[1] + nb[1][0] * URxy[2], nb[0][1] * URxy[1] + nb[1][1] * URxy[2], URxy[3]};
-    double FLf[4], FRf[4];
+    double UL[kMaxV] = {ULxy[0], nb[0][0] * ULxy[1] + nb[1][0] * ULxy[2], nb[0][1] * ULxy[1] + nb[1][1] * ULxy[2], ULxy[3]};
+    double UR[kMaxV] = {URxy[0], nb[0][0] * URxy[1] + nb[1][0] * URxy[2], nb[0][1] * URxy[1] + nb[1][1] * URxy[2], URxy[3]};
+    for (int v = 4; v < nv; v++) { UL[v] = ULxy[v]; UR[v] = URxy[v]; }
+    double FLf[kMaxV] = {0}, FRf[kMaxV] = {0};
     {
       double Lm[4] = {ULm[0], nb[0][0] * ULm[1] + nb[1][0] * ULm[2], nb[0][1] * ULm[1] + nb[1][1] * ULm[2], ULm[3]};
       double Rm[4] = {URm[0], nb[0][0] * URm[1] + nb[1][0] * URm[2], nb[0][1] * URm[1] + nb[1][1] * URm[2], URm[3]};
@@ -1184,10 +1211,23 @@ void face_flux(const orc_ctx& c, int64_t f, double t, double fl[3][4], double* g
       FLf[1] = nb[0][0] * a1 + nb[0][1] * a2; FLf[2] = nb[1][0] * a1 + nb[1][1] * a2;
       a1 = FRf[1]; a2 = FRf[2];
       FRf[1] = nb[0][0] * a1 + nb[0][1] * a2; FRf[2] = nb[1][0] * a1 + nb[1][1] * a2;
+      if (nv > 4) { FLf[4] = wL[1] * ULm[4]; FRf[4] = wR[1] * URm[4]; }  // F_5 = rhoNut * un
     }
-    double F[4];
+    double F[kMaxV] = {0};
     if (c.s.riemann == 2) hllc_flux(UL, UR, gamma, F);
     else roe_flux(UL, UR, gamma, F, c.deltaLambdaFace[f]);
+    if (nv > 4) {
+      // the SA variable: central flux with upwinding by the contact wave, |Roe normal velocity|
+      // (Roe) or |mean normal velocity| (HLLC) (DNDS_FV_EulerEvaluator.hpp:540-553)
+      double lam123;
+      if (c.s.riemann == 2) {
+        lam123 = std::fabs(UL[1] / UL[0] + UR[1] / UR[0]) * 0.5;
+      } else {
+        double sL = std::sqrt(UL[0]), sR = std::sqrt(UR[0]);
+        lam123 = std::fabs((sL * UL[1] / UL[0] + sR * UR[1] / UR[0]) / (sL + sR));
+      }
+      F[4] = ((UL[1] / UL[0] * UL[4] + UR[1] / UR[0] * UR[4]) - (UR[4] - UL[4]) * lam123) * 0.5;
+    }
     double a1 = F[1], a2 = F[2];
     F[1] = nb[0][0] * a1 + nb[0][1] * a2; F[2] = nb[1][0] * a1 + nb[1][1] * a2;
     if (c.s.mu_gas > 0) {
@@ -1195,9 +1235,9 @@ void face_flux(const orc_ctx& c, int64_t f, double t, double fl[3][4], double* g
       // (DNDS_FV_EulerEvaluator.cpp:279-370): the mean of both sides' reconstructed gradients
       // (the inner one's on a boundary) plus the jump (UR - UL) n / distGRP, distGRP =
       // 2 min(V_L, V_R) / A, made effectively infinite at walls
-      double GL[2][4], GR[2][4], G[2][4];
+      double GL[2][kMaxV], GR[2][kMaxV], G[2][kMaxV];
       for (int d = 0; d < 2; d++)
-        for (int v = 0; v < 4; v++) {
+        for (int v = 0; v < nv; v++) {
           double sL = 0, sR = 0;
           for (int q = 0; q < 5; q++) sL += fg.D[ig][0][1 + d][q + 1] * c.urec[(fg.L * 5 + q) * nv + v];
           if (fg.R >= 0)
@@ -1210,19 +1250,38 @@ void face_flux(const orc_ctx& c, int64_t f, double t, double fl[3][4], double* g
       double distGRP = minVol / fg.area * 2;
       if (fg.bc == kWallEuler || fg.bc == kWallNoSlip) distGRP += 3e200;
       for (int d = 0; d < 2; d++)
-        for (int v = 0; v < 4; v++) G[d][v] = (GR[d][v] + GL[d][v]) * 0.5 + (1.0 / distGRP) * un[d] * (URxy[v] - ULxy[v]);
-      double Um[4];
-      for (int v = 0; v < 4; v++) Um[v] = 0.5 * (ULxy[v] + URxy[v]);
+        for (int v = 0; v < nv; v++) G[d][v] = (GR[d][v] + GL[d][v]) * 0.5 + (1.0 / distGRP) * un[d] * (URxy[v] - ULxy[v]);
+      double Um[kMaxV];
+      for (int v = 0; v < nv; v++) Um[v] = 0.5 * (ULxy[v] + URxy[v]);
       double pm, am, Hm;
       thermal(Um[3], Um[0], sqr(Um[1] / Um[0]) + sqr(Um[2] / Um[0]), gamma, pm, am, Hm);
-      const double mu = sutherland_mu(c.s, pm, Um[0]);
-      const double kc = c.s.cp_gas * mu / c.s.pr_gas;
+      const double mufPhy = sutherland_mu(c.s, pm, Um[0]);
+      double muf = mufPhy;
+      if (nv > 4) muf *= sa_mu_factor(c.s, Um[4], mufPhy);
+      const double kc = c.s.cp_gas * (muf - mufPhy) / 0.9 + c.s.cp_gas * mufPhy / c.s.pr_gas;
+      double Gf[2][4];
+      for (int d = 0; d < 2; d++) for (int v = 0; v < 4; v++) Gf[d][v] = G[d][v];
       double Fv[4];
-      viscous_flux_n(Um, G, un, fg.bc == kWallNoSlip, gamma, mu, kc, c.s.cp_gas, Fv);
+      viscous_flux_n(Um, Gf, un, fg.bc == kWallNoSlip, gamma, muf, kc, c.s.cp_gas, Fv);
       for (int k = 0; k < 4; k++) F[k] -= Fv[k];
+      if (nv > 4) {
+        // the SA diffusion (DNDS_FV_EulerEvaluator.hpp:463-480)
+        const double muRef = c.s.mu_gas, sigma = 2. / 3., cn1 = 16;
+        double fn = 1;
+        if (Um[4] < 0) {
+          const double Chi = Um[4] * muRef / mufPhy;
+          fn = (cn1 + Chi * Chi * Chi) / (cn1 - Chi * Chi * Chi);
+        }
+        double dn = 0;
+        for (int d = 0; d < 2; d++) {
+          const double diffNu = (G[d][4] * muRef - Um[4] * muRef / Um[0] * G[d][0]) / Um[0];
+          dn += un[d] * diffNu * (mufPhy + Um[4] * muRef * fn) / sigma / muRef;
+        }
+        F[4] -= dn;
+      }
     }
     double w = nn * fg.wq[ig];
-    for (int k = 0; k < 4; k++) {
+    for (int k = 0; k < nv; k++) {
       fl[0][k] += -F[k] * w;
       fl[1][k] += FLf[k] * w;
       fl[2][k] += FRf[k] * w;
@@ -1230,41 +1289,162 @@ void face_flux(const orc_ctx& c, int64_t f, double t, double fl[3][4], double* g
   }
 }
 
+// EulerEvaluator::source and sourceJacobianDiag for NS_SA (DNDS_FV_EulerEvaluator.hpp:593-864,
+// USE_NS_SA_NEGATIVE_MODEL): the SA-neg production, destruction and cb2 diffusion of the
+// last variable at one point; U is the (compressed) reconstructed state, G[d][v] its gradient
+void sa_source(const orc_ctx& c, const double* U, const double G[2][kMaxV], double dWall, double& src,
+               double& jac) {
+  const double d = std::min(dWall, std::pow(3e200, 1. / 6.));
+  const double cb1 = 0.1355, cb2 = 0.622, sigma = 2. / 3., cnu1 = 7.1, cnu2 = 0.7, cnu3 = 0.9, cw2 = 0.3, cw3 = 2,
+               kappa = 0.41, rlim = 10, ct3 = 1.2, ct4 = 0.5;
+  const double cw1 = cb1 / sqr(kappa) + (1 + cb2) / sigma;
+  const double gamma = c.s.gamma;
+  double p, a2, H;
+  thermal(U[3], U[0], sqr(U[1] / U[0]) + sqr(U[2] / U[0]), gamma, p, a2, H);
+  const double muRef = c.s.mu_gas;
+  const double nuh = U[4] * muRef / U[0];
+  const double mufPhy = sutherland_mu(c.s, p, U[0]);
+  const double Chi = U[4] * muRef / mufPhy;
+  const double fnu1 = std::pow(Chi, 3) / (std::pow(Chi, 3) + std::pow(cnu1, 3));
+  const double fnu2 = 1 - Chi / (1 + Chi * fnu1);
+  const double velo[2] = {U[1] / U[0], U[2] / U[0]};
+  double diffNu[2], diffRho[2], diffU[2][2];
+  for (int i = 0; i < 2; i++) {
+    diffRho[i] = G[i][0];
+    diffNu[i] = (G[i][4] * muRef - nuh * G[i][0]) / U[0];
+    for (int j = 0; j < 2; j++) diffU[i][j] = (G[i][1 + j] - G[i][0] * velo[j]) / U[0];
+  }
+  // Omega = (diffU^T - diffU) / 2, S = |Omega|_F sqrt(2)
+  const double w01 = 0.5 * (diffU[1][0] - diffU[0][1]);
+  const double S = std::sqrt(2 * w01 * w01) * std::sqrt(2.0);
+  const double Sbar = nuh / (sqr(kappa) * sqr(d)) * fnu2;
+  double Sh;
+  if (Sbar < -cnu2 * S) Sh = S + S * (sqr(cnu2) * S + cnu3 * Sbar) / ((cnu3 - 2 * cnu2) * S - Sbar);
+  else Sh = S + Sbar;
+  const double r = std::min(nuh / (Sh * sqr(kappa * d) + kVerySmall), rlim);
+  const double g = r + cw2 * (std::pow(r, 6) - r);
+  const double fw = g * std::pow((1 + std::pow(cw3, 6)) / (std::pow(g, 6) + std::pow(cw3, 6)), 1. / 6.);
+  const double ft2 = ct3 * std::exp(-ct4 * sqr(Chi));
+  double D = (cw1 * fw - cb1 / sqr(kappa) * ft2) * sqr(nuh / d);
+  double P = cb1 * (1 - ft2) * Sh * nuh;
+  double fn = 1;
+  if (U[4] < 0) {
+    const double cn1 = 16;
+    fn = (cn1 + std::pow(Chi, 3)) / (cn1 - std::pow(Chi, 3));
+    P = cb1 * (1 - ct3) * S * nuh;
+    D = -cw1 * sqr(nuh / d);
+  }
+  const double dn2 = diffNu[0] * diffNu[0] + diffNu[1] * diffNu[1];
+  const double rn = diffRho[0] * diffNu[0] + diffRho[1] * diffNu[1];
+  src = U[0] * (P - D + dn2 * cb2 / sigma) / muRef - (U[4] * fn * muRef + mufPhy) / (U[0] * sigma) * rn / muRef;
+  jac = -std::min(U[0] * (P * 0 - D * 2) / muRef / (U[4] + kVerySmall), -kVerySmall);
+}
+
 void eval_rhs(orc_ctx& c, double t, double* rhs, double* wallFlux, int* nreduced) {
   const int nv = c.nv;
-  std::vector<double> buf(c.F * 12);
+  const int FW = 3 * kMaxV;
+  std::vector<double> buf(c.F * FW);
   std::atomic<int> red{0};
   parallel_for(c.nthreads, c.F, [&](int64_t b, int64_t e) {
     int r = 0;
     for (int64_t f = b; f < e; f++) {
-      double fl[3][4];
+      double fl[3][kMaxV];
       face_flux(c, f, t, fl, nullptr, &r);
-      std::memcpy(&buf[f * 12], fl, sizeof(fl));
+      std::memcpy(&buf[f * FW], fl, sizeof(fl));
     }
     red += r;
   });
   for (int64_t k = 0; k < c.N * nv; k++) rhs[k] = 0;
-  double wf[4] = {0, 0, 0, 0};
+  double wf[kMaxV] = {0};
   // scatter in face order (DNDS_FV_EulerEvaluator.cpp:501-516)
   for (int64_t f = 0; f < c.F; f++) {
     const FaceGeo& fg = c.fg[f];
-    const double* fl = &buf[f * 12];
+    const double* fl = &buf[f * FW];
     double vL = c.cg[fg.L].vol;
-    for (int k = 0; k < 4; k++) rhs[fg.L * nv + k] += fl[k] / vL;
+    for (int k = 0; k < nv; k++) rhs[fg.L * nv + k] += fl[k] / vL;
     if (fg.R >= 0) {
       double vR = c.cg[fg.R].vol;
-      for (int k = 0; k < 4; k++) rhs[fg.R * nv + k] -= fl[k] / vR;
+      for (int k = 0; k < nv; k++) rhs[fg.R * nv + k] -= fl[k] / vR;
     }
-    for (int k = 0; k < 4; k++) rhs[fg.L * nv + k] -= fl[4 + k] / vL;
+    for (int k = 0; k < nv; k++) rhs[fg.L * nv + k] -= fl[kMaxV + k] / vL;
     if (fg.R >= 0) {
       double vR = c.cg[fg.R].vol;
-      for (int k = 0; k < 4; k++) rhs[fg.R * nv + k] += fl[8 + k] / vR;
+      for (int k = 0; k < nv; k++) rhs[fg.R * nv + k] += fl[2 * kMaxV + k] / vR;
     }
     if (fg.bc == kWallNoSlip || fg.bc == kWallEuler)
-      for (int k = 0; k < 4; k++) wf[k] -= fl[k];
+      for (int k = 0; k < nv; k++) wf[k] -= fl[k];
   }
-  if (wallFlux) for (int k = 0; k < 4; k++) wallFlux[k] = wf[k];
+  if (wallFlux) for (int k = 0; k < nv; k++) wallFlux[k] = wf[k];
   if (nreduced) *nreduced = red.load();
+  // cell source loop (DNDS_FV_EulerEvaluator.cpp:520-638): the SA source and its diagonal Jacobian
+  // integrated over the cell's quadrature with the reconstructed value and gradient
+  c.srcJac.assign(c.N * nv, 0.0);
+  if (nv < 5) return;
+  const Quad q3 = tri4(), q4 = quad9();
+  parallel_for(c.nthreads, c.N, [&](int64_t b, int64_t e) {
+    for (int64_t i = b; i < e; i++) {
+      const CellGeo& g = c.cg[i];
+      const Quad& q = g.nn == 3 ? q3 : q4;
+      double sv = 0, sj = 0;
+      for (int ig = 0; ig < q.n; ig++) {
+        double N[4], dN[2][4], x = 0, y = 0, J[2][2] = {{0, 0}, {0, 0}};
+        shape(g.nn, q.p[ig][0], q.p[ig][1], N, dN);
+        for (int k = 0; k < g.nn; k++) {
+          x += N[k] * g.xy[k][0]; y += N[k] * g.xy[k][1];
+          for (int d = 0; d < 2; d++) { J[d][0] += dN[d][k] * g.xy[k][0]; J[d][1] += dN[d][k] * g.xy[k][1]; }
+        }
+        const double wdet = q.w[ig] * (J[0][0] * J[1][1] - J[0][1] * J[1][0]);
+        double D[kND][kND];
+        diff_base_value(c, g, x, y, g.moment, D);
+        double inc[kMaxV], U[kMaxV], G[2][kMaxV];
+        for (int v = 0; v < nv; v++) {
+          double s0 = 0, s1 = 0, s2 = 0;
+          for (int r = 0; r < 5; r++) {
+            const double a = c.urec[(i * 5 + r) * nv + v];
+            s0 += D[0][r + 1] * a; s1 += D[1][r + 1] * a; s2 += D[2][r + 1] * a;
+          }
+          inc[v] = s0; G[0][v] = s1; G[1][v] = s2;
+        }
+        bool red2 = false;
+        compress_rec_part(&c.u[i * nv], inc, U, red2, nv);
+        double src, jac;
+        sa_source(c, U, G, c.dWall[i], src, jac);
+        sv += src * wdet;
+        sj += jac * wdet;
+      }
+      rhs[i * nv + 4] += sv / g.vol;
+      c.srcJac[i * nv + 4] = sj / g.vol;
+    }
+  });
+}
+
+// first-order wall distance (USE_FIRST_ORDER_WALL_DIST, DNDS_FV_EulerEvaluator.hpp:227-363): from
+// each cell's barycentre to the nearest Wall_NoSlip face segment
+void wall_distance(orc_ctx& c, const orc_mesh& m) {
+  std::vector<std::array<double, 4>> seg;
+  for (int64_t f = 0; f < c.F; f++)
+    if (c.fg[f].bc == kWallNoSlip) {
+      const int a = m.face_nodes[2 * f], b = m.face_nodes[2 * f + 1];
+      seg.push_back({m.node_xy[2 * a], m.node_xy[2 * a + 1], m.node_xy[2 * b], m.node_xy[2 * b + 1]});
+    }
+  c.dWall.assign(c.N, std::pow(3e200, 1. / 6.));
+  parallel_for(c.nthreads, c.N, [&](int64_t b, int64_t e) {
+    for (int64_t i = b; i < e; i++) {
+      const double px = c.cg[i].bary[0], py = c.cg[i].bary[1];
+      double best = std::pow(3e200, 1. / 6.);
+      for (const auto& sg : seg) {
+        const double ex = sg[2] - sg[0], ey = sg[3] - sg[1];
+        const double L2 = std::sqrt(ex * ex + ey * ey);
+        const double bx = px - sg[0], by = py - sg[1];
+        const double LB = (bx * ex + by * ey) / L2;
+        double d;
+        if (LB >= 0 && LB <= L2) d = std::sqrt(sqr(bx - LB * ex / L2) + sqr(by - LB * ey / L2));
+        else d = std::min(std::sqrt(bx * bx + by * by), std::sqrt(sqr(px - sg[2]) + sqr(py - sg[3])));
+        best = std::min(best, d);
+      }
+      c.dWall[i] = best;
+    }
+  });
 }
 
 // ------------------------------------------------------------------ implicit path
@@ -1272,7 +1452,8 @@ void eval_rhs(orc_ctx& c, double t, double* rhs, double* wallFlux, int* nreduced
 // the inviscid flux increment of dU about U through the unit normal n
 // (Gas::IdealGasUIncrement, GasInviscidFluxFacialIncrement, DNDS_Gas.hpp:122-146),
 // minus lambdaMain * dU
-void flux_jac_times_du(const double* U, const double* n, const double* dU, double lam, double gamma, double* dF) {
+void flux_jac_times_du(const double* U, const double* n, const double* dU, double lam, double gamma, double* dF,
+                       int nv = 4) {
   const double vx = U[1] / U[0], vy = U[2] / U[0];
   double p, a2, H;
   thermal(U[3], U[0], vx * vx + vy * vy, gamma, p, a2, H);
@@ -1284,12 +1465,26 @@ void flux_jac_times_du(const double* U, const double* n, const double* dU, doubl
   dF[2] = dU[2] * vn + U[2] * dvn + n[1] * dp;
   dF[3] = (dU[3] + dp) * vn + (U[3] + p) * dvn;
   for (int k = 0; k < 4; k++) dF[k] -= lam * dU[k];
+  for (int k = 4; k < nv; k++) dF[k] = dU[k] * vn + U[k] * dvn - dU[k] * lam;  // the SA variable
 }
 
-// LUSGSMatrixInit (DNDS_FV_EulerEvaluator.cpp:995-1047), jacobianCode 0, no source term:
+// CompressInc (DNDS_FV_EulerEvaluator.hpp:1362-1406): the SA variable may not go negative; an
+// increment that would make it so is replaced by an exponential decay, floored at 1e-6
+void compress_inc(const orc_ctx& c, const double* u, double* inc) {
+  if (c.nv < 5) return;
+  if (u[4] + inc[4] < 0) {
+    const double declineV = inc[4] / (u[4] + 1e-6);
+    const double newu5 = std::max(1e-6, u[4] * std::exp(declineV));
+    inc[4] = newu5 - u[4];
+  }
+}
+
+// LUSGSMatrixInit (DNDS_FV_EulerEvaluator.cpp:995-1047), jacobianCode 0:
 // D_i = 1/dTau_i + 1/dt + sum_f (alpha/2) A_f lambdaFace_f / V_i, kept as its inverse
 void lusgs_matrix_init(orc_ctx& c, const double* dTau, double dt, double alpha) {
-  c.Dinv.assign(c.N, 0.0);
+  const int nv = c.nv;
+  c.Dinv.assign(c.N * nv, 0.0);
+  const bool src = c.srcJac.size() == (size_t)(c.N * nv);
   for (int64_t i = 0; i < c.N; i++) {
     const CellGeo& g = c.cg[i];
     double d = 1.0 / dTau[i] + 1.0 / dt;
@@ -1297,7 +1492,8 @@ void lusgs_matrix_init(orc_ctx& c, const double* dTau, double dt, double alpha) 
       const int f = g.faces[k];
       d += (0.5 * alpha) * c.fg[f].area * c.lambdaFace[f] / g.vol;
     }
-    c.Dinv[i] = 1.0 / d;
+    // + alpha * jacobianCellSourceDiag, kept diagonal
+    for (int v = 0; v < nv; v++) c.Dinv[i * nv + v] = 1.0 / (d + (src ? alpha * c.srcJac[i * nv + v] : 0.0));
   }
 }
 
@@ -1315,9 +1511,10 @@ void lusgs_offdiag(const orc_ctx& c, int64_t i, int64_t si, const std::vector<in
     const double nn = std::sqrt(sqr(fg.ncenter[0]) + sqr(fg.ncenter[1]));
     const double sg = fg.L == i ? 1.0 : -1.0;  // faces out of i
     const double n[2] = {sg * fg.ncenter[0] / nn, sg * fg.ncenter[1] / nn};
-    double dF[4];
-    flux_jac_times_du(&c.u[j * 4], n, &inc[j * 4], c.lambdaFace[f], c.s.gamma, dF);
-    for (int v = 0; v < 4; v++) buf[v] -= (0.5 * alpha) * fg.area / g.vol * dF[v];
+    const int nv = c.nv;
+    double dF[kMaxV];
+    flux_jac_times_du(&c.u[j * nv], n, &inc[j * nv], c.lambdaFace[f], c.s.gamma, dF, nv);
+    for (int v = 0; v < nv; v++) buf[v] -= (0.5 * alpha) * fg.area / g.vol * dF[v];
   }
 }
 
@@ -1337,17 +1534,19 @@ void lusgs_sweeps(const orc_ctx& c, double alpha, const double* rhs, double* inc
   if (doForward)
     for (int64_t s = 0; s < c.N; s++) {
       const int64_t i = order[s];
-      double buf[4];
-      for (int v = 0; v < 4; v++) buf[v] = rhs[i * 4 + v];
+      const int nv = c.nv;
+      double buf[kMaxV];
+      for (int v = 0; v < nv; v++) buf[v] = rhs[i * nv + v];
       lusgs_offdiag(c, i, s, pos, true, alpha, inc, buf);
-      for (int v = 0; v < 4; v++) inc[i * 4 + v] = c.Dinv[i] * buf[v];
+      for (int v = 0; v < nv; v++) inc[i * nv + v] = c.Dinv[i * nv + v] * buf[v];
     }
   if (doBackward)
     for (int64_t s = c.N - 1; s >= 0; s--) {
       const int64_t i = order[s];
-      double buf[4] = {0, 0, 0, 0};
+      const int nv = c.nv;
+      double buf[kMaxV] = {0};
       lusgs_offdiag(c, i, s, pos, false, alpha, inc, buf);
-      for (int v = 0; v < 4; v++) inc[i * 4 + v] += c.Dinv[i] * buf[v];
+      for (int v = 0; v < nv; v++) inc[i * nv + v] += c.Dinv[i * nv + v] * buf[v];
     }
 }
 
@@ -1361,10 +1560,12 @@ int orc_create(const orc_mesh* mesh, const orc_settings* s, orc_ctx** out) {
   auto* c = new orc_ctx();
   c->s = *s;
   c->nv = s->nvars;
-  if (c->nv != 4) { c->err = "only nvars=4 (NS_2D) is restated"; *out = c; return 2; }
+  if (c->nv != 4 && c->nv != 5) { c->err = "nvars must be 4 (NS_2D) or 5 (NS_2D with SA)"; *out = c; return 2; }
+  if (c->nv == 5 && !(s->mu_gas > 0)) { c->err = "the SA model needs mu_gas > 0"; *out = c; return 2; }
   if (s->rec_order != 2) { c->err = "only rec_order=2 (P2) is restated"; *out = c; return 2; }
   c->nthreads = s->n_threads > 0 ? s->n_threads : (int)std::max(1u, std::thread::hardware_concurrency());
   int rc = setup(*c, *mesh);
+  if (rc == 0 && c->nv == 5) wall_distance(*c, *mesh);
   *out = c;
   return rc;
 }
@@ -1473,8 +1674,8 @@ int orc_eval_rhs(orc_ctx* c, double t, double* rhs_out, double* wall_flux) {
 int orc_face_values(orc_ctx* c, double t, double* out) {
   parallel_for(c->nthreads, c->F, [&](int64_t b, int64_t e) {
     for (int64_t f = b; f < e; f++) {
-      double fl[3][4];
-      face_flux(*c, f, t, fl, &out[f * 24], nullptr);
+      double fl[3][kMaxV];
+      face_flux(*c, f, t, fl, &out[f * 6 * c->nv], nullptr);
     }
   });
   return 0;
@@ -1531,13 +1732,13 @@ int orc_lusgs_matrix_init(orc_ctx* c, const double* dtau, double dt, double alph
 }
 
 int orc_lusgs_forward(orc_ctx* c, double alpha, const double* rhs, double* inc, const int64_t* scan2cell) {
-  if (c->Dinv.size() != (size_t)c->N) return 1;
+  if (c->Dinv.size() != (size_t)(c->N * c->nv)) return 1;
   lusgs_sweeps(*c, alpha, rhs, inc, scan2cell, true, false);
   return 0;
 }
 
 int orc_lusgs_backward(orc_ctx* c, double alpha, const double* rhs, double* inc, const int64_t* scan2cell) {
-  if (c->Dinv.size() != (size_t)c->N) return 1;
+  if (c->Dinv.size() != (size_t)(c->N * c->nv)) return 1;
   lusgs_sweeps(*c, alpha, rhs, inc, scan2cell, false, true);
   return 0;
 }
@@ -1548,7 +1749,7 @@ int orc_lusgs_backward(orc_ctx* c, double alpha, const double* rhs, double* inc,
 // rhs = alpha R - (x - xLast)/dt; LU-SGS forward + backward from zero; x += inc
 int orc_implicit_iteration(orc_ctx* c, double cfl, double dt, double alpha, const double* x_last,
                            const int64_t* scan2cell, double t, int n_rec, double* inc_out) {
-  const int64_t n = c->N * 4;
+  const int64_t n = c->N * c->nv;
   double dtMin;
   eval_dt(*c, cfl, 1e100, true, &dtMin);
   std::vector<double> dTau(c->N), rhs(n), inc(n, 0.0);
@@ -1562,7 +1763,17 @@ int orc_implicit_iteration(orc_ctx* c, double cfl, double dt, double alpha, cons
     rhs[k] += x_last[k] / dt;
   }
   lusgs_matrix_init(*c, dTau.data(), dt, alpha);
+  const int nv = c->nv;
+  // fsolve's positivity fixes (DNDS_FV_EulerSolver.hpp:874-912): CompressInc on rhs * dTau, then
+  // on the increment
+  for (int64_t i = 0; i < c->N; i++) {
+    double r[kMaxV];
+    for (int v = 0; v < nv; v++) r[v] = rhs[i * nv + v] * dTau[i];
+    compress_inc(*c, &c->u[i * nv], r);
+    for (int v = 0; v < nv; v++) rhs[i * nv + v] = r[v] / dTau[i];
+  }
   lusgs_sweeps(*c, alpha, rhs.data(), inc.data(), scan2cell, true, true);
+  for (int64_t i = 0; i < c->N; i++) compress_inc(*c, &c->u[i * nv], &inc[i * nv]);
   for (int64_t k = 0; k < n; k++) c->u[k] += inc[k];
   if (inc_out) std::memcpy(inc_out, inc.data(), sizeof(double) * n);
   return 0;
