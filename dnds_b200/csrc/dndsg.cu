@@ -15,6 +15,7 @@
 #include "dndsg_bodies.cuh"
 #include "dndsg_limiter.cuh"
 #include "dndsg_mlp.cuh"
+#include "dndsg_sa.cuh"
 
 using namespace dg;
 
@@ -44,6 +45,11 @@ struct dndsg_ctx {
   void* vrOp = nullptr;       // T
   void* faceBasis = nullptr;  // T
   void* faceGrad = nullptr;   // T, viscous contexts only
+  // SA contexts (nvars 5): the fifth variable in its own arrays
+  bool sa = false;
+  double *saU = nullptr, *saULast = nullptr, *saRhs = nullptr, *saFlux = nullptr, *saInc = nullptr, *saDinv = nullptr,
+         *saSrcJac = nullptr, *saDWall = nullptr, *saCellGp = nullptr;
+  void *saUrec = nullptr, *saUrecNew = nullptr;  // T [N][5]
   double* Ainv = nullptr;
   double *limFace = nullptr, *faceInd = nullptr, *indicator = nullptr;  // CWBAP limiter data
   int32_t* wallCells = nullptr;  // cells with a Wall_Euler / Wall_NoSlip face
@@ -129,6 +135,14 @@ __global__ void k_setup_face(MeshView m, SetupParams p, const CellSetup* cells, 
   int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (f >= m.F) return;
   setup_face<T>(f, m, p, cells, faceW, normal, area, center, w0, basis, nullptr);
+}
+
+__global__ void k_setup_sa_cells(int64_t N, const CellSetup* cells, const double* seg, int64_t nw, double* gp,
+                                 double* dWall) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  setup_sa_cell_gp(i, cells, gp);
+  dWall[i] = sa_wall_distance(cells[i].bary[0], cells[i].bary[1], seg, nw);
 }
 
 template <class T>
@@ -507,6 +521,15 @@ HotView<T> view(dndsg_ctx* c) {
   return h;
 }
 
+template <class T>
+SaView<T> sa_view(dndsg_ctx* c) {
+  SaView<T> v;
+  v.u = c->saU; v.uLast = c->saULast; v.urec = (const T*)c->saUrec; v.urecNew = (T*)c->saUrecNew;
+  v.rhs = c->saRhs; v.flux = c->saFlux; v.inc = c->saInc; v.Dinv = c->saDinv; v.srcJac = c->saSrcJac;
+  v.dWall = c->saDWall; v.cellGp = c->saCellGp; v.far5 = c->s.far_field[4];
+  return v;
+}
+
 inline cudaStream_t st(void* s) { return (cudaStream_t)s; }
 
 // ------------------------------------------------------------------ hot-path drivers (templated on T)
@@ -732,6 +755,30 @@ int setup_run(dndsg_ctx* c, const dndsg_mesh_desc* md) {
     k_setup_face_grad<T><<<grid_for(F), kBlock>>>(m, cells, (T*)c->faceGrad);
     if ((rc = check_launch(c))) return rc;
   }
+  if (c->sa) {
+    // wall segments for the first-order wall distance, and the cell quadrature data of the source
+    std::vector<double> seg;
+    for (int64_t f = 0; f < F; f++)
+      if (md->face_bc[f] == BC_WALL_NOSLIP) {
+        const int32_t a = md->face_nodes[2 * f], b = md->face_nodes[2 * f + 1];
+        seg.insert(seg.end(), {md->node_xy[2 * a], md->node_xy[2 * a + 1], md->node_xy[2 * b], md->node_xy[2 * b + 1]});
+      }
+    double* dSeg = nullptr;
+    const int64_t nw = (int64_t)seg.size() / 4;
+    if (nw > 0) {
+      if ((rc = dalloc(c, dSeg, sizeof(double) * seg.size()))) return rc;
+      DG_CUDA(c, cudaMemcpy(dSeg, seg.data(), sizeof(double) * seg.size(), cudaMemcpyHostToDevice));
+    }
+    if ((rc = dalloc(c, c->saCellGp, sizeof(double) * N * kSaGp * kSaGpE)) || (rc = dalloc(c, c->saDWall, sizeof(double) * N)))
+      return rc;
+    k_setup_sa_cells<<<grid_for(N), kBlock>>>(N, cells, dSeg, nw, c->saCellGp, c->saDWall);
+    if ((rc = check_launch(c))) return rc;
+    DG_CUDA(c, cudaDeviceSynchronize());
+    if (dSeg) {
+      auto it = std::find(c->allocs.begin(), c->allocs.end(), (void*)dSeg);
+      if (it != c->allocs.end()) { cudaFree(dSeg); c->allocs.erase(it); }
+    }
+  }
   // ---- VR matrices
   if ((rc = dalloc(c, c->cellFace, sizeof(int32_t) * slots.size()))) return rc;
   DG_CUDA(c, cudaMemcpy(c->cellFace, slots.data(), sizeof(int32_t) * slots.size(), cudaMemcpyHostToDevice));
@@ -812,10 +859,29 @@ int setup_run(dndsg_ctx* c, const dndsg_mesh_desc* md) {
   DG_CUDA(c, cudaMemset(c->scal, 0, sizeof(double) * S_NSLOT));
   DG_CUDA(c, cudaMemset(c->flags, 0, sizeof(unsigned)));
   DG_CUDA(c, cudaMemset(c->nreduced, 0, sizeof(unsigned long long)));
+  if (c->sa) {
+    for (double** q : {&c->saU, &c->saULast, &c->saRhs, &c->saInc, &c->saDinv, &c->saSrcJac})
+      if ((rc = dalloc(c, *q, sizeof(double) * N))) return rc;
+    if ((rc = dalloc(c, c->saFlux, sizeof(double) * F)) || (rc = dalloc(c, c->saUrec, sizeof(T) * 5 * N)) ||
+        (rc = dalloc(c, c->saUrecNew, sizeof(T) * 5 * N)))
+      return rc;
+    for (double* q : {c->saU, c->saULast, c->saRhs, c->saInc, c->saSrcJac}) DG_CUDA(c, cudaMemset(q, 0, sizeof(double) * N));
+    DG_CUDA(c, cudaMemset(c->saFlux, 0, sizeof(double) * F));
+    DG_CUDA(c, cudaMemset(c->saUrec, 0, sizeof(T) * 5 * N));
+    DG_CUDA(c, cudaMemset(c->saUrecNew, 0, sizeof(T) * 5 * N));
+  }
   DG_CUDA(c, cudaDeviceSynchronize());
   return 0;
 }
 
+}  // namespace
+
+// SA-context drivers, defined with their kernels at the end of this file
+namespace {
+int sa_vr_steps(dndsg_ctx* c, int nsweeps, cudaStream_t s);
+int sa_eval_dt(dndsg_ctx* c, double cfl, double maxDt, cudaStream_t s);
+int sa_eval_rhs(dndsg_ctx* c, cudaStream_t s);
+int sa_implicit(dndsg_ctx* c, double cfl, double dtPhys, double alpha, int nRec, int volWise, cudaStream_t s);
 }  // namespace
 
 // ====================================================================== C ABI
@@ -829,7 +895,10 @@ int dndsg_create(const dndsg_mesh_desc* mesh, const dndsg_settings* settings, in
   if (!mesh || !settings) return fail(c, DNDSG_BAD_ARGUMENT, "null mesh or settings");
   c->s = *settings;
   c->device = device;
-  if (c->s.nvars != 4) return fail(c, DNDSG_UNSUPPORTED, "nvars must be 4 (NS_2D)");
+  if (c->s.nvars != 4 && c->s.nvars != 5) return fail(c, DNDSG_UNSUPPORTED, "nvars must be 4 (NS_2D) or 5 (with SA)");
+  c->sa = c->s.nvars == 5;
+  if (c->sa && !(c->s.mu_gas > 0)) return fail(c, DNDSG_UNSUPPORTED, "the SA model needs mu_gas > 0");
+  if (c->sa && c->s.limiter) return fail(c, DNDSG_UNSUPPORTED, "the SA contexts run without the limiter");
   if (c->s.rec_order != 2) return fail(c, DNDSG_UNSUPPORTED, "rec_order must be 2 (P2)");
   if (c->s.sor_instead) return fail(c, DNDSG_UNSUPPORTED, "the GPU VR sweep is Jacobi (sor_instead must be 0)");
   if (c->s.riemann != 1 && c->s.riemann != 2) return fail(c, DNDSG_UNSUPPORTED, "riemann must be 1 (Roe) or 2 (HLLC)");
@@ -879,12 +948,33 @@ int64_t dndsg_n_faces(dndsg_ctx* c) { return c ? c->F : -1; }
 
 int dndsg_set_u(dndsg_ctx* c, const double* u, void* s) {
   if (!c || !u) return DNDSG_BAD_ARGUMENT;
+  if (c->sa) {  // [N][5] -> flow [N][4] + U5 [N]
+    std::vector<double> a(4 * c->N), b(c->N);
+    for (int64_t i = 0; i < c->N; i++) {
+      for (int v = 0; v < 4; v++) a[4 * i + v] = u[5 * i + v];
+      b[i] = u[5 * i + 4];
+    }
+    DG_CUDA(c, cudaMemcpy(c->u, a.data(), sizeof(double) * 4 * c->N, cudaMemcpyHostToDevice));
+    DG_CUDA(c, cudaMemcpy(c->saU, b.data(), sizeof(double) * c->N, cudaMemcpyHostToDevice));
+    return 0;
+  }
   DG_CUDA(c, cudaMemcpyAsync(c->u, u, sizeof(double) * 4 * c->N, cudaMemcpyHostToDevice, st(s)));
   DG_CUDA(c, cudaStreamSynchronize(st(s)));
   return 0;
 }
 int dndsg_get_u(dndsg_ctx* c, double* u, void* s) {
   if (!c || !u) return DNDSG_BAD_ARGUMENT;
+  if (c->sa) {
+    DG_CUDA(c, cudaStreamSynchronize(st(s)));
+    std::vector<double> a(4 * c->N), b(c->N);
+    DG_CUDA(c, cudaMemcpy(a.data(), c->u, sizeof(double) * 4 * c->N, cudaMemcpyDeviceToHost));
+    DG_CUDA(c, cudaMemcpy(b.data(), c->saU, sizeof(double) * c->N, cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < c->N; i++) {
+      for (int v = 0; v < 4; v++) u[5 * i + v] = a[4 * i + v];
+      u[5 * i + 4] = b[i];
+    }
+    return 0;
+  }
   DG_CUDA(c, cudaMemcpyAsync(u, c->u, sizeof(double) * 4 * c->N, cudaMemcpyDeviceToHost, st(s)));
   DG_CUDA(c, cudaStreamSynchronize(st(s)));
   return 0;
@@ -896,8 +986,41 @@ int dndsg_get_dt(dndsg_ctx* c, double* dt, void* s) {
   return 0;
 }
 
+}  // extern "C"
+
+namespace {
+// host-side split / merge of [N][5][5] coefficients of an SA context, in the context's precision
+template <class T>
+int sa_urec_io(dndsg_ctx* c, double* r, bool set) {
+  const int64_t N = c->N;
+  std::vector<T> a(20 * N), b(5 * N);
+  if (set) {
+    for (int64_t i = 0; i < N; i++)
+      for (int q = 0; q < 5; q++) {
+        for (int v = 0; v < 4; v++) a[20 * i + 4 * q + v] = (T)r[25 * i + 5 * q + v];
+        b[5 * i + q] = (T)r[25 * i + 5 * q + 4];
+      }
+    DG_CUDA(c, cudaMemcpy(c->urec, a.data(), sizeof(T) * 20 * N, cudaMemcpyHostToDevice));
+    DG_CUDA(c, cudaMemcpy(c->saUrec, b.data(), sizeof(T) * 5 * N, cudaMemcpyHostToDevice));
+  } else {
+    DG_CUDA(c, cudaDeviceSynchronize());
+    DG_CUDA(c, cudaMemcpy(a.data(), c->urec, sizeof(T) * 20 * N, cudaMemcpyDeviceToHost));
+    DG_CUDA(c, cudaMemcpy(b.data(), c->saUrec, sizeof(T) * 5 * N, cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < N; i++)
+      for (int q = 0; q < 5; q++) {
+        for (int v = 0; v < 4; v++) r[25 * i + 5 * q + v] = (double)a[20 * i + 4 * q + v];
+        r[25 * i + 5 * q + 4] = (double)b[5 * i + q];
+      }
+  }
+  return 0;
+}
+}  // namespace
+
+extern "C" {
+
 int dndsg_set_urec(dndsg_ctx* c, const double* r, void* s) {
   if (!c || !r) return DNDSG_BAD_ARGUMENT;
+  if (c->sa) return c->fp32 ? sa_urec_io<float>(c, const_cast<double*>(r), true) : sa_urec_io<double>(c, const_cast<double*>(r), true);
   const int64_t n = 20 * c->N;
   if (!c->fp32) {
     DG_CUDA(c, cudaMemcpyAsync(c->urec, r, sizeof(double) * n, cudaMemcpyHostToDevice, st(s)));
@@ -913,6 +1036,7 @@ int dndsg_set_urec(dndsg_ctx* c, const double* r, void* s) {
 }
 int dndsg_get_urec(dndsg_ctx* c, double* r, void* s) {
   if (!c || !r) return DNDSG_BAD_ARGUMENT;
+  if (c->sa) return c->fp32 ? sa_urec_io<float>(c, r, false) : sa_urec_io<double>(c, r, false);
   const int64_t n = 20 * c->N;
   if (!c->fp32) {
     DG_CUDA(c, cudaMemcpyAsync(r, c->urec, sizeof(double) * n, cudaMemcpyDeviceToHost, st(s)));
@@ -953,6 +1077,10 @@ int dndsg_set_time(dndsg_ctx* c, double t, void* s) {
 
 int dndsg_vr_jacobi_step(dndsg_ctx* c, int nsweeps, double* inc_out, void* s) {
   if (!c || nsweeps < 0) return DNDSG_BAD_ARGUMENT;
+  if (c->sa) {
+    if (inc_out) return fail(c, DNDSG_UNSUPPORTED, "SA contexts report no sweep increment");
+    return sa_vr_steps(c, nsweeps, st(s));
+  }
   for (int k = 0; k < nsweeps; k++) {
     bool last = inc_out && k == nsweeps - 1;
     if (last) k_init_dtmin<<<1, 1, 0, st(s)>>>(c->scal);
@@ -986,7 +1114,10 @@ int dndsg_limiter_wbap(dndsg_ctx* c, int if_all, double* indicator_out, void* s)
 
 int dndsg_eval_dt(dndsg_ctx* c, double cfl, double max_dt, int use_local_dt, double* dt_min_out, void* s) {
   if (!c) return DNDSG_BAD_ARGUMENT;
-  if (c->fp32) run_dt<float>(c, cfl, max_dt, false, st(s));
+  if (c->sa) {
+    int rc0 = sa_eval_dt(c, cfl, max_dt, st(s));
+    if (rc0) return rc0;
+  } else if (c->fp32) run_dt<float>(c, cfl, max_dt, false, st(s));
   else run_dt<double>(c, cfl, max_dt, false, st(s));
   if (!use_local_dt) k_fill_dt<<<grid_for(c->N), kBlock, 0, st(s)>>>(c->dt, c->N, c->scal);
   int rc = check_launch(c);
@@ -1002,6 +1133,21 @@ int dndsg_eval_dt(dndsg_ctx* c, double cfl, double max_dt, int use_local_dt, dou
 
 int dndsg_eval_rhs(dndsg_ctx* c, double t, double* rhs_out, void* s) {
   if (!c) return DNDSG_BAD_ARGUMENT;
+  if (c->sa) {
+    int rc0 = sa_eval_rhs(c, st(s));
+    if (rc0) return rc0;
+    if (rhs_out) {
+      DG_CUDA(c, cudaStreamSynchronize(st(s)));
+      std::vector<double> a(4 * c->N), b(c->N);
+      DG_CUDA(c, cudaMemcpy(a.data(), c->rhs, sizeof(double) * 4 * c->N, cudaMemcpyDeviceToHost));
+      DG_CUDA(c, cudaMemcpy(b.data(), c->saRhs, sizeof(double) * c->N, cudaMemcpyDeviceToHost));
+      for (int64_t i = 0; i < c->N; i++) {
+        for (int v = 0; v < 4; v++) rhs_out[5 * i + v] = a[4 * i + v];
+        rhs_out[5 * i + 4] = b[i];
+      }
+    }
+    return 0;
+  }
   if (c->fp32) run_rhs<float>(c, t, st(s));
   else run_rhs<double>(c, t, st(s));
   int rc = check_launch(c);
@@ -1015,6 +1161,7 @@ int dndsg_eval_rhs(dndsg_ctx* c, double t, double* rhs_out, void* s) {
 
 int dndsg_ssprk3_step(dndsg_ctx* c, double cfl, double t_end, void* s) {
   if (!c) return DNDSG_BAD_ARGUMENT;
+  if (c->sa) return fail(c, DNDSG_UNSUPPORTED, "SA contexts run the implicit path (dndsg_implicit_iteration)");
   if (c->fp32) run_step<float>(c, cfl, t_end, st(s));
   else run_step<double>(c, cfl, t_end, st(s));
   return check_launch(c);
@@ -1034,11 +1181,24 @@ int dndsg_residual(dndsg_ctx* c, int p, int vol_wise, double* out, void* s) {
     for (unsigned b = 0; b < nb; b++) a = p < 3 ? a + part[4 * b + v] : std::max(a, part[4 * b + v]);
     out[v] = p < 3 ? std::pow(a, 1.0 / p) : a;
   }
+  if (c->sa) {  // the U5 component (host reduction)
+    std::vector<double> r(c->N), vol(c->N);
+    DG_CUDA(c, cudaMemcpy(r.data(), c->saRhs, sizeof(double) * c->N, cudaMemcpyDeviceToHost));
+    DG_CUDA(c, cudaMemcpy(vol.data(), c->vol, sizeof(double) * c->N, cudaMemcpyDeviceToHost));
+    double a = 0;
+    for (int64_t i = 0; i < c->N; i++) {
+      const double x = std::fabs(r[i]);
+      if (p < 3) a += std::pow(x, (double)p) * (vol_wise ? vol[i] : 1.0);
+      else a = std::max(a, x);
+    }
+    out[4] = p < 3 ? std::pow(a, 1.0 / p) : a;
+  }
   return 0;
 }
 
 int dndsg_face_values(dndsg_ctx* c, double t, double* out, void* s) {
   if (!c || !out) return DNDSG_BAD_ARGUMENT;
+  if (c->sa) return fail(c, DNDSG_UNSUPPORTED, "face values are reported for 4-variable contexts");
   double* d;
   size_t bytes = sizeof(double) * 24 * c->F;
   DG_CUDA(c, cudaMallocAsync((void**)&d, bytes, st(s)));
@@ -1125,7 +1285,7 @@ void run_rhs_noalloc(dndsg_ctx* c, const double* u, const void* urec, double* rh
 
 extern "C" int dndsg_eval_rhs_noalloc(dndsg_ctx* c, const double* u, const void* urec, double* rhs, double t,
                                       void* s) {
-  if (c && c->s.mu_gas > 0)
+  if (c && (c->s.mu_gas > 0 || c->sa))
     return fail(c, DNDSG_UNSUPPORTED, "the allocation-free RHS covers the inviscid model only (mu_gas = 0)");
   if (!c || !u || !urec || !rhs) return DNDSG_BAD_ARGUMENT;
   if (c->F > kNoAllocMaxFaces)
@@ -1500,6 +1660,7 @@ int dndsg_mlp_train_step(dndsg_mlp* m, const float* X, const float* Tg, int64_t 
 
 int dndsg_mlp_features(dndsg_ctx* c, float* X, float* scales, void* s) {
   if (!c || !X || !scales) return DNDSG_BAD_ARGUMENT;
+  if (c->sa) return fail(c, DNDSG_UNSUPPORTED, "the learned warm start is for 4-variable contexts");
   int rc = c->fp32 ? ensure_mlp_buffers<float>(c) : ensure_mlp_buffers<double>(c);
   if (rc) return rc;
   // x1 = J(x0), x2 = J(x1) into work buffers; the context's coefficients are left as they are
@@ -1520,6 +1681,7 @@ int dndsg_mlp_features(dndsg_ctx* c, float* X, float* scales, void* s) {
 int dndsg_vr_to_tolerance(dndsg_ctx* c, const dndsg_mlp* m, double tol, int max_sweeps, int* sweeps_out,
                           int64_t* accepted_out, float* harvest_x, float* harvest_t, void* s) {
   if (!c || max_sweeps < 1 || !(tol >= 0)) return DNDSG_BAD_ARGUMENT;
+  if (c->sa) return fail(c, DNDSG_UNSUPPORTED, "the learned warm start is for 4-variable contexts");
   if (m && m->device != c->device) return fail(c, DNDSG_BAD_ARGUMENT, "network and context on different devices");
   return c->fp32 ? vr_to_tol<float>(c, m, tol, max_sweeps, sweeps_out, accepted_out, harvest_x, harvest_t, st(s))
                  : vr_to_tol<double>(c, m, tol, max_sweeps, sweeps_out, accepted_out, harvest_x, harvest_t, st(s));
@@ -1528,6 +1690,7 @@ int dndsg_vr_to_tolerance(dndsg_ctx* c, const dndsg_mlp* m, double tol, int max_
 int dndsg_ssprk3_step_tol(dndsg_ctx* c, const dndsg_mlp* m, double cfl, double t_end, double tol, int max_sweeps,
                           int* sweeps_out, float* harvest_x, float* harvest_t, void* s) {
   if (!c || max_sweeps < 1 || !(tol >= 0)) return DNDSG_BAD_ARGUMENT;
+  if (c->sa) return fail(c, DNDSG_UNSUPPORTED, "the learned warm start is for 4-variable contexts");
   if (m && m->device != c->device) return fail(c, DNDSG_BAD_ARGUMENT, "network and context on different devices");
   return c->fp32 ? run_step_tol<float>(c, m, cfl, t_end, tol, max_sweeps, sweeps_out, harvest_x, harvest_t, st(s))
                  : run_step_tol<double>(c, m, cfl, t_end, tol, max_sweeps, sweeps_out, harvest_x, harvest_t, st(s));
@@ -1847,7 +2010,7 @@ int ensure_lusgs(dndsg_ctx* c) {
   group_by(rev, ncol, bwd, c->bwdOff);
   if ((rc = dalloc(c, c->rankOf, sizeof(int32_t) * N)) || (rc = dalloc(c, c->fwdCells, sizeof(int32_t) * N)) ||
       (rc = dalloc(c, c->bwdCells, sizeof(int32_t) * N)) || (rc = dalloc(c, c->Dinv, sizeof(double) * N)) ||
-      (rc = dalloc(c, c->inc, sizeof(double) * 4 * N)) || (rc = dalloc(c, c->resAcc, sizeof(double) * 8)))
+      (rc = dalloc(c, c->inc, sizeof(double) * 4 * N)) || (rc = dalloc(c, c->resAcc, sizeof(double) * 16)))
     return rc;
   c->colourHost = col;
   c->lusgsOrder = 0;
@@ -1998,7 +2161,7 @@ int run_implicit(dndsg_ctx* c, double cfl, double dtPhys, double alpha, int nRec
   k_lusgs_init<T><<<grid_for(c->N), kBlock, 0, s>>>(h, dtInv, alpha, c->Dinv);
   launch_lusgs_sweep<T>(c, true, alpha, c->rhs, c->inc, s);
   launch_lusgs_sweep<T>(c, false, alpha, c->rhs, c->inc, s);
-  DG_CUDA(c, cudaMemsetAsync(c->resAcc, 0, sizeof(double) * 8, s));
+  DG_CUDA(c, cudaMemsetAsync(c->resAcc, 0, sizeof(double) * 16, s));
   k_add_inc<<<grid_for(c->N), kBlock, 0, s>>>(c->N, c->u, c->inc, c->vol, volWise, c->resAcc);
   if (c->F > c->Fi)
     k_wall_flux<<<grid_for(c->F - c->Fi), kBlock, 0, s>>>(c->Fi, c->F, c->faceBC, c->flux, c->resAcc + 4);
@@ -2049,6 +2212,7 @@ int dndsg_lusgs_matrix_init(dndsg_ctx* c, double dt_phys, double alpha, void* s)
 
 static int lusgs_sweep_api(dndsg_ctx* c, bool fwd, double alpha, const double* rhs, double* inc, void* s) {
   if (!c || !rhs || !inc) return DNDSG_BAD_ARGUMENT;
+  if (c->sa) return fail(c, DNDSG_UNSUPPORTED, "SA contexts sweep inside dndsg_implicit_iteration");
   if (!c->rankOf) return fail(c, DNDSG_BAD_ARGUMENT, "dndsg_lusgs_matrix_init first");
   int rc;
   if ((rc = set_device(c))) return rc;
@@ -2070,6 +2234,7 @@ int dndsg_bdf_begin(dndsg_ctx* c, void* s) {
   int rc;
   if ((rc = set_device(c))) return rc;
   DG_CUDA(c, cudaMemcpyAsync(c->uLast, c->u, sizeof(double) * 4 * c->N, cudaMemcpyDeviceToDevice, st(s)));
+  if (c->sa) DG_CUDA(c, cudaMemcpyAsync(c->saULast, c->saU, sizeof(double) * c->N, cudaMemcpyDeviceToDevice, st(s)));
   return 0;
 }
 
@@ -2078,17 +2243,239 @@ int dndsg_implicit_iteration(dndsg_ctx* c, double cfl, double dt_phys, double al
   if (!c || !(cfl > 0) || !(dt_phys > 0) || !(alpha > 0) || n_rec < 0) return DNDSG_BAD_ARGUMENT;
   int rc;
   if ((rc = set_device(c))) return rc;
-  rc = c->fp32 ? run_implicit<float>(c, cfl, dt_phys, alpha, n_rec, vol_wise, t, st(s))
-               : run_implicit<double>(c, cfl, dt_phys, alpha, n_rec, vol_wise, t, st(s));
+  if (c->sa) rc = sa_implicit(c, cfl, dt_phys, alpha, n_rec, vol_wise, st(s));
+  else
+    rc = c->fp32 ? run_implicit<float>(c, cfl, dt_phys, alpha, n_rec, vol_wise, t, st(s))
+                 : run_implicit<double>(c, cfl, dt_phys, alpha, n_rec, vol_wise, t, st(s));
   if (rc) return rc;
   if (inc_res_out || wall_flux_out) {
-    double acc[8];
+    double acc[16];
     DG_CUDA(c, cudaMemcpyAsync(acc, c->resAcc, sizeof(acc), cudaMemcpyDeviceToHost, st(s)));
     DG_CUDA(c, cudaStreamSynchronize(st(s)));
     if (inc_res_out) for (int v = 0; v < 4; v++) inc_res_out[v] = acc[v];
     if (wall_flux_out) for (int v = 0; v < 4; v++) wall_flux_out[v] = acc[4 + v];
+    if (c->sa) {
+      if (inc_res_out) inc_res_out[4] = acc[8];
+      if (wall_flux_out) wall_flux_out[4] = acc[9];
+    }
   }
   return 0;
 }
 
 }  // extern "C"
+
+// ====================================================================== SA contexts (nvars 5)
+namespace {
+
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_sa_vr(HotView<T> h, SaView<T> sa) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < h.N) sa_vr_cell<T>(i, h, sa);
+}
+
+template <class T, int RIEMANN, bool BND>
+__global__ void __launch_bounds__(kBlock) k_face_flux_sa(HotView<T> h, SaView<T> sa, int64_t f0, int64_t f1,
+                                                         unsigned* flags, unsigned long long* nred) {
+  const int64_t f = f0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int r = 0;
+  bool bad = false;
+  if (f < f1) {
+    double out[4], outS;
+    r = face_flux_sa<T, RIEMANN, BND>(f, h, sa, out, outS, bad);
+    double* o = &h.flux[f * 4];
+    *reinterpret_cast<double2*>(o) = make_double2(out[0], out[1]);
+    *reinterpret_cast<double2*>(o + 2) = make_double2(out[2], out[3]);
+    sa.flux[f] = outS;
+  }
+  unsigned anyBad = __ballot_sync(0xffffffffu, bad);
+  int rs = __reduce_add_sync(0xffffffffu, r);
+  if ((threadIdx.x & 31) == 0) {
+    if (anyBad) atomicOr(flags, 1u);
+    if (rs) atomicAdd(nred, (unsigned long long)rs);
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_sa_cell_rhs(HotView<T> h, SaView<T> sa) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < h.N) sa_cell_rhs<T>(i, h, sa);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_dt_face_sa(HotView<T> h, SaView<T> sa) {
+  const int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (f < h.F) dt_face_sa<T>(f, h, sa);
+}
+
+template <class T, bool FWD>
+__global__ void __launch_bounds__(kBlock) k_lusgs_batch_sa(HotView<T> h, SaView<T> sa, const int32_t* rankOf,
+                                                           const int32_t* cells, int64_t n, double alpha,
+                                                           const double* Dinv, const double* rhs, double* inc) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t < n) lusgs_cell_sa<T, FWD>(h, sa, rankOf, cells[t], alpha, Dinv, rhs, inc);
+}
+
+// all narrow levels of one sweep in one block (as k_lusgs_levels), 5 variables
+template <class T, bool FWD>
+__global__ void __launch_bounds__(kLevelBlock) k_lusgs_levels_sa(HotView<T> h, SaView<T> sa, const int32_t* rankOf,
+                                                                 const int32_t* cells, const int64_t* off, int nlev,
+                                                                 double alpha, const double* Dinv, const double* rhs,
+                                                                 double* inc) {
+  for (int l = 0; l < nlev; l++) {
+    const int64_t b = off[l], e = off[l + 1];
+    for (int64_t t = b + threadIdx.x; t < e; t += blockDim.x)
+      lusgs_cell_sa<T, FWD>(h, sa, rankOf, cells[t], alpha, Dinv, rhs, inc);
+    __syncthreads();
+  }
+}
+
+// the U5 diagonal: the flow one plus alpha * the source Jacobian (LUSGSMatrixInit)
+__global__ void k_sa_diag(int64_t N, const double* Dinv, const double* srcJac, double alpha, double* DinvS) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < N) DinvS[i] = 1.0 / (1.0 / Dinv[i] + alpha * srcJac[i]);
+}
+
+// U5 parts of one pseudo-time iteration: the BDF rhs, CompressInc of rhs * dTau (dTau = dt / alpha)
+__global__ void k_sa_rhs_fix(int64_t N, const double* u, const double* uLast, const double* dt, double alpha,
+                             double dtPhysInv, double* rhs) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  double r = alpha * rhs[i] - u[i] * dtPhysInv + uLast[i] * dtPhysInv;
+  const double dTau = dt[i] / alpha;
+  r = sa_compress_inc(u[i], r * dTau) / dTau;
+  rhs[i] = r;
+}
+
+// CompressInc of the U5 increment, u5 += inc, its L1 norm, and the U5 wall flux
+__global__ void __launch_bounds__(kBlock) k_sa_add_inc(int64_t N, double* u, double* inc, const double* vol,
+                                                       int volWise, double* acc) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  double a = 0;
+  if (i < N) {
+    const double d = sa_compress_inc(u[i], inc[i]);
+    inc[i] = d;
+    u[i] += d;
+    a = fabs(d) * (volWise ? vol[i] : 1.0);
+  }
+  a = warp_sum(a);
+  if ((threadIdx.x & 31) == 0 && a != 0.0) atomicAdd(acc, a);
+}
+
+__global__ void __launch_bounds__(kBlock) k_sa_wall_flux(int64_t Fi, int64_t F, const int32_t* faceBC,
+                                                         const double* flux, double* acc) {
+  const int64_t f = Fi + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  double a = 0;
+  if (f < F && (faceBC[f] == BC_WALL_NOSLIP || faceBC[f] == BC_WALL_EULER)) a = -flux[f];
+  a = warp_sum(a);
+  if ((threadIdx.x & 31) == 0 && a != 0.0) atomicAdd(acc, a);
+}
+
+template <class T>
+void run_vr_sa(dndsg_ctx* c, cudaStream_t s) {
+  run_vr<T>(c, false, s);
+  k_sa_vr<T><<<grid_for(c->N), kBlock, 0, s>>>(view<T>(c), sa_view<T>(c));
+  std::swap(c->saUrec, c->saUrecNew);
+}
+
+template <class T>
+void run_dt_sa(dndsg_ctx* c, double cfl, double maxDt, cudaStream_t s) {
+  HotView<T> h = view<T>(c);
+  k_init_dtmin<<<1, 1, 0, s>>>(c->scal);
+  k_dt_face_sa<T><<<grid_for(c->F), kBlock, 0, s>>>(h, sa_view<T>(c));
+  k_dt_cell<T, false><<<grid_for(c->N), kBlock, 0, s>>>(h, cfl, maxDt, c->scal);
+}
+
+template <class T>
+void run_rhs_sa(dndsg_ctx* c, cudaStream_t s) {
+  HotView<T> h = view<T>(c);
+  SaView<T> sa = sa_view<T>(c);
+  const int64_t Fi = c->Fi, F = c->F;
+  if (c->s.riemann == 2) {
+    if (Fi > 0) k_face_flux_sa<T, 2, false><<<grid_for(Fi), kBlock, 0, s>>>(h, sa, 0, Fi, c->flags, c->nreduced);
+    if (F > Fi) k_face_flux_sa<T, 2, true><<<grid_for(F - Fi), kBlock, 0, s>>>(h, sa, Fi, F, c->flags, c->nreduced);
+  } else {
+    if (Fi > 0) k_face_flux_sa<T, 1, false><<<grid_for(Fi), kBlock, 0, s>>>(h, sa, 0, Fi, c->flags, c->nreduced);
+    if (F > Fi) k_face_flux_sa<T, 1, true><<<grid_for(F - Fi), kBlock, 0, s>>>(h, sa, Fi, F, c->flags, c->nreduced);
+  }
+  k_cell_update<T, -1><<<grid_for(c->N), kBlock, 0, s>>>(h, c->scal);
+  k_sa_cell_rhs<T><<<grid_for(c->N), kBlock, 0, s>>>(h, sa);
+}
+
+template <class T>
+void launch_lusgs_sweep_sa(dndsg_ctx* c, bool forward, double alpha, cudaStream_t s) {
+  HotView<T> h = view<T>(c);
+  SaView<T> sa = sa_view<T>(c);
+  const std::vector<int64_t>& off = forward ? c->fwdOff : c->bwdOff;
+  const int32_t* cells = forward ? c->fwdCells : c->bwdCells;
+  const int nb = (int)off.size() - 1;
+  if (c->lusgsOrder == 1) {  // many narrow levels: one block walks them all
+    const int64_t* od = forward ? c->fwdOffDev : c->bwdOffDev;
+    if (forward)
+      k_lusgs_levels_sa<T, true><<<1, kLevelBlock, 0, s>>>(h, sa, c->rankOf, cells, od, nb, alpha, c->Dinv, c->rhs, c->inc);
+    else
+      k_lusgs_levels_sa<T, false><<<1, kLevelBlock, 0, s>>>(h, sa, c->rankOf, cells, od, nb, alpha, c->Dinv, c->rhs, c->inc);
+    return;
+  }
+  for (int k = 0; k < nb; k++) {
+    const int64_t b = off[k], n = off[k + 1] - b;
+    if (n == 0) continue;
+    if (forward)
+      k_lusgs_batch_sa<T, true><<<grid_for(n), kBlock, 0, s>>>(h, sa, c->rankOf, cells + b, n, alpha, c->Dinv, c->rhs, c->inc);
+    else
+      k_lusgs_batch_sa<T, false><<<grid_for(n), kBlock, 0, s>>>(h, sa, c->rankOf, cells + b, n, alpha, c->Dinv, c->rhs, c->inc);
+  }
+}
+
+// one pseudo-time iteration of an SA context (as run_implicit, with the U5 equation and the
+// positivity fixes of fsolve)
+template <class T>
+int run_implicit_sa(dndsg_ctx* c, double cfl, double dtPhys, double alpha, int nRec, int volWise, cudaStream_t s) {
+  int rc;
+  if ((rc = ensure_lusgs(c))) return rc;
+  run_dt_sa<T>(c, cfl, 1e100, s);
+  for (int k = 0; k < nRec; k++) run_vr_sa<T>(c, s);
+  run_rhs_sa<T>(c, s);
+  const double dtInv = 1.0 / dtPhys;
+  const int64_t n4 = c->N * 4;
+  k_bdf_rhs<<<(unsigned)((n4 + kBlock - 1) / kBlock), kBlock, 0, s>>>(n4, c->u, c->uLast, alpha, dtInv, c->rhs);
+  k_sa_rhs_fix<<<grid_for(c->N), kBlock, 0, s>>>(c->N, c->saU, c->saULast, c->dt, alpha, dtInv, c->saRhs);
+  HotView<T> h = view<T>(c);
+  k_lusgs_init<T><<<grid_for(c->N), kBlock, 0, s>>>(h, dtInv, alpha, c->Dinv);
+  k_sa_diag<<<grid_for(c->N), kBlock, 0, s>>>(c->N, c->Dinv, c->saSrcJac, alpha, c->saDinv);
+  launch_lusgs_sweep_sa<T>(c, true, alpha, s);
+  launch_lusgs_sweep_sa<T>(c, false, alpha, s);
+  DG_CUDA(c, cudaMemsetAsync(c->resAcc, 0, sizeof(double) * 16, s));
+  k_add_inc<<<grid_for(c->N), kBlock, 0, s>>>(c->N, c->u, c->inc, c->vol, volWise, c->resAcc);
+  k_sa_add_inc<<<grid_for(c->N), kBlock, 0, s>>>(c->N, c->saU, c->saInc, c->vol, volWise, c->resAcc + 8);
+  if (c->F > c->Fi) {
+    k_wall_flux<<<grid_for(c->F - c->Fi), kBlock, 0, s>>>(c->Fi, c->F, c->faceBC, c->flux, c->resAcc + 4);
+    k_sa_wall_flux<<<grid_for(c->F - c->Fi), kBlock, 0, s>>>(c->Fi, c->F, c->faceBC, c->saFlux, c->resAcc + 9);
+  }
+  return check_launch(c);
+}
+
+}  // namespace
+
+namespace {
+int sa_vr_steps(dndsg_ctx* c, int nsweeps, cudaStream_t s) {
+  for (int k = 0; k < nsweeps; k++) {
+    if (c->fp32) run_vr_sa<float>(c, s);
+    else run_vr_sa<double>(c, s);
+  }
+  return check_launch(c);
+}
+int sa_eval_dt(dndsg_ctx* c, double cfl, double maxDt, cudaStream_t s) {
+  if (c->fp32) run_dt_sa<float>(c, cfl, maxDt, s);
+  else run_dt_sa<double>(c, cfl, maxDt, s);
+  return check_launch(c);
+}
+int sa_eval_rhs(dndsg_ctx* c, cudaStream_t s) {
+  if (c->fp32) run_rhs_sa<float>(c, s);
+  else run_rhs_sa<double>(c, s);
+  return check_launch(c);
+}
+int sa_implicit(dndsg_ctx* c, double cfl, double dtPhys, double alpha, int nRec, int volWise, cudaStream_t s) {
+  return c->fp32 ? run_implicit_sa<float>(c, cfl, dtPhys, alpha, nRec, volWise, s)
+                 : run_implicit_sa<double>(c, cfl, dtPhys, alpha, nRec, volWise, s);
+}
+}  // namespace

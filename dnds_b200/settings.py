@@ -214,11 +214,27 @@ NACA0012_LAMINAR = {
 }
 
 
+def naca0012_sa(mach: float = 0.15, alpha: float = 10.0, reynolds: float = 6e6, nut_ratio: float = 3.0) -> dict:
+    """RANS-SA over the NACA 0012 (5 variables: rho, rho u, rho v, E, rho nu~ / muGas) with the
+    NACA0012 vfvSetting; the free-stream SA variable is nut_ratio times the laminar viscosity."""
+    gas = laminar_gas(mach, reynolds)
+    return {
+        "nvars": 5,
+        "recOrder": 2,
+        "vfvSetting": dict(NACA0012["vfvSetting"]),
+        "eulerSetting": {
+            "riemannSolverType": "Roe",
+            "idealGasProperty": gas,
+            "farFieldStaticValue": free_stream(mach, alpha) + [nut_ratio],
+        },
+    }
+
+
 def preset(name: str, **overrides) -> dict:
     import copy
 
     base = {"vortex": ISENTROPIC_VORTEX, "riemann": RIEMANN_2D, "naca0012": NACA0012,
-            "naca0012_laminar": NACA0012_LAMINAR}[name]
+            "naca0012_laminar": NACA0012_LAMINAR, "naca0012_sa": naca0012_sa()}[name]
     cfg = copy.deepcopy(base)
     for k, v in overrides.items():
         if isinstance(v, dict) and isinstance(cfg.get(k), dict):

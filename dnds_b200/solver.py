@@ -59,7 +59,7 @@ class Solver:
             raise DndsgError(rc, msg)
         self.N = mesh.n_cells
         self.F = mesh.n_faces
-        self.nv = 4
+        self.nv = int(s.nvars)
 
     # ------------------------------------------------------------------ lifetime
     def close(self):
@@ -76,21 +76,21 @@ class Solver:
 
     # ------------------------------------------------------------------ state
     def set_u(self, u):
-        u = np.ascontiguousarray(u, dtype=np.float64).reshape(self.N, 4)
+        u = np.ascontiguousarray(u, dtype=np.float64).reshape(self.N, self.nv)
         self._check(self.L.dndsg_set_u(self.h, _p(u), self.stream))
 
     def get_u(self, out: np.ndarray | None = None) -> np.ndarray:
-        u = np.empty((self.N, 4)) if out is None else out
+        u = np.empty((self.N, self.nv)) if out is None else out
         assert u.dtype == np.float64 and u.flags.c_contiguous and u.size == self.N * 4
         self._check(self.L.dndsg_get_u(self.h, _p(u), self.stream))
         return u
 
     def set_urec(self, r):
-        r = np.ascontiguousarray(r, dtype=np.float64).reshape(self.N, 5, 4)
+        r = np.ascontiguousarray(r, dtype=np.float64).reshape(self.N, 5, self.nv)
         self._check(self.L.dndsg_set_urec(self.h, _p(r), self.stream))
 
     def get_urec(self) -> np.ndarray:
-        r = np.empty((self.N, 5, 4))
+        r = np.empty((self.N, 5, self.nv))
         self._check(self.L.dndsg_get_urec(self.h, _p(r), self.stream))
         return r
 
@@ -133,7 +133,7 @@ class Solver:
         return dmin.value
 
     def EvaluateRHS(self, t: float = 0.0, copy: bool = True):
-        rhs = np.empty((self.N, 4)) if copy else None
+        rhs = np.empty((self.N, self.nv)) if copy else None
         self._check(self.L.dndsg_eval_rhs(self.h, float(t), _p(rhs) if copy else None, self.stream))
         return rhs
 
@@ -146,7 +146,7 @@ class Solver:
                                                   C.c_void_p(rhs_ptr), float(t), self.stream))
 
     def EvaluateResidual(self, p: int = 1, vol_wise: bool = False) -> np.ndarray:
-        out = np.empty(4)
+        out = np.empty(self.nv)
         self._check(self.L.dndsg_residual(self.h, int(p), int(vol_wise), _p(out), self.stream))
         return out
 
@@ -189,8 +189,8 @@ class Solver:
     def implicit_iteration(self, cfl: float, dt: float = 1e100, alpha_diag: float = 1.0, n_rec: int = 1,
                            vol_wise: bool = False, t: float = 0.0):
         """One first-order BDF pseudo-time iteration; returns (L1 norm of the increment, wall flux)."""
-        res = np.empty(4)
-        wf = np.empty(4)
+        res = np.empty(self.nv)
+        wf = np.empty(self.nv)
         self._check(self.L.dndsg_implicit_iteration(self.h, float(cfl), float(dt), float(alpha_diag), int(n_rec),
                                                     int(vol_wise), float(t), _p(res), _p(wf), self.stream))
         return res, wf
@@ -202,8 +202,8 @@ class Solver:
         Returns (iterations, relative residual, wall flux of the last iteration)."""
         self.bdf_begin()
         base = None
-        rel = np.ones(4)
-        wf = np.zeros(4)
+        rel = np.ones(self.nv)
+        wf = np.zeros(self.nv)
         it = 0
         for it in range(1, max_iter + 1):
             res, wf = self.implicit_iteration(cfl, dt, 1.0, n_rec, vol_wise)
@@ -217,7 +217,7 @@ class Solver:
 
     # ------------------------------------------------------------------ learned warm start
     def mlp_features(self, X_ptr: int, scales_ptr: int):
-        """Features [N][44] and scales [N][4] of the current state into device arrays."""
+        """Features [N][64] and scales [N][4] of the current state into device arrays."""
         self._check(self.L.dndsg_mlp_features(self.h, C.c_void_p(X_ptr), C.c_void_p(scales_ptr), self.stream))
 
     def vr_to_tolerance(self, tol: float, max_sweeps: int = 200, mlp=None, harvest_x: int = 0,
