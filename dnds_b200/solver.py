@@ -81,7 +81,7 @@ class Solver:
 
     def get_u(self, out: np.ndarray | None = None) -> np.ndarray:
         u = np.empty((self.N, self.nv)) if out is None else out
-        assert u.dtype == np.float64 and u.flags.c_contiguous and u.size == self.N * 4
+        assert u.dtype == np.float64 and u.flags.c_contiguous and u.size == self.N * self.nv
         self._check(self.L.dndsg_get_u(self.h, _p(u), self.stream))
         return u
 
