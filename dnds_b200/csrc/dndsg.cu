@@ -2315,6 +2315,82 @@ __global__ void __launch_bounds__(kBlock) k_lusgs_batch_sa(HotView<T> h, SaView<
   if (t < n) lusgs_cell_sa<T, FWD>(h, sa, rankOf, cells[t], alpha, Dinv, rhs, inc);
 }
 
+// the pipelined level walk of k_lusgs_levels_pipe with the U5 row: the neighbour records give
+// independent loads, and the next level's static data is requested before each barrier
+template <class T, bool FWD>
+__device__ __forceinline__ void lusgs_prefetch_sa(const HotView<T>& h, const SaView<T>& sa, const int32_t* cells,
+                                                  const int32_t* nbF, const int32_t* nbJ, int64_t t, double alpha,
+                                                  const double* Dinv, const double* rhs, LusgsPre& p, double uS[4],
+                                                  double& baseS, double& diS) {
+  lusgs_prefetch<T, FWD>(h, cells, nbF, nbJ, t, alpha, Dinv, rhs, p);
+  for (int k = 0; k < 4; k++) uS[k] = sa.u[p.j[k]];
+  baseS = FWD ? sa.rhs[p.i] : 0.0;
+  diS = sa.Dinv[p.i];
+}
+
+template <class T, bool FWD>
+__device__ __forceinline__ void lusgs_finish_sa(const HotView<T>& h, const SaView<T>& sa, const LusgsPre& p,
+                                                const double uS[4], double baseS, double diS, double* inc) {
+  double buf[4], bufS = baseS;
+  for (int v = 0; v < 4; v++) buf[v] = FWD ? p.base[v] : 0.0;
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    if (!p.use[q]) continue;
+    double dU[4], dF[4];
+    load4<T>(&inc[(int64_t)p.j[q] * 4], dU);
+    const double dS = sa.inc[p.j[q]];
+    flux_jac_times_du(p.U[q], p.nx[q], p.ny[q], dU, p.lam[q], h.gamma, dF);
+    const double* U = p.U[q];
+    const double ir = 1.0 / U[0];
+    const double vn = (U[1] * p.nx[q] + U[2] * p.ny[q]) * ir;
+    const double dvn = ((dU[1] - U[1] * ir * dU[0]) * p.nx[q] + (dU[2] - U[2] * ir * dU[0]) * p.ny[q]) * ir;
+    const double dFS = dS * vn + uS[q] * dvn - dS * p.lam[q];
+    for (int v = 0; v < 4; v++) buf[v] += p.w[q] * dF[v];
+    bufS += p.w[q] * dFS;
+  }
+  double* o = &inc[p.i * 4];
+  if (FWD) {
+    for (int v = 0; v < 4; v++) o[v] = p.di * buf[v];
+    sa.inc[p.i] = diS * bufS;
+  } else {
+    for (int v = 0; v < 4; v++) o[v] += p.di * buf[v];
+    sa.inc[p.i] += diS * bufS;
+  }
+}
+
+template <class T, bool FWD>
+__global__ void __launch_bounds__(kPipeBlock) k_lusgs_levels_pipe_sa(HotView<T> h, SaView<T> sa, const int32_t* nbF,
+                                                                     const int32_t* nbJ, const int32_t* cells,
+                                                                     const int64_t* off, int nlev, double alpha,
+                                                                     const double* Dinv, const double* rhs,
+                                                                     double* inc) {
+  __shared__ int64_t so[kPipeMaxLevels + 1];
+  for (int l = threadIdx.x; l <= nlev; l += blockDim.x) so[l] = off[l];
+  __syncthreads();
+  LusgsPre p;
+  double uS[4], baseS = 0, diS = 0;
+  bool have = false;
+  if (nlev > 0 && so[0] + threadIdx.x < so[1]) {
+    lusgs_prefetch_sa<T, FWD>(h, sa, cells, nbF, nbJ, so[0] + threadIdx.x, alpha, Dinv, rhs, p, uS, baseS, diS);
+    have = true;
+  }
+  for (int l = 0; l < nlev; l++) {
+    if (have) lusgs_finish_sa<T, FWD>(h, sa, p, uS, baseS, diS, inc);
+    for (int64_t t = so[l] + threadIdx.x + blockDim.x; t < so[l + 1]; t += blockDim.x) {
+      LusgsPre q;
+      double qS[4], qb, qd;
+      lusgs_prefetch_sa<T, FWD>(h, sa, cells, nbF, nbJ, t, alpha, Dinv, rhs, q, qS, qb, qd);
+      lusgs_finish_sa<T, FWD>(h, sa, q, qS, qb, qd, inc);
+    }
+    have = false;
+    if (l + 1 < nlev && so[l + 1] + threadIdx.x < so[l + 2]) {
+      lusgs_prefetch_sa<T, FWD>(h, sa, cells, nbF, nbJ, so[l + 1] + threadIdx.x, alpha, Dinv, rhs, p, uS, baseS, diS);
+      have = true;
+    }
+    __syncthreads();
+  }
+}
+
 // all narrow levels of one sweep in one block (as k_lusgs_levels), 5 variables
 template <class T, bool FWD>
 __global__ void __launch_bounds__(kLevelBlock) k_lusgs_levels_sa(HotView<T> h, SaView<T> sa, const int32_t* rankOf,
@@ -2408,6 +2484,16 @@ void launch_lusgs_sweep_sa(dndsg_ctx* c, bool forward, double alpha, cudaStream_
   const std::vector<int64_t>& off = forward ? c->fwdOff : c->bwdOff;
   const int32_t* cells = forward ? c->fwdCells : c->bwdCells;
   const int nb = (int)off.size() - 1;
+  if (c->lusgsOrder == 1 && nb <= kPipeMaxLevels && c->maxLevelWidth <= 8 * kPipeBlock && c->nfmax <= 4) {
+    const int64_t* od = forward ? c->fwdOffDev : c->bwdOffDev;
+    if (forward)
+      k_lusgs_levels_pipe_sa<T, true><<<1, kPipeBlock, 0, s>>>(h, sa, c->fwdNbF, c->fwdNbJ, cells, od, nb, alpha,
+                                                               c->Dinv, c->rhs, c->inc);
+    else
+      k_lusgs_levels_pipe_sa<T, false><<<1, kPipeBlock, 0, s>>>(h, sa, c->bwdNbF, c->bwdNbJ, cells, od, nb, alpha,
+                                                                c->Dinv, c->rhs, c->inc);
+    return;
+  }
   if (c->lusgsOrder == 1) {  // many narrow levels: one block walks them all
     const int64_t* od = forward ? c->fwdOffDev : c->bwdOffDev;
     if (forward)
