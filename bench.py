@@ -325,7 +325,7 @@ def learned_leg(dev, grid, tol=1e-7, log=None):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="dnds_b200", choices=["dnds_b200", "reference"])
     ap.add_argument("--no-accuracy", action="store_true")
