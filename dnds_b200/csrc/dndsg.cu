@@ -65,6 +65,7 @@ struct dndsg_ctx {
   std::vector<int64_t> fwdOff, bwdOff;
   int64_t *fwdOffDev = nullptr, *bwdOffDev = nullptr;  // level offsets on the device (scan-order mode)
   int32_t *fwdNbF = nullptr, *fwdNbJ = nullptr, *bwdNbF = nullptr, *bwdNbJ = nullptr;  // [pos][4] records
+  void* lusgsRec = nullptr;  // packed per-position records of one sweep (scan-order mode)
   int64_t maxLevelWidth = 0;
   std::vector<int32_t> colourHost;  // greedy colouring, kept for dndsg_lusgs_colours
   int lusgsOrder = 0;               // 0 colour batches, 1 level-scheduled scan order
@@ -1834,61 +1835,123 @@ __device__ __forceinline__ void lusgs_prefetch(const HotView<T>& h, const int32_
   }
 }
 
-template <class T, bool FWD>
-__device__ __forceinline__ void lusgs_finish(const HotView<T>& h, const LusgsPre& p, double* inc) {
-  double buf[4];
-  for (int v = 0; v < 4; v++) buf[v] = FWD ? p.base[v] : 0.0;
+constexpr int kRecMaxLevels = 4095;  // level offsets of one sweep held in shared memory
+
+// one schedule position of a level-scheduled sweep, everything but the neighbours' increments,
+// packed for a single contiguous copy (the U5 fields are used by SA contexts only)
+struct __align__(16) LuRec {
+  double U[4][4];
+  double nx[4], ny[4], lam[4], w[4];
+  double base[4];
+  double di;
+  double uS[4];
+  double baseS, diS;
+  int32_t i;
+  int32_t j[4];
+  int32_t use;
+  int32_t pad[4];
+};
+static_assert(sizeof(LuRec) == 384, "LuRec is copied in 16-byte pieces");
+
+// packs every schedule position of one sweep, all positions in parallel
+template <class T, bool FWD, bool SA>
+__global__ void __launch_bounds__(kBlock) k_lusgs_pack(HotView<T> h, SaView<T> sa, const int32_t* cells,
+                                                       const int32_t* nbF, const int32_t* nbJ, int64_t n, double alpha,
+                                                       const double* Dinv, const double* rhs, LuRec* rec) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  LusgsPre p;
+  lusgs_prefetch<T, FWD>(h, cells, nbF, nbJ, t, alpha, Dinv, rhs, p);
+  LuRec& r = rec[t];
+  int use = 0;
+  for (int k = 0; k < 4; k++) {
+    for (int v = 0; v < 4; v++) r.U[k][v] = p.U[k][v];
+    r.nx[k] = p.nx[k]; r.ny[k] = p.ny[k]; r.lam[k] = p.lam[k]; r.w[k] = p.w[k];
+    r.j[k] = p.j[k];
+    use |= p.use[k] ? 1 << k : 0;
+    r.uS[k] = SA ? sa.u[p.j[k]] : 0.0;
+  }
+  for (int v = 0; v < 4; v++) r.base[v] = FWD ? p.base[v] : 0.0;
+  r.di = p.di;
+  r.baseS = SA && FWD ? sa.rhs[p.i] : 0.0;
+  r.diS = SA ? sa.Dinv[p.i] : 0.0;
+  r.i = (int32_t)p.i;
+  r.use = use;
+}
+
+template <class T, bool FWD, bool SA>
+__device__ __forceinline__ void lusgs_finish_rec(const HotView<T>& h, const SaView<T>& sa, const LuRec& r,
+                                                 double* inc) {
+  double buf[4], bufS = r.baseS;
+  for (int v = 0; v < 4; v++) buf[v] = r.base[v];
 #pragma unroll
   for (int q = 0; q < 4; q++) {
-    if (!p.use[q]) continue;
-    double dU[4], dF[4];
-    load4<T>(&inc[(int64_t)p.j[q] * 4], dU);
-    flux_jac_times_du(p.U[q], p.nx[q], p.ny[q], dU, p.lam[q], h.gamma, dF);
-    for (int v = 0; v < 4; v++) buf[v] += p.w[q] * dF[v];
+    if (!(r.use >> q & 1)) continue;
+    double U[4], dU[4], dF[4];
+    for (int v = 0; v < 4; v++) U[v] = r.U[q][v];
+    load4<T>(&inc[(int64_t)r.j[q] * 4], dU);
+    flux_jac_times_du(U, r.nx[q], r.ny[q], dU, r.lam[q], h.gamma, dF);
+    for (int v = 0; v < 4; v++) buf[v] += r.w[q] * dF[v];
+    if (SA) {
+      const double ir = 1.0 / U[0];
+      const double vn = (U[1] * r.nx[q] + U[2] * r.ny[q]) * ir;
+      const double dvn = ((dU[1] - U[1] * ir * dU[0]) * r.nx[q] + (dU[2] - U[2] * ir * dU[0]) * r.ny[q]) * ir;
+      const double dS = sa.inc[r.j[q]];
+      bufS += r.w[q] * (dS * vn + r.uS[q] * dvn - dS * r.lam[q]);
+    }
   }
-  double* o = &inc[p.i * 4];
+  double* o = &inc[(int64_t)r.i * 4];
   if (FWD) {
-    for (int v = 0; v < 4; v++) o[v] = p.di * buf[v];
+    for (int v = 0; v < 4; v++) o[v] = r.di * buf[v];
+    if (SA) sa.inc[r.i] = r.diS * bufS;
   } else {
-    for (int v = 0; v < 4; v++) o[v] += p.di * buf[v];
+    for (int v = 0; v < 4; v++) o[v] += r.di * buf[v];
+    if (SA) sa.inc[r.i] += r.diS * bufS;
   }
 }
 
-// a whole sweep of narrow dependency levels in one thread block, software-pipelined: before the
-// barrier that ends a level, each thread requests what its cell of the next level needs (all but
-// the neighbours' fresh increments), so after the barrier one dependent load per neighbour is
-// left.  Level offsets sit in shared memory.
-constexpr int kPipeBlock = 256, kPipeMaxLevels = 4095;
-template <class T, bool FWD>
-__global__ void __launch_bounds__(kPipeBlock) k_lusgs_levels_pipe(HotView<T> h, const int32_t* nbF,
-                                                                  const int32_t* nbJ, const int32_t* cells,
-                                                                  const int64_t* off,
-                                                                  int nlev, double alpha, const double* Dinv,
-                                                                  const double* rhs, double* inc) {
-  __shared__ int64_t so[kPipeMaxLevels + 1];
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// a whole level-scheduled sweep in one block over packed records: while level l is finished, the
+// records of level l + 1 stream into the other half of a shared-memory double buffer by
+// asynchronous copies (each thread copies and later reads only its own record, so waiting for its
+// own copy group is enough); the block barrier per level publishes the increments
+constexpr int kRecBlock = 128;
+constexpr size_t kRecSmem = sizeof(int64_t) * (kRecMaxLevels + 1) + sizeof(LuRec) * 2 * kRecBlock;
+template <class T, bool FWD, bool SA>
+__global__ void __launch_bounds__(kRecBlock) k_lusgs_levels_rec(HotView<T> h, SaView<T> sa, const LuRec* rec,
+                                                                const int64_t* off, int nlev, double* inc) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  int64_t* so = reinterpret_cast<int64_t*>(smraw);
+  LuRec* buf = reinterpret_cast<LuRec*>(smraw + sizeof(int64_t) * (kRecMaxLevels + 1));
   for (int l = threadIdx.x; l <= nlev; l += blockDim.x) so[l] = off[l];
   __syncthreads();
-  LusgsPre p;
-  bool have = false;
-  if (nlev > 0 && so[0] + threadIdx.x < so[1]) {
-    lusgs_prefetch<T, FWD>(h, cells, nbF, nbJ, so[0] + threadIdx.x, alpha, Dinv, rhs, p);
-    have = true;
-  }
+  const int tid = threadIdx.x;
+  auto issue = [&](int l) {
+    if (l < nlev) {
+      const int64_t t = so[l] + tid;
+      if (t < so[l + 1]) {
+        const char* src = reinterpret_cast<const char*>(&rec[t]);
+        char* dst = reinterpret_cast<char*>(&buf[(l & 1) * kRecBlock + tid]);
+        for (int k = 0; k < (int)(sizeof(LuRec) / 16); k++) cp_async16(dst + 16 * k, src + 16 * k);
+      }
+    }
+    cp_async_commit();
+  };
+  issue(0);
   for (int l = 0; l < nlev; l++) {
-    if (have) lusgs_finish<T, FWD>(h, p, inc);
-    for (int64_t t = so[l] + threadIdx.x + blockDim.x; t < so[l + 1]; t += blockDim.x) {
-      LusgsPre q;
-      lusgs_prefetch<T, FWD>(h, cells, nbF, nbJ, t, alpha, Dinv, rhs, q);
-      lusgs_finish<T, FWD>(h, q, inc);
-    }
-    // the next level's static data, requested before the barrier
-    have = false;
-    if (l + 1 < nlev && so[l + 1] + threadIdx.x < so[l + 2]) {
-      lusgs_prefetch<T, FWD>(h, cells, nbF, nbJ, so[l + 1] + threadIdx.x, alpha, Dinv, rhs, p);
-      have = true;
-    }
+    issue(l + 1);
+    cp_async_wait1();
+    if (so[l] + tid < so[l + 1]) lusgs_finish_rec<T, FWD, SA>(h, sa, buf[(l & 1) * kRecBlock + tid], inc);
+    for (int64_t t = so[l] + tid + kRecBlock; t < so[l + 1]; t += kRecBlock) lusgs_finish_rec<T, FWD, SA>(h, sa, rec[t], inc);
     __syncthreads();
   }
+  cp_async_wait0();
 }
 
 // a whole sweep of narrow batches (dependency levels) in one thread block: the levels run one
@@ -2104,6 +2167,12 @@ int set_scan_order(dndsg_ctx* c, const int64_t* scan2cell) {
   DG_CUDA(c, cudaMemcpy(c->fwdNbJ, fj.data(), sizeof(int32_t) * 4 * N, cudaMemcpyHostToDevice));
   DG_CUDA(c, cudaMemcpy(c->bwdNbF, bf.data(), sizeof(int32_t) * 4 * N, cudaMemcpyHostToDevice));
   DG_CUDA(c, cudaMemcpy(c->bwdNbJ, bj.data(), sizeof(int32_t) * 4 * N, cudaMemcpyHostToDevice));
+  if (!c->lusgsRec && (rc = dalloc(c, c->lusgsRec, sizeof(LuRec) * N))) return rc;
+  for (const void* fn : {(const void*)k_lusgs_levels_rec<float, true, false>, (const void*)k_lusgs_levels_rec<float, false, false>,
+                         (const void*)k_lusgs_levels_rec<float, true, true>, (const void*)k_lusgs_levels_rec<float, false, true>,
+                         (const void*)k_lusgs_levels_rec<double, true, false>, (const void*)k_lusgs_levels_rec<double, false, false>,
+                         (const void*)k_lusgs_levels_rec<double, true, true>, (const void*)k_lusgs_levels_rec<double, false, true>})
+    DG_CUDA(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRecSmem));
   c->lusgsOrder = 1;
   return upload_schedule(c, pos, fwd, bwd);
 }
@@ -2114,15 +2183,21 @@ void launch_lusgs_sweep(dndsg_ctx* c, bool forward, double alpha, const double* 
   const std::vector<int64_t>& off = forward ? c->fwdOff : c->bwdOff;
   const int32_t* cells = forward ? c->fwdCells : c->bwdCells;
   const int nb = (int)off.size() - 1;
-  // many narrow levels: one block walks them all (a launch per level would cost more than the work)
-  if (c->lusgsOrder == 1 && nb <= kPipeMaxLevels && c->maxLevelWidth <= 8 * kPipeBlock && c->nfmax <= 4) {
+  // many narrow levels: one block walks them all over records packed in parallel beforehand
+  // (a launch per level would cost more than the work)
+  if (c->lusgsOrder == 1 && nb <= kRecMaxLevels && c->nfmax <= 4) {
     const int64_t* od = forward ? c->fwdOffDev : c->bwdOffDev;
-    if (forward)
-      k_lusgs_levels_pipe<T, true><<<1, kPipeBlock, 0, s>>>(h, c->fwdNbF, c->fwdNbJ, cells, od, nb, alpha, c->Dinv,
-                                                            rhs, inc);
-    else
-      k_lusgs_levels_pipe<T, false><<<1, kPipeBlock, 0, s>>>(h, c->bwdNbF, c->bwdNbJ, cells, od, nb, alpha, c->Dinv,
-                                                             rhs, inc);
+    const int32_t* nf = forward ? c->fwdNbF : c->bwdNbF;
+    const int32_t* nj = forward ? c->fwdNbJ : c->bwdNbJ;
+    SaView<T> none{};
+    LuRec* rec = (LuRec*)c->lusgsRec;
+    if (forward) {
+      k_lusgs_pack<T, true, false><<<grid_for(c->N), kBlock, 0, s>>>(h, none, cells, nf, nj, c->N, alpha, c->Dinv, rhs, rec);
+      k_lusgs_levels_rec<T, true, false><<<1, kRecBlock, kRecSmem, s>>>(h, none, rec, od, nb, inc);
+    } else {
+      k_lusgs_pack<T, false, false><<<grid_for(c->N), kBlock, 0, s>>>(h, none, cells, nf, nj, c->N, alpha, c->Dinv, rhs, rec);
+      k_lusgs_levels_rec<T, false, false><<<1, kRecBlock, kRecSmem, s>>>(h, none, rec, od, nb, inc);
+    }
     return;
   }
   if (c->lusgsOrder == 1 && c->maxLevelWidth <= 8 * kLevelBlock) {
@@ -2315,82 +2390,6 @@ __global__ void __launch_bounds__(kBlock) k_lusgs_batch_sa(HotView<T> h, SaView<
   if (t < n) lusgs_cell_sa<T, FWD>(h, sa, rankOf, cells[t], alpha, Dinv, rhs, inc);
 }
 
-// the pipelined level walk of k_lusgs_levels_pipe with the U5 row: the neighbour records give
-// independent loads, and the next level's static data is requested before each barrier
-template <class T, bool FWD>
-__device__ __forceinline__ void lusgs_prefetch_sa(const HotView<T>& h, const SaView<T>& sa, const int32_t* cells,
-                                                  const int32_t* nbF, const int32_t* nbJ, int64_t t, double alpha,
-                                                  const double* Dinv, const double* rhs, LusgsPre& p, double uS[4],
-                                                  double& baseS, double& diS) {
-  lusgs_prefetch<T, FWD>(h, cells, nbF, nbJ, t, alpha, Dinv, rhs, p);
-  for (int k = 0; k < 4; k++) uS[k] = sa.u[p.j[k]];
-  baseS = FWD ? sa.rhs[p.i] : 0.0;
-  diS = sa.Dinv[p.i];
-}
-
-template <class T, bool FWD>
-__device__ __forceinline__ void lusgs_finish_sa(const HotView<T>& h, const SaView<T>& sa, const LusgsPre& p,
-                                                const double uS[4], double baseS, double diS, double* inc) {
-  double buf[4], bufS = baseS;
-  for (int v = 0; v < 4; v++) buf[v] = FWD ? p.base[v] : 0.0;
-#pragma unroll
-  for (int q = 0; q < 4; q++) {
-    if (!p.use[q]) continue;
-    double dU[4], dF[4];
-    load4<T>(&inc[(int64_t)p.j[q] * 4], dU);
-    const double dS = sa.inc[p.j[q]];
-    flux_jac_times_du(p.U[q], p.nx[q], p.ny[q], dU, p.lam[q], h.gamma, dF);
-    const double* U = p.U[q];
-    const double ir = 1.0 / U[0];
-    const double vn = (U[1] * p.nx[q] + U[2] * p.ny[q]) * ir;
-    const double dvn = ((dU[1] - U[1] * ir * dU[0]) * p.nx[q] + (dU[2] - U[2] * ir * dU[0]) * p.ny[q]) * ir;
-    const double dFS = dS * vn + uS[q] * dvn - dS * p.lam[q];
-    for (int v = 0; v < 4; v++) buf[v] += p.w[q] * dF[v];
-    bufS += p.w[q] * dFS;
-  }
-  double* o = &inc[p.i * 4];
-  if (FWD) {
-    for (int v = 0; v < 4; v++) o[v] = p.di * buf[v];
-    sa.inc[p.i] = diS * bufS;
-  } else {
-    for (int v = 0; v < 4; v++) o[v] += p.di * buf[v];
-    sa.inc[p.i] += diS * bufS;
-  }
-}
-
-template <class T, bool FWD>
-__global__ void __launch_bounds__(kPipeBlock) k_lusgs_levels_pipe_sa(HotView<T> h, SaView<T> sa, const int32_t* nbF,
-                                                                     const int32_t* nbJ, const int32_t* cells,
-                                                                     const int64_t* off, int nlev, double alpha,
-                                                                     const double* Dinv, const double* rhs,
-                                                                     double* inc) {
-  __shared__ int64_t so[kPipeMaxLevels + 1];
-  for (int l = threadIdx.x; l <= nlev; l += blockDim.x) so[l] = off[l];
-  __syncthreads();
-  LusgsPre p;
-  double uS[4], baseS = 0, diS = 0;
-  bool have = false;
-  if (nlev > 0 && so[0] + threadIdx.x < so[1]) {
-    lusgs_prefetch_sa<T, FWD>(h, sa, cells, nbF, nbJ, so[0] + threadIdx.x, alpha, Dinv, rhs, p, uS, baseS, diS);
-    have = true;
-  }
-  for (int l = 0; l < nlev; l++) {
-    if (have) lusgs_finish_sa<T, FWD>(h, sa, p, uS, baseS, diS, inc);
-    for (int64_t t = so[l] + threadIdx.x + blockDim.x; t < so[l + 1]; t += blockDim.x) {
-      LusgsPre q;
-      double qS[4], qb, qd;
-      lusgs_prefetch_sa<T, FWD>(h, sa, cells, nbF, nbJ, t, alpha, Dinv, rhs, q, qS, qb, qd);
-      lusgs_finish_sa<T, FWD>(h, sa, q, qS, qb, qd, inc);
-    }
-    have = false;
-    if (l + 1 < nlev && so[l + 1] + threadIdx.x < so[l + 2]) {
-      lusgs_prefetch_sa<T, FWD>(h, sa, cells, nbF, nbJ, so[l + 1] + threadIdx.x, alpha, Dinv, rhs, p, uS, baseS, diS);
-      have = true;
-    }
-    __syncthreads();
-  }
-}
-
 // all narrow levels of one sweep in one block (as k_lusgs_levels), 5 variables
 template <class T, bool FWD>
 __global__ void __launch_bounds__(kLevelBlock) k_lusgs_levels_sa(HotView<T> h, SaView<T> sa, const int32_t* rankOf,
@@ -2484,14 +2483,18 @@ void launch_lusgs_sweep_sa(dndsg_ctx* c, bool forward, double alpha, cudaStream_
   const std::vector<int64_t>& off = forward ? c->fwdOff : c->bwdOff;
   const int32_t* cells = forward ? c->fwdCells : c->bwdCells;
   const int nb = (int)off.size() - 1;
-  if (c->lusgsOrder == 1 && nb <= kPipeMaxLevels && c->maxLevelWidth <= 8 * kPipeBlock && c->nfmax <= 4) {
+  if (c->lusgsOrder == 1 && nb <= kRecMaxLevels && c->nfmax <= 4) {
     const int64_t* od = forward ? c->fwdOffDev : c->bwdOffDev;
-    if (forward)
-      k_lusgs_levels_pipe_sa<T, true><<<1, kPipeBlock, 0, s>>>(h, sa, c->fwdNbF, c->fwdNbJ, cells, od, nb, alpha,
-                                                               c->Dinv, c->rhs, c->inc);
-    else
-      k_lusgs_levels_pipe_sa<T, false><<<1, kPipeBlock, 0, s>>>(h, sa, c->bwdNbF, c->bwdNbJ, cells, od, nb, alpha,
-                                                                c->Dinv, c->rhs, c->inc);
+    const int32_t* nf = forward ? c->fwdNbF : c->bwdNbF;
+    const int32_t* nj = forward ? c->fwdNbJ : c->bwdNbJ;
+    LuRec* rec = (LuRec*)c->lusgsRec;
+    if (forward) {
+      k_lusgs_pack<T, true, true><<<grid_for(c->N), kBlock, 0, s>>>(h, sa, cells, nf, nj, c->N, alpha, c->Dinv, c->rhs, rec);
+      k_lusgs_levels_rec<T, true, true><<<1, kRecBlock, kRecSmem, s>>>(h, sa, rec, od, nb, c->inc);
+    } else {
+      k_lusgs_pack<T, false, true><<<grid_for(c->N), kBlock, 0, s>>>(h, sa, cells, nf, nj, c->N, alpha, c->Dinv, c->rhs, rec);
+      k_lusgs_levels_rec<T, false, true><<<1, kRecBlock, kRecSmem, s>>>(h, sa, rec, od, nb, c->inc);
+    }
     return;
   }
   if (c->lusgsOrder == 1) {  // many narrow levels: one block walks them all
