@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/dndsg.h"
@@ -65,7 +66,8 @@ struct dndsg_ctx {
   std::vector<int64_t> fwdOff, bwdOff;
   int64_t *fwdOffDev = nullptr, *bwdOffDev = nullptr;  // level offsets on the device (scan-order mode)
   int32_t *fwdNbF = nullptr, *fwdNbJ = nullptr, *bwdNbF = nullptr, *bwdNbJ = nullptr;  // [pos][4] records
-  void* lusgsRec = nullptr;  // packed per-position records of one sweep (scan-order mode)
+  void* lusgsMat = nullptr;  // per-position neighbour-matrix records of one sweep (scan-order mode)
+  int32_t *fwdNbP = nullptr, *bwdNbP = nullptr;  // [pos][4] neighbour schedule positions
   int64_t maxLevelWidth = 0;
   std::vector<int32_t> colourHost;  // greedy colouring, kept for dndsg_lusgs_colours
   int lusgsOrder = 0;               // 0 colour batches, 1 level-scheduled scan order
@@ -1837,121 +1839,204 @@ __device__ __forceinline__ void lusgs_prefetch(const HotView<T>& h, const int32_
 
 constexpr int kRecMaxLevels = 4095;  // level offsets of one sweep held in shared memory
 
-// one schedule position of a level-scheduled sweep, everything but the neighbours' increments,
-// packed for a single contiguous copy (the U5 fields are used by SA contexts only)
-struct __align__(16) LuRec {
-  double U[4][4];
-  double nx[4], ny[4], lam[4], w[4];
-  double base[4];
+// ---- scan-order sweep over precomputed neighbour matrices.
+// The neighbour term of UpdateLUSGSForward/Backward, w_q (dF(U_q; n_q, dU_q) - lam_q dU_q)
+// (fluxJacobian0_Right_Times_du, DNDS_FV_EulerEvaluator.hpp:928-956), is linear in the neighbour's
+// increment dU_q, and its matrix depends only on data that is fixed during the sweep.  So one
+// parallel pass writes, per schedule position, the 4x4 matrices of its up to 4 neighbours (plus the
+// U5 transport row for SA contexts), and the sequential level walk is left with matrix-vector
+// products over increments that mostly sit in a shared-memory ring.
+struct __align__(16) LuMatF {
+  double M[4][16];  // per face slot: row-major w (A_n(U) - lam I)
+  double base[4];   // initial sum: the BDF rhs (forward) or 0 (backward)
+  double add[4];    // added to di * sum: 0 (forward) or the forward increment (backward)
   double di;
-  double uS[4];
-  double baseS, diS;
-  int32_t i;
-  int32_t j[4];
-  int32_t use;
-  int32_t pad[4];
+  int32_t i, use;   // cell; bit k set when slot k holds a neighbour that enters this sweep
+  int32_t j[4];     // neighbour cell
+  int32_t p[4];     // neighbour schedule position in this sweep
 };
-static_assert(sizeof(LuRec) == 384, "LuRec is copied in 16-byte pieces");
+struct __align__(16) LuMatS {
+  LuMatF f;
+  double S[4][4];  // per face slot: coefficients of dU0, dU1, dU2 and dU5 in the U5 row
+  double baseS, addS, diS, padS;
+};
+static_assert(sizeof(LuMatF) == 624 && sizeof(LuMatS) == 784, "records are bulk-copied in 16-byte units");
+template <bool SA>
+using LuMat = typename std::conditional<SA, LuMatS, LuMatF>::type;
+__device__ __forceinline__ LuMatF& mat_flow(LuMatF& r) { return r; }
+__device__ __forceinline__ LuMatF& mat_flow(LuMatS& r) { return r.f; }
+__device__ __forceinline__ const LuMatF& mat_flow(const LuMatF& r) { return r; }
+__device__ __forceinline__ const LuMatF& mat_flow(const LuMatS& r) { return r.f; }
 
-// packs every schedule position of one sweep, all positions in parallel
+// w (A_n(U) - lam I), the matrix of flux_jac_times_du: with q2 = |v|^2, H = (E + p)/rho,
+// dp = (gamma - 1)(dU3 - vx dU1 - vy dU2 + q2/2 dU0) and dvn = (nx dU1 + ny dU2 - vn dU0)/rho
+__device__ __forceinline__ void flux_jac_matrix(const double U[4], double nx, double ny, double lam, double w,
+                                                double gamma, double* M) {
+  const double ir = 1.0 / U[0];
+  const double vx = U[1] * ir, vy = U[2] * ir, q2 = vx * vx + vy * vy, g1 = gamma - 1;
+  const double p = g1 * (U[3] - 0.5 * U[0] * q2), H = (U[3] + p) * ir, vn = vx * nx + vy * ny, k = 0.5 * g1 * q2;
+  const double m[16] = {-lam, nx, ny, 0.0,
+                        k * nx - vx * vn, vn + vx * nx - g1 * vx * nx - lam, vx * ny - g1 * vy * nx, g1 * nx,
+                        k * ny - vy * vn, vy * nx - g1 * vx * ny, vn + vy * ny - g1 * vy * ny - lam, g1 * ny,
+                        vn * (k - H), H * nx - g1 * vx * vn, H * ny - g1 * vy * vn, gamma * vn - lam};
+  for (int e = 0; e < 16; e++) M[e] = w * m[e];
+}
+
+// writes the record of every schedule position of one sweep, all positions in parallel
 template <class T, bool FWD, bool SA>
-__global__ void __launch_bounds__(kBlock) k_lusgs_pack(HotView<T> h, SaView<T> sa, const int32_t* cells,
-                                                       const int32_t* nbF, const int32_t* nbJ, int64_t n, double alpha,
-                                                       const double* Dinv, const double* rhs, LuRec* rec) {
+__global__ void __launch_bounds__(kBlock) k_lusgs_pack_mat(HotView<T> h, SaView<T> sa, const int32_t* cells,
+                                                           const int32_t* nbF, const int32_t* nbJ, const int32_t* nbP,
+                                                           int64_t n, double alpha, const double* Dinv,
+                                                           const double* rhs, const double* inc, LuMat<SA>* rec) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (t >= n) return;
   LusgsPre p;
   lusgs_prefetch<T, FWD>(h, cells, nbF, nbJ, t, alpha, Dinv, rhs, p);
-  LuRec& r = rec[t];
+  LuMatF& f = mat_flow(rec[t]);
+  const int4 p4 = reinterpret_cast<const int4*>(nbP)[t];
+  const int32_t pa[4] = {p4.x, p4.y, p4.z, p4.w};
   int use = 0;
   for (int k = 0; k < 4; k++) {
-    for (int v = 0; v < 4; v++) r.U[k][v] = p.U[k][v];
-    r.nx[k] = p.nx[k]; r.ny[k] = p.ny[k]; r.lam[k] = p.lam[k]; r.w[k] = p.w[k];
-    r.j[k] = p.j[k];
+    flux_jac_matrix(p.U[k], p.nx[k], p.ny[k], p.lam[k], p.w[k], h.gamma, f.M[k]);
+    f.j[k] = p.j[k];
+    f.p[k] = pa[k];
     use |= p.use[k] ? 1 << k : 0;
-    r.uS[k] = SA ? sa.u[p.j[k]] : 0.0;
   }
-  for (int v = 0; v < 4; v++) r.base[v] = FWD ? p.base[v] : 0.0;
-  r.di = p.di;
-  r.baseS = SA && FWD ? sa.rhs[p.i] : 0.0;
-  r.diS = SA ? sa.Dinv[p.i] : 0.0;
-  r.i = (int32_t)p.i;
-  r.use = use;
+  double add[4] = {0, 0, 0, 0};
+  if (!FWD) load4<double>(&inc[p.i * 4], add);
+  for (int v = 0; v < 4; v++) {
+    f.base[v] = FWD ? p.base[v] : 0.0;
+    f.add[v] = add[v];
+  }
+  f.di = p.di;
+  f.i = (int32_t)p.i;
+  f.use = use;
+  if constexpr (SA) {
+    LuMatS& r = rec[t];
+    for (int k = 0; k < 4; k++) {
+      const double* U = p.U[k];
+      const double ir = 1.0 / U[0];
+      const double vn = (U[1] * p.nx[k] + U[2] * p.ny[k]) * ir, c = p.w[k] * sa.u[p.j[k]] * ir;
+      r.S[k][0] = -c * vn;
+      r.S[k][1] = c * p.nx[k];
+      r.S[k][2] = c * p.ny[k];
+      r.S[k][3] = p.w[k] * (vn - p.lam[k]);
+    }
+    r.baseS = FWD ? sa.rhs[p.i] : 0.0;
+    r.addS = FWD ? 0.0 : sa.inc[p.i];
+    r.diS = sa.Dinv[p.i];
+    r.padS = 0.0;
+  }
 }
 
-template <class T, bool FWD, bool SA>
-__device__ __forceinline__ void lusgs_finish_rec(const HotView<T>& h, const SaView<T>& sa, const LuRec& r,
-                                                 double* inc) {
-  double buf[4], bufS = r.baseS;
-  for (int v = 0; v < 4; v++) buf[v] = r.base[v];
+constexpr int kRecBlock = 128;  // threads of the level walk, and records buffered per level
+constexpr int kMatRing = 256;   // increments of the most recent schedule positions kept in shared memory
+constexpr uint32_t kBulkChunk = 16384;
+template <bool SA>
+constexpr size_t mat_smem() {
+  return 16 + sizeof(int32_t) * (kRecMaxLevels + 1) + sizeof(double) * kMatRing * (SA ? 5 : 4) +
+         sizeof(LuMat<SA>) * 2 * kRecBlock;
+}
+static_assert(mat_smem<true>() <= 227 * 1024, "level walk fits the shared memory of one block");
+
+// one position of the level walk.  A neighbour's increment comes from the ring when its position
+// is at or after ringLo (it was written there by this walk and not yet overwritten), else from
+// global memory.  The sum runs over the slots in the order of lusgs_cell.
+template <bool FWD, bool SA, class T>
+__device__ __forceinline__ void lusgs_mat_cell(const SaView<T>& sa, const LuMat<SA>& r, int32_t t, int32_t ringLo,
+                                               double* ringF, double* ringS, double* inc) {
+  const LuMatF& f = mat_flow(r);
+  double buf[4], bufS = 0.0;
+  for (int v = 0; v < 4; v++) buf[v] = f.base[v];
+  if constexpr (SA) bufS = r.baseS;
 #pragma unroll
   for (int q = 0; q < 4; q++) {
-    if (!(r.use >> q & 1)) continue;
-    double U[4], dU[4], dF[4];
-    for (int v = 0; v < 4; v++) U[v] = r.U[q][v];
-    load4<T>(&inc[(int64_t)r.j[q] * 4], dU);
-    flux_jac_times_du(U, r.nx[q], r.ny[q], dU, r.lam[q], h.gamma, dF);
-    for (int v = 0; v < 4; v++) buf[v] += r.w[q] * dF[v];
-    if (SA) {
-      const double ir = 1.0 / U[0];
-      const double vn = (U[1] * r.nx[q] + U[2] * r.ny[q]) * ir;
-      const double dvn = ((dU[1] - U[1] * ir * dU[0]) * r.nx[q] + (dU[2] - U[2] * ir * dU[0]) * r.ny[q]) * ir;
-      const double dS = sa.inc[r.j[q]];
-      bufS += r.w[q] * (dS * vn + r.uS[q] * dvn - dS * r.lam[q]);
+    if (!(f.use >> q & 1)) continue;
+    const int32_t pj = f.p[q];
+    double dU[4], dS = 0.0;
+    if (pj >= ringLo) {
+      const double2* s = reinterpret_cast<const double2*>(ringF + 4 * (pj % kMatRing));
+      const double2 a = s[0], b = s[1];
+      dU[0] = a.x; dU[1] = a.y; dU[2] = b.x; dU[3] = b.y;
+      if constexpr (SA) dS = ringS[pj % kMatRing];
+    } else {
+      load4<double>(&inc[(int64_t)f.j[q] * 4], dU);
+      if constexpr (SA) dS = sa.inc[f.j[q]];
     }
+    const double* M = f.M[q];
+    for (int v = 0; v < 4; v++) buf[v] += M[4 * v] * dU[0] + M[4 * v + 1] * dU[1] + M[4 * v + 2] * dU[2] + M[4 * v + 3] * dU[3];
+    if constexpr (SA) bufS += r.S[q][0] * dU[0] + r.S[q][1] * dU[1] + r.S[q][2] * dU[2] + r.S[q][3] * dS;
   }
-  double* o = &inc[(int64_t)r.i * 4];
-  if (FWD) {
-    for (int v = 0; v < 4; v++) o[v] = r.di * buf[v];
-    if (SA) sa.inc[r.i] = r.diS * bufS;
-  } else {
-    for (int v = 0; v < 4; v++) o[v] += r.di * buf[v];
-    if (SA) sa.inc[r.i] += r.diS * bufS;
+  double o[4];
+  for (int v = 0; v < 4; v++) o[v] = f.add[v] + f.di * buf[v];
+  double2* g = reinterpret_cast<double2*>(&inc[(int64_t)f.i * 4]);
+  double2* s = reinterpret_cast<double2*>(ringF + 4 * (t % kMatRing));
+  g[0] = s[0] = make_double2(o[0], o[1]);
+  g[1] = s[1] = make_double2(o[2], o[3]);
+  if constexpr (SA) {
+    const double oS = r.addS + r.diS * bufS;
+    sa.inc[f.i] = oS;
+    ringS[t % kMatRing] = oS;
   }
 }
 
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
-// a whole level-scheduled sweep in one block over packed records: while level l is finished, the
-// records of level l + 1 stream into the other half of a shared-memory double buffer by
-// asynchronous copies (each thread copies and later reads only its own record, so waiting for its
-// own copy group is enough); the block barrier per level publishes the increments
-constexpr int kRecBlock = 128;
-constexpr size_t kRecSmem = sizeof(int64_t) * (kRecMaxLevels + 1) + sizeof(LuRec) * 2 * kRecBlock;
+// a whole level-scheduled sweep in one block.  One thread bulk-copies the next level's records
+// (contiguous in schedule order) into the other half of a shared-memory double buffer on an
+// mbarrier while the block finishes the current level; the block barrier per level publishes the
+// increments (global memory and the ring).  Positions of a level beyond kRecBlock read their
+// records from global memory.  A bulk copy that does not land in time sets kFlagTimeout and ends
+// the walk.
 template <class T, bool FWD, bool SA>
-__global__ void __launch_bounds__(kRecBlock) k_lusgs_levels_rec(HotView<T> h, SaView<T> sa, const LuRec* rec,
-                                                                const int64_t* off, int nlev, double* inc) {
+__global__ void __launch_bounds__(kRecBlock) k_lusgs_levels_mat(SaView<T> sa, const LuMat<SA>* rec,
+                                                                const int64_t* off, int nlev, double* inc,
+                                                                unsigned* flags) {
+  using R = LuMat<SA>;
   extern __shared__ __align__(16) unsigned char smraw[];
-  int64_t* so = reinterpret_cast<int64_t*>(smraw);
-  LuRec* buf = reinterpret_cast<LuRec*>(smraw + sizeof(int64_t) * (kRecMaxLevels + 1));
-  for (int l = threadIdx.x; l <= nlev; l += blockDim.x) so[l] = off[l];
-  __syncthreads();
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smraw);
+  int32_t* so = reinterpret_cast<int32_t*>(smraw + 16);
+  double* ringF = reinterpret_cast<double*>(smraw + 16 + sizeof(int32_t) * (kRecMaxLevels + 1));
+  double* ringS = ringF + 4 * kMatRing;
+  R* buf = reinterpret_cast<R*>(ringS + (SA ? kMatRing : 0));
   const int tid = threadIdx.x;
-  auto issue = [&](int l) {
-    if (l < nlev) {
-      const int64_t t = so[l] + tid;
-      if (t < so[l + 1]) {
-        const char* src = reinterpret_cast<const char*>(&rec[t]);
-        char* dst = reinterpret_cast<char*>(&buf[(l & 1) * kRecBlock + tid]);
-        for (int k = 0; k < (int)(sizeof(LuRec) / 16); k++) cp_async16(dst + 16 * k, src + 16 * k);
-      }
-    }
-    cp_async_commit();
-  };
-  issue(0);
-  for (int l = 0; l < nlev; l++) {
-    issue(l + 1);
-    cp_async_wait1();
-    if (so[l] + tid < so[l + 1]) lusgs_finish_rec<T, FWD, SA>(h, sa, buf[(l & 1) * kRecBlock + tid], inc);
-    for (int64_t t = so[l] + tid + kRecBlock; t < so[l + 1]; t += kRecBlock) lusgs_finish_rec<T, FWD, SA>(h, sa, rec[t], inc);
-    __syncthreads();
+  for (int l = tid; l <= nlev; l += blockDim.x) so[l] = (int32_t)off[l];
+  if (tid == 0) {
+    mbar_init(smem_u32(&bars[0]), 1);
+    mbar_init(smem_u32(&bars[1]), 1);
+    fence_mbar_init();
   }
-  cp_async_wait0();
+  __syncthreads();
+  auto issue = [&](int l) {  // thread 0
+    const int32_t b = so[l];
+    const int32_t n = min(so[l + 1] - b, kRecBlock);
+    const uint32_t bar = smem_u32(&bars[l & 1]), bytes = (uint32_t)(n * sizeof(R));
+    const uint32_t dst = smem_u32(buf + (l & 1) * kRecBlock);
+    const char* src = reinterpret_cast<const char*>(rec + b);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(bar, bytes);
+    for (uint32_t o = 0; o < bytes; o += kBulkChunk) bulk_g2s(dst + o, src + o, min(kBulkChunk, bytes - o), bar);
+  };
+  if (tid == 0 && nlev > 0) issue(0);
+  int lo = 0, l = 0;
+  bool failed = false;
+  for (; l < nlev; l++) {
+    if (tid == 0 && l + 1 < nlev) issue(l + 1);
+    while (so[l + 1] - so[lo] > kMatRing) lo++;
+    const int32_t ringLo = so[lo], b = so[l], e = so[l + 1];
+    const bool ok = mbar_wait(smem_u32(&bars[l & 1]), (l >> 1) & 1, kWaitLimit);
+    if (ok)
+      for (int32_t t = b + tid; t < e; t += kRecBlock)
+        lusgs_mat_cell<FWD, SA>(sa, t - b < kRecBlock ? buf[(l & 1) * kRecBlock + (t - b)] : rec[t], t, ringLo, ringF,
+                                ringS, inc);
+    if (__syncthreads_or(!ok)) {
+      failed = true;
+      break;
+    }
+  }
+  if (failed && tid == 0) {  // let the copies in flight land before the block exits
+    atomicOr(flags, kFlagTimeout);
+    mbar_wait(smem_u32(&bars[l & 1]), (l >> 1) & 1, kWaitLimit);
+    if (l + 1 < nlev) mbar_wait(smem_u32(&bars[(l + 1) & 1]), ((l + 1) >> 1) & 1, kWaitLimit);
+  }
 }
 
 // a whole sweep of narrow batches (dependency levels) in one thread block: the levels run one
@@ -2140,9 +2225,12 @@ int set_scan_order(dndsg_ctx* c, const int64_t* scan2cell) {
   DG_CUDA(c, cudaMemcpy(L.data(), c->faceL, sizeof(int32_t) * c->F, cudaMemcpyDeviceToHost));
   DG_CUDA(c, cudaMemcpy(R.data(), c->faceR, sizeof(int32_t) * c->F, cudaMemcpyDeviceToHost));
   auto records = [&](const std::vector<int32_t>& cellsOf, bool forward, std::vector<int32_t>& nf,
-                     std::vector<int32_t>& nj) {
+                     std::vector<int32_t>& nj, std::vector<int32_t>& np) {
     nf.assign(4 * N, kEmptySlot);
     nj.assign(4 * N, -1);
+    np.assign(4 * N, -1);
+    std::vector<int32_t> at(N);
+    for (int64_t t = 0; t < N; t++) at[cellsOf[t]] = (int32_t)t;
     for (int64_t t = 0; t < N; t++) {
       const int64_t i = cellsOf[t];
       for (int k = 0; k < c->nfmax && k < 4; k++) {
@@ -2152,27 +2240,34 @@ int set_scan_order(dndsg_ctx* c, const int64_t* scan2cell) {
         const int32_t f = sf >= 0 ? sf : ~sf;
         const int32_t j = sf >= 0 ? R[f] : L[f];
         if (j < 0) continue;
-        if (forward ? pos[j] < pos[i] : pos[j] > pos[i]) nj[4 * t + k] = j;
+        if (forward ? pos[j] < pos[i] : pos[j] > pos[i]) {
+          nj[4 * t + k] = j;
+          np[4 * t + k] = at[j];
+        }
       }
     }
   };
-  std::vector<int32_t> ff, fj, bf, bj;
-  records(fwd, true, ff, fj);
-  records(bwd, false, bf, bj);
+  std::vector<int32_t> ff, fj, fp, bf, bj, bp;
+  records(fwd, true, ff, fj, fp);
+  records(bwd, false, bf, bj, bp);
   if (!c->fwdNbF)
     if ((rc = dalloc(c, c->fwdNbF, sizeof(int32_t) * 4 * N)) || (rc = dalloc(c, c->fwdNbJ, sizeof(int32_t) * 4 * N)) ||
-        (rc = dalloc(c, c->bwdNbF, sizeof(int32_t) * 4 * N)) || (rc = dalloc(c, c->bwdNbJ, sizeof(int32_t) * 4 * N)))
+        (rc = dalloc(c, c->bwdNbF, sizeof(int32_t) * 4 * N)) || (rc = dalloc(c, c->bwdNbJ, sizeof(int32_t) * 4 * N)) ||
+        (rc = dalloc(c, c->fwdNbP, sizeof(int32_t) * 4 * N)) || (rc = dalloc(c, c->bwdNbP, sizeof(int32_t) * 4 * N)))
       return rc;
+  DG_CUDA(c, cudaMemcpy(c->fwdNbP, fp.data(), sizeof(int32_t) * 4 * N, cudaMemcpyHostToDevice));
+  DG_CUDA(c, cudaMemcpy(c->bwdNbP, bp.data(), sizeof(int32_t) * 4 * N, cudaMemcpyHostToDevice));
   DG_CUDA(c, cudaMemcpy(c->fwdNbF, ff.data(), sizeof(int32_t) * 4 * N, cudaMemcpyHostToDevice));
   DG_CUDA(c, cudaMemcpy(c->fwdNbJ, fj.data(), sizeof(int32_t) * 4 * N, cudaMemcpyHostToDevice));
   DG_CUDA(c, cudaMemcpy(c->bwdNbF, bf.data(), sizeof(int32_t) * 4 * N, cudaMemcpyHostToDevice));
   DG_CUDA(c, cudaMemcpy(c->bwdNbJ, bj.data(), sizeof(int32_t) * 4 * N, cudaMemcpyHostToDevice));
-  if (!c->lusgsRec && (rc = dalloc(c, c->lusgsRec, sizeof(LuRec) * N))) return rc;
-  for (const void* fn : {(const void*)k_lusgs_levels_rec<float, true, false>, (const void*)k_lusgs_levels_rec<float, false, false>,
-                         (const void*)k_lusgs_levels_rec<float, true, true>, (const void*)k_lusgs_levels_rec<float, false, true>,
-                         (const void*)k_lusgs_levels_rec<double, true, false>, (const void*)k_lusgs_levels_rec<double, false, false>,
-                         (const void*)k_lusgs_levels_rec<double, true, true>, (const void*)k_lusgs_levels_rec<double, false, true>})
-    DG_CUDA(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRecSmem));
+  if (!c->lusgsMat && (rc = dalloc(c, c->lusgsMat, (c->sa ? sizeof(LuMatS) : sizeof(LuMatF)) * N))) return rc;
+  for (const void* fn : {(const void*)k_lusgs_levels_mat<float, true, false>, (const void*)k_lusgs_levels_mat<float, false, false>,
+                         (const void*)k_lusgs_levels_mat<double, true, false>, (const void*)k_lusgs_levels_mat<double, false, false>})
+    DG_CUDA(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mat_smem<false>()));
+  for (const void* fn : {(const void*)k_lusgs_levels_mat<float, true, true>, (const void*)k_lusgs_levels_mat<float, false, true>,
+                         (const void*)k_lusgs_levels_mat<double, true, true>, (const void*)k_lusgs_levels_mat<double, false, true>})
+    DG_CUDA(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mat_smem<true>()));
   c->lusgsOrder = 1;
   return upload_schedule(c, pos, fwd, bwd);
 }
@@ -2189,14 +2284,17 @@ void launch_lusgs_sweep(dndsg_ctx* c, bool forward, double alpha, const double* 
     const int64_t* od = forward ? c->fwdOffDev : c->bwdOffDev;
     const int32_t* nf = forward ? c->fwdNbF : c->bwdNbF;
     const int32_t* nj = forward ? c->fwdNbJ : c->bwdNbJ;
+    const int32_t* np = forward ? c->fwdNbP : c->bwdNbP;
     SaView<T> none{};
-    LuRec* rec = (LuRec*)c->lusgsRec;
+    LuMatF* rec = (LuMatF*)c->lusgsMat;
     if (forward) {
-      k_lusgs_pack<T, true, false><<<grid_for(c->N), kBlock, 0, s>>>(h, none, cells, nf, nj, c->N, alpha, c->Dinv, rhs, rec);
-      k_lusgs_levels_rec<T, true, false><<<1, kRecBlock, kRecSmem, s>>>(h, none, rec, od, nb, inc);
+      k_lusgs_pack_mat<T, true, false><<<grid_for(c->N), kBlock, 0, s>>>(h, none, cells, nf, nj, np, c->N, alpha, c->Dinv,
+                                                                          rhs, inc, rec);
+      k_lusgs_levels_mat<T, true, false><<<1, kRecBlock, mat_smem<false>(), s>>>(none, rec, od, nb, inc, c->flags);
     } else {
-      k_lusgs_pack<T, false, false><<<grid_for(c->N), kBlock, 0, s>>>(h, none, cells, nf, nj, c->N, alpha, c->Dinv, rhs, rec);
-      k_lusgs_levels_rec<T, false, false><<<1, kRecBlock, kRecSmem, s>>>(h, none, rec, od, nb, inc);
+      k_lusgs_pack_mat<T, false, false><<<grid_for(c->N), kBlock, 0, s>>>(h, none, cells, nf, nj, np, c->N, alpha, c->Dinv,
+                                                                           rhs, inc, rec);
+      k_lusgs_levels_mat<T, false, false><<<1, kRecBlock, mat_smem<false>(), s>>>(none, rec, od, nb, inc, c->flags);
     }
     return;
   }
@@ -2487,13 +2585,16 @@ void launch_lusgs_sweep_sa(dndsg_ctx* c, bool forward, double alpha, cudaStream_
     const int64_t* od = forward ? c->fwdOffDev : c->bwdOffDev;
     const int32_t* nf = forward ? c->fwdNbF : c->bwdNbF;
     const int32_t* nj = forward ? c->fwdNbJ : c->bwdNbJ;
-    LuRec* rec = (LuRec*)c->lusgsRec;
+    const int32_t* np = forward ? c->fwdNbP : c->bwdNbP;
+    LuMatS* rec = (LuMatS*)c->lusgsMat;
     if (forward) {
-      k_lusgs_pack<T, true, true><<<grid_for(c->N), kBlock, 0, s>>>(h, sa, cells, nf, nj, c->N, alpha, c->Dinv, c->rhs, rec);
-      k_lusgs_levels_rec<T, true, true><<<1, kRecBlock, kRecSmem, s>>>(h, sa, rec, od, nb, c->inc);
+      k_lusgs_pack_mat<T, true, true><<<grid_for(c->N), kBlock, 0, s>>>(h, sa, cells, nf, nj, np, c->N, alpha, c->Dinv,
+                                                                         c->rhs, c->inc, rec);
+      k_lusgs_levels_mat<T, true, true><<<1, kRecBlock, mat_smem<true>(), s>>>(sa, rec, od, nb, c->inc, c->flags);
     } else {
-      k_lusgs_pack<T, false, true><<<grid_for(c->N), kBlock, 0, s>>>(h, sa, cells, nf, nj, c->N, alpha, c->Dinv, c->rhs, rec);
-      k_lusgs_levels_rec<T, false, true><<<1, kRecBlock, kRecSmem, s>>>(h, sa, rec, od, nb, c->inc);
+      k_lusgs_pack_mat<T, false, true><<<grid_for(c->N), kBlock, 0, s>>>(h, sa, cells, nf, nj, np, c->N, alpha, c->Dinv,
+                                                                          c->rhs, c->inc, rec);
+      k_lusgs_levels_mat<T, false, true><<<1, kRecBlock, mat_smem<true>(), s>>>(sa, rec, od, nb, c->inc, c->flags);
     }
     return;
   }
