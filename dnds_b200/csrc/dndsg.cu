@@ -1930,7 +1930,7 @@ __global__ void __launch_bounds__(kBlock) k_lusgs_pack_mat(HotView<T> h, SaView<
 }
 
 constexpr int kRecBlock = 128;  // threads of the level walk, and records buffered per level
-constexpr int kMatRing = 256;   // increments of the most recent schedule positions kept in shared memory
+constexpr int kMatRing = 256;   // (a power of 2) increments of the most recent schedule positions kept in shared memory
 constexpr uint32_t kBulkChunk = 16384;
 template <bool SA>
 constexpr size_t mat_smem() {
@@ -1955,10 +1955,10 @@ __device__ __forceinline__ void lusgs_mat_cell(const SaView<T>& sa, const LuMat<
     const int32_t pj = f.p[q];
     double dU[4], dS = 0.0;
     if (pj >= ringLo) {
-      const double2* s = reinterpret_cast<const double2*>(ringF + 4 * (pj % kMatRing));
+      const double2* s = reinterpret_cast<const double2*>(ringF + 4 * (pj & (kMatRing - 1)));
       const double2 a = s[0], b = s[1];
       dU[0] = a.x; dU[1] = a.y; dU[2] = b.x; dU[3] = b.y;
-      if constexpr (SA) dS = ringS[pj % kMatRing];
+      if constexpr (SA) dS = ringS[pj & (kMatRing - 1)];
     } else {
       load4<double>(&inc[(int64_t)f.j[q] * 4], dU);
       if constexpr (SA) dS = sa.inc[f.j[q]];
@@ -1970,27 +1970,29 @@ __device__ __forceinline__ void lusgs_mat_cell(const SaView<T>& sa, const LuMat<
   double o[4];
   for (int v = 0; v < 4; v++) o[v] = f.add[v] + f.di * buf[v];
   double2* g = reinterpret_cast<double2*>(&inc[(int64_t)f.i * 4]);
-  double2* s = reinterpret_cast<double2*>(ringF + 4 * (t % kMatRing));
+  double2* s = reinterpret_cast<double2*>(ringF + 4 * (t & (kMatRing - 1)));
   g[0] = s[0] = make_double2(o[0], o[1]);
   g[1] = s[1] = make_double2(o[2], o[3]);
   if constexpr (SA) {
     const double oS = r.addS + r.diS * bufS;
     sa.inc[f.i] = oS;
-    ringS[t % kMatRing] = oS;
+    ringS[t & (kMatRing - 1)] = oS;
   }
 }
 
-// a whole level-scheduled sweep in one block.  One thread bulk-copies the next level's records
-// (contiguous in schedule order) into the other half of a shared-memory double buffer on an
-// mbarrier while the block finishes the current level; the block barrier per level publishes the
-// increments (global memory and the ring).  Positions of a level beyond kRecBlock read their
-// records from global memory.  A bulk copy that does not land in time sets kFlagTimeout and ends
-// the walk.
+// a whole level-scheduled sweep in one block, one thread per position and a producer warp.  The
+// producer bulk-copies the next level's records (contiguous in schedule order) into the other half
+// of a shared-memory double buffer on an mbarrier while the other warps finish the current level; the block barrier per level publishes the increments (global memory and the
+// ring).  Positions of a level beyond kRecBlock read their records from global memory.  A bulk
+// copy that does not land in time sets kFlagTimeout and ends the walk.
+template <bool SA>
+constexpr int mat_threads() { return kRecBlock + 32; }
 template <class T, bool FWD, bool SA>
-__global__ void __launch_bounds__(kRecBlock) k_lusgs_levels_mat(SaView<T> sa, const LuMat<SA>* rec,
-                                                                const int64_t* off, int nlev, double* inc,
-                                                                unsigned* flags) {
+__global__ void __launch_bounds__(mat_threads<SA>()) k_lusgs_levels_mat(SaView<T> sa, const LuMat<SA>* rec,
+                                                                        const int64_t* off, int nlev, double* inc,
+                                                                        unsigned* flags) {
   using R = LuMat<SA>;
+  constexpr int NT = kRecBlock;
   extern __shared__ __align__(16) unsigned char smraw[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(smraw);
   int32_t* so = reinterpret_cast<int32_t*>(smraw + 16);
@@ -1998,6 +2000,7 @@ __global__ void __launch_bounds__(kRecBlock) k_lusgs_levels_mat(SaView<T> sa, co
   double* ringS = ringF + 4 * kMatRing;
   R* buf = reinterpret_cast<R*>(ringS + (SA ? kMatRing : 0));
   const int tid = threadIdx.x;
+  const bool producer = tid == NT;
   for (int l = tid; l <= nlev; l += blockDim.x) so[l] = (int32_t)off[l];
   if (tid == 0) {
     mbar_init(smem_u32(&bars[0]), 1);
@@ -2005,7 +2008,7 @@ __global__ void __launch_bounds__(kRecBlock) k_lusgs_levels_mat(SaView<T> sa, co
     fence_mbar_init();
   }
   __syncthreads();
-  auto issue = [&](int l) {  // thread 0
+  auto issue = [&](int l) {  // producer
     const int32_t b = so[l];
     const int32_t n = min(so[l + 1] - b, kRecBlock);
     const uint32_t bar = smem_u32(&bars[l & 1]), bytes = (uint32_t)(n * sizeof(R));
@@ -2015,24 +2018,27 @@ __global__ void __launch_bounds__(kRecBlock) k_lusgs_levels_mat(SaView<T> sa, co
     mbar_expect_tx(bar, bytes);
     for (uint32_t o = 0; o < bytes; o += kBulkChunk) bulk_g2s(dst + o, src + o, min(kBulkChunk, bytes - o), bar);
   };
-  if (tid == 0 && nlev > 0) issue(0);
+  if (producer && nlev > 0) issue(0);
   int lo = 0, l = 0;
   bool failed = false;
   for (; l < nlev; l++) {
-    if (tid == 0 && l + 1 < nlev) issue(l + 1);
+    if (producer && l + 1 < nlev) issue(l + 1);
     while (so[l + 1] - so[lo] > kMatRing) lo++;
     const int32_t ringLo = so[lo], b = so[l], e = so[l + 1];
-    const bool ok = mbar_wait(smem_u32(&bars[l & 1]), (l >> 1) & 1, kWaitLimit);
-    if (ok)
-      for (int32_t t = b + tid; t < e; t += kRecBlock)
-        lusgs_mat_cell<FWD, SA>(sa, t - b < kRecBlock ? buf[(l & 1) * kRecBlock + (t - b)] : rec[t], t, ringLo, ringF,
-                                ringS, inc);
+    bool ok = true;
+    if (tid < NT && b + tid < e) {
+      ok = mbar_wait(smem_u32(&bars[l & 1]), (l >> 1) & 1, kWaitLimit);
+      if (ok)
+        for (int32_t t = b + tid; t < e; t += kRecBlock)
+          lusgs_mat_cell<FWD, SA>(sa, t - b < kRecBlock ? buf[(l & 1) * kRecBlock + (t - b)] : rec[t], t, ringLo, ringF,
+                                  ringS, inc);
+    }
     if (__syncthreads_or(!ok)) {
       failed = true;
       break;
     }
   }
-  if (failed && tid == 0) {  // let the copies in flight land before the block exits
+  if (failed && producer) {  // let the copies in flight land before the block exits
     atomicOr(flags, kFlagTimeout);
     mbar_wait(smem_u32(&bars[l & 1]), (l >> 1) & 1, kWaitLimit);
     if (l + 1 < nlev) mbar_wait(smem_u32(&bars[(l + 1) & 1]), ((l + 1) >> 1) & 1, kWaitLimit);
@@ -2290,11 +2296,11 @@ void launch_lusgs_sweep(dndsg_ctx* c, bool forward, double alpha, const double* 
     if (forward) {
       k_lusgs_pack_mat<T, true, false><<<grid_for(c->N), kBlock, 0, s>>>(h, none, cells, nf, nj, np, c->N, alpha, c->Dinv,
                                                                           rhs, inc, rec);
-      k_lusgs_levels_mat<T, true, false><<<1, kRecBlock, mat_smem<false>(), s>>>(none, rec, od, nb, inc, c->flags);
+      k_lusgs_levels_mat<T, true, false><<<1, mat_threads<false>(), mat_smem<false>(), s>>>(none, rec, od, nb, inc, c->flags);
     } else {
       k_lusgs_pack_mat<T, false, false><<<grid_for(c->N), kBlock, 0, s>>>(h, none, cells, nf, nj, np, c->N, alpha, c->Dinv,
                                                                            rhs, inc, rec);
-      k_lusgs_levels_mat<T, false, false><<<1, kRecBlock, mat_smem<false>(), s>>>(none, rec, od, nb, inc, c->flags);
+      k_lusgs_levels_mat<T, false, false><<<1, mat_threads<false>(), mat_smem<false>(), s>>>(none, rec, od, nb, inc, c->flags);
     }
     return;
   }
@@ -2590,11 +2596,11 @@ void launch_lusgs_sweep_sa(dndsg_ctx* c, bool forward, double alpha, cudaStream_
     if (forward) {
       k_lusgs_pack_mat<T, true, true><<<grid_for(c->N), kBlock, 0, s>>>(h, sa, cells, nf, nj, np, c->N, alpha, c->Dinv,
                                                                          c->rhs, c->inc, rec);
-      k_lusgs_levels_mat<T, true, true><<<1, kRecBlock, mat_smem<true>(), s>>>(sa, rec, od, nb, c->inc, c->flags);
+      k_lusgs_levels_mat<T, true, true><<<1, mat_threads<true>(), mat_smem<true>(), s>>>(sa, rec, od, nb, c->inc, c->flags);
     } else {
       k_lusgs_pack_mat<T, false, true><<<grid_for(c->N), kBlock, 0, s>>>(h, sa, cells, nf, nj, np, c->N, alpha, c->Dinv,
                                                                           c->rhs, c->inc, rec);
-      k_lusgs_levels_mat<T, false, true><<<1, kRecBlock, mat_smem<true>(), s>>>(sa, rec, od, nb, c->inc, c->flags);
+      k_lusgs_levels_mat<T, false, true><<<1, mat_threads<true>(), mat_smem<true>(), s>>>(sa, rec, od, nb, c->inc, c->flags);
     }
     return;
   }
