@@ -20,12 +20,19 @@ EXPORTS = [
     "dndsg_mlp_get_params", "dndsg_mlp_forward", "dndsg_mlp_gradient", "dndsg_mlp_train_step",
     "dndsg_mlp_features", "dndsg_vr_to_tolerance", "dndsg_ssprk3_step_tol",
     "dndsg_lusgs_colours", "dndsg_lusgs_set_order", "dndsg_lusgs_matrix_init", "dndsg_lusgs_forward", "dndsg_lusgs_backward",
-    "dndsg_bdf_begin", "dndsg_implicit_iteration",
+    "dndsg_bdf_begin", "dndsg_implicit_iteration", "dndsg_dual_reset", "dndsg_dual_step", "dndsg_lusgs_matvec", "dndsg_gmres_lusgs",
 ]
 _NO_STATUS = ("dndsg_destroy", "dndsg_last_error", "dndsg_n_cells", "dndsg_n_faces", "dndsg_mlp_destroy",
               "dndsg_mlp_last_error")
 
 MLP_IN, MLP_OUT, MLP_NPARAM = 64, 20, 14560
+
+
+class DualSettings(C.Structure):
+    """dndsg_dual_settings (include/dndsg.h), field for field."""
+    _fields_ = [("scheme", C.c_int), ("bdf_order", C.c_int), ("cfl", C.c_double), ("max_iter", C.c_int),
+                ("threshold", C.c_double), ("n_rec", C.c_int), ("vol_wise", C.c_int), ("gmres_code", C.c_int),
+                ("n_gmres_space", C.c_int), ("n_gmres_iter", C.c_int)]
 
 
 class MeshDesc(C.Structure):
@@ -95,6 +102,10 @@ def lib():
     L.dndsg_lusgs_backward.argtypes = [vp, dbl, vp, vp, vp]
     L.dndsg_bdf_begin.argtypes = [vp, vp]
     L.dndsg_implicit_iteration.argtypes = [vp, dbl, dbl, dbl, i32, i32, dbl, vp, vp, vp]
+    L.dndsg_dual_reset.argtypes = [vp]
+    L.dndsg_dual_step.argtypes = [vp, C.POINTER(DualSettings), dbl, dbl, vp, vp, vp]
+    L.dndsg_lusgs_matvec.argtypes = [vp, dbl, vp, vp, vp]
+    L.dndsg_gmres_lusgs.argtypes = [vp, dbl, i32, i32, vp, vp, vp]
     for nm in EXPORTS:
         if nm not in _NO_STATUS:
             getattr(L, nm).restype = i32

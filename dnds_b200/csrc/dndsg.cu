@@ -72,6 +72,13 @@ struct dndsg_ctx {
   std::vector<int32_t> colourHost;  // greedy colouring, kept for dndsg_lusgs_colours
   int lusgsOrder = 0;               // 0 colour batches, 1 level-scheduled scan order
   double *Dinv = nullptr, *inc = nullptr, *resAcc = nullptr;
+  double* Dmat = nullptr;  // the LU-SGS diagonal itself (GMRES matrix-vector product)
+  // dual time stepping: BDF history (earlier steps' states) or the SDIRK stage right-hand sides,
+  // the GMRES Krylov basis, Hessenberg matrix and reduction scratch
+  std::vector<double*> odeVec, gmV;
+  int odeOrder = 0, odeCnPrev = 0, odePrevStart = 0;
+  double odeDtPrev = 0.0;
+  double *gmTmp = nullptr, *gmMLb = nullptr, *gmH = nullptr, *gmPartial = nullptr;
   // state
   double *u = nullptr, *uLast = nullptr, *rhs = nullptr, *dt = nullptr, *flux = nullptr, *lamA = nullptr,
          *dLam = nullptr, *scal = nullptr, *partial = nullptr;
@@ -1725,7 +1732,8 @@ __device__ __forceinline__ void flux_jac_times_du(const double U[4], double nx, 
 // scalar per cell, D_i = alpha/dt_i + 1/dtPhys + sum_f (alpha/2) lambda_f A_f / V_i, where dt_i is
 // the EvaluateDt step (dTau = dt_i / alpha) and lamA holds lambda_f A_f
 template <class T>
-__global__ void __launch_bounds__(kBlock) k_lusgs_init(HotView<T> h, double dtPhysInv, double alpha, double* Dinv) {
+__global__ void __launch_bounds__(kBlock) k_lusgs_init(HotView<T> h, double dtPhysInv, double alpha, double* Dinv,
+                                                       double* D) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= h.N) return;
   double sum = 0;
@@ -1736,6 +1744,7 @@ __global__ void __launch_bounds__(kBlock) k_lusgs_init(HotView<T> h, double dtPh
   }
   const double d = alpha / h.dt[i] + dtPhysInv + 0.5 * alpha * sum / h.vol[i];
   Dinv[i] = 1.0 / d;
+  D[i] = d;
 }
 
 // rhs of the first-order BDF pseudo-time system (ImplicitBDFDualTimeStep::Step,
@@ -2164,6 +2173,7 @@ int ensure_lusgs(dndsg_ctx* c) {
   group_by(rev, ncol, bwd, c->bwdOff);
   if ((rc = dalloc(c, c->rankOf, sizeof(int32_t) * N)) || (rc = dalloc(c, c->fwdCells, sizeof(int32_t) * N)) ||
       (rc = dalloc(c, c->bwdCells, sizeof(int32_t) * N)) || (rc = dalloc(c, c->Dinv, sizeof(double) * N)) ||
+      (rc = dalloc(c, c->Dmat, sizeof(double) * N)) ||
       (rc = dalloc(c, c->inc, sizeof(double) * 4 * N)) || (rc = dalloc(c, c->resAcc, sizeof(double) * 16)))
     return rc;
   c->colourHost = col;
@@ -2337,7 +2347,7 @@ int run_implicit(dndsg_ctx* c, double cfl, double dtPhys, double alpha, int nRec
   const int64_t n4 = c->N * 4;
   k_bdf_rhs<<<(unsigned)((n4 + kBlock - 1) / kBlock), kBlock, 0, s>>>(n4, c->u, c->uLast, alpha, dtInv, c->rhs);
   HotView<T> h = view<T>(c);
-  k_lusgs_init<T><<<grid_for(c->N), kBlock, 0, s>>>(h, dtInv, alpha, c->Dinv);
+  k_lusgs_init<T><<<grid_for(c->N), kBlock, 0, s>>>(h, dtInv, alpha, c->Dinv, c->Dmat);
   launch_lusgs_sweep<T>(c, true, alpha, c->rhs, c->inc, s);
   launch_lusgs_sweep<T>(c, false, alpha, c->rhs, c->inc, s);
   DG_CUDA(c, cudaMemsetAsync(c->resAcc, 0, sizeof(double) * 16, s));
@@ -2384,8 +2394,8 @@ int dndsg_lusgs_matrix_init(dndsg_ctx* c, double dt_phys, double alpha, void* s)
   if (!c || !(dt_phys > 0) || !(alpha > 0)) return DNDSG_BAD_ARGUMENT;
   int rc;
   if ((rc = set_device(c)) || (rc = ensure_lusgs(c))) return rc;
-  if (c->fp32) k_lusgs_init<float><<<grid_for(c->N), kBlock, 0, st(s)>>>(view<float>(c), 1.0 / dt_phys, alpha, c->Dinv);
-  else k_lusgs_init<double><<<grid_for(c->N), kBlock, 0, st(s)>>>(view<double>(c), 1.0 / dt_phys, alpha, c->Dinv);
+  if (c->fp32) k_lusgs_init<float><<<grid_for(c->N), kBlock, 0, st(s)>>>(view<float>(c), 1.0 / dt_phys, alpha, c->Dinv, c->Dmat);
+  else k_lusgs_init<double><<<grid_for(c->N), kBlock, 0, st(s)>>>(view<double>(c), 1.0 / dt_phys, alpha, c->Dinv, c->Dmat);
   return check_launch(c);
 }
 
@@ -2636,7 +2646,7 @@ int run_implicit_sa(dndsg_ctx* c, double cfl, double dtPhys, double alpha, int n
   k_bdf_rhs<<<(unsigned)((n4 + kBlock - 1) / kBlock), kBlock, 0, s>>>(n4, c->u, c->uLast, alpha, dtInv, c->rhs);
   k_sa_rhs_fix<<<grid_for(c->N), kBlock, 0, s>>>(c->N, c->saU, c->saULast, c->dt, alpha, dtInv, c->saRhs);
   HotView<T> h = view<T>(c);
-  k_lusgs_init<T><<<grid_for(c->N), kBlock, 0, s>>>(h, dtInv, alpha, c->Dinv);
+  k_lusgs_init<T><<<grid_for(c->N), kBlock, 0, s>>>(h, dtInv, alpha, c->Dinv, c->Dmat);
   k_sa_diag<<<grid_for(c->N), kBlock, 0, s>>>(c->N, c->Dinv, c->saSrcJac, alpha, c->saDinv);
   launch_lusgs_sweep_sa<T>(c, true, alpha, s);
   launch_lusgs_sweep_sa<T>(c, false, alpha, s);
@@ -2675,3 +2685,5 @@ int sa_implicit(dndsg_ctx* c, double cfl, double dtPhys, double alpha, int nRec,
                  : run_implicit_sa<double>(c, cfl, dtPhys, alpha, nRec, volWise, s);
 }
 }  // namespace
+
+#include "dndsg_dual.cuh"

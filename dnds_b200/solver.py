@@ -195,6 +195,40 @@ class Solver:
                                                     int(vol_wise), float(t), _p(res), _p(wf), self.stream))
         return res, wf
 
+    def dual_reset(self):
+        """A fresh dual-time integrator: the BDF history is forgotten."""
+        self._check(self.L.dndsg_dual_reset(self.h))
+
+    def dual_step(self, dt: float, t: float = 0.0, scheme: str = "sdirk4", bdf_order: int = 2, cfl: float = 100.0,
+                  max_iter: int = 10, threshold: float = 1e-100, n_rec: int = 1, vol_wise: bool = False,
+                  gmres_code: int = 0, n_gmres_space: int = 10, n_gmres_iter: int = 2):
+        """One physical step of the reference's implicit driver: ImplicitSDIRK4DualTimeStep
+        (scheme "sdirk4", odeCode 0) or ImplicitBDFDualTimeStep of order bdf_order (scheme "bdf",
+        odeCode 1), DNDS_ODE.hpp:269-497; fsolve by LU-SGS (gmres_code 0), GMRES over LU-SGS (1), or
+        LU-SGS then GMRES (2).  Returns (internal iterations per stage, last fstop ratios)."""
+        from ._lib import DualSettings
+
+        d = DualSettings(scheme={"sdirk4": 0, "bdf": 1}[scheme], bdf_order=int(bdf_order), cfl=float(cfl),
+                         max_iter=int(max_iter), threshold=float(threshold), n_rec=int(n_rec),
+                         vol_wise=int(vol_wise), gmres_code=int(gmres_code), n_gmres_space=int(n_gmres_space),
+                         n_gmres_iter=int(n_gmres_iter))
+        its = np.zeros(3, dtype=np.int32)
+        res = np.zeros(4)
+        self._check(self.L.dndsg_dual_step(self.h, C.byref(d), float(dt), float(t), _p(its), _p(res), self.stream))
+        return its, res
+
+    def LUSGSMatrixVec(self, alpha_diag: float, x_ptr: int, ax_ptr: int):
+        """LUSGSMatrixVec (DNDS_FV_EulerEvaluator.cpp:1062-1143) on device arrays [N][4], with the
+        diagonal of the last LUSGSMatrixInit."""
+        self._check(self.L.dndsg_lusgs_matvec(self.h, float(alpha_diag), C.c_void_p(x_ptr), C.c_void_p(ax_ptr),
+                                              self.stream))
+
+    def gmres_lusgs(self, alpha_diag: float, n_space: int, n_restart: int, b_ptr: int, x_ptr: int):
+        """GMRES_LeftPreconditioned over LUSGSMatrixVec with the LU-SGS sweeps as preconditioner, on
+        device arrays [N][4]; x holds the initial guess and receives the result."""
+        self._check(self.L.dndsg_gmres_lusgs(self.h, float(alpha_diag), int(n_space), int(n_restart),
+                                             C.c_void_p(b_ptr), C.c_void_p(x_ptr), self.stream))
+
     def steady_solve(self, cfl: float, threshold: float = 1e-8, max_iter: int = 10000, dt: float = 1e100,
                      n_rec: int = 1, vol_wise: bool = False, history: list | None = None):
         """Pseudo-time iterations until the density component of the increment norm, relative to its

@@ -232,6 +232,57 @@ int dndsg_implicit_iteration(dndsg_ctx* ctx, double cfl, double dt_phys, double 
                              double t, double* inc_res_out, double* wall_flux_out, void* stream);
 
 /* ---------------------------------------------------------------------------
+ * Dual time stepping, the reference's implicit driver: one physical step of
+ * ImplicitBDFDualTimeStep (order k; DNDS_ODE.hpp:392-497) or of the 3-stage
+ * ImplicitSDIRK4DualTimeStep (DNDS_ODE.hpp:269-390), each internal iteration
+ * being the EulerSolver's fdtau / frhs / fsolve / fstop
+ * (DNDS_FV_EulerSolver.hpp:713-1061).  fsolve per gmres_code (gmresCode):
+ * 0 the LU-SGS forward + backward sweeps; 1 GMRES_LeftPreconditioned
+ * (DNDS_Linear.hpp:12-107) from a zero start, n_gmres_space Krylov vectors
+ * (nGmresSpace) and n_gmres_iter restarts (nGmresIter), over LUSGSMatrixVec
+ * with the LU-SGS sweeps as left preconditioner; 2 the sweeps, then GMRES from
+ * their result.  fstop: the L1 norm of the increment (volume-weighted when
+ * vol_wise) over its running maximum in the stage; an internal loop ends when
+ * the density entry drops below threshold (rhsThresholdInternal) or after
+ * max_iter (nTimeStepInternal) iterations.  The sweep order is the one of
+ * dndsg_lusgs_set_order.  4-variable contexts.
+ * ------------------------------------------------------------------------ */
+#define DNDSG_DUAL_SDIRK4 0 /* odeCode 0 */
+#define DNDSG_DUAL_BDF 1    /* odeCode 1 (the reference's driver uses bdf_order 2) */
+typedef struct dndsg_dual_settings {
+  int scheme;       /* DNDSG_DUAL_SDIRK4 or DNDSG_DUAL_BDF */
+  int bdf_order;    /* 1..4 (BDF only) */
+  double cfl;       /* CFL of the local pseudo time step */
+  int max_iter;     /* nTimeStepInternal */
+  double threshold; /* rhsThresholdInternal */
+  int n_rec;        /* nInternalRecStep */
+  int vol_wise;     /* useVolWiseResidual */
+  int gmres_code;   /* 0, 1, 2 */
+  int n_gmres_space;
+  int n_gmres_iter;
+} dndsg_dual_settings;
+/* a fresh integrator: forgets the BDF history (also implied by a change of
+ * bdf_order between calls) */
+int dndsg_dual_reset(dndsg_ctx* ctx);
+/* one physical step of size dt from time t, in place on the context's u;
+ * iters_out [3] (host, may be NULL): internal iterations per stage (BDF: [0]);
+ * res_out [4] (host, may be NULL): the last fstop ratios.  A BDF history built
+ * with another dt is an error (the reference asserts a constant dt). */
+int dndsg_dual_step(dndsg_ctx* ctx, const dndsg_dual_settings* settings, double dt, double t, int* iters_out,
+                    double* res_out, void* stream);
+/* GMRES_LeftPreconditioned::solve (DNDS_Linear.hpp:47-105) of LUSGSMatrixVec x = b,
+ * the LU-SGS forward + backward sweeps as left preconditioner, n_space Krylov
+ * vectors (1..32), n_restart restarts; x [n_cells][4] (device) holds the
+ * initial guess and receives the result; b [n_cells][4] (device).  Uses the
+ * diagonal and spectral radii of the last dndsg_lusgs_matrix_init. */
+int dndsg_gmres_lusgs(dndsg_ctx* ctx, double alpha, int n_space, int n_restart, const double* b, double* x,
+                      void* stream);
+/* LUSGSMatrixVec (DNDS_FV_EulerEvaluator.cpp:1062-1143): ax = D x + sum over all
+ * neighbours of (alpha/2) A_f / V_i dF(u_j; n, x_j), with D from the last
+ * dndsg_lusgs_matrix_init; x, ax [n_cells][4] (device) */
+int dndsg_lusgs_matvec(dndsg_ctx* ctx, double alpha, const double* x, double* ax, void* stream);
+
+/* ---------------------------------------------------------------------------
  * Learned warm start for the VR coefficients.  No counterpart in the
  * reference: a per-cell network 64 -> 64 -> 64 -> 64 -> 20 (SiLU), BF16
  * weights and activations with FP32 accumulation on the tensor cores, trained

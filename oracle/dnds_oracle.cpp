@@ -144,6 +144,12 @@ struct orc_ctx {
   std::vector<double> dtFace, lambdaFace, deltaLambdaFace, lambdaCell;
   std::vector<double> dtCell;
   std::vector<double> Dinv;      // LU-SGS diagonal inverse [N][nv] (diagonal per variable)
+  std::vector<double> Dmat;      // the diagonal itself (jacobianCell, for LUSGSMatrixVec)
+  // dual time stepping: BDF history (prevStart / cnPrev as ImplicitBDFDualTimeStep) or SDIRK
+  // stage right-hand sides
+  std::vector<std::vector<double>> odeVec;
+  int odeOrder = 0, odeCnPrev = 0, odePrevStart = 0;
+  double odeDtPrev = 0;
   std::vector<double> dWall;     // SA: wall distance per cell (first-order, from the cell barycentre)
   std::vector<double> srcJac;    // SA: jacobianCellSourceDiag [N][nv] of the last RHS
   double lastInc = 0;
@@ -1484,6 +1490,7 @@ void compress_inc(const orc_ctx& c, const double* u, double* inc) {
 void lusgs_matrix_init(orc_ctx& c, const double* dTau, double dt, double alpha) {
   const int nv = c.nv;
   c.Dinv.assign(c.N * nv, 0.0);
+  c.Dmat.assign(c.N * nv, 0.0);
   const bool src = c.srcJac.size() == (size_t)(c.N * nv);
   for (int64_t i = 0; i < c.N; i++) {
     const CellGeo& g = c.cg[i];
@@ -1493,7 +1500,10 @@ void lusgs_matrix_init(orc_ctx& c, const double* dTau, double dt, double alpha) 
       d += (0.5 * alpha) * c.fg[f].area * c.lambdaFace[f] / g.vol;
     }
     // + alpha * jacobianCellSourceDiag, kept diagonal
-    for (int v = 0; v < nv; v++) c.Dinv[i * nv + v] = 1.0 / (d + (src ? alpha * c.srcJac[i * nv + v] : 0.0));
+    for (int v = 0; v < nv; v++) {
+      c.Dmat[i * nv + v] = d + (src ? alpha * c.srcJac[i * nv + v] : 0.0);
+      c.Dinv[i * nv + v] = 1.0 / c.Dmat[i * nv + v];
+    }
   }
 }
 
@@ -1548,6 +1558,103 @@ void lusgs_sweeps(const orc_ctx& c, double alpha, const double* rhs, double* inc
       lusgs_offdiag(c, i, s, pos, false, alpha, inc, buf);
       for (int v = 0; v < nv; v++) inc[i * nv + v] += c.Dinv[i * nv + v] * buf[v];
     }
+}
+
+
+// LUSGSMatrixVec (DNDS_FV_EulerEvaluator.cpp:1062-1143): Ax_i = D_i x_i - buf,
+// buf -= (alpha/2) A_f / V_i fluxJacobian0_Right_Times_du(u_j, n_out, x_j) over every neighbour
+void lusgs_matvec(const orc_ctx& c, double alpha, const double* x, double* Ax) {
+  const int nv = c.nv;
+  for (int64_t i = 0; i < c.N; i++) {
+    const CellGeo& g = c.cg[i];
+    double buf[kMaxV] = {0};
+    for (int k = 0; k < g.nface; k++) {
+      const int f = g.faces[k];
+      const FaceGeo& fg = c.fg[f];
+      const int64_t j = fg.L == i ? fg.R : fg.L;
+      if (j < 0) continue;
+      const double nn = std::sqrt(sqr(fg.ncenter[0]) + sqr(fg.ncenter[1]));
+      const double sg = fg.L == i ? 1.0 : -1.0;
+      const double n[2] = {sg * fg.ncenter[0] / nn, sg * fg.ncenter[1] / nn};
+      double dF[kMaxV];
+      flux_jac_times_du(&c.u[j * nv], n, &x[j * nv], c.lambdaFace[f], c.s.gamma, dF, nv);
+      for (int v = 0; v < nv; v++) buf[v] -= (0.5 * alpha) * fg.area / g.vol * dF[v];
+    }
+    for (int v = 0; v < nv; v++) Ax[i * nv + v] = c.Dmat[i * nv + v] * x[i * nv + v] - buf[v];
+  }
+}
+
+double vdot(const std::vector<double>& a, const std::vector<double>& b) {
+  double s = 0;
+  for (size_t k = 0; k < a.size(); k++) s += a[k] * b[k];
+  return s;
+}
+
+// least squares min |H y - rhs| for an m x n matrix (row-major) by Householder QR
+void lsq_householder(std::vector<double> H, int m, int n, std::vector<double> rhs, double* y) {
+  for (int j = 0; j < n; j++) {
+    double nrm = 0;
+    for (int i = j; i < m; i++) nrm += H[i * n + j] * H[i * n + j];
+    nrm = std::sqrt(nrm);
+    if (nrm == 0) continue;
+    const double alpha = H[j * n + j] > 0 ? -nrm : nrm;
+    std::vector<double> v(m, 0.0);
+    for (int i = j; i < m; i++) v[i] = H[i * n + j];
+    v[j] -= alpha;
+    double vv = 0;
+    for (int i = j; i < m; i++) vv += v[i] * v[i];
+    if (vv == 0) continue;
+    for (int q = j; q < n; q++) {
+      double d = 0;
+      for (int i = j; i < m; i++) d += v[i] * H[i * n + q];
+      for (int i = j; i < m; i++) H[i * n + q] -= 2 * d / vv * v[i];
+    }
+    double d = 0;
+    for (int i = j; i < m; i++) d += v[i] * rhs[i];
+    for (int i = j; i < m; i++) rhs[i] -= 2 * d / vv * v[i];
+  }
+  for (int j = n - 1; j >= 0; j--) {
+    double r = rhs[j];
+    for (int q = j + 1; q < n; q++) r -= H[j * n + q] * y[q];
+    y[j] = r / H[j * n + j];
+  }
+}
+
+// GMRES_LeftPreconditioned::solve (DNDS_Linear.hpp:47-105) with the EulerSolver's FStop (never
+// stops early): FA = LUSGSMatrixVec, FML = LU-SGS forward + backward with the argument as rhs
+void gmres_solve(const orc_ctx& c, int K, int nRestart, double alpha, const std::vector<double>& b,
+                 std::vector<double>& x, const int64_t* scan2cell) {
+  const size_t n = b.size();
+  auto FML = [&](const std::vector<double>& in, std::vector<double>& out) {
+    out.assign(n, 0.0);
+    lusgs_sweeps(c, alpha, in.data(), out.data(), scan2cell, true, true);
+  };
+  std::vector<double> MLb, tmp(n);
+  std::vector<std::vector<double>> V(K + 1, std::vector<double>(n));
+  FML(b, MLb);
+  for (int iRestart = 0; iRestart <= nRestart; iRestart++) {
+    lusgs_matvec(c, alpha, x.data(), tmp.data());
+    FML(tmp, V[0]);
+    for (size_t e = 0; e < n; e++) V[0][e] += MLb[e] * -1.0;
+    const double beta = std::sqrt(vdot(V[0], V[0]));
+    if (std::abs(beta) < 1e-200 || iRestart == nRestart) break;
+    for (size_t e = 0; e < n; e++) V[0][e] *= -1.0 / beta;
+    std::vector<double> h((size_t)(K + 1) * K, 0.0);  // row-major (K+1) x K
+    for (int j = 0; j < K; j++) {
+      lusgs_matvec(c, alpha, V[j].data(), tmp.data());
+      FML(tmp, V[j + 1]);
+      for (int i = 0; i <= j; i++) h[i * K + j] = vdot(V[j + 1], V[i]);
+      for (int i = 0; i <= j; i++)
+        for (size_t e = 0; e < n; e++) V[j + 1][e] += V[i][e] * -h[i * K + j];
+      h[(j + 1) * K + j] = std::sqrt(vdot(V[j + 1], V[j + 1]));
+      for (size_t e = 0; e < n; e++) V[j + 1][e] *= 1.0 / h[(j + 1) * K + j];
+    }
+    std::vector<double> eb(K + 1, 0.0), y(K);
+    eb[0] = beta;
+    lsq_householder(h, K + 1, K, eb, y.data());
+    for (int j = 0; j < K; j++)
+      for (size_t e = 0; e < n; e++) x[e] += V[j][e] * y[j];
+  }
 }
 
 }  // namespace
@@ -1776,6 +1883,144 @@ int orc_implicit_iteration(orc_ctx* c, double cfl, double dt, double alpha, cons
   for (int64_t i = 0; i < c->N; i++) compress_inc(*c, &c->u[i * nv], &inc[i * nv]);
   for (int64_t k = 0; k < n; k++) c->u[k] += inc[k];
   if (inc_out) std::memcpy(inc_out, inc.data(), sizeof(double) * n);
+  return 0;
+}
+
+int orc_lusgs_matvec(orc_ctx* c, double alpha, const double* x, double* ax) {
+  if (c->Dmat.size() != (size_t)(c->N * c->nv)) return 1;
+  lusgs_matvec(*c, alpha, x, ax);
+  return 0;
+}
+
+int orc_gmres_lusgs(orc_ctx* c, double alpha, int n_space, int n_restart, const double* b, double* x,
+                    const int64_t* scan2cell) {
+  if (c->Dmat.size() != (size_t)(c->N * c->nv) || n_space < 1) return 1;
+  const size_t n = (size_t)(c->N * c->nv);
+  std::vector<double> bv(b, b + n), xv(x, x + n);
+  gmres_solve(*c, n_space, n_restart, alpha, bv, xv, scan2cell);
+  std::memcpy(x, xv.data(), sizeof(double) * n);
+  return 0;
+}
+
+int orc_dual_reset(orc_ctx* c) {
+  c->odeOrder = c->odeCnPrev = c->odePrevStart = 0;
+  c->odeDtPrev = 0;
+  return 0;
+}
+
+// one physical step of ImplicitBDFDualTimeStep (order k, DNDS_ODE.hpp:392-497) or
+// ImplicitSDIRK4DualTimeStep (DNDS_ODE.hpp:269-390) with the EulerSolver lambdas
+// (DNDS_FV_EulerSolver.hpp:713-1061): fdtau = local EvaluateDt / alphaDiag; frhs = Jacobi sweeps,
+// [limiter], EvaluateRHS at t + ct dt; fsolve = LUSGSMatrixInit, CompressInc of rhs dTau, LU-SGS
+// and / or GMRES, CompressInc of the increment; fstop = the L1 (volume-weighted) increment norm
+// over its running maximum, density entry against the threshold
+int orc_dual_step(orc_ctx* c, const orc_dual_settings* d, double dt, double t, const int64_t* scan2cell,
+                  int* iters_out, double* res_out) {
+  static const double bdf[4][5] = {{1.0, 1.0, 0, 0, 0},
+                                   {2. / 3., 4. / 3., -1. / 3., 0, 0},
+                                   {6. / 11., 18. / 11., -9. / 11., 2. / 11., 0},
+                                   {12. / 25., 48. / 25., -36. / 25., 16. / 25., -3. / 25.}};
+  const double z = 0.128886400515;
+  const double A[3][3] = {{z, 0, 0}, {0.5 - z, z, 0}, {2 * z, 1 - 4 * z, z}};
+  const double C[3] = {z, 0.5, 1 - z};
+  const double B[3] = {1. / (6 * sqr(2 * z - 1)), (4 * sqr(z) - 4 * z + 2. / 3.) / sqr(2 * z - 1),
+                       1. / (6 * sqr(2 * z - 1))};
+  const int nv = c->nv;
+  const int64_t n = c->N * nv;
+  const bool bdfScheme = d->scheme == 1;
+  if (bdfScheme && (d->bdf_order < 1 || d->bdf_order > 4)) return 1;
+  if (bdfScheme && c->odeOrder != d->bdf_order) {
+    c->odeOrder = d->bdf_order;
+    c->odeCnPrev = 0;
+    c->odePrevStart = std::max(0, d->bdf_order - 2);
+  }
+  const size_t nOde = bdfScheme ? (size_t)(d->bdf_order - 1) : 3;
+  while (c->odeVec.size() < nOde) c->odeVec.emplace_back(n, 0.0);
+  std::vector<double> xLast = c->u, rhs(n), inc(n), dTau(c->N);
+  double base[kMaxV] = {0}, rel[kMaxV] = {0};
+  // one internal iteration; true when fstop says stop
+  auto iteration = [&](int iter, double alphaDiag, double ct, const std::function<void(std::vector<double>&)>& compose) {
+    double dtMin;
+    eval_dt(*c, d->cfl, 1e100, true, &dtMin);
+    for (int64_t i = 0; i < c->N; i++) dTau[i] = c->dtCell[i] / alphaDiag;
+    for (int k = 0; k < d->n_rec; k++) vr_sweep(*c);
+    if (c->s.limiter) limiter_wbap(*c, false, nullptr);
+    eval_rhs(*c, t + ct * dt, rhs.data(), nullptr, nullptr);
+    compose(rhs);
+    lusgs_matrix_init(*c, dTau.data(), dt, alphaDiag);
+    for (int64_t i = 0; i < c->N; i++) {
+      double r[kMaxV];
+      for (int v = 0; v < nv; v++) r[v] = rhs[i * nv + v] * dTau[i];
+      compress_inc(*c, &c->u[i * nv], r);
+      for (int v = 0; v < nv; v++) rhs[i * nv + v] = r[v] / dTau[i];
+    }
+    std::fill(inc.begin(), inc.end(), 0.0);
+    if (d->gmres_code == 0 || d->gmres_code == 2) {
+      lusgs_sweeps(*c, alphaDiag, rhs.data(), inc.data(), scan2cell, true, true);
+      for (int64_t i = 0; i < c->N; i++) compress_inc(*c, &c->u[i * nv], &inc[i * nv]);
+    }
+    if (d->gmres_code != 0) {
+      gmres_solve(*c, d->n_gmres_space, d->n_gmres_iter, alphaDiag, rhs, inc, scan2cell);
+      for (int64_t i = 0; i < c->N; i++) compress_inc(*c, &c->u[i * nv], &inc[i * nv]);
+    }
+    double res[kMaxV] = {0};
+    for (int64_t i = 0; i < c->N; i++)
+      for (int v = 0; v < nv; v++) res[v] += std::abs(inc[i * nv + v]) * (d->vol_wise ? c->cg[i].vol : 1.0);
+    for (int64_t k = 0; k < n; k++) c->u[k] += inc[k];
+    for (int v = 0; v < nv; v++) {
+      base[v] = iter == 1 ? res[v] : std::max(base[v], res[v]);
+      rel[v] = res[v] / base[v];
+    }
+    return rel[0] < d->threshold;
+  };
+  if (bdfScheme) {
+    const int prevSiz = d->bdf_order - 1, kCur = c->odeCnPrev + 1;
+    if (c->odeCnPrev > 0 && !(std::abs(c->odeDtPrev - dt) < dt * 1e-8)) return 1;
+    int iter = 1;
+    for (; iter <= d->max_iter; iter++) {
+      const bool stop = iteration(iter, bdf[kCur - 1][0], 1.0, [&](std::vector<double>& r) {
+        for (int64_t k = 0; k < n; k++) {
+          r[k] *= bdf[kCur - 1][0];
+          r[k] += c->u[k] * (-1. / dt);
+          r[k] += xLast[k] * (bdf[kCur - 1][1] / dt);
+          for (int ip = 0; ip < c->odeCnPrev; ip++)
+            r[k] += c->odeVec[(ip + c->odePrevStart) % prevSiz][k] * (bdf[kCur - 1][2 + ip] / dt);
+        }
+      });
+      if (stop) break;
+    }
+    if (iters_out) iters_out[0] = std::min(iter, d->max_iter);
+    if (prevSiz) {
+      c->odePrevStart = ((c->odePrevStart - 1) % prevSiz + prevSiz) % prevSiz;
+      c->odeVec[c->odePrevStart] = xLast;
+      c->odeDtPrev = dt;
+      c->odeCnPrev = std::min(c->odeCnPrev + 1, prevSiz);
+    }
+  } else {
+    for (int iB = 0; iB < 3; iB++) {
+      c->u = xLast;
+      int iter = 1;
+      for (; iter <= d->max_iter; iter++) {
+        const bool stop = iteration(iter, A[iB][iB], C[iB], [&](std::vector<double>& r) {
+          c->odeVec[iB] = r;
+          for (int64_t k = 0; k < n; k++) {
+            double v = xLast[k];
+            v -= c->u[k];
+            v *= 1.0 / dt;
+            for (int jB = 0; jB <= iB; jB++) v += c->odeVec[jB][k] * A[iB][jB];
+            r[k] = v;
+          }
+        });
+        if (stop) break;
+      }
+      if (iters_out) iters_out[iB] = std::min(iter, d->max_iter);
+    }
+    c->u = xLast;
+    for (int jB = 0; jB < 3; jB++)
+      for (int64_t k = 0; k < n; k++) c->u[k] += c->odeVec[jB][k] * (B[jB] * dt);
+  }
+  if (res_out)
+    for (int v = 0; v < nv; v++) res_out[v] = rel[v];
   return 0;
 }
 

@@ -16,7 +16,10 @@
  *   - LU-SGS (LUSGSMatrixInit, UpdateLUSGSForward/Backward,
  *     fluxJacobian0_Right_Times_du)  DNDS_FV_EulerEvaluator.cpp:995-1357,
  *                                   DNDS_FV_EulerEvaluator.hpp:928-956
- *   - ImplicitBDFDualTimeStep::Step DNDS_ODE.hpp:420-497 (order 1)
+ *   - ImplicitBDFDualTimeStep::Step DNDS_ODE.hpp:392-497 (orders 1-4)
+ *   - ImplicitSDIRK4DualTimeStep    DNDS_ODE.hpp:269-390
+ *   - GMRES_LeftPreconditioned      DNDS_Linear.hpp:12-107, over
+ *     LUSGSMatrixVec                DNDS_FV_EulerEvaluator.cpp:1062-1143
  *   - EvaluateResidual              DNDS_FV_EulerEvaluator.cpp:1557-1592
  * Deviations (documented where they occur): no Eigen (the 5x5 inverse is a
  * pivoted Gauss-Jordan instead of JacobiSVD; A_ii is SPD so both give A^-1),
@@ -139,6 +142,29 @@ int orc_lusgs_backward(orc_ctx* c, double alpha, const double* rhs, double* inc,
  * is the state at the start of the physical step; inc_out [n][nvars] may be NULL */
 int orc_implicit_iteration(orc_ctx* c, double cfl, double dt, double alpha, const double* x_last,
                            const int64_t* scan2cell, double t, int n_rec, double* inc_out);
+
+/* LUSGSMatrixVec (DNDS_FV_EulerEvaluator.cpp:1062-1143) with the diagonal of the
+ * last orc_lusgs_matrix_init; x, ax [n][nvars] */
+int orc_lusgs_matvec(orc_ctx* c, double alpha, const double* x, double* ax);
+/* GMRES_LeftPreconditioned::solve (DNDS_Linear.hpp:47-105) of LUSGSMatrixVec x = b
+ * with the LU-SGS sweeps as left preconditioner, x [n][nvars] in place (initial guess) */
+int orc_gmres_lusgs(orc_ctx* c, double alpha, int n_space, int n_restart, const double* b, double* x,
+                    const int64_t* scan2cell);
+/* dual time stepping: ImplicitBDFDualTimeStep (scheme 1, order 1..4) or
+ * ImplicitSDIRK4DualTimeStep (scheme 0), DNDS_ODE.hpp:269-497, with fsolve by
+ * LU-SGS (gmres_code 0), GMRES_LeftPreconditioned (1, DNDS_Linear.hpp:12-107)
+ * or both (2) */
+typedef struct orc_dual_settings {
+  int scheme, bdf_order;
+  double cfl;
+  int max_iter;
+  double threshold;
+  int n_rec, vol_wise, gmres_code, n_gmres_space, n_gmres_iter;
+} orc_dual_settings;
+int orc_dual_reset(orc_ctx* c);
+/* one physical step of size dt from t on the internal u; iters_out [3], res_out [nvars] may be NULL */
+int orc_dual_step(orc_ctx* c, const orc_dual_settings* d, double dt, double t, const int64_t* scan2cell,
+                  int* iters_out, double* res_out);
 
 /* setup products, for cross-checks: [n][5][5], [n][4][5][5], [n][4][5] */
 int orc_get_vr_blocks(orc_ctx* c, double* ainv, double* ainvb, double* ainv_b);

@@ -101,6 +101,10 @@ def lib():
         L.orc_lusgs_forward.argtypes = [vp, dbl, vp, vp, vp]
         L.orc_lusgs_backward.argtypes = [vp, dbl, vp, vp, vp]
         L.orc_implicit_iteration.argtypes = [vp, dbl, dbl, dbl, vp, vp, dbl, i32, vp]
+        L.orc_lusgs_matvec.argtypes = [vp, dbl, vp, vp]
+        L.orc_gmres_lusgs.argtypes = [vp, dbl, i32, i32, vp, vp, vp]
+        L.orc_dual_reset.argtypes = [vp]
+        L.orc_dual_step.argtypes = [vp, C.POINTER(OrcDual), dbl, dbl, vp, vp, vp]
         L.orc_riemann_flux.argtypes = [i32, vp, vp, dbl, dbl, vp]
         L.orc_riemann_flux.restype = None
         _lib = L
@@ -117,6 +121,23 @@ def riemann_flux(kind: int, ul, ur, gamma=1.4, dlambda=0.0) -> np.ndarray:
     f = np.zeros(4)
     lib().orc_riemann_flux(kind, _p(ul), _p(ur), gamma, dlambda, _p(f))
     return f
+
+
+class OrcDual(C.Structure):
+    """orc_dual_settings (dnds_oracle.h), field for field."""
+    _fields_ = [("scheme", C.c_int), ("bdf_order", C.c_int), ("cfl", C.c_double), ("max_iter", C.c_int),
+                ("threshold", C.c_double), ("n_rec", C.c_int), ("vol_wise", C.c_int), ("gmres_code", C.c_int),
+                ("n_gmres_space", C.c_int), ("n_gmres_iter", C.c_int)]
+
+
+def dual_settings(scheme="sdirk4", bdf_order=2, cfl=100.0, max_iter=10, threshold=1e-100, n_rec=1, vol_wise=False,
+                  gmres_code=0, n_gmres_space=10, n_gmres_iter=2):
+    """The dual-time settings with the reference's config names in mind: odeCode (scheme "sdirk4" = 0,
+    "bdf" = 1), nTimeStepInternal, rhsThresholdInternal, nInternalRecStep, useVolWiseResidual,
+    gmresCode, nGmresSpace, nGmresIter."""
+    return dict(scheme={"sdirk4": 0, "bdf": 1}[scheme], bdf_order=bdf_order, cfl=cfl, max_iter=max_iter,
+                threshold=threshold, n_rec=n_rec, vol_wise=int(vol_wise), gmres_code=gmres_code,
+                n_gmres_space=n_gmres_space, n_gmres_iter=n_gmres_iter)
 
 
 class Oracle:
@@ -257,6 +278,37 @@ class Oracle:
         o, op = self._order(scan2cell)
         lib().orc_implicit_iteration(self.h, cfl, dt, alpha, _p(xl), op, t, n_rec, _p(inc))
         return inc
+
+    def lusgs_matvec(self, x, alpha=1.0):
+        """LUSGSMatrixVec with the diagonal of the last lusgs_matrix_init."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        ax = np.empty_like(x)
+        if lib().orc_lusgs_matvec(self.h, alpha, _p(x), _p(ax)):
+            raise RuntimeError("orc_lusgs_matvec: lusgs_matrix_init first")
+        return ax
+
+    def gmres_lusgs(self, b, x0=None, alpha=1.0, n_space=10, n_restart=2, scan2cell=None):
+        """GMRES over LUSGSMatrixVec, LU-SGS preconditioned, from x0 (zero by default)."""
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=np.float64)
+        o, op = self._order(scan2cell)
+        if lib().orc_gmres_lusgs(self.h, alpha, n_space, n_restart, _p(b), _p(x), op):
+            raise RuntimeError("orc_gmres_lusgs: lusgs_matrix_init first")
+        return x
+
+    def dual_reset(self):
+        lib().orc_dual_reset(self.h)
+
+    def dual_step(self, dt, t=0.0, scan2cell=None, **settings):
+        """One physical dual-time step (see dual_settings); returns (iterations per stage, last fstop
+        ratios)."""
+        d = OrcDual(**dual_settings(**settings))
+        its = np.zeros(3, dtype=np.int32)
+        res = np.zeros(self.nv)
+        o, op = self._order(scan2cell)
+        if lib().orc_dual_step(self.h, C.byref(d), dt, t, op, _p(its), _p(res)):
+            raise RuntimeError("orc_dual_step: bad settings or a BDF history of another dt")
+        return its, res
 
     def residual(self, rhs, p=1, vol_wise=False):
         rhs = np.ascontiguousarray(rhs, dtype=np.float64)
