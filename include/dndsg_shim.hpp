@@ -11,6 +11,11 @@
 //   ImplicitSteadyGPU::Step                             ImplicitBDFDualTimeStep::Step (order 1) with the
 //                                                       EulerSolver lambdas, DNDS_ODE.hpp:444-486 and
 //                                                       DNDS_FV_EulerSolver.hpp:713-994
+//   ImplicitDualTimeStepGPU::Step                       ImplicitSDIRK4DualTimeStep / ImplicitBDFDualTimeStep
+//                                                       ::Step, DNDS_ODE.hpp:269-497, with the EulerSolver
+//                                                       lambdas (odeCode, gmresCode), :594-1226
+//   EulerEvaluatorGPU::LUSGSMatrixVec                   DNDS_FV_EulerEvaluator.cpp:1062-1143
+//   GMRES_LeftPreconditionedGPU::solve                  GMRES_LeftPreconditioned, DNDS_Linear.hpp:47-105
 //
 // The reference's ArrayDOFV / ArrayRecV live in host memory and are passed to
 // every call; here the state is resident on the GPU, and the shim moves it
@@ -121,6 +126,9 @@ class EulerEvaluatorGPU {
     c_.check(dndsg_lusgs_backward(c_.get(), alphaDiag, rhs, uInc, stream));
   }
   // sweep order: mode 0 colour batches, 1 the sequential order scan2cell (nullptr: natural), level-scheduled
+  void LUSGSMatrixVec(double alphaDiag, const double* x, double* Ax, void* stream = nullptr) {
+    c_.check(dndsg_lusgs_matvec(c_.get(), alphaDiag, x, Ax, stream));
+  }
   int SetLUSGSOrder(int mode, const int64_t* scan2cell = nullptr) {
     int nb = 0;
     c_.check(dndsg_lusgs_set_order(c_.get(), mode, scan2cell, &nb));
@@ -155,6 +163,54 @@ class ImplicitSteadyGPU {
 
  private:
   Context& c_;
+};
+
+// the reference's implicit driver: one physical step of SDIRK4 (odeCode 0) or BDF of order k
+// (odeCode 1) in dual time, fsolve by LU-SGS / GMRES per gmresCode; the ODE object's history (BDF)
+// lives in the context, Reset() where the driver would construct a new ODE object
+class ImplicitDualTimeStepGPU {
+ public:
+  ImplicitDualTimeStepGPU(Context& c, int odeCode, int bdfOrder = 2) : c_(c) {
+    d_.scheme = odeCode == 0 ? DNDSG_DUAL_SDIRK4 : DNDSG_DUAL_BDF;
+    d_.bdf_order = bdfOrder;
+    c_.check(dndsg_dual_reset(c_.get()));
+  }
+  // returns the internal iterations of the last stage
+  int Step(double dt, double tSimu, double CFL, int nTimeStepInternal, double rhsThresholdInternal,
+           int nInternalRecStep = 1, bool useVolWiseResidual = false, int gmresCode = 0, int nGmresSpace = 10,
+           int nGmresIter = 2, void* stream = nullptr) {
+    d_.cfl = CFL;
+    d_.max_iter = nTimeStepInternal;
+    d_.threshold = rhsThresholdInternal;
+    d_.n_rec = nInternalRecStep;
+    d_.vol_wise = useVolWiseResidual ? 1 : 0;
+    d_.gmres_code = gmresCode;
+    d_.n_gmres_space = nGmresSpace;
+    d_.n_gmres_iter = nGmresIter;
+    int its[3] = {0, 0, 0};
+    double res[4];
+    c_.check(dndsg_dual_step(c_.get(), &d_, dt, tSimu, its, res, stream));
+    return d_.scheme == DNDSG_DUAL_SDIRK4 ? its[2] : its[0];
+  }
+  void Reset() { c_.check(dndsg_dual_reset(c_.get())); }
+
+ private:
+  Context& c_;
+  dndsg_dual_settings d_{};
+};
+
+// GMRES over LUSGSMatrixVec with the LU-SGS sweeps as left preconditioner (the EulerSolver's
+// FA / FML pair), on device arrays; x holds the initial guess and receives the result
+class GMRES_LeftPreconditionedGPU {
+ public:
+  GMRES_LeftPreconditionedGPU(Context& c, int kSubspace) : c_(c), k_(kSubspace) {}
+  void solve(double alphaDiag, const double* b, double* x, int nRestart, void* stream = nullptr) {
+    c_.check(dndsg_gmres_lusgs(c_.get(), alphaDiag, k_, nRestart, b, x, stream));
+  }
+
+ private:
+  Context& c_;
+  int k_;
 };
 
 }  // namespace dndsg
