@@ -6,7 +6,8 @@ colour-batched or scan-order LU-SGS, stopping on the relative density increment 
 
 Cases: `euler` (inviscid, M 0.15, alpha 10), `laminar` (M 0.5, Re 5000, alpha 0), `sa` (RANS-SA,
 M 0.15, alpha 10, Re 6e6).  Prints the increment history every --every iterations and CL / CD from
-the wall force (per unit chord, free-stream dynamic pressure 0.5).
+the wall force (per unit chord, free-stream dynamic pressure 0.5); --plt writes the final state in
+the reference's Tecplot binary layout.
 """
 from __future__ import annotations
 
@@ -43,6 +44,7 @@ def main(argv=None):
     ap.add_argument("--order", choices=["natural", "colour", "lines"], default="natural")
     ap.add_argument("--precision", type=int, default=0, help="0 FP64, 1 FP32 bulk")
     ap.add_argument("--every", type=int, default=100)
+    ap.add_argument("--plt", default=None, help="write the final state as a Tecplot binary file (PrintData)")
     a = ap.parse_args(argv)
     preset, wall, mkw, alpha = CASES[a.case]
     m = M.naca0012_cmesh(wall_bc=wall, **mkw)
@@ -67,6 +69,11 @@ def main(argv=None):
             break
     cl, cd = force_coefficients(wf, alpha)
     flags, nred = s.status()
+    if a.plt:
+        from .tecplot import print_data
+
+        print_data(a.plt, m, s.get_u(), cfg, rhs=s.EvaluateRHS(0.0))
+        print(f"wrote {a.plt}")
     print(f"done: {it} iterations, rel {rel:.3e}, CL {cl:.5f}, CD {cd:.5f}, flags {flags}")
     return 0 if flags == 0 else 1
 
