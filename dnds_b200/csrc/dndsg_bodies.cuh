@@ -1054,129 +1054,4 @@ DG_HD void vr_wall_fixup(int64_t i, const HotView<T>& h) {
     for (int c = 0; c < 4; c++) h.urecNew[i * 20 + r * 4 + c] += T(h.relax * add[r][c]);
 }
 
-// -area (F(uL) + F(uR)) . n / 2 of an interior face: the FP64 part of the flux-difference form
-DG_HD void face_mean_flux(int64_t f, const double uL[4], const double uR[4], double nx, double ny, double area,
-                          double gamma, double out[4]) {
-  double FL[4], FR[4];
-  flux_n_f64(uL, nx, ny, gamma, FL);
-  flux_n_f64(uR, nx, ny, gamma, FR);
-  for (int k = 0; k < 4; k++) out[k] = -area * 0.5 * (FL[k] + FR[k]);
-}
-
-// gauss point g of an interior face, FP32 flux-difference Roe: returns -jw * (the FP32 part)
-DG_HD int gp_flux_delta32(int64_t f, int g, const HotView<float>& h, const double uL[4], const double uR[4],
-                          double nxd, double nyd, double area, float out[4], bool& bad) {
-  const int32_t L = h.faceL[f], R = h.faceR[f];
-  const float gamma = (float)h.gamma, dl = (float)h.dLam[f];
-  const float nx = (float)nxd, ny = (float)nyd;
-  float phiL[5], phiR[5];
-  for (int q = 0; q < 5; q++) {
-    phiL[q] = h.faceBasis[aos(f, g * 5 + q, 30)];
-    phiR[q] = h.faceBasis[aos(f, 15 + g * 5 + q, 30)];
-  }
-  float iL[4] = {0.f, 0.f, 0.f, 0.f}, iR[4] = {0.f, 0.f, 0.f, 0.f};
-  const float* rl = &h.urec[(int64_t)L * 20];
-  const float* rr = &h.urec[(int64_t)R * 20];
-  for (int q = 0; q < 5; q++) {
-    float a[4], b[4];
-    load_row(rl + 4 * q, a);
-    load_row(rr + 4 * q, b);
-    for (int c = 0; c < 4; c++) { iL[c] += phiL[q] * a[c]; iR[c] += phiR[q] * b[c]; }
-  }
-  float bL[4], bR[4], dmean[4], dL[4], dR[4];
-  {
-    float tL[4] = {(float)uL[0], (float)uL[1], (float)uL[2], (float)uL[3]};
-    float tR[4] = {(float)uR[0], (float)uR[1], (float)uR[2], (float)uR[3]};
-    float tD[4] = {(float)(uR[0] - uL[0]), (float)(uR[1] - uL[1]), (float)(uR[2] - uL[2]), (float)(uR[3] - uL[3])};
-    to_normal_frame(tL, nx, ny, bL);
-    to_normal_frame(tR, nx, ny, bR);
-    to_normal_frame(tD, nx, ny, dmean);
-    to_normal_frame(iL, nx, ny, dL);
-    to_normal_frame(iR, nx, ny, dR);
-  }
-  int nred = 0;
-  float UL[4], UR[4];
-  for (int c = 0; c < 4; c++) { UL[c] = bL[c] + dL[c]; UR[c] = bR[c] + dR[c]; }
-  if (UL[0] < 0.f || UL[3] - (UL[1] * UL[1] + UL[2] * UL[2]) * 0.5f / UL[0] < 0.f) {
-    for (int c = 0; c < 4; c++) { dL[c] = 0.f; UL[c] = bL[c]; }
-    nred++;
-  }
-  if (UR[0] < 0.f || UR[3] - (UR[1] * UR[1] + UR[2] * UR[2]) * 0.5f / UR[0] < 0.f) {
-    for (int c = 0; c < 4; c++) { dR[c] = 0.f; UR[c] = bR[c]; }
-    nred++;
-  }
-  if (!(UL[0] > 0.f && UR[0] > 0.f)) bad = true;
-  float DL[4], DR[4];
-  flux_delta_f32(bL, dL, gamma, DL);
-  flux_delta_f32(bR, dR, gamma, DR);
-  const float irL = 1.0f / UL[0], irR = 1.0f / UR[0];
-  const float u1 = UL[1] * irL, v1 = UL[2] * irL, u2 = UR[1] * irR, v2 = UR[2] * irR;
-  const float pL = (gamma - 1.0f) * (UL[3] - 0.5f * (UL[1] * u1 + UL[2] * v1));
-  const float pR = (gamma - 1.0f) * (UR[3] - 0.5f * (UR[1] * u2 + UR[2] * v2));
-  const float HL = (UL[3] + pL) * irL, HR = (UR[3] + pR) * irR;
-  const float sL = sqrtf(UL[0]), sR = sqrtf(UR[0]), isum = 1.0f / (sL + sR);
-  const float u = (sL * u1 + sR * u2) * isum, v = (sL * v1 + sR * v2) * isum;
-  const float vs = u * u + v * v;
-  const float H = (sL * HL + sR * HR) * isum;
-  const float a2 = (gamma - 1.0f) * (H - 0.5f * vs);
-  const float a = sqrtf(a2);
-  float lam0 = fabsf(u - a), lam1 = fabsf(u), lam3 = fabsf(u + a);
-  const float thr = fmaxf(0.05f * (sqrtf(vs) + a), dl), thrS = thr * thr;
-  if (lam0 < thr) lam0 = (lam0 * lam0 + thrS) / (2.0f * thr);
-  if (lam3 < thr) lam3 = (lam3 * lam3 + thrS) / (2.0f * thr);
-  const float d0 = dmean[0] + (dR[0] - dL[0]), d1 = dmean[1] + (dR[1] - dL[1]);
-  const float d2 = dmean[2] + (dR[2] - dL[2]), d3 = dmean[3] + (dR[3] - dL[3]);
-  const float al2 = d2 - v * d0;
-  const float d3b = d3 - al2 * v;
-  const float al1 = (gamma - 1.0f) / a2 * (d0 * (H - u * u) + u * d1 - d3b);
-  const float al0 = (d0 * (u + a) - d1 - a * al1) / (2.0f * a);
-  const float al3 = d0 - (al0 + al1);
-  const float w0 = lam0 * al0, w1 = lam1 * al1, w2 = lam1 * al2, w3 = lam3 * al3;
-  float G[4];
-  G[0] = 0.5f * (DL[0] + DR[0]) - 0.5f * (w0 + w1 + w3);
-  G[1] = 0.5f * (DL[1] + DR[1]) - 0.5f * ((u - a) * w0 + u * w1 + (u + a) * w3);
-  G[2] = 0.5f * (DL[2] + DR[2]) - 0.5f * (v * (w0 + w1 + w3) + w2);
-  G[3] = 0.5f * (DL[3] + DR[3]) - 0.5f * ((H - u * a) * w0 + 0.5f * vs * w1 + v * w2 + (H + u * a) * w3);
-  from_normal_frame(G, nx, ny);
-  const float jw = (float)(0.5 * area * l3_weight(g));
-  for (int k = 0; k < 4; k++) out[k] = -G[k] * jw;
-  return nred;
-}
-
-// gauss point g of an interior face with the full-precision Riemann solver: -jw F(UL, UR).n
-template <class T, int RIEMANN>
-DG_HD int gp_flux_full(int64_t f, int g, const HotView<T>& h, const double uL[4], const double uR[4], double nx,
-                       double ny, double area, double out[4], bool& bad) {
-  const int32_t L = h.faceL[f], R = h.faceR[f];
-  T phiL[5], phiR[5];
-  for (int q = 0; q < 5; q++) {
-    phiL[q] = h.faceBasis[aos(f, g * 5 + q, 30)];
-    phiR[q] = h.faceBasis[aos(f, 15 + g * 5 + q, 30)];
-  }
-  T iL[4] = {T(0), T(0), T(0), T(0)}, iR[4] = {T(0), T(0), T(0), T(0)};
-  const T* rl = &h.urec[(int64_t)L * 20];
-  const T* rr = &h.urec[(int64_t)R * 20];
-  for (int q = 0; q < 5; q++) {
-    T a[4], b[4];
-    load_row(rl + 4 * q, a);
-    load_row(rr + 4 * q, b);
-    for (int c = 0; c < 4; c++) { iL[c] += phiL[q] * a[c]; iR[c] += phiR[q] * b[c]; }
-  }
-  double UL[4], UR[4], incd[4];
-  for (int c = 0; c < 4; c++) incd[c] = (double)iL[c];
-  int nred = compress_rec_part(uL, incd, UL) ? 1 : 0;
-  for (int c = 0; c < 4; c++) incd[c] = (double)iR[c];
-  nred += compress_rec_part(uR, incd, UR) ? 1 : 0;
-  double a[4], b[4], F[4];
-  to_normal_frame(UL, nx, ny, a);
-  to_normal_frame(UR, nx, ny, b);
-  if (!(a[0] > 0 && b[0] > 0)) bad = true;
-  if (RIEMANN == 2) hllc_flux(a, b, h.gamma, F);
-  else roe_flux(a, b, h.gamma, h.dLam[f], F);
-  from_normal_frame(F, nx, ny);
-  const double jw = 0.5 * area * l3_weight(g);
-  for (int k = 0; k < 4; k++) out[k] = -F[k] * jw;
-  return nred;
-}
-
 }  // namespace dg
