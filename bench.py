@@ -303,6 +303,23 @@ def learned_leg(dev, grid, tol=1e-7, log=None):
            "train_samples_per_s": 20 * X.shape[0] / t_train, "val_loss": val,
            "target_mean_square": float((T ** 2).mean()), "tolerance_rms_increment": tol}
     del X, T, Xs, Ts
+    # inference throughput of the tensor-core forward (tcgen05): 4,194,304 rows of 64 features
+    rows = 4_194_304
+    Xf = torch.randn((rows, 64), device=dev, dtype=torch.float32)
+    Yf = net.forward(Xf)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        Yf = net.forward(Xf)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / 5
+    flop = 2 * (64 * 64 * 3 + 64 * 20) * rows
+    out["forward_tc"] = {"rows": rows, "ms": ms, "rows_per_s": rows / (ms * 1e-3), "tflops": flop / (ms * 1e-3) / 1e12,
+                         "gbs": rows * (64 * 4 + 20 * 4) / (ms * 1e-3) / 1e9,
+                         "note": "tcgen05.mma kind::f16, BF16 operands, FP32 accumulator in tensor memory; "
+                                 "bytes are the FP32 features read and outputs written"}
+    del Xf, Yf
     m = M.vortex_mesh(grid, True, jitter=0.2, seed=9999)
     for name, use in (("plain", None), ("learned", net)):
         s = Solver(m, cfg, device=dev, precision=1)

@@ -9,7 +9,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libdndsg.so")
 SOURCES = [os.path.join(HERE, "csrc", f) for f in ("dndsg.cu", "dndsg_bodies.cuh", "dndsg_math.cuh", "dndsg_limiter.cuh",
-                                                         "dndsg_mlp.cuh", "dndsg_sa.cuh", "dndsg_dual.cuh")]
+                                                         "dndsg_mlp.cuh", "dndsg_sa.cuh", "dndsg_dual.cuh", "dndsg_async.cuh")]
 HEADERS = [os.path.join(ROOT, "include", "dndsg.h")]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -15,6 +15,7 @@
 #include "../../include/dndsg.h"
 #include "dndsg_bodies.cuh"
 #include "dndsg_limiter.cuh"
+#include "dndsg_async.cuh"
 #include "dndsg_mlp.cuh"
 #include "dndsg_sa.cuh"
 
@@ -214,36 +215,6 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 2 : 1) k_vr(HotView<T
     if ((threadIdx.x & 31) == 0 && d2 != 0.0) atomicAdd(incAcc, d2);
   }
 }
-
-// ------------------------------------------------------------------ bulk-copy (TMA) helpers
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-// one contiguous global -> shared bulk copy completing on an mbarrier (no multicast)
-__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-               "l"(src), "r"(bytes), "r"(bar)
-               : "memory");
-}
-// bounded wait for an mbarrier phase; false if the limit ran out
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint32_t limit) {
-  uint32_t done = 0;
-  for (uint32_t it = 0; it < limit && !done; ++it) {
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(bar), "r"(parity)
-        : "memory");
-  }
-  return done != 0;
-}
-constexpr uint32_t kWaitLimit = 1u << 22;
-constexpr unsigned kFlagTimeout = 4u;
 
 // VR operator of the CTA's tile in shared memory, same AoSoA order as in global memory
 template <class T>
@@ -1320,6 +1291,7 @@ struct dndsg_mlp {
   float *P = nullptr, *M = nullptr, *V = nullptr, *G = nullptr;
   __nv_bfloat16* W = nullptr;
   double* loss = nullptr;
+  unsigned* flags = nullptr;  // kFlagTimeout from the tensor-core forward
   int64_t step = 0;
   bool attrFwd = false, attrTrain = false;
   std::string err;
@@ -1426,8 +1398,8 @@ int ensure_mlp_buffers(dndsg_ctx* c) {
       (rc = dalloc(c, c->mlpH, bytes)) || (rc = dalloc(c, c->mlpSc, sizeof(float) * 4 * c->N)) ||
       (rc = dalloc(c, c->accCount, sizeof(unsigned long long))))
     return rc;
-  DG_CUDA(c, cudaFuncSetAttribute(k_mlp_warm_start<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)sizeof(InfSmem)));
+  DG_CUDA(c, cudaFuncSetAttribute(k_mlp_tc<TcCellFeatures<T>, TcWarmStart<T>>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TcSmem)));
   return 0;
 }
 
@@ -1464,8 +1436,10 @@ int vr_to_tol(dndsg_ctx* c, const dndsg_mlp* m, double tol, int maxSweeps, int* 
       DG_CUDA(c, cudaMemsetAsync(c->accCount, 0, sizeof(unsigned long long), s));
       int sms = 148;
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-      k_mlp_warm_start<T><<<sms * 2, kInfWarps * 32, sizeof(InfSmem), s>>>(
-          view<T>(c), iters<T>(c, c->urec, c->mlpA, c->mlpB), mlp_dev(m), (T*)c->mlpM);
+      const int64_t tiles = (c->N + kTcRows - 1) / kTcRows;
+      k_mlp_tc<<<(unsigned)std::min<int64_t>(tiles, 4 * sms), kTcRows, sizeof(TcSmem), s>>>(
+          mlp_dev(m), TcCellFeatures<T>{view<T>(c), iters<T>(c, c->urec, c->mlpA, c->mlpB)},
+          TcWarmStart<T>{(const T*)c->mlpB, (T*)c->mlpM}, c->N, c->flags);
       launch_vr_from<T>(c, c->mlpB, c->urecNew, false, s);  // J(x2)
       launch_vr_from<T>(c, c->mlpM, c->mlpH, false, s);     // J(xm)
       k_zero_scalar<<<1, 1, 0, s>>>(c->scal + S_INC);
@@ -1558,7 +1532,8 @@ int dndsg_mlp_create(int device, uint64_t seed, dndsg_mlp** out) {
       cudaMalloc(&m->M, sizeof(float) * kNParam) != cudaSuccess ||
       cudaMalloc(&m->V, sizeof(float) * kNParam) != cudaSuccess ||
       cudaMalloc(&m->G, sizeof(float) * kNParam) != cudaSuccess ||
-      cudaMalloc(&m->W, sizeof(__nv_bfloat16) * kNW) != cudaSuccess || cudaMalloc(&m->loss, sizeof(double)) != cudaSuccess)
+      cudaMalloc(&m->W, sizeof(__nv_bfloat16) * kNW) != cudaSuccess || cudaMalloc(&m->loss, sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&m->flags, sizeof(unsigned)) != cudaSuccess || cudaMemset(m->flags, 0, sizeof(unsigned)) != cudaSuccess)
     return bail(DNDSG_CUDA_ERROR);
   // Glorot-uniform weights from a 64-bit LCG, zero biases and padding
   std::vector<float> p(kNParam, 0.f);
@@ -1585,7 +1560,7 @@ int dndsg_mlp_create(int device, uint64_t seed, dndsg_mlp** out) {
 void dndsg_mlp_destroy(dndsg_mlp* m) {
   if (!m) return;
   cudaSetDevice(m->device);
-  for (void* q : {(void*)m->P, (void*)m->M, (void*)m->V, (void*)m->G, (void*)m->W, (void*)m->loss})
+  for (void* q : {(void*)m->P, (void*)m->M, (void*)m->V, (void*)m->G, (void*)m->W, (void*)m->loss, (void*)m->flags})
     if (q) cudaFree(q);
   delete m;
 }
@@ -1603,14 +1578,21 @@ int dndsg_mlp_forward(dndsg_mlp* m, const float* X, int64_t n, float* Y, void* s
   if (!m || !X || !Y || n < 0) return DNDSG_BAD_ARGUMENT;
   DG_MCUDA(m, cudaSetDevice(m->device));
   if (!m->attrFwd) {
-    DG_MCUDA(m, cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(FwdSmem)));
+    DG_MCUDA(m, cudaFuncSetAttribute(k_mlp_tc<TcFeaturesX, TcOutY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sizeof(TcSmem)));
     m->attrFwd = true;
   }
   if (n == 0) return 0;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m->device);
-  k_mlp_forward<<<sms * 2, kInfWarps * 32, sizeof(FwdSmem), st(s)>>>(mlp_dev(m), X, n, Y);
+  const int64_t tiles = (n + kTcRows - 1) / kTcRows;
+  k_mlp_tc<<<(unsigned)std::min<int64_t>(tiles, 4 * sms), kTcRows, sizeof(TcSmem), st(s)>>>(
+      mlp_dev(m), TcFeaturesX{X}, TcOutY{Y}, n, m->flags);
   DG_MCUDA(m, cudaGetLastError());
+  unsigned f = 0;  // a tensor-core completion that timed out (the bounded wait ran out)
+  DG_MCUDA(m, cudaMemcpyAsync(&f, m->flags, sizeof(f), cudaMemcpyDeviceToHost, st(s)));
+  DG_MCUDA(m, cudaStreamSynchronize(st(s)));
+  if (f) return mfail(m, DNDSG_CUDA_ERROR, "tensor-core completion wait timed out");
   return 0;
 }
 

@@ -1,8 +1,9 @@
 // dndsg_mlp.cuh -- learned warm start for the VR coefficients (no counterpart in
 // the reference): a per-cell MLP 64 -> 64 -> 64 -> 64 -> 20 (SiLU), BF16 weights
-// and activations, FP32 accumulation, on the tensor cores through warp-level
-// 16x16x16 BF16 MMA (wmma), for inference and for training (forward, backward,
-// Adam).
+// and activations, FP32 accumulation.  Inference runs on the 5th-generation tensor
+// cores (tcgen05.mma with the accumulator in tensor memory, k_mlp_tc); training
+// (forward, backward, Adam) uses warp-level 16x16x16 BF16 MMA (wmma), whose
+// backward products (dz W and dz^T x over 64-row tiles) are small and transposed.
 //
 // The network extrapolates the Jacobi sequence: from the starting coefficients
 // x0 and two plain sweeps x1 = J(x0), x2 = J(x1) it proposes the converged
@@ -167,125 +168,234 @@ struct MlpDev {
   const bf16* W;    // BF16 weight matrices [kNW]
 };
 
-// ---------------------------------------------------------------- inference: features + MLP + warm start
-// dst[i] = x2[i] + y(features_i) * r, for cells i; 8 warps x 16 cells per CTA
-constexpr int kInfWarps = 8;
-struct InfSmem {
-  bf16 W[kNW];
+// ---------------------------------------------------------------- inference on the tensor cores (tcgen05)
+// 128 rows (cells) per tile, one per thread of a 128-thread CTA.  Each layer is one 128 x N x 64
+// product, four tcgen05.mma (kind::f16: BF16 operands in shared memory, FP32 accumulator in
+// tensor memory, K = 16 each) issued by one thread and completed on an mbarrier; every thread then
+// reads its own accumulator row with tcgen05.ld (warp w owns tensor-memory lanes 32w..32w+31, which
+// are rows 32w..32w+31 of the 128-row accumulator), adds the bias, applies SiLU and writes the next
+// layer's operand row.  Operands use the K-major, no-swizzle canonical layout: 8-row x 16-byte core
+// matrices, core matrices along K 128 B apart (leading byte offset), 8-row groups 1024 B apart
+// (stride byte offset), so the K step k0 of an instruction starts 32 k0 / 16 bytes further.
+constexpr int kTcRows = 128;
+constexpr int kTcCols = 64;  // tensor-memory columns: the widest layer (N = 64, FP32)
+struct TcSmem {
+  alignas(128) unsigned char W[4][kHid * 64 * 2];  // W1..W4 (W4: 32 rows used), core-matrix layout
+  alignas(128) unsigned char A[kTcRows * 64 * 2];  // the current layer's input rows, same layout
   float b[3 * kHid + kOutP];
-  bf16 x[kInfWarps][16 * kInP];
-  float z[kInfWarps][16 * 64];
-  bf16 hA[kInfWarps][16 * 64];
-  float sc[kInfWarps][16 * 4];
+  uint64_t bar;
+  uint32_t tmem;
 };
 
-template <class T>
-__global__ void __launch_bounds__(kInfWarps * 32) k_mlp_warm_start(HotView<T> h, MlpIters<T> it, MlpDev m, T* dst) {
-  extern __shared__ __align__(128) unsigned char raw[];
-  InfSmem& S = *reinterpret_cast<InfSmem*>(raw);
-  for (int e = threadIdx.x; e < kNW; e += blockDim.x) S.W[e] = m.W[e];
-  for (int e = threadIdx.x; e < 3 * kHid + kOutP; e += blockDim.x) {
-    int off = e < kHid ? kOffB1 + e : e < 2 * kHid ? kOffB2 + e - kHid : e < 3 * kHid ? kOffB3 + e - 2 * kHid
-                                                                                    : kOffB4 + e - 3 * kHid;
-    S.b[e] = m.P[off];
-  }
-  __syncthreads();
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t tiles = (h.N + 15) / 16;
-  for (int64_t tile = (int64_t)blockIdx.x * kInfWarps + w; tile < tiles; tile += (int64_t)gridDim.x * kInfWarps) {
-    const int64_t i0 = tile * 16;
-    if (lane < 16) {
-      const int64_t i = i0 + lane;
-      float x[kInP], sc[4];
-      if (i < h.N) mlp_cell_features<T>(i, h, it, x, sc);
-      else { for (int k = 0; k < kInP; k++) x[k] = 0.f; for (int v = 0; v < 4; v++) sc[v] = 0.f; }
-      for (int k = 0; k < kInP; k++) S.x[w][lane * kInP + k] = __float2bfloat16(x[k]);
-      for (int v = 0; v < 4; v++) S.sc[w][lane * 4 + v] = sc[v];
-    }
-    __syncwarp();
-    const bf16* in = S.x[w];
-    int ldin = kInP;
-    for (int layer = 0; layer < 4; layer++) {
-      if (layer == 0) warp_gemm_xwT<kInP, kHid>(in, ldin, S.W + kWOff1, S.z[w]);
-      else if (layer == 1) warp_gemm_xwT<kHid, kHid>(in, ldin, S.W + kWOff2, S.z[w]);
-      else if (layer == 2) warp_gemm_xwT<kHid, kHid>(in, ldin, S.W + kWOff3, S.z[w]);
-      else warp_gemm_xwT<kHid, kOutP>(in, ldin, S.W + kWOff4, S.z[w]);
-      __syncwarp();
-      if (layer < 3) {
-        for (int e = lane; e < 16 * 64; e += 32) {
-          float zz = S.z[w][e] + S.b[layer * kHid + (e & 63)];
-          S.hA[w][e] = __float2bfloat16(silu(zz));
-        }
-        __syncwarp();
-        in = S.hA[w];
-        ldin = 64;
-      }
-    }
-    // y = z + b4; dst = x2 + y * r
-    for (int e = lane; e < 16 * kOut; e += 32) {
-      const int r = e / kOut, o = e - r * kOut;
-      const int64_t i = i0 + r;
-      if (i < h.N) {
-        const float y = S.z[w][r * 64 + o] + S.b[3 * kHid + o];
-        const int v = o & 3;
-        dst[i * 20 + o] = (T)((double)it.x2[i * 20 + o] + (double)y * (double)S.sc[w][r * 4 + v]);
-      }
-    }
-    __syncwarp();
+// byte offset of element (row, k) of a 64-wide K-major operand in the core-matrix layout
+__device__ __forceinline__ uint32_t cm_off(int row, int k) {
+  return (uint32_t)((row >> 3) * 1024 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
+}
+// shared-memory matrix descriptor: start address, leading byte offset 128, stride byte offset 1024,
+// descriptor version 1, no swizzle (all addresses and offsets in 16-byte units)
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         (1ull << 46);
+}
+// instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both K-major, M = 128, N
+__host__ __device__ constexpr uint32_t umma_idesc(int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kTcRows >> 4) << 24);
+}
+__device__ __forceinline__ void umma_bf16(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, int acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+          dtmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc)
+      : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void proxy_fence_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// 16 consecutive FP32 columns of this thread's accumulator row
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float v[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr)
+      : "memory");
+  for (int k = 0; k < 16; k++) v[k] = __uint_as_float(r[k]);
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+constexpr int kTcRowsX = kTcRows;
+__device__ __forceinline__ uint32_t cm_off_x(int row, int k) { return cm_off(row, k); }
+
+// one 64-value row of the layer input, as BF16, into the operand buffer
+__device__ __forceinline__ void tc_store_row(unsigned char* A, int row, const float* x) {
+  for (int kc = 0; kc < 8; kc++) {
+    __nv_bfloat162 p[4];
+    for (int e = 0; e < 4; e++) p[e] = __floats2bfloat162_rn(x[8 * kc + 2 * e], x[8 * kc + 2 * e + 1]);
+    *reinterpret_cast<uint4*>(A + cm_off(row, 8 * kc)) = *reinterpret_cast<uint4*>(p);
   }
 }
 
-// plain forward on given features X [n][36] -> Y [n][20] (FP32), for tests
-struct FwdSmem {
-  bf16 W[kNW];
-  float b[3 * kHid + kOutP];
-  bf16 x[kInfWarps][16 * kInP];
-  float z[kInfWarps][16 * 64];
-  bf16 hA[kInfWarps][16 * 64];
+// inputs and outputs of the tensor-core forward
+// Src::kTile: the whole tile is loaded by the CTA together (coalesced), else row by row;
+// Dst::kTile: the outputs go through shared memory and leave as one contiguous block
+struct TcFeaturesX {  // given features X [n][64]
+  static constexpr bool kTile = true;
+  const float* X;
+  // the 128 x 64 tile starting at row r0 into the operand buffer, 32 B of X per thread and step
+  __device__ void load_tile(int64_t r0, int64_t n, unsigned char* A) const {
+    for (int e = threadIdx.x; e < kTcRowsX * 8; e += blockDim.x) {
+      const int row = e >> 3, kc = e & 7;
+      float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      if (r0 + row < n) {
+        const float4* q = reinterpret_cast<const float4*>(X + (r0 + row) * kIn + 8 * kc);
+        const float4 a = q[0], b = q[1];
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+      }
+      __nv_bfloat162 p[4];
+      for (int j = 0; j < 4; j++) p[j] = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+      *reinterpret_cast<uint4*>(A + cm_off_x(row, 8 * kc)) = *reinterpret_cast<uint4*>(p);
+    }
+  }
+  __device__ void load(int64_t, int64_t, float*, float*) const {}
 };
-__global__ void __launch_bounds__(kInfWarps * 32) k_mlp_forward(MlpDev m, const float* X, int64_t n, float* Y) {
+struct TcOutY {  // Y [n][20] = the network output
+  static constexpr bool kTile = true;
+  float* Y;
+  // stage [128][20] FP32 (in the free operand buffer) -> one contiguous store of the tile
+  __device__ void store_tile(int64_t r0, int64_t n, const float* stage) const {
+    const int64_t m = min((int64_t)kTcRowsX, n - r0) * kOut;
+    for (int64_t e = threadIdx.x; e < m; e += blockDim.x) Y[r0 * kOut + e] = stage[e];
+  }
+  __device__ void store(int64_t, int64_t, const float*, const float*) const {}
+};
+template <class T>
+struct TcCellFeatures {  // the warm-start features of cell r
+  static constexpr bool kTile = false;
+  HotView<T> h;
+  MlpIters<T> it;
+  __device__ void load(int64_t r, int64_t n, float x[kInP], float sc[4]) const {
+    if (r < n) mlp_cell_features<T>(r, h, it, x, sc);
+    else {
+      for (int k = 0; k < kInP; k++) x[k] = 0.f;
+      for (int v = 0; v < 4; v++) sc[v] = 0.f;
+    }
+  }
+  __device__ void load_tile(int64_t, int64_t, unsigned char*) const {}
+};
+template <class T>
+struct TcWarmStart {  // dst = x2 + y r
+  static constexpr bool kTile = false;
+  const T* x2;
+  T* dst;
+  __device__ void store(int64_t r, int64_t n, const float* y, const float* sc) const {
+    if (r < n)
+      for (int o = 0; o < kOut; o++) dst[r * 20 + o] = (T)((double)x2[r * 20 + o] + (double)y[o] * (double)sc[o & 3]);
+  }
+  __device__ void store_tile(int64_t, int64_t, const float*) const {}
+};
+
+template <class Src, class Dst>
+__global__ void __launch_bounds__(kTcRows) k_mlp_tc(MlpDev m, Src src, Dst dst, int64_t n, unsigned* flags) {
   extern __shared__ __align__(128) unsigned char raw[];
-  FwdSmem& S = *reinterpret_cast<FwdSmem*>(raw);
-  for (int e = threadIdx.x; e < kNW; e += blockDim.x) S.W[e] = m.W[e];
-  for (int e = threadIdx.x; e < 3 * kHid + kOutP; e += blockDim.x) {
-    int off = e < kHid ? kOffB1 + e : e < 2 * kHid ? kOffB2 + e - kHid : e < 3 * kHid ? kOffB3 + e - 2 * kHid
-                                                                                    : kOffB4 + e - 3 * kHid;
+  TcSmem& S = *reinterpret_cast<TcSmem*>(raw);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  // the weights (row-major [N][64] BF16 in global memory) into the core-matrix layout, 16 B at a time
+  for (int e = tid; e < (3 * kHid + kOutP) * 8; e += blockDim.x) {
+    const int row = e >> 3, kc = e & 7;
+    const int layer = row < 3 * kHid ? row / kHid : 3, rl = row - layer * kHid;
+    const int woff = layer == 0 ? kWOff1 : layer == 1 ? kWOff2 : layer == 2 ? kWOff3 : kWOff4;
+    *reinterpret_cast<uint4*>(S.W[layer] + cm_off(rl, 8 * kc)) =
+        *reinterpret_cast<const uint4*>(m.W + woff + rl * 64 + 8 * kc);
+  }
+  for (int e = tid; e < 3 * kHid + kOutP; e += blockDim.x) {
+    const int off = e < kHid ? kOffB1 + e : e < 2 * kHid ? kOffB2 + e - kHid : e < 3 * kHid ? kOffB3 + e - 2 * kHid
+                                                                                          : kOffB4 + e - 3 * kHid;
     S.b[e] = m.P[off];
   }
+  const uint32_t bar = smem_u32(&S.bar);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem)),
+                 "r"(kTcCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    fence_mbar_init();
+  }
+  tc_fence_before();
   __syncthreads();
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t tiles = (n + 15) / 16;
-  for (int64_t tile = (int64_t)blockIdx.x * kInfWarps + w; tile < tiles; tile += (int64_t)gridDim.x * kInfWarps) {
-    const int64_t r0 = tile * 16;
-    for (int e = lane; e < 16 * kInP; e += 32) {
-      const int r = e / kInP, k = e - r * kInP;
-      const float v = (r0 + r < n && k < kIn) ? X[(r0 + r) * kIn + k] : 0.f;
-      S.x[w][e] = __float2bfloat16(v);
+  tc_fence_after();
+  const uint32_t tbase = S.tmem, trow = tbase + ((uint32_t)(warp * 32) << 16);
+  const uint32_t aAddr = smem_u32(S.A);
+  uint32_t phase = 0;
+  bool failed = false;
+  for (int64_t tile = blockIdx.x; tile * kTcRows < n && !failed; tile += gridDim.x) {
+    const int64_t r = tile * kTcRows + tid;
+    float x[kInP], sc[4] = {0.f, 0.f, 0.f, 0.f};
+    if constexpr (Src::kTile) {
+      src.load_tile(tile * kTcRows, n, S.A);
+    } else {
+      src.load(r, n, x, sc);
+      tc_store_row(S.A, tid, x);
     }
-    __syncwarp();
-    const bf16* in = S.x[w];
-    int ldin = kInP;
-    for (int layer = 0; layer < 4; layer++) {
-      if (layer == 0) warp_gemm_xwT<kInP, kHid>(in, ldin, S.W + kWOff1, S.z[w]);
-      else if (layer == 1) warp_gemm_xwT<kHid, kHid>(in, ldin, S.W + kWOff2, S.z[w]);
-      else if (layer == 2) warp_gemm_xwT<kHid, kHid>(in, ldin, S.W + kWOff3, S.z[w]);
-      else warp_gemm_xwT<kHid, kOutP>(in, ldin, S.W + kWOff4, S.z[w]);
-      __syncwarp();
+    for (int layer = 0; layer < 4 && !failed; layer++) {
+      const int N = layer < 3 ? kHid : kOutP;
+      proxy_fence_smem();  // the operand rows written by this thread, to the tensor cores
+      tc_fence_before();
+      __syncthreads();
+      if (tid == 0) {
+        tc_fence_after();
+        const uint32_t wAddr = smem_u32(S.W[layer]);
+        for (int ks = 0; ks < 4; ks++)
+          umma_bf16(tbase, umma_desc(aAddr + 256 * ks), umma_desc(wAddr + 256 * ks), layer < 3 ? umma_idesc(kHid)
+                                                                                              : umma_idesc(kOutP),
+                    ks > 0);
+        umma_commit(bar);
+      }
+      const bool ok = mbar_wait(bar, phase, kWaitLimit);
+      phase ^= 1u;
+      if (__syncthreads_or(!ok)) {
+        failed = true;
+        break;
+      }
+      tc_fence_after();
+      float z[64];
+      for (int c0 = 0; c0 < N; c0 += 16) tmem_ld16(trow + c0, z + c0);
+      tmem_wait_ld();
       if (layer < 3) {
-        for (int e = lane; e < 16 * 64; e += 32) {
-          float zz = S.z[w][e] + S.b[layer * kHid + (e & 63)];
-          S.hA[w][e] = __float2bfloat16(silu(zz));
+        for (int k = 0; k < 64; k++) x[k] = silu(z[k] + S.b[layer * kHid + k]);
+        tc_store_row(S.A, tid, x);
+      } else {
+        float y[kOut];
+        for (int o = 0; o < kOut; o++) y[o] = z[o] + S.b[3 * kHid + o];
+        if constexpr (Dst::kTile) {  // the operand buffer is free once the last product completed
+          float* stage = reinterpret_cast<float*>(S.A);
+          for (int o = 0; o < kOut; o++) stage[tid * kOut + o] = y[o];
+          __syncthreads();
+          dst.store_tile(tile * kTcRows, n, stage);
+        } else {
+          dst.store(r, n, y, sc);
         }
-        __syncwarp();
-        in = S.hA[w];
-        ldin = 64;
       }
     }
-    for (int e = lane; e < 16 * kOut; e += 32) {
-      const int r = e / kOut, o = e - r * kOut;
-      if (r0 + r < n) Y[(r0 + r) * kOut + o] = S.z[w][r * 64 + o] + S.b[3 * kHid + o];
-    }
-    __syncwarp();
+    tc_fence_before();
+    __syncthreads();  // every row is read out before the next tile's products overwrite the accumulator
+    tc_fence_after();
+  }
+  if (failed && tid == 0) {
+    atomicOr(flags, kFlagTimeout);
+    mbar_wait(bar, phase ^ 1u, kWaitLimit);  // the last commit, if it is still in flight
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(kTcCols) : "memory");
   }
 }
 

@@ -311,7 +311,10 @@ const char* dndsg_mlp_last_error(dndsg_mlp* mlp);
  * set_params also resets the Adam moments */
 int dndsg_mlp_set_params(dndsg_mlp* mlp, const float* params);
 int dndsg_mlp_get_params(dndsg_mlp* mlp, float* params);
-/* Y [n][20] = network(X [n][64]), device arrays */
+/* Y [n][20] = network(X [n][64]), device arrays.  Runs on the 5th-generation
+ * tensor cores (tcgen05.mma, 128 rows per tile, FP32 accumulator in tensor
+ * memory); returns when the forward is complete, DNDSG_CUDA_ERROR if a
+ * tensor-core completion wait ran out (bounded wait) */
 int dndsg_mlp_forward(dndsg_mlp* mlp, const float* X, int64_t n, float* Y, void* stream);
 /* mean-square loss over n rows x 20 outputs against targets T [n][20] (device)
  * and its gradient (host [DNDSG_MLP_NPARAM], may be NULL); synchronous */

@@ -80,6 +80,24 @@ def test_forward_matches_oracle():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 127, 128, 129, 4097])
+def test_forward_tile_edges_and_row_independence(n):
+    """The tensor-core forward works on 128-row tiles: partial tiles agree with the oracle, and each
+    row's output depends on that row only (permuting the rows permutes the outputs bit for bit)."""
+    torch, dev = _torch()
+    from dnds_b200.learned import WarmStartNet
+
+    p = mo.random_params(5)
+    net = WarmStartNet(0, params=p)
+    X = np.random.default_rng(n).normal(size=(n, mo.N_IN)).astype(np.float32)
+    Y = net.forward(torch.from_numpy(X).to(dev)).cpu().numpy()
+    assert _rel(Y, mo.forward(p, X, bf=True)) < 1e-3
+    perm = np.random.default_rng(1).permutation(n)
+    Yp = net.forward(torch.from_numpy(X[perm]).to(dev)).cpu().numpy()
+    assert np.array_equal(Yp, Y[perm])
+
+
+@pytest.mark.gpu
 def test_gradient_matches_oracle():
     torch, dev = _torch()
     from dnds_b200.learned import WarmStartNet
