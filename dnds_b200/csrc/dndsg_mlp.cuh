@@ -187,6 +187,10 @@ struct TcSmem {
   uint32_t tmem;
 };
 
+// tensor memory: every resident CTA holds kTcCols of the SM's 512 columns, and an allocation that
+// cannot be met waits; the launch keeps at most 4 CTAs per SM (shared memory and registers allow 4)
+static_assert(sizeof(TcSmem) > 233472 / 9, "at most 8 CTAs of k_mlp_tc per SM");
+
 // byte offset of element (row, k) of a 64-wide K-major operand in the core-matrix layout
 __device__ __forceinline__ uint32_t cm_off(int row, int k) {
   return (uint32_t)((row >> 3) * 1024 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
@@ -226,6 +230,15 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float v[16]) {
   for (int k = 0; k < 16; k++) v[k] = __uint_as_float(r[k]);
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+// SiLU through the identity sigmoid(z) = (1 + tanh(z / 2)) / 2 with the hardware tanh: one
+// special-function operation per activation instead of an exponential and a reciprocal (the
+// special-function unit bounds this kernel's epilogue); its error (about 2^-11 relative) is below
+// the BF16 rounding the activation gets next
+__device__ __forceinline__ float silu_tanh(float z) {
+  float t;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(0.5f * z));
+  return 0.5f * z * (1.0f + t);
+}
 
 constexpr int kTcRowsX = kTcRows;
 __device__ __forceinline__ uint32_t cm_off_x(int row, int k) { return cm_off(row, k); }
@@ -368,7 +381,7 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_tc(MlpDev m, Src src, Dst dst, 
       for (int c0 = 0; c0 < N; c0 += 16) tmem_ld16(trow + c0, z + c0);
       tmem_wait_ld();
       if (layer < 3) {
-        for (int k = 0; k < 64; k++) x[k] = silu(z[k] + S.b[layer * kHid + k]);
+        for (int k = 0; k < 64; k++) x[k] = silu_tanh(z[k] + S.b[layer * kHid + k]);
         tc_store_row(S.A, tid, x);
       } else {
         float y[kOut];
