@@ -205,13 +205,44 @@ def training_set(tol: float = 1e-7, steps: int = 8, n: int = 256, seeds=(11, 12)
     return torch.cat(Xs), torch.cat(Ts)
 
 
+def time_forward(rows_list=(1 << 20, 1 << 22), reps: int = 5, seed: int = 7):
+    """CUDA-event time of the tensor-core forward on random features; returns [(rows, ms)]."""
+    import torch
+
+    net = WarmStartNet(0, seed=seed)
+    dev = torch.device("cuda:0")
+    out = []
+    for rows in rows_list:
+        X = torch.randn((rows, N_IN), device=dev)
+        net.forward(X)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            net.forward(X)
+        e1.record()
+        torch.cuda.synchronize()
+        out.append((rows, e0.elapsed_time(e1) / reps))
+    return out
+
+
 def main(argv=None):
     import argparse
     import time
 
     import torch
 
-    ap = argparse.ArgumentParser(description="harvest, train and save the VR warm-start network")
+    if argv is None:
+        import sys
+
+        argv = sys.argv[1:]
+    if "--time-forward" in argv:
+        for rows, ms in time_forward():
+            flop = 2 * (N_IN * 64 + 64 * 64 * 2 + 64 * N_OUT) * rows
+            print(f"{rows} rows: {ms:.4f} ms, {rows / ms / 1e6:.3f}e9 rows/s, {flop / ms / 1e9:.1f} TFLOP/s, "
+                  f"{rows * (4 * N_IN + 4 * N_OUT) / ms / 1e6:.0f} GB/s")
+        return
+    ap = argparse.ArgumentParser(description="harvest, train and save the VR warm-start network "
+                                             "(--time-forward: time the tensor-core forward instead)")
     ap.add_argument("--out", default=WEIGHTS)
     ap.add_argument("--tol", type=float, default=1e-7)
     ap.add_argument("--steps", type=int, default=8)
