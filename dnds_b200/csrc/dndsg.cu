@@ -223,8 +223,12 @@ struct VrOpSmem {
   __device__ __forceinline__ T operator()(int k, int e) const { return p[(k * 30 + e) * 32]; }
 };
 
+// cells per CTA of the VR sweep: one 32-cell AoSoA block (the smallest contiguous operator tile).
+// Small tiles keep many CTAs resident per SM, so tile loads and gathers of different CTAs overlap
+// (measured on 2,097,152 triangles, FP32: 128 cells 0.233 ms = 77% of HBM peak, 64: 0.226, 32:
+// 0.212 = 85%; FP64: 64 cells 0.367 ms, 32: 0.358)
 template <class T>
-constexpr int vr_tile() { return sizeof(T) == 4 ? 128 : 64; }
+constexpr int vr_tile() { return 32; }
 
 // VR Jacobi sweep, 4 threads per cell (one per conserved variable).  One
 // elected thread bulk-copies the CTA's TILE-cell operator tile (contiguous in the
