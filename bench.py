@@ -43,7 +43,7 @@ KERNELS_PER_STEP = 14  # init, dt face, dt cell, dt finalize, 3 x (VR, flux, upd
 # DRAM bytes (read + write) per launch of the FP32 VR sweep: ncu dram__bytes_read.sum +
 # dram__bytes_write.sum on the 512x512 mesh (292.25 MB for 524,288 cells, see
 # profiles/vr_sweep_fp32_vortex_tri512.md) scaled by the cell count (x4) to this workload
-VR_TRAFFIC_FP32 = 290.09e6 * 4  # ncu DRAM read+write of one FP32 VR sweep on 524,288 cells, scaled to 2,097,152
+VR_TRAFFIC_FP32 = 291.23e6 * 4  # ncu DRAM read+write of one FP32 VR sweep on 524,288 cells, scaled to 2,097,152
 
 
 def dist_env():
