@@ -49,6 +49,7 @@ struct dndsg_ctx {
   void* faceGrad = nullptr;   // T, viscous contexts only
   // SA contexts (nvars 5): the fifth variable in its own arrays
   bool sa = false;
+  double* saDmat = nullptr;  // the U5 LU-SGS diagonal itself (GMRES matrix-vector product)
   double *saU = nullptr, *saULast = nullptr, *saRhs = nullptr, *saFlux = nullptr, *saInc = nullptr, *saDinv = nullptr,
          *saSrcJac = nullptr, *saDWall = nullptr, *saCellGp = nullptr;
   void *saUrec = nullptr, *saUrecNew = nullptr;  // T [N][5]
@@ -79,7 +80,7 @@ struct dndsg_ctx {
   std::vector<double*> odeVec, gmV;
   int odeOrder = 0, odeCnPrev = 0, odePrevStart = 0;
   double odeDtPrev = 0.0;
-  double *gmTmp = nullptr, *gmMLb = nullptr, *gmH = nullptr, *gmPartial = nullptr;
+  double *gmTmp = nullptr, *gmMLb = nullptr, *gmH = nullptr, *gmPartial = nullptr, *gmB = nullptr, *gmX = nullptr;
   // state
   double *u = nullptr, *uLast = nullptr, *rhs = nullptr, *dt = nullptr, *flux = nullptr, *lamA = nullptr,
          *dLam = nullptr, *scal = nullptr, *partial = nullptr;
@@ -2507,10 +2508,14 @@ __global__ void __launch_bounds__(kLevelBlock) k_lusgs_levels_sa(HotView<T> h, S
   }
 }
 
-// the U5 diagonal: the flow one plus alpha * the source Jacobian (LUSGSMatrixInit)
-__global__ void k_sa_diag(int64_t N, const double* Dinv, const double* srcJac, double alpha, double* DinvS) {
+// the U5 diagonal: the flow one plus alpha * the source Jacobian (LUSGSMatrixInit), its inverse
+// for the sweeps and (DS, may be null) itself for LUSGSMatrixVec
+__global__ void k_sa_diag(int64_t N, const double* D, const double* srcJac, double alpha, double* DinvS, double* DS) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i < N) DinvS[i] = 1.0 / (1.0 / Dinv[i] + alpha * srcJac[i]);
+  if (i >= N) return;
+  const double d = D[i] + alpha * srcJac[i];
+  DinvS[i] = 1.0 / d;
+  if (DS) DS[i] = d;
 }
 
 // U5 parts of one pseudo-time iteration: the BDF rhs, CompressInc of rhs * dTau (dTau = dt / alpha)
@@ -2580,9 +2585,12 @@ void run_rhs_sa(dndsg_ctx* c, cudaStream_t s) {
 }
 
 template <class T>
-void launch_lusgs_sweep_sa(dndsg_ctx* c, bool forward, double alpha, cudaStream_t s) {
+void launch_lusgs_sweep_sa(dndsg_ctx* c, bool forward, double alpha, const double* rhs4, double* inc4,
+                           const double* rhs5, double* inc5, cudaStream_t s) {
   HotView<T> h = view<T>(c);
   SaView<T> sa = sa_view<T>(c);
+  sa.rhs = const_cast<double*>(rhs5);  // read only by the sweeps
+  sa.inc = inc5;
   const std::vector<int64_t>& off = forward ? c->fwdOff : c->bwdOff;
   const int32_t* cells = forward ? c->fwdCells : c->bwdCells;
   const int nb = (int)off.size() - 1;
@@ -2594,30 +2602,30 @@ void launch_lusgs_sweep_sa(dndsg_ctx* c, bool forward, double alpha, cudaStream_
     LuMatS* rec = (LuMatS*)c->lusgsMat;
     if (forward) {
       k_lusgs_pack_mat<T, true, true><<<grid_for(c->N), kBlock, 0, s>>>(h, sa, cells, nf, nj, np, c->N, alpha, c->Dinv,
-                                                                         c->rhs, c->inc, rec);
-      k_lusgs_levels_mat<T, true, true><<<1, mat_threads<true>(), mat_smem<true>(), s>>>(sa, rec, od, nb, c->inc, c->flags);
+                                                                         rhs4, inc4, rec);
+      k_lusgs_levels_mat<T, true, true><<<1, mat_threads<true>(), mat_smem<true>(), s>>>(sa, rec, od, nb, inc4, c->flags);
     } else {
       k_lusgs_pack_mat<T, false, true><<<grid_for(c->N), kBlock, 0, s>>>(h, sa, cells, nf, nj, np, c->N, alpha, c->Dinv,
-                                                                          c->rhs, c->inc, rec);
-      k_lusgs_levels_mat<T, false, true><<<1, mat_threads<true>(), mat_smem<true>(), s>>>(sa, rec, od, nb, c->inc, c->flags);
+                                                                          rhs4, inc4, rec);
+      k_lusgs_levels_mat<T, false, true><<<1, mat_threads<true>(), mat_smem<true>(), s>>>(sa, rec, od, nb, inc4, c->flags);
     }
     return;
   }
   if (c->lusgsOrder == 1) {  // many narrow levels: one block walks them all
     const int64_t* od = forward ? c->fwdOffDev : c->bwdOffDev;
     if (forward)
-      k_lusgs_levels_sa<T, true><<<1, kLevelBlock, 0, s>>>(h, sa, c->rankOf, cells, od, nb, alpha, c->Dinv, c->rhs, c->inc);
+      k_lusgs_levels_sa<T, true><<<1, kLevelBlock, 0, s>>>(h, sa, c->rankOf, cells, od, nb, alpha, c->Dinv, rhs4, inc4);
     else
-      k_lusgs_levels_sa<T, false><<<1, kLevelBlock, 0, s>>>(h, sa, c->rankOf, cells, od, nb, alpha, c->Dinv, c->rhs, c->inc);
+      k_lusgs_levels_sa<T, false><<<1, kLevelBlock, 0, s>>>(h, sa, c->rankOf, cells, od, nb, alpha, c->Dinv, rhs4, inc4);
     return;
   }
   for (int k = 0; k < nb; k++) {
     const int64_t b = off[k], n = off[k + 1] - b;
     if (n == 0) continue;
     if (forward)
-      k_lusgs_batch_sa<T, true><<<grid_for(n), kBlock, 0, s>>>(h, sa, c->rankOf, cells + b, n, alpha, c->Dinv, c->rhs, c->inc);
+      k_lusgs_batch_sa<T, true><<<grid_for(n), kBlock, 0, s>>>(h, sa, c->rankOf, cells + b, n, alpha, c->Dinv, rhs4, inc4);
     else
-      k_lusgs_batch_sa<T, false><<<grid_for(n), kBlock, 0, s>>>(h, sa, c->rankOf, cells + b, n, alpha, c->Dinv, c->rhs, c->inc);
+      k_lusgs_batch_sa<T, false><<<grid_for(n), kBlock, 0, s>>>(h, sa, c->rankOf, cells + b, n, alpha, c->Dinv, rhs4, inc4);
   }
 }
 
@@ -2636,9 +2644,9 @@ int run_implicit_sa(dndsg_ctx* c, double cfl, double dtPhys, double alpha, int n
   k_sa_rhs_fix<<<grid_for(c->N), kBlock, 0, s>>>(c->N, c->saU, c->saULast, c->dt, alpha, dtInv, c->saRhs);
   HotView<T> h = view<T>(c);
   k_lusgs_init<T><<<grid_for(c->N), kBlock, 0, s>>>(h, dtInv, alpha, c->Dinv, c->Dmat);
-  k_sa_diag<<<grid_for(c->N), kBlock, 0, s>>>(c->N, c->Dinv, c->saSrcJac, alpha, c->saDinv);
-  launch_lusgs_sweep_sa<T>(c, true, alpha, s);
-  launch_lusgs_sweep_sa<T>(c, false, alpha, s);
+  k_sa_diag<<<grid_for(c->N), kBlock, 0, s>>>(c->N, c->Dmat, c->saSrcJac, alpha, c->saDinv, nullptr);
+  launch_lusgs_sweep_sa<T>(c, true, alpha, c->rhs, c->inc, c->saRhs, c->saInc, s);
+  launch_lusgs_sweep_sa<T>(c, false, alpha, c->rhs, c->inc, c->saRhs, c->saInc, s);
   DG_CUDA(c, cudaMemsetAsync(c->resAcc, 0, sizeof(double) * 16, s));
   k_add_inc<<<grid_for(c->N), kBlock, 0, s>>>(c->N, c->u, c->inc, c->vol, volWise, c->resAcc);
   k_sa_add_inc<<<grid_for(c->N), kBlock, 0, s>>>(c->N, c->saU, c->saInc, c->vol, volWise, c->resAcc + 8);

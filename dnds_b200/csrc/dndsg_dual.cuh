@@ -4,7 +4,8 @@
 // with the EulerSolver lambdas fdtau / frhs / fsolve / fstop (DNDS_FV_EulerSolver.hpp:713-1061), and
 // fsolve's Krylov option: GMRES_LeftPreconditioned (DNDS_Linear.hpp:12-107) over LUSGSMatrixVec
 // (DNDS_FV_EulerEvaluator.cpp:1062-1143), the LU-SGS forward + backward sweeps being the left
-// preconditioner.  Contexts with 4 variables.
+// preconditioner.  Contexts with 4 variables, and SA contexts (the U5 part of every vector after
+// the [N][4] flow part; its rhs and increment pass through CompressInc as in fsolve).
 //
 // Vectors are the [N][4] increments / states in device memory.  The Arnoldi loop keeps the
 // Hessenberg matrix on the device (dot products by a two-pass reduction whose summation order
@@ -160,6 +161,49 @@ __global__ void __launch_bounds__(kBlock) k_lusgs_matvec(HotView<T> h, double al
   for (int v = 0; v < 4; v++) Ax[i * 4 + v] = d * x[i * 4 + v] - buf[v];
 }
 
+// the U5 row of LUSGSMatrixVec: Ax5_i = D5_i x5_i + sum_j (alpha/2) A_f / V_i dF5 with
+// dF5 = x5_j vn + u5_j dvn - lambda_f x5_j (the U5 entry of fluxJacobian0_Right_Times_du)
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_lusgs_matvec_sa5(HotView<T> h, const double* u5, double alpha,
+                                                             const double* D5, const double* x4, const double* x5,
+                                                             double* Ax5) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= h.N) return;
+  double buf = 0;
+  for (int k = 0; k < h.nfmax; k++) {
+    const int32_t sf = h.cellFace[aos(i, k, h.nfmax)];
+    if (sf == kEmptySlot) continue;
+    const int32_t f = sf >= 0 ? sf : ~sf;
+    const int32_t j = sf >= 0 ? h.faceR[f] : h.faceL[f];
+    if (j < 0) continue;
+    const double sg = sf >= 0 ? 1.0 : -1.0, area = h.faceArea[f];
+    const double nx = sg * h.faceNormal[2 * f], ny = sg * h.faceNormal[2 * f + 1], lam = h.lamA[f] / area;
+    double U[4], dU[4];
+    load4<T>(&h.u[(int64_t)j * 4], U);
+    load4<double>(&x4[(int64_t)j * 4], dU);
+    const double ir = 1.0 / U[0];
+    const double vn = (U[1] * nx + U[2] * ny) * ir;
+    const double dvn = ((dU[1] - U[1] * ir * dU[0]) * nx + (dU[2] - U[2] * ir * dU[0]) * ny) * ir;
+    const double dS = x5[j];
+    const double dF = dS * vn + u5[j] * dvn - dS * lam;
+    buf -= (0.5 * alpha) * area / h.vol[i] * dF;
+  }
+  Ax5[i] = D5[i] * x5[i] - buf;
+}
+
+// CompressInc of the U5 right-hand side as fsolve applies it: rhs = CompressInc(u, rhs dTau) / dTau
+__global__ void k_sa_compress_rhs(int64_t N, const double* u, const double* dt, double alpha, double* rhs) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const double dTau = dt[i] / alpha;
+  rhs[i] = sa_compress_inc(u[i], rhs[i] * dTau) / dTau;
+}
+// CompressInc of the U5 increment in place
+__global__ void k_sa_compress_inc(int64_t N, const double* u, double* inc) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < N) inc[i] = sa_compress_inc(u[i], inc[i]);
+}
+
 inline unsigned vgrid(int64_t n) { return (unsigned)((n + kBlock - 1) / kBlock); }
 
 struct DualOpts {
@@ -173,13 +217,14 @@ struct DualOpts {
 int ensure_dual(dndsg_ctx* c, const DualOpts& o) {
   int rc;
   if ((rc = ensure_lusgs(c))) return rc;
-  const size_t bytes = sizeof(double) * 4 * c->N;
+  const size_t bytes = sizeof(double) * (c->sa ? 5 : 4) * c->N;  // [N][4] flow, then [N] U5
   const size_t nOde = o.scheme == DNDSG_DUAL_SDIRK4 ? 3 : (size_t)(o.order - 1);
   while (c->odeVec.size() < nOde) {
     double* p = nullptr;
     if ((rc = dalloc(c, p, bytes))) return rc;
     c->odeVec.push_back(p);
   }
+  if (c->sa && !c->saDmat && (rc = dalloc(c, c->saDmat, sizeof(double) * c->N))) return rc;
   if (o.gmresCode != 0) {
     while (c->gmV.size() < (size_t)o.nSpace + 1) {
       double* p = nullptr;
@@ -188,6 +233,7 @@ int ensure_dual(dndsg_ctx* c, const DualOpts& o) {
     }
     if (!c->gmTmp)
       if ((rc = dalloc(c, c->gmTmp, bytes)) || (rc = dalloc(c, c->gmMLb, bytes)) ||
+          (rc = dalloc(c, c->gmB, bytes)) || (rc = dalloc(c, c->gmX, bytes)) ||
           (rc = dalloc(c, c->gmH, sizeof(double) * (kMaxKrylov + 1) * (kMaxKrylov + 1))) ||
           (rc = dalloc(c, c->gmPartial, sizeof(double) * (kMaxKrylov + 1) * kDotBlocks)))
         return rc;
@@ -196,8 +242,10 @@ int ensure_dual(dndsg_ctx* c, const DualOpts& o) {
 }
 
 // out[k] = dot(w, V_k) (or its square root), k < m, on the device
+inline int64_t dual_len(const dndsg_ctx* c) { return (c->sa ? 5 : 4) * c->N; }
+
 void launch_dots(dndsg_ctx* c, const double* w, const VecList& V, int m, double* out, bool root, cudaStream_t s) {
-  const int64_t n = 4 * c->N;
+  const int64_t n = dual_len(c);
   k_dots_partial<<<kDotBlocks, kBlock, 0, s>>>(n, w, V, m, c->gmPartial);
   k_dots_final<<<m, kBlock, 0, s>>>(c->gmPartial, kDotBlocks, out, root ? 1 : 0);
 }
@@ -205,8 +253,24 @@ void launch_dots(dndsg_ctx* c, const double* w, const VecList& V, int m, double*
 // the preconditioner FML: LU-SGS forward + backward with rhs x into MLx
 template <class T>
 void gmres_fml(dndsg_ctx* c, double alpha, const double* x, double* MLx, cudaStream_t s) {
+  if (c->sa) {
+    const int64_t n4 = 4 * c->N;
+    launch_lusgs_sweep_sa<T>(c, true, alpha, x, MLx, x + n4, MLx + n4, s);
+    launch_lusgs_sweep_sa<T>(c, false, alpha, x, MLx, x + n4, MLx + n4, s);
+    return;
+  }
   launch_lusgs_sweep<T>(c, true, alpha, x, MLx, s);
   launch_lusgs_sweep<T>(c, false, alpha, x, MLx, s);
+}
+// the matrix FA: LUSGSMatrixVec (the U5 row as well for SA contexts)
+template <class T>
+void gmres_fa(dndsg_ctx* c, double alpha, const double* x, double* Ax, cudaStream_t s) {
+  HotView<T> h = view<T>(c);
+  k_lusgs_matvec<T><<<grid_for(c->N), kBlock, 0, s>>>(h, alpha, c->Dmat, x, Ax);
+  if (c->sa) {
+    const int64_t n4 = 4 * c->N;
+    k_lusgs_matvec_sa5<T><<<grid_for(c->N), kBlock, 0, s>>>(h, c->saU, alpha, c->saDmat, x, x + n4, Ax + n4);
+  }
 }
 
 // least squares min |h y - beta e1| for the (k+1) x k upper Hessenberg h (column j at h + j (K+1)),
@@ -239,14 +303,13 @@ void hessenberg_lsq(const double* hcols, int K, int k, double beta, double* y) {
 // GMRES_LeftPreconditioned::solve with FStop always false (the EulerSolver's), x in place
 template <class T>
 int gmres_solve(dndsg_ctx* c, int K, int nRestart, double alpha, const double* b, double* x, cudaStream_t s) {
-  const int64_t n = 4 * c->N;
-  HotView<T> h = view<T>(c);
+  const int64_t n = dual_len(c);
   double* const H = c->gmH;
   gmres_fml<T>(c, alpha, b, c->gmMLb, s);
   std::vector<double> hHost((size_t)(K + 1) * K), y(K);
   for (int iRestart = 0; iRestart <= nRestart; iRestart++) {
     double* V0 = c->gmV[0];
-    k_lusgs_matvec<T><<<grid_for(c->N), kBlock, 0, s>>>(h, alpha, c->Dmat, x, c->gmTmp);
+    gmres_fa<T>(c, alpha, x, c->gmTmp, s);
     gmres_fml<T>(c, alpha, c->gmTmp, V0, s);
     VecList m1{};
     m1.p[0] = c->gmMLb;
@@ -262,7 +325,7 @@ int gmres_solve(dndsg_ctx* c, int K, int nRestart, double alpha, const double* b
     k_vec_scale<<<vgrid(n), kBlock, 0, s>>>(n, V0, -1.0 / beta, nullptr);
     for (int j = 0; j < K; j++) {
       double* w = c->gmV[j + 1];
-      k_lusgs_matvec<T><<<grid_for(c->N), kBlock, 0, s>>>(h, alpha, c->Dmat, c->gmV[j], c->gmTmp);
+      gmres_fa<T>(c, alpha, c->gmV[j], c->gmTmp, s);
       gmres_fml<T>(c, alpha, c->gmTmp, w, s);
       VecList V{};
       for (int i = 0; i <= j; i++) V.p[i] = c->gmV[i];
@@ -291,6 +354,12 @@ int gmres_solve(dndsg_ctx* c, int K, int nRestart, double alpha, const double* b
 // nInternalRecStep Jacobi sweeps, [limiter], EvaluateRHS at tEval into c->rhs
 template <class T>
 void dual_frhs(dndsg_ctx* c, const DualOpts& o, double tEval, cudaStream_t s) {
+  if (c->sa) {
+    run_dt_sa<T>(c, o.cfl, 1e100, s);
+    for (int k = 0; k < o.nRec; k++) run_vr_sa<T>(c, s);
+    run_rhs_sa<T>(c, s);
+    return;
+  }
   run_dt<T>(c, o.cfl, 1e100, false, s);
   for (int k = 0; k < o.nRec; k++) run_vr<T>(c, false, s);
   if (c->s.limiter) run_limiter<T>(c, 0, s);
@@ -301,14 +370,37 @@ void dual_frhs(dndsg_ctx* c, const DualOpts& o, double tEval, cudaStream_t s) {
 template <class T>
 int dual_fsolve(dndsg_ctx* c, const DualOpts& o, double dt, double alpha, cudaStream_t s) {
   HotView<T> h = view<T>(c);
-  k_lusgs_init<T><<<grid_for(c->N), kBlock, 0, s>>>(h, 1.0 / dt, alpha, c->Dinv, c->Dmat);
+  const int64_t N = c->N, n4 = 4 * N;
+  k_lusgs_init<T><<<grid_for(N), kBlock, 0, s>>>(h, 1.0 / dt, alpha, c->Dinv, c->Dmat);
+  if (c->sa) {
+    k_sa_diag<<<grid_for(N), kBlock, 0, s>>>(N, c->Dmat, c->saSrcJac, alpha, c->saDinv, c->saDmat);
+    k_sa_compress_rhs<<<grid_for(N), kBlock, 0, s>>>(N, c->saU, c->dt, alpha, c->saRhs);
+  }
   if (o.gmresCode == 0 || o.gmresCode == 2) {
-    launch_lusgs_sweep<T>(c, true, alpha, c->rhs, c->inc, s);
-    launch_lusgs_sweep<T>(c, false, alpha, c->rhs, c->inc, s);
+    if (c->sa) {
+      launch_lusgs_sweep_sa<T>(c, true, alpha, c->rhs, c->inc, c->saRhs, c->saInc, s);
+      launch_lusgs_sweep_sa<T>(c, false, alpha, c->rhs, c->inc, c->saRhs, c->saInc, s);
+      k_sa_compress_inc<<<grid_for(N), kBlock, 0, s>>>(N, c->saU, c->saInc);
+    } else {
+      launch_lusgs_sweep<T>(c, true, alpha, c->rhs, c->inc, s);
+      launch_lusgs_sweep<T>(c, false, alpha, c->rhs, c->inc, s);
+    }
   }
   if (o.gmresCode != 0) {
-    if (o.gmresCode == 1) DG_CUDA(c, cudaMemsetAsync(c->inc, 0, sizeof(double) * 4 * c->N, s));
-    return gmres_solve<T>(c, o.nSpace, o.nRestart, alpha, c->rhs, c->inc, s);
+    if (o.gmresCode == 1) {
+      DG_CUDA(c, cudaMemsetAsync(c->inc, 0, sizeof(double) * n4, s));
+      if (c->sa) DG_CUDA(c, cudaMemsetAsync(c->saInc, 0, sizeof(double) * N, s));
+    }
+    if (!c->sa) return gmres_solve<T>(c, o.nSpace, o.nRestart, alpha, c->rhs, c->inc, s);
+    // SA: the flow and U5 parts side by side in one vector for the Krylov solve
+    DG_CUDA(c, cudaMemcpyAsync(c->gmB, c->rhs, sizeof(double) * n4, cudaMemcpyDeviceToDevice, s));
+    DG_CUDA(c, cudaMemcpyAsync(c->gmB + n4, c->saRhs, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
+    DG_CUDA(c, cudaMemcpyAsync(c->gmX, c->inc, sizeof(double) * n4, cudaMemcpyDeviceToDevice, s));
+    DG_CUDA(c, cudaMemcpyAsync(c->gmX + n4, c->saInc, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
+    int rc;
+    if ((rc = gmres_solve<T>(c, o.nSpace, o.nRestart, alpha, c->gmB, c->gmX, s))) return rc;
+    DG_CUDA(c, cudaMemcpyAsync(c->inc, c->gmX, sizeof(double) * n4, cudaMemcpyDeviceToDevice, s));
+    DG_CUDA(c, cudaMemcpyAsync(c->saInc, c->gmX + n4, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
   }
   return 0;
 }
@@ -316,17 +408,20 @@ int dual_fsolve(dndsg_ctx* c, const DualOpts& o, double dt, double alpha, cudaSt
 // x += inc and fstop: the L1 increment norm (volume-weighted on request) against its running
 // maximum over the iterations; true when the density entry drops below the threshold
 struct Fstop {
-  double base[4] = {0, 0, 0, 0}, rel[4] = {0, 0, 0, 0};
+  double base[5] = {0, 0, 0, 0, 0}, rel[5] = {0, 0, 0, 0, 0};
 };
 template <class T>
 int dual_add_and_test(dndsg_ctx* c, const DualOpts& o, int iter, Fstop& f, bool& stop, cudaStream_t s) {
   DG_CUDA(c, cudaMemsetAsync(c->resAcc, 0, sizeof(double) * 16, s));
   k_add_inc<<<grid_for(c->N), kBlock, 0, s>>>(c->N, c->u, c->inc, c->vol, o.volWise, c->resAcc);
-  if (c->F > c->Fi) k_wall_flux<<<grid_for(c->F - c->Fi), kBlock, 0, s>>>(c->Fi, c->F, c->faceBC, c->flux, c->resAcc + 4);
-  double res[4];
-  DG_CUDA(c, cudaMemcpyAsync(res, c->resAcc, sizeof(res), cudaMemcpyDeviceToHost, s));
+  if (c->sa)  // CompressInc of the U5 increment (after the Krylov solve too), u5 += inc
+    k_sa_add_inc<<<grid_for(c->N), kBlock, 0, s>>>(c->N, c->saU, c->saInc, c->vol, o.volWise, c->resAcc + 8);
+  double acc[16];
+  DG_CUDA(c, cudaMemcpyAsync(acc, c->resAcc, sizeof(acc), cudaMemcpyDeviceToHost, s));
   DG_CUDA(c, cudaStreamSynchronize(s));
-  for (int v = 0; v < 4; v++) {
+  const int nv = c->sa ? 5 : 4;
+  double res[5] = {acc[0], acc[1], acc[2], acc[3], acc[8]};
+  for (int v = 0; v < nv; v++) {
     f.base[v] = iter == 1 ? res[v] : std::max(f.base[v], res[v]);
     f.rel[v] = res[v] / f.base[v];
   }
@@ -338,8 +433,20 @@ template <class T>
 int dual_step(dndsg_ctx* c, const DualOpts& o, double dt, double t, int* itersOut, double* resOut, cudaStream_t s) {
   int rc;
   if ((rc = ensure_dual(c, o))) return rc;
-  const int64_t n = 4 * c->N;
-  DG_CUDA(c, cudaMemcpyAsync(c->uLast, c->u, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  // a dual-time vector is [N][4] flow then, for SA contexts, [N] U5: the state, xLast and the rhs
+  // live in separate arrays, so each vector operation runs once per part
+  const int64_t N = c->N, n = 4 * N;
+  const bool sa = c->sa;
+  auto copy = [&](double* dst4, double* dst5, const double* src4, const double* src5) -> int {
+    DG_CUDA(c, cudaMemcpyAsync(dst4, src4, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    if (sa) DG_CUDA(c, cudaMemcpyAsync(dst5, src5, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
+    return 0;
+  };
+  auto part5 = [&](VecList L, int m) {  // the same list, pointing at the U5 parts of the vectors
+    for (int k = 0; k < m; k++) L.p[k] += n;
+    return L;
+  };
+  if ((rc = copy(c->uLast, c->saULast, c->u, c->saU))) return rc;
   Fstop f;
   if (o.scheme == DNDSG_DUAL_BDF) {
     const int prevSiz = o.order - 1, kCur = c->odeCnPrev + 1;
@@ -356,7 +463,13 @@ int dual_step(dndsg_ctx* c, const DualOpts& o, double dt, double t, int* itersOu
         X.p[1 + k] = c->odeVec[(size_t)((k + c->odePrevStart) % prevSiz)];
         X.a[1 + k] = coef[2 + k] / dt;
       }
-      k_dual_bdf_rhs<<<vgrid(n), kBlock, 0, s>>>(n, c->u, coef[0], -1. / dt, X, 1 + c->odeCnPrev, c->rhs);
+      const int m = 1 + c->odeCnPrev;
+      k_dual_bdf_rhs<<<vgrid(n), kBlock, 0, s>>>(n, c->u, coef[0], -1. / dt, X, m, c->rhs);
+      if (sa) {
+        VecList X5 = part5(X, m);
+        X5.p[0] = c->saULast;
+        k_dual_bdf_rhs<<<vgrid(N), kBlock, 0, s>>>(N, c->saU, coef[0], -1. / dt, X5, m, c->saRhs);
+      }
       if ((rc = dual_fsolve<T>(c, o, dt, coef[0], s))) return rc;
       bool stop = false;
       if ((rc = dual_add_and_test<T>(c, o, iter, f, stop, s))) return rc;
@@ -365,25 +478,28 @@ int dual_step(dndsg_ctx* c, const DualOpts& o, double dt, double t, int* itersOu
     if (itersOut) itersOut[0] = std::min(iter, o.maxIter);
     if (prevSiz) {
       c->odePrevStart = ((c->odePrevStart - 1) % prevSiz + prevSiz) % prevSiz;
-      DG_CUDA(c, cudaMemcpyAsync(c->odeVec[(size_t)c->odePrevStart], c->uLast, sizeof(double) * n,
-                                 cudaMemcpyDeviceToDevice, s));
+      double* h = c->odeVec[(size_t)c->odePrevStart];
+      if ((rc = copy(h, h + n, c->uLast, c->saULast))) return rc;
       c->odeDtPrev = dt;
       c->odeCnPrev = std::min(c->odeCnPrev + 1, prevSiz);
     }
   } else {
     const Sdirk4 tb = sdirk4_tableau();
     for (int iB = 0; iB < 3; iB++) {
-      DG_CUDA(c, cudaMemcpyAsync(c->u, c->uLast, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+      if ((rc = copy(c->u, c->saU, c->uLast, c->saULast))) return rc;
       int iter = 1;
       for (; iter <= o.maxIter; iter++) {
         dual_frhs<T>(c, o, t + tb.c[iB] * dt, s);
-        DG_CUDA(c, cudaMemcpyAsync(c->odeVec[iB], c->rhs, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+        if ((rc = copy(c->odeVec[iB], c->odeVec[iB] + n, c->rhs, c->saRhs))) return rc;
         VecList R{};
         for (int j = 0; j <= iB; j++) {
           R.p[j] = c->odeVec[j];
           R.a[j] = tb.A[iB][j];
         }
         k_dual_sdirk_rhs<<<vgrid(n), kBlock, 0, s>>>(n, c->uLast, c->u, 1.0 / dt, R, iB + 1, c->rhs);
+        if (sa)
+          k_dual_sdirk_rhs<<<vgrid(N), kBlock, 0, s>>>(N, c->saULast, c->saU, 1.0 / dt, part5(R, iB + 1), iB + 1,
+                                                       c->saRhs);
         if ((rc = dual_fsolve<T>(c, o, dt, tb.A[iB][iB], s))) return rc;
         bool stop = false;
         if ((rc = dual_add_and_test<T>(c, o, iter, f, stop, s))) return rc;
@@ -397,9 +513,10 @@ int dual_step(dndsg_ctx* c, const DualOpts& o, double dt, double t, int* itersOu
       R.a[j] = tb.b[j] * dt;
     }
     k_vec_combine<<<vgrid(n), kBlock, 0, s>>>(n, c->uLast, R, 3, c->u);
+    if (sa) k_vec_combine<<<vgrid(N), kBlock, 0, s>>>(N, c->saULast, part5(R, 3), 3, c->saU);
   }
   if (resOut)
-    for (int v = 0; v < 4; v++) resOut[v] = f.rel[v];
+    for (int v = 0; v < (sa ? 5 : 4); v++) resOut[v] = f.rel[v];
   return check_launch(c);
 }
 
@@ -415,7 +532,6 @@ int dual_opts(dndsg_ctx* c, const dndsg_dual_settings* d, DualOpts& o) {
     return fail(c, DNDSG_BAD_ARGUMENT, "cfl > 0, max_iter >= 1, n_rec >= 0, gmres_code 0..2");
   if (o.gmresCode != 0 && (o.nSpace < 1 || o.nSpace > kMaxKrylov || o.nRestart < 0))
     return fail(c, DNDSG_BAD_ARGUMENT, "n_gmres_space must be 1..32 and n_gmres_iter >= 0");
-  if (c->sa) return fail(c, DNDSG_UNSUPPORTED, "dual time stepping runs on 4-variable contexts");
   return 0;
 }
 

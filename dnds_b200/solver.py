@@ -213,7 +213,7 @@ class Solver:
                          vol_wise=int(vol_wise), gmres_code=int(gmres_code), n_gmres_space=int(n_gmres_space),
                          n_gmres_iter=int(n_gmres_iter))
         its = np.zeros(3, dtype=np.int32)
-        res = np.zeros(4)
+        res = np.zeros(self.nv)
         self._check(self.L.dndsg_dual_step(self.h, C.byref(d), float(dt), float(t), _p(its), _p(res), self.stream))
         return its, res
 

@@ -245,7 +245,8 @@ int dndsg_implicit_iteration(dndsg_ctx* ctx, double cfl, double dt_phys, double 
  * vol_wise) over its running maximum in the stage; an internal loop ends when
  * the density entry drops below threshold (rhsThresholdInternal) or after
  * max_iter (nTimeStepInternal) iterations.  The sweep order is the one of
- * dndsg_lusgs_set_order.  4-variable contexts.
+ * dndsg_lusgs_set_order.  4-variable and SA contexts (SA: the U5 rhs and
+ * increment pass through CompressInc as in fsolve).
  * ------------------------------------------------------------------------ */
 #define DNDSG_DUAL_SDIRK4 0 /* odeCode 0 */
 #define DNDSG_DUAL_BDF 1    /* odeCode 1 (the reference's driver uses bdf_order 2) */
@@ -266,7 +267,7 @@ typedef struct dndsg_dual_settings {
 int dndsg_dual_reset(dndsg_ctx* ctx);
 /* one physical step of size dt from time t, in place on the context's u;
  * iters_out [3] (host, may be NULL): internal iterations per stage (BDF: [0]);
- * res_out [4] (host, may be NULL): the last fstop ratios.  A BDF history built
+ * res_out [nvars] (host, may be NULL): the last fstop ratios.  A BDF history built
  * with another dt is an error (the reference asserts a constant dt). */
 int dndsg_dual_step(dndsg_ctx* ctx, const dndsg_dual_settings* settings, double dt, double t, int* iters_out,
                     double* res_out, void* stream);

@@ -188,7 +188,7 @@ class ImplicitDualTimeStepGPU {
     d_.n_gmres_space = nGmresSpace;
     d_.n_gmres_iter = nGmresIter;
     int its[3] = {0, 0, 0};
-    double res[4];
+    double res[5];
     c_.check(dndsg_dual_step(c_.get(), &d_, dt, tSimu, its, res, stream));
     return d_.scheme == DNDSG_DUAL_SDIRK4 ? its[2] : its[0];
   }

@@ -209,6 +209,45 @@ def test_dual_step_colour_batches_match_oracle_in_colour_order(oracle_lib):
     assert np.isfinite(ref).all() and _rel(u, ref) < 1e-10
 
 
+def _sa_case():
+    m = M.naca0012_cmesh(32, 16, 16, first=1e-3, far=10.0)  # no-slip wall
+    return m, S.naca0012_sa(0.15, 10.0, 1e5)
+
+
+def test_oracle_sa_bdf1_step_is_the_pseudo_time_iteration(oracle_lib):
+    m, cfg = _sa_case()
+    u0 = np.tile(np.array(cfg["eulerSetting"]["farFieldStaticValue"]), (m.n_cells, 1))
+    a = oracle_lib.Oracle(m, cfg, n_threads=4)
+    a.set_u(u0)
+    a.dual_step(0.01, scheme="bdf", bdf_order=1, cfl=20.0, max_iter=4)
+    b = oracle_lib.Oracle(m, cfg, n_threads=4)
+    b.set_u(u0)
+    for _ in range(4):
+        b.implicit_iteration(20.0, u0, dt=0.01)
+    assert _rel(a.get_u(), b.get_u()) < 1e-12
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("scheme,gmres_code", [("bdf", 0), ("bdf", 2), ("sdirk4", 1)])
+def test_sa_dual_step_matches_oracle(oracle_lib, scheme, gmres_code):
+    """RANS-SA (5 variables, no-slip wall) in dual time: the U5 rhs and increment pass through
+    CompressInc; BDF2 runs 2 steps so the history is used."""
+    m, cfg = _sa_case()
+    u0 = np.tile(np.array(cfg["eulerSetting"]["farFieldStaticValue"]), (m.n_cells, 1))
+    s, o = _pair(oracle_lib, m, cfg, u0)
+    kw = dict(scheme=scheme, bdf_order=2, cfl=20.0, max_iter=3, threshold=1e-100, gmres_code=gmres_code,
+              n_gmres_space=4, n_gmres_iter=1)
+    for k in range(2 if scheme == "bdf" else 1):
+        its, res = s.dual_step(1e-3, 1e-3 * k, **kw)
+        rits, rres = o.dual_step(1e-3, 1e-3 * k, **kw)
+        assert list(its) == list(rits) and len(res) == 5
+    u, ref = s.get_u(), o.get_u()
+    assert np.isfinite(ref).all() and ref[:, 4].min() > 0
+    assert _rel(u[:, :4], ref[:, :4]) < 1e-9 and _rel(u[:, 4], ref[:, 4]) < 1e-9
+    flags, _ = s.status()
+    assert flags == 0
+
+
 @pytest.mark.gpu
 def test_lusgs_matvec_matches_oracle(oracle_lib):
     import torch
