@@ -1981,9 +1981,10 @@ __device__ __forceinline__ void lusgs_mat_cell(const SaView<T>& sa, const LuMat<
 
 // a whole level-scheduled sweep in one block, one thread per position and a producer warp.  The
 // producer bulk-copies the next level's records (contiguous in schedule order) into the other half
-// of a shared-memory double buffer on an mbarrier while the other warps finish the current level; the block barrier per level publishes the increments (global memory and the
-// ring).  Positions of a level beyond kRecBlock read their records from global memory.  A bulk
-// copy that does not land in time sets kFlagTimeout and ends the walk.
+// of a shared-memory double buffer on an mbarrier while the other warps finish the current level;
+// the block barrier per level publishes the increments (global memory and the ring).  Positions of
+// a level beyond kRecBlock read their records from global memory.  A bulk copy that does not land
+// in time sets kFlagTimeout and ends the walk.
 template <bool SA>
 constexpr int mat_threads() { return kRecBlock + 32; }
 template <class T, bool FWD, bool SA>
