@@ -1606,17 +1606,19 @@ int dndsg_mlp_forward(dndsg_mlp* m, const float* X, int64_t n, float* Y, void* s
 namespace {
 int mlp_grad(dndsg_mlp* m, const float* X, const float* Tg, int64_t n, cudaStream_t s) {
   if (!m->attrTrain) {
-    DG_MCUDA(m, cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TrSmem)));
+    DG_MCUDA(m, cudaFuncSetAttribute(k_mlp_train_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sizeof(TrTcSmem)));
     m->attrTrain = true;
   }
   DG_MCUDA(m, cudaMemsetAsync(m->G, 0, sizeof(float) * kNParam, s));
   DG_MCUDA(m, cudaMemsetAsync(m->loss, 0, sizeof(double), s));
+  if (n == 0) return 0;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m->device);
-  const int64_t tiles = (n + 63) / 64;
-  const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(tiles, sms));
-  k_mlp_train<<<grid, kTrWarps * 32, sizeof(TrSmem), s>>>(mlp_dev(m), X, Tg, n, 1.0f / (float)(n * kOut), m->G,
-                                                          m->loss);
+  const int64_t tiles = (n + kTcRows - 1) / kTcRows;
+  const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(tiles, sms));  // one CTA per SM
+  k_mlp_train_tc<<<grid, kTcRows, sizeof(TrTcSmem), s>>>(mlp_dev(m), X, Tg, n, 1.0f / (float)(n * kOut), m->G,
+                                                         m->loss, m->flags);
   DG_MCUDA(m, cudaGetLastError());
   return 0;
 }
@@ -1632,7 +1634,10 @@ int dndsg_mlp_gradient(dndsg_mlp* m, const float* X, const float* Tg, int64_t n,
   double l = 0;
   DG_MCUDA(m, cudaMemcpyAsync(&l, m->loss, sizeof(double), cudaMemcpyDeviceToHost, st(s)));
   if (grad) DG_MCUDA(m, cudaMemcpyAsync(grad, m->G, sizeof(float) * kNParam, cudaMemcpyDeviceToHost, st(s)));
+  unsigned f = 0;
+  DG_MCUDA(m, cudaMemcpyAsync(&f, m->flags, sizeof(f), cudaMemcpyDeviceToHost, st(s)));
   DG_MCUDA(m, cudaStreamSynchronize(st(s)));
+  if (f) return mfail(m, DNDSG_CUDA_ERROR, "tensor-core completion wait timed out");
   if (loss) *loss = l / (double)(n * kOut);
   return 0;
 }

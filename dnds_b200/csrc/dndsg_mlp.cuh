@@ -1,9 +1,9 @@
 // dndsg_mlp.cuh -- learned warm start for the VR coefficients (no counterpart in
 // the reference): a per-cell MLP 64 -> 64 -> 64 -> 64 -> 20 (SiLU), BF16 weights
-// and activations, FP32 accumulation.  Inference runs on the 5th-generation tensor
-// cores (tcgen05.mma with the accumulator in tensor memory, k_mlp_tc); training
-// (forward, backward, Adam) uses warp-level 16x16x16 BF16 MMA (wmma), whose
-// backward products (dz W and dz^T x over 64-row tiles) are small and transposed.
+// and activations, FP32 accumulation, on the 5th-generation tensor cores
+// (tcgen05.mma with the accumulators in tensor memory): inference (k_mlp_tc) and
+// training (k_mlp_train_tc: forward, backward with the weight and input
+// gradients, then Adam on the FP32 master parameters).
 //
 // The network extrapolates the Jacobi sequence: from the starting coefficients
 // x0 and two plain sweeps x1 = J(x0), x2 = J(x1) it proposes the converged
@@ -23,7 +23,6 @@
 // Scales are floored so that a converged or uniform region gives finite features.
 #pragma once
 #include <cuda_bf16.h>
-#include <mma.h>
 
 #include "dndsg_bodies.cuh"
 
@@ -100,67 +99,11 @@ DG_HD void mlp_cell_features(int64_t i, const HotView<T>& h, const MlpIters<T>& 
 
 #if defined(__CUDACC__)
 namespace dg {
-namespace wm = nvcuda::wmma;
 typedef __nv_bfloat16 bf16;
 
 __device__ __forceinline__ double warp_sum_d(double v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
-}
-
-// out[16][N] (FP32, ld 64) = in[16][K] (BF16, ld ldin) . W^T, W [N][K] BF16 row-major (ld K)
-template <int K, int N>
-__device__ __forceinline__ void warp_gemm_xwT(const bf16* in, int ldin, const bf16* W, float* out) {
-  for (int nt = 0; nt < N / 16; nt++) {
-    wm::fragment<wm::accumulator, 16, 16, 16, float> acc;
-    wm::fill_fragment(acc, 0.0f);
-    for (int kt = 0; kt < K / 16; kt++) {
-      wm::fragment<wm::matrix_a, 16, 16, 16, bf16, wm::row_major> a;
-      wm::fragment<wm::matrix_b, 16, 16, 16, bf16, wm::col_major> b;
-      wm::load_matrix_sync(a, in + kt * 16, ldin);
-      wm::load_matrix_sync(b, W + nt * 16 * K + kt * 16, K);
-      wm::mma_sync(acc, a, b, acc);
-    }
-    wm::store_matrix_sync(out + nt * 16, acc, 64, wm::mem_row_major);
-  }
-}
-
-// out[16][K] (FP32, ld 64) = dz[16][N] (BF16, ld 64) . W, W [N][K] BF16 row-major (ld K)
-template <int N, int K>
-__device__ __forceinline__ void warp_gemm_dzW(const bf16* dz, const bf16* W, float* out) {
-  for (int kt = 0; kt < K / 16; kt++) {
-    wm::fragment<wm::accumulator, 16, 16, 16, float> acc;
-    wm::fill_fragment(acc, 0.0f);
-    for (int nt = 0; nt < N / 16; nt++) {
-      wm::fragment<wm::matrix_a, 16, 16, 16, bf16, wm::row_major> a;
-      wm::fragment<wm::matrix_b, 16, 16, 16, bf16, wm::row_major> b;
-      wm::load_matrix_sync(a, dz + nt * 16, 64);
-      wm::load_matrix_sync(b, W + nt * 16 * K + kt * 16, K);
-      wm::mma_sync(acc, a, b, acc);
-    }
-    wm::store_matrix_sync(out + kt * 16, acc, 64, wm::mem_row_major);
-  }
-}
-
-// one 16x16 tile (n-tile nt, k-tile kt) of dW[N][K] += dz^T . x over 64 rows;
-// dz [64][*] BF16 ld 64, x [64][*] BF16 ld ldx; result added into g (FP32, ld K)
-template <int K>
-__device__ __forceinline__ void cta_tile_dW(const bf16* dz, const bf16* x, int ldx, int nt, int kt, float* scratch,
-                                            float* g) {
-  wm::fragment<wm::accumulator, 16, 16, 16, float> acc;
-  wm::fill_fragment(acc, 0.0f);
-  for (int rt = 0; rt < 4; rt++) {
-    wm::fragment<wm::matrix_a, 16, 16, 16, bf16, wm::col_major> a;
-    wm::fragment<wm::matrix_b, 16, 16, 16, bf16, wm::row_major> b;
-    wm::load_matrix_sync(a, dz + rt * 16 * 64 + nt * 16, 64);
-    wm::load_matrix_sync(b, x + rt * 16 * ldx + kt * 16, ldx);
-    wm::mma_sync(acc, a, b, acc);
-  }
-  wm::store_matrix_sync(scratch, acc, 16, wm::mem_row_major);
-  __syncwarp();
-  const int lane = threadIdx.x & 31;
-  for (int e = lane; e < 256; e += 32) g[(nt * 16 + e / 16) * K + kt * 16 + (e & 15)] += scratch[e];
-  __syncwarp();
 }
 
 struct MlpDev {
@@ -190,6 +133,12 @@ struct TcSmem {
 // tensor memory: every resident CTA holds kTcCols of the SM's 512 columns, and an allocation that
 // cannot be met waits; the launch keeps at most 4 CTAs per SM (shared memory and registers allow 4)
 static_assert(sizeof(TcSmem) > 233472 / 9, "at most 8 CTAs of k_mlp_tc per SM");
+
+// the bias of layer l, entry k, from the FP32 master parameters
+__device__ __forceinline__ float tc_bias_s(const float* P, int layer, int k) {
+  const int off = layer == 0 ? kOffB1 : layer == 1 ? kOffB2 : layer == 2 ? kOffB3 : kOffB4;
+  return P[off + k];
+}
 
 // byte offset of element (row, k) of a 64-wide K-major operand in the core-matrix layout
 __device__ __forceinline__ uint32_t cm_off(int row, int k) {
@@ -412,148 +361,230 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_tc(MlpDev m, Src src, Dst dst, 
   }
 }
 
-// ---------------------------------------------------------------- training: forward + backward
 // loss = mean over rows and the 20 outputs of (y - t)^2; gradients accumulate into G
-constexpr int kTrWarps = 4;
-struct TrSmem {
-  bf16 W[kNW];
-  float b[3 * kHid + kOutP];
-  bf16 x[64 * kInP];
-  bf16 h1[64 * 64], h2[64 * 64], h3[64 * 64];
-  float z1[64 * 64], z2[64 * 64], z3[64 * 64];
-  float dy[64 * 64];  // y, then dy (first 32 columns), then dH scratch
-  bf16 dz[64 * 64];
-  float g[kNParam];
-  float scratch[kTrWarps][256];
+// ---------------------------------------------------------------- training on the tensor cores (tcgen05)
+// 128 rows per tile, one per thread; one CTA per SM holding all 512 tensor-memory columns:
+//   cols   0-191  the pre-activations z1, z2, z3 of the tile (FP32, kept for the backward pass)
+//   cols 192-255  the layer-4 output, then each backward product dH = dz W
+//   cols 256-511  dW1 .. dW4, accumulated over all of the CTA's tiles (rows = output units)
+// Every product is M = 128, K-major, BF16 x BF16 -> FP32.  The weight-gradient product
+// dW = dz^T h runs over the 128 rows of the tile as its K dimension: dz^T and h^T are written
+// transposed into shared memory (128-wide K, stride byte offset 2048), dz^T padded to 128 rows with
+// zeros (the unused accumulator rows stay zero).  dH = dz W uses the transposed weights W^T.
+constexpr int kTrCols = 512;
+struct TrTcSmem {
+  alignas(128) unsigned char Wf[3 * kHid * 128 + kOutP * 128];  // W_l [N][64], core-matrix layout
+  alignas(128) unsigned char Wt[4][64 * 128];                    // W_l^T [64][64] (W4^T: columns >= 32 zero)
+  alignas(128) unsigned char A[kTcRows * 128];                   // x, h1, h2, h3, then dz, [128][64]
+  alignas(128) unsigned char XT[64 * 256];                       // x^T [64][128]
+  alignas(128) unsigned char HT[3][64 * 256];                    // h_l^T [64][128]
+  alignas(128) unsigned char DZT[kTcRows * 256];                 // dz^T [128][128], rows >= N zero
+  float gb[3 * kHid + kOutP];                                    // bias gradients of the CTA
+  uint64_t bar;
+  uint32_t tmem;
 };
+static_assert(sizeof(TrTcSmem) > 233472 / 2, "one CTA per SM: it holds all 512 tensor-memory columns");
 
-__global__ void __launch_bounds__(kTrWarps * 32) k_mlp_train(MlpDev m, const float* X, const float* Tg, int64_t n,
-                                                             float invCount, float* G, double* lossAcc) {
+// byte offset of element (row, k) of a 128-wide K-major operand
+__device__ __forceinline__ uint32_t cm_off128(int row, int k) {
+  return (uint32_t)((row >> 3) * 2048 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
+}
+__device__ __forceinline__ uint64_t umma_desc_sbo(uint32_t saddr, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(sbo >> 4) << 32) |
+         (1ull << 46);
+}
+// one thread issues D (+)= A B for K = 16 ksteps (A and B K-major with the given stride byte offsets)
+__device__ __forceinline__ void umma_chain(uint32_t d, uint32_t a, uint32_t sboA, uint32_t b, uint32_t sboB,
+                                           uint32_t idesc, int ksteps, bool accumulate) {
+  for (int ks = 0; ks < ksteps; ks++)
+    umma_bf16(d, umma_desc_sbo(a + 256 * ks, sboA), umma_desc_sbo(b + 256 * ks, sboB), idesc, accumulate || ks > 0);
+}
+__device__ __forceinline__ void st_bf16(unsigned char* base, uint32_t off, float v) {
+  *reinterpret_cast<__nv_bfloat16*>(base + off) = __float2bfloat16(v);
+}
+// sum over the 128 rows (threads) of column values v[16], added into gb[c0 .. c0 + 15]
+__device__ __forceinline__ void tr_bias_sum(const float* v, float* gb, int c0) {
+  for (int k = 0; k < 16; k++) {
+    float a = v[k];
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&gb[c0 + k], a);
+  }
+}
+
+__global__ void __launch_bounds__(kTcRows) k_mlp_train_tc(MlpDev m, const float* X, const float* Tg, int64_t n,
+                                                          float invCount, float* G, double* lossAcc, unsigned* flags) {
   extern __shared__ __align__(128) unsigned char raw[];
-  TrSmem& S = *reinterpret_cast<TrSmem*>(raw);
-  const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
-  for (int e = tid; e < kNW; e += blockDim.x) S.W[e] = m.W[e];
-  for (int e = tid; e < 3 * kHid + kOutP; e += blockDim.x) {
-    int off = e < kHid ? kOffB1 + e : e < 2 * kHid ? kOffB2 + e - kHid : e < 3 * kHid ? kOffB3 + e - 2 * kHid
-                                                                                    : kOffB4 + e - 3 * kHid;
-    S.b[e] = m.P[off];
+  TrTcSmem& S = *reinterpret_cast<TrTcSmem*>(raw);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  // weights: W_l in the forward layout and W_l^T for dH = dz W
+  for (int e = tid; e < (3 * kHid + kOutP) * 64; e += blockDim.x) {
+    const int row = e >> 6, k = e & 63;
+    const int layer = row < 3 * kHid ? row / kHid : 3, rl = row - layer * kHid;
+    const int woff = layer == 0 ? kWOff1 : layer == 1 ? kWOff2 : layer == 2 ? kWOff3 : kWOff4;
+    const bf16 w = m.W[woff + rl * 64 + k];
+    *reinterpret_cast<bf16*>(S.Wf + layer * kHid * 128 + cm_off(rl, k)) = w;
+    *reinterpret_cast<bf16*>(S.Wt[layer] + cm_off(k, rl)) = w;
   }
-  for (int e = tid; e < kNParam; e += blockDim.x) S.g[e] = 0.f;
+  for (int e = tid; e < 64 * kOutP; e += blockDim.x)  // W4^T columns 32..63
+    *reinterpret_cast<bf16*>(S.Wt[3] + cm_off(e >> 5, kOutP + (e & 31))) = __float2bfloat16(0.f);
+  for (int e = tid; e < kTcRows * 128; e += blockDim.x) S.DZT[e * 2] = 0, S.DZT[e * 2 + 1] = 0;
+  for (int e = tid; e < 3 * kHid + kOutP; e += blockDim.x) S.gb[e] = 0.f;
+  const uint32_t bar = smem_u32(&S.bar);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem)),
+                 "r"(kTrCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    fence_mbar_init();
+  }
+  tc_fence_before();
   __syncthreads();
+  tc_fence_after();
+  const uint32_t tb = S.tmem, lane0 = (uint32_t)(warp * 32) << 16;
+  const uint32_t aA = smem_u32(S.A), aXT = smem_u32(S.XT), aDZT = smem_u32(S.DZT);
+  const uint32_t idesc64 = umma_idesc(kHid), idesc32 = umma_idesc(kOutP);
+  uint32_t phase = 0;
+  bool failed = false, first = true;
   double lossLocal = 0.0;
-  const int64_t tiles = (n + 63) / 64;
-  for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-    const int64_t r0 = tile * 64;
-    for (int e = tid; e < 64 * kInP; e += blockDim.x) {
-      const int r = e / kInP, k = e - r * kInP;
-      const float v = (r0 + r < n && k < kIn) ? X[(r0 + r) * kIn + k] : 0.f;
-      S.x[e] = __float2bfloat16(v);
-    }
+  // all threads: make the operand writes visible to the tensor cores, then tid 0 issues `issue`
+  auto run = [&](auto issue) -> bool {
+    proxy_fence_smem();
+    tc_fence_before();
     __syncthreads();
-    // ---- forward, warp w on rows 16w..16w+15
-    const int rw = 16 * w;
-    warp_gemm_xwT<kInP, kHid>(S.x + rw * kInP, kInP, S.W + kWOff1, S.z1 + rw * 64);
-    __syncwarp();
-    for (int e = lane; e < 16 * 64; e += 32) {
-      float zz = S.z1[rw * 64 + e] + S.b[e & 63];
-      S.z1[rw * 64 + e] = zz;
-      S.h1[rw * 64 + e] = __float2bfloat16(silu(zz));
+    if (tid == 0) {
+      tc_fence_after();
+      issue();
+      umma_commit(bar);
     }
-    __syncwarp();
-    warp_gemm_xwT<kHid, kHid>(S.h1 + rw * 64, 64, S.W + kWOff2, S.z2 + rw * 64);
-    __syncwarp();
-    for (int e = lane; e < 16 * 64; e += 32) {
-      float zz = S.z2[rw * 64 + e] + S.b[kHid + (e & 63)];
-      S.z2[rw * 64 + e] = zz;
-      S.h2[rw * 64 + e] = __float2bfloat16(silu(zz));
-    }
-    __syncwarp();
-    warp_gemm_xwT<kHid, kHid>(S.h2 + rw * 64, 64, S.W + kWOff3, S.z3 + rw * 64);
-    __syncwarp();
-    for (int e = lane; e < 16 * 64; e += 32) {
-      float zz = S.z3[rw * 64 + e] + S.b[2 * kHid + (e & 63)];
-      S.z3[rw * 64 + e] = zz;
-      S.h3[rw * 64 + e] = __float2bfloat16(silu(zz));
-    }
-    __syncwarp();
-    warp_gemm_xwT<kHid, kOutP>(S.h3 + rw * 64, 64, S.W + kWOff4, S.dy + rw * 64);
-    __syncwarp();
-    // loss and dy = 2 (y - t) / count on the 20 real outputs
-    for (int e = lane; e < 16 * 64; e += 32) {
-      const int r = e >> 6, o = e & 63;
-      const int64_t row = r0 + rw + r;
-      float d = 0.f;
-      if (o < kOut && row < n) {
-        const float y = S.dy[rw * 64 + e] + S.b[3 * kHid + o];
-        const float dd = y - Tg[row * kOut + o];
-        lossLocal += (double)dd * dd;
-        d = 2.f * dd * invCount;
+    const bool ok = mbar_wait(bar, phase, kWaitLimit);
+    phase ^= 1u;
+    if (__syncthreads_or(!ok)) return false;
+    tc_fence_after();
+    return true;
+  };
+  for (int64_t tile = blockIdx.x; tile * kTcRows < n && !failed; tile += gridDim.x) {
+    const int64_t r0 = tile * kTcRows, r = r0 + tid;
+    // x: coalesced 32-B pieces into A (K-major) and x^T
+    for (int e = tid; e < kTcRows * 8; e += blockDim.x) {
+      const int row = e >> 3, kc = e & 7;
+      float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      if (r0 + row < n) {
+        const float4* q = reinterpret_cast<const float4*>(X + (r0 + row) * kIn + 8 * kc);
+        const float4 a = q[0], b = q[1];
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
       }
-      S.dy[rw * 64 + e] = d;
-      S.dz[rw * 64 + e] = __float2bfloat16(d);
+      __nv_bfloat162 p[4];
+      for (int j = 0; j < 4; j++) p[j] = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+      *reinterpret_cast<uint4*>(S.A + cm_off(row, 8 * kc)) = *reinterpret_cast<uint4*>(p);
+      for (int j = 0; j < 8; j++) st_bf16(S.XT, cm_off128(8 * kc + j, row), v[j]);
     }
-    __syncthreads();
-    // ---- layer 4: dW4 [32][64] (8 tiles), db4, dH3 = dz4 . W4
-    for (int t = w; t < 8; t += kTrWarps) cta_tile_dW<kHid>(S.dz, S.h3, 64, t >> 2, t & 3, S.scratch[w], S.g + kOffW4);
-    if (tid < kOutP) {
-      float a = 0.f;
-      for (int r = 0; r < 64; r++) a += S.dy[r * 64 + tid];
-      S.g[kOffB4 + tid] += a;
+    // ---- forward: z_l into tensor memory, h_l = SiLU(z_l + b_l) into A and h_l^T
+    for (int l = 0; l < 4 && !failed; l++) {
+      const uint32_t dcol = l < 3 ? 64u * l : 192u;
+      if (!run([&] {
+            umma_chain(tb + dcol, aA, 1024, smem_u32(S.Wf + l * kHid * 128), 1024, l < 3 ? idesc64 : idesc32, 4, false);
+          })) {
+        failed = true;
+        break;
+      }
+      if (l < 3) {
+        for (int c0 = 0; c0 < 64; c0 += 16) {
+          float z[16];
+          tmem_ld16(tb + lane0 + dcol + c0, z);
+          tmem_wait_ld();
+          for (int k = 0; k < 16; k++) {
+            const float h = silu(z[k] + tc_bias_s(m.P, l, c0 + k));
+            st_bf16(S.A, cm_off(tid, c0 + k), h);
+            st_bf16(S.HT[l], cm_off128(c0 + k, tid), h);
+          }
+        }
+      } else {  // y = z4 + b4, dz4 = 2 (y - t) / count on the 20 outputs
+        float z[32], dz[32];
+        tmem_ld16(tb + lane0 + 192, z);
+        tmem_ld16(tb + lane0 + 208, z + 16);
+        tmem_wait_ld();
+        for (int o = 0; o < 32; o++) {
+          float d = 0.f;
+          if (o < kOut && r < n) {
+            const float y = z[o] + tc_bias_s(m.P, 3, o);
+            const float dd = y - Tg[r * kOut + o];
+            lossLocal += (double)dd * dd;
+            d = 2.f * dd * invCount;
+          }
+          dz[o] = d;
+        }
+        for (int o = 0; o < 64; o++) st_bf16(S.A, cm_off(tid, o), o < 32 ? dz[o] : 0.f);
+        for (int o = 0; o < 32; o++) st_bf16(S.DZT, cm_off128(o, tid), dz[o]);
+        tr_bias_sum(dz, S.gb + 3 * kHid, 0);
+        tr_bias_sum(dz + 16, S.gb + 3 * kHid, 16);
+      }
     }
-    __syncthreads();  // dy is read whole above and overwritten row-wise below
-    warp_gemm_dzW<kOutP, kHid>(S.dz + rw * 64, S.W + kWOff4, S.dy + rw * 64);
-    __syncthreads();
-    for (int e = lane; e < 16 * 64; e += 32) {
-      const float dz = S.dy[rw * 64 + e] * silu_grad(S.z3[rw * 64 + e]);
-      S.z3[rw * 64 + e] = dz;  // FP32 dz3 for the bias gradient
-      S.dz[rw * 64 + e] = __float2bfloat16(dz);
+    // ---- backward: dW_l += dz_l^T h_{l-1}; dH = dz_l W_l; dz_{l-1} = dH SiLU'(z_{l-1} + b_{l-1})
+    for (int l = 3; l >= 0 && !failed; l--) {
+      const uint32_t hT = l > 0 ? smem_u32(S.HT[l - 1]) : aXT;
+      const bool acc = !first;
+      if (!run([&] {
+            umma_chain(tb + 256 + 64u * l, aDZT, 2048, hT, 2048, idesc64, 8, acc);
+            if (l > 0) umma_chain(tb + 192, aA, 1024, smem_u32(S.Wt[l]), 1024, idesc64, 4, false);
+          })) {
+        failed = true;
+        break;
+      }
+      if (l > 0) {
+        for (int c0 = 0; c0 < 64; c0 += 16) {
+          float dh[16], z[16], dz[16];
+          tmem_ld16(tb + lane0 + 192 + c0, dh);
+          tmem_ld16(tb + lane0 + 64u * (l - 1) + c0, z);
+          tmem_wait_ld();
+          for (int k = 0; k < 16; k++) {
+            dz[k] = r < n ? dh[k] * silu_grad(z[k] + tc_bias_s(m.P, l - 1, c0 + k)) : 0.f;
+            st_bf16(S.A, cm_off(tid, c0 + k), dz[k]);
+            st_bf16(S.DZT, cm_off128(c0 + k, tid), dz[k]);
+          }
+          tr_bias_sum(dz, S.gb + (l - 1) * kHid, c0);
+        }
+      }
     }
-    __syncthreads();
-    // ---- layer 3
-    for (int t = w; t < 16; t += kTrWarps) cta_tile_dW<kHid>(S.dz, S.h2, 64, t >> 2, t & 3, S.scratch[w], S.g + kOffW3);
-    for (int c = tid; c < kHid; c += blockDim.x) {
-      float a = 0.f;
-      for (int r = 0; r < 64; r++) a += S.z3[r * 64 + c];
-      S.g[kOffB3 + c] += a;
-    }
-    warp_gemm_dzW<kHid, kHid>(S.dz + rw * 64, S.W + kWOff3, S.dy + rw * 64);
-    __syncthreads();
-    for (int e = lane; e < 16 * 64; e += 32) {
-      const float dz = S.dy[rw * 64 + e] * silu_grad(S.z2[rw * 64 + e]);
-      S.z2[rw * 64 + e] = dz;
-      S.dz[rw * 64 + e] = __float2bfloat16(dz);
-    }
-    __syncthreads();
-    // ---- layer 2
-    for (int t = w; t < 16; t += kTrWarps) cta_tile_dW<kHid>(S.dz, S.h1, 64, t >> 2, t & 3, S.scratch[w], S.g + kOffW2);
-    for (int c = tid; c < kHid; c += blockDim.x) {
-      float a = 0.f;
-      for (int r = 0; r < 64; r++) a += S.z2[r * 64 + c];
-      S.g[kOffB2 + c] += a;
-    }
-    warp_gemm_dzW<kHid, kHid>(S.dz + rw * 64, S.W + kWOff2, S.dy + rw * 64);
-    __syncthreads();
-    for (int e = lane; e < 16 * 64; e += 32) {
-      const float dz = S.dy[rw * 64 + e] * silu_grad(S.z1[rw * 64 + e]);
-      S.z1[rw * 64 + e] = dz;
-      S.dz[rw * 64 + e] = __float2bfloat16(dz);
-    }
-    __syncthreads();
-    // ---- layer 1: dW1 [64][kInP], db1
-    constexpr int kT1 = kInP / 16;
-    for (int t = w; t < 4 * kT1; t += kTrWarps)
-      cta_tile_dW<kInP>(S.dz, S.x, kInP, t / kT1, t % kT1, S.scratch[w], S.g + kOffW1);
-    for (int c = tid; c < kHid; c += blockDim.x) {
-      float a = 0.f;
-      for (int r = 0; r < 64; r++) a += S.z1[r * 64 + c];
-      S.g[kOffB1 + c] += a;
-    }
-    __syncthreads();
+    first = false;
   }
-  for (int e = tid; e < kNParam; e += blockDim.x)
-    if (S.g[e] != 0.f) atomicAdd(&G[e], S.g[e]);
+  if (failed && tid == 0) {
+    atomicOr(flags, kFlagTimeout);
+    mbar_wait(bar, phase ^ 1u, kWaitLimit);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  // the CTA's weight gradients (rows < N of each accumulator) and bias gradients into G
+  if (!failed && !first) {
+    for (int l = 0; l < 4; l++) {
+      const int N = l < 3 ? kHid : kOutP;
+      const int woff = l == 0 ? kOffW1 : l == 1 ? kOffW2 : l == 2 ? kOffW3 : kOffW4;
+      for (int c0 = 0; c0 < 64; c0 += 16) {
+        float g[16];
+        tmem_ld16(tb + lane0 + 256 + 64u * l + c0, g);
+        tmem_wait_ld();
+        if (tid < N)
+          for (int k = 0; k < 16; k++)
+            if (g[k] != 0.f) atomicAdd(&G[woff + tid * 64 + c0 + k], g[k]);
+      }
+    }
+    for (int e = tid; e < 3 * kHid + kOutP; e += blockDim.x) {
+      const int off = e < kHid ? kOffB1 + e : e < 2 * kHid ? kOffB2 + e - kHid : e < 3 * kHid ? kOffB3 + e - 2 * kHid
+                                                                                            : kOffB4 + e - 3 * kHid;
+      if (S.gb[e] != 0.f) atomicAdd(&G[off], S.gb[e]);
+    }
+  }
   lossLocal = warp_sum_d(lossLocal);
-  if (lane == 0 && lossLocal != 0.0) atomicAdd(lossAcc, lossLocal);
+  if ((tid & 31) == 0 && lossLocal != 0.0) atomicAdd(lossAcc, lossLocal);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tb), "r"(kTrCols) : "memory");
+  }
 }
 
 // Adam (Kingma & Ba) on the FP32 master parameters; padded entries stay zero; refreshes the BF16 copy

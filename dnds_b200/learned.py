@@ -225,6 +225,25 @@ def time_forward(rows_list=(1 << 20, 1 << 22), reps: int = 5, seed: int = 7):
     return out
 
 
+def time_train_step(rows: int = 1 << 20, reps: int = 10, seed: int = 7):
+    """CUDA-event time of one training step (forward, backward, Adam) on random features and
+    targets; returns ms per step."""
+    import torch
+
+    net = WarmStartNet(0, seed=seed)
+    dev = torch.device("cuda:0")
+    X = torch.randn((rows, N_IN), device=dev)
+    T = 0.1 * torch.randn((rows, N_OUT), device=dev)
+    net.train_step(X, T, 1e-4)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        net.train_step(X, T, 1e-4)
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
 def main(argv=None):
     import argparse
     import time
@@ -235,6 +254,13 @@ def main(argv=None):
         import sys
 
         argv = sys.argv[1:]
+    if "--time-train" in argv:
+        rows = 1 << 20
+        ms = time_train_step(rows)
+        flop = 3 * 2 * (N_IN * 64 + 64 * 64 * 2 + 64 * N_OUT) * rows
+        print(f"{rows} rows: {ms:.4f} ms per training step, {rows / ms / 1e6:.3f}e9 samples/s, "
+              f"{flop / ms / 1e9:.1f} TFLOP/s (forward + backward, 3x the forward)")
+        return
     if "--time-forward" in argv:
         for rows, ms in time_forward():
             flop = 2 * (N_IN * 64 + 64 * 64 * 2 + 64 * N_OUT) * rows
