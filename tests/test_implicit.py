@@ -240,6 +240,36 @@ def test_level_scheduled_natural_order_matches_sequential_oracle(oracle_lib):
 
 
 @pytest.mark.gpu
+def test_scan_order_beyond_the_shared_level_table_matches_oracle(oracle_lib):
+    """A 2200 x 2 channel in the natural order has 2201 levels per sweep; a scan order that walks the
+    channel back and forth (rows alternately forward and reversed) makes more than 4095 levels
+    (the level table one block keeps in shared memory), so the sweep runs on the general
+    level-by-level path.  Both agree with the oracle's sequential sweep."""
+    from dnds_b200.solver import DndsgError
+
+    m = M.structured_grid(2200, 2, 440.0, 0.4, periodic=False)
+    cfg = S.preset("naca0012", eulerSetting={"riemannSolverType": "Roe", "idealGasProperty": {"gamma": 1.4},
+                                             "farFieldStaticValue": S.free_stream(0.5, 2.0)})
+    rng = np.random.default_rng(2)
+    u0 = _free_stream(m, cfg) * (1 + 0.02 * rng.uniform(size=(m.n_cells, 1)))
+    s = _gpu(m, cfg)
+    with pytest.raises(DndsgError):
+        s.lusgs_set_order(1, np.zeros(m.n_cells, dtype=np.int64))  # not a permutation
+    assert s.lusgs_set_order(1) == 2 * 2201  # natural order: levels i + j
+    order = np.concatenate([np.arange(2200), np.arange(4399, 2199, -1)])  # row 1 walked backwards
+    assert s.lusgs_set_order(1, order) == 2 * 4400
+    s.set_u(u0)
+    s.bdf_begin()
+    o = _oracle(oracle_lib, m, cfg)
+    o.set_u(u0)
+    for _ in range(3):
+        s.implicit_iteration(20.0)
+        o.implicit_iteration(20.0, u0, scan2cell=order)
+    ref = o.get_u()
+    assert np.abs(s.get_u() - ref).max() < 1e-10 * np.abs(ref).max()
+
+
+@pytest.mark.gpu
 def test_line_scan_order_matches_oracle(oracle_lib):
     """A caller-given scan order (wall-normal lines, even then odd) runs as nj + 1 levels per
     sweep (the odd lines follow the even ones one level behind) and computes what the oracle's
