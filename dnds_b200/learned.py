@@ -18,7 +18,7 @@ this module only drives them:
                      the network, for the sweeps-saved comparison
 
 The plain Jacobi sweep (ReconstructionJacobiStep, DNDS_FV_VR.hpp:1474-1713)
-stays the judge: it iterates to the same tolerance either way, and per cell
+decides: it iterates to the same tolerance either way, and per cell
 the learned start is kept only where the Jacobi increment from it is smaller
 than from the plain start.  Device arrays are torch CUDA tensors (plumbing
 only); no computation of the path runs in torch.
