@@ -11,7 +11,7 @@ path is timed beside it.  Synthetic data generated here; no dataset.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl dnds_b200|reference]
 
 With N > 1 (torchrun, one rank per GPU) every rank runs an independent
-replica (the reference partitions the mesh with MPI halos; this build runs
+replica (the reference partitions the mesh with MPI halos; this implementation runs
 one mesh per GPU), and `value` is the sum over ranks (weak scaling).
 `--impl reference` times the FP64 CPU restatement of the reference (oracle/)
 on the host cores.

@@ -167,7 +167,7 @@ class ImplicitSteadyGPU {
 
 // the reference's implicit driver: one physical step of SDIRK4 (odeCode 0) or BDF of order k
 // (odeCode 1) in dual time, fsolve by LU-SGS / GMRES per gmresCode; the ODE object's history (BDF)
-// lives in the context, Reset() where the driver would construct a new ODE object
+// lives in the context, Reset() where the reference's solver would construct a new ODE object
 class ImplicitDualTimeStepGPU {
  public:
   ImplicitDualTimeStepGPU(Context& c, int odeCode, int bdfOrder = 2) : c_(c) {
