@@ -196,21 +196,23 @@ def test_features_and_harvest():
 
 
 @pytest.mark.gpu
-def test_gate_keeps_the_jacobi_tolerance():
+@pytest.mark.parametrize("precision", [1, 0])
+def test_gate_keeps_the_jacobi_tolerance(precision):
     """With any network -- trained, random or absurd -- the iteration still stops only at the
-    plain Jacobi tolerance, and the reconstruction matches the plain one to that tolerance."""
+    plain Jacobi tolerance, and the reconstruction matches the plain one to that tolerance
+    (FP32-bulk and FP64 contexts: the tensor-core warm start reads either coefficient type)."""
     torch, dev = _torch()
     from dnds_b200.learned import WarmStartNet
 
     tol = 1e-7
-    ref = _vortex(48, 22)
+    ref = _vortex(48, 22, precision)
     ref.ssprk3_step(0.5)
     n0, _ = ref.vr_to_tolerance(tol, 2000)
     x_ref = ref.get_urec()
     u_ref = ref.get_u()
     for scale in (1.0, 1e3):
         net = WarmStartNet(0, params=mo.random_params(23, scale=scale))
-        s = _vortex(48, 22)
+        s = _vortex(48, 22, precision)
         s.ssprk3_step(0.5)
         n1, acc = s.vr_to_tolerance(tol, 2000, net)
         assert n1 < 2000 and 0 <= acc <= s.N
