@@ -21,6 +21,8 @@ EXPORTS = [
     "dndsg_mlp_features", "dndsg_vr_to_tolerance", "dndsg_ssprk3_step_tol",
     "dndsg_lusgs_colours", "dndsg_lusgs_set_order", "dndsg_lusgs_matrix_init", "dndsg_lusgs_forward", "dndsg_lusgs_backward",
     "dndsg_bdf_begin", "dndsg_implicit_iteration", "dndsg_dual_reset", "dndsg_dual_step", "dndsg_lusgs_matvec", "dndsg_gmres_lusgs",
+    "dndsg_set_owned", "dndsg_rk_dt", "dndsg_rk_set_dt", "dndsg_rk_vr", "dndsg_rk_limit", "dndsg_rk_stage",
+    "dndsg_rk_finish", "dndsg_halo_pack", "dndsg_halo_unpack",
 ]
 _NO_STATUS = ("dndsg_destroy", "dndsg_last_error", "dndsg_n_cells", "dndsg_n_faces", "dndsg_mlp_destroy",
               "dndsg_mlp_last_error")
@@ -106,6 +108,15 @@ def lib():
     L.dndsg_dual_step.argtypes = [vp, C.POINTER(DualSettings), dbl, dbl, vp, vp, vp]
     L.dndsg_lusgs_matvec.argtypes = [vp, dbl, vp, vp, vp]
     L.dndsg_gmres_lusgs.argtypes = [vp, dbl, i32, i32, vp, vp, vp]
+    L.dndsg_set_owned.argtypes = [vp, vp]
+    L.dndsg_rk_dt.argtypes = [vp, dbl, C.POINTER(dbl), vp]
+    L.dndsg_rk_set_dt.argtypes = [vp, dbl, vp]
+    L.dndsg_rk_vr.argtypes = [vp, vp]
+    L.dndsg_rk_limit.argtypes = [vp, vp]
+    L.dndsg_rk_stage.argtypes = [vp, i32, vp]
+    L.dndsg_rk_finish.argtypes = [vp, vp]
+    L.dndsg_halo_pack.argtypes = [vp, i32, vp, i64, vp, vp]
+    L.dndsg_halo_unpack.argtypes = [vp, i32, vp, i64, vp, vp]
     for nm in EXPORTS:
         if nm not in _NO_STATUS:
             getattr(L, nm).restype = i32

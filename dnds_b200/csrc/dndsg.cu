@@ -87,6 +87,8 @@ struct dndsg_ctx {
   void *urec = nullptr, *urecNew = nullptr;  // T
   unsigned* flags = nullptr;
   unsigned long long* nreduced = nullptr;
+  uint8_t* owned = nullptr;  // [N] owned-cell mask of a partitioned run (null: every cell owned)
+  uint8_t* ownedBuf = nullptr;
   std::vector<void*> allocs;
 
   size_t tsize() const { return fp32 ? sizeof(float) : sizeof(double); }
@@ -389,6 +391,7 @@ __global__ void __launch_bounds__(kBlock) k_dt_cell(HotView<T> h, double cfl, do
   if (i < h.N) {
     d = dt_cell<T>(i, h, cfl, maxDt);
     h.dt[i] = d;
+    if (h.owned && !h.owned[i]) d = 1e300;  // a ghost cell's faces are incomplete: not in the minimum
     if (COPY_LAST) {
       const double2* s = reinterpret_cast<const double2*>(&h.u[i * 4]);
       double2* o = reinterpret_cast<double2*>(&h.uLast[i * 4]);
@@ -454,10 +457,11 @@ __global__ void __launch_bounds__(kBlock) k_cell_update(HotView<T> h, const doub
 }
 
 // per-block partial sums / maxima of |rhs|^p (EvaluateResidual)
-__global__ void k_residual(const double* rhs, const double* vol, int64_t n, int p, int volWise, double* partial) {
+__global__ void k_residual(const double* rhs, const double* vol, int64_t n, int p, int volWise, double* partial,
+                           const uint8_t* owned) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   double a[4] = {0, 0, 0, 0};
-  if (i < n)
+  if (i < n && (!owned || owned[i]))
     for (int v = 0; v < 4; v++) {
       double x = fabs(rhs[i * 4 + v]);
       if (p < 3) {
@@ -501,7 +505,7 @@ HotView<T> view(dndsg_ctx* c) {
   h.faceCenter = c->faceCenter; h.faceW0 = c->faceW0;
   h.u = c->u; h.uLast = c->uLast; h.rhs = c->rhs; h.dt = c->dt;
   h.urec = (const T*)c->urec; h.urecNew = (T*)c->urecNew;
-  h.flux = c->flux; h.lamA = c->lamA; h.dLam = c->dLam;
+  h.flux = c->flux; h.lamA = c->lamA; h.dLam = c->dLam; h.owned = c->owned;
   h.gamma = c->s.gamma;
   for (int k = 0; k < 4; k++) h.farU[k] = c->s.far_field[k];
   h.relax = c->s.jacobi_relax;
@@ -624,6 +628,28 @@ int run_step(dndsg_ctx* c, double cfl, double tEnd, cudaStream_t s) {
   }
   k_advance_time<<<1, 1, 0, s>>>(c->scal);
   return 0;
+}
+
+// stage k of SSP-RK3 after its VR sweep (and limiter): the face fluxes and the stage update
+template <class T>
+void run_rk_stage(dndsg_ctx* c, int stg, cudaStream_t s) {
+  const double cst[3] = {0.0, 1.0, 0.5};
+  launch_flux<T>(c, 1, 0.0, cst[stg], s);
+  HotView<T> h = view<T>(c);
+  if (stg == 0) k_cell_update<T, 0><<<grid_for(c->N), kBlock, 0, s>>>(h, c->scal);
+  else if (stg == 1) k_cell_update<T, 1><<<grid_for(c->N), kBlock, 0, s>>>(h, c->scal);
+  else k_cell_update<T, 2><<<grid_for(c->N), kBlock, 0, s>>>(h, c->scal);
+}
+
+// halo exchange buffers: PACK buf[k][0..w) = a[cells[k]][0..w), else the reverse
+template <class T, bool PACK>
+__global__ void k_halo_copy(T* a, const int32_t* cells, int64_t n, int w, T* buf) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= n * w) return;
+  const int64_t k = e / w, v = e - k * w;
+  const int64_t i = cells[k];
+  if (PACK) buf[e] = a[i * w + v];
+  else a[i * w + v] = buf[e];
 }
 
 template <class T>
@@ -1156,10 +1182,105 @@ int dndsg_ssprk3_step(dndsg_ctx* c, double cfl, double t_end, void* s) {
   return check_launch(c);
 }
 
+// ---- partitioned runs: owned-cell mask, SSP-RK3 by stage, halo pack / unpack
+int dndsg_set_owned(dndsg_ctx* c, const uint8_t* owned) {
+  if (!c) return DNDSG_BAD_ARGUMENT;
+  int rc;
+  if ((rc = set_device(c))) return rc;
+  if (!owned) {
+    c->owned = nullptr;
+    return 0;
+  }
+  if (!c->ownedBuf && (rc = dalloc(c, c->ownedBuf, sizeof(uint8_t) * c->N))) return rc;
+  DG_CUDA(c, cudaMemcpy(c->ownedBuf, owned, sizeof(uint8_t) * c->N, cudaMemcpyHostToDevice));
+  c->owned = c->ownedBuf;
+  return 0;
+}
+
+int dndsg_rk_dt(dndsg_ctx* c, double cfl, double* dt_min_out, void* s) {
+  if (!c || !dt_min_out || !(cfl > 0)) return DNDSG_BAD_ARGUMENT;
+  if (c->sa) return fail(c, DNDSG_UNSUPPORTED, "SA contexts run the implicit path");
+  int rc;
+  if ((rc = set_device(c))) return rc;
+  if (c->fp32) run_dt<float>(c, cfl, 1e100, true, st(s));
+  else run_dt<double>(c, cfl, 1e100, true, st(s));
+  if ((rc = check_launch(c))) return rc;
+  unsigned long long bits = 0;
+  DG_CUDA(c, cudaMemcpyAsync(&bits, c->scal + S_DTMIN, sizeof(bits), cudaMemcpyDeviceToHost, st(s)));
+  DG_CUDA(c, cudaStreamSynchronize(st(s)));
+  std::memcpy(dt_min_out, &bits, sizeof(double));
+  return 0;
+}
+
+int dndsg_rk_set_dt(dndsg_ctx* c, double dt, void* s) {
+  if (!c || !(dt >= 0)) return DNDSG_BAD_ARGUMENT;
+  int rc;
+  if ((rc = set_device(c))) return rc;
+  DG_CUDA(c, cudaMemcpyAsync(c->scal + S_DT, &dt, sizeof(double), cudaMemcpyHostToDevice, st(s)));
+  DG_CUDA(c, cudaStreamSynchronize(st(s)));
+  return 0;
+}
+
+int dndsg_rk_vr(dndsg_ctx* c, void* s) {
+  if (!c) return DNDSG_BAD_ARGUMENT;
+  if (c->fp32) run_vr<float>(c, false, st(s));
+  else run_vr<double>(c, false, st(s));
+  return check_launch(c);
+}
+
+int dndsg_rk_limit(dndsg_ctx* c, void* s) {
+  if (!c) return DNDSG_BAD_ARGUMENT;
+  if (!c->s.limiter) return 0;
+  if (c->fp32) run_limiter<float>(c, 0, st(s));
+  else run_limiter<double>(c, 0, st(s));
+  return check_launch(c);
+}
+
+int dndsg_rk_stage(dndsg_ctx* c, int stage, void* s) {
+  if (!c || stage < 0 || stage > 2) return DNDSG_BAD_ARGUMENT;
+  if (c->fp32) run_rk_stage<float>(c, stage, st(s));
+  else run_rk_stage<double>(c, stage, st(s));
+  return check_launch(c);
+}
+
+int dndsg_rk_finish(dndsg_ctx* c, void* s) {
+  if (!c) return DNDSG_BAD_ARGUMENT;
+  k_advance_time<<<1, 1, 0, st(s)>>>(c->scal);
+  return check_launch(c);
+}
+
+int dndsg_halo_pack(dndsg_ctx* c, int what, const int32_t* cells, int64_t n, void* buf, void* s) {
+  if (!c || (what != DNDSG_HALO_U && what != DNDSG_HALO_UREC) || n < 0 || (n && (!cells || !buf)))
+    return DNDSG_BAD_ARGUMENT;
+  if (n == 0) return 0;
+  const int w = what == DNDSG_HALO_U ? 4 : 20;
+  if (what == DNDSG_HALO_U)
+    k_halo_copy<double, true><<<grid_for(n * w), kBlock, 0, st(s)>>>(c->u, cells, n, w, (double*)buf);
+  else if (c->fp32)
+    k_halo_copy<float, true><<<grid_for(n * w), kBlock, 0, st(s)>>>((float*)c->urec, cells, n, w, (float*)buf);
+  else
+    k_halo_copy<double, true><<<grid_for(n * w), kBlock, 0, st(s)>>>((double*)c->urec, cells, n, w, (double*)buf);
+  return check_launch(c);
+}
+
+int dndsg_halo_unpack(dndsg_ctx* c, int what, const int32_t* cells, int64_t n, const void* buf, void* s) {
+  if (!c || (what != DNDSG_HALO_U && what != DNDSG_HALO_UREC) || n < 0 || (n && (!cells || !buf)))
+    return DNDSG_BAD_ARGUMENT;
+  if (n == 0) return 0;
+  const int w = what == DNDSG_HALO_U ? 4 : 20;
+  if (what == DNDSG_HALO_U)
+    k_halo_copy<double, false><<<grid_for(n * w), kBlock, 0, st(s)>>>(c->u, cells, n, w, (double*)buf);
+  else if (c->fp32)
+    k_halo_copy<float, false><<<grid_for(n * w), kBlock, 0, st(s)>>>((float*)c->urec, cells, n, w, (float*)buf);
+  else
+    k_halo_copy<double, false><<<grid_for(n * w), kBlock, 0, st(s)>>>((double*)c->urec, cells, n, w, (double*)buf);
+  return check_launch(c);
+}
+
 int dndsg_residual(dndsg_ctx* c, int p, int vol_wise, double* out, void* s) {
   if (!c || !out) return DNDSG_BAD_ARGUMENT;
   unsigned nb = grid_for(c->N);
-  k_residual<<<nb, kBlock, 0, st(s)>>>(c->rhs, c->vol, c->N, p, vol_wise, c->partial);
+  k_residual<<<nb, kBlock, 0, st(s)>>>(c->rhs, c->vol, c->N, p, vol_wise, c->partial, c->owned);
   int rc = check_launch(c);
   if (rc) return rc;
   std::vector<double> part(4 * (size_t)nb);

@@ -265,6 +265,7 @@ struct HotView {
   double* flux;             // [F][4]
   double* lamA;             // [F]
   double* dLam;             // [F]
+  const uint8_t* owned;     // [N] 1 for cells this context owns, or null (all owned); partitioned runs
   double gamma;
   double farU[4];
   double relax;

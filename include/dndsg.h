@@ -232,6 +232,36 @@ int dndsg_implicit_iteration(dndsg_ctx* ctx, double cfl, double dt_phys, double 
                              double t, double* inc_res_out, double* wall_flux_out, void* stream);
 
 /* ---------------------------------------------------------------------------
+ * Partitioned runs (the reference's MPI domain decomposition, one partition per
+ * context): a context built on a partition's cells plus its ghost cells (two
+ * layers; the outer layer closed with far-field faces) computes the owned cells
+ * exactly as the whole mesh would, given the ghosts' values after every VR
+ * sweep (and limiter) and every stage update.  dndsg_set_owned marks the owned
+ * cells (host [n_cells] 0/1; NULL: all owned): the dt minimum and
+ * dndsg_residual run over owned cells only.  One SSP-RK3 step by stage
+ * (ExplicitSSPRK3LocalDt::Step, DNDS_ODE.hpp:131-177):
+ *   dndsg_rk_dt (local minimum; the caller reduces it over all partitions and
+ *   clips it to the end time) -> dndsg_rk_set_dt -> 3 x [dndsg_rk_vr ->
+ *   exchange urec -> dndsg_rk_limit -> exchange urec -> dndsg_rk_stage(k) ->
+ *   exchange u] -> dndsg_rk_finish.
+ * dndsg_halo_pack / unpack gather / scatter whole cells of u ([n][4] double) or
+ * urec ([n][5][4] of the context's precision) at device cell indices, to or
+ * from a device buffer (the caller moves buffers between partitions: a device
+ * copy on one GPU, NCCL send / receive across GPUs).
+ * ------------------------------------------------------------------------ */
+#define DNDSG_HALO_U 0
+#define DNDSG_HALO_UREC 1
+int dndsg_set_owned(dndsg_ctx* ctx, const uint8_t* owned);
+int dndsg_rk_dt(dndsg_ctx* ctx, double cfl, double* dt_min_out, void* stream);
+int dndsg_rk_set_dt(dndsg_ctx* ctx, double dt, void* stream);
+int dndsg_rk_vr(dndsg_ctx* ctx, void* stream);
+int dndsg_rk_limit(dndsg_ctx* ctx, void* stream);
+int dndsg_rk_stage(dndsg_ctx* ctx, int stage, void* stream);
+int dndsg_rk_finish(dndsg_ctx* ctx, void* stream);
+int dndsg_halo_pack(dndsg_ctx* ctx, int what, const int32_t* cells, int64_t n, void* buf, void* stream);
+int dndsg_halo_unpack(dndsg_ctx* ctx, int what, const int32_t* cells, int64_t n, const void* buf, void* stream);
+
+/* ---------------------------------------------------------------------------
  * Dual time stepping, the reference's implicit driver: one physical step of
  * ImplicitBDFDualTimeStep (order k; DNDS_ODE.hpp:392-497) or of the 3-stage
  * ImplicitSDIRK4DualTimeStep (DNDS_ODE.hpp:269-390), each internal iteration
