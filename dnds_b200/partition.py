@@ -188,3 +188,92 @@ class PartitionedRun:
     def close(self):
         for s in self.solvers:
             s.close()
+
+
+def halo_exchange(send: dict, recv: dict, group=None):
+    """Point-to-point exchange of packed halo buffers between ranks: ``send[q]`` goes to rank q and
+    ``recv[q]`` (preallocated, same length as what q sends) is filled from rank q.  One batch of
+    paired send / receive operations, so that no ordering of the ranks can deadlock (NCCL for device
+    buffers, gloo for host buffers)."""
+    import torch.distributed as dist
+
+    ops = []
+    for q in sorted(set(send) | set(recv)):
+        if q in send:
+            ops.append(dist.P2POp(dist.isend, send[q], q, group))
+        if q in recv:
+            ops.append(dist.P2POp(dist.irecv, recv[q], q, group))
+    if ops:
+        for r in dist.batch_isend_irecv(ops):
+            r.wait()
+
+
+class DistributedRun:
+    """One part per rank (``torch.distributed`` initialised, rank r on GPU LOCAL_RANK): every rank
+    partitions the mesh the same way and holds part ``rank``; ghosts travel by ``halo_exchange`` of
+    the buffers that ``dndsg_halo_pack`` fills, dt is reduced by an all-reduce (MIN)."""
+
+    def __init__(self, mesh: M.Mesh, cfg: dict, precision: int = 0, device: int = 0):
+        import torch
+        import torch.distributed as dist
+
+        from .solver import Solver
+
+        self.rank, world = dist.get_rank(), dist.get_world_size()
+        self.mesh, self.parts = mesh, partition_mesh(mesh, world)
+        self.part = self.parts[self.rank]
+        self.s = Solver(self.part.mesh, cfg, device=device, precision=precision)
+        self.dev = torch.device(f"cuda:{device}")
+        self.urec_dtype = torch.float32 if precision == 1 else torch.float64
+        self.limiter = bool(cfg.get("useLimiter", False))
+        mask = np.zeros(self.part.mesh.n_cells, dtype=np.uint8)
+        mask[: self.part.n_owned] = 1
+        self.s._check(self.s.L.dndsg_set_owned(self.s.h, mask.ctypes.data_as(C.c_void_p)))
+        self.send_idx = {q: torch.tensor(v, device=self.dev) for q, v in self.part.send.items()}
+        self.recv_idx = {q: torch.tensor(v, device=self.dev) for q, v in self.part.recv.items()}
+
+    def set_u(self, u: np.ndarray):
+        self.s.set_u(np.ascontiguousarray(u[self.part.cells]))
+
+    def owned_u(self) -> np.ndarray:
+        return self.s.get_u()[: self.part.n_owned]
+
+    def exchange(self, what: int):
+        import torch
+
+        s, w = self.s, 4 if what == 0 else 20
+        dt = torch.float64 if what == 0 else self.urec_dtype
+        send, recv = {}, {}
+        for q, idx in self.send_idx.items():
+            send[q] = torch.empty((len(idx), w), dtype=dt, device=self.dev)
+            s._check(s.L.dndsg_halo_pack(s.h, what, C.c_void_p(idx.data_ptr()), len(idx),
+                                         C.c_void_p(send[q].data_ptr()), s.stream))
+        for q, idx in self.recv_idx.items():
+            recv[q] = torch.empty((len(idx), w), dtype=dt, device=self.dev)
+        torch.cuda.synchronize(self.dev)
+        halo_exchange(send, recv)
+        for q, idx in self.recv_idx.items():
+            s._check(s.L.dndsg_halo_unpack(s.h, what, C.c_void_p(idx.data_ptr()), len(idx),
+                                           C.c_void_p(recv[q].data_ptr()), s.stream))
+
+    def ssprk3_step(self, cfl: float, t_end: float = 1e300) -> float:
+        import torch
+        import torch.distributed as dist
+
+        s = self.s
+        d = C.c_double()
+        s._check(s.L.dndsg_rk_dt(s.h, float(cfl), C.byref(d), s.stream))
+        dmin = torch.tensor([d.value], dtype=torch.float64, device=self.dev)
+        dist.all_reduce(dmin, op=dist.ReduceOp.MIN)
+        dt = max(0.0, min(float(dmin.item()), t_end - s.time))
+        s._check(s.L.dndsg_rk_set_dt(s.h, dt, s.stream))
+        for k in range(3):
+            s._check(s.L.dndsg_rk_vr(s.h, s.stream))
+            self.exchange(1)
+            if self.limiter:
+                s._check(s.L.dndsg_rk_limit(s.h, s.stream))
+                self.exchange(1)
+            s._check(s.L.dndsg_rk_stage(s.h, k, s.stream))
+            self.exchange(0)
+        s._check(s.L.dndsg_rk_finish(s.h, s.stream))
+        return dt
