@@ -233,8 +233,9 @@ int dndsg_implicit_iteration(dndsg_ctx* ctx, double cfl, double dt_phys, double 
 
 /* ---------------------------------------------------------------------------
  * Partitioned runs (the reference's MPI domain decomposition, one partition per
- * context): a context built on a partition's cells plus its ghost cells (two
- * layers; the outer layer closed with far-field faces) computes the owned cells
+ * context): a context built on a partition's cells plus one layer of ghost cells
+ * (every cell across a face of an owned cell; a ghost's faces to cells outside
+ * the partition closed as far-field faces) computes the owned cells
  * exactly as the whole mesh would, given the ghosts' values after every VR
  * sweep (and limiter) and every stage update.  dndsg_set_owned marks the owned
  * cells (host [n_cells] 0/1; NULL: all owned): the dt minimum and
