@@ -1964,17 +1964,25 @@ __device__ __forceinline__ void lusgs_prefetch(const HotView<T>& h, const int32_
 
 constexpr int kRecMaxLevels = 4095;  // level offsets of one sweep held in shared memory
 
-// ---- scan-order sweep over precomputed neighbour matrices.
+// ---- scan-order sweep over precomputed neighbour records.
 // The neighbour term of UpdateLUSGSForward/Backward, w_q (dF(U_q; n_q, dU_q) - lam_q dU_q)
 // (fluxJacobian0_Right_Times_du, DNDS_FV_EulerEvaluator.hpp:928-956), is linear in the neighbour's
-// increment dU_q, and its matrix depends only on data that is fixed during the sweep.  So one
-// parallel pass writes, per schedule position, the 4x4 matrices of its up to 4 neighbours (plus the
-// U5 transport row for SA contexts), and the sequential level walk is left with matrix-vector
-// products over increments that mostly sit in a shared-memory ring.
+// increment dU_q, and everything else in it is fixed during the sweep.  So one parallel pass writes,
+// per schedule position, the dU-independent quantities of its up to 4 neighbour terms, and the
+// sequential level walk is left with a short product per neighbour over increments that mostly sit
+// in a shared-memory ring.  With a = nx dU1 + ny dU2 - vn dU0 (= rho dvn) and
+// dp = (gamma - 1)(dU3 - vx dU1 - vy dU2 + kq dU0), kq = |v|^2 / 2:
+//   dF = (nx dU1 + ny dU2, vn dU1 + vx a + nx dp, vn dU2 + vy a + ny dp, H a + vn (dU3 + dp)),
+// the term is w dF - wl dU (wl = w lam), and the U5 row of an SA context adds c a + (w vn - wl) dU5
+// with c = w nuTilde_q / rho_q.  Ten doubles per neighbour instead of the 4x4 matrix (16, plus 4 for
+// the U5 row): the walk moves every record through one SM's shared memory, and record bytes are
+// what its levels wait on.  Fields are grouped in 16-byte pairs and read as such.
+struct __align__(16) LuSlot {
+  double vx, vy, vn, H, kq, wl, nx, ny, w, c;
+};
 struct __align__(16) LuMatF {
-  double M[4][16];  // per face slot: row-major w (A_n(U) - lam I)
-  double base[4];   // initial sum: the BDF rhs (forward) or 0 (backward)
-  double add[4];    // added to di * sum: 0 (forward) or the forward increment (backward)
+  LuSlot s[4];      // per face slot
+  double x0[4];     // forward: the BDF rhs, where the sum starts; backward: the forward increment, added to di * sum
   double di;
   int32_t i, use;   // cell; bit k set when slot k holds a neighbour that enters this sweep
   int32_t j[4];     // neighbour cell
@@ -1982,30 +1990,16 @@ struct __align__(16) LuMatF {
 };
 struct __align__(16) LuMatS {
   LuMatF f;
-  double S[4][4];  // per face slot: coefficients of dU0, dU1, dU2 and dU5 in the U5 row
-  double baseS, addS, diS, padS;
+  double x0S, diS;  // the U5 part of x0 and di
+  double pad[2];    // 432-B stride: 16-byte loads of 32 consecutive records hit every bank evenly
 };
-static_assert(sizeof(LuMatF) == 624 && sizeof(LuMatS) == 784, "records are bulk-copied in 16-byte units");
+static_assert(sizeof(LuMatF) == 400 && sizeof(LuMatS) == 432, "records are bulk-copied in 16-byte units");
 template <bool SA>
 using LuMat = typename std::conditional<SA, LuMatS, LuMatF>::type;
 __device__ __forceinline__ LuMatF& mat_flow(LuMatF& r) { return r; }
 __device__ __forceinline__ LuMatF& mat_flow(LuMatS& r) { return r.f; }
 __device__ __forceinline__ const LuMatF& mat_flow(const LuMatF& r) { return r; }
 __device__ __forceinline__ const LuMatF& mat_flow(const LuMatS& r) { return r.f; }
-
-// w (A_n(U) - lam I), the matrix of flux_jac_times_du: with q2 = |v|^2, H = (E + p)/rho,
-// dp = (gamma - 1)(dU3 - vx dU1 - vy dU2 + q2/2 dU0) and dvn = (nx dU1 + ny dU2 - vn dU0)/rho
-__device__ __forceinline__ void flux_jac_matrix(const double U[4], double nx, double ny, double lam, double w,
-                                                double gamma, double* M) {
-  const double ir = 1.0 / U[0];
-  const double vx = U[1] * ir, vy = U[2] * ir, q2 = vx * vx + vy * vy, g1 = gamma - 1;
-  const double p = g1 * (U[3] - 0.5 * U[0] * q2), H = (U[3] + p) * ir, vn = vx * nx + vy * ny, k = 0.5 * g1 * q2;
-  const double m[16] = {-lam, nx, ny, 0.0,
-                        k * nx - vx * vn, vn + vx * nx - g1 * vx * nx - lam, vx * ny - g1 * vy * nx, g1 * nx,
-                        k * ny - vy * vn, vy * nx - g1 * vx * ny, vn + vy * ny - g1 * vy * ny - lam, g1 * ny,
-                        vn * (k - H), H * nx - g1 * vx * vn, H * ny - g1 * vy * vn, gamma * vn - lam};
-  for (int e = 0; e < 16; e++) M[e] = w * m[e];
-}
 
 // writes the record of every schedule position of one sweep, all positions in parallel
 template <class T, bool FWD, bool SA>
@@ -2020,37 +2014,39 @@ __global__ void __launch_bounds__(kBlock) k_lusgs_pack_mat(HotView<T> h, SaView<
   LuMatF& f = mat_flow(rec[t]);
   const int4 p4 = reinterpret_cast<const int4*>(nbP)[t];
   const int32_t pa[4] = {p4.x, p4.y, p4.z, p4.w};
+  const double g1 = h.gamma - 1;
   int use = 0;
   for (int k = 0; k < 4; k++) {
-    flux_jac_matrix(p.U[k], p.nx[k], p.ny[k], p.lam[k], p.w[k], h.gamma, f.M[k]);
+    const double* U = p.U[k];
+    const double ir = 1.0 / U[0];
+    const double vx = U[1] * ir, vy = U[2] * ir, q2 = vx * vx + vy * vy;
+    const double pr = g1 * (U[3] - 0.5 * U[0] * q2);
+    LuSlot& q = f.s[k];
+    q.vx = vx;
+    q.vy = vy;
+    q.vn = vx * p.nx[k] + vy * p.ny[k];
+    q.H = (U[3] + pr) * ir;
+    q.kq = 0.5 * q2;
+    q.wl = p.w[k] * p.lam[k];
+    q.nx = p.nx[k];
+    q.ny = p.ny[k];
+    q.w = p.w[k];
+    q.c = SA ? p.w[k] * sa.u[p.j[k]] * ir : 0.0;
     f.j[k] = p.j[k];
     f.p[k] = pa[k];
     use |= p.use[k] ? 1 << k : 0;
   }
   double add[4] = {0, 0, 0, 0};
   if (!FWD) load4<double>(&inc[p.i * 4], add);
-  for (int v = 0; v < 4; v++) {
-    f.base[v] = FWD ? p.base[v] : 0.0;
-    f.add[v] = add[v];
-  }
+  for (int v = 0; v < 4; v++) f.x0[v] = FWD ? p.base[v] : add[v];
   f.di = p.di;
   f.i = (int32_t)p.i;
   f.use = use;
   if constexpr (SA) {
     LuMatS& r = rec[t];
-    for (int k = 0; k < 4; k++) {
-      const double* U = p.U[k];
-      const double ir = 1.0 / U[0];
-      const double vn = (U[1] * p.nx[k] + U[2] * p.ny[k]) * ir, c = p.w[k] * sa.u[p.j[k]] * ir;
-      r.S[k][0] = -c * vn;
-      r.S[k][1] = c * p.nx[k];
-      r.S[k][2] = c * p.ny[k];
-      r.S[k][3] = p.w[k] * (vn - p.lam[k]);
-    }
-    r.baseS = FWD ? sa.rhs[p.i] : 0.0;
-    r.addS = FWD ? 0.0 : sa.inc[p.i];
+    r.x0S = FWD ? sa.rhs[p.i] : sa.inc[p.i];
     r.diS = sa.Dinv[p.i];
-    r.padS = 0.0;
+    r.pad[0] = r.pad[1] = 0.0;
   }
 }
 
@@ -2067,17 +2063,28 @@ static_assert(mat_smem<true>() <= 227 * 1024, "level walk fits the shared memory
 // one position of the level walk.  A neighbour's increment comes from the ring when its position
 // is at or after ringLo (it was written there by this walk and not yet overwritten), else from
 // global memory.  The sum runs over the slots in the order of lusgs_cell.
+__device__ __forceinline__ double2 ld2(const double* p) { return *reinterpret_cast<const double2*>(p); }
 template <bool FWD, bool SA, class T>
 __device__ __forceinline__ void lusgs_mat_cell(const SaView<T>& sa, const LuMat<SA>& r, int32_t t, int32_t ringLo,
-                                               double* ringF, double* ringS, double* inc) {
+                                               double* ringF, double* ringS, double* inc, double g1) {
   const LuMatF& f = mat_flow(r);
-  double buf[4], bufS = 0.0;
-  for (int v = 0; v < 4; v++) buf[v] = f.base[v];
-  if constexpr (SA) bufS = r.baseS;
+  const double2 x01 = ld2(&f.x0[0]), x23 = ld2(&f.x0[2]);
+  const double x0[4] = {x01.x, x01.y, x23.x, x23.y};
+  double buf[4], bufS = 0.0, x0S = 0.0, diS = 0.0;
+  for (int v = 0; v < 4; v++) buf[v] = FWD ? x0[v] : 0.0;
+  if constexpr (SA) {
+    const double2 sd = ld2(&r.x0S);
+    x0S = sd.x;
+    diS = sd.y;
+    bufS = FWD ? x0S : 0.0;
+  }
+  const int4 j4 = *reinterpret_cast<const int4*>(f.j), p4 = *reinterpret_cast<const int4*>(f.p);
+  const int32_t ja[4] = {j4.x, j4.y, j4.z, j4.w}, pa[4] = {p4.x, p4.y, p4.z, p4.w};
+  const int use = f.use;
 #pragma unroll
   for (int q = 0; q < 4; q++) {
-    if (!(f.use >> q & 1)) continue;
-    const int32_t pj = f.p[q];
+    if (!(use >> q & 1)) continue;
+    const int32_t pj = pa[q];
     double dU[4], dS = 0.0;
     if (pj >= ringLo) {
       const double2* s = reinterpret_cast<const double2*>(ringF + 4 * (pj & (kMatRing - 1)));
@@ -2085,21 +2092,27 @@ __device__ __forceinline__ void lusgs_mat_cell(const SaView<T>& sa, const LuMat<
       dU[0] = a.x; dU[1] = a.y; dU[2] = b.x; dU[3] = b.y;
       if constexpr (SA) dS = ringS[pj & (kMatRing - 1)];
     } else {
-      load4<double>(&inc[(int64_t)f.j[q] * 4], dU);
-      if constexpr (SA) dS = sa.inc[f.j[q]];
+      load4<double>(&inc[(int64_t)ja[q] * 4], dU);
+      if constexpr (SA) dS = sa.inc[ja[q]];
     }
-    const double* M = f.M[q];
-    for (int v = 0; v < 4; v++) buf[v] += M[4 * v] * dU[0] + M[4 * v + 1] * dU[1] + M[4 * v + 2] * dU[2] + M[4 * v + 3] * dU[3];
-    if constexpr (SA) bufS += r.S[q][0] * dU[0] + r.S[q][1] * dU[1] + r.S[q][2] * dU[2] + r.S[q][3] * dS;
+    const double* sl = &f.s[q].vx;
+    const double2 vxy = ld2(sl), vnH = ld2(sl + 2), kwl = ld2(sl + 4), nxy = ld2(sl + 6), wc = ld2(sl + 8);
+    const double dmn = nxy.x * dU[1] + nxy.y * dU[2];
+    const double a = dmn - vnH.x * dU[0];
+    const double dp = g1 * (dU[3] - vxy.x * dU[1] - vxy.y * dU[2] + kwl.x * dU[0]);
+    const double dF[4] = {dmn, vnH.x * dU[1] + vxy.x * a + nxy.x * dp, vnH.x * dU[2] + vxy.y * a + nxy.y * dp,
+                          vnH.y * a + vnH.x * (dU[3] + dp)};
+    for (int v = 0; v < 4; v++) buf[v] += wc.x * dF[v] - kwl.y * dU[v];
+    if constexpr (SA) bufS += wc.y * a + (wc.x * vnH.x - kwl.y) * dS;
   }
   double o[4];
-  for (int v = 0; v < 4; v++) o[v] = f.add[v] + f.di * buf[v];
+  for (int v = 0; v < 4; v++) o[v] = FWD ? f.di * buf[v] : x0[v] + f.di * buf[v];
   double2* g = reinterpret_cast<double2*>(&inc[(int64_t)f.i * 4]);
   double2* s = reinterpret_cast<double2*>(ringF + 4 * (t & (kMatRing - 1)));
   g[0] = s[0] = make_double2(o[0], o[1]);
   g[1] = s[1] = make_double2(o[2], o[3]);
   if constexpr (SA) {
-    const double oS = r.addS + r.diS * bufS;
+    const double oS = FWD ? diS * bufS : x0S + diS * bufS;
     sa.inc[f.i] = oS;
     ringS[t & (kMatRing - 1)] = oS;
   }
@@ -2116,7 +2129,7 @@ constexpr int mat_threads() { return kRecBlock + 32; }
 template <class T, bool FWD, bool SA>
 __global__ void __launch_bounds__(mat_threads<SA>()) k_lusgs_levels_mat(SaView<T> sa, const LuMat<SA>* rec,
                                                                         const int64_t* off, int nlev, double* inc,
-                                                                        unsigned* flags) {
+                                                                        double g1, unsigned* flags) {
   using R = LuMat<SA>;
   constexpr int NT = kRecBlock;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -2157,7 +2170,7 @@ __global__ void __launch_bounds__(mat_threads<SA>()) k_lusgs_levels_mat(SaView<T
       if (ok)
         for (int32_t t = b + tid; t < e; t += kRecBlock)
           lusgs_mat_cell<FWD, SA>(sa, t - b < kRecBlock ? buf[(l & 1) * kRecBlock + (t - b)] : rec[t], t, ringLo, ringF,
-                                  ringS, inc);
+                                  ringS, inc, g1);
     }
     if (__syncthreads_or(!ok)) {
       failed = true;
@@ -2423,11 +2436,11 @@ void launch_lusgs_sweep(dndsg_ctx* c, bool forward, double alpha, const double* 
     if (forward) {
       k_lusgs_pack_mat<T, true, false><<<grid_for(c->N), kBlock, 0, s>>>(h, none, cells, nf, nj, np, c->N, alpha, c->Dinv,
                                                                           rhs, inc, rec);
-      k_lusgs_levels_mat<T, true, false><<<1, mat_threads<false>(), mat_smem<false>(), s>>>(none, rec, od, nb, inc, c->flags);
+      k_lusgs_levels_mat<T, true, false><<<1, mat_threads<false>(), mat_smem<false>(), s>>>(none, rec, od, nb, inc, h.gamma - 1, c->flags);
     } else {
       k_lusgs_pack_mat<T, false, false><<<grid_for(c->N), kBlock, 0, s>>>(h, none, cells, nf, nj, np, c->N, alpha, c->Dinv,
                                                                            rhs, inc, rec);
-      k_lusgs_levels_mat<T, false, false><<<1, mat_threads<false>(), mat_smem<false>(), s>>>(none, rec, od, nb, inc, c->flags);
+      k_lusgs_levels_mat<T, false, false><<<1, mat_threads<false>(), mat_smem<false>(), s>>>(none, rec, od, nb, inc, h.gamma - 1, c->flags);
     }
     return;
   }
@@ -2730,11 +2743,11 @@ void launch_lusgs_sweep_sa(dndsg_ctx* c, bool forward, double alpha, const doubl
     if (forward) {
       k_lusgs_pack_mat<T, true, true><<<grid_for(c->N), kBlock, 0, s>>>(h, sa, cells, nf, nj, np, c->N, alpha, c->Dinv,
                                                                          rhs4, inc4, rec);
-      k_lusgs_levels_mat<T, true, true><<<1, mat_threads<true>(), mat_smem<true>(), s>>>(sa, rec, od, nb, inc4, c->flags);
+      k_lusgs_levels_mat<T, true, true><<<1, mat_threads<true>(), mat_smem<true>(), s>>>(sa, rec, od, nb, inc4, h.gamma - 1, c->flags);
     } else {
       k_lusgs_pack_mat<T, false, true><<<grid_for(c->N), kBlock, 0, s>>>(h, sa, cells, nf, nj, np, c->N, alpha, c->Dinv,
                                                                           rhs4, inc4, rec);
-      k_lusgs_levels_mat<T, false, true><<<1, mat_threads<true>(), mat_smem<true>(), s>>>(sa, rec, od, nb, inc4, c->flags);
+      k_lusgs_levels_mat<T, false, true><<<1, mat_threads<true>(), mat_smem<true>(), s>>>(sa, rec, od, nb, inc4, h.gamma - 1, c->flags);
     }
     return;
   }
