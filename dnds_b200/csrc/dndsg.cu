@@ -2167,10 +2167,12 @@ __global__ void __launch_bounds__(mat_threads<SA>()) k_lusgs_levels_mat(SaView<T
     bool ok = true;
     if (tid < NT && b + tid < e) {
       ok = mbar_wait(smem_u32(&bars[l & 1]), (l >> 1) & 1, kWaitLimit);
-      if (ok)
-        for (int32_t t = b + tid; t < e; t += kRecBlock)
-          lusgs_mat_cell<FWD, SA>(sa, t - b < kRecBlock ? buf[(l & 1) * kRecBlock + (t - b)] : rec[t], t, ringLo, ringF,
-                                  ringS, inc, g1);
+      if (ok) {
+        // the record from the shared buffer, as a shared-memory reference (ld.shared, not generic loads)
+        lusgs_mat_cell<FWD, SA>(sa, buf[(l & 1) * kRecBlock + tid], b + tid, ringLo, ringF, ringS, inc, g1);
+        for (int32_t t = b + tid + kRecBlock; t < e; t += kRecBlock)
+          lusgs_mat_cell<FWD, SA>(sa, rec[t], t, ringLo, ringF, ringS, inc, g1);
+      }
     }
     if (__syncthreads_or(!ok)) {
       failed = true;
