@@ -69,7 +69,7 @@ struct dndsg_ctx {
   int64_t *fwdOffDev = nullptr, *bwdOffDev = nullptr;  // level offsets on the device (scan-order mode)
   int32_t *fwdNbF = nullptr, *fwdNbJ = nullptr, *bwdNbF = nullptr, *bwdNbJ = nullptr;  // [pos][4] records
   void* lusgsMat = nullptr;  // per-position neighbour-matrix records of one sweep (scan-order mode)
-  int32_t *fwdNbP = nullptr, *bwdNbP = nullptr;  // [pos][4] neighbour schedule positions
+  int32_t *fwdNbP = nullptr, *bwdNbP = nullptr;  // [pos][4] neighbour schedule positions (-1: not in the ring)
   int64_t maxLevelWidth = 0;
   std::vector<int32_t> colourHost;  // greedy colouring, kept for dndsg_lusgs_colours
   int lusgsOrder = 0;               // 0 colour batches, 1 level-scheduled scan order
@@ -2060,13 +2060,14 @@ constexpr size_t mat_smem() {
 }
 static_assert(mat_smem<true>() <= 227 * 1024, "level walk fits the shared memory of one block");
 
-// one position of the level walk.  A neighbour's increment comes from the ring when its position
-// is at or after ringLo (it was written there by this walk and not yet overwritten), else from
-// global memory.  The sum runs over the slots in the order of lusgs_cell.
+// one position of the level walk.  A neighbour's increment comes from the ring when the record
+// gives its position (the schedule set that up: written there by this walk and not yet
+// overwritten), else (position -1) from global memory.  The sum runs over the slots in the order
+// of lusgs_cell.
 __device__ __forceinline__ double2 ld2(const double* p) { return *reinterpret_cast<const double2*>(p); }
 template <bool FWD, bool SA, class T>
-__device__ __forceinline__ void lusgs_mat_cell(const SaView<T>& sa, const LuMat<SA>& r, int32_t t, int32_t ringLo,
-                                               double* ringF, double* ringS, double* inc, double g1) {
+__device__ __forceinline__ void lusgs_mat_cell(const SaView<T>& sa, const LuMat<SA>& r, int32_t t, double* ringF,
+                                               double* ringS, double* inc, double g1) {
   const LuMatF& f = mat_flow(r);
   const double2 x01 = ld2(&f.x0[0]), x23 = ld2(&f.x0[2]);
   const double x0[4] = {x01.x, x01.y, x23.x, x23.y};
@@ -2086,7 +2087,7 @@ __device__ __forceinline__ void lusgs_mat_cell(const SaView<T>& sa, const LuMat<
     if (!(use >> q & 1)) continue;
     const int32_t pj = pa[q];
     double dU[4], dS = 0.0;
-    if (pj >= ringLo) {
+    if (pj >= 0) {
       const double2* s = reinterpret_cast<const double2*>(ringF + 4 * (pj & (kMatRing - 1)));
       const double2 a = s[0], b = s[1];
       dU[0] = a.x; dU[1] = a.y; dU[2] = b.x; dU[3] = b.y;
@@ -2158,26 +2159,28 @@ __global__ void __launch_bounds__(mat_threads<SA>()) k_lusgs_levels_mat(SaView<T
     for (uint32_t o = 0; o < bytes; o += kBulkChunk) bulk_g2s(dst + o, src + o, min(kBulkChunk, bytes - o), bar);
   };
   if (producer && nlev > 0) issue(0);
-  int lo = 0, l = 0;
+  int l = 0;
   bool failed = false;
+  int32_t b = so[0], e = nlev > 0 ? so[1] : 0;
   for (; l < nlev; l++) {
     if (producer && l + 1 < nlev) issue(l + 1);
-    while (so[l + 1] - so[lo] > kMatRing) lo++;
-    const int32_t ringLo = so[lo], b = so[l], e = so[l + 1];
+    const int32_t e2 = so[min(l + 2, nlev)];  // the next level's end, read ahead
     bool ok = true;
     if (tid < NT && b + tid < e) {
       ok = mbar_wait(smem_u32(&bars[l & 1]), (l >> 1) & 1, kWaitLimit);
       if (ok) {
         // the record from the shared buffer, as a shared-memory reference (ld.shared, not generic loads)
-        lusgs_mat_cell<FWD, SA>(sa, buf[(l & 1) * kRecBlock + tid], b + tid, ringLo, ringF, ringS, inc, g1);
+        lusgs_mat_cell<FWD, SA>(sa, buf[(l & 1) * kRecBlock + tid], b + tid, ringF, ringS, inc, g1);
         for (int32_t t = b + tid + kRecBlock; t < e; t += kRecBlock)
-          lusgs_mat_cell<FWD, SA>(sa, rec[t], t, ringLo, ringF, ringS, inc, g1);
+          lusgs_mat_cell<FWD, SA>(sa, rec[t], t, ringF, ringS, inc, g1);
       }
     }
     if (__syncthreads_or(!ok)) {
       failed = true;
       break;
     }
+    b = e;
+    e = e2;
   }
   if (failed && producer) {  // let the copies in flight land before the block exits
     atomicOr(flags, kFlagTimeout);
@@ -2395,9 +2398,20 @@ int set_scan_order(dndsg_ctx* c, const int64_t* scan2cell) {
       }
     }
   };
+  // the level walk keeps the increments of the last kMatRing positions in a ring; a neighbour at
+  // position pj is still there during level l when pj + kMatRing >= off[l + 1] (the position that
+  // overwrites its slot comes later).  Otherwise the walk reads global memory: position -1.
+  auto ring_or_global = [&](const std::vector<int64_t>& off, std::vector<int32_t>& np) {
+    for (size_t l = 0; l + 1 < off.size(); l++)
+      for (int64_t t = off[l]; t < off[l + 1]; t++)
+        for (int k = 0; k < 4; k++)
+          if (np[4 * t + k] >= 0 && np[4 * t + k] + kMatRing < off[l + 1]) np[4 * t + k] = -1;
+  };
   std::vector<int32_t> ff, fj, fp, bf, bj, bp;
   records(fwd, true, ff, fj, fp);
   records(bwd, false, bf, bj, bp);
+  ring_or_global(c->fwdOff, fp);
+  ring_or_global(c->bwdOff, bp);
   if (!c->fwdNbF)
     if ((rc = dalloc(c, c->fwdNbF, sizeof(int32_t) * 4 * N)) || (rc = dalloc(c, c->fwdNbJ, sizeof(int32_t) * 4 * N)) ||
         (rc = dalloc(c, c->bwdNbF, sizeof(int32_t) * 4 * N)) || (rc = dalloc(c, c->bwdNbJ, sizeof(int32_t) * 4 * N)) ||

@@ -291,6 +291,30 @@ def test_line_scan_order_matches_oracle(oracle_lib):
 
 
 @pytest.mark.gpu
+def test_wide_levels_read_records_and_increments_from_global_memory(oracle_lib):
+    """The line order on a C-mesh 300 cells around makes levels of about 300 positions: a level
+    holds more positions than the walk buffers records for (128; the rest are read from global
+    memory), and a neighbour one level back is sometimes more than the 256 positions of the
+    increment ring behind (read from global memory), sometimes not.  The sweep still computes what
+    the oracle's sequential sweep in that order computes."""
+    m = M.naca0012_cmesh(200, 50, 8, first=2e-3, far=10.0, wall_bc=M.BC_WALL_EULER)
+    cfg = _cfg()
+    scan = M.line_scan_order(m)
+    u0 = _free_stream(m, cfg)
+    s = _gpu(m, cfg)
+    assert s.lusgs_set_order(1, scan) == 2 * (8 + 1)
+    s.set_u(u0)
+    s.bdf_begin()
+    o = _oracle(oracle_lib, m, cfg)
+    o.set_u(u0)
+    for it in range(5):
+        s.implicit_iteration(100.0)
+        o.implicit_iteration(100.0, u0, scan2cell=scan)
+    ref = o.get_u()
+    assert np.abs(s.get_u() - ref).max() < 1e-10 * np.abs(ref).max()
+
+
+@pytest.mark.gpu
 def test_steady_state_matches_natural_order_oracle(oracle_lib):
     m, cfg = _naca_small(), _cfg()
     u0 = _free_stream(m, cfg)
