@@ -1984,9 +1984,9 @@ struct __align__(16) LuMatF {
   LuSlot s[4];      // per face slot
   double x0[4];     // forward: the BDF rhs, where the sum starts; backward: the forward increment, added to di * sum
   double di;
-  int32_t i, use;   // cell; bit k set when slot k holds a neighbour that enters this sweep
+  int32_t i, nu;    // cell; number of neighbours that enter this sweep, in s / j / p [0, nu) in face-slot order
   int32_t j[4];     // neighbour cell
-  int32_t p[4];     // neighbour schedule position in this sweep
+  int32_t p[4];     // neighbour schedule position in this sweep (-1: not in the ring; read global memory)
 };
 struct __align__(16) LuMatS {
   LuMatF f;
@@ -2015,13 +2015,18 @@ __global__ void __launch_bounds__(kBlock) k_lusgs_pack_mat(HotView<T> h, SaView<
   const int4 p4 = reinterpret_cast<const int4*>(nbP)[t];
   const int32_t pa[4] = {p4.x, p4.y, p4.z, p4.w};
   const double g1 = h.gamma - 1;
-  int use = 0;
+  int nu = 0;
+  for (int k = 0; k < 4; k++) {  // the used slots first, in slot order (the order of lusgs_cell's sum)
+    f.j[k] = p.i;
+    f.p[k] = 0;
+  }
   for (int k = 0; k < 4; k++) {
+    if (!p.use[k]) continue;
     const double* U = p.U[k];
     const double ir = 1.0 / U[0];
     const double vx = U[1] * ir, vy = U[2] * ir, q2 = vx * vx + vy * vy;
     const double pr = g1 * (U[3] - 0.5 * U[0] * q2);
-    LuSlot& q = f.s[k];
+    LuSlot& q = f.s[nu];
     q.vx = vx;
     q.vy = vy;
     q.vn = vx * p.nx[k] + vy * p.ny[k];
@@ -2032,16 +2037,17 @@ __global__ void __launch_bounds__(kBlock) k_lusgs_pack_mat(HotView<T> h, SaView<
     q.ny = p.ny[k];
     q.w = p.w[k];
     q.c = SA ? p.w[k] * sa.u[p.j[k]] * ir : 0.0;
-    f.j[k] = p.j[k];
-    f.p[k] = pa[k];
-    use |= p.use[k] ? 1 << k : 0;
+    f.j[nu] = p.j[k];
+    f.p[nu] = pa[k];
+    nu++;
   }
+  for (int k = nu; k < 4; k++) f.s[k] = LuSlot{};
   double add[4] = {0, 0, 0, 0};
   if (!FWD) load4<double>(&inc[p.i * 4], add);
   for (int v = 0; v < 4; v++) f.x0[v] = FWD ? p.base[v] : add[v];
   f.di = p.di;
   f.i = (int32_t)p.i;
-  f.use = use;
+  f.nu = nu;
   if constexpr (SA) {
     LuMatS& r = rec[t];
     r.x0S = FWD ? sa.rhs[p.i] : sa.inc[p.i];
@@ -2052,11 +2058,12 @@ __global__ void __launch_bounds__(kBlock) k_lusgs_pack_mat(HotView<T> h, SaView<
 
 constexpr int kRecBlock = 128;  // threads of the level walk, and records buffered per level
 constexpr int kMatRing = 256;   // (a power of 2) increments of the most recent schedule positions kept in shared memory
+constexpr int kRecStages = 2;   // levels of records in flight: the current one and the next (3 measured no faster)
 constexpr uint32_t kBulkChunk = 16384;
 template <bool SA>
 constexpr size_t mat_smem() {
-  return 16 + sizeof(int32_t) * (kRecMaxLevels + 1) + sizeof(double) * kMatRing * (SA ? 5 : 4) +
-         sizeof(LuMat<SA>) * 2 * kRecBlock;
+  return 32 + sizeof(int32_t) * (kRecMaxLevels + 1) + sizeof(double) * kMatRing * (SA ? 5 : 4) +
+         sizeof(LuMat<SA>) * kRecStages * kRecBlock;
 }
 static_assert(mat_smem<true>() <= 227 * 1024, "level walk fits the shared memory of one block");
 
@@ -2079,32 +2086,43 @@ __device__ __forceinline__ void lusgs_mat_cell(const SaView<T>& sa, const LuMat<
     diS = sd.y;
     bufS = FWD ? x0S : 0.0;
   }
-  const int4 j4 = *reinterpret_cast<const int4*>(f.j), p4 = *reinterpret_cast<const int4*>(f.p);
-  const int32_t ja[4] = {j4.x, j4.y, j4.z, j4.w}, pa[4] = {p4.x, p4.y, p4.z, p4.w};
-  const int use = f.use;
+  const int4 p4 = *reinterpret_cast<const int4*>(f.p);
+  const int32_t pa[4] = {p4.x, p4.y, p4.z, p4.w};
+  const int nu = f.nu;
+  // the neighbours' increments, all ring reads issued together (any position is a valid ring
+  // slot; values past nu are never used); the rare neighbour outside the ring from global memory
+  double dU[4][4], dS[4] = {0, 0, 0, 0};
 #pragma unroll
   for (int q = 0; q < 4; q++) {
-    if (!(use >> q & 1)) continue;
-    const int32_t pj = pa[q];
-    double dU[4], dS = 0.0;
-    if (pj >= 0) {
-      const double2* s = reinterpret_cast<const double2*>(ringF + 4 * (pj & (kMatRing - 1)));
-      const double2 a = s[0], b = s[1];
-      dU[0] = a.x; dU[1] = a.y; dU[2] = b.x; dU[3] = b.y;
-      if constexpr (SA) dS = ringS[pj & (kMatRing - 1)];
-    } else {
-      load4<double>(&inc[(int64_t)ja[q] * 4], dU);
-      if constexpr (SA) dS = sa.inc[ja[q]];
-    }
+    const int r = pa[q] & (kMatRing - 1);
+    const double2* s = reinterpret_cast<const double2*>(ringF + 4 * r);
+    const double2 a = s[0], b = s[1];
+    dU[q][0] = a.x; dU[q][1] = a.y; dU[q][2] = b.x; dU[q][3] = b.y;
+    if constexpr (SA) dS[q] = ringS[r];
+  }
+  if ((pa[0] | pa[1] | pa[2] | pa[3]) < 0) {
+    const int4 j4 = *reinterpret_cast<const int4*>(f.j);
+    const int32_t ja[4] = {j4.x, j4.y, j4.z, j4.w};
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+      if (q < nu && pa[q] < 0) {
+        load4<double>(&inc[(int64_t)ja[q] * 4], dU[q]);
+        if constexpr (SA) dS[q] = sa.inc[ja[q]];
+      }
+  }
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    if (q >= nu) break;
     const double* sl = &f.s[q].vx;
     const double2 vxy = ld2(sl), vnH = ld2(sl + 2), kwl = ld2(sl + 4), nxy = ld2(sl + 6), wc = ld2(sl + 8);
-    const double dmn = nxy.x * dU[1] + nxy.y * dU[2];
-    const double a = dmn - vnH.x * dU[0];
-    const double dp = g1 * (dU[3] - vxy.x * dU[1] - vxy.y * dU[2] + kwl.x * dU[0]);
-    const double dF[4] = {dmn, vnH.x * dU[1] + vxy.x * a + nxy.x * dp, vnH.x * dU[2] + vxy.y * a + nxy.y * dp,
-                          vnH.y * a + vnH.x * (dU[3] + dp)};
-    for (int v = 0; v < 4; v++) buf[v] += wc.x * dF[v] - kwl.y * dU[v];
-    if constexpr (SA) bufS += wc.y * a + (wc.x * vnH.x - kwl.y) * dS;
+    const double* d = dU[q];
+    const double dmn = nxy.x * d[1] + nxy.y * d[2];
+    const double a = dmn - vnH.x * d[0];
+    const double dp = g1 * (d[3] - vxy.x * d[1] - vxy.y * d[2] + kwl.x * d[0]);
+    const double dF[4] = {dmn, vnH.x * d[1] + vxy.x * a + nxy.x * dp, vnH.x * d[2] + vxy.y * a + nxy.y * dp,
+                          vnH.y * a + vnH.x * (d[3] + dp)};
+    for (int v = 0; v < 4; v++) buf[v] += wc.x * dF[v] - kwl.y * d[v];
+    if constexpr (SA) bufS += wc.y * a + (wc.x * vnH.x - kwl.y) * dS[q];
   }
   double o[4];
   for (int v = 0; v < 4; v++) o[v] = FWD ? f.di * buf[v] : x0[v] + f.di * buf[v];
@@ -2135,42 +2153,45 @@ __global__ void __launch_bounds__(mat_threads<SA>()) k_lusgs_levels_mat(SaView<T
   constexpr int NT = kRecBlock;
   extern __shared__ __align__(16) unsigned char smraw[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(smraw);
-  int32_t* so = reinterpret_cast<int32_t*>(smraw + 16);
-  double* ringF = reinterpret_cast<double*>(smraw + 16 + sizeof(int32_t) * (kRecMaxLevels + 1));
+  int32_t* so = reinterpret_cast<int32_t*>(smraw + 32);
+  double* ringF = reinterpret_cast<double*>(smraw + 32 + sizeof(int32_t) * (kRecMaxLevels + 1));
   double* ringS = ringF + 4 * kMatRing;
   R* buf = reinterpret_cast<R*>(ringS + (SA ? kMatRing : 0));
   const int tid = threadIdx.x;
   const bool producer = tid == NT;
   for (int l = tid; l <= nlev; l += blockDim.x) so[l] = (int32_t)off[l];
   if (tid == 0) {
-    mbar_init(smem_u32(&bars[0]), 1);
-    mbar_init(smem_u32(&bars[1]), 1);
+    for (int k = 0; k < kRecStages; k++) mbar_init(smem_u32(&bars[k]), 1);
     fence_mbar_init();
   }
   __syncthreads();
+  // level l uses buffer and mbarrier l % kRecStages, in phase (l / kRecStages) & 1
   auto issue = [&](int l) {  // producer
     const int32_t b = so[l];
     const int32_t n = min(so[l + 1] - b, kRecBlock);
-    const uint32_t bar = smem_u32(&bars[l & 1]), bytes = (uint32_t)(n * sizeof(R));
-    const uint32_t dst = smem_u32(buf + (l & 1) * kRecBlock);
+    const uint32_t bar = smem_u32(&bars[l % kRecStages]), bytes = (uint32_t)(n * sizeof(R));
+    const uint32_t dst = smem_u32(buf + (l % kRecStages) * kRecBlock);
     const char* src = reinterpret_cast<const char*>(rec + b);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     mbar_expect_tx(bar, bytes);
     for (uint32_t o = 0; o < bytes; o += kBulkChunk) bulk_g2s(dst + o, src + o, min(kBulkChunk, bytes - o), bar);
   };
-  if (producer && nlev > 0) issue(0);
+  if (producer)
+    for (int k = 0; k < kRecStages - 1 && k < nlev; k++) issue(k);
   int l = 0;
   bool failed = false;
   int32_t b = so[0], e = nlev > 0 ? so[1] : 0;
   for (; l < nlev; l++) {
-    if (producer && l + 1 < nlev) issue(l + 1);
+    // the buffer of level l + kRecStages - 1 held level l - 1, finished at the last barrier
+    if (producer && l + kRecStages - 1 < nlev) issue(l + kRecStages - 1);
     const int32_t e2 = so[min(l + 2, nlev)];  // the next level's end, read ahead
+    const int stage = l % kRecStages;
     bool ok = true;
     if (tid < NT && b + tid < e) {
-      ok = mbar_wait(smem_u32(&bars[l & 1]), (l >> 1) & 1, kWaitLimit);
+      ok = mbar_wait(smem_u32(&bars[stage]), (l / kRecStages) & 1, kWaitLimit);
       if (ok) {
         // the record from the shared buffer, as a shared-memory reference (ld.shared, not generic loads)
-        lusgs_mat_cell<FWD, SA>(sa, buf[(l & 1) * kRecBlock + tid], b + tid, ringF, ringS, inc, g1);
+        lusgs_mat_cell<FWD, SA>(sa, buf[stage * kRecBlock + tid], b + tid, ringF, ringS, inc, g1);
         for (int32_t t = b + tid + kRecBlock; t < e; t += kRecBlock)
           lusgs_mat_cell<FWD, SA>(sa, rec[t], t, ringF, ringS, inc, g1);
       }
@@ -2182,10 +2203,10 @@ __global__ void __launch_bounds__(mat_threads<SA>()) k_lusgs_levels_mat(SaView<T
     b = e;
     e = e2;
   }
-  if (failed && producer) {  // let the copies in flight land before the block exits
+  if (failed && producer) {  // let the copies in flight (levels l to l + kRecStages - 1) land before the block exits
     atomicOr(flags, kFlagTimeout);
-    mbar_wait(smem_u32(&bars[l & 1]), (l >> 1) & 1, kWaitLimit);
-    if (l + 1 < nlev) mbar_wait(smem_u32(&bars[(l + 1) & 1]), ((l + 1) >> 1) & 1, kWaitLimit);
+    for (int k = l; k < l + kRecStages && k < nlev; k++)
+      mbar_wait(smem_u32(&bars[k % kRecStages]), (k / kRecStages) & 1, kWaitLimit);
   }
 }
 
