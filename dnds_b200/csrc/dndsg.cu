@@ -2072,6 +2072,12 @@ static_assert(mat_smem<true>() <= 227 * 1024, "level walk fits the shared memory
 // overwritten), else (position -1) from global memory.  The sum runs over the slots in the order
 // of lusgs_cell.
 __device__ __forceinline__ double2 ld2(const double* p) { return *reinterpret_cast<const double2*>(p); }
+// the ring holds 32 B per position, two 16-B halves; the halves of every other group of four
+// positions are swapped, so 16-B accesses by 32 consecutive positions spread over all banks
+__device__ __forceinline__ double2* ring_half(double* ringF, int32_t pos, int h) {
+  const int r = pos & (kMatRing - 1);
+  return reinterpret_cast<double2*>(ringF + 4 * r + 2 * (h ^ ((r >> 2) & 1)));
+}
 template <bool FWD, bool SA, class T>
 __device__ __forceinline__ void lusgs_mat_cell(const SaView<T>& sa, const LuMat<SA>& r, int32_t t, double* ringF,
                                                double* ringS, double* inc, double g1) {
@@ -2094,11 +2100,9 @@ __device__ __forceinline__ void lusgs_mat_cell(const SaView<T>& sa, const LuMat<
   double dU[4][4], dS[4] = {0, 0, 0, 0};
 #pragma unroll
   for (int q = 0; q < 4; q++) {
-    const int r = pa[q] & (kMatRing - 1);
-    const double2* s = reinterpret_cast<const double2*>(ringF + 4 * r);
-    const double2 a = s[0], b = s[1];
+    const double2 a = *ring_half(ringF, pa[q], 0), b = *ring_half(ringF, pa[q], 1);
     dU[q][0] = a.x; dU[q][1] = a.y; dU[q][2] = b.x; dU[q][3] = b.y;
-    if constexpr (SA) dS[q] = ringS[r];
+    if constexpr (SA) dS[q] = ringS[pa[q] & (kMatRing - 1)];
   }
   if ((pa[0] | pa[1] | pa[2] | pa[3]) < 0) {
     const int4 j4 = *reinterpret_cast<const int4*>(f.j);
@@ -2127,9 +2131,8 @@ __device__ __forceinline__ void lusgs_mat_cell(const SaView<T>& sa, const LuMat<
   double o[4];
   for (int v = 0; v < 4; v++) o[v] = FWD ? f.di * buf[v] : x0[v] + f.di * buf[v];
   double2* g = reinterpret_cast<double2*>(&inc[(int64_t)f.i * 4]);
-  double2* s = reinterpret_cast<double2*>(ringF + 4 * (t & (kMatRing - 1)));
-  g[0] = s[0] = make_double2(o[0], o[1]);
-  g[1] = s[1] = make_double2(o[2], o[3]);
+  g[0] = *ring_half(ringF, t, 0) = make_double2(o[0], o[1]);
+  g[1] = *ring_half(ringF, t, 1) = make_double2(o[2], o[3]);
   if constexpr (SA) {
     const double oS = FWD ? diS * bufS : x0S + diS * bufS;
     sa.inc[f.i] = oS;
