@@ -2654,10 +2654,21 @@ __global__ void __launch_bounds__(kBlock) k_face_flux_sa(HotView<T> h, SaView<T>
   }
 }
 
+// one thread per (cell, quadrature point): the source's transcendental chain per point is long and
+// one thread per cell left too few warps resident on a 65,536-cell mesh; thread ig == 0 of each cell
+// then sums the points in order (the same sum as a sequential loop over the points)
+constexpr int kSaRhsCells = 32;
 template <class T>
-__global__ void __launch_bounds__(kBlock) k_sa_cell_rhs(HotView<T> h, SaView<T> sa) {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i < h.N) sa_cell_rhs<T>(i, h, sa);
+__global__ void __launch_bounds__(kSaRhsCells * kSaGp) k_sa_cell_rhs(HotView<T> h, SaView<T> sa) {
+  __shared__ double sv[kSaRhsCells * kSaGp], sj[kSaRhsCells * kSaGp];
+  const int64_t i = blockIdx.x * (int64_t)kSaRhsCells + threadIdx.x / kSaGp;
+  const int ig = threadIdx.x % kSaGp;
+  double src = 0, jac = 0;
+  if (i < h.N) sa_cell_point<T>(i, ig, h, sa, src, jac);
+  sv[threadIdx.x] = src;
+  sj[threadIdx.x] = jac;
+  __syncthreads();
+  if (ig == 0 && i < h.N) sa_cell_rhs<T>(i, h, sa, &sv[threadIdx.x], &sj[threadIdx.x]);
 }
 
 template <class T>
@@ -2761,7 +2772,7 @@ void run_rhs_sa(dndsg_ctx* c, cudaStream_t s) {
     if (F > Fi) k_face_flux_sa<T, 1, true><<<grid_for(F - Fi), kBlock, 0, s>>>(h, sa, Fi, F, c->flags, c->nreduced);
   }
   k_cell_update<T, -1><<<grid_for(c->N), kBlock, 0, s>>>(h, c->scal);
-  k_sa_cell_rhs<T><<<grid_for(c->N), kBlock, 0, s>>>(h, sa);
+  k_sa_cell_rhs<T><<<(unsigned)((c->N + kSaRhsCells - 1) / kSaRhsCells), kSaRhsCells * kSaGp, 0, s>>>(h, sa);
 }
 
 template <class T>

@@ -350,10 +350,43 @@ DG_HD void sa_source_point(const HotView<T>& h, const double U[4], double U5, co
   jac = -dmin(U[0] * (P * 0 - D * 2) / muRef / (U5 + 1e-200), -1e-200);
 }
 
-// U5 rhs of cell i: the face fluxes, the flux-balance term -U5_i (v_i . closure_i) / V_i, and the
-// source integrated over the cell quadrature; the source Jacobian into srcJac
+// the SA source and its Jacobian at cell quadrature point ig of cell i, times the point's weight
+// (0 for the zero-weight padding of a triangle's 4 points)
 template <class T>
-DG_HD void sa_cell_rhs(int64_t i, const HotView<T>& h, const SaView<T>& sa) {
+DG_HD void sa_cell_point(int64_t i, int ig, const HotView<T>& h, const SaView<T>& sa, double& src, double& jac) {
+  src = jac = 0;
+  const double* gp = &sa.cellGp[(i * kSaGp + ig) * kSaGpE];
+  const double wdet = gp[0];
+  if (wdet == 0.0) return;
+  double U[4];
+  load4<T>(&h.u[i * 4], U);
+  const T* rc = &h.urec[i * 20];
+  const T* rs = &sa.urec[i * 5];
+  double inc[4] = {0, 0, 0, 0}, G[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}}, incS = 0, gS[2] = {0, 0};
+  for (int q = 0; q < 5; q++) {
+    const double b0 = gp[1 + q], bx = gp[6 + q], by = gp[11 + q];
+    for (int v = 0; v < 4; v++) {
+      const double a = (double)rc[4 * q + v];
+      inc[v] += b0 * a; G[0][v] += bx * a; G[1][v] += by * a;
+    }
+    const double a = (double)rs[q];
+    incS += b0 * a; gS[0] += bx * a; gS[1] += by * a;
+  }
+  double Ug[4];
+  const double u5 = sa.u[i];
+  const bool comp = compress_rec_part(U, inc, Ug);
+  const double U5g = comp ? u5 : u5 + incS;
+  double s, j;
+  sa_source_point(h, Ug, U5g, G, gS, sa.dWall[i], s, j);
+  src = s * wdet;
+  jac = j * wdet;
+}
+
+// U5 rhs of cell i: the face fluxes, the flux-balance term -U5_i (v_i . closure_i) / V_i, and the
+// source integrated over the cell quadrature (src / jac: the kSaGp weighted point values, summed in
+// point order); the source Jacobian into srcJac
+template <class T>
+DG_HD void sa_cell_rhs(int64_t i, const HotView<T>& h, const SaView<T>& sa, const double* src, const double* jac) {
   double s = 0;
   for (int k = 0; k < h.nfmax; k++) {
     const int32_t sf = h.cellFace[aos(i, k, h.nfmax)];
@@ -365,31 +398,10 @@ DG_HD void sa_cell_rhs(int64_t i, const HotView<T>& h, const SaView<T>& sa) {
   const double u5 = sa.u[i];
   const double vn = (U[1] * h.closure[2 * i] + U[2] * h.closure[2 * i + 1]) / U[0];
   double r = (s - u5 * vn) / h.vol[i];
-  // source over the cell quadrature
-  const T* rc = &h.urec[i * 20];
-  const T* rs = &sa.urec[i * 5];
   double sv = 0, sj = 0;
   for (int ig = 0; ig < kSaGp; ig++) {
-    const double* gp = &sa.cellGp[(i * kSaGp + ig) * kSaGpE];
-    const double wdet = gp[0];
-    if (wdet == 0.0) continue;
-    double inc[4] = {0, 0, 0, 0}, G[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}}, incS = 0, gS[2] = {0, 0};
-    for (int q = 0; q < 5; q++) {
-      const double b0 = gp[1 + q], bx = gp[6 + q], by = gp[11 + q];
-      for (int v = 0; v < 4; v++) {
-        const double a = (double)rc[4 * q + v];
-        inc[v] += b0 * a; G[0][v] += bx * a; G[1][v] += by * a;
-      }
-      const double a = (double)rs[q];
-      incS += b0 * a; gS[0] += bx * a; gS[1] += by * a;
-    }
-    double Ug[4];
-    const bool comp = compress_rec_part(U, inc, Ug);
-    const double U5g = comp ? u5 : u5 + incS;
-    double src, jac;
-    sa_source_point(h, Ug, U5g, G, gS, sa.dWall[i], src, jac);
-    sv += src * wdet;
-    sj += jac * wdet;
+    sv += src[ig];
+    sj += jac[ig];
   }
   sa.rhs[i] = r + sv / h.vol[i];
   sa.srcJac[i] = sj / h.vol[i];
