@@ -2632,19 +2632,36 @@ __global__ void __launch_bounds__(kBlock) k_sa_vr(HotView<T> h, SaView<T> sa) {
   if (i < h.N) sa_vr_cell<T>(i, h, sa);
 }
 
+// one thread per (face, Gauss point), as for the cell source: three times the resident warps for the
+// long per-point chain (Roe, gradients, viscous and U5 fluxes).  Thread g == 0 of each face sums the
+// points in order.
+constexpr int kSaFluxFaces = 64;
+inline unsigned sa_flux_grid(int64_t n) { return (unsigned)((n + kSaFluxFaces - 1) / kSaFluxFaces); }
 template <class T, int RIEMANN, bool BND>
-__global__ void __launch_bounds__(kBlock) k_face_flux_sa(HotView<T> h, SaView<T> sa, int64_t f0, int64_t f1,
-                                                         unsigned* flags, unsigned long long* nred) {
-  const int64_t f = f0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(kSaFluxFaces * 3) k_face_flux_sa(HotView<T> h, SaView<T> sa, int64_t f0, int64_t f1,
+                                                                   unsigned* flags, unsigned long long* nred) {
+  __shared__ double part[kSaFluxFaces * 3][5];
+  const int64_t f = f0 + blockIdx.x * (int64_t)kSaFluxFaces + threadIdx.x / 3;
+  const int g = threadIdx.x % 3;
   int r = 0;
   bool bad = false;
   if (f < f1) {
-    double out[4], outS;
-    r = face_flux_sa<T, RIEMANN, BND>(f, h, sa, out, outS, bad);
+    double c[4], cS;
+    r = face_flux_sa_point<T, RIEMANN, BND>(f, g, h, sa, c, cS, bad);
+    for (int k = 0; k < 4; k++) part[threadIdx.x][k] = c[k];
+    part[threadIdx.x][4] = cS;
+  }
+  __syncthreads();
+  if (f < f1 && g == 0) {
+    double acc[5] = {0, 0, 0, 0, 0};
+    for (int q = 0; q < 3; q++)
+      for (int k = 0; k < 5; k++) acc[k] -= part[threadIdx.x + q][k];
+    for (int k = 0; k < 5; k++)
+      if (!(acc[k] == acc[k])) bad = true;
     double* o = &h.flux[f * 4];
-    *reinterpret_cast<double2*>(o) = make_double2(out[0], out[1]);
-    *reinterpret_cast<double2*>(o + 2) = make_double2(out[2], out[3]);
-    sa.flux[f] = outS;
+    *reinterpret_cast<double2*>(o) = make_double2(acc[0], acc[1]);
+    *reinterpret_cast<double2*>(o + 2) = make_double2(acc[2], acc[3]);
+    sa.flux[f] = acc[4];
   }
   unsigned anyBad = __ballot_sync(0xffffffffu, bad);
   int rs = __reduce_add_sync(0xffffffffu, r);
@@ -2765,11 +2782,11 @@ void run_rhs_sa(dndsg_ctx* c, cudaStream_t s) {
   SaView<T> sa = sa_view<T>(c);
   const int64_t Fi = c->Fi, F = c->F;
   if (c->s.riemann == 2) {
-    if (Fi > 0) k_face_flux_sa<T, 2, false><<<grid_for(Fi), kBlock, 0, s>>>(h, sa, 0, Fi, c->flags, c->nreduced);
-    if (F > Fi) k_face_flux_sa<T, 2, true><<<grid_for(F - Fi), kBlock, 0, s>>>(h, sa, Fi, F, c->flags, c->nreduced);
+    if (Fi > 0) k_face_flux_sa<T, 2, false><<<sa_flux_grid(Fi), kSaFluxFaces * 3, 0, s>>>(h, sa, 0, Fi, c->flags, c->nreduced);
+    if (F > Fi) k_face_flux_sa<T, 2, true><<<sa_flux_grid(F - Fi), kSaFluxFaces * 3, 0, s>>>(h, sa, Fi, F, c->flags, c->nreduced);
   } else {
-    if (Fi > 0) k_face_flux_sa<T, 1, false><<<grid_for(Fi), kBlock, 0, s>>>(h, sa, 0, Fi, c->flags, c->nreduced);
-    if (F > Fi) k_face_flux_sa<T, 1, true><<<grid_for(F - Fi), kBlock, 0, s>>>(h, sa, Fi, F, c->flags, c->nreduced);
+    if (Fi > 0) k_face_flux_sa<T, 1, false><<<sa_flux_grid(Fi), kSaFluxFaces * 3, 0, s>>>(h, sa, 0, Fi, c->flags, c->nreduced);
+    if (F > Fi) k_face_flux_sa<T, 1, true><<<sa_flux_grid(F - Fi), kSaFluxFaces * 3, 0, s>>>(h, sa, Fi, F, c->flags, c->nreduced);
   }
   k_cell_update<T, -1><<<grid_for(c->N), kBlock, 0, s>>>(h, c->scal);
   k_sa_cell_rhs<T><<<(unsigned)((c->N + kSaRhsCells - 1) / kSaRhsCells), kSaRhsCells * kSaGp, 0, s>>>(h, sa);

@@ -209,10 +209,35 @@ DG_HD void sa_point(const HotView<T>& h, const SaView<T>& sa, int64_t f, int g, 
   }
 }
 
-// face flux of an SA context: the flow flux with the eddy viscosity and the U5 transport and
-// diffusion (fluxFace, DNDS_FV_EulerEvaluator.hpp:371-591, SA branches)
+// the reconstruction increments of both cells at face Gauss point g (face_increments for one point,
+// the same sums)
+template <class T>
+DG_HD void face_increment_point(int64_t f, int g, int32_t L, int32_t R, const HotView<T>& h, T incL[4], T incR[4]) {
+  for (int v = 0; v < 4; v++) incL[v] = incR[v] = T(0);
+  const T* rl = &h.urec[(int64_t)L * 20];
+  for (int q = 0; q < 5; q++) {
+    const T phi = h.faceBasis[aos(f, g * 5 + q, 30)];
+    T row[4];
+    load_row(rl + 4 * q, row);
+    for (int v = 0; v < 4; v++) incL[v] += phi * row[v];
+  }
+  if (R >= 0) {
+    const T* rr = &h.urec[(int64_t)R * 20];
+    for (int q = 0; q < 5; q++) {
+      const T phi = h.faceBasis[aos(f, 15 + g * 5 + q, 30)];
+      T row[4];
+      load_row(rr + 4 * q, row);
+      for (int v = 0; v < 4; v++) incR[v] += phi * row[v];
+    }
+  }
+}
+
+// face flux of an SA context at Gauss point g: the flow flux with the eddy viscosity and the U5
+// transport and diffusion (fluxFace, DNDS_FV_EulerEvaluator.hpp:371-591, SA branches), weighted;
+// the face flux is minus the sum of the three points' c / cS in point order
 template <class T, int RIEMANN, bool BND>
-DG_HD int face_flux_sa(int64_t f, const HotView<T>& h, const SaView<T>& sa, double out[4], double& outS, bool& bad) {
+DG_HD int face_flux_sa_point(int64_t f, int g, const HotView<T>& h, const SaView<T>& sa, double c[4], double& cS,
+                             bool& bad) {
   const int32_t L = h.faceL[f], R = h.faceR[f];
   const double nx = h.faceNormal[2 * f], ny = h.faceNormal[2 * f + 1], area = h.faceArea[f];
   double uL[4], uR[4] = {0, 0, 0, 0};
@@ -226,13 +251,12 @@ DG_HD int face_flux_sa(int64_t f, const HotView<T>& h, const SaView<T>& sa, doub
   const double invD = wall ? 0.0 : area / (2.0 * minVol);
   const double dl = h.dLam[f];
   const double muRef = h.mu;
-  T incL[3][4], incR[3][4];
-  face_increments(f, L, R, h, incL, incR);
+  T incL[4], incR[4];
+  face_increment_point(f, g, L, inner ? R : -1, h, incL, incR);
   int nred = 0;
-  double acc[4] = {0, 0, 0, 0}, accS = 0;
-  for (int g = 0; g < 3; g++) {
+  {
     double UL[4], UR[4], a[4], b[4], F[4], sL, sR;
-    sa_point(h, sa, f, g, L, R, inner, uL, uR, incL[g], incR[g], UL, UR, sL, sR, nred);
+    sa_point(h, sa, f, g, L, R, inner, uL, uR, incL, incR, UL, UR, sL, sR, nred);
     to_normal_frame(UL, nx, ny, a);
     to_normal_frame(UR, nx, ny, b);
     if (!(a[0] > 0 && b[0] > 0)) bad = true;
@@ -286,15 +310,9 @@ DG_HD int face_flux_sa(int64_t f, const HotView<T>& h, const SaView<T>& sa, doub
       FvS += gn[d] * diffNu * (mufPhy + Sm * muRef * fn) / (2. / 3.) / muRef;
     }
     const double jw = 0.5 * area * l3_weight(g);
-    for (int k = 0; k < 4; k++) acc[k] -= (F[k] - Fv[k]) * jw;
-    accS -= (FS - FvS) * jw;
+    for (int k = 0; k < 4; k++) c[k] = (F[k] - Fv[k]) * jw;
+    cS = (FS - FvS) * jw;
   }
-  for (int k = 0; k < 4; k++) {
-    if (!(acc[k] == acc[k])) bad = true;
-    out[k] = acc[k];
-  }
-  if (!(accS == accS)) bad = true;
-  outS = accS;
   return nred;
 }
 
