@@ -283,6 +283,71 @@ def steady_leg(dev, iters=1000, log=None):
     return out
 
 
+# algorithmic bytes per triangle cell of one ReconstructionWBAPLimitFacialV3 pass that limits every cell:
+# coefficients read 20s and written 20s, means 32 B, the indicator's face basis rows (1.5 faces x 2 sides
+# x 6 x 5 s) and the neighbour mapping matrices (1.5 faces x 2 sides x 25 s): 205s + 32 B
+WBAP_BYTES_PER_CELL = {4: 205 * 4 + 32, 8: 205 * 8 + 32}
+
+
+def riemann_leg(dev, steps=20, grid=2048, log=None):
+    """The four-quadrant 2-D Riemann problem at its configured size (2048 x 2048 quads on [0,1]^2,
+    interior nodes jittered by U(-0.15h, 0.15h), seed 4321, split into 8,388,608 triangles; P2 VR,
+    CWBAP limiter, HLLC, SSP-RK3 at CFL 0.4 towards t = 0.3): cell-RK-stage updates/s in FP32 bulk and
+    FP64, and the limiter alone (ReconstructionWBAPLimitFacialV3) with the smooth-indicator gate and
+    with every cell limited, against its algorithmic bytes.  Timed outside the headline."""
+    import torch
+
+    from dnds_b200 import geometry as G
+    from dnds_b200 import mesh as M
+    from dnds_b200 import settings as S
+    from dnds_b200.solver import Solver
+
+    m = M.riemann_mesh(grid)
+    cfg = S.preset("riemann")
+    u0 = G.quadrant_states(m, S.RIEMANN_2D_STATES)
+    peak, peak_kind = measured_peak()
+    out = {"workload": f"2-D Riemann, [0,1]^2, {grid}x{grid} jittered quads -> {m.n_cells:,} triangles, P2 VR + "
+                       "CWBAP + HLLC, SSP-RK3 CFL 0.4", "cells": m.n_cells, "steps": steps}
+    ev = lambda: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))  # noqa: E731
+    for prec, name in ((1, "fp32"), (0, "fp64")):
+        s = Solver(m, cfg, device=dev, precision=prec)
+        s.set_u(u0)
+        for _ in range(3):
+            s.ssprk3_step(0.4, 0.3)
+        e0, e1 = ev()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(steps):
+            s.ssprk3_step(0.4, 0.3)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        r = {"ms_per_step": ms, "value": m.n_cells * 3 / (ms * 1e-3), "unit": UNIT, "t": s.time}
+        nk = 10
+        for if_all, key in ((False, "limiter_ms"), (True, "limiter_all_cells_ms")):
+            e0, e1 = ev()
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(nk):
+                s.ReconstructionWBAPLimitFacialV3(if_all)
+            e1.record()
+            torch.cuda.synchronize()
+            r[key] = e0.elapsed_time(e1) / nk
+        sz = 4 if prec == 1 else 8
+        ach = WBAP_BYTES_PER_CELL[sz] * m.n_cells / (r["limiter_all_cells_ms"] * 1e-3) / 1e9
+        r["limiter_roofline"] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                                 "peak_kind": f"{peak_kind} hbm_gbs", "alg_bytes_per_cell": WBAP_BYTES_PER_CELL[sz]}
+        flags, nred = s.status()
+        r["flags"] = flags
+        r["reduced_order_points"] = nred
+        out[name] = r
+        s.close()
+        if log:
+            log(name, r)
+    out["speedup_fp32_over_fp64"] = out["fp64"]["ms_per_step"] / out["fp32"]["ms_per_step"]
+    return out
+
+
 def learned_leg(dev, grid, tol=1e-7, log=None):
     """The learned VR warm start: harvest on two 256 x 256 x 2 vortex meshes, train on the GPU,
     then Jacobi sweeps per SSP-RK3 step to the same rms-increment tolerance, with and without the
@@ -369,6 +434,8 @@ def main():
     ap.add_argument("--precisions", default="fp32,fp64")
     ap.add_argument("--no-steady", action="store_true", help="skip the implicit steady RANS-SA NACA 0012 report")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start report")
+    ap.add_argument("--no-riemann", action="store_true", help="skip the 8.4M-triangle Riemann / CWBAP report")
+    ap.add_argument("--riemann-grid", type=int, default=2048, help="grid size of the Riemann / CWBAP report")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -523,6 +590,8 @@ def main():
         out["cpu_baseline"] = cpu_baseline()
     if rank == 0 and ws == 1 and not args.no_steady:
         out["steady_naca0012_sa"] = steady_leg(dev)
+    if rank == 0 and ws == 1 and not args.no_riemann:
+        out["riemann_cwbap"] = riemann_leg(dev, grid=args.riemann_grid)
     if rank == 0 and ws == 1 and not args.no_learned:
         out["learned_vr"] = learned_leg(dev, args.grid)
     if rank == 0:

@@ -55,6 +55,8 @@ struct dndsg_ctx {
   void *saUrec = nullptr, *saUrecNew = nullptr;  // T [N][5]
   double* Ainv = nullptr;
   double *limFace = nullptr, *faceInd = nullptr, *indicator = nullptr;  // CWBAP limiter data
+  int32_t *limList = nullptr, *limCount = nullptr;  // cells the limiter pass limits, and their number
+  int sms = 0;                                      // multiprocessors of the device (queried on first use)
   int32_t* wallCells = nullptr;  // cells with a Wall_Euler / Wall_NoSlip face
   float* mlpGeom = nullptr;  // [N][8] slot face centres in each cell's polynomial frame
   void *mlpM = nullptr, *mlpA = nullptr, *mlpB = nullptr, *mlpH = nullptr;  // learned warm start work (T)
@@ -286,18 +288,44 @@ __global__ void k_setup_limiter(MeshView m, SetupParams p, const CellSetup* cell
   if (f < m.F && !setup_limiter_face(f, m, p, cells, faceW, lim)) atomicOr(bad, 4);
 }
 template <class T>
-__global__ void k_lim_face(LimView v, const T* urec) {
+__global__ void k_lim_face(LimView v, const T* urec, int32_t* count) {
   int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (f == 0) *count = 0;  // the list of cells to limit, filled by the next launch
   if (f < v.F) limiter_face_indicator<T>(f, v, urec);
 }
-__global__ void k_lim_cell_indicator(LimView v) {
-  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i < v.N) v.indicator[i] = limiter_cell_indicator(i, v);
-}
+// the indicator of every cell; a cell with si >= scale (or every cell, ifAll) is appended to the
+// list (order of the list is immaterial: each cell's result depends on the unlimited data only),
+// the others copy their coefficients to out
 template <class T>
-__global__ void __launch_bounds__(kBlock) k_lim_apply(LimView v, const T* urec, T* out) {
-  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i < v.N) limiter_cell<T>(i, v, urec, out);
+__global__ void __launch_bounds__(kBlock) k_lim_cell_indicator(LimView v, const T* urec, T* out, int32_t* list,
+                                                               int32_t* count) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  bool lim = false;
+  if (i < v.N) {
+    const double ind = limiter_cell_indicator(i, v);
+    v.indicator[i] = ind;
+    lim = !(ind < v.scale) || v.ifAll;
+    if (!lim) {
+      constexpr int W = 16 / sizeof(T);  // elements per 16-byte vector
+      const int4* src = reinterpret_cast<const int4*>(urec + i * 20);
+      int4* dst = reinterpret_cast<int4*>(out + i * 20);
+      for (int k = 0; k < 20 / W; k++) dst[k] = src[k];
+    }
+  }
+  const unsigned b = __ballot_sync(0xffffffffu, lim);
+  const int lane = threadIdx.x & 31;
+  int base = 0;
+  if (lane == 0 && b) base = atomicAdd(count, __popc(b));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (lim) list[base + __popc(b & ((1u << lane) - 1))] = (int32_t)i;
+}
+// the listed cells, one thread each (limiter_cell), in a grid-stride loop
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_lim_apply(LimView v, const T* urec, T* out, const int32_t* list,
+                                                      const int32_t* count) {
+  const int64_t n = *count;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+    limiter_cell<T>(list[t], v, urec, out);
 }
 
 
@@ -565,9 +593,12 @@ LimView lim_view(dndsg_ctx* c, int ifAll) {
 template <class T>
 void run_limiter(dndsg_ctx* c, int ifAll, cudaStream_t s) {
   LimView v = lim_view(c, ifAll);
-  k_lim_face<T><<<grid_for(c->F), kBlock, 0, s>>>(v, (const T*)c->urec);
-  k_lim_cell_indicator<<<grid_for(c->N), kBlock, 0, s>>>(v);
-  k_lim_apply<T><<<grid_for(c->N), kBlock, 0, s>>>(v, (const T*)c->urec, (T*)c->urecNew);
+  k_lim_face<T><<<grid_for(c->F), kBlock, 0, s>>>(v, (const T*)c->urec, c->limCount);
+  k_lim_cell_indicator<T><<<grid_for(c->N), kBlock, 0, s>>>(v, (const T*)c->urec, (T*)c->urecNew, c->limList,
+                                                          c->limCount);
+  if (!c->sms && cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess) c->sms = 148;
+  k_lim_apply<T><<<(unsigned)std::min<int64_t>(grid_for(c->N), 4 * c->sms), kBlock, 0, s>>>(
+      v, (const T*)c->urec, (T*)c->urecNew, c->limList, c->limCount);
   std::swap(c->urec, c->urecNew);
 }
 
@@ -821,6 +852,7 @@ int setup_run(dndsg_ctx* c, const dndsg_mesh_desc* md) {
     if ((rc = dalloc(c, c->limFace, sizeof(double) * aos_size(F, kLimE)))) return rc;
     if ((rc = dalloc(c, c->faceInd, sizeof(double) * 4 * F))) return rc;
     if ((rc = dalloc(c, c->indicator, sizeof(double) * N))) return rc;
+    if ((rc = dalloc(c, c->limList, sizeof(int32_t) * N)) || (rc = dalloc(c, c->limCount, sizeof(int32_t)))) return rc;
     k_setup_limiter<<<grid_for(F), kBlock>>>(m, p, cells, faceW, c->limFace, dBad);
     if ((rc = check_launch(c))) return rc;
   }

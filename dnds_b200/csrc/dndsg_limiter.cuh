@@ -3,14 +3,16 @@
 // DNDS_FV_Limiters.hpp:341-449 and the characteristic matrices fML/fMR of
 // DNDS_FV_EulerSolver.hpp:749-795.  Arithmetic in FP64 for both storage precisions.
 //
-// Three passes, each one thread per item:
+// Three passes:
 //   face:  smoothness-indicator integrals IJI, ISI of rho and E at the face's
 //          first gauss point (the reference integrates with LINE_1 weight 2 but
-//          reads the LINE_3 data of point 0);
-//   cell:  indicator si = sqrt(max_k IJI_k / ISI_k) * P^2 (P = 2);
-//   cell:  for limited cells, order-by-order (P2 rows 2..4, then P1 rows 0..1)
-//          biway WBAP against each neighbour in characteristic space and a
-//          multiway WBAP of the results; other cells copy their coefficients.
+//          reads the LINE_3 data of point 0), one thread per face;
+//   cell:  indicator si = sqrt(max_k IJI_k / ISI_k) * P^2 (P = 2), one thread per
+//          cell, which lists the cells to limit and copies the coefficients of
+//          the others;
+//   limit: one thread per listed cell, order-by-order (P2 rows 2..4, then P1
+//          rows 0..1) biway WBAP against each neighbour in characteristic space
+//          and a multiway WBAP of the results.
 #pragma once
 #include "dndsg_bodies.cuh"
 
