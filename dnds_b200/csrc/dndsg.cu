@@ -56,6 +56,7 @@ struct dndsg_ctx {
   double* Ainv = nullptr;
   double *limFace = nullptr, *faceInd = nullptr, *indicator = nullptr;  // CWBAP limiter data
   int32_t *limList = nullptr, *limCount = nullptr;  // cells the limiter pass limits, and their number
+  float* limD32 = nullptr;                          // FP32 bulk: limFace elements [0, kLimDE) in FP32
   int sms = 0;                                      // multiprocessors of the device (queried on first use)
   int32_t* wallCells = nullptr;  // cells with a Wall_Euler / Wall_NoSlip face
   float* mlpGeom = nullptr;  // [N][8] slot face centres in each cell's polynomial frame
@@ -287,6 +288,11 @@ __global__ void k_setup_limiter(MeshView m, SetupParams p, const CellSetup* cell
   int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (f < m.F && !setup_limiter_face(f, m, p, cells, faceW, lim)) atomicOr(bad, 4);
 }
+__global__ void k_lim_d32(const double* limFace, int64_t F, float* d32) {
+  const int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (f < F)
+    for (int e = 0; e < kLimDE; e++) d32[aos(f, e, kLimDE)] = (float)limFace[aos(f, e, kLimE)];
+}
 template <class T>
 __global__ void k_lim_face(LimView v, const T* urec, int32_t* count) {
   int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -294,23 +300,14 @@ __global__ void k_lim_face(LimView v, const T* urec, int32_t* count) {
   if (f < v.F) limiter_face_indicator<T>(f, v, urec);
 }
 // the indicator of every cell; a cell with si >= scale (or every cell, ifAll) is appended to the
-// list (order of the list is immaterial: each cell's result depends on the unlimited data only),
-// the others copy their coefficients to out
-template <class T>
-__global__ void __launch_bounds__(kBlock) k_lim_cell_indicator(LimView v, const T* urec, T* out, int32_t* list,
-                                                               int32_t* count) {
+// list (order of the list is immaterial: each cell's result depends on the unlimited data only)
+__global__ void __launch_bounds__(kBlock) k_lim_cell_indicator(LimView v, int32_t* list, int32_t* count) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   bool lim = false;
   if (i < v.N) {
     const double ind = limiter_cell_indicator(i, v);
     v.indicator[i] = ind;
     lim = !(ind < v.scale) || v.ifAll;
-    if (!lim) {
-      constexpr int W = 16 / sizeof(T);  // elements per 16-byte vector
-      const int4* src = reinterpret_cast<const int4*>(urec + i * 20);
-      int4* dst = reinterpret_cast<int4*>(out + i * 20);
-      for (int k = 0; k < 20 / W; k++) dst[k] = src[k];
-    }
   }
   const unsigned b = __ballot_sync(0xffffffffu, lim);
   const int lane = threadIdx.x & 31;
@@ -319,15 +316,25 @@ __global__ void __launch_bounds__(kBlock) k_lim_cell_indicator(LimView v, const 
   base = __shfl_sync(0xffffffffu, base, 0);
   if (lim) list[base + __popc(b & ((1u << lane) - 1))] = (int32_t)i;
 }
-// the listed cells, one thread each (limiter_cell), in a grid-stride loop
+// the listed cells, one thread each (limiter_cell), into buf[t] for list entry t; a grid-stride loop
 template <class T>
-__global__ void __launch_bounds__(kBlock) k_lim_apply(LimView v, const T* urec, T* out, const int32_t* list,
+__global__ void __launch_bounds__(kBlock) k_lim_apply(LimView v, const T* urec, T* buf, const int32_t* list,
                                                       const int32_t* count) {
   const int64_t n = *count;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
-    limiter_cell<T>(list[t], v, urec, out);
+    limiter_cell<T>(list[t], v, urec, buf + t * 20);
 }
-
+// the limited coefficients back over the listed cells' ones, 16 bytes per thread
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_lim_scatter(T* urec, const T* buf, const int32_t* list,
+                                                        const int32_t* count) {
+  constexpr int W = 16 / sizeof(T), V = 20 / W;  // elements per vector, vectors per cell
+  const int64_t n = (int64_t)*count * V;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t t = e / V, k = e - t * V;
+    reinterpret_cast<int4*>(urec + (int64_t)list[t] * 20)[k] = reinterpret_cast<const int4*>(buf + t * 20)[k];
+  }
+}
 
 __device__ __forceinline__ double stage_time(const double* scal, int useDev, double tHost, double c) {
   return useDev ? scal[S_T] + c * scal[S_DT] : tHost;
@@ -580,7 +587,7 @@ LimView lim_view(dndsg_ctx* c, int ifAll) {
   LimView v;
   v.N = c->N; v.F = c->F; v.Fi = c->Fi; v.nfmax = c->nfmax;
   v.cellFace = c->cellFace; v.faceL = c->faceL; v.faceR = c->faceR;
-  v.faceNormal = c->faceNormal; v.faceArea = c->faceArea; v.limFace = c->limFace;
+  v.faceNormal = c->faceNormal; v.faceArea = c->faceArea; v.limFace = c->limFace; v.limD32 = c->limD32;
   v.u = c->u; v.faceInd = c->faceInd; v.indicator = c->indicator;
   v.gamma = c->s.gamma; v.tangWeight = c->s.tang_weight; v.tangModMin = c->s.tang_weight_mod_min;
   v.tangModPower = c->s.tang_weight_mod_power; v.tangModLoc = c->s.tang_weight_mod_loc; v.vol = c->vol;
@@ -594,12 +601,12 @@ template <class T>
 void run_limiter(dndsg_ctx* c, int ifAll, cudaStream_t s) {
   LimView v = lim_view(c, ifAll);
   k_lim_face<T><<<grid_for(c->F), kBlock, 0, s>>>(v, (const T*)c->urec, c->limCount);
-  k_lim_cell_indicator<T><<<grid_for(c->N), kBlock, 0, s>>>(v, (const T*)c->urec, (T*)c->urecNew, c->limList,
-                                                          c->limCount);
+  k_lim_cell_indicator<<<grid_for(c->N), kBlock, 0, s>>>(v, c->limList, c->limCount);
+  // urecNew (the previous sweep's coefficients, free until the next sweep) holds the limited ones
   if (!c->sms && cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess) c->sms = 148;
-  k_lim_apply<T><<<(unsigned)std::min<int64_t>(grid_for(c->N), 4 * c->sms), kBlock, 0, s>>>(
-      v, (const T*)c->urec, (T*)c->urecNew, c->limList, c->limCount);
-  std::swap(c->urec, c->urecNew);
+  const unsigned g = (unsigned)std::min<int64_t>(grid_for(c->N), 4 * c->sms);
+  k_lim_apply<T><<<g, kBlock, 0, s>>>(v, (const T*)c->urec, (T*)c->urecNew, c->limList, c->limCount);
+  k_lim_scatter<T><<<g, kBlock, 0, s>>>((T*)c->urec, (const T*)c->urecNew, c->limList, c->limCount);
 }
 
 template <class T>
@@ -855,6 +862,11 @@ int setup_run(dndsg_ctx* c, const dndsg_mesh_desc* md) {
     if ((rc = dalloc(c, c->limList, sizeof(int32_t) * N)) || (rc = dalloc(c, c->limCount, sizeof(int32_t)))) return rc;
     k_setup_limiter<<<grid_for(F), kBlock>>>(m, p, cells, faceW, c->limFace, dBad);
     if ((rc = check_launch(c))) return rc;
+    if (sizeof(T) == 4) {  // FP32 bulk: the indicator's basis derivatives and weights in FP32
+      if ((rc = dalloc(c, c->limD32, sizeof(float) * aos_size(F, kLimDE)))) return rc;
+      k_lim_d32<<<grid_for(F), kBlock>>>(c->limFace, F, c->limD32);
+      if ((rc = check_launch(c))) return rc;
+    }
   }
   DG_CUDA(c, cudaDeviceSynchronize());
   int bad = 0;

@@ -8,11 +8,12 @@
 //          first gauss point (the reference integrates with LINE_1 weight 2 but
 //          reads the LINE_3 data of point 0), one thread per face;
 //   cell:  indicator si = sqrt(max_k IJI_k / ISI_k) * P^2 (P = 2), one thread per
-//          cell, which lists the cells to limit and copies the coefficients of
-//          the others;
+//          cell, which lists the cells to limit;
 //   limit: one thread per listed cell, order-by-order (P2 rows 2..4, then P1
 //          rows 0..1) biway WBAP against each neighbour in characteristic space
-//          and a multiway WBAP of the results.
+//          and a multiway WBAP of the results, into a compact buffer that a last
+//          pass scatters back over the listed cells' coefficients (the others
+//          keep theirs: nothing is copied).
 #pragma once
 #include "dndsg_bodies.cuh"
 
@@ -24,6 +25,7 @@ namespace dg {
 //   [66, 91)  msR2L (right-cell coefficients -> left basis), row-major
 //   [91, 116) msL2R
 constexpr int kLimE = 116;
+constexpr int kLimDE = 66;  // the elements the indicator reads (D at gauss point 0, face weights)
 
 struct LimView {
   int64_t N, F, Fi;
@@ -34,6 +36,7 @@ struct LimView {
   const double* faceNormal;
   const double* faceArea;
   const double* limFace;   // AoSoA kLimE
+  const float* limD32;     // FP32 bulk contexts: its elements [0, kLimDE) in FP32, AoSoA kLimDE
   const double* u;
   double* faceInd;         // [F][4]: IJI_rho, IJI_E, ISI_rho, ISI_E
   double* indicator;       // [N]
@@ -80,6 +83,12 @@ DG_HD bool setup_limiter_face(int64_t f, const MeshView& m, const SetupParams& p
 // face pass of the smoothness indicator (DNDS_FV_VR.hpp:2075-2127)
 template <class T>
 DG_HD void limiter_face_indicator(int64_t f, const LimView& v, const T* urec) {
+  // element e of the face's indicator data: FP32 bulk contexts read the FP32 copy (half the bytes of
+  // the kernel's largest stream), FP64 contexts the FP64 table
+  auto D = [&](int e) -> double {
+    if constexpr (sizeof(T) == 4) return (double)v.limD32[aos(f, e, kLimDE)];
+    else return v.limFace[aos(f, e, kLimE)];
+  };
   int32_t L = v.faceL[f], R = v.faceR[f];
   double* out = &v.faceInd[f * 4];
   if (R < 0) { out[0] = out[1] = out[2] = out[3] = 0; return; }
@@ -94,8 +103,8 @@ DG_HD void limiter_face_indicator(int64_t f, const LimView& v, const T* urec) {
     for (int d = 0; d < 6; d++) {
       double sL = 0, sR = 0;
       for (int q = 0; q < 5; q++) {
-        sL += v.limFace[aos(f, d * 5 + q, kLimE)] * rl[q];
-        sR += v.limFace[aos(f, 30 + d * 5 + q, kLimE)] * rr[q];
+        sL += D(d * 5 + q) * rl[q];
+        sR += D(30 + d * 5 + q) * rr[q];
       }
       if (d == 0) { sL += v.u[(int64_t)L * 4 + var[c]]; sR += v.u[(int64_t)R * 4 + var[c]]; }
       val[d][c] = (sL + sR) * 0.5;
@@ -103,7 +112,7 @@ DG_HD void limiter_face_indicator(int64_t f, const LimView& v, const T* urec) {
     }
   }
   double W[6];
-  for (int k = 0; k < 6; k++) W[k] = v.limFace[aos(f, 60 + k, kLimE)];
+  for (int k = 0; k < 6; k++) W[k] = D(60 + k);
   const double area = v.faceArea[f];
   double sL = sqrt(v.vol[L]) / area, sR = sqrt(v.vol[R]) / area;
   double arMax = dmax(1.0, dmax(sL, sR));
@@ -175,15 +184,10 @@ DG_HD double wbap_biway(double u1, double u2, double n) {
   return u1 * (n + th1) / (n + th2);
 }
 
-// limiting pass for one cell; writes all 20 coefficients of the cell into out
+// limiting pass for one cell (one the indicator pass listed); writes its 20 limited coefficients to o
 template <class T>
-DG_HD void limiter_cell(int64_t i, const LimView& v, const T* urec, T* out) {
-  double ind = v.indicator[i];
+DG_HD void limiter_cell(int64_t i, const LimView& v, const T* urec, T* o) {
   const T* ri = &urec[i * 20];
-  if (ind < v.scale && !v.ifAll) {
-    for (int k = 0; k < 20; k++) out[i * 20 + k] = ri[k];
-    return;
-  }
   const double sm4 = 1e-50;  // verySmallReal^(1/4)
   double res[5][4];
   double uFaces[4][3][4];  // biway results of the P2 pass per face, this cell's basis
@@ -250,7 +254,7 @@ DG_HD void limiter_cell(int64_t i, const LimView& v, const T* urec, T* out) {
         res[ls + r][c] = u0 * (up[r][c] + v.nStd) / (down[r][c] + v.nStd);
       }
   }
-  for (int q = 0; q < 5; q++) for (int c = 0; c < 4; c++) out[i * 20 + q * 4 + c] = (T)res[q][c];
+  for (int q = 0; q < 5; q++) for (int c = 0; c < 4; c++) o[q * 4 + c] = (T)res[q][c];
 }
 
 }  // namespace dg
