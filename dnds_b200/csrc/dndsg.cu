@@ -293,8 +293,10 @@ __global__ void k_lim_d32(const double* limFace, int64_t F, float* d32) {
   if (f < F)
     for (int e = 0; e < kLimDE; e++) d32[aos(f, e, kLimDE)] = (float)limFace[aos(f, e, kLimE)];
 }
+// FP32 at 3 blocks per SM (80 registers; measured per SSP-RK3 step of the 8,388,608-triangle Riemann
+// problem: 2 blocks 11.42 ms, 3: 11.27, 4: 12.50; FP64 is best left at 2)
 template <class T>
-__global__ void k_lim_face(LimView v, const T* urec, int32_t* count) {
+__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 3 : 2) k_lim_face(LimView v, const T* urec, int32_t* count) {
   int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (f == 0) *count = 0;  // the list of cells to limit, filled by the next launch
   if (f < v.F) limiter_face_indicator<T>(f, v, urec);
