@@ -40,6 +40,12 @@ N_GRID = 1024
 # write urec 20s (s = bytes per real), cell means 4x8, 3 neighbour indices 3x4
 VR_BYTES_PER_CELL = {4: 130 * 4 + 32 + 12, 8: 130 * 8 + 32 + 12}
 KERNELS_PER_STEP = 14  # init, dt face, dt cell, dt finalize, 3 x (VR, flux, update), time advance
+# algorithmic bytes per triangle cell of one whole SSP-RK3 step: 3 stages x (VR sweep, face flux with
+# 1.5 faces per cell (basis 30s, normal / length / dLambda / indices ~40 B, flux out 32 B) plus the
+# cell's coefficients 20s and means 32 B once, cell update 136 B) + EvaluateDt ~74 B.  FP32 bulk
+# 3 x (564 + 412 + 136) + 74 = 3410 B, FP64 3 x (1084 + 660 + 136) + 74 = 5714 B: at equal HBM
+# efficiency the FP32-bulk step can be at most 5714 / 3410 = 1.68 times faster
+STEP_BYTES_PER_CELL = {4: 3 * (564 + 412 + 136) + 74, 8: 3 * (1084 + 660 + 136) + 74}
 # DRAM bytes (read + write) per launch of the FP32 VR sweep: ncu dram__bytes_read.sum +
 # dram__bytes_write.sum on the 512x512 mesh (292.25 MB for 524,288 cells, see
 # profiles/vr_sweep_fp32_vortex_tri512.md) scaled by the cell count (x4) to this workload
@@ -569,6 +575,13 @@ def main():
         "fp64_path": {"value": value64, "ms_per_step": r64["ms"] / args.steps, "vr_ms": r64["vr_ms"],
                       "rhs_ms": r64["rhs_ms"]},
         "speedup_fp32_over_fp64": value / value64,
+        "step_roofline": {
+            name: {"alg_bytes_per_cell": STEP_BYTES_PER_CELL[sz],
+                   "achieved": STEP_BYTES_PER_CELL[sz] * N / (r["ms"] / args.steps * 1e-3) / 1e9,
+                   "frac": STEP_BYTES_PER_CELL[sz] * N / (r["ms"] / args.steps * 1e-3) / 1e9 / peak,
+                   "unit": "GB/s"}
+            for name, r, sz in (("fp32", r32, 4), ("fp64", r64, 8))},
+        "speedup_bound_by_bytes": STEP_BYTES_PER_CELL[8] / STEP_BYTES_PER_CELL[4],
         "kernels_ms": {"vr_sweep_fp32": r32["vr_ms"], "rhs_fp32": r32["rhs_ms"]},
         "roofline": {"kernel": "vr_sweep (FP32)", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": f"{peak_kind} hbm_gbs",
