@@ -354,6 +354,45 @@ def riemann_leg(dev, steps=20, grid=2048, log=None):
     return out
 
 
+def small_mesh_leg(dev, steps=2000):
+    """The launch-bound small case: the isentropic vortex on 40 x 40 periodic quads (1,600 cells), P2 VR +
+    Roe, SSP-RK3 CFL 0.5: ms per step with one kernel launch per kernel (dndsg_ssprk3_step) and with
+    pairs of steps replayed from a CUDA graph (dndsg_ssprk3_steps).  Timed outside the headline."""
+    import torch
+
+    from dnds_b200 import geometry as G
+    from dnds_b200 import mesh as M
+    from dnds_b200 import settings as S
+    from dnds_b200.solver import Solver
+
+    m = M.vortex_mesh(40, False)
+    cfg = S.preset("vortex")
+    u0 = G.isentropic_vortex(m)
+    out = {"workload": "isentropic vortex, periodic [0,10]^2, 40x40 quads (1,600 cells), P2 VR + Roe, SSP-RK3 CFL 0.5",
+           "cells": m.n_cells, "steps": steps}
+    for prec, name in ((1, "fp32"), (0, "fp64")):
+        s = Solver(m, cfg, device=dev, precision=prec)
+        s.set_u(u0)
+        s.ssprk3_steps(0.5, 10)
+        r = {}
+        for mode in ("launches", "graph"):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            if mode == "graph":
+                s.ssprk3_steps(0.5, steps)
+            else:
+                for _ in range(steps):
+                    s.ssprk3_step(0.5)
+            e1.record()
+            torch.cuda.synchronize()
+            r[f"ms_per_step_{mode}"] = e0.elapsed_time(e1) / steps
+        r["value_graph"] = m.n_cells * 3 / (r["ms_per_step_graph"] * 1e-3)
+        out[name] = r
+        s.close()
+    return out
+
+
 def learned_leg(dev, grid, tol=1e-7, log=None):
     """The learned VR warm start: harvest on two 256 x 256 x 2 vortex meshes, train on the GPU,
     then Jacobi sweeps per SSP-RK3 step to the same rms-increment tolerance, with and without the
@@ -603,6 +642,8 @@ def main():
         out["cpu_baseline"] = cpu_baseline()
     if rank == 0 and ws == 1 and not args.no_steady:
         out["steady_naca0012_sa"] = steady_leg(dev)
+    if rank == 0 and ws == 1 and not args.no_riemann:
+        out["small_mesh_c1"] = small_mesh_leg(dev)
     if rank == 0 and ws == 1 and not args.no_riemann:
         out["riemann_cwbap"] = riemann_leg(dev, grid=args.riemann_grid)
     if rank == 0 and ws == 1 and not args.no_learned:

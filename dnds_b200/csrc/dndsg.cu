@@ -57,7 +57,15 @@ struct dndsg_ctx {
   double *limFace = nullptr, *faceInd = nullptr, *indicator = nullptr;  // CWBAP limiter data
   int32_t *limList = nullptr, *limCount = nullptr;  // cells the limiter pass limits, and their number
   float* limD32 = nullptr;                          // FP32 bulk: limFace elements [0, kLimDE) in FP32
-  int sms = 0;                                      // multiprocessors of the device (queried on first use)
+  int sms = 0;                                      // multiprocessors of the device
+  // dndsg_ssprk3_steps: CUDA graphs of two SSP-RK3 steps, one per coefficient buffer holding urec at
+  // the start (a step swaps the buffers three times), for the cfl / t_end they were captured with
+  struct StepGraph {
+    cudaGraphExec_t exec = nullptr;
+    double cfl = 0, tEnd = 0;
+    void* urec = nullptr;
+  } stepGraph[2];
+  cudaStream_t capStream = nullptr;
   int32_t* wallCells = nullptr;  // cells with a Wall_Euler / Wall_NoSlip face
   float* mlpGeom = nullptr;  // [N][8] slot face centres in each cell's polynomial frame
   void *mlpM = nullptr, *mlpA = nullptr, *mlpB = nullptr, *mlpH = nullptr;  // learned warm start work (T)
@@ -974,6 +982,7 @@ int dndsg_create(const dndsg_mesh_desc* mesh, const dndsg_settings* settings, in
   c->nfmax = anyQuad ? 4 : 3;
   int rc = set_device(c);
   if (rc) return rc;
+  if (cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess) c->sms = 148;
   // internal face order: interior faces first, then boundary faces, so the hot
   // flux kernel carries no boundary-condition code
   const int64_t F = c->F;
@@ -1000,6 +1009,9 @@ int dndsg_create(const dndsg_mesh_desc* mesh, const dndsg_settings* settings, in
 void dndsg_destroy(dndsg_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
+  for (auto& g : c->stepGraph)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  if (c->capStream) cudaStreamDestroy(c->capStream);
   for (void* p : c->allocs) cudaFree(p);
   delete c;
 }
@@ -1226,6 +1238,52 @@ int dndsg_ssprk3_step(dndsg_ctx* c, double cfl, double t_end, void* s) {
   if (c->sa) return fail(c, DNDSG_UNSUPPORTED, "SA contexts run the implicit path (dndsg_implicit_iteration)");
   if (c->fp32) run_step<float>(c, cfl, t_end, st(s));
   else run_step<double>(c, cfl, t_end, st(s));
+  return check_launch(c);
+}
+
+// n SSP-RK3 steps, pairs of them replayed from a CUDA graph: on small meshes a step is a handful of
+// microseconds of work behind 14 launches, and one graph launch replaces 28.  The graph is captured
+// (on a private stream) the first time a cfl / t_end / buffer parity is seen and kept.
+int dndsg_ssprk3_steps(dndsg_ctx* c, double cfl, double t_end, int64_t n, void* s) {
+  if (!c || n < 0) return DNDSG_BAD_ARGUMENT;
+  if (c->sa) return fail(c, DNDSG_UNSUPPORTED, "SA contexts run the implicit path (dndsg_implicit_iteration)");
+  int rc;
+  if ((rc = set_device(c))) return rc;
+  if (n >= 2) {
+    int slot = -1;
+    for (int k = 0; k < 2; k++)
+      if (c->stepGraph[k].exec && c->stepGraph[k].urec == c->urec) slot = k;
+    if (slot < 0) slot = c->stepGraph[0].exec ? 1 : 0;
+    dndsg_ctx::StepGraph& g = c->stepGraph[slot];
+    if (!g.exec || g.cfl != cfl || g.tEnd != t_end) {
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+      g.exec = nullptr;
+      if (!c->capStream) DG_CUDA(c, cudaStreamCreateWithFlags(&c->capStream, cudaStreamNonBlocking));
+      void* urec0 = c->urec;
+      DG_CUDA(c, cudaStreamBeginCapture(c->capStream, cudaStreamCaptureModeThreadLocal));
+      for (int k = 0; k < 2; k++) {  // six buffer swaps: urec is back in its buffer afterwards
+        if (c->fp32) run_step<float>(c, cfl, t_end, c->capStream);
+        else run_step<double>(c, cfl, t_end, c->capStream);
+      }
+      cudaGraph_t graph = nullptr;
+      const cudaError_t e = cudaStreamEndCapture(c->capStream, &graph);
+      if (e != cudaSuccess) return fail(c, DNDSG_CUDA_ERROR, std::string("step capture: ") + cudaGetErrorString(e));
+      const cudaError_t e2 = cudaGraphInstantiate(&g.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e2 != cudaSuccess) {
+        g.exec = nullptr;
+        return fail(c, DNDSG_CUDA_ERROR, std::string("step graph: ") + cudaGetErrorString(e2));
+      }
+      g.cfl = cfl;
+      g.tEnd = t_end;
+      g.urec = urec0;
+    }
+    for (int64_t k = 0; k < n / 2; k++) DG_CUDA(c, cudaGraphLaunch(g.exec, st(s)));
+  }
+  if (n & 1) {
+    if (c->fp32) run_step<float>(c, cfl, t_end, st(s));
+    else run_step<double>(c, cfl, t_end, st(s));
+  }
   return check_launch(c);
 }
 

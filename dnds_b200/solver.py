@@ -153,6 +153,10 @@ class Solver:
     def ssprk3_step(self, cfl: float, t_end: float = 1e300):
         self._check(self.L.dndsg_ssprk3_step(self.h, cfl, t_end, self.stream))
 
+    def ssprk3_steps(self, cfl: float, n: int, t_end: float = 1e300):
+        """n SSP-RK3 steps, pairs of them replayed from a CUDA graph (dndsg_ssprk3_steps)."""
+        self._check(self.L.dndsg_ssprk3_steps(self.h, cfl, t_end, int(n), self.stream))
+
     # ------------------------------------------------------------------ implicit steady path
     def lusgs_colours(self):
         """(colour of every cell, number of colours) of the LU-SGS colouring."""

@@ -155,6 +155,12 @@ int dndsg_eval_rhs(dndsg_ctx* ctx, double t, double* rhs_out, void* stream);
  * the call is asynchronous and can be captured in a CUDA graph. */
 int dndsg_ssprk3_step(dndsg_ctx* ctx, double cfl, double t_end, void* stream);
 
+/* n calls of dndsg_ssprk3_step, with the same results: pairs of steps are
+ * replayed from a CUDA graph captured on first use for this cfl / t_end (one
+ * graph launch instead of 28 kernel launches; small meshes are launch-bound).
+ * Same arguments as dndsg_ssprk3_step plus the step count n >= 0. */
+int dndsg_ssprk3_steps(dndsg_ctx* ctx, double cfl, double t_end, int64_t n, void* stream);
+
 /* EulerEvaluator::EvaluateResidual (DNDS_FV_EulerEvaluator.cpp:1557-1592) of
  * DNDSG_BUF_RHS: p < 3 gives the p-norm (volume-weighted when vol_wise), else
  * the max norm; out [nvars] (host), FP64. */

@@ -102,6 +102,64 @@ def test_limiter_matches_golden(precision, tol):
     assert flags == 0
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_limiter_changes_only_the_cells_it_lists(precision):
+    """The indicator pass lists the cells with si >= WBAP_SmoothIndicatorScale and only those are
+    limited: every other cell keeps its coefficients bit for bit.  A free stream lists no cell at all."""
+    m = M.riemann_mesh(48, jitter=0.15, seed=4321)
+    cfg = S.preset("riemann")
+    scale = cfg["vfvSetting"]["WBAP_SmoothIndicatorScale"]
+    s = _solver(m, cfg, precision)
+    s.set_u(G.quadrant_states(m, S.RIEMANN_2D_STATES))
+    s.ReconstructionJacobiStep(3)
+    before = s.get_urec()
+    ind = s.ReconstructionWBAPLimitFacialV3(False, indicator=True)
+    after = s.get_urec()
+    keep = ind < scale
+    assert keep.any() and (~keep).any()
+    assert np.array_equal(after[keep], before[keep])
+    assert not np.array_equal(after[~keep], before[~keep])
+    # a free stream: the reconstruction vanishes, no indicator reaches the scale, nothing changes
+    s.set_u(np.tile(G.quadrant_states(m, S.RIEMANN_2D_STATES)[:1], (m.n_cells, 1)))
+    s.set_urec(np.zeros((m.n_cells, 5, 4)))
+    s.ReconstructionJacobiStep(2)
+    before = s.get_urec()
+    ind = s.ReconstructionWBAPLimitFacialV3(False, indicator=True)
+    assert (ind < scale).all()
+    assert np.array_equal(s.get_urec(), before)
+    flags, _ = s.status()
+    assert flags == 0
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_graph_replayed_steps_equal_single_steps(precision):
+    """dndsg_ssprk3_steps (pairs of steps from a CUDA graph) computes what the same number of
+    dndsg_ssprk3_step calls computes, bit for bit: odd counts, a coefficient-buffer parity flipped by a
+    lone VR sweep in between, a new cfl (a second capture), and the limiter on the Riemann mesh."""
+    cases = [(M.vortex_mesh(16, True, jitter=0.2), S.preset("vortex"), None, 0.5),
+             (M.riemann_mesh(16, jitter=0.15, seed=4321), S.preset("riemann"), S.RIEMANN_2D_STATES, 0.4)]
+    for m, cfg, states, cfl in cases:
+        u0 = G.isentropic_vortex(m) if states is None else G.quadrant_states(m, states)
+        a, b = _solver(m, cfg, precision), _solver(m, cfg, precision)
+        for s in (a, b):
+            s.set_u(u0)
+        for k in range(5):
+            a.ssprk3_step(cfl)
+        b.ssprk3_steps(cfl, 5)
+        assert np.array_equal(a.get_u(), b.get_u()) and a.time == b.time
+        for s in (a, b):
+            s.ReconstructionJacobiStep(1)
+        for k in range(4):
+            a.ssprk3_step(0.8 * cfl)
+        b.ssprk3_steps(0.8 * cfl, 4)
+        assert np.array_equal(a.get_u(), b.get_u()) and np.array_equal(a.get_urec(), b.get_urec())
+        b.ssprk3_steps(cfl, 0)
+        for s in (a, b):
+            flags, _ = s.status()
+            assert flags == 0
+            s.close()
+
+
 def test_vortex_c1_against_oracle(oracle_lib):
     """40x40 periodic quads, P2 VR + Roe, SSP-RK3 CFL 0.5: 20 steps GPU vs oracle."""
     m = M.vortex_mesh(40, False)
