@@ -139,6 +139,22 @@ class EulerEvaluatorGPU {
   Context& c_;
 };
 
+// the explicit driver: ExplicitSSPRK3LocalDt::Step with the frhs body (DNDS_ODE.hpp:131-177,
+// DNDS_FV_EulerSolver.hpp:713-837), one step or n of them (pairs replayed from a CUDA graph)
+class ExplicitSSPRK3GPU {
+ public:
+  explicit ExplicitSSPRK3GPU(Context& c) : c_(c) {}
+  void Step(double CFL, double tEnd = 1e300, void* stream = nullptr) {
+    c_.check(dndsg_ssprk3_step(c_.get(), CFL, tEnd, stream));
+  }
+  void Steps(double CFL, int64_t n, double tEnd = 1e300, void* stream = nullptr) {
+    c_.check(dndsg_ssprk3_steps(c_.get(), CFL, tEnd, n, stream));
+  }
+
+ private:
+  Context& c_;
+};
+
 // the steady path: pseudo-time iterations of a first-order BDF step until the density increment,
 // relative to its largest value so far, drops below rhsThresholdInternal (fstop)
 class ImplicitSteadyGPU {
