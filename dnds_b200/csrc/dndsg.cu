@@ -1292,6 +1292,11 @@ int dndsg_set_owned(dndsg_ctx* c, const uint8_t* owned) {
   if (!c) return DNDSG_BAD_ARGUMENT;
   int rc;
   if ((rc = set_device(c))) return rc;
+  // the step graphs of dndsg_ssprk3_steps hold the mask pointer of their capture: recapture
+  for (auto& g : c->stepGraph) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    g = dndsg_ctx::StepGraph{};
+  }
   if (!owned) {
     c->owned = nullptr;
     return 0;

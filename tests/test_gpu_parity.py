@@ -160,6 +160,35 @@ def test_graph_replayed_steps_equal_single_steps(precision):
             s.close()
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_graph_steps_follow_a_new_owned_mask(precision):
+    """An owned-cell mask set after the step graph was captured takes effect in the graph steps: the
+    cell with the smallest dt is left out of the dt minimum, the steps equal single steps with the
+    same mask and differ from steps without it."""
+    import ctypes as C
+
+    m, cfg = M.vortex_mesh(16, True, jitter=0.2), S.preset("vortex")
+    u0 = G.isentropic_vortex(m)
+    a, b, c = (_solver(m, cfg, precision) for _ in range(3))
+    for s in (a, b, c):
+        s.set_u(u0)
+        s.ssprk3_steps(0.5, 2)
+    a.EvaluateDt(0.5, use_local_dt=True)
+    mask = np.ones(m.n_cells, dtype=np.uint8)
+    mask[int(np.argmin(a.get_dt()))] = 0
+    for s in (a, b):
+        s._check(s.L.dndsg_set_owned(s.h, mask.ctypes.data_as(C.c_void_p)))
+    t0 = a.time
+    a.ssprk3_steps(0.5, 2)
+    for _ in range(2):
+        b.ssprk3_step(0.5)
+    c.ssprk3_steps(0.5, 2)
+    assert np.array_equal(a.get_u(), b.get_u()) and a.time == b.time
+    assert a.time - t0 > c.time - t0
+    for s in (a, b, c):
+        s.close()
+
+
 def test_vortex_c1_against_oracle(oracle_lib):
     """40x40 periodic quads, P2 VR + Roe, SSP-RK3 CFL 0.5: 20 steps GPU vs oracle."""
     m = M.vortex_mesh(40, False)
