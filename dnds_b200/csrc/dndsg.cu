@@ -56,7 +56,7 @@ struct dndsg_ctx {
   double* Ainv = nullptr;
   double *limFace = nullptr, *faceInd = nullptr, *indicator = nullptr;  // CWBAP limiter data
   int32_t *limList = nullptr, *limCount = nullptr;  // cells the limiter pass limits, and their number
-  float* limD32 = nullptr;                          // FP32 bulk: limFace elements [0, kLimDE) in FP32
+  void *limG = nullptr, *limCell = nullptr;         // the indicator's compact face and cell data (T)
   int sms = 0;                                      // multiprocessors of the device
   // dndsg_ssprk3_steps: CUDA graphs of two SSP-RK3 steps, one per coefficient buffer holding urec at
   // the start (a step swaps the buffers three times), for the cfl / t_end they were captured with
@@ -296,15 +296,15 @@ __global__ void k_setup_limiter(MeshView m, SetupParams p, const CellSetup* cell
   int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (f < m.F && !setup_limiter_face(f, m, p, cells, faceW, lim)) atomicOr(bad, 4);
 }
-__global__ void k_lim_d32(const double* limFace, int64_t F, float* d32) {
-  const int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (f < F)
-    for (int e = 0; e < kLimDE; e++) d32[aos(f, e, kLimDE)] = (float)limFace[aos(f, e, kLimE)];
-}
-// FP32 at 3 blocks per SM (80 registers; measured per SSP-RK3 step of the 8,388,608-triangle Riemann
-// problem: 2 blocks 11.42 ms, 3: 11.27, 4: 12.50; FP64 is best left at 2)
 template <class T>
-__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 3 : 2) k_lim_face(LimView v, const T* urec, int32_t* count) {
+__global__ void k_setup_lim_compact(MeshView m, const CellSetup* cells, const double* faceW, T* g, T* cellFr) {
+  const int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  setup_limiter_compact<T>(f, m, cells, faceW, g, cellFr);
+}
+// 2 blocks per SM (at 3 the FP32 variant spills the basis derivatives it rebuilds from the cell frames;
+// measured per FP32 SSP-RK3 step of the 8,388,608-triangle Riemann problem: 2 blocks 11.10 ms, 3: 11.25)
+template <class T>
+__global__ void __launch_bounds__(kBlock, 2) k_lim_face(LimView v, const T* urec, int32_t* count) {
   int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (f == 0) *count = 0;  // the list of cells to limit, filled by the next launch
   if (f < v.F) limiter_face_indicator<T>(f, v, urec);
@@ -598,7 +598,7 @@ LimView lim_view(dndsg_ctx* c, int ifAll) {
   LimView v;
   v.N = c->N; v.F = c->F; v.Fi = c->Fi; v.nfmax = c->nfmax;
   v.cellFace = c->cellFace; v.faceL = c->faceL; v.faceR = c->faceR;
-  v.faceNormal = c->faceNormal; v.faceArea = c->faceArea; v.limFace = c->limFace; v.limD32 = c->limD32;
+  v.faceNormal = c->faceNormal; v.faceArea = c->faceArea; v.limFace = c->limFace; v.limG = c->limG; v.limCell = c->limCell;
   v.u = c->u; v.faceInd = c->faceInd; v.indicator = c->indicator;
   v.gamma = c->s.gamma; v.tangWeight = c->s.tang_weight; v.tangModMin = c->s.tang_weight_mod_min;
   v.tangModPower = c->s.tang_weight_mod_power; v.tangModLoc = c->s.tang_weight_mod_loc; v.vol = c->vol;
@@ -873,11 +873,11 @@ int setup_run(dndsg_ctx* c, const dndsg_mesh_desc* md) {
     if ((rc = dalloc(c, c->limList, sizeof(int32_t) * N)) || (rc = dalloc(c, c->limCount, sizeof(int32_t)))) return rc;
     k_setup_limiter<<<grid_for(F), kBlock>>>(m, p, cells, faceW, c->limFace, dBad);
     if ((rc = check_launch(c))) return rc;
-    if (sizeof(T) == 4) {  // FP32 bulk: the indicator's basis derivatives and weights in FP32
-      if ((rc = dalloc(c, c->limD32, sizeof(float) * aos_size(F, kLimDE)))) return rc;
-      k_lim_d32<<<grid_for(F), kBlock>>>(c->limFace, F, c->limD32);
-      if ((rc = check_launch(c))) return rc;
-    }
+    if ((rc = dalloc(c, c->limG, sizeof(T) * aos_size(F, kLimG))) ||
+        (rc = dalloc(c, c->limCell, sizeof(T) * kLimCell * N)))
+      return rc;
+    k_setup_lim_compact<T><<<grid_for(std::max<int64_t>(F, N)), kBlock>>>(m, cells, faceW, (T*)c->limG, (T*)c->limCell);
+    if ((rc = check_launch(c))) return rc;
   }
   DG_CUDA(c, cudaDeviceSynchronize());
   int bad = 0;

@@ -25,7 +25,12 @@ namespace dg {
 //   [66, 91)  msR2L (right-cell coefficients -> left basis), row-major
 //   [91, 116) msL2R
 constexpr int kLimE = 116;
-constexpr int kLimDE = 66;  // the elements the indicator reads (D at gauss point 0, face weights)
+// the indicator's compact data, in the context's precision: per face (AoSoA E = kLimG) the frame
+// coordinates (xi, eta) of gauss point 0 in the left and the right cell and the 6 face weights; per
+// cell ([N][kLimCell]) the frame's Pinv (row-major) and basis moments.  D at the point follows from
+// these (p2_diffs_at), a fifth of the bytes of storing it.
+constexpr int kLimG = 10;
+constexpr int kLimCell = 9;
 
 struct LimView {
   int64_t N, F, Fi;
@@ -36,7 +41,8 @@ struct LimView {
   const double* faceNormal;
   const double* faceArea;
   const double* limFace;   // AoSoA kLimE
-  const float* limD32;     // FP32 bulk contexts: its elements [0, kLimDE) in FP32, AoSoA kLimDE
+  const void* limG;        // T [F] AoSoA kLimG (T = the context's precision)
+  const void* limCell;     // T [N][kLimCell]
   const double* u;
   double* faceInd;         // [F][4]: IJI_rho, IJI_E, ISI_rho, ISI_E
   double* indicator;       // [N]
@@ -81,38 +87,65 @@ DG_HD bool setup_limiter_face(int64_t f, const MeshView& m, const SetupParams& p
 }
 
 // face pass of the smoothness indicator (DNDS_FV_VR.hpp:2075-2127)
+// the setup of the compact data: face f's frame coordinates and weights, and (f < N) cell f's frame
+template <class T>
+DG_HD void setup_limiter_compact(int64_t f, const MeshView& m, const CellSetup* cells, const double* faceW, T* g,
+                                 T* cellFr) {
+  if (f < m.F) {
+    const int32_t L = m.face_cells[2 * f], R = m.face_cells[2 * f + 1];
+    const FaceGeom fg = face_geom(f, m);
+    const double sx = m.face_shift ? m.face_shift[2 * f] : 0.0, sy = m.face_shift ? m.face_shift[2 * f + 1] : 0.0;
+    double xe[4] = {0, 0, 0, 0};
+    p2_frame_coords(cells[L].fr, fg.gx[0], fg.gy[0], xe[0], xe[1]);
+    if (R >= 0) p2_frame_coords(cells[R].fr, fg.gx[0] - sx, fg.gy[0] - sy, xe[2], xe[3]);
+    for (int k = 0; k < 4; k++) g[aos(f, k, kLimG)] = (T)xe[k];
+    for (int k = 0; k < 6; k++) g[aos(f, 4 + k, kLimG)] = (T)faceW[f * 6 + k];
+  }
+  if (f < m.N) {
+    const CellFrame& fr = cells[f].fr;
+    T* o = cellFr + f * kLimCell;
+    o[0] = (T)fr.Pinv[0][0]; o[1] = (T)fr.Pinv[0][1]; o[2] = (T)fr.Pinv[1][0]; o[3] = (T)fr.Pinv[1][1];
+    for (int k = 0; k < 5; k++) o[4 + k] = (T)fr.moment[k];
+  }
+}
+
 template <class T>
 DG_HD void limiter_face_indicator(int64_t f, const LimView& v, const T* urec) {
-  // element e of the face's indicator data: FP32 bulk contexts read the FP32 copy (half the bytes of
-  // the kernel's largest stream), FP64 contexts the FP64 table
-  auto D = [&](int e) -> double {
-    if constexpr (sizeof(T) == 4) return (double)v.limD32[aos(f, e, kLimDE)];
-    else return v.limFace[aos(f, e, kLimE)];
-  };
   int32_t L = v.faceL[f], R = v.faceR[f];
   double* out = &v.faceInd[f * 4];
   if (R < 0) { out[0] = out[1] = out[2] = out[3] = 0; return; }
-  double val[6][2], jump[6][2];
+  // per side: the rows of the cell's basis derivatives at gauss point 0 (from the cell's frame) times
+  // its rho and E coefficients, the mean added to the value row; one side's derivatives live at a time
+  const T* g = static_cast<const T*>(v.limG);
+  const T* cf = static_cast<const T*>(v.limCell);
   const int var[2] = {0, 3};
-  for (int c = 0; c < 2; c++) {
-    double rl[5], rr[5];
-    for (int q = 0; q < 5; q++) {
-      rl[q] = (double)urec[(int64_t)L * 20 + q * 4 + var[c]];
-      rr[q] = (double)urec[(int64_t)R * 20 + q * 4 + var[c]];
-    }
-    for (int d = 0; d < 6; d++) {
-      double sL = 0, sR = 0;
-      for (int q = 0; q < 5; q++) {
-        sL += D(d * 5 + q) * rl[q];
-        sR += D(30 + d * 5 + q) * rr[q];
+  double sv[2][6][2];
+  for (int side = 0; side < 2; side++) {
+    const int64_t cell = side ? R : L;
+    const T* c = cf + cell * kLimCell;
+    const double Q[2][2] = {{(double)c[0], (double)c[1]}, {(double)c[2], (double)c[3]}};
+    const double mo[5] = {(double)c[4], (double)c[5], (double)c[6], (double)c[7], (double)c[8]};
+    double D[6][5];
+    p2_diffs_at(Q, mo, (double)g[aos(f, 2 * side, kLimG)], (double)g[aos(f, 2 * side + 1, kLimG)], D);
+    for (int k = 0; k < 2; k++) {
+      double r[5];
+      for (int q = 0; q < 5; q++) r[q] = (double)urec[cell * 20 + q * 4 + var[k]];
+      for (int d = 0; d < 6; d++) {
+        double a = 0;
+        for (int q = 0; q < 5; q++) a += D[d][q] * r[q];
+        if (d == 0) a += v.u[cell * 4 + var[k]];
+        sv[side][d][k] = a;
       }
-      if (d == 0) { sL += v.u[(int64_t)L * 4 + var[c]]; sR += v.u[(int64_t)R * 4 + var[c]]; }
-      val[d][c] = (sL + sR) * 0.5;
-      jump[d][c] = (sL - sR) * 0.5;
     }
   }
+  double val[6][2], jump[6][2];
+  for (int c = 0; c < 2; c++)
+    for (int d = 0; d < 6; d++) {
+      val[d][c] = (sv[0][d][c] + sv[1][d][c]) * 0.5;
+      jump[d][c] = (sv[0][d][c] - sv[1][d][c]) * 0.5;
+    }
   double W[6];
-  for (int k = 0; k < 6; k++) W[k] = D(60 + k);
+  for (int k = 0; k < 6; k++) W[k] = (double)g[aos(f, 4 + k, kLimG)];
   const double area = v.faceArea[f];
   double sL = sqrt(v.vol[L]) / area, sR = sqrt(v.vol[R]) / area;
   double arMax = dmax(1.0, dmax(sL, sR));

@@ -259,13 +259,19 @@ DG_HD void p2_monomials(double xi, double eta, double m[5]) {
   m[0] = xi; m[1] = eta; m[2] = xi * xi; m[3] = xi * eta; m[4] = eta * eta;
 }
 
-DG_HD void p2_diffs(const CellFrame& f, double x, double y, double D[6][5]) {
-  const double (*Q)[2] = f.Pinv;
-  double dx = x - f.c[0], dy = y - f.c[1];
-  double xi = Q[0][0] * dx + Q[0][1] * dy, eta = Q[1][0] * dx + Q[1][1] * dy;
+// the frame coordinates of a point: xi = Pinv (x - c)
+DG_HD void p2_frame_coords(const CellFrame& f, double x, double y, double& xi, double& eta) {
+  const double dx = x - f.c[0], dy = y - f.c[1];
+  xi = f.Pinv[0][0] * dx + f.Pinv[0][1] * dy;
+  eta = f.Pinv[1][0] * dx + f.Pinv[1][1] * dy;
+}
+
+// value, gradient and Hessian rows of the basis at frame coordinates (xi, eta), from the frame's
+// Pinv and moments alone
+DG_HD void p2_diffs_at(const double Q[2][2], const double moment[5], double xi, double eta, double D[6][5]) {
   double m[5];
   p2_monomials(xi, eta, m);
-  for (int k = 0; k < 5; k++) D[0][k] = m[k] - f.moment[k];
+  for (int k = 0; k < 5; k++) D[0][k] = m[k] - moment[k];
   // d(xi)/dx = Q[0][0], d(xi)/dy = Q[0][1], d(eta)/dx = Q[1][0], d(eta)/dy = Q[1][1]
   double gxi[5] = {1, 0, 2 * xi, eta, 0};   // dm/dxi
   double get[5] = {0, 1, 0, xi, 2 * eta};   // dm/deta
@@ -281,6 +287,12 @@ DG_HD void p2_diffs(const CellFrame& f, double x, double y, double D[6][5]) {
     D[4][k] = hxx[k] * Q[0][0] * Q[0][1] + hxy[k] * (Q[0][0] * Q[1][1] + Q[1][0] * Q[0][1]) + hyy[k] * Q[1][0] * Q[1][1];
     D[5][k] = hxx[k] * Q[0][1] * Q[0][1] + 2 * hxy[k] * Q[0][1] * Q[1][1] + hyy[k] * Q[1][1] * Q[1][1];
   }
+}
+
+DG_HD void p2_diffs(const CellFrame& f, double x, double y, double D[6][5]) {
+  double xi, eta;
+  p2_frame_coords(f, x, y, xi, eta);
+  p2_diffs_at(f.Pinv, f.moment, xi, eta, D);
 }
 
 // only the value row (what the flux needs)
