@@ -19,12 +19,12 @@
 
 namespace dg {
 
-// per-face limiter data, tile-major AoSoA with E = kLimE:
-//   [0, 60)   D at gauss point 0, [side][diff][basis]
-//   [60, 66)  face weights
-//   [66, 91)  msR2L (right-cell coefficients -> left basis), row-major
-//   [91, 116) msL2R
-constexpr int kLimE = 116;
+// per-face data of the limiting pass, tile-major AoSoA with E = kLimE (FP64):
+//   [0, 25)   msR2L (right-cell coefficients -> left basis), row-major
+//   [25, 50)  msL2R
+// (the indicator's data is the compact limG / limCell below)
+constexpr int kLimE = 50;
+constexpr int kMsR2L = 0, kMsL2R = 25;
 // the indicator's compact data, in the context's precision: per face (AoSoA E = kLimG) the frame
 // coordinates (xi, eta) of gauss point 0 in the left and the right cell and the 6 face weights; per
 // cell ([N][kLimCell]) the frame's Pinv (row-major) and basis moments.  D at the point follows from
@@ -63,15 +63,9 @@ DG_HD bool setup_limiter_face(int64_t f, const MeshView& m, const SetupParams& p
                               const double* faceW, double* lim) {
   int32_t L = m.face_cells[2 * f], R = m.face_cells[2 * f + 1];
   for (int e = 0; e < kLimE; e++) lim[aos(f, e, kLimE)] = 0.0;
-  for (int k = 0; k < 6; k++) lim[aos(f, 60 + k, kLimE)] = faceW[f * 6 + k];
   if (R < 0) return true;
   FaceGeom g = face_geom(f, m);
   double sx = m.face_shift ? m.face_shift[2 * f] : 0.0, sy = m.face_shift ? m.face_shift[2 * f + 1] : 0.0;
-  double D[6][5];
-  p2_diffs(cells[L].fr, g.gx[0], g.gy[0], D);
-  for (int d = 0; d < 6; d++) for (int q = 0; q < 5; q++) lim[aos(f, d * 5 + q, kLimE)] = D[d][q];
-  p2_diffs(cells[R].fr, g.gx[0] - sx, g.gy[0] - sy, D);
-  for (int d = 0; d < 6; d++) for (int q = 0; q < 5; q++) lim[aos(f, 30 + d * 5 + q, kLimE)] = D[d][q];
   double DL[6][5], DR[6][5];
   p2_diffs(cells[L].fr, g.cx, g.cy, DL);
   p2_diffs(cells[R].fr, g.cx - sx, g.cy - sy, DR);
@@ -79,10 +73,10 @@ DG_HD bool setup_limiter_face(int64_t f, const MeshView& m, const SetupParams& p
   double A[5][5], B[5][5];
   for (int i = 0; i < 5; i++) for (int j = 0; j < 5; j++) { A[i][j] = DL[i + 1][j]; B[i][j] = DR[i + 1][j]; }
   bool ok = lu5_solve(A, B);
-  for (int i = 0; i < 5; i++) for (int j = 0; j < 5; j++) lim[aos(f, 66 + i * 5 + j, kLimE)] = B[i][j];
+  for (int i = 0; i < 5; i++) for (int j = 0; j < 5; j++) lim[aos(f, kMsR2L + i * 5 + j, kLimE)] = B[i][j];
   for (int i = 0; i < 5; i++) for (int j = 0; j < 5; j++) { A[i][j] = DR[i + 1][j]; B[i][j] = DL[i + 1][j]; }
   ok = lu5_solve(A, B) && ok;
-  for (int i = 0; i < 5; i++) for (int j = 0; j < 5; j++) lim[aos(f, 91 + i * 5 + j, kLimE)] = B[i][j];
+  for (int i = 0; i < 5; i++) for (int j = 0; j < 5; j++) lim[aos(f, kMsL2R + i * 5 + j, kLimE)] = B[i][j];
   return ok;
 }
 
@@ -237,7 +231,7 @@ DG_HD void limiter_cell(int64_t i, const LimView& v, const T* urec, T* o) {
       int32_t j = side == 0 ? v.faceR[f] : v.faceL[f];
       if (j < 0) continue;
       // ms: other -> this basis; msO: this -> other basis
-      const int eMs = side == 0 ? 66 : 91, eMsO = side == 0 ? 91 : 66;
+      const int eMs = side == 0 ? kMsR2L : kMsL2R, eMsO = side == 0 ? kMsL2R : kMsR2L;
       double uOO[5][4];
       for (int q = 0; q < 5; q++) for (int c = 0; c < 4; c++) uOO[q][c] = (double)urec[(int64_t)j * 20 + q * 4 + c];
       if (pass == 1) {
