@@ -46,10 +46,11 @@ KERNELS_PER_STEP = 14  # init, dt face, dt cell, dt finalize, 3 x (VR, flux, upd
 # 3 x (564 + 412 + 136) + 74 = 3410 B, FP64 3 x (1084 + 660 + 136) + 74 = 5714 B: at equal HBM
 # efficiency the FP32-bulk step can be at most 5714 / 3410 = 1.68 times faster
 STEP_BYTES_PER_CELL = {4: 3 * (564 + 412 + 136) + 74, 8: 3 * (1084 + 660 + 136) + 74}
-# DRAM bytes (read + write) per launch of the FP32 VR sweep: ncu dram__bytes_read.sum +
-# dram__bytes_write.sum on the 512x512 mesh (292.25 MB for 524,288 cells, see
-# profiles/vr_sweep_fp32_vortex_tri512.md) scaled by the cell count (x4) to this workload
-VR_TRAFFIC_FP32 = 291.23e6 * 4  # ncu DRAM read+write of one FP32 VR sweep on 524,288 cells, scaled to 2,097,152
+# DRAM bytes (read + write) per launch of the FP32 VR sweep: ncu --metrics dram__bytes_read.sum,
+# dram__bytes_write.sum --clock-control none on one k_vr_tma4<float,32,3> launch over the 512x512 version of
+# this mesh (524,288 cells; 291.23 MB read + written, 555 B per cell against the 564 B algorithmic), scaled by
+# the cell count (x4) to this workload: the working set exceeds L2 at both sizes, so traffic is per cell
+VR_TRAFFIC_FP32 = 291.23e6 * 4
 
 
 def dist_env():
@@ -87,7 +88,9 @@ def measured_peak():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled every 100 ms over the FP32 leg (warm-up, the
+    timed steps, the per-kernel timings, the end-to-end loop and the accuracy run): the timed region
+    itself is tens of milliseconds, shorter than the sampling interval, and runs the same kernels."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -98,7 +101,7 @@ class ClockSampler:
         self.f = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                       "-i", str(gpu_index), "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+                                       "-i", str(gpu_index), "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
 
@@ -154,24 +157,26 @@ def cpu_baseline(max_seconds=12.0):
                       f"{el:.1f} s, {cores} threads"}
 
 
-REF_BUDGET_S = 150.0  # wall-clock target of the whole reference arm
+REF_BUDGET_S = 240.0  # wall-clock target of the whole reference arm
 
 
 def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
         return
-    cb = cpu_baseline(max_seconds=1.0)  # warm the build; the measured arm follows
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
+
+    pyoracle.build()
     from dnds_b200 import geometry as G
     from dnds_b200 import mesh as M
     from dnds_b200 import settings as S
 
     cores = os.cpu_count() or 1
-    # each step is a bounded sample of the workload: the mesh is sized (at most 512 x 512 x 2) so that the
-    # whole --warmup W --steps K run takes about REF_BUDGET_S, from the cost of one calibration step
-    cal = M.vortex_mesh(64, True, jitter=0.2, seed=1234)
+    # each step runs the full workload (1024 x 1024 x 2 = 2,097,152 triangles, about 2 s per step on 16
+    # host threads) when the whole --warmup W --steps K run fits in about REF_BUDGET_S, from the cost of one
+    # calibration step; with more steps than that the mesh shrinks to a bounded sample of the workload
+    cal = M.vortex_mesh(128, True, jitter=0.2, seed=1234)
     oc = pyoracle.Oracle(cal, S.preset("vortex"), n_threads=cores)
     oc.set_u(G.isentropic_vortex(cal))
     _, d = oc.eval_dt(0.5)
@@ -182,7 +187,7 @@ def run_reference(args):
     per_cell = (time.perf_counter() - t0) / cal.n_cells
     del oc
     cells = REF_BUDGET_S / max(args.steps + args.warmup, 1) / max(per_cell, 1e-12)
-    n = int(max(32, min(512, (cells / 2) ** 0.5)))
+    n = int(max(32, min(N_GRID, (cells / 2) ** 0.5)))
     m = M.vortex_mesh(n, True, jitter=0.2, seed=1234)
     o = pyoracle.Oracle(m, S.preset("vortex"), n_threads=cores)
     o.set_u(G.isentropic_vortex(m))
@@ -203,14 +208,15 @@ def run_reference(args):
         "warmup": args.warmup, "ms_per_step": el / max(args.steps, 1) * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "cells": m.n_cells, "parallelism": "host threads",
+                   "same_mesh_as_gpu_arm": n == N_GRID,
                    "note": "FP64 CPU restatement of the reference (the reference needs Eigen/MPI/METIS, absent here); "
-                           f"each step is a {n}x{n}x2 = {m.n_cells:,}-triangle sample of the workload, sized so "
-                           "that the run ends within minutes; the metric is per cell"},
+                           f"each step runs the {n}x{n}x2 = {m.n_cells:,}-triangle mesh"
+                           + (" of the workload" if n == N_GRID else ", a sample of the workload sized so that the "
+                              "run ends within minutes; the metric is per cell")},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": f"{args.steps} timed SSP-RK3 steps on {m.n_cells:,} triangles, {cores} threads"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    del cb
     print(json.dumps(out))
 
 
@@ -354,6 +360,54 @@ def riemann_leg(dev, steps=20, grid=2048, log=None):
     return out
 
 
+def riemann_to_end_leg(dev, grid=512, t_end=0.3, log=None):
+    """The 2-D Riemann problem run to its configured end time t = 0.3 (SSP-RK3, CFL 0.4, P2 VR, CWBAP,
+    HLLC) in FP32 bulk and in FP64 on a grid x grid jittered mesh (2 grid^2 triangles): steps, device
+    time of the whole run, cell-RK-stage updates/s over it, and the density difference of the two
+    precisions at t = 0.3 (L2 volume-weighted and Linf, absolute and relative to the density's own L2).
+    The configured 2048 x 2048 mesh takes about 39,000 steps per precision (python bench.py
+    --riemann-full); the default run uses a coarser grid so that the bench ends within minutes."""
+    import torch
+
+    from dnds_b200 import geometry as G
+    from dnds_b200 import mesh as M
+    from dnds_b200 import settings as S
+    from dnds_b200.solver import Solver
+
+    m = M.riemann_mesh(grid)
+    cfg = S.preset("riemann")
+    u0 = G.quadrant_states(m, S.RIEMANN_2D_STATES)
+    vol = G.cell_quadrature(m)[1].sum(1)
+    out = {"workload": f"2-D Riemann, [0,1]^2, {grid}x{grid} jittered quads -> {m.n_cells:,} triangles, P2 VR + "
+                       f"CWBAP + HLLC, SSP-RK3 CFL 0.4 to t = {t_end}", "cells": m.n_cells}
+    us = {}
+    for prec, name in ((1, "fp32"), (0, "fp64")):
+        s = Solver(m, cfg, device=dev, precision=prec)
+        s.set_u(u0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        steps = s.run_to(t_end, 0.4)
+        e1.record()
+        torch.cuda.synchronize()
+        sec = e0.elapsed_time(e1) * 1e-3
+        us[name] = s.get_u()
+        flags, nred = s.status()
+        out[name] = {"steps": steps, "t": s.time, "seconds": sec, "ms_per_step": sec * 1e3 / steps,
+                     "value": m.n_cells * 3 * steps / sec, "unit": UNIT, "flags": flags,
+                     "reduced_order_points": nred}
+        s.close()
+        if log:
+            log(name, out[name])
+    d = us["fp32"][:, 0] - us["fp64"][:, 0]
+    l2 = float(np.sqrt((d * d * vol).sum() / vol.sum()))
+    rho_l2 = float(np.sqrt((us["fp64"][:, 0] ** 2 * vol).sum() / vol.sum()))
+    out["rho_fp32_vs_fp64"] = {"l2": l2, "linf": float(np.abs(d).max()), "l2_relative": l2 / rho_l2,
+                               "l1": float((np.abs(d) * vol).sum() / vol.sum())}
+    out["speedup_fp32_over_fp64"] = out["fp64"]["seconds"] / out["fp32"]["seconds"]
+    return out
+
+
 def small_mesh_leg(dev, steps=2000):
     """The launch-bound small case: the isentropic vortex on 40 x 40 periodic quads (1,600 cells), P2 VR +
     Roe, SSP-RK3 CFL 0.5: ms per step with one kernel launch per kernel (dndsg_ssprk3_step) and with
@@ -472,7 +526,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="dnds_b200", choices=["dnds_b200", "reference"])
     ap.add_argument("--no-accuracy", action="store_true")
-    ap.add_argument("--accuracy-t", type=float, default=0.5, help="end time of the accuracy runs (the config asks t=2)")
+    ap.add_argument("--accuracy-t", type=float, default=2.0, help="end time of the accuracy runs (the config's t=2)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--grid", type=int, default=N_GRID, help="grid size n (n x n quads -> 2 n^2 triangles)")
@@ -481,12 +535,26 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start report")
     ap.add_argument("--no-riemann", action="store_true", help="skip the 8.4M-triangle Riemann / CWBAP report")
     ap.add_argument("--riemann-grid", type=int, default=2048, help="grid size of the Riemann / CWBAP report")
+    ap.add_argument("--riemann-end-grid", type=int, default=512,
+                    help="grid size of the Riemann run to t = 0.3 in the default bench")
+    ap.add_argument("--riemann-full", action="store_true",
+                    help="only the Riemann problem to t = 0.3 on the configured 2048 x 2048 mesh (both precisions, "
+                         "about 17 minutes); prints one JSON line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
 
     import torch
+
+    if args.riemann_full:
+        torch.cuda.set_device(0)
+        clk = ClockSampler(0)
+        r = riemann_to_end_leg(0, grid=2048, log=lambda *a: print(*a, file=sys.stderr, flush=True))
+        r["clocks"] = clk.stop()
+        r["command"] = "python bench.py --riemann-full"
+        print(json.dumps(r))
+        return
 
     ws, rank, local = dist_env()
     if ws > 1:
@@ -534,11 +602,10 @@ def main():
             continue
         s = Solver(m, cfg, device=dev, precision=prec)
         s.set_u(u0)
+        clk = ClockSampler(dev) if name == "fp32" else None
         for _ in range(args.warmup):
             s.ssprk3_step(0.5, 1e300)
-        clk = ClockSampler(dev) if name == "fp32" else None
         ms = time_steps(s, args.steps)
-        clocks = clk.stop() if clk else None
         # per-kernel: the VR sweep alone, and the RHS (face flux + gather)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         nk = 20
@@ -557,7 +624,7 @@ def main():
         torch.cuda.synchronize()
         rhs_ms = e0.elapsed_time(e1) / nk
         flags, nred = s.status()
-        results[name] = dict(ms=ms, vr_ms=vr_ms, rhs_ms=rhs_ms, clocks=clocks, flags=flags, nred=nred)
+        results[name] = dict(ms=ms, vr_ms=vr_ms, rhs_ms=rhs_ms, clocks=None, flags=flags, nred=nred)
         # end-to-end through the public API with host buffers: per step h2d of the
         # state u (pinned), one SSP-RK3 step, d2h of the new state
         if name == "fp32" and not args.no_e2e:
@@ -586,6 +653,8 @@ def main():
             results[name]["linf_rho"] = float(np.abs(d).max())
             results[name]["steps_to_t2"] = steps
             results[name]["u_t2"] = u
+        if clk:
+            results[name]["clocks"] = clk.stop()
         s.close()
 
     if len(results) == 2 and "u_t2" in results["fp32"]:
@@ -611,6 +680,7 @@ def main():
         "config": {"workload": WORKLOAD if args.grid == N_GRID else f"{WORKLOAD} (grid {args.grid})", "cells": N, "faces": m.n_faces, "precision": "fp32-bulk",
                    "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU",
                    "l2_flush": "no flush: per-step working set ~1.3 GB > 126 MB L2"},
+        "value_fp64": value64,
         "fp64_path": {"value": value64, "ms_per_step": r64["ms"] / args.steps, "vr_ms": r64["vr_ms"],
                       "rhs_ms": r64["rhs_ms"]},
         "speedup_fp32_over_fp64": value / value64,
@@ -637,6 +707,8 @@ def main():
         out["accuracy"] = {"t_end": args.accuracy_t, "l2_rho_fp32": r32["l2_rho"], "l2_rho_fp64": r64["l2_rho"],
                            "linf_rho_fp32": r32["linf_rho"], "linf_rho_fp64": r64["linf_rho"],
                            "l2_rho_fp32_vs_fp64": l2_vs64, "steps": r32["steps_to_t2"],
+                           "l2_ratio_fp32_over_fp64": r32["l2_rho"] / r64["l2_rho"],
+                           "equal_l2_within_1pct": abs(r32["l2_rho"] / r64["l2_rho"] - 1.0) <= 0.01,
                            "reference": "exact advected vortex (cell averages), density"}
     if rank == 0 and ws == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline()
@@ -646,6 +718,11 @@ def main():
         out["small_mesh_c1"] = small_mesh_leg(dev)
     if rank == 0 and ws == 1 and not args.no_riemann:
         out["riemann_cwbap"] = riemann_leg(dev, grid=args.riemann_grid)
+        out["riemann_to_t03"] = riemann_to_end_leg(dev, grid=args.riemann_end_grid)
+        rec = os.path.join(ROOT, "profiles", "riemann_full_tri2048_t0.3.json")
+        if os.path.exists(rec):  # the configured mesh to t = 0.3, recorded by --riemann-full (too long for here)
+            with open(rec) as fh:
+                out["riemann_to_t03_2048_recorded"] = json.load(fh)
     if rank == 0 and ws == 1 and not args.no_learned:
         out["learned_vr"] = learned_leg(dev, args.grid)
     if rank == 0:

@@ -22,7 +22,7 @@ EXPORTS = [
     "dndsg_lusgs_colours", "dndsg_lusgs_set_order", "dndsg_lusgs_matrix_init", "dndsg_lusgs_forward", "dndsg_lusgs_backward",
     "dndsg_bdf_begin", "dndsg_implicit_iteration", "dndsg_dual_reset", "dndsg_dual_step", "dndsg_lusgs_matvec", "dndsg_gmres_lusgs",
     "dndsg_set_owned", "dndsg_rk_dt", "dndsg_rk_set_dt", "dndsg_rk_vr", "dndsg_rk_limit", "dndsg_rk_stage",
-    "dndsg_rk_finish", "dndsg_halo_pack", "dndsg_halo_unpack",
+    "dndsg_rk_finish", "dndsg_halo_pack", "dndsg_halo_unpack", "dndsg_steady_solve",
 ]
 _NO_STATUS = ("dndsg_destroy", "dndsg_last_error", "dndsg_n_cells", "dndsg_n_faces", "dndsg_mlp_destroy",
               "dndsg_mlp_last_error")
@@ -35,6 +35,14 @@ class DualSettings(C.Structure):
     _fields_ = [("scheme", C.c_int), ("bdf_order", C.c_int), ("cfl", C.c_double), ("max_iter", C.c_int),
                 ("threshold", C.c_double), ("n_rec", C.c_int), ("vol_wise", C.c_int), ("gmres_code", C.c_int),
                 ("n_gmres_space", C.c_int), ("n_gmres_iter", C.c_int)]
+
+
+class SteadySettings(C.Structure):
+    """dndsg_steady_settings (include/dndsg.h), field for field."""
+    _fields_ = [("cfl", C.c_double), ("cfl_ramp_end", C.c_double), ("cfl_ramp_start", C.c_int),
+                ("cfl_ramp_length", C.c_int), ("max_iter", C.c_int), ("threshold", C.c_double), ("dt", C.c_double),
+                ("n_rec", C.c_int), ("vol_wise", C.c_int), ("gmres_code", C.c_int), ("n_gmres_space", C.c_int),
+                ("n_gmres_iter", C.c_int)]
 
 
 class MeshDesc(C.Structure):
@@ -118,6 +126,7 @@ def lib():
     L.dndsg_rk_finish.argtypes = [vp, vp]
     L.dndsg_halo_pack.argtypes = [vp, i32, vp, i64, vp, vp]
     L.dndsg_halo_unpack.argtypes = [vp, i32, vp, i64, vp, vp]
+    L.dndsg_steady_solve.argtypes = [vp, C.POINTER(SteadySettings), C.POINTER(i32), vp, vp, vp, vp]
     for nm in EXPORTS:
         if nm not in _NO_STATUS:
             getattr(L, nm).restype = i32

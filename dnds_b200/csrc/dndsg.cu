@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -98,6 +99,7 @@ struct dndsg_ctx {
   void *urec = nullptr, *urecNew = nullptr;  // T
   unsigned* flags = nullptr;
   unsigned long long* nreduced = nullptr;
+  bool dead = false;  // a kernel's bounded wait ran out: the context refuses further work
   uint8_t* owned = nullptr;  // [N] owned-cell mask of a partitioned run (null: every cell owned)
   uint8_t* ownedBuf = nullptr;
   std::vector<void*> allocs;
@@ -620,9 +622,9 @@ void run_limiter(dndsg_ctx* c, int ifAll, cudaStream_t s) {
   k_lim_scatter<T><<<g, kBlock, 0, s>>>((T*)c->urec, (const T*)c->urecNew, c->limList, c->limCount);
 }
 
+// the face-flux launches of EvaluateRHS over the arrays of h (interior faces, then boundary faces)
 template <class T>
-void launch_flux(dndsg_ctx* c, int useDev, double tHost, double cst, cudaStream_t s) {
-  HotView<T> h = view<T>(c);
+void launch_flux_h(dndsg_ctx* c, const HotView<T>& h, int useDev, double tHost, double cst, cudaStream_t s) {
   const int64_t Fi = c->Fi, F = c->F;
   if (c->s.mu_gas > 0) {
     if (c->s.riemann == 2) {
@@ -649,6 +651,11 @@ void launch_flux(dndsg_ctx* c, int useDev, double tHost, double cst, cudaStream_
     if (F > Fi)
       k_face_flux<T, 1, true><<<grid_for(F - Fi), kBlock, 0, s>>>(h, Fi, F, c->scal, useDev, tHost, cst, c->flags, c->nreduced);
   }
+}
+
+template <class T>
+void launch_flux(dndsg_ctx* c, int useDev, double tHost, double cst, cudaStream_t s) {
+  launch_flux_h<T>(c, view<T>(c), useDev, tHost, cst, s);
 }
 
 template <class T>
@@ -718,6 +725,27 @@ int check_launch(dndsg_ctx* c) {
 int set_device(dndsg_ctx* c) {
   cudaError_t e = cudaSetDevice(c->device);
   if (e != cudaSuccess) return fail(c, DNDSG_CUDA_ERROR, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+  return 0;
+}
+
+// A bounded wait inside a kernel that ran out (kFlagTimeout: an mbarrier phase of a bulk copy or of a
+// tensor-core commit, or a level-walk handshake, not complete within its poll limit) leaves the
+// context's resident data unreliable: the kernel skipped its work, and a copy may still have been in
+// flight when it returned.  Entry points that synchronise with the device read the flag word in that
+// synchronisation; once the bit is seen the context is dead and every later call on it returns
+// DNDSG_TIMEOUT (dndsg_destroy and dndsg_last_error still work).
+int refuse_dead(dndsg_ctx* c) {
+  return fail(c, DNDSG_TIMEOUT, "a bounded wait in a kernel ran out earlier; the context refuses further work");
+}
+
+int observe_timeout(dndsg_ctx* c, cudaStream_t s) {
+  unsigned f = 0;
+  DG_CUDA(c, cudaMemcpyAsync(&f, c->flags, sizeof(f), cudaMemcpyDeviceToHost, s));
+  DG_CUDA(c, cudaStreamSynchronize(s));
+  if (f & kFlagTimeout) {
+    c->dead = true;
+    return fail(c, DNDSG_TIMEOUT, "a bounded wait in a kernel ran out (timeout flag); the context refuses further work");
+  }
   return 0;
 }
 
@@ -1022,6 +1050,7 @@ int64_t dndsg_n_faces(dndsg_ctx* c) { return c ? c->F : -1; }
 
 int dndsg_set_u(dndsg_ctx* c, const double* u, void* s) {
   if (!c || !u) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   if (c->sa) {  // [N][5] -> flow [N][4] + U5 [N]
     std::vector<double> a(4 * c->N), b(c->N);
     for (int64_t i = 0; i < c->N; i++) {
@@ -1038,6 +1067,7 @@ int dndsg_set_u(dndsg_ctx* c, const double* u, void* s) {
 }
 int dndsg_get_u(dndsg_ctx* c, double* u, void* s) {
   if (!c || !u) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   if (c->sa) {
     DG_CUDA(c, cudaStreamSynchronize(st(s)));
     std::vector<double> a(4 * c->N), b(c->N);
@@ -1047,14 +1077,14 @@ int dndsg_get_u(dndsg_ctx* c, double* u, void* s) {
       for (int v = 0; v < 4; v++) u[5 * i + v] = a[4 * i + v];
       u[5 * i + 4] = b[i];
     }
-    return 0;
+    return observe_timeout(c, st(s));
   }
   DG_CUDA(c, cudaMemcpyAsync(u, c->u, sizeof(double) * 4 * c->N, cudaMemcpyDeviceToHost, st(s)));
-  DG_CUDA(c, cudaStreamSynchronize(st(s)));
-  return 0;
+  return observe_timeout(c, st(s));
 }
 int dndsg_get_dt(dndsg_ctx* c, double* dt, void* s) {
   if (!c || !dt) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   DG_CUDA(c, cudaMemcpyAsync(dt, c->dt, sizeof(double) * c->N, cudaMemcpyDeviceToHost, st(s)));
   DG_CUDA(c, cudaStreamSynchronize(st(s)));
   return 0;
@@ -1094,6 +1124,7 @@ extern "C" {
 
 int dndsg_set_urec(dndsg_ctx* c, const double* r, void* s) {
   if (!c || !r) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   if (c->sa) return c->fp32 ? sa_urec_io<float>(c, const_cast<double*>(r), true) : sa_urec_io<double>(c, const_cast<double*>(r), true);
   const int64_t n = 20 * c->N;
   if (!c->fp32) {
@@ -1110,6 +1141,7 @@ int dndsg_set_urec(dndsg_ctx* c, const double* r, void* s) {
 }
 int dndsg_get_urec(dndsg_ctx* c, double* r, void* s) {
   if (!c || !r) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   if (c->sa) return c->fp32 ? sa_urec_io<float>(c, r, false) : sa_urec_io<double>(c, r, false);
   const int64_t n = 20 * c->N;
   if (!c->fp32) {
@@ -1127,6 +1159,7 @@ int dndsg_get_urec(dndsg_ctx* c, double* r, void* s) {
 
 int dndsg_device_buffer(dndsg_ctx* c, int which, void** ptr, int64_t* bytes) {
   if (!c || !ptr) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   switch (which) {
     case DNDSG_BUF_U: *ptr = c->u; if (bytes) *bytes = sizeof(double) * 4 * c->N; return 0;
     case DNDSG_BUF_UREC: *ptr = c->urec; if (bytes) *bytes = (int64_t)c->tsize() * 20 * c->N; return 0;
@@ -1138,12 +1171,13 @@ int dndsg_device_buffer(dndsg_ctx* c, int which, void** ptr, int64_t* bytes) {
 
 int dndsg_get_time(dndsg_ctx* c, double* t, void* s) {
   if (!c || !t) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   DG_CUDA(c, cudaMemcpyAsync(t, c->scal + S_T, sizeof(double), cudaMemcpyDeviceToHost, st(s)));
-  DG_CUDA(c, cudaStreamSynchronize(st(s)));
-  return 0;
+  return observe_timeout(c, st(s));
 }
 int dndsg_set_time(dndsg_ctx* c, double t, void* s) {
   if (!c) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   DG_CUDA(c, cudaMemcpyAsync(c->scal + S_T, &t, sizeof(double), cudaMemcpyHostToDevice, st(s)));
   DG_CUDA(c, cudaStreamSynchronize(st(s)));
   return 0;
@@ -1151,6 +1185,7 @@ int dndsg_set_time(dndsg_ctx* c, double t, void* s) {
 
 int dndsg_vr_jacobi_step(dndsg_ctx* c, int nsweeps, double* inc_out, void* s) {
   if (!c || nsweeps < 0) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   if (c->sa) {
     if (inc_out) return fail(c, DNDSG_UNSUPPORTED, "SA contexts report no sweep increment");
     return sa_vr_steps(c, nsweeps, st(s));
@@ -1174,6 +1209,7 @@ int dndsg_vr_jacobi_step(dndsg_ctx* c, int nsweeps, double* inc_out, void* s) {
 
 int dndsg_limiter_wbap(dndsg_ctx* c, int if_all, double* indicator_out, void* s) {
   if (!c) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   if (!c->limFace) return fail(c, DNDSG_UNSUPPORTED, "context was created without the limiter (settings.limiter = 0)");
   if (c->fp32) run_limiter<float>(c, if_all, st(s));
   else run_limiter<double>(c, if_all, st(s));
@@ -1188,6 +1224,7 @@ int dndsg_limiter_wbap(dndsg_ctx* c, int if_all, double* indicator_out, void* s)
 
 int dndsg_eval_dt(dndsg_ctx* c, double cfl, double max_dt, int use_local_dt, double* dt_min_out, void* s) {
   if (!c) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   if (c->sa) {
     int rc0 = sa_eval_dt(c, cfl, max_dt, st(s));
     if (rc0) return rc0;
@@ -1207,6 +1244,7 @@ int dndsg_eval_dt(dndsg_ctx* c, double cfl, double max_dt, int use_local_dt, dou
 
 int dndsg_eval_rhs(dndsg_ctx* c, double t, double* rhs_out, void* s) {
   if (!c) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   if (c->sa) {
     int rc0 = sa_eval_rhs(c, st(s));
     if (rc0) return rc0;
@@ -1235,6 +1273,7 @@ int dndsg_eval_rhs(dndsg_ctx* c, double t, double* rhs_out, void* s) {
 
 int dndsg_ssprk3_step(dndsg_ctx* c, double cfl, double t_end, void* s) {
   if (!c) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   if (c->sa) return fail(c, DNDSG_UNSUPPORTED, "SA contexts run the implicit path (dndsg_implicit_iteration)");
   if (c->fp32) run_step<float>(c, cfl, t_end, st(s));
   else run_step<double>(c, cfl, t_end, st(s));
@@ -1246,6 +1285,7 @@ int dndsg_ssprk3_step(dndsg_ctx* c, double cfl, double t_end, void* s) {
 // (on a private stream) the first time a cfl / t_end / buffer parity is seen and kept.
 int dndsg_ssprk3_steps(dndsg_ctx* c, double cfl, double t_end, int64_t n, void* s) {
   if (!c || n < 0) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   if (c->sa) return fail(c, DNDSG_UNSUPPORTED, "SA contexts run the implicit path (dndsg_implicit_iteration)");
   int rc;
   if ((rc = set_device(c))) return rc;
@@ -1290,8 +1330,12 @@ int dndsg_ssprk3_steps(dndsg_ctx* c, double cfl, double t_end, int64_t n, void* 
 // ---- partitioned runs: owned-cell mask, SSP-RK3 by stage, halo pack / unpack
 int dndsg_set_owned(dndsg_ctx* c, const uint8_t* owned) {
   if (!c) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   int rc;
   if ((rc = set_device(c))) return rc;
+  // work queued earlier on any stream (a caller's non-blocking stream included) may still read the
+  // mask or replay a step graph: let it finish before either changes
+  DG_CUDA(c, cudaDeviceSynchronize());
   // the step graphs of dndsg_ssprk3_steps hold the mask pointer of their capture: recapture
   for (auto& g : c->stepGraph) {
     if (g.exec) cudaGraphExecDestroy(g.exec);
@@ -1309,6 +1353,7 @@ int dndsg_set_owned(dndsg_ctx* c, const uint8_t* owned) {
 
 int dndsg_rk_dt(dndsg_ctx* c, double cfl, double* dt_min_out, void* s) {
   if (!c || !dt_min_out || !(cfl > 0)) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   if (c->sa) return fail(c, DNDSG_UNSUPPORTED, "SA contexts run the implicit path");
   int rc;
   if ((rc = set_device(c))) return rc;
@@ -1324,6 +1369,7 @@ int dndsg_rk_dt(dndsg_ctx* c, double cfl, double* dt_min_out, void* s) {
 
 int dndsg_rk_set_dt(dndsg_ctx* c, double dt, void* s) {
   if (!c || !(dt >= 0)) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   int rc;
   if ((rc = set_device(c))) return rc;
   DG_CUDA(c, cudaMemcpyAsync(c->scal + S_DT, &dt, sizeof(double), cudaMemcpyHostToDevice, st(s)));
@@ -1333,6 +1379,7 @@ int dndsg_rk_set_dt(dndsg_ctx* c, double dt, void* s) {
 
 int dndsg_rk_vr(dndsg_ctx* c, void* s) {
   if (!c) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   if (c->fp32) run_vr<float>(c, false, st(s));
   else run_vr<double>(c, false, st(s));
   return check_launch(c);
@@ -1340,6 +1387,7 @@ int dndsg_rk_vr(dndsg_ctx* c, void* s) {
 
 int dndsg_rk_limit(dndsg_ctx* c, void* s) {
   if (!c) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   if (!c->s.limiter) return 0;
   if (c->fp32) run_limiter<float>(c, 0, st(s));
   else run_limiter<double>(c, 0, st(s));
@@ -1348,6 +1396,7 @@ int dndsg_rk_limit(dndsg_ctx* c, void* s) {
 
 int dndsg_rk_stage(dndsg_ctx* c, int stage, void* s) {
   if (!c || stage < 0 || stage > 2) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   if (c->fp32) run_rk_stage<float>(c, stage, st(s));
   else run_rk_stage<double>(c, stage, st(s));
   return check_launch(c);
@@ -1355,6 +1404,7 @@ int dndsg_rk_stage(dndsg_ctx* c, int stage, void* s) {
 
 int dndsg_rk_finish(dndsg_ctx* c, void* s) {
   if (!c) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   k_advance_time<<<1, 1, 0, st(s)>>>(c->scal);
   return check_launch(c);
 }
@@ -1362,6 +1412,7 @@ int dndsg_rk_finish(dndsg_ctx* c, void* s) {
 int dndsg_halo_pack(dndsg_ctx* c, int what, const int32_t* cells, int64_t n, void* buf, void* s) {
   if (!c || (what != DNDSG_HALO_U && what != DNDSG_HALO_UREC) || n < 0 || (n && (!cells || !buf)))
     return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   if (n == 0) return 0;
   const int w = what == DNDSG_HALO_U ? 4 : 20;
   if (what == DNDSG_HALO_U)
@@ -1376,6 +1427,7 @@ int dndsg_halo_pack(dndsg_ctx* c, int what, const int32_t* cells, int64_t n, voi
 int dndsg_halo_unpack(dndsg_ctx* c, int what, const int32_t* cells, int64_t n, const void* buf, void* s) {
   if (!c || (what != DNDSG_HALO_U && what != DNDSG_HALO_UREC) || n < 0 || (n && (!cells || !buf)))
     return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   if (n == 0) return 0;
   const int w = what == DNDSG_HALO_U ? 4 : 20;
   if (what == DNDSG_HALO_U)
@@ -1389,6 +1441,7 @@ int dndsg_halo_unpack(dndsg_ctx* c, int what, const int32_t* cells, int64_t n, c
 
 int dndsg_residual(dndsg_ctx* c, int p, int vol_wise, double* out, void* s) {
   if (!c || !out) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   unsigned nb = grid_for(c->N);
   k_residual<<<nb, kBlock, 0, st(s)>>>(c->rhs, c->vol, c->N, p, vol_wise, c->partial, c->owned);
   int rc = check_launch(c);
@@ -1418,6 +1471,7 @@ int dndsg_residual(dndsg_ctx* c, int p, int vol_wise, double* out, void* s) {
 
 int dndsg_face_values(dndsg_ctx* c, double t, double* out, void* s) {
   if (!c || !out) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   if (c->sa) return fail(c, DNDSG_UNSUPPORTED, "face values are reported for 4-variable contexts");
   double* d;
   size_t bytes = sizeof(double) * 24 * c->F;
@@ -1445,6 +1499,10 @@ int dndsg_get_status(dndsg_ctx* c, uint32_t* flags, uint64_t* n_reduced, void* s
   DG_CUDA(c, cudaStreamSynchronize(st(s)));
   if (flags) *flags = f;
   if (n_reduced) *n_reduced = r;
+  if (f & kFlagTimeout) {
+    c->dead = true;
+    return fail(c, DNDSG_TIMEOUT, "a bounded wait in a kernel ran out (timeout flag); the context refuses further work");
+  }
   return 0;
 }
 
@@ -1466,12 +1524,17 @@ constexpr int64_t kNoAllocMaxFaces = DNDSG_NOALLOC_MAX_FACES;
 static __device__ __align__(256) double g_noalloc_flux[kNoAllocMaxFaces * 4];
 constexpr int kMaxDevices = 64;
 double* g_noalloc_ptr[kMaxDevices] = {nullptr};
+std::mutex g_noalloc_mutex;
 
 // Host code must not pass g_noalloc_flux itself to a kernel (on the host it is
 // only a stand-in symbol); the device address comes from cudaGetSymbolAddress,
-// once per device, with that device current.
+// once per device, with that device current.  The lookup is serialised, so two
+// host threads making their first call on one device at the same time look it
+// up once.  A device reset (cudaDeviceReset) invalidates the cached address;
+// the library does not support calls after one.
 int noalloc_scratch(dndsg_ctx* c, double** out) {
   if (c->device < 0 || c->device >= kMaxDevices) return fail(c, DNDSG_BAD_ARGUMENT, "device index out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
   if (!g_noalloc_ptr[c->device]) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_flux);
@@ -1483,6 +1546,8 @@ int noalloc_scratch(dndsg_ctx* c, double** out) {
   return 0;
 }
 
+// the kernels of dndsg_eval_rhs (face fluxes, then the gather into rhs) over the caller's arrays,
+// with the face fluxes in the scratch array
 template <class T>
 void run_rhs_noalloc(dndsg_ctx* c, const double* u, const void* urec, double* rhs, double* scratch, double t,
                      cudaStream_t s) {
@@ -1491,16 +1556,11 @@ void run_rhs_noalloc(dndsg_ctx* c, const double* u, const void* urec, double* rh
   h.urec = (const T*)urec;
   h.rhs = rhs;
   h.flux = scratch;
-  const int64_t Fi = c->Fi, F = c->F;
-  if (c->s.riemann == 2) {
-    if (Fi > 0) k_face_flux<T, 2, false><<<grid_for(Fi), kBlock, 0, s>>>(h, 0, Fi, c->scal, 0, t, 0.0, c->flags, c->nreduced);
-    if (F > Fi) k_face_flux<T, 2, true><<<grid_for(F - Fi), kBlock, 0, s>>>(h, Fi, F, c->scal, 0, t, 0.0, c->flags, c->nreduced);
-  } else {
-    if (Fi > 0) k_face_flux<T, 1, false><<<grid_for(Fi), kBlock, 0, s>>>(h, 0, Fi, c->scal, 0, t, 0.0, c->flags, c->nreduced);
-    if (F > Fi) k_face_flux<T, 1, true><<<grid_for(F - Fi), kBlock, 0, s>>>(h, Fi, F, c->scal, 0, t, 0.0, c->flags, c->nreduced);
-  }
+  launch_flux_h<T>(c, h, 0, t, 0.0, s);
   k_cell_update<T, -1><<<grid_for(c->N), kBlock, 0, s>>>(h, c->scal);
 }
+
+bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 }  // namespace
 
 extern "C" int dndsg_eval_rhs_noalloc(dndsg_ctx* c, const double* u, const void* urec, double* rhs, double t,
@@ -1508,6 +1568,10 @@ extern "C" int dndsg_eval_rhs_noalloc(dndsg_ctx* c, const double* u, const void*
   if (c && (c->s.mu_gas > 0 || c->sa))
     return fail(c, DNDSG_UNSUPPORTED, "the allocation-free RHS covers the inviscid model only (mu_gas = 0)");
   if (!c || !u || !urec || !rhs) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
+  // the kernels read and write these arrays in 16-byte vectors
+  if (!aligned16(u) || !aligned16(urec) || !aligned16(rhs))
+    return fail(c, DNDSG_BAD_ARGUMENT, "dndsg_eval_rhs_noalloc: u, urec and rhs must be 16-byte aligned");
   if (c->F > kNoAllocMaxFaces)
     return fail(c, DNDSG_BAD_ARGUMENT,
                 "dndsg_eval_rhs_noalloc: mesh has " + std::to_string(c->F) + " faces, more than its scratch limit of " +
@@ -1828,7 +1892,7 @@ int dndsg_mlp_forward(dndsg_mlp* m, const float* X, int64_t n, float* Y, void* s
   unsigned f = 0;  // a tensor-core completion that timed out (the bounded wait ran out)
   DG_MCUDA(m, cudaMemcpyAsync(&f, m->flags, sizeof(f), cudaMemcpyDeviceToHost, st(s)));
   DG_MCUDA(m, cudaStreamSynchronize(st(s)));
-  if (f) return mfail(m, DNDSG_CUDA_ERROR, "tensor-core completion wait timed out");
+  if (f) return mfail(m, DNDSG_TIMEOUT, "tensor-core completion wait timed out");
   return 0;
 }
 
@@ -1868,7 +1932,7 @@ int dndsg_mlp_gradient(dndsg_mlp* m, const float* X, const float* Tg, int64_t n,
   unsigned f = 0;
   DG_MCUDA(m, cudaMemcpyAsync(&f, m->flags, sizeof(f), cudaMemcpyDeviceToHost, st(s)));
   DG_MCUDA(m, cudaStreamSynchronize(st(s)));
-  if (f) return mfail(m, DNDSG_CUDA_ERROR, "tensor-core completion wait timed out");
+  if (f) return mfail(m, DNDSG_TIMEOUT, "tensor-core completion wait timed out");
   if (loss) *loss = l / (double)(n * kOut);
   return 0;
 }
@@ -1896,6 +1960,7 @@ int dndsg_mlp_train_step(dndsg_mlp* m, const float* X, const float* Tg, int64_t 
 
 int dndsg_mlp_features(dndsg_ctx* c, float* X, float* scales, void* s) {
   if (!c || !X || !scales) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   if (c->sa) return fail(c, DNDSG_UNSUPPORTED, "the learned warm start is for 4-variable contexts");
   int rc = c->fp32 ? ensure_mlp_buffers<float>(c) : ensure_mlp_buffers<double>(c);
   if (rc) return rc;
@@ -1917,19 +1982,23 @@ int dndsg_mlp_features(dndsg_ctx* c, float* X, float* scales, void* s) {
 int dndsg_vr_to_tolerance(dndsg_ctx* c, const dndsg_mlp* m, double tol, int max_sweeps, int* sweeps_out,
                           int64_t* accepted_out, float* harvest_x, float* harvest_t, void* s) {
   if (!c || max_sweeps < 1 || !(tol >= 0)) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   if (c->sa) return fail(c, DNDSG_UNSUPPORTED, "the learned warm start is for 4-variable contexts");
   if (m && m->device != c->device) return fail(c, DNDSG_BAD_ARGUMENT, "network and context on different devices");
-  return c->fp32 ? vr_to_tol<float>(c, m, tol, max_sweeps, sweeps_out, accepted_out, harvest_x, harvest_t, st(s))
-                 : vr_to_tol<double>(c, m, tol, max_sweeps, sweeps_out, accepted_out, harvest_x, harvest_t, st(s));
+  int rc = c->fp32 ? vr_to_tol<float>(c, m, tol, max_sweeps, sweeps_out, accepted_out, harvest_x, harvest_t, st(s))
+                   : vr_to_tol<double>(c, m, tol, max_sweeps, sweeps_out, accepted_out, harvest_x, harvest_t, st(s));
+  return rc ? rc : observe_timeout(c, st(s));
 }
 
 int dndsg_ssprk3_step_tol(dndsg_ctx* c, const dndsg_mlp* m, double cfl, double t_end, double tol, int max_sweeps,
                           int* sweeps_out, float* harvest_x, float* harvest_t, void* s) {
   if (!c || max_sweeps < 1 || !(tol >= 0)) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   if (c->sa) return fail(c, DNDSG_UNSUPPORTED, "the learned warm start is for 4-variable contexts");
   if (m && m->device != c->device) return fail(c, DNDSG_BAD_ARGUMENT, "network and context on different devices");
-  return c->fp32 ? run_step_tol<float>(c, m, cfl, t_end, tol, max_sweeps, sweeps_out, harvest_x, harvest_t, st(s))
-                 : run_step_tol<double>(c, m, cfl, t_end, tol, max_sweeps, sweeps_out, harvest_x, harvest_t, st(s));
+  int rc = c->fp32 ? run_step_tol<float>(c, m, cfl, t_end, tol, max_sweeps, sweeps_out, harvest_x, harvest_t, st(s))
+                   : run_step_tol<double>(c, m, cfl, t_end, tol, max_sweeps, sweeps_out, harvest_x, harvest_t, st(s));
+  return rc ? rc : observe_timeout(c, st(s));
 }
 
 }  // extern "C"
@@ -2642,6 +2711,7 @@ extern "C" {
 
 int dndsg_lusgs_colours(dndsg_ctx* c, int32_t* colour_out, int* n_colours) {
   if (!c) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   int rc;
   if ((rc = set_device(c)) || (rc = ensure_lusgs(c))) return rc;
   if (colour_out) std::memcpy(colour_out, c->colourHost.data(), sizeof(int32_t) * c->N);
@@ -2651,6 +2721,7 @@ int dndsg_lusgs_colours(dndsg_ctx* c, int32_t* colour_out, int* n_colours) {
 
 int dndsg_lusgs_set_order(dndsg_ctx* c, int mode, const int64_t* scan2cell, int* n_batches) {
   if (!c || (mode != 0 && mode != 1)) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   int rc;
   if ((rc = set_device(c)) || (rc = ensure_lusgs(c))) return rc;
   if (mode == 1) {
@@ -2672,6 +2743,7 @@ int dndsg_lusgs_set_order(dndsg_ctx* c, int mode, const int64_t* scan2cell, int*
 
 int dndsg_lusgs_matrix_init(dndsg_ctx* c, double dt_phys, double alpha, void* s) {
   if (!c || !(dt_phys > 0) || !(alpha > 0)) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   int rc;
   if ((rc = set_device(c)) || (rc = ensure_lusgs(c))) return rc;
   if (c->fp32) k_lusgs_init<float><<<grid_for(c->N), kBlock, 0, st(s)>>>(view<float>(c), 1.0 / dt_phys, alpha, c->Dinv, c->Dmat);
@@ -2681,6 +2753,7 @@ int dndsg_lusgs_matrix_init(dndsg_ctx* c, double dt_phys, double alpha, void* s)
 
 static int lusgs_sweep_api(dndsg_ctx* c, bool fwd, double alpha, const double* rhs, double* inc, void* s) {
   if (!c || !rhs || !inc) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   if (c->sa) return fail(c, DNDSG_UNSUPPORTED, "SA contexts sweep inside dndsg_implicit_iteration");
   if (!c->rankOf) return fail(c, DNDSG_BAD_ARGUMENT, "dndsg_lusgs_matrix_init first");
   int rc;
@@ -2700,6 +2773,7 @@ int dndsg_lusgs_backward(dndsg_ctx* c, double alpha, const double* rhs, double* 
 
 int dndsg_bdf_begin(dndsg_ctx* c, void* s) {
   if (!c) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   int rc;
   if ((rc = set_device(c))) return rc;
   DG_CUDA(c, cudaMemcpyAsync(c->uLast, c->u, sizeof(double) * 4 * c->N, cudaMemcpyDeviceToDevice, st(s)));
@@ -2710,6 +2784,7 @@ int dndsg_bdf_begin(dndsg_ctx* c, void* s) {
 int dndsg_implicit_iteration(dndsg_ctx* c, double cfl, double dt_phys, double alpha, int n_rec, int vol_wise,
                              double t, double* inc_res_out, double* wall_flux_out, void* s) {
   if (!c || !(cfl > 0) || !(dt_phys > 0) || !(alpha > 0) || n_rec < 0) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   int rc;
   if ((rc = set_device(c))) return rc;
   if (c->sa) rc = sa_implicit(c, cfl, dt_phys, alpha, n_rec, vol_wise, st(s));
@@ -2727,6 +2802,7 @@ int dndsg_implicit_iteration(dndsg_ctx* c, double cfl, double dt_phys, double al
       if (inc_res_out) inc_res_out[4] = acc[8];
       if (wall_flux_out) wall_flux_out[4] = acc[9];
     }
+    return observe_timeout(c, st(s));
   }
   return 0;
 }

@@ -520,6 +520,72 @@ int dual_step(dndsg_ctx* c, const DualOpts& o, double dt, double t, int* itersOu
   return check_launch(c);
 }
 
+// The steady internal loop of EulerSolver with ifSteadyQuit: first-order BDF pseudo-time
+// iterations (DNDS_ODE.hpp:444-486) with the fstop lambda's CFL ramp (DNDS_FV_EulerSolver.hpp:
+// 1047-1052), until the density fstop ratio drops below the threshold
+template <class T>
+int steady_solve(dndsg_ctx* c, const dndsg_steady_settings* st, int* itersOut, double* resOut, double* wallOut,
+                 double* hist, cudaStream_t s) {
+  DualOpts o{DNDSG_DUAL_BDF, 1, st->cfl, st->max_iter, st->threshold, st->n_rec, st->vol_wise,
+             st->gmres_code, st->n_gmres_space, st->n_gmres_iter};
+  int rc;
+  if ((rc = ensure_dual(c, o))) return rc;
+  const int64_t N = c->N, n = 4 * N;
+  const bool sa = c->sa;
+  const double dt = st->dt;
+  DG_CUDA(c, cudaMemcpyAsync(c->uLast, c->u, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  if (sa) DG_CUDA(c, cudaMemcpyAsync(c->saULast, c->saU, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
+  Fstop f;
+  double cflNow = st->cfl, acc[16] = {0};
+  int iter = 1;
+  for (; iter <= st->max_iter; iter++) {
+    o.cfl = cflNow;
+    dual_frhs<T>(c, o, 0.0, s);
+    VecList X{};
+    X.p[0] = c->uLast;
+    X.a[0] = 1.0 / dt;
+    k_dual_bdf_rhs<<<vgrid(n), kBlock, 0, s>>>(n, c->u, 1.0, -1. / dt, X, 1, c->rhs);
+    if (sa) {
+      VecList X5{};
+      X5.p[0] = c->saULast;
+      X5.a[0] = 1.0 / dt;
+      k_dual_bdf_rhs<<<vgrid(N), kBlock, 0, s>>>(N, c->saU, 1.0, -1. / dt, X5, 1, c->saRhs);
+    }
+    if ((rc = dual_fsolve<T>(c, o, dt, 1.0, s))) return rc;
+    // x += inc with the increment norms, and the wall force of this iteration's residual
+    DG_CUDA(c, cudaMemsetAsync(c->resAcc, 0, sizeof(double) * 16, s));
+    k_add_inc<<<grid_for(N), kBlock, 0, s>>>(N, c->u, c->inc, c->vol, o.volWise, c->resAcc);
+    if (sa) k_sa_add_inc<<<grid_for(N), kBlock, 0, s>>>(N, c->saU, c->saInc, c->vol, o.volWise, c->resAcc + 8);
+    if (c->F > c->Fi) {
+      k_wall_flux<<<grid_for(c->F - c->Fi), kBlock, 0, s>>>(c->Fi, c->F, c->faceBC, c->flux, c->resAcc + 4);
+      if (sa) k_sa_wall_flux<<<grid_for(c->F - c->Fi), kBlock, 0, s>>>(c->Fi, c->F, c->faceBC, c->saFlux, c->resAcc + 9);
+    }
+    DG_CUDA(c, cudaMemcpyAsync(acc, c->resAcc, sizeof(acc), cudaMemcpyDeviceToHost, s));
+    DG_CUDA(c, cudaStreamSynchronize(s));
+    if ((rc = check_launch(c))) return rc;
+    const double res[5] = {acc[0], acc[1], acc[2], acc[3], acc[8]};
+    for (int v = 0; v < (sa ? 5 : 4); v++) {
+      f.base[v] = iter == 1 ? res[v] : std::max(f.base[v], res[v]);
+      f.rel[v] = res[v] / f.base[v];
+    }
+    if (hist) hist[iter - 1] = f.rel[0];
+    if (!(res[0] == res[0])) return fail(c, DNDSG_NUMERIC_ERROR, "steady solve: NaN increment");
+    if (f.rel[0] < st->threshold) break;
+    if (iter >= st->cfl_ramp_start && iter <= st->cfl_ramp_start + st->cfl_ramp_length && st->cfl_ramp_length > 0) {
+      const double inter = double(iter - st->cfl_ramp_start) / st->cfl_ramp_length;
+      cflNow = std::exp(std::log(st->cfl) + std::log(st->cfl_ramp_end / st->cfl) * inter);
+    }
+  }
+  if (itersOut) *itersOut = std::min(iter, st->max_iter);
+  if (resOut)
+    for (int v = 0; v < (sa ? 5 : 4); v++) resOut[v] = f.rel[v];
+  if (wallOut) {
+    for (int v = 0; v < 4; v++) wallOut[v] = acc[4 + v];
+    if (sa) wallOut[4] = acc[9];
+  }
+  return 0;
+}
+
 int dual_opts(dndsg_ctx* c, const dndsg_dual_settings* d, DualOpts& o) {
   if (!d) return DNDSG_BAD_ARGUMENT;
   o = DualOpts{d->scheme, d->bdf_order, d->cfl, d->max_iter, d->threshold, d->n_rec, d->vol_wise,
@@ -541,6 +607,7 @@ extern "C" {
 
 int dndsg_dual_reset(dndsg_ctx* c) {
   if (!c) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   c->odeCnPrev = 0;
   c->odePrevStart = 0;
   c->odeOrder = 0;
@@ -551,6 +618,7 @@ int dndsg_dual_reset(dndsg_ctx* c) {
 int dndsg_dual_step(dndsg_ctx* c, const dndsg_dual_settings* d, double dt, double t, int* iters_out, double* res_out,
                     void* s) {
   if (!c || !(dt > 0)) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   DualOpts o;
   int rc;
   if ((rc = dual_opts(c, d, o)) || (rc = set_device(c))) return rc;
@@ -559,12 +627,30 @@ int dndsg_dual_step(dndsg_ctx* c, const dndsg_dual_settings* d, double dt, doubl
     c->odePrevStart = o.order - 2 > 0 ? o.order - 2 : 0;
     c->odeOrder = o.order;
   }
-  return c->fp32 ? dual_step<float>(c, o, dt, t, iters_out, res_out, st(s))
-                 : dual_step<double>(c, o, dt, t, iters_out, res_out, st(s));
+  rc = c->fp32 ? dual_step<float>(c, o, dt, t, iters_out, res_out, st(s))
+              : dual_step<double>(c, o, dt, t, iters_out, res_out, st(s));
+  return rc ? rc : observe_timeout(c, st(s));
+}
+
+int dndsg_steady_solve(dndsg_ctx* c, const dndsg_steady_settings* ss, int* iters_out, double* res_out,
+                       double* wall_flux_out, double* history, void* s) {
+  if (!c || !ss) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
+  if (!(ss->cfl > 0) || !(ss->cfl_ramp_end > 0) || ss->max_iter < 1 || !(ss->dt > 0) || ss->n_rec < 0 ||
+      ss->gmres_code < 0 || ss->gmres_code > 2 || ss->cfl_ramp_length < 0 ||
+      (ss->gmres_code != 0 && (ss->n_gmres_space < 1 || ss->n_gmres_space > kMaxKrylov || ss->n_gmres_iter < 0)))
+    return fail(c, DNDSG_BAD_ARGUMENT, "steady settings: cfl, cfl_ramp_end, dt > 0; max_iter >= 1; n_rec >= 0; "
+                                       "gmres_code 0..2 with n_gmres_space 1..32");
+  int rc;
+  if ((rc = set_device(c))) return rc;
+  rc = c->fp32 ? steady_solve<float>(c, ss, iters_out, res_out, wall_flux_out, history, st(s))
+               : steady_solve<double>(c, ss, iters_out, res_out, wall_flux_out, history, st(s));
+  return rc ? rc : observe_timeout(c, st(s));
 }
 
 int dndsg_gmres_lusgs(dndsg_ctx* c, double alpha, int n_space, int n_restart, const double* b, double* x, void* s) {
   if (!c || !b || !x || n_space < 1 || n_space > kMaxKrylov || n_restart < 0) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   if (c->sa) return fail(c, DNDSG_UNSUPPORTED, "4-variable contexts");
   if (!c->rankOf) return fail(c, DNDSG_BAD_ARGUMENT, "dndsg_lusgs_matrix_init first");
   DualOpts o{DNDSG_DUAL_BDF, 1, 1.0, 1, 0.0, 0, 0, 1, n_space, n_restart};
@@ -576,6 +662,7 @@ int dndsg_gmres_lusgs(dndsg_ctx* c, double alpha, int n_space, int n_restart, co
 
 int dndsg_lusgs_matvec(dndsg_ctx* c, double alpha, const double* x, double* ax, void* s) {
   if (!c || !x || !ax) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
   if (c->sa) return fail(c, DNDSG_UNSUPPORTED, "4-variable contexts");
   if (!c->rankOf) return fail(c, DNDSG_BAD_ARGUMENT, "dndsg_lusgs_matrix_init first");
   int rc;

@@ -148,8 +148,14 @@ class PartitionedRun:
         return out
 
     def exchange(self, what: int):
-        """Ghost values from their owners: pack on the owner, unpack on the holder."""
+        """Ghost values from their owners: pack on the owner, unpack on the holder.  The pack and
+        the unpack are ordered only by their stream: every part must run on one stream (the
+        solvers here use the legacy default stream), which is checked."""
         import torch
+
+        streams = {s.stream.value if s.stream else None for s in self.solvers}
+        if len(streams) != 1:
+            raise ValueError("PartitionedRun.exchange needs every part on one stream")
 
         w = 4 if what == 0 else 20
         for (pi, q), (recv, send) in self._lists.items():

@@ -233,6 +233,29 @@ class Solver:
         self._check(self.L.dndsg_gmres_lusgs(self.h, float(alpha_diag), int(n_space), int(n_restart),
                                              C.c_void_p(b_ptr), C.c_void_p(x_ptr), self.stream))
 
+    def steady_run(self, cfl: float = 100.0, threshold: float = 1e-8, max_iter: int = 10000, dt: float = 1e100,
+                   cfl_ramp_start: int = 10**9, cfl_ramp_length: int = 0, cfl_ramp_end: float | None = None,
+                   gmres_code: int = 0, n_gmres_space: int = 10, n_gmres_iter: int = 2, n_rec: int = 1,
+                   vol_wise: bool = False, history: bool = False):
+        """The steady internal loop of EulerSolver with ifSteadyQuit in one C call (dndsg_steady_solve):
+        first-order BDF pseudo time with the CFL ramp of fstop and fsolve per gmresCode, until the
+        density increment ratio drops below threshold.  Returns (iterations, fstop ratios, wall flux,
+        density ratio per iteration or None)."""
+        from ._lib import SteadySettings
+
+        st = SteadySettings(cfl=float(cfl), cfl_ramp_end=float(cfl if cfl_ramp_end is None else cfl_ramp_end),
+                            cfl_ramp_start=int(cfl_ramp_start), cfl_ramp_length=int(cfl_ramp_length),
+                            max_iter=int(max_iter), threshold=float(threshold), dt=float(dt), n_rec=int(n_rec),
+                            vol_wise=int(vol_wise), gmres_code=int(gmres_code), n_gmres_space=int(n_gmres_space),
+                            n_gmres_iter=int(n_gmres_iter))
+        it = C.c_int()
+        rel = np.zeros(self.nv)
+        wf = np.zeros(self.nv)
+        hist = np.zeros(max_iter) if history else None
+        self._check(self.L.dndsg_steady_solve(self.h, C.byref(st), C.byref(it), _p(rel), _p(wf),
+                                              _p(hist) if history else None, self.stream))
+        return it.value, rel, wf, (hist[: it.value] if history else None)
+
     def steady_solve(self, cfl: float, threshold: float = 1e-8, max_iter: int = 10000, dt: float = 1e100,
                      n_rec: int = 1, vol_wise: bool = False, history: list | None = None):
         """Pseudo-time iterations until the density component of the increment norm, relative to its
@@ -291,13 +314,19 @@ class Solver:
         return f.value, n.value
 
     def run_to(self, t_end: float, cfl: float, max_steps: int = 10**9) -> int:
-        """SSP-RK3 steps until the device clock reaches t_end (last step clipped)."""
+        """SSP-RK3 steps until the device clock reaches t_end (last step clipped); returns the steps
+        taken.  Steps go in batches of at most half the remaining steps at the last batch's mean dt
+        (at most 64), so the host reads the clock rarely and no zero-length step is run or counted."""
         steps = 0
-        chunk = 16
-        while steps < max_steps:
-            for _ in range(min(chunk, max_steps - steps)):
+        t = self.time
+        dts = 0.0
+        while steps < max_steps and t < t_end - 1e-12 * max(1.0, abs(t_end)):
+            k = int(min(64, max(1, 0.5 * (t_end - t) / dts))) if dts > 0 else 1
+            k = min(k, max_steps - steps)
+            for _ in range(k):
                 self.ssprk3_step(cfl, t_end)
-                steps += 1
-            if self.time >= t_end - 1e-12:
-                break
+            t_new = self.time
+            dts = (t_new - t) / k
+            steps += k
+            t = t_new
         return steps

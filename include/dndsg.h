@@ -28,7 +28,9 @@ enum dndsg_status {
   DNDSG_CUDA_ERROR = 2,
   DNDSG_UNSUPPORTED = 3,
   DNDSG_NUMERIC_ERROR = 4, /* NaN / non-positive state seen by a kernel */
-  DNDSG_SETUP_ERROR = 5    /* degenerate mesh or singular VR matrix */
+  DNDSG_SETUP_ERROR = 5,   /* degenerate mesh or singular VR matrix */
+  DNDSG_TIMEOUT = 6        /* a bounded wait inside a kernel ran out: the kernel skipped its work,
+                              and the context refuses every later call (destroy it) */
 };
 
 /* Mesh topology and geometry.  Replaces CompactFacedMeshSerialRW
@@ -187,12 +189,20 @@ int dndsg_face_values(dndsg_ctx* ctx, double t, double* out, void* stream);
  * before any stream capture.  All calls share the one scratch array: calls
  * that overlap on the GPU (different streams or contexts at the same time)
  * race and must be serialised by the caller.  The Roe entropy fix uses the
- * face data of the context's last dndsg_eval_dt, as dndsg_eval_rhs does. */
+ * face data of the context's last dndsg_eval_dt, as dndsg_eval_rhs does.
+ * u, urec and rhs must be 16-byte aligned (the kernels move them in 16-byte
+ * vectors; cudaMalloc'd arrays are); other pointers are rejected with
+ * DNDSG_BAD_ARGUMENT before anything is launched. */
 #define DNDSG_NOALLOC_MAX_FACES 262144
 int dndsg_eval_rhs_noalloc(dndsg_ctx* ctx, const double* u, const void* urec, double* rhs, double t, void* stream);
 
 /* Error flags raised by kernels since the last call (bit 0: NaN or
- * non-positive density/pressure in a flux; bit 1: reduced-order face point). */
+ * non-positive density/pressure in a flux; bit 1: reduced-order face point;
+ * bit 2: a bounded wait inside a kernel ran out).  Bit 2 makes this call, and
+ * every later call on the context, return DNDSG_TIMEOUT; so do the calls that
+ * read results back from the device (dndsg_get_u, dndsg_get_time,
+ * dndsg_implicit_iteration, dndsg_dual_step, dndsg_vr_to_tolerance,
+ * dndsg_ssprk3_step_tol) when they see it. */
 int dndsg_get_status(dndsg_ctx* ctx, uint32_t* flags, uint64_t* n_reduced, void* stream);
 
 /* ---------------------------------------------------------------------------
@@ -245,7 +255,9 @@ int dndsg_implicit_iteration(dndsg_ctx* ctx, double cfl, double dt_phys, double 
  * exactly as the whole mesh would, given the ghosts' values after every VR
  * sweep (and limiter) and every stage update.  dndsg_set_owned marks the owned
  * cells (host [n_cells] 0/1; NULL: all owned): the dt minimum and
- * dndsg_residual run over owned cells only.  One SSP-RK3 step by stage
+ * dndsg_residual run over owned cells only.  It first waits for all work on
+ * the device (cudaDeviceSynchronize), so steps queued before it on any stream
+ * see the old mask and steps after it the new one.  One SSP-RK3 step by stage
  * (ExplicitSSPRK3LocalDt::Step, DNDS_ODE.hpp:131-177):
  *   dndsg_rk_dt (local minimum; the caller reduces it over all partitions and
  *   clips it to the end time) -> dndsg_rk_set_dt -> 3 x [dndsg_rk_vr ->
@@ -308,6 +320,38 @@ int dndsg_dual_reset(dndsg_ctx* ctx);
  * with another dt is an error (the reference asserts a constant dt). */
 int dndsg_dual_step(dndsg_ctx* ctx, const dndsg_dual_settings* settings, double dt, double t, int* iters_out,
                     double* res_out, void* stream);
+
+/* Steady solve: the internal loop of one implicit step of the reference's
+ * EulerSolver run with ifSteadyQuit (DNDS_FV_EulerSolver.hpp:609-615,
+ * 713-1061; ImplicitBDFDualTimeStep::Step of order 1, DNDS_ODE.hpp:444-486)
+ * until fstop: each iteration is fdtau (EvaluateDt at the current CFL, local
+ * dt), frhs (n_rec VR sweeps, [limiter], EvaluateRHS), the first-order BDF
+ * right-hand side with physical step dt (1e100: steady), fsolve per
+ * gmres_code as in dndsg_dual_step, and u += inc.  fstop: the L1 increment
+ * norm (volume-weighted when vol_wise) over its running maximum; the loop ends
+ * when the density entry drops below threshold or after max_iter iterations.
+ * The CFL ramp of fstop: between iterations cfl_ramp_start and
+ * cfl_ramp_start + cfl_ramp_length the CFL moves log-linearly from cfl to
+ * cfl_ramp_end and then stays there (nCFLRampStart, nCFLRampLength,
+ * CFLRampEnd).  Outputs (host, each may be NULL): iters_out; res_out [nvars]
+ * the last fstop ratios; wall_flux_out [nvars] fluxWallSum of the last
+ * residual; history [max_iter] the density fstop ratio of every iteration. */
+typedef struct dndsg_steady_settings {
+  double cfl;          /* CFL */
+  double cfl_ramp_end; /* CFLRampEnd */
+  int cfl_ramp_start;  /* nCFLRampStart (a large value: no ramp) */
+  int cfl_ramp_length; /* nCFLRampLength */
+  int max_iter;        /* nTimeStepInternal */
+  double threshold;    /* rhsThresholdInternal */
+  double dt;           /* dtImplicit (1e100: steady) */
+  int n_rec;           /* nInternalRecStep */
+  int vol_wise;        /* useVolWiseResidual */
+  int gmres_code;      /* 0, 1, 2 */
+  int n_gmres_space;   /* nGmresSpace */
+  int n_gmres_iter;    /* nGmresIter */
+} dndsg_steady_settings;
+int dndsg_steady_solve(dndsg_ctx* ctx, const dndsg_steady_settings* settings, int* iters_out, double* res_out,
+                       double* wall_flux_out, double* history, void* stream);
 /* GMRES_LeftPreconditioned::solve (DNDS_Linear.hpp:47-105) of LUSGSMatrixVec x = b,
  * the LU-SGS forward + backward sweeps as left preconditioner, n_space Krylov
  * vectors (1..32), n_restart restarts; x [n_cells][4] (device) holds the
