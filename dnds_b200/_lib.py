@@ -14,7 +14,7 @@ EXPORTS = [
     "dndsg_create", "dndsg_destroy", "dndsg_last_error", "dndsg_n_cells", "dndsg_n_faces",
     "dndsg_set_u", "dndsg_get_u", "dndsg_set_urec", "dndsg_get_urec", "dndsg_get_dt",
     "dndsg_device_buffer", "dndsg_get_time", "dndsg_set_time", "dndsg_vr_jacobi_step",
-    "dndsg_limiter_wbap", "dndsg_eval_dt", "dndsg_eval_rhs", "dndsg_ssprk3_step", "dndsg_ssprk3_steps",
+    "dndsg_limiter_wbap", "dndsg_limiter_wbap_v2", "dndsg_eval_dt", "dndsg_eval_rhs", "dndsg_ssprk3_step", "dndsg_ssprk3_steps",
     "dndsg_residual", "dndsg_face_values", "dndsg_get_status", "dndsg_eval_rhs_noalloc",
     "dndsg_mlp_create", "dndsg_mlp_destroy", "dndsg_mlp_last_error", "dndsg_mlp_set_params",
     "dndsg_mlp_get_params", "dndsg_mlp_forward", "dndsg_mlp_gradient", "dndsg_mlp_train_step",
@@ -85,6 +85,7 @@ def lib():
     L.dndsg_set_time.argtypes = [vp, dbl, vp]
     L.dndsg_vr_jacobi_step.argtypes = [vp, i32, C.POINTER(dbl), vp]
     L.dndsg_limiter_wbap.argtypes = [vp, i32, vp, vp]
+    L.dndsg_limiter_wbap_v2.argtypes = [vp, i32, vp, vp]
     L.dndsg_eval_dt.argtypes = [vp, dbl, dbl, i32, C.POINTER(dbl), vp]
     L.dndsg_eval_rhs.argtypes = [vp, dbl, vp, vp]
     L.dndsg_ssprk3_step.argtypes = [vp, dbl, dbl, vp]

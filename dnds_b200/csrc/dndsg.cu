@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -55,7 +56,8 @@ struct dndsg_ctx {
          *saSrcJac = nullptr, *saDWall = nullptr, *saCellGp = nullptr;
   void *saUrec = nullptr, *saUrecNew = nullptr;  // T [N][5]
   double* Ainv = nullptr;
-  double *limFace = nullptr, *faceInd = nullptr, *indicator = nullptr;  // CWBAP limiter data
+  void* limFace = nullptr;                                 // T: the limiting pass's per-face matrices
+  double *faceInd = nullptr, *indicator = nullptr;         // the indicator's integrals and values
   int32_t *limList = nullptr, *limCount = nullptr;  // cells the limiter pass limits, and their number
   void *limG = nullptr, *limCell = nullptr;         // the indicator's compact face and cell data (T)
   int sms = 0;                                      // multiprocessors of the device
@@ -293,7 +295,8 @@ __global__ void k_vr_wall_fixup(HotView<T> h, const int32_t* cells, int64_t n) {
   if (k < n) vr_wall_fixup<T>(cells[k], h);
 }
 // ---- CWBAP limiter: face indicator integrals, cell indicator, limiting pass
-__global__ void k_setup_limiter(MeshView m, SetupParams p, const CellSetup* cells, const double* faceW, double* lim,
+template <class T>
+__global__ void k_setup_limiter(MeshView m, SetupParams p, const CellSetup* cells, const double* faceW, T* lim,
                                 int* bad) {
   int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (f < m.F && !setup_limiter_face(f, m, p, cells, faceW, lim)) atomicOr(bad, 4);
@@ -328,13 +331,23 @@ __global__ void __launch_bounds__(kBlock) k_lim_cell_indicator(LimView v, int32_
   base = __shfl_sync(0xffffffffu, base, 0);
   if (lim) list[base + __popc(b & ((1u << lane) - 1))] = (int32_t)i;
 }
-// the listed cells, one thread each (limiter_cell), into buf[t] for list entry t; a grid-stride loop
-template <class T>
-__global__ void __launch_bounds__(kBlock) k_lim_apply(LimView v, const T* urec, T* buf, const int32_t* list,
-                                                      const int32_t* count) {
+// the limiting pass over the listed cells, four lanes per cell (limiter_cell4), into buf[t] for list
+// entry t: V3 = true both orders of ReconstructionWBAPLimitFacialV3; V3 = false the order PASS of
+// ReconstructionWBAPLimitFacialV2.  A grid-stride loop whose trip count is the same for all lanes of a
+// warp (eight cells per warp per trip), so the width-4 shuffles always have all 32 lanes
+template <class T, bool V3, int PASS, int NF>
+__global__ void __launch_bounds__(kBlock) k_lim_apply4(LimView v, const T* urec, T* buf, const int32_t* list,
+                                                       const int32_t* count) {
   const int64_t n = *count;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
-    limiter_cell<T>(list[t], v, urec, buf + t * 20);
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t base = warp * 8; base < n; base += nwarps * 8) {
+    const int64_t t = base + (lane >> 2);
+    const bool valid = t < n;
+    const int64_t i = valid ? list[t] : 0;
+    limiter_cell4<T, V3, PASS, NF>(valid, i, lane & 3, v, urec, buf + (valid ? t : 0) * 20);
+  }
 }
 // the limited coefficients back over the listed cells' ones, 16 bytes per thread
 template <class T>
@@ -369,6 +382,8 @@ __global__ void __launch_bounds__(kBlock, (sizeof(T) == 4 && RIEMANN == 1 && !BN
     double t = stage_time(scal, useDev, tHost, c);
     if constexpr (sizeof(T) == 4 && RIEMANN == 1 && !BND)
       r = face_flux_roe_delta32(f, h, out, bad);
+    else if constexpr (sizeof(T) == 4 && RIEMANN == 2 && !BND)
+      r = face_flux_hllc_delta32(f, h, out, bad);
     else
       r = face_flux<T, RIEMANN, BND>(f, h, t, out, bad);
     double* o = &h.flux[f * 4];
@@ -611,15 +626,41 @@ LimView lim_view(dndsg_ctx* c, int ifAll) {
 
 // ReconstructionWBAPLimitFacialV3 on the resident urec (result swapped into urec)
 template <class T>
-void run_limiter(dndsg_ctx* c, int ifAll, cudaStream_t s) {
+void run_limiter_v3(dndsg_ctx* c, int ifAll, cudaStream_t s) {
   LimView v = lim_view(c, ifAll);
   k_lim_face<T><<<grid_for(c->F), kBlock, 0, s>>>(v, (const T*)c->urec, c->limCount);
   k_lim_cell_indicator<<<grid_for(c->N), kBlock, 0, s>>>(v, c->limList, c->limCount);
   // urecNew (the previous sweep's coefficients, free until the next sweep) holds the limited ones
   if (!c->sms && cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess) c->sms = 148;
   const unsigned g = (unsigned)std::min<int64_t>(grid_for(c->N), 4 * c->sms);
-  k_lim_apply<T><<<g, kBlock, 0, s>>>(v, (const T*)c->urec, (T*)c->urecNew, c->limList, c->limCount);
+  if (c->nfmax == 3) k_lim_apply4<T, true, 0, 3><<<g, kBlock, 0, s>>>(v, (const T*)c->urec, (T*)c->urecNew, c->limList, c->limCount);
+  else k_lim_apply4<T, true, 0, 4><<<g, kBlock, 0, s>>>(v, (const T*)c->urec, (T*)c->urecNew, c->limList, c->limCount);
   k_lim_scatter<T><<<g, kBlock, 0, s>>>((T*)c->urec, (const T*)c->urecNew, c->limList, c->limCount);
+}
+
+// ReconstructionWBAPLimitFacialV2 on the resident urec: the same indicator and list, then the P2 pass
+// over the listed cells scattered back before the P1 pass reads it, as the reference's order loop
+// copies uRecNewBuf1 into uRecNewBuf between the orders
+template <class T>
+void run_limiter_v2(dndsg_ctx* c, int ifAll, cudaStream_t s) {
+  LimView v = lim_view(c, ifAll);
+  k_lim_face<T><<<grid_for(c->F), kBlock, 0, s>>>(v, (const T*)c->urec, c->limCount);
+  k_lim_cell_indicator<<<grid_for(c->N), kBlock, 0, s>>>(v, c->limList, c->limCount);
+  if (!c->sms && cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess) c->sms = 148;
+  const unsigned g = (unsigned)std::min<int64_t>(grid_for(c->N), 4 * c->sms);
+  if (c->nfmax == 3) k_lim_apply4<T, false, 0, 3><<<g, kBlock, 0, s>>>(v, (const T*)c->urec, (T*)c->urecNew, c->limList, c->limCount);
+  else k_lim_apply4<T, false, 0, 4><<<g, kBlock, 0, s>>>(v, (const T*)c->urec, (T*)c->urecNew, c->limList, c->limCount);
+  k_lim_scatter<T><<<g, kBlock, 0, s>>>((T*)c->urec, (const T*)c->urecNew, c->limList, c->limCount);
+  if (c->nfmax == 3) k_lim_apply4<T, false, 1, 3><<<g, kBlock, 0, s>>>(v, (const T*)c->urec, (T*)c->urecNew, c->limList, c->limCount);
+  else k_lim_apply4<T, false, 1, 4><<<g, kBlock, 0, s>>>(v, (const T*)c->urec, (T*)c->urecNew, c->limList, c->limCount);
+  k_lim_scatter<T><<<g, kBlock, 0, s>>>((T*)c->urec, (const T*)c->urecNew, c->limList, c->limCount);
+}
+
+// the limiter of the stage compositions: limiterProcedure 1 (CWBAP, V3) or 0 (3WBAP, V2)
+template <class T>
+void run_limiter(dndsg_ctx* c, int ifAll, cudaStream_t s) {
+  if (c->s.limiter == 2) run_limiter_v2<T>(c, ifAll, s);
+  else run_limiter_v3<T>(c, ifAll, s);
 }
 
 // the face-flux launches of EvaluateRHS over the arrays of h (interior faces, then boundary faces)
@@ -749,6 +790,47 @@ int observe_timeout(dndsg_ctx* c, cudaStream_t s) {
   return 0;
 }
 
+// A cell's face slots in element-local face order, the order of the reference's cell2face (vol2face is
+// filled per local face, DNDS_Mesh.hpp:288-320): slot k holds the face joining nodes k and k+1
+// (FaceNodeList of TRI3 / QUAD4, DNDS_Elements.hpp:248-253).  A face is matched by its node pair, or --
+// a periodic face seen from its translated side -- by its midpoint against the edge midpoint moved by
+// the face shift.  Sums over a cell's faces run in slot order, and V2's multiway WBAP is centred on
+// the first slot's neighbour.  slot[k] encodes the face as f (left side) or ~f (right side).
+void order_cell_slots(const dndsg_mesh_desc* md, int64_t i, int32_t* slot, int nf) {
+  const int nn = md->cell_nodes[4 * i + 3] < 0 ? 3 : 4;
+  if (nf != nn) return;
+  int32_t out[4] = {0, 0, 0, 0};
+  bool got[4] = {false, false, false, false}, used[4] = {false, false, false, false};
+  for (int pass = 0; pass < 2; pass++)
+    for (int e = 0; e < nn; e++) {
+      if (got[e]) continue;
+      const int32_t p = md->cell_nodes[4 * i + e], q = md->cell_nodes[4 * i + (e + 1) % nn];
+      const double mx = 0.5 * (md->node_xy[2 * p] + md->node_xy[2 * q]);
+      const double my = 0.5 * (md->node_xy[2 * p + 1] + md->node_xy[2 * q + 1]);
+      const double len = std::hypot(md->node_xy[2 * q] - md->node_xy[2 * p], md->node_xy[2 * q + 1] - md->node_xy[2 * p + 1]);
+      for (int k = 0; k < nf && !got[e]; k++) {
+        if (used[k]) continue;
+        const int32_t f = slot[k] >= 0 ? slot[k] : ~slot[k];
+        const int32_t a = md->face_nodes[2 * f], b = md->face_nodes[2 * f + 1];
+        bool hit = (a == p && b == q) || (a == q && b == p);
+        if (!hit && pass == 1 && md->face_shift) {
+          const double fx = 0.5 * (md->node_xy[2 * a] + md->node_xy[2 * b]);
+          const double fy = 0.5 * (md->node_xy[2 * a + 1] + md->node_xy[2 * b + 1]);
+          const double sx = md->face_shift[2 * f], sy = md->face_shift[2 * f + 1];
+          for (int sg = -1; sg <= 1 && !hit; sg += 2)
+            hit = std::fabs(mx + sg * sx - fx) + std::fabs(my + sg * sy - fy) < 1e-9 * len;
+        }
+        if (hit) {
+          out[e] = slot[k];
+          got[e] = used[k] = true;
+        }
+      }
+    }
+  for (int e = 0; e < nn; e++)
+    if (!got[e]) return;  // unmatched: keep the given order
+  for (int e = 0; e < nn; e++) slot[e] = out[e];
+}
+
 template <class T>
 int setup_run(dndsg_ctx* c, const dndsg_mesh_desc* md) {
   const int64_t N = c->N, F = c->F;
@@ -785,6 +867,10 @@ int setup_run(dndsg_ctx* c, const dndsg_mesh_desc* md) {
       if (nd < 0 || nd >= md->n_nodes) return fail(c, DNDSG_BAD_ARGUMENT, "cell_nodes out of range");
     }
     if (cnt[i] != nn) return fail(c, DNDSG_BAD_ARGUMENT, "cell face count differs from its node count");
+    int32_t sl[4];
+    for (int k = 0; k < nn; k++) sl[k] = slots[aos(i, k, c->nfmax)];
+    order_cell_slots(md, i, sl, nn);
+    for (int k = 0; k < nn; k++) slots[aos(i, k, c->nfmax)] = sl[k];
   }
   c->hasWallCorr = hasWallCorr;
   // ---- device mesh
@@ -895,11 +981,11 @@ int setup_run(dndsg_ctx* c, const dndsg_mesh_desc* md) {
   k_setup_mlp_geom<<<grid_for(N), kBlock>>>(m, cells, c->cellFace, c->nfmax, c->faceCenter, c->mlpGeom);
   if ((rc = check_launch(c))) return rc;
   if (c->s.limiter) {
-    if ((rc = dalloc(c, c->limFace, sizeof(double) * aos_size(F, kLimE)))) return rc;
+    if ((rc = dalloc(c, c->limFace, sizeof(T) * aos_size(F, kLimE)))) return rc;
     if ((rc = dalloc(c, c->faceInd, sizeof(double) * 4 * F))) return rc;
     if ((rc = dalloc(c, c->indicator, sizeof(double) * N))) return rc;
     if ((rc = dalloc(c, c->limList, sizeof(int32_t) * N)) || (rc = dalloc(c, c->limCount, sizeof(int32_t)))) return rc;
-    k_setup_limiter<<<grid_for(F), kBlock>>>(m, p, cells, faceW, c->limFace, dBad);
+    k_setup_limiter<T><<<grid_for(F), kBlock>>>(m, p, cells, faceW, (T*)c->limFace, dBad);
     if ((rc = check_launch(c))) return rc;
     if ((rc = dalloc(c, c->limG, sizeof(T) * aos_size(F, kLimG))) ||
         (rc = dalloc(c, c->limCell, sizeof(T) * kLimCell * N)))
@@ -1207,12 +1293,17 @@ int dndsg_vr_jacobi_step(dndsg_ctx* c, int nsweeps, double* inc_out, void* s) {
   return 0;
 }
 
-int dndsg_limiter_wbap(dndsg_ctx* c, int if_all, double* indicator_out, void* s) {
+static int limiter_api(dndsg_ctx* c, int version, int if_all, double* indicator_out, void* s) {
   if (!c) return DNDSG_BAD_ARGUMENT;
   if (c->dead) return refuse_dead(c);
   if (!c->limFace) return fail(c, DNDSG_UNSUPPORTED, "context was created without the limiter (settings.limiter = 0)");
-  if (c->fp32) run_limiter<float>(c, if_all, st(s));
-  else run_limiter<double>(c, if_all, st(s));
+  if (version == 3) {
+    if (c->fp32) run_limiter_v3<float>(c, if_all, st(s));
+    else run_limiter_v3<double>(c, if_all, st(s));
+  } else {
+    if (c->fp32) run_limiter_v2<float>(c, if_all, st(s));
+    else run_limiter_v2<double>(c, if_all, st(s));
+  }
   int rc = check_launch(c);
   if (rc) return rc;
   if (indicator_out) {
@@ -1220,6 +1311,14 @@ int dndsg_limiter_wbap(dndsg_ctx* c, int if_all, double* indicator_out, void* s)
     DG_CUDA(c, cudaStreamSynchronize(st(s)));
   }
   return 0;
+}
+
+int dndsg_limiter_wbap(dndsg_ctx* c, int if_all, double* indicator_out, void* s) {
+  return limiter_api(c, 3, if_all, indicator_out, s);
+}
+
+int dndsg_limiter_wbap_v2(dndsg_ctx* c, int if_all, double* indicator_out, void* s) {
+  return limiter_api(c, 2, if_all, indicator_out, s);
 }
 
 int dndsg_eval_dt(dndsg_ctx* c, double cfl, double max_dt, int use_local_dt, double* dt_min_out, void* s) {

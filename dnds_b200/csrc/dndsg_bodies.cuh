@@ -733,6 +733,125 @@ DG_HD int face_flux_roe_delta32(int64_t f, const HotView<float>& h, double out[4
   return nred;
 }
 
+// HLLC flux of an interior face for the FP32-bulk path, in flux-difference form.  With the flux
+// jump dF = F(UR) - F(UL) and the contact-speed offset sigma = S* - u_L, the HLLC flux of
+// Gas::HLLCFlux_IdealGas_HartenYee<2> (DNDS_Gas.hpp:312-403) is, exactly:
+//   0 <= SL:      F = F_mid - dF / 2                      SR <= 0:  F = F_mid + dF / 2
+//   S* >= 0:      F = F_mid - dF / 2 + SL (U*L - UL)      else:     F = F_mid + dF / 2 + SR (U*R - UR)
+//   F_mid = (F(UL) + F(UR)) / 2,  U*K - UK = (sigma_K / (SK - S*)) UK + chi_K sigma_K (0, rho_K, 0, rho_K S* + p_K / (SK - u_K)),
+//   chi_K = (SK - u_K) / (SK - S*),  sigma_L = (dp - rho_R (SR - u_R) du) / (rho_L (SL - u_L) - rho_R (SR - u_R)),
+//   sigma_R = sigma_L - du
+// (the reference's star flux ((UK SK - FK) S* + D* (p_K + rho_K (SK - u_K)(S* - u_K)) SK) / (SK - S*)
+// written as FK + SK (U*K - UK)).  F_mid is 1/2 (F(uL) + F(uR)) in FP64 once per face plus the FP32
+// increments 1/2 (F(UL) - F(uL) + F(UR) - F(uR)); the jumps dF, du, dp are formed from the FP64 mean
+// difference plus the FP32 increment difference, so every FP32 term's rounding scales with the
+// reconstruction increment or the jump across the face, not with the flux itself.
+DG_HD int face_flux_hllc_delta32(int64_t f, const HotView<float>& h, double out[4], bool& bad) {
+  const int32_t L = h.faceL[f], R = h.faceR[f];
+  const double nxd = h.faceNormal[2 * f], nyd = h.faceNormal[2 * f + 1], area = h.faceArea[f];
+  double uL[4], uR[4];
+  load4<float>(&h.u[(int64_t)L * 4], uL);
+  load4<float>(&h.u[(int64_t)R * 4], uR);
+  float incL[3][4], incR[3][4];
+  face_increments(f, L, R, h, incL, incR);
+  const float gamma = (float)h.gamma, gm1 = gamma - 1.0f;
+  const float nx = (float)nxd, ny = (float)nyd;
+  double FL[4], FR[4];
+  flux_n_f64(uL, nxd, nyd, h.gamma, FL);
+  flux_n_f64(uR, nxd, nyd, h.gamma, FR);
+  float bL[4], bR[4], dmean[4], dFmean[4];
+  {
+    const float tL[4] = {(float)uL[0], (float)uL[1], (float)uL[2], (float)uL[3]};
+    const float tR[4] = {(float)uR[0], (float)uR[1], (float)uR[2], (float)uR[3]};
+    const float tD[4] = {(float)(uR[0] - uL[0]), (float)(uR[1] - uL[1]), (float)(uR[2] - uL[2]), (float)(uR[3] - uL[3])};
+    const float tF[4] = {(float)(FR[0] - FL[0]), (float)(FR[1] - FL[1]), (float)(FR[2] - FL[2]), (float)(FR[3] - FL[3])};
+    to_normal_frame(tL, nx, ny, bL);
+    to_normal_frame(tR, nx, ny, bR);
+    to_normal_frame(tD, nx, ny, dmean);
+    to_normal_frame(tF, nx, ny, dFmean);
+  }
+  int nred = 0;
+  float acc[4] = {0.f, 0.f, 0.f, 0.f};
+  for (int g = 0; g < 3; g++) {
+    float dL[4], dR[4];
+    to_normal_frame(incL[g], nx, ny, dL);
+    to_normal_frame(incR[g], nx, ny, dR);
+    float UL[4], UR[4];
+    for (int v = 0; v < 4; v++) { UL[v] = bL[v] + dL[v]; UR[v] = bR[v] + dR[v]; }
+    // CompressRecPart: the mean where density or internal energy would be negative
+    if (UL[0] < 0.f || 2.f * UL[0] * UL[3] < UL[1] * UL[1] + UL[2] * UL[2]) {
+      for (int v = 0; v < 4; v++) { dL[v] = 0.f; UL[v] = bL[v]; }
+      nred++;
+    }
+    if (UR[0] < 0.f || 2.f * UR[0] * UR[3] < UR[1] * UR[1] + UR[2] * UR[2]) {
+      for (int v = 0; v < 4; v++) { dR[v] = 0.f; UR[v] = bR[v]; }
+      nred++;
+    }
+    if (!(UL[0] > 0.f && UR[0] > 0.f)) bad = true;
+    float DL[4], DR[4];
+    flux_delta_f32(bL, dL, gamma, DL);
+    flux_delta_f32(bR, dR, gamma, DR);
+    float J[4], dF[4], G[4];
+    for (int v = 0; v < 4; v++) {
+      J[v] = dmean[v] + (dR[v] - dL[v]);
+      dF[v] = dFmean[v] + (DR[v] - DL[v]);
+      G[v] = 0.5f * (DL[v] + DR[v]);
+    }
+    const float rL = UL[0], rR = UR[0], irL = 1.0f / rL, irR = 1.0f / rR;
+    const float uL1 = UL[1] * irL, vL1 = UL[2] * irL, uR1 = UR[1] * irR, vR1 = UR[2] * irR;
+    const float pL = gm1 * (UL[3] - 0.5f * (UL[1] * uL1 + UL[2] * vL1));
+    const float pR = gm1 * (UR[3] - 0.5f * (UR[1] * uR1 + UR[2] * vR1));
+    // exact jumps of the normal velocity, tangential velocity and pressure from J
+    const float du = (J[1] - uL1 * J[0]) * irR, dv = (J[2] - vL1 * J[0]) * irR;
+    const float dp = gm1 * (J[3] - 0.5f * (UL[1] * du + J[1] * uR1 + UL[2] * dv + J[2] * vR1));
+    const float sL = sqrtf(rL), sR = sqrtf(rR), isum = 1.0f / (sL + sR);
+    const float um = (sL * uL1 + sR * uR1) * isum;
+    const float eta2 = 0.5f * (sL * sR) * isum * isum;
+    const float dsqr = (gamma * pL * irL * sL + gamma * pR * irR * sR) * isum + eta2 * du * du;
+    const float sq = sqrtf(dsqr), SL = um - sq, SR = um + sq;
+    if (0.f <= SL) {
+      for (int v = 0; v < 4; v++) G[v] -= 0.5f * dF[v];
+    } else if (SR <= 0.f) {
+      for (int v = 0; v < 4; v++) G[v] += 0.5f * dF[v];
+    } else {
+      const float div = rL * (SL - uL1) - rR * (SR - uR1);
+      const float sigL = fabsf(div) > 1e-37f ? (dp - rR * (SR - uR1) * du) / div : -uL1;  // S* = 0 if degenerate
+      const float SS = uL1 + sigL;
+      if (SS >= 0.f) {
+        const float d = SL - SS;
+        for (int v = 0; v < 4; v++) G[v] -= 0.5f * dF[v];
+        if (fabsf(d) >= 1e-37f) {
+          const float a = sigL / d, chi = (SL - uL1) / d;
+          const float q1 = chi * sigL * rL, q3 = chi * sigL * (rL * SS + pL / (SL - uL1));
+          G[0] += SL * (a * UL[0]);
+          G[1] += SL * (a * UL[1] + q1);
+          G[2] += SL * (a * UL[2]);
+          G[3] += SL * (a * UL[3] + q3);
+        }
+      } else {
+        const float d = SR - SS, sigR = sigL - du;
+        for (int v = 0; v < 4; v++) G[v] += 0.5f * dF[v];
+        if (fabsf(d) >= 1e-37f) {
+          const float a = sigR / d, chi = (SR - uR1) / d;
+          const float q1 = chi * sigR * rR, q3 = chi * sigR * (rR * SS + pR / (SR - uR1));
+          G[0] += SR * (a * UR[0]);
+          G[1] += SR * (a * UR[1] + q1);
+          G[2] += SR * (a * UR[2]);
+          G[3] += SR * (a * UR[3] + q3);
+        }
+      }
+    }
+    from_normal_frame(G, nx, ny);
+    const float jw = (float)(0.5 * area * l3_weight(g));
+    for (int k = 0; k < 4; k++) acc[k] += G[k] * jw;
+  }
+  for (int k = 0; k < 4; k++) {
+    out[k] = -(area * 0.5 * (FL[k] + FR[k]) + (double)acc[k]);
+    if (!(out[k] == out[k])) bad = true;
+  }
+  return nred;
+}
+
 // EvaluateDt face part (DNDS_FV_EulerEvaluator.cpp:25-137): lambda_f * area, deltaLambdaFace
 template <class T>
 DG_HD void dt_face(int64_t f, const HotView<T>& h) {

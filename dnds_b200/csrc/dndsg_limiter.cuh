@@ -1,25 +1,28 @@
 // dndsg_limiter.cuh -- the CWBAP limiter, VRFiniteVolume2D::ReconstructionWBAPLimitFacialV3
-// (DNDS_FV_VR.hpp:2053-2329) with the biway/multiway WBAP kernels of
+// (DNDS_FV_VR.hpp:2053-2329), and the 3WBAP limiter ReconstructionWBAPLimitFacialV2 (:1749-2047, at
+// the end of this file), with the biway/multiway WBAP kernels of
 // DNDS_FV_Limiters.hpp:341-449 and the characteristic matrices fML/fMR of
-// DNDS_FV_EulerSolver.hpp:749-795.  Arithmetic in FP64 for both storage precisions.
+// DNDS_FV_EulerSolver.hpp:749-795.  Arithmetic in the storage precision: FP64 in FP64 contexts, FP32 in
+// FP32-bulk contexts.
 //
-// Three passes:
+// Passes:
 //   face:  smoothness-indicator integrals IJI, ISI of rho and E at the face's
 //          first gauss point (the reference integrates with LINE_1 weight 2 but
 //          reads the LINE_3 data of point 0), one thread per face;
 //   cell:  indicator si = sqrt(max_k IJI_k / ISI_k) * P^2 (P = 2), one thread per
 //          cell, which lists the cells to limit;
-//   limit: one thread per listed cell, order-by-order (P2 rows 2..4, then P1
-//          rows 0..1) biway WBAP against each neighbour in characteristic space
-//          and a multiway WBAP of the results, into a compact buffer that a last
-//          pass scatters back over the listed cells' coefficients (the others
-//          keep theirs: nothing is copied).
+//   limit: four lanes per listed cell (one per conserved variable; the
+//          characteristic projections exchange values by shuffles), order by
+//          order (P2 rows 2..4, then P1 rows 0..1) biway WBAP against each
+//          neighbour in characteristic space and a multiway WBAP of the results,
+//          into a compact buffer that a last pass scatters back over the listed
+//          cells' coefficients (the others keep theirs: nothing is copied).
 #pragma once
 #include "dndsg_bodies.cuh"
 
 namespace dg {
 
-// per-face data of the limiting pass, tile-major AoSoA with E = kLimE (FP64):
+// per-face data of the limiting pass, tile-major AoSoA with E = kLimE, in the context's precision:
 //   [0, 25)   msR2L (right-cell coefficients -> left basis), row-major
 //   [25, 50)  msL2R
 // (the indicator's data is the compact limG / limCell below)
@@ -40,7 +43,7 @@ struct LimView {
   const int32_t* faceR;
   const double* faceNormal;
   const double* faceArea;
-  const double* limFace;   // AoSoA kLimE
+  const void* limFace;     // T [F] AoSoA kLimE (T = the context's precision)
   const void* limG;        // T [F] AoSoA kLimG (T = the context's precision)
   const void* limCell;     // T [N][kLimCell]
   const double* u;
@@ -59,10 +62,11 @@ struct LimView {
 // setup: the limiter data of one interior face (face part of initBaseDiffCache,
 // DNDS_FV_VR.cpp:536-712): D at gauss point 0 for both sides and the secondary
 // reconstruction matrices from the derivative matrices at the face centre
+template <class T>
 DG_HD bool setup_limiter_face(int64_t f, const MeshView& m, const SetupParams& p, const CellSetup* cells,
-                              const double* faceW, double* lim) {
+                              const double* faceW, T* lim) {
   int32_t L = m.face_cells[2 * f], R = m.face_cells[2 * f + 1];
-  for (int e = 0; e < kLimE; e++) lim[aos(f, e, kLimE)] = 0.0;
+  for (int e = 0; e < kLimE; e++) lim[aos(f, e, kLimE)] = T(0);
   if (R < 0) return true;
   FaceGeom g = face_geom(f, m);
   double sx = m.face_shift ? m.face_shift[2 * f] : 0.0, sy = m.face_shift ? m.face_shift[2 * f + 1] : 0.0;
@@ -73,10 +77,10 @@ DG_HD bool setup_limiter_face(int64_t f, const MeshView& m, const SetupParams& p
   double A[5][5], B[5][5];
   for (int i = 0; i < 5; i++) for (int j = 0; j < 5; j++) { A[i][j] = DL[i + 1][j]; B[i][j] = DR[i + 1][j]; }
   bool ok = lu5_solve(A, B);
-  for (int i = 0; i < 5; i++) for (int j = 0; j < 5; j++) lim[aos(f, kMsR2L + i * 5 + j, kLimE)] = B[i][j];
+  for (int i = 0; i < 5; i++) for (int j = 0; j < 5; j++) lim[aos(f, kMsR2L + i * 5 + j, kLimE)] = (T)B[i][j];
   for (int i = 0; i < 5; i++) for (int j = 0; j < 5; j++) { A[i][j] = DR[i + 1][j]; B[i][j] = DL[i + 1][j]; }
   ok = lu5_solve(A, B) && ok;
-  for (int i = 0; i < 5; i++) for (int j = 0; j < 5; j++) lim[aos(f, kMsL2R + i * 5 + j, kLimE)] = B[i][j];
+  for (int i = 0; i < 5; i++) for (int j = 0; j < 5; j++) lim[aos(f, kMsL2R + i * 5 + j, kLimE)] = (T)B[i][j];
   return ok;
 }
 
@@ -103,8 +107,11 @@ DG_HD void setup_limiter_compact(int64_t f, const MeshView& m, const CellSetup* 
   }
 }
 
+// the indicator integrals of one face, in the storage precision T: FP64 in FP64 contexts, FP32 in
+// FP32-bulk contexts (the four integrals are stored in FP64 for the cell pass)
 template <class T>
 DG_HD void limiter_face_indicator(int64_t f, const LimView& v, const T* urec) {
+  using C = T;
   int32_t L = v.faceL[f], R = v.faceR[f];
   double* out = &v.faceInd[f * 4];
   if (R < 0) { out[0] = out[1] = out[2] = out[3] = 0; return; }
@@ -113,48 +120,53 @@ DG_HD void limiter_face_indicator(int64_t f, const LimView& v, const T* urec) {
   const T* g = static_cast<const T*>(v.limG);
   const T* cf = static_cast<const T*>(v.limCell);
   const int var[2] = {0, 3};
-  double sv[2][6][2];
+  C sv[2][6][2];
   for (int side = 0; side < 2; side++) {
     const int64_t cell = side ? R : L;
     const T* c = cf + cell * kLimCell;
-    const double Q[2][2] = {{(double)c[0], (double)c[1]}, {(double)c[2], (double)c[3]}};
-    const double mo[5] = {(double)c[4], (double)c[5], (double)c[6], (double)c[7], (double)c[8]};
-    double D[6][5];
-    p2_diffs_at(Q, mo, (double)g[aos(f, 2 * side, kLimG)], (double)g[aos(f, 2 * side + 1, kLimG)], D);
+    const C Q[2][2] = {{c[0], c[1]}, {c[2], c[3]}};
+    const C mo[5] = {c[4], c[5], c[6], c[7], c[8]};
+    C D[6][5];
+    p2_diffs_at<C>(Q, mo, g[aos(f, 2 * side, kLimG)], g[aos(f, 2 * side + 1, kLimG)], D);
     for (int k = 0; k < 2; k++) {
-      double r[5];
-      for (int q = 0; q < 5; q++) r[q] = (double)urec[cell * 20 + q * 4 + var[k]];
+      C r[5];
+      for (int q = 0; q < 5; q++) r[q] = urec[cell * 20 + q * 4 + var[k]];
       for (int d = 0; d < 6; d++) {
-        double a = 0;
+        C a = C(0);
         for (int q = 0; q < 5; q++) a += D[d][q] * r[q];
-        if (d == 0) a += v.u[cell * 4 + var[k]];
+        if (d == 0) a += (C)v.u[cell * 4 + var[k]];
         sv[side][d][k] = a;
       }
     }
   }
-  double val[6][2], jump[6][2];
+  C val[6][2], jump[6][2];
   for (int c = 0; c < 2; c++)
     for (int d = 0; d < 6; d++) {
-      val[d][c] = (sv[0][d][c] + sv[1][d][c]) * 0.5;
-      jump[d][c] = (sv[0][d][c] - sv[1][d][c]) * 0.5;
+      val[d][c] = (sv[0][d][c] + sv[1][d][c]) * C(0.5);
+      jump[d][c] = (sv[0][d][c] - sv[1][d][c]) * C(0.5);
     }
-  double W[6];
-  for (int k = 0; k < 6; k++) W[k] = (double)g[aos(f, 4 + k, kLimG)];
+  C W[6];
+  for (int k = 0; k < 6; k++) W[k] = g[aos(f, 4 + k, kLimG)];
   const double area = v.faceArea[f];
-  double sL = sqrt(v.vol[L]) / area, sR = sqrt(v.vol[R]) / area;
-  double arMax = dmax(1.0, dmax(sL, sR));
-  double tm = pow((1.0 / arMax) * (1 - v.tangModMin) + v.tangModMin, v.tangModPower);
-  FaceFunctional Fn = make_functional(W, v.faceNormal[2 * f], v.faceNormal[2 * f + 1], v.tangWeight, tm, v.tangModLoc);
-  double ij[2] = {0, 0}, is[2] = {0, 0};
+  C tm = C(1);  // the tangential-weight modifier; exactly 1 when tangWeightModMin is 1
+  if (v.tangModMin != 1.0) {
+    const double sL = sqrt(v.vol[L]) / area, sR = sqrt(v.vol[R]) / area;
+    const double arMax = dmax(1.0, dmax(sL, sR));
+    tm = (C)pow((1.0 / arMax) * (1 - v.tangModMin) + v.tangModMin, v.tangModPower);
+  }
+  const FaceFunctionalT<C> Fn = make_functional<C>(W, (C)v.faceNormal[2 * f], (C)v.faceNormal[2 * f + 1],
+                                                   (C)v.tangWeight, tm, v.tangModLoc);
+  C ij[2] = {C(0), C(0)}, is[2] = {C(0), C(0)};
   for (int a = 0; a < 6; a++)
     for (int c = 0; c < 2; c++) {
-      double pj = 0, ps = 0;
+      C pj = C(0), ps = C(0);
       for (int r = 0; r < 6; r++) { pj += Fn.t[a][r] * jump[r][c]; ps += Fn.t[a][r] * val[r][c]; }
       ij[c] += pj * pj;
       is[c] += ps * ps;
     }
   // |n| of gauss point 0 is area/2, times the LINE_1 weight 2
-  out[0] = ij[0] * area; out[1] = ij[1] * area; out[2] = is[0] * area; out[3] = is[1] * area;
+  out[0] = (double)ij[0] * area; out[1] = (double)ij[1] * area; out[2] = (double)is[0] * area;
+  out[3] = (double)is[1] * area;
 }
 
 // cell pass of the indicator: si = sqrt(max |IJI/ISI|) * P^2
@@ -171,38 +183,8 @@ DG_HD double limiter_cell_indicator(int64_t i, const LimView& v) {
   return sqrt(dmax(fabs(s0), fabs(s1))) * v.porder2;
 }
 
-// characteristic matrices at the face mean state (fML / fMR, DNDS_FV_EulerSolver.hpp:749-795)
-DG_HD void char_matrices(double gamma, const double* UL, const double* UR, double nx, double ny, double Lm[4][4],
-                         double Rm[4][4]) {
-  double UC[4], r[4];
-  for (int k = 0; k < 4; k++) UC[k] = (UL[k] + UR[k]) * 0.5;
-  to_normal_frame(UC, nx, ny, r);
-  double ir = 1.0 / r[0];
-  double vx = r[1] * ir, vy = r[2] * ir, vs = vx * vx + vy * vy, p, a2, H;
-  thermal(r[3], r[0], vs, gamma, p, a2, H);
-  double a = sqrt(a2), gb = gamma - 1, sc = gb / (2 * a * a);
-  double L0[4][4] = {{H + a / gb * (vx - a), -vx - a / gb, -vy, 1},
-                     {-2 * H + 4 / gb * (a * a), vx * 2, vy * 2, -2},
-                     {vy * (-2 * (a * a) / gb), 0, 2 * (a * a) / gb, 0},
-                     {H - a / gb * (vx + a), -vx + a / gb, -vy, 1}};
-  // L = L0 * diag(1, base^T) in the momentum block: columns 1,2 times [[nx, ny], [-ny, nx]]
-  for (int i = 0; i < 4; i++) {
-    double c1 = L0[i][1] * sc, c2 = L0[i][2] * sc;
-    Lm[i][0] = L0[i][0] * sc;
-    Lm[i][1] = c1 * nx - c2 * ny;
-    Lm[i][2] = c1 * ny + c2 * nx;
-    Lm[i][3] = L0[i][3] * sc;
-  }
-  double R0[4][4] = {{1, 1, 0, 1}, {vx - a, vx, 0, vx + a}, {vy, vy, 1, vy}, {H - vx * a, 0.5 * vs, vy, H + vx * a}};
-  for (int j = 0; j < 4; j++) {
-    Rm[0][j] = R0[0][j];
-    Rm[1][j] = nx * R0[1][j] - ny * R0[2][j];
-    Rm[2][j] = ny * R0[1][j] + nx * R0[2][j];
-    Rm[3][j] = R0[3][j];
-  }
-}
-
 DG_HD double signE(double x) { return x > 0 ? 1.0 : (x < 0 ? -1.0 : 0.0); }
+DG_HD float signE(float x) { return x > 0 ? 1.0f : (x < 0 ? -1.0f : 0.0f); }
 
 // FWBAP_L2_Biway(u1, u2, out, n) (DNDS_FV_Limiters.hpp:410-449), p = 4
 DG_HD double wbap_biway(double u1, double u2, double n) {
@@ -210,78 +192,148 @@ DG_HD double wbap_biway(double u1, double u2, double n) {
   double th1 = frac * frac * frac, th2 = (frac * frac) * (frac * frac);
   return u1 * (n + th1) / (n + th2);
 }
+// the same in FP32: |frac| is capped at 1e9 so that frac^4 stays finite (above the cap the
+// FP64 result is below 1e-9 |u1|, under FP32 resolution of u1, and the capped one is as small)
+DG_HD float wbap_biway(float u1, float u2, float n) {
+  float frac = u1 / (fabsf(u2) + 1e-12f) * signE(u2);
+  frac = copysignf(fminf(fabsf(frac), 1e9f), frac);
+  const float th1 = frac * frac * frac, th2 = (frac * frac) * (frac * frac);
+  return u1 * (n + th1) / (n + th2);
+}
+// one term of FWBAP_L2_Multiway (DNDS_FV_Limiters.hpp:341-405): theta = u0 / (|s| + verySmall^(1/4))
+// * sign(s), accumulated as theta^4 (down) and theta^3 (up); in FP32 capped at 1e9 as above
+DG_HD void wbap_multi_term(double u0, double s, double& up, double& down) {
+  const double ti = u0 / (fabs(s) + 1e-50) * signE(s);
+  down += (ti * ti) * (ti * ti);
+  up += ti * ti * ti;
+}
+DG_HD void wbap_multi_term(float u0, float s, float& up, float& down) {
+  float ti = s != 0.f ? u0 / fabsf(s) * signE(s) : 0.f;
+  ti = copysignf(fminf(fabsf(ti), 1e9f), ti);
+  down += (ti * ti) * (ti * ti);
+  up += ti * ti * ti;
+}
 
-// limiting pass for one cell (one the indicator pass listed); writes its 20 limited coefficients to o
-template <class T>
-DG_HD void limiter_cell(int64_t i, const LimView& v, const T* urec, T* o) {
-  const T* ri = &urec[i * 20];
-  const double sm4 = 1e-50;  // verySmallReal^(1/4)
-  double res[5][4];
-  double uFaces[4][3][4];  // biway results of the P2 pass per face, this cell's basis
-  const double* ui = &v.u[i * 4];
-  for (int pass = 0; pass < 2; pass++) {
+// Row `a` of the left and right characteristic matrices fML / fMR at the face mean state
+// (DNDS_FV_EulerSolver.hpp:749-795, Gas::EulerGasLeft/RightEigenVector, DNDS_Gas.hpp:17-71):
+// Lrow[q] = L[a][q] and Rrow[q] = R[a][q], in the arithmetic type C.
+template <class C>
+DG_HD void char_rows(int a, C gamma, const double* UL, const double* UR, C nx, C ny, C Lrow[4], C Rrow[4]) {
+  C UC[4], r[4];
+  for (int k = 0; k < 4; k++) UC[k] = (C)((UL[k] + UR[k]) * 0.5);
+  to_normal_frame(UC, nx, ny, r);
+  const C ir = C(1) / r[0];
+  const C vx = r[1] * ir, vy = r[2] * ir, vs = vx * vx + vy * vy;
+  C p, a2, H;
+  thermal(r[3], r[0], vs, gamma, p, a2, H);
+  const C as = sqrt(a2), gb = gamma - C(1), sc = gb / (C(2) * as * as);
+  C L0[4];
+  if (a == 0) { L0[0] = H + as / gb * (vx - as); L0[1] = -vx - as / gb; L0[2] = -vy; L0[3] = C(1); }
+  else if (a == 1) { L0[0] = -C(2) * H + C(4) / gb * (as * as); L0[1] = vx * 2; L0[2] = vy * 2; L0[3] = -C(2); }
+  else if (a == 2) { L0[0] = vy * (-C(2) * (as * as) / gb); L0[1] = C(0); L0[2] = C(2) * (as * as) / gb; L0[3] = C(0); }
+  else { L0[0] = H - as / gb * (vx + as); L0[1] = -vx + as / gb; L0[2] = -vy; L0[3] = C(1); }
+  // L = L0 * diag(1, base^T) in the momentum block: columns 1, 2 times [[nx, ny], [-ny, nx]]
+  const C c1 = L0[1] * sc, c2 = L0[2] * sc;
+  Lrow[0] = L0[0] * sc; Lrow[1] = c1 * nx - c2 * ny; Lrow[2] = c1 * ny + c2 * nx; Lrow[3] = L0[3] * sc;
+  // R0 rows 1 and 2 mix under the rotation: R[1] = nx R0[1] - ny R0[2], R[2] = ny R0[1] + nx R0[2]
+  const C R1[4] = {vx - as, vx, C(0), vx + as}, R2[4] = {vy, vy, C(1), vy};
+  if (a == 0) { Rrow[0] = C(1); Rrow[1] = C(1); Rrow[2] = C(0); Rrow[3] = C(1); }
+  else if (a == 3) { Rrow[0] = H - vx * as; Rrow[1] = C(0.5) * vs; Rrow[2] = vy; Rrow[3] = H + vx * as; }
+  else if (a == 1) { for (int j = 0; j < 4; j++) Rrow[j] = nx * R1[j] - ny * R2[j]; }
+  else { for (int j = 0; j < 4; j++) Rrow[j] = ny * R1[j] + nx * R2[j]; }
+}
+
+// The limiting pass of one listed cell on four lanes of a warp (the group's lane c owns conservative
+// variable c of every coefficient row and row c of the characteristic matrices), into o (the cell's 20
+// limited coefficients; rows a pass does not limit are copied).  V3 = true: ReconstructionWBAPLimitFacialV3
+// (CWBAP), both orders per cell (P2 rows 2..4, then P1 rows 0..1 against the neighbour's secondary
+// reconstruction whose rows 2..4 come from this cell's P2 biway results), biway with n = 1, multiway
+// with n = WBAP_nStd centred on the cell's own coefficients.  V3 = false: one pass of
+// ReconstructionWBAPLimitFacialV2 (3WBAP) for rows [LS, LS + NR), biway with n = WBAP_nStd, multiway
+// with n = 1 centred on the first neighbour's result (a cell without interior faces keeps its rows).
+// Arithmetic in the storage precision T.  All 32 lanes of the warp call this together (valid = false
+// for a group without a cell): the characteristic projections exchange values by width-4 shuffles.
+template <class T, bool V3, int PASS, int NF>
+__device__ __forceinline__ void limiter_cell4(bool valid, int64_t i, int c, const LimView& v, const T* urec, T* o) {
+  using C = T;
+  const T* ms = static_cast<const T*>(v.limFace);
+  const C gamma = (C)v.gamma, nStd = (C)v.nStd;
+  C ri[5];
+  for (int q = 0; q < 5; q++) ri[q] = valid ? urec[i * 20 + q * 4 + c] : C(0);
+  double ui[4] = {1.0, 0.0, 0.0, 2.5};
+  if (valid) for (int k = 0; k < 4; k++) ui[k] = v.u[i * 4 + k];
+  C res[5];
+  for (int q = 0; q < 5; q++) res[q] = ri[q];
+  C uFaces[NF][3];  // V3: this cell's P2 biway results per face slot (column c)
+  for (int k = 0; k < NF; k++) for (int r = 0; r < 3; r++) uFaces[k][r] = C(0);
+  constexpr int nPass = V3 ? 2 : 1;
+#pragma unroll
+  for (int pp = 0; pp < nPass; pp++) {
+    const int pass = V3 ? pp : PASS;
     const int ls = pass == 0 ? 2 : 0, nr = pass == 0 ? 3 : 2;
-    double up[3][4], down[3][4];
-    for (int r = 0; r < 3; r++) for (int c = 0; c < 4; c++) { up[r][c] = 0; down[r][c] = 0; }
-    for (int k = 0; k < v.nfmax; k++) {
-      int32_t sf = v.cellFace[aos(i, k, v.nfmax)];
-      if (sf == kEmptySlot) continue;
-      int32_t f = sf >= 0 ? sf : ~sf;
-      int side = sf >= 0 ? 0 : 1;
-      int32_t j = side == 0 ? v.faceR[f] : v.faceL[f];
-      if (j < 0) continue;
-      // ms: other -> this basis; msO: this -> other basis
+    C up[3] = {C(0), C(0), C(0)}, down[3] = {C(0), C(0), C(0)}, first[3] = {C(0), C(0), C(0)};
+    int nO = 0;
+#pragma unroll
+    for (int k = 0; k < NF; k++) {
+      int32_t sf = valid ? v.cellFace[aos(i, k, NF)] : kEmptySlot;
+      const int32_t f0 = sf >= 0 ? sf : ~sf;
+      const int side = sf >= 0 ? 0 : 1;
+      int32_t j = -1;
+      if (sf != kEmptySlot) j = side == 0 ? v.faceR[f0] : v.faceL[f0];
+      // every lane runs every slot (the shuffles below need all 32 lanes); a slot without an interior
+      // neighbour computes on this cell's own data and is not accumulated
+      const bool has = j >= 0;
+      const int64_t jj = has ? j : (valid ? i : 0);
+      const int64_t ff = has ? f0 : 0;
       const int eMs = side == 0 ? kMsR2L : kMsL2R, eMsO = side == 0 ? kMsL2R : kMsR2L;
-      double uOO[5][4];
-      for (int q = 0; q < 5; q++) for (int c = 0; c < 4; c++) uOO[q][c] = (double)urec[(int64_t)j * 20 + q * 4 + c];
-      if (pass == 1) {
-        for (int q = 2; q < 5; q++)
-          for (int c = 0; c < 4; c++) {
-            double s = 0;
-            for (int t = 2; t < 5; t++) s += v.limFace[aos(f, eMsO + q * 5 + t, kLimE)] * uFaces[k][t - 2][c];
-            uOO[q][c] = s;
-          }
-      }
-      double oin[3][4], tin[3][4];
-      for (int r = 0; r < nr; r++)
-        for (int c = 0; c < 4; c++) {
-          double s = 0;
-          for (int q = 0; q < 5; q++) s += v.limFace[aos(f, eMs + (ls + r) * 5 + q, kLimE)] * uOO[q][c];
-          oin[r][c] = s;
-          tin[r][c] = (double)ri[(ls + r) * 4 + c];
+      C uOO[5];
+      for (int q = 0; q < 5; q++) uOO[q] = urec[jj * 20 + q * 4 + c];
+      if (V3 && pass == 1) {  // successive SR: the neighbour's rows 2..4 from this cell's P2 results
+        for (int q = 2; q < 5; q++) {
+          C s = C(0);
+          for (int t = 2; t < 5; t++) s += (C)ms[aos(ff, eMsO + q * 5 + t, kLimE)] * uFaces[k][t - 2];
+          uOO[q] = s;
         }
-      const double* uj = &v.u[(int64_t)j * 4];
-      const double* uL = side ? uj : ui;
-      const double* uR = side ? ui : uj;
-      double Lm[4][4], Rm[4][4];
-      char_matrices(v.gamma, uL, uR, v.faceNormal[2 * f], v.faceNormal[2 * f + 1], Lm, Rm);
+      }
+      double uo[4];
+      for (int q = 0; q < 4; q++) uo[q] = has ? v.u[jj * 4 + q] : ui[q];
+      const int64_t f = ff;
+      C Lrow[4], Rrow[4];
+      char_rows<C>(c, gamma, side ? uo : ui, side ? ui : uo, (C)v.faceNormal[2 * f], (C)v.faceNormal[2 * f + 1],
+                   Lrow, Rrow);
       for (int r = 0; r < nr; r++) {
-        double co[4], ct[4], lim[4];
-        for (int a = 0; a < 4; a++) {
-          double so = 0, st2 = 0;
-          for (int q = 0; q < 4; q++) { so += Lm[a][q] * oin[r][q]; st2 += Lm[a][q] * tin[r][q]; }
-          co[a] = so; ct[a] = st2;
+        C oin = C(0);
+        for (int q = 0; q < 5; q++) oin += (C)ms[aos(f, eMs + (ls + r) * 5 + q, kLimE)] * uOO[q];
+        const C tin = ri[ls + r];
+        // characteristic components co[c] = L[c] . oin, ct[c] = L[c] . tin over the group's lanes
+        C co = C(0), ct = C(0);
+        for (int q = 0; q < 4; q++) {
+          const C oq = __shfl_sync(0xffffffffu, oin, q, 4), tq = __shfl_sync(0xffffffffu, tin, q, 4);
+          co += Lrow[q] * oq;
+          ct += Lrow[q] * tq;
         }
-        for (int a = 0; a < 4; a++) lim[a] = wbap_biway(ct[a], co[a], 1.0);
-        for (int a = 0; a < 4; a++) {
-          double s = 0;
-          for (int q = 0; q < 4; q++) s += Rm[a][q] * lim[q];
-          if (pass == 0) uFaces[k][r][a] = s;
-          // FWBAP_L2_Multiway accumulation against uOthers[0] = this cell's coefficients
-          double u0 = (double)ri[(ls + r) * 4 + a];
-          double ti = u0 / (fabs(s) + sm4) * signE(s);
-          down[r][a] += (ti * ti) * (ti * ti);
-          up[r][a] += ti * ti * ti;
+        const C limc = wbap_biway(ct, co, V3 ? C(1) : nStd);
+        C sback = C(0);  // back to conservative variables: R[c] . lim
+        for (int q = 0; q < 4; q++) sback += Rrow[q] * __shfl_sync(0xffffffffu, limc, q, 4);
+        if (!has) continue;
+        if (V3) {
+          if (pass == 0) uFaces[k][r] = sback;
+          wbap_multi_term(ri[ls + r], sback, up[r], down[r]);
+        } else if (nO == 0) {
+          first[r] = sback;
+        } else {
+          wbap_multi_term(first[r], sback, up[r], down[r]);
         }
       }
+      if (has) nO++;
     }
-    for (int r = 0; r < nr; r++)
-      for (int c = 0; c < 4; c++) {
-        double u0 = (double)ri[(ls + r) * 4 + c];
-        res[ls + r][c] = u0 * (up[r][c] + v.nStd) / (down[r][c] + v.nStd);
-      }
+    for (int r = 0; r < nr; r++) {
+      if (V3) res[ls + r] = ri[ls + r] * (up[r] + nStd) / (down[r] + nStd);
+      else if (nO > 0) res[ls + r] = first[r] * (up[r] + C(1)) / (down[r] + C(1));
+    }
   }
-  for (int q = 0; q < 5; q++) for (int c = 0; c < 4; c++) o[q * 4 + c] = (T)res[q][c];
+  if (valid)
+    for (int q = 0; q < 5; q++) o[q * 4 + c] = (T)res[q];
 }
 
 }  // namespace dg

@@ -255,7 +255,8 @@ struct CellFrame {
   double moment[5];  // moments of m_1..m_5 (m_0 = 1 has moment 1)
 };
 
-DG_HD void p2_monomials(double xi, double eta, double m[5]) {
+template <class C>
+DG_HD void p2_monomials(C xi, C eta, C m[5]) {
   m[0] = xi; m[1] = eta; m[2] = xi * xi; m[3] = xi * eta; m[4] = eta * eta;
 }
 
@@ -268,19 +269,22 @@ DG_HD void p2_frame_coords(const CellFrame& f, double x, double y, double& xi, d
 
 // value, gradient and Hessian rows of the basis at frame coordinates (xi, eta), from the frame's
 // Pinv and moments alone
-DG_HD void p2_diffs_at(const double Q[2][2], const double moment[5], double xi, double eta, double D[6][5]) {
-  double m[5];
+// basis value and derivative rows at frame coordinates (xi, eta), in the arithmetic type C
+template <class C>
+DG_HD void p2_diffs_at(const C Q[2][2], const C moment[5], C xi, C eta, C D[6][5]) {
+  C m[5];
   p2_monomials(xi, eta, m);
   for (int k = 0; k < 5; k++) D[0][k] = m[k] - moment[k];
   // d(xi)/dx = Q[0][0], d(xi)/dy = Q[0][1], d(eta)/dx = Q[1][0], d(eta)/dy = Q[1][1]
-  double gxi[5] = {1, 0, 2 * xi, eta, 0};   // dm/dxi
-  double get[5] = {0, 1, 0, xi, 2 * eta};   // dm/deta
+  const C gxi[5] = {C(1), C(0), 2 * xi, eta, C(0)};  // dm/dxi
+  const C get[5] = {C(0), C(1), C(0), xi, 2 * eta};  // dm/deta
   for (int k = 0; k < 5; k++) {
     D[1][k] = gxi[k] * Q[0][0] + get[k] * Q[1][0];
     D[2][k] = gxi[k] * Q[0][1] + get[k] * Q[1][1];
   }
   // second derivatives: Hxi = {m_xixi, m_xieta, m_etaeta} per monomial
-  double hxx[5] = {0, 0, 2, 0, 0}, hxy[5] = {0, 0, 0, 1, 0}, hyy[5] = {0, 0, 0, 0, 2};
+  const C hxx[5] = {C(0), C(0), C(2), C(0), C(0)}, hxy[5] = {C(0), C(0), C(0), C(1), C(0)},
+          hyy[5] = {C(0), C(0), C(0), C(0), C(2)};
   for (int k = 0; k < 5; k++) {
     // d2/dxa dxb = sum_ij H_ij Q[i][a] Q[j][b]
     D[3][k] = hxx[k] * Q[0][0] * Q[0][0] + 2 * hxy[k] * Q[0][0] * Q[1][0] + hyy[k] * Q[1][0] * Q[1][0];
@@ -309,28 +313,32 @@ DG_HD void p2_values(const CellFrame& f, double x, double y, double v[5]) {
 // as a sum of squares: conj(I,J) = sum_a (T_a D_I)^T (T_a D_J).  proj() forms
 // the six rows T_a D for one side.  The mixed second-derivative row keeps the
 // reference's coefficients {n0 t0, 2 n0 t1, n1 t1}.
-struct FaceFunctional {
-  double t[6][6];  // t[a][r]: weight of derivative row r in term a
+template <class C>
+struct FaceFunctionalT {
+  C t[6][6];  // t[a][r]: weight of derivative row r in term a
 };
+using FaceFunctional = FaceFunctionalT<double>;
 
-DG_HD FaceFunctional make_functional(const double W[6], double unx, double uny, double tangWeight,
-                                     double tangModifier, int modLoc) {
-  FaceFunctional F;
-  for (int a = 0; a < 6; a++) for (int r = 0; r < 6; r++) F.t[a][r] = 0;
-  double w2r = 0, length = 0;
-  if (fabs(W[1]) >= 1e-50 || fabs(W[2]) >= 1e-50) {
+// the functional's rows, in the arithmetic type C (the weights' zero test and 1e-50 threshold are the
+// reference's; in FP32 a weight below 1e-50 is zero already)
+template <class C>
+DG_HD FaceFunctionalT<C> make_functional(const C W[6], C unx, C uny, C tangWeight, C tangModifier, int modLoc) {
+  FaceFunctionalT<C> F;
+  for (int a = 0; a < 6; a++) for (int r = 0; r < 6; r++) F.t[a][r] = C(0);
+  C w2r = C(0), length = C(0);
+  if (fabs((double)W[1]) >= 1e-50 || fabs((double)W[2]) >= 1e-50) {
     w2r = fabs(W[1]) >= fabs(W[2]) ? W[3] / (W[1] * W[1]) : W[5] / (W[2] * W[2]);
     length = sqrt(W[1] * W[1] + W[2] * W[2]);
   }
-  double n0 = unx * length, n1 = uny * length;
-  double tf = tangWeight * tangModifier * (modLoc == 1 ? tangModifier : 1.0);
-  double t0 = -n1 * tf, t1 = n0 * tf;
-  double tm = modLoc == 0 ? tangModifier : 1.0;  // sqrt of the reference's sqr(tangModifier)
+  const C n0 = unx * length, n1 = uny * length;
+  const C tf = tangWeight * tangModifier * (modLoc == 1 ? tangModifier : C(1));
+  const C t0 = -n1 * tf, t1 = n0 * tf;
+  const C tm = modLoc == 0 ? tangModifier : C(1);  // sqrt of the reference's sqr(tangModifier)
   F.t[0][0] = W[0];
   F.t[1][1] = n0; F.t[1][2] = n1;
   F.t[2][1] = t0 * tm; F.t[2][2] = t1 * tm;
   F.t[3][3] = n0 * n0 * w2r; F.t[3][4] = 2 * n0 * n1 * w2r; F.t[3][5] = n1 * n1 * w2r;
-  double s2 = sqrt(2.0) * tm;
+  const C s2 = sqrt(C(2)) * tm;
   F.t[4][3] = n0 * t0 * w2r * s2; F.t[4][4] = 2 * n0 * t1 * w2r * s2; F.t[4][5] = n1 * t1 * w2r * s2;
   F.t[5][3] = t0 * t0 * w2r * tm; F.t[5][4] = 2 * t0 * t1 * w2r * tm; F.t[5][5] = t1 * t1 * w2r * tm;
   return F;

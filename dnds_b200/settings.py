@@ -74,7 +74,9 @@ def make_settings(cfg: dict) -> Settings:
     s.anisotropic_lengths = 1 if vfv.get("anisotropicLengths", False) else 0
     s.weight_scheme_geom = WEIGHT_GEOM[vfv.get("weightSchemeGeom", "None")]
     s.weight_scheme_dir = WEIGHT_DIR[vfv.get("weightSchemeDir", "None")]
-    s.limiter = 1 if cfg.get("useLimiter", False) else 0
+    # limiterProcedure (DNDS_FV_EulerSolver.hpp:108): 0 = ReconstructionWBAPLimitFacialV2 (3WBAP, the
+    # reference's default), 1 = ReconstructionWBAPLimitFacialV3 (CWBAP); settings.limiter 2 and 1
+    s.limiter = (1 if int(cfg.get("limiterProcedure", 0)) == 1 else 2) if cfg.get("useLimiter", False) else 0
     s.weight_len_scale = float(vfv.get("weightLenScale", 1.0))
     s.wall_weight = float(vfv.get("wallWeight", 1.0))
     s.far_weight = float(vfv.get("farWeight", 0.0))
@@ -124,10 +126,11 @@ ISENTROPIC_VORTEX = {
     },
 }
 
-# vfvSetting of data/euler_config_2DRiemann.json:60-91, HLLC flux, CWBAP limiter
+# vfvSetting of data/euler_config_2DRiemann.json:60-91, HLLC flux, CWBAP limiter (limiterProcedure 1, :27)
 RIEMANN_2D = {
     "recOrder": 2,
     "useLimiter": True,
+    "limiterProcedure": 1,
     "vfvSetting": {
         "SOR_Instead": False,
         "JacobiRelax": 1.0,

@@ -127,6 +127,12 @@ class Solver:
         self._check(self.L.dndsg_limiter_wbap(self.h, int(if_all), _p(ind) if indicator else None, self.stream))
         return ind
 
+    def ReconstructionWBAPLimitFacialV2(self, if_all: bool = False, indicator: bool = False):
+        """3WBAP limiting (DNDS_FV_VR.hpp:1749-2047) of the resident coefficients in place."""
+        ind = np.empty(self.N) if indicator else None
+        self._check(self.L.dndsg_limiter_wbap_v2(self.h, int(if_all), _p(ind) if indicator else None, self.stream))
+        return ind
+
     def EvaluateDt(self, cfl: float, max_dt: float = 1e100, use_local_dt: bool = False) -> float:
         dmin = C.c_double()
         self._check(self.L.dndsg_eval_dt(self.h, cfl, max_dt, int(use_local_dt), C.byref(dmin), self.stream))

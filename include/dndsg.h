@@ -74,7 +74,8 @@ typedef struct {
   int32_t anisotropic_lengths;
   int32_t weight_scheme_geom;    /* 0 None, 1 D, 2 S, 3 SDHQM */
   int32_t weight_scheme_dir;     /* 0 None, 1 optHQM */
-  int32_t limiter;               /* 0 none, 1 CWBAP limiter in every stage */
+  int32_t limiter;               /* limiter in every stage: 0 none, 1 CWBAP (V3, limiterProcedure 1),
+                                    2 3WBAP (V2, limiterProcedure 0) */
   double weight_len_scale;
   double wall_weight;
   double far_weight;
@@ -138,6 +139,14 @@ int dndsg_vr_jacobi_step(dndsg_ctx* ctx, int nsweeps, double* inc_out, void* str
  * CWBAP limiting of the resident urec in place.  indicator_out (nullable) gets
  * the smoothness indicator per cell [n_cells]. */
 int dndsg_limiter_wbap(dndsg_ctx* ctx, int if_all, double* indicator_out, void* stream);
+
+/* VRFiniteVolume2D::ReconstructionWBAPLimitFacialV2 (DNDS_FV_VR.hpp:1749-2047,
+ * "3WBAP", limiterProcedure 0): the same indicator; then the P2 rows of every
+ * listed cell, then its P1 rows against the neighbours' P2-limited
+ * coefficients; biway WBAP with n = WBAP_nStd, multiway with n = 1 centred on
+ * the first neighbour (faces in element-local order).  In place, as above.
+ * The stage compositions run this one when settings.limiter = 2. */
+int dndsg_limiter_wbap_v2(dndsg_ctx* ctx, int if_all, double* indicator_out, void* stream);
 
 /* EulerEvaluator::EvaluateDt (DNDS_FV_EulerEvaluator.cpp:14-183): per-cell dt
  * into DNDSG_BUF_DT and the face spectral data used by the Roe entropy fix.

@@ -507,6 +507,40 @@ inline void compress_rec_part(const double* umean, const double* inc, double* re
 }
 
 // ------------------------------------------------------------------ setup
+// A cell's faces in element-local face order, the order of the reference's cell2face (vol2face is
+// filled per local face iface, DNDS_Mesh.hpp:288-320): face k joins nodes k and k+1 (FaceNodeList of
+// TRI3 / QUAD4, DNDS_Elements.hpp:248-253).  A face is matched by its node pair, or -- a periodic face
+// seen from its translated side -- by its midpoint against the edge midpoint moved by the face shift.
+// Sums over a cell's faces run in this order, and V2's multiway WBAP is centred on the first face.
+void order_cell_faces(const orc_mesh& m, int64_t i, int* faces, int nf) {
+  const int nn = m.cell_nodes[4 * i + 3] < 0 ? 3 : 4;
+  if (nf != nn) return;
+  int out[4] = {-1, -1, -1, -1};
+  bool used[4] = {false, false, false, false};
+  for (int pass = 0; pass < 2; pass++)
+    for (int e = 0; e < nn; e++) {
+      if (out[e] >= 0) continue;
+      const int p = m.cell_nodes[4 * i + e], q = m.cell_nodes[4 * i + (e + 1) % nn];
+      const double mx = 0.5 * (m.node_xy[2 * p] + m.node_xy[2 * q]), my = 0.5 * (m.node_xy[2 * p + 1] + m.node_xy[2 * q + 1]);
+      const double len = std::hypot(m.node_xy[2 * q] - m.node_xy[2 * p], m.node_xy[2 * q + 1] - m.node_xy[2 * p + 1]);
+      for (int k = 0; k < nf && out[e] < 0; k++) {
+        if (used[k]) continue;
+        const int f = faces[k], a = m.face_nodes[2 * f], b = m.face_nodes[2 * f + 1];
+        bool hit = (a == p && b == q) || (a == q && b == p);
+        if (!hit && pass == 1 && m.face_shift) {
+          const double fx = 0.5 * (m.node_xy[2 * a] + m.node_xy[2 * b]), fy = 0.5 * (m.node_xy[2 * a + 1] + m.node_xy[2 * b + 1]);
+          const double sx = m.face_shift[2 * f], sy = m.face_shift[2 * f + 1];
+          for (int sg = -1; sg <= 1 && !hit; sg += 2)
+            hit = std::fabs(mx + sg * sx - fx) + std::fabs(my + sg * sy - fy) < 1e-9 * len;
+        }
+        if (hit) { out[e] = f; used[k] = true; }
+      }
+    }
+  for (int e = 0; e < nn; e++)
+    if (out[e] < 0) return;  // unmatched: keep the given order
+  for (int e = 0; e < nn; e++) faces[e] = out[e];
+}
+
 int setup(orc_ctx& c, const orc_mesh& m) {
   const orc_settings& s = c.s;
   c.N = m.n_cells; c.F = m.n_faces;
@@ -524,6 +558,7 @@ int setup(orc_ctx& c, const orc_mesh& m) {
       c.cg[R].faces[c.cg[R].nface++] = (int)f;
     }
   }
+  for (int64_t i = 0; i < c.N; i++) order_cell_faces(m, i, c.cg[i].faces, c.cg[i].nface);
   // --- cells: ImplicitFiniteVolume2D volumes, initMoment (DNDS_FV_VR.cpp:82-181)
   int bad = 0;
   parallel_for(c.nthreads, c.N, [&](int64_t b, int64_t e) {
@@ -919,8 +954,9 @@ void char_matrices(double gamma, const double* UL, const double* UR, const doubl
   std::memcpy(Rm, R, sizeof(R));
 }
 
-// ReconstructionWBAPLimitFacialV3 (DNDS_FV_VR.hpp:2053-2329), normWBAP=false
-void limiter_wbap(orc_ctx& c, bool ifAll, double* indicator_out) {
+// the smoothness indicator of both WBAP limiters (DNDS_FV_VR.hpp:2075-2138 for V3, the same
+// integrals at :1771-1836 for V2): si = sqrt(max over rho, E of sum_f IJI / ISI) * P^2
+std::vector<double> limiter_indicator(orc_ctx& c) {
   const int nv = c.nv;
   const int I4 = 3;
   std::vector<double> ind(c.N);
@@ -964,6 +1000,13 @@ void limiter_wbap(orc_ctx& c, bool ifAll, double* indicator_out) {
       ind[i] = std::sqrt(smax) * porder2;
     }
   });
+  return ind;
+}
+
+// ReconstructionWBAPLimitFacialV3 (DNDS_FV_VR.hpp:2053-2329), normWBAP=false
+void limiter_wbap(orc_ctx& c, bool ifAll, double* indicator_out) {
+  const int nv = c.nv;
+  std::vector<double> ind = limiter_indicator(c);
   if (indicator_out) std::memcpy(indicator_out, ind.data(), sizeof(double) * c.N);
   const double scale = c.s.wbap_smooth_indicator_scale;
   const double nStd = c.s.wbap_n_std;
@@ -1056,6 +1099,101 @@ void limiter_wbap(orc_ctx& c, bool ifAll, double* indicator_out) {
     if (ind[i] < scale && !ifAll) continue;
     for (int k = 0; k < 5 * nv; k++) c.urec[i * 5 * nv + k] = c.urec1[i * 5 * nv + k];
   }
+}
+
+// ReconstructionWBAPLimitFacialV2 (DNDS_FV_VR.hpp:1749-2047, "3WBAP", limiterProcedure 0), normWBAP=false.
+// The indicator as V3.  Then order by order over all cells -- P2 rows 2..4, then P1 rows 0..1 -- each pass
+// reading the coefficients as the previous one left them (uRecNewBuf; after the P2 pass the listed
+// cells' rows 2..4 are limited): against every neighbour j, the secondary reconstruction of j's whole
+// coefficient set in this cell's basis (matrixSecondary * uRecNewBuf[j], rows of the pass), both sides
+// projected to characteristic space (M = L(face mean)), FWBAP_L2_Biway with n = WBAP_nStd, back with R;
+// then FWBAP_L2_Multiway over those results with n = 1, centred on the FIRST neighbour's result (the
+// reference's uOthers holds only the neighbours' results, in cell2face order).  A cell with no
+// interior face keeps its coefficients (the reference would read past an empty list there).
+void limiter_wbap_v2(orc_ctx& c, bool ifAll, double* indicator_out) {
+  const int nv = c.nv;
+  std::vector<double> ind = limiter_indicator(c);
+  if (indicator_out) std::memcpy(indicator_out, ind.data(), sizeof(double) * c.N);
+  const double scale = c.s.wbap_smooth_indicator_scale;
+  const double nStd = c.s.wbap_n_std;
+  const double sm4 = std::pow(kVerySmall, 1.0 / 4);
+  std::vector<double>& buf = c.urec;   // uRecNewBuf (starts as uRec)
+  std::vector<double>& out = c.urec1;  // uRecNewBuf1
+  for (int pass = 0; pass < 2; pass++) {
+    const int ls = pass == 0 ? 2 : 0, le = pass == 0 ? 4 : 1, nr = le - ls + 1;
+    parallel_for(c.nthreads, c.N, [&](int64_t b, int64_t e) {
+      for (int64_t i = b; i < e; i++) {
+        if (ind[i] < scale && !ifAll) continue;
+        const CellGeo& g = c.cg[i];
+        double first[3][kMaxV], up[3][kMaxV], down[3][kMaxV];
+        for (int r = 0; r < 3; r++) for (int v = 0; v < kMaxV; v++) { first[r][v] = up[r][v] = down[r][v] = 0; }
+        int nO = 0;
+        for (int k = 0; k < g.nface; k++) {
+          const FaceGeo& f = c.fg[g.faces[k]];
+          const int side = f.L == i ? 0 : 1;
+          const int j = side == 0 ? f.R : f.L;
+          if (j < 0) continue;
+          const double nn = std::sqrt(sqr(f.ncenter[0]) + sqr(f.ncenter[1]));
+          const double un[2] = {f.ncenter[0] / nn, f.ncenter[1] / nn};
+          const double(*ms)[5] = side ? f.msL2R : f.msR2L;  // other -> this
+          double uOtherIn[3][kMaxV], uThisIn[3][kMaxV];
+          for (int r = 0; r < nr; r++)
+            for (int v = 0; v < nv; v++) {
+              double s = 0;
+              for (int q = 0; q < 5; q++) s += ms[ls + r][q] * buf[(j * 5 + q) * nv + v];
+              uOtherIn[r][v] = s;
+              uThisIn[r][v] = buf[(i * 5 + ls + r) * nv + v];
+            }
+          const double* uR = side ? &c.u[i * nv] : &c.u[j * nv];
+          const double* uL = side ? &c.u[j * nv] : &c.u[i * nv];
+          double Lm[4][4], Rm[4][4];
+          char_matrices(c.s.gamma, uL, uR, un, Lm, Rm);
+          double cO[3][kMaxV], cT[3][kMaxV], lim[3][kMaxV];
+          for (int r = 0; r < nr; r++)
+            for (int a = 0; a < nv; a++) {
+              double so = 0, st = 0;
+              for (int q = 0; q < nv; q++) { so += Lm[a][q] * uOtherIn[r][q]; st += Lm[a][q] * uThisIn[r][q]; }
+              cO[r][a] = so; cT[r][a] = st;
+            }
+          // FWBAP_L2_Biway(uThis, uOther, out, WBAP_nStd)
+          for (int r = 0; r < nr; r++)
+            for (int a = 0; a < nv; a++) {
+              const double u1 = cT[r][a], u2 = cO[r][a];
+              const double frac = u1 / (std::fabs(u2) + 1e-12) * signE(u2);
+              const double th1 = frac * frac * frac, th2 = sqr(frac) * sqr(frac);
+              lim[r][a] = u1 * (nStd + th1) / (nStd + th2);
+            }
+          for (int r = 0; r < nr; r++)
+            for (int a = 0; a < nv; a++) {
+              double s = 0;
+              for (int q = 0; q < nv; q++) s += Rm[a][q] * lim[r][q];
+              if (nO == 0) {
+                first[r][a] = s;
+              } else {  // FWBAP_L2_Multiway accumulation, uOthers[0] = the first neighbour's result
+                const double ti = first[r][a] / (std::fabs(s) + sm4) * signE(s);
+                down[r][a] += sqr(ti) * sqr(ti);
+                up[r][a] += ti * ti * ti;
+              }
+            }
+          nO++;
+        }
+        for (int r = 0; r < nr; r++)
+          for (int v = 0; v < nv; v++)
+            out[(i * 5 + ls + r) * nv + v] =
+                nO ? first[r][v] * (up[r][v] + 1.0) / (down[r][v] + 1.0) : buf[(i * 5 + ls + r) * nv + v];
+      }
+    });
+    for (int64_t i = 0; i < c.N; i++) {
+      if (ind[i] < scale && !ifAll) continue;
+      for (int k = ls * nv; k < (le + 1) * nv; k++) buf[i * 5 * nv + k] = out[i * 5 * nv + k];
+    }
+  }
+}
+
+// the limiter of the stage composition: limiterProcedure 1 (CWBAP, V3) or 0 (3WBAP, V2)
+void limiter_stage(orc_ctx& c) {
+  if (c.s.limiter == 2) limiter_wbap_v2(c, false, nullptr);
+  else if (c.s.limiter) limiter_wbap(c, false, nullptr);
 }
 
 // ------------------------------------------------------------------ dt
@@ -1762,6 +1900,10 @@ int orc_vr_step(orc_ctx* c, int nsweeps) {
 }
 double orc_vr_last_increment(orc_ctx* c) { return c->lastInc; }
 
+int orc_limiter_wbap_v2(orc_ctx* c, int if_all, double* ind) {
+  limiter_wbap_v2(*c, if_all != 0, ind);
+  return 0;
+}
 int orc_limiter_wbap(orc_ctx* c, int if_all, double* ind) {
   limiter_wbap(*c, if_all != 0, ind);
   return 0;
@@ -1798,7 +1940,7 @@ int orc_ssprk3_step(orc_ctx* c, double dt, double t) {
   const double coef[3] = {1.0, 0.25, 2.0 / 3.0};
   for (int st = 0; st < 3; st++) {
     vr_sweep(*c);
-    if (c->s.limiter) limiter_wbap(*c, false, nullptr);
+    if (c->s.limiter) limiter_stage(*c);
     eval_rhs(*c, t + cst[st] * dt, rhs.data(), nullptr, nullptr);
     for (int64_t k = 0; k < n; k++) rhs[k] *= dt;
     for (int64_t k = 0; k < n; k++) c->u[k] += rhs[k];
@@ -1862,7 +2004,7 @@ int orc_implicit_iteration(orc_ctx* c, double cfl, double dt, double alpha, cons
   std::vector<double> dTau(c->N), rhs(n), inc(n, 0.0);
   for (int64_t i = 0; i < c->N; i++) dTau[i] = c->dtCell[i] / alpha;
   for (int k = 0; k < n_rec; k++) vr_sweep(*c);
-  if (c->s.limiter) limiter_wbap(*c, false, nullptr);
+  if (c->s.limiter) limiter_stage(*c);
   eval_rhs(*c, t, rhs.data(), nullptr, nullptr);
   for (int64_t k = 0; k < n; k++) {
     rhs[k] *= alpha;
@@ -1944,7 +2086,7 @@ int orc_dual_step(orc_ctx* c, const orc_dual_settings* d, double dt, double t, c
     eval_dt(*c, d->cfl, 1e100, true, &dtMin);
     for (int64_t i = 0; i < c->N; i++) dTau[i] = c->dtCell[i] / alphaDiag;
     for (int k = 0; k < d->n_rec; k++) vr_sweep(*c);
-    if (c->s.limiter) limiter_wbap(*c, false, nullptr);
+    if (c->s.limiter) limiter_stage(*c);
     eval_rhs(*c, t + ct * dt, rhs.data(), nullptr, nullptr);
     compose(rhs);
     lusgs_matrix_init(*c, dTau.data(), dt, alphaDiag);

@@ -71,7 +71,7 @@ typedef struct {
   int32_t anisotropic_lengths;
   int32_t weight_scheme_geom;    /* 0 None, 1 D, 2 S, 3 SDHQM */
   int32_t weight_scheme_dir;     /* 0 None, 1 optHQM */
-  int32_t limiter;               /* 0 none, 1 CWBAP (V3) */
+  int32_t limiter;               /* 0 none, 1 CWBAP (V3, limiterProcedure 1), 2 3WBAP (V2, limiterProcedure 0) */
   double weight_len_scale;
   double wall_weight;
   double far_weight;
@@ -118,6 +118,8 @@ int orc_vr_step(orc_ctx* c, int nsweeps);
 double orc_vr_last_increment(orc_ctx* c);
 /* ReconstructionWBAPLimitFacialV3 on the internal urec (in place) */
 int orc_limiter_wbap(orc_ctx* c, int if_all, double* indicator_out /*[n] or NULL*/);
+/* ReconstructionWBAPLimitFacialV2 (3WBAP, limiterProcedure 0), in place on urec */
+int orc_limiter_wbap_v2(orc_ctx* c, int if_all, double* indicator_out /*[n] or NULL*/);
 /* EvaluateDt */
 int orc_eval_dt(orc_ctx* c, double cfl, double max_dt, int use_local_dt, double* dt_out, double* dt_min);
 /* EvaluateRHS on the internal u/urec; rhs_out [n][nvars]; wall_flux [nvars] may be NULL */

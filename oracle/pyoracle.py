@@ -90,6 +90,7 @@ def lib():
         L.orc_vr_last_increment.argtypes = [vp]
         L.orc_vr_last_increment.restype = dbl
         L.orc_limiter_wbap.argtypes = [vp, i32, vp]
+        L.orc_limiter_wbap_v2.argtypes = [vp, i32, vp]
         L.orc_eval_dt.argtypes = [vp, dbl, dbl, i32, vp, vp]
         L.orc_eval_rhs.argtypes = [vp, dbl, vp, vp]
         L.orc_face_values.argtypes = [vp, dbl, vp]
@@ -224,6 +225,12 @@ class Oracle:
     def limiter(self, if_all=False):
         ind = np.empty(self.N)
         lib().orc_limiter_wbap(self.h, int(if_all), _p(ind))
+        return ind
+
+    def limiter_v2(self, if_all=False):
+        """ReconstructionWBAPLimitFacialV2 (3WBAP) in place; returns the smoothness indicator."""
+        ind = np.empty(self.N)
+        lib().orc_limiter_wbap_v2(self.h, int(if_all), _p(ind))
         return ind
 
     def eval_dt(self, cfl, max_dt=1e100, use_local_dt=False):

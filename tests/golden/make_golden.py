@@ -55,18 +55,24 @@ def perturbed_quadrants(m):
     return G.cell_average(m, f)
 
 
-def make_limiter_case():
-    """2-D Riemann mesh with the CWBAP limiter: indicator and limited face states
-    after 3 VR sweeps, then 2 SSP-RK3 steps with the limiter in every stage."""
+def make_limiter_case(procedure=1):
+    """2-D Riemann mesh with the CWBAP limiter (procedure 1, ReconstructionWBAPLimitFacialV3) or the
+    3WBAP limiter (procedure 0, ReconstructionWBAPLimitFacialV2): indicator and limited face states
+    after 3 VR sweeps, the same with every cell limited (from a fresh reconstruction), then 2 SSP-RK3
+    steps with the limiter in every stage."""
     m = M.riemann_mesh(16, jitter=0.15, seed=4321)
-    cfg = S.preset("riemann")
+    cfg = S.preset("riemann", limiterProcedure=procedure)
     o = pyoracle.Oracle(m, cfg, n_threads=1)
+    lim = o.limiter if procedure == 1 else o.limiter_v2
     u0 = G.quadrant_states(m, S.RIEMANN_2D_STATES)
     o.set_u(u0)
     o.vr_step(3)
-    ind = o.limiter(False)
+    ind = lim(False)
     fv = o.face_values(0.0)
-    o.limiter(True)
+    # every cell limited, from the same unlimited reconstruction
+    o.set_urec(np.zeros((m.n_cells, 5, 4)))
+    o.vr_step(3)
+    lim(True)
     fv_all = o.face_values(0.0)
     up = perturbed_quadrants(m)
     o.set_u(up)
@@ -82,7 +88,9 @@ def make_limiter_case():
 
 def make_case(name):
     if name == "riemann_tri16_limiter":
-        return make_limiter_case()
+        return make_limiter_case(1)
+    if name == "riemann_tri16_limiter_v2":
+        return make_limiter_case(0)
     mk, pre, init = CASES[name]
     m = mk()
     cfg = S.preset(pre, useLimiter=False)
@@ -105,7 +113,7 @@ def make_case(name):
     return dict(u0=u0, face_values=fv, dt=dt, dtmin=dtmin, rhs=rhs, u_rk2=u2, t_rk2=t)
 
 
-LIMITER_CASES = ["riemann_tri16_limiter"]
+LIMITER_CASES = ["riemann_tri16_limiter", "riemann_tri16_limiter_v2"]
 
 if __name__ == "__main__":
     pyoracle.build()

@@ -77,18 +77,25 @@ def test_fp32_bulk_close_to_golden(name):
     assert _rel(rhs, ref["rhs"]) < 2e-5
 
 
+@pytest.mark.parametrize("procedure", [1, 0])
 @pytest.mark.parametrize("precision,tol", [(0, 1e-10), (1, 1e-4)])
-def test_limiter_matches_golden(precision, tol):
-    """CWBAP limiter (ReconstructionWBAPLimitFacialV3) and SSP-RK3 with the limiter, 2-D Riemann mesh."""
+def test_limiter_matches_golden(precision, tol, procedure):
+    """The WBAP limiters and SSP-RK3 with the limiter in every stage, 2-D Riemann mesh: CWBAP
+    (limiterProcedure 1, ReconstructionWBAPLimitFacialV3) and 3WBAP (limiterProcedure 0,
+    ReconstructionWBAPLimitFacialV2)."""
     m = M.riemann_mesh(16, jitter=0.15, seed=4321)
-    ref = np.load(os.path.join(GOLDEN, "riemann_tri16_limiter.npz"))
-    s = _solver(m, S.preset("riemann"), precision)
+    name = "riemann_tri16_limiter" if procedure == 1 else "riemann_tri16_limiter_v2"
+    ref = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    s = _solver(m, S.preset("riemann", limiterProcedure=procedure), precision)
+    limit = s.ReconstructionWBAPLimitFacialV3 if procedure == 1 else s.ReconstructionWBAPLimitFacialV2
     s.set_u(ref["u0"])
     s.ReconstructionJacobiStep(3)
-    ind = s.ReconstructionWBAPLimitFacialV3(False, indicator=True)
+    ind = limit(False, indicator=True)
     assert _rel(ind, ref["indicator"]) < tol
     assert _rel(s.face_values(0.0), ref["face_values_lim"]) < tol
-    s.ReconstructionWBAPLimitFacialV3(True)
+    s.set_urec(np.zeros((m.n_cells, 5, 4)))
+    s.ReconstructionJacobiStep(3)
+    limit(True)
     assert _rel(s.face_values(0.0), ref["face_values_limall"]) < tol
     # multi-step parity on a smoothly perturbed state (no coefficient is zero up to rounding,
     # where the reference's sign(u2) in the biway WBAP is discontinuous)
