@@ -306,10 +306,9 @@ __global__ void k_setup_lim_compact(MeshView m, const CellSetup* cells, const do
   const int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   setup_limiter_compact<T>(f, m, cells, faceW, g, cellFr);
 }
-// 2 blocks per SM (at 3 the FP32 variant spills the basis derivatives it rebuilds from the cell frames;
-// measured per FP32 SSP-RK3 step of the 8,388,608-triangle Riemann problem: 2 blocks 11.10 ms, 3: 11.25)
+// FP64: 2 blocks per SM.  FP32 (FP32 arithmetic, 95 registers at 2 blocks): 3 blocks per SM
 template <class T>
-__global__ void __launch_bounds__(kBlock, 2) k_lim_face(LimView v, const T* urec, int32_t* count) {
+__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 3 : 2) k_lim_face(LimView v, const T* urec, int32_t* count) {
   int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (f == 0) *count = 0;  // the list of cells to limit, filled by the next launch
   if (f < v.F) limiter_face_indicator<T>(f, v, urec);
@@ -336,7 +335,7 @@ __global__ void __launch_bounds__(kBlock) k_lim_cell_indicator(LimView v, int32_
 // ReconstructionWBAPLimitFacialV2.  A grid-stride loop whose trip count is the same for all lanes of a
 // warp (eight cells per warp per trip), so the width-4 shuffles always have all 32 lanes
 template <class T, bool V3, int PASS, int NF>
-__global__ void __launch_bounds__(kBlock) k_lim_apply4(LimView v, const T* urec, T* buf, const int32_t* list,
+__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 4 : 2) k_lim_apply4(LimView v, const T* urec, T* buf, const int32_t* list,
                                                        const int32_t* count) {
   const int64_t n = *count;
   const int lane = threadIdx.x & 31;
@@ -981,7 +980,7 @@ int setup_run(dndsg_ctx* c, const dndsg_mesh_desc* md) {
   k_setup_mlp_geom<<<grid_for(N), kBlock>>>(m, cells, c->cellFace, c->nfmax, c->faceCenter, c->mlpGeom);
   if ((rc = check_launch(c))) return rc;
   if (c->s.limiter) {
-    if ((rc = dalloc(c, c->limFace, sizeof(T) * aos_size(F, kLimE)))) return rc;
+    if ((rc = dalloc(c, c->limFace, sizeof(T) * kLimStride * F))) return rc;
     if ((rc = dalloc(c, c->faceInd, sizeof(double) * 4 * F))) return rc;
     if ((rc = dalloc(c, c->indicator, sizeof(double) * N))) return rc;
     if ((rc = dalloc(c, c->limList, sizeof(int32_t) * N)) || (rc = dalloc(c, c->limCount, sizeof(int32_t)))) return rc;
@@ -1251,6 +1250,12 @@ int dndsg_device_buffer(dndsg_ctx* c, int which, void** ptr, int64_t* bytes) {
     case DNDSG_BUF_UREC: *ptr = c->urec; if (bytes) *bytes = (int64_t)c->tsize() * 20 * c->N; return 0;
     case DNDSG_BUF_RHS: *ptr = c->rhs; if (bytes) *bytes = sizeof(double) * 4 * c->N; return 0;
     case DNDSG_BUF_DT: *ptr = c->dt; if (bytes) *bytes = sizeof(double) * c->N; return 0;
+    case DNDSG_BUF_SA_U:
+      if (!c->sa) break;
+      *ptr = c->saU; if (bytes) *bytes = sizeof(double) * c->N; return 0;
+    case DNDSG_BUF_SA_UREC:
+      if (!c->sa) break;
+      *ptr = c->saUrec; if (bytes) *bytes = (int64_t)c->tsize() * 5 * c->N; return 0;
   }
   return fail(c, DNDSG_BAD_ARGUMENT, "unknown buffer id");
 }

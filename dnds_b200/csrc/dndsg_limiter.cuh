@@ -22,11 +22,15 @@
 
 namespace dg {
 
-// per-face data of the limiting pass, tile-major AoSoA with E = kLimE, in the context's precision:
+// per-face data of the limiting pass, one row of kLimStride values per face (the cell-centric limiting
+// pass reads a face's matrix rows together; the row is padded to 16-byte multiples), in the context's
+// precision:
 //   [0, 25)   msR2L (right-cell coefficients -> left basis), row-major
 //   [25, 50)  msL2R
 // (the indicator's data is the compact limG / limCell below)
 constexpr int kLimE = 50;
+constexpr int kLimStride = 52;
+DG_HD int64_t lim_at(int64_t f, int e) { return f * kLimStride + e; }
 constexpr int kMsR2L = 0, kMsL2R = 25;
 // the indicator's compact data, in the context's precision: per face (AoSoA E = kLimG) the frame
 // coordinates (xi, eta) of gauss point 0 in the left and the right cell and the 6 face weights; per
@@ -43,7 +47,7 @@ struct LimView {
   const int32_t* faceR;
   const double* faceNormal;
   const double* faceArea;
-  const void* limFace;     // T [F] AoSoA kLimE (T = the context's precision)
+  const void* limFace;     // T [F][kLimStride] (T = the context's precision)
   const void* limG;        // T [F] AoSoA kLimG (T = the context's precision)
   const void* limCell;     // T [N][kLimCell]
   const double* u;
@@ -66,7 +70,7 @@ template <class T>
 DG_HD bool setup_limiter_face(int64_t f, const MeshView& m, const SetupParams& p, const CellSetup* cells,
                               const double* faceW, T* lim) {
   int32_t L = m.face_cells[2 * f], R = m.face_cells[2 * f + 1];
-  for (int e = 0; e < kLimE; e++) lim[aos(f, e, kLimE)] = T(0);
+  for (int e = 0; e < kLimStride; e++) lim[lim_at(f, e)] = T(0);
   if (R < 0) return true;
   FaceGeom g = face_geom(f, m);
   double sx = m.face_shift ? m.face_shift[2 * f] : 0.0, sy = m.face_shift ? m.face_shift[2 * f + 1] : 0.0;
@@ -77,10 +81,10 @@ DG_HD bool setup_limiter_face(int64_t f, const MeshView& m, const SetupParams& p
   double A[5][5], B[5][5];
   for (int i = 0; i < 5; i++) for (int j = 0; j < 5; j++) { A[i][j] = DL[i + 1][j]; B[i][j] = DR[i + 1][j]; }
   bool ok = lu5_solve(A, B);
-  for (int i = 0; i < 5; i++) for (int j = 0; j < 5; j++) lim[aos(f, kMsR2L + i * 5 + j, kLimE)] = (T)B[i][j];
+  for (int i = 0; i < 5; i++) for (int j = 0; j < 5; j++) lim[lim_at(f, kMsR2L + i * 5 + j)] = (T)B[i][j];
   for (int i = 0; i < 5; i++) for (int j = 0; j < 5; j++) { A[i][j] = DR[i + 1][j]; B[i][j] = DL[i + 1][j]; }
   ok = lu5_solve(A, B) && ok;
-  for (int i = 0; i < 5; i++) for (int j = 0; j < 5; j++) lim[aos(f, kMsL2R + i * 5 + j, kLimE)] = (T)B[i][j];
+  for (int i = 0; i < 5; i++) for (int j = 0; j < 5; j++) lim[lim_at(f, kMsL2R + i * 5 + j)] = (T)B[i][j];
   return ok;
 }
 
@@ -262,75 +266,80 @@ __device__ __forceinline__ void limiter_cell4(bool valid, int64_t i, int c, cons
   for (int q = 0; q < 5; q++) ri[q] = valid ? urec[i * 20 + q * 4 + c] : C(0);
   double ui[4] = {1.0, 0.0, 0.0, 2.5};
   if (valid) for (int k = 0; k < 4; k++) ui[k] = v.u[i * 4 + k];
+  // multiway sums per coefficient row; V2 also keeps the first neighbour's result (its centre)
+  C up[5], down[5], first[5];
+  for (int q = 0; q < 5; q++) up[q] = down[q] = first[q] = C(0);
+  int nO = 0;
+#pragma unroll
+  for (int k = 0; k < NF; k++) {
+    const int32_t sf = valid ? v.cellFace[aos(i, k, NF)] : kEmptySlot;
+    const int32_t f0 = sf >= 0 ? sf : ~sf;
+    const int side = sf >= 0 ? 0 : 1;
+    int32_t j = -1;
+    if (sf != kEmptySlot) j = side == 0 ? v.faceR[f0] : v.faceL[f0];
+    // every lane runs every slot (the shuffles below need all 32 lanes); a slot without an interior
+    // neighbour computes on this cell's own data and is not accumulated
+    const bool has = j >= 0;
+    const int64_t jj = has ? j : (valid ? i : 0);
+    const int64_t f = has ? f0 : 0;
+    const int eMs = side == 0 ? kMsR2L : kMsL2R, eMsO = side == 0 ? kMsL2R : kMsR2L;
+    C uOO[5];
+    for (int q = 0; q < 5; q++) uOO[q] = urec[jj * 20 + q * 4 + c];
+    double uo[4];
+    for (int q = 0; q < 4; q++) uo[q] = has ? v.u[jj * 4 + q] : ui[q];
+    C Lrow[4], Rrow[4];  // the face's characteristic rows, shared by both orders
+    char_rows<C>(c, gamma, side ? uo : ui, side ? ui : uo, (C)v.faceNormal[2 * f], (C)v.faceNormal[2 * f + 1],
+                 Lrow, Rrow);
+    // biway WBAP of coefficient row q against this neighbour, in characteristic space, back to
+    // conservative variables (column c of the result)
+    auto biway_row = [&](int q, const C* other) -> C {
+      C oin = C(0);
+      for (int t = 0; t < 5; t++) oin += (C)ms[lim_at(f, eMs + q * 5 + t)] * other[t];
+      const C tin = ri[q];
+      C co = C(0), ct = C(0);
+      for (int a = 0; a < 4; a++) {
+        co += Lrow[a] * __shfl_sync(0xffffffffu, oin, a, 4);
+        ct += Lrow[a] * __shfl_sync(0xffffffffu, tin, a, 4);
+      }
+      const C limc = wbap_biway(ct, co, V3 ? C(1) : nStd);
+      C sback = C(0);
+      for (int a = 0; a < 4; a++) sback += Rrow[a] * __shfl_sync(0xffffffffu, limc, a, 4);
+      return sback;
+    };
+    if (V3) {
+      // P2 rows 2..4 against the neighbour's secondary reconstruction; then P1 rows 0..1 against it
+      // with rows 2..4 from this face's P2 results (successive SR): the two orders' multiway sums are
+      // independent, so one pass over the faces does both
+      C uF[3];
+      for (int r = 0; r < 3; r++) {
+        uF[r] = biway_row(2 + r, uOO);
+        if (has) wbap_multi_term(ri[2 + r], uF[r], up[2 + r], down[2 + r]);
+      }
+      C uO1[5] = {uOO[0], uOO[1], C(0), C(0), C(0)};
+      for (int q = 2; q < 5; q++)
+        for (int t = 2; t < 5; t++) uO1[q] += (C)ms[lim_at(f, eMsO + q * 5 + t)] * uF[t - 2];
+      for (int r = 0; r < 2; r++) {
+        const C sb = biway_row(r, uO1);
+        if (has) wbap_multi_term(ri[r], sb, up[r], down[r]);
+      }
+    } else {
+      constexpr int ls = PASS == 0 ? 2 : 0, nr = PASS == 0 ? 3 : 2;
+      for (int r = 0; r < nr; r++) {
+        const C sb = biway_row(ls + r, uOO);
+        if (!has) continue;
+        if (nO == 0) first[ls + r] = sb;
+        else wbap_multi_term(first[ls + r], sb, up[ls + r], down[ls + r]);
+      }
+    }
+    if (has) nO++;
+  }
   C res[5];
   for (int q = 0; q < 5; q++) res[q] = ri[q];
-  C uFaces[NF][3];  // V3: this cell's P2 biway results per face slot (column c)
-  for (int k = 0; k < NF; k++) for (int r = 0; r < 3; r++) uFaces[k][r] = C(0);
-  constexpr int nPass = V3 ? 2 : 1;
-#pragma unroll
-  for (int pp = 0; pp < nPass; pp++) {
-    const int pass = V3 ? pp : PASS;
-    const int ls = pass == 0 ? 2 : 0, nr = pass == 0 ? 3 : 2;
-    C up[3] = {C(0), C(0), C(0)}, down[3] = {C(0), C(0), C(0)}, first[3] = {C(0), C(0), C(0)};
-    int nO = 0;
-#pragma unroll
-    for (int k = 0; k < NF; k++) {
-      int32_t sf = valid ? v.cellFace[aos(i, k, NF)] : kEmptySlot;
-      const int32_t f0 = sf >= 0 ? sf : ~sf;
-      const int side = sf >= 0 ? 0 : 1;
-      int32_t j = -1;
-      if (sf != kEmptySlot) j = side == 0 ? v.faceR[f0] : v.faceL[f0];
-      // every lane runs every slot (the shuffles below need all 32 lanes); a slot without an interior
-      // neighbour computes on this cell's own data and is not accumulated
-      const bool has = j >= 0;
-      const int64_t jj = has ? j : (valid ? i : 0);
-      const int64_t ff = has ? f0 : 0;
-      const int eMs = side == 0 ? kMsR2L : kMsL2R, eMsO = side == 0 ? kMsL2R : kMsR2L;
-      C uOO[5];
-      for (int q = 0; q < 5; q++) uOO[q] = urec[jj * 20 + q * 4 + c];
-      if (V3 && pass == 1) {  // successive SR: the neighbour's rows 2..4 from this cell's P2 results
-        for (int q = 2; q < 5; q++) {
-          C s = C(0);
-          for (int t = 2; t < 5; t++) s += (C)ms[aos(ff, eMsO + q * 5 + t, kLimE)] * uFaces[k][t - 2];
-          uOO[q] = s;
-        }
-      }
-      double uo[4];
-      for (int q = 0; q < 4; q++) uo[q] = has ? v.u[jj * 4 + q] : ui[q];
-      const int64_t f = ff;
-      C Lrow[4], Rrow[4];
-      char_rows<C>(c, gamma, side ? uo : ui, side ? ui : uo, (C)v.faceNormal[2 * f], (C)v.faceNormal[2 * f + 1],
-                   Lrow, Rrow);
-      for (int r = 0; r < nr; r++) {
-        C oin = C(0);
-        for (int q = 0; q < 5; q++) oin += (C)ms[aos(f, eMs + (ls + r) * 5 + q, kLimE)] * uOO[q];
-        const C tin = ri[ls + r];
-        // characteristic components co[c] = L[c] . oin, ct[c] = L[c] . tin over the group's lanes
-        C co = C(0), ct = C(0);
-        for (int q = 0; q < 4; q++) {
-          const C oq = __shfl_sync(0xffffffffu, oin, q, 4), tq = __shfl_sync(0xffffffffu, tin, q, 4);
-          co += Lrow[q] * oq;
-          ct += Lrow[q] * tq;
-        }
-        const C limc = wbap_biway(ct, co, V3 ? C(1) : nStd);
-        C sback = C(0);  // back to conservative variables: R[c] . lim
-        for (int q = 0; q < 4; q++) sback += Rrow[q] * __shfl_sync(0xffffffffu, limc, q, 4);
-        if (!has) continue;
-        if (V3) {
-          if (pass == 0) uFaces[k][r] = sback;
-          wbap_multi_term(ri[ls + r], sback, up[r], down[r]);
-        } else if (nO == 0) {
-          first[r] = sback;
-        } else {
-          wbap_multi_term(first[r], sback, up[r], down[r]);
-        }
-      }
-      if (has) nO++;
-    }
-    for (int r = 0; r < nr; r++) {
-      if (V3) res[ls + r] = ri[ls + r] * (up[r] + nStd) / (down[r] + nStd);
-      else if (nO > 0) res[ls + r] = first[r] * (up[r] + C(1)) / (down[r] + C(1));
-    }
+  if (V3) {
+    for (int q = 0; q < 5; q++) res[q] = ri[q] * (up[q] + nStd) / (down[q] + nStd);
+  } else if (nO > 0) {
+    constexpr int ls = PASS == 0 ? 2 : 0, nr = PASS == 0 ? 3 : 2;
+    for (int r = 0; r < nr; r++) res[ls + r] = first[ls + r] * (up[ls + r] + C(1)) / (down[ls + r] + C(1));
   }
   if (valid)
     for (int q = 0; q < 5; q++) o[q * 4 + c] = (T)res[q];

@@ -384,13 +384,11 @@ def line_scan_order(m: Mesh) -> np.ndarray:
     return np.concatenate([idx[0::2].ravel(), idx[1::2].ravel()]).astype(np.int64)
 
 
-def read_gmsh2(path: str) -> Mesh:
-    """Gmsh 2.2 ASCII reader for 2-D meshes (SerialGmshReader2d, DNDS_Mesh.hpp:87-236).
-
-    Cells are Tri3 (type 2) and Quad4 (type 3); boundary lines (type 1) carry
-    the physical-group names of ``GMSH_BC_NAMES``.  Faces are extracted from
-    the cell edges; cells are made counter-clockwise.
-    """
+def parse_gmsh2(path: str) -> dict:
+    """The raw content of a Gmsh 2.2 ASCII file (SerialGmshReader2d, DNDS_Mesh.hpp:87-236), for 2-D
+    meshes: nodes [n][2] indexed by Gmsh node id (row 0 unused), cells [n][4] Gmsh node ids (Tri3 with
+    slot 3 = -1, Quad4), boundary lines [n][3] (node, node, physical group) and the physical-group
+    names."""
     with open(path) as fh:
         lines = [ln.strip() for ln in fh]
     k = 0
@@ -426,16 +424,31 @@ def read_gmsh2(path: str) -> Mesh:
                     cells.append(conn[:3] + [-1])
                 elif et == 3:
                     cells.append(conn[:4])
+                else:
+                    raise ValueError(f"{path}: element type {et} is not a 2-D Line2 / Tri3 / Quad4 element")
             k += cnt + 3
         else:
             k += 1
-    assert nodes is not None
-    used = np.unique(np.array([c for cc in cells for c in cc if c >= 0] + [b[0] for b in bnd] + [b[1] for b in bnd]))
+    if nodes is None:
+        raise ValueError(f"{path}: no $Nodes section")
+    return {"nodes": nodes, "cells": np.array(cells, dtype=np.int64).reshape(-1, 4),
+            "bnd": np.array(bnd, dtype=np.int64).reshape(-1, 3),
+            "names": names}
+
+
+def gmsh_mesh(g: dict, name: str = "gmsh") -> Mesh:
+    """The mesh of parsed Gmsh content (parse_gmsh2): cells made counter-clockwise, faces extracted from
+    the cell edges in cell order and local edge order (the reference's vol2face construction,
+    DNDS_Mesh.hpp:260-320), boundary faces typed from their physical-group names as in
+    DNDS_Mesh.hpp:801-829 (bc-1 Wall, bc-2 Farfield, bc-3 Wall_Euler, bc-4 Wall_NoSlip, bc-DMRFar,
+    bc-RTFar, bc-IVFar, bc-2DRiemannFar).  A boundary face without a line element, or on a line of
+    another name, is an error (the reference asserts)."""
+    nodes, cells, bnd, names = g["nodes"], g["cells"], g["bnd"], g["names"]
+    used = np.unique(np.concatenate([cells[cells >= 0].ravel(), bnd[:, :2].ravel()]))
     remap = -np.ones(nodes.shape[0], dtype=np.int64)
     remap[used] = np.arange(used.size)
     node_xy = nodes[used]
-    cn = np.array(cells, dtype=np.int64)
-    cn = np.where(cn >= 0, remap[np.maximum(cn, 0)], -1)
+    cn = np.where(cells >= 0, remap[np.maximum(cells, 0)], -1)
     # orient counter-clockwise
     for i in range(cn.shape[0]):
         nn = 3 if cn[i, 3] < 0 else 4
@@ -446,8 +459,10 @@ def read_gmsh2(path: str) -> Mesh:
     bmap = {}
     for a, b, phys in bnd:
         key = (min(remap[a], remap[b]), max(remap[a], remap[b]))
-        nm = names.get(phys, "")
-        bmap[key] = GMSH_BC_NAMES.get(nm, BC_FARFIELD)
+        nm = names.get(int(phys), "")
+        if nm not in GMSH_BC_NAMES:
+            raise ValueError(f"boundary physical group {phys} named {nm!r} is not a DNDS boundary name")
+        bmap[key] = GMSH_BC_NAMES[nm]
     edges = {}
     fn, fc, fb = [], [], []
     for i in range(cn.shape[0]):
@@ -463,6 +478,17 @@ def read_gmsh2(path: str) -> Mesh:
                 fc.append([i, -1])
     for f, (a, b) in enumerate(fn):
         key = (min(a, b), max(a, b))
-        fb.append(BC_INNER if fc[f][1] >= 0 else bmap.get(key, BC_FARFIELD))
+        if fc[f][1] >= 0:
+            fb.append(BC_INNER)
+        elif key in bmap:
+            fb.append(bmap[key])
+        else:
+            raise ValueError(f"boundary face ({a}, {b}) has no boundary line element")
     nf = len(fn)
-    return _as_mesh(node_xy, cn, (np.array(fn), np.array(fc), np.array(fb), np.zeros((nf, 2))), path, {})
+    return _as_mesh(node_xy, cn, (np.array(fn), np.array(fc), np.array(fb), np.zeros((nf, 2))), name, {})
+
+
+def read_gmsh2(path: str) -> Mesh:
+    """Gmsh 2.2 ASCII reader for 2-D meshes (SerialGmshReader2d, DNDS_Mesh.hpp:87-236, and the face
+    and boundary set-up of DNDS_Mesh.hpp:260-320, 801-829): parse_gmsh2, then gmsh_mesh."""
+    return gmsh_mesh(parse_gmsh2(path), path)

@@ -23,7 +23,7 @@ from . import _lib
 from .mesh import Mesh
 from .settings import make_settings
 
-BUF_U, BUF_UREC, BUF_RHS, BUF_DT = 0, 1, 2, 3
+BUF_U, BUF_UREC, BUF_RHS, BUF_DT, BUF_SA_U, BUF_SA_UREC = 0, 1, 2, 3, 4, 5
 
 
 class DndsgError(RuntimeError):

@@ -99,10 +99,12 @@ typedef struct dndsg_ctx dndsg_ctx;
 
 /* device buffers reachable through dndsg_device_buffer */
 enum dndsg_buffer {
-  DNDSG_BUF_U = 0,    /* double [n_cells][nvars] cell means */
-  DNDSG_BUF_UREC = 1, /* double or float [n_cells][5][nvars] VR coefficients */
-  DNDSG_BUF_RHS = 2,  /* double [n_cells][nvars] */
-  DNDSG_BUF_DT = 3    /* double [n_cells] */
+  DNDSG_BUF_U = 0,    /* double [n_cells][4] cell means (the flow part in SA contexts) */
+  DNDSG_BUF_UREC = 1, /* double or float [n_cells][5][4] VR coefficients (flow part) */
+  DNDSG_BUF_RHS = 2,  /* double [n_cells][4] */
+  DNDSG_BUF_DT = 3,   /* double [n_cells] */
+  DNDSG_BUF_SA_U = 4,   /* SA contexts: double [n_cells], the fifth variable's means */
+  DNDSG_BUF_SA_UREC = 5 /* SA contexts: double or float [n_cells][5], its VR coefficients */
 };
 
 /* Build the context on CUDA device `device`: uploads the mesh and runs the
