@@ -220,13 +220,20 @@ def run_reference(args):
     print(json.dumps(out))
 
 
-def steady_leg(dev, iters=1000, log=None):
+STEADY_RAMP = dict(cfl=100.0, cfl_ramp_start=100, cfl_ramp_length=1000, cfl_ramp_end=1000.0)
+
+
+def steady_leg(dev, iters=10000, log=None):
     """The implicit steady RANS-SA path on the 512 x 128 NACA 0012 C-mesh (first spacing 1e-6 chord, far
     field 20 chords, no-slip wall), M 0.15, alpha 10 deg, Re 6e6, SA variable 3x the laminar viscosity in
-    the free stream, CFL 100, first-order BDF pseudo time, LU-SGS in the reference's natural scan order
-    (level-scheduled) and, for timing, in colour batches (which does not converge on these stretched
-    cells): ms per pseudo-time iteration (CUDA events), the density increment after `iters` iterations
-    relative to its largest value, and CL / CD from the wall force.  Timed outside the headline."""
+    the free stream: first-order BDF pseudo time, LU-SGS in the reference's natural scan order
+    (level-scheduled), CFL 100 ramped log-linearly to 1000 over iterations 100-1100 (the fstop ramp),
+    one C call per run (dndsg_steady_solve).  Reported: ms per pseudo-time iteration (CUDA events),
+    the density increment ratio of fstop after `iters` iterations and CL / CD from the wall force, in
+    FP64 and FP32 bulk; the colour-batched sweep's ms per iteration (it does not converge on these
+    stretched cells); the oracle's iteration time on the host cores.  The full convergence to the
+    1e-8 drop takes about 190,000 iterations (python bench.py --steady-full).  Timed outside the
+    headline."""
     import math
 
     import torch
@@ -240,40 +247,41 @@ def steady_leg(dev, iters=1000, log=None):
     u0 = np.tile(np.array(cfg["eulerSetting"]["farFieldStaticValue"]), (m.n_cells, 1))
     a = math.radians(10.0)
     out = {"workload": "RANS-SA NACA 0012, C-mesh 512x128 (65,536 quads), first spacing 1e-6 chord, M 0.15, "
-                       "alpha 10, Re 6e6, CFL 100, BDF1 pseudo time, 5 variables",
-           "cells": m.n_cells}
+                       "alpha 10, Re 6e6, BDF1 pseudo time, CFL 100 ramped to 1000, 5 variables",
+           "cells": m.n_cells, "iterations": iters}
     for prec, name in ((0, "fp64"), (1, "fp32")):
-        for mode, mname in ((1, "natural_order"), (0, "colour_batches")):
-            s = Solver(m, cfg, device=dev, precision=prec)
-            nb = s.lusgs_set_order(mode)
-            s.set_u(u0)
-            s.bdf_begin()
-            for _ in range(5):
-                s.implicit_iteration(100.0)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            k = 30
-            torch.cuda.synchronize()
-            e0.record()
-            for _ in range(k):
-                s._check(s.L.dndsg_implicit_iteration(s.h, 100.0, 1e100, 1.0, 1, 0, 0.0, None, None, s.stream))
-            e1.record()
-            torch.cuda.synchronize()
-            ms = e0.elapsed_time(e1) / k
-            r = {"batches_per_iteration": nb, "ms_per_iteration": ms, "cell_iterations_per_s": m.n_cells / (ms * 1e-3)}
-            if mode == 1:
-                s.set_u(u0)
-                t0 = time.perf_counter()
-                it, rel, wf = s.steady_solve(100.0, 1e-8, iters)
-                r["iterations"] = it
-                r["wall_s"] = time.perf_counter() - t0
-                r["rel_residual_rho"] = float(rel[0])
-                q = 0.5
-                r["CL"] = float((-wf[1] * math.sin(a) + wf[2] * math.cos(a)) / q)
-                r["CD"] = float((wf[1] * math.cos(a) + wf[2] * math.sin(a)) / q)
-            out[f"{name}_{mname}"] = r
-            s.close()
-            if log:
-                log(name, mname, r)
+        s = Solver(m, cfg, device=dev, precision=prec)
+        s.lusgs_set_order(1)
+        s.set_u(u0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        it, rel, wf, _ = s.steady_run(threshold=1e-8, max_iter=iters, **STEADY_RAMP)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        r = {"iterations": it, "seconds": ms * 1e-3, "ms_per_iteration": ms / it,
+             "cell_iterations_per_s": m.n_cells * it / (ms * 1e-3), "rel_residual_rho": float(rel[0]),
+             "CL": float((-wf[1] * math.sin(a) + wf[2] * math.cos(a)) / 0.5),
+             "CD": float((wf[1] * math.cos(a) + wf[2] * math.sin(a)) / 0.5)}
+        s.close()
+        # the colour-batched sweep, timed only
+        s = Solver(m, cfg, device=dev, precision=prec)
+        nb = s.lusgs_set_order(0)
+        s.set_u(u0)
+        s.steady_run(cfl=100.0, max_iter=5, threshold=0.0)
+        torch.cuda.synchronize()
+        e0.record()
+        s.steady_run(cfl=100.0, max_iter=30, threshold=0.0)
+        e1.record()
+        torch.cuda.synchronize()
+        r["colour_batches"] = {"batches_per_iteration": nb, "ms_per_iteration": e0.elapsed_time(e1) / 30}
+        s.close()
+        out[name] = r
+        if log:
+            log(name, r)
+    out["dCL_fp32_vs_fp64"] = abs(out["fp32"]["CL"] - out["fp64"]["CL"])
+    out["dCD_fp32_vs_fp64"] = abs(out["fp32"]["CD"] - out["fp64"]["CD"])
     # the oracle's sequential sweep on the host cores, a bounded sample of iterations
     try:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -292,6 +300,52 @@ def steady_leg(dev, iters=1000, log=None):
                              "sample": "5 pseudo-time iterations, natural order"}
     except Exception as e:  # the CPU figure is a side report
         out["cpu_oracle"] = {"error": str(e)[:200]}
+    return out
+
+
+def steady_full(dev, log=None):
+    """The steady RANS-SA run of steady_leg to the configured 1e-8 drop of the density increment ratio:
+    the 512 x 128 C-mesh in FP64 (about 190,000 iterations) and FP32 bulk (whose rounding floor is near
+    1e-7: it stops at 150,000 iterations), and the coarse 128 x 32 C-mesh in FP64.  Time to the
+    residual, iterations, CL and CD."""
+    import math
+
+    import torch
+
+    from dnds_b200 import mesh as M
+    from dnds_b200 import settings as S
+    from dnds_b200.solver import Solver
+
+    cfg = S.preset("naca0012_sa")
+    far = np.array(cfg["eulerSetting"]["farFieldStaticValue"])
+    a = math.radians(10.0)
+    out = {"workload": "RANS-SA NACA 0012 C-mesh, M 0.15, alpha 10, Re 6e6, BDF1 pseudo time, LU-SGS natural order, "
+                       "CFL 100 ramped to 1000, fstop: density increment ratio < 1e-8"}
+    for key, kw, prec, maxit in (("c512x128_fp64", {}, 0, 300000), ("c512x128_fp32", {}, 1, 150000),
+                                 ("c128x32_fp64", dict(n_airfoil=64, n_wake=32, nj=32), 0, 200000)):
+        m = M.naca0012_cmesh(**kw)
+        s = Solver(m, cfg, device=dev, precision=prec)
+        s.lusgs_set_order(1)
+        s.set_u(np.tile(far, (m.n_cells, 1)))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        it, rel, wf, hist = s.steady_run(threshold=1e-8, max_iter=maxit, history=True, **STEADY_RAMP)
+        e1.record()
+        torch.cuda.synchronize()
+        sec = e0.elapsed_time(e1) * 1e-3
+        marks = {}
+        for lvl in (1e-4, 1e-5, 1e-6, 1e-7, 1e-8):
+            hit = np.nonzero(hist <= lvl)[0]
+            marks[f"{lvl:.0e}"] = int(hit[0] + 1) if len(hit) else None
+        out[key] = {"cells": m.n_cells, "iterations": it, "seconds": sec, "ms_per_iteration": sec * 1e3 / it,
+                    "rel_residual_rho": float(rel[0]), "reached_1e-8": bool(rel[0] < 1e-8),
+                    "iterations_to": marks,
+                    "CL": float((-wf[1] * math.sin(a) + wf[2] * math.cos(a)) / 0.5),
+                    "CD": float((wf[1] * math.cos(a) + wf[2] * math.sin(a)) / 0.5)}
+        s.close()
+        if log:
+            log(key, out[key])
     return out
 
 
@@ -448,74 +502,56 @@ def small_mesh_leg(dev, steps=2000):
 
 
 def learned_leg(dev, grid, tol=1e-7, log=None):
-    """The learned VR warm start: harvest on two 256 x 256 x 2 vortex meshes, train on the GPU,
-    then Jacobi sweeps per SSP-RK3 step to the same rms-increment tolerance, with and without the
-    network, on a fresh seed of the headline mesh.  Timed outside the headline."""
+    """The learned VR warm start (BF16 MLP on tcgen05), both input designs: each is harvested from
+    tolerance-mode runs of the three explicit workloads (the vortex on 40 x 40 quads and on two
+    256 x 256 x 2 jittered triangle meshes, the Riemann problem with the limiter on 256 x 256 x 2), trained
+    on the GPU, and evaluated as Jacobi sweeps per SSP-RK3 step to the same rms-increment tolerance,
+    with and without the network, on fresh-seed (9999) 1448 x 1448 x 2 = 4,193,408-triangle vortex and
+    Riemann meshes.  Design 0 extrapolates two plain sweeps; design 1 is the configured input (neighbour
+    mean differences and the previous-step coefficients).  Plus the tensor-core forward's throughput.
+    Timed outside the headline."""
     import torch
 
-    from dnds_b200 import geometry as G
-    from dnds_b200 import mesh as M
-    from dnds_b200 import settings as S
-    from dnds_b200.learned import WarmStartNet, harvest, train
-    from dnds_b200.solver import Solver
+    from dnds_b200.learned import WarmStartNet, evaluate, train, training_set
 
-    cfg = S.preset("vortex")
-    Xs, Ts = [], []
-    t0 = time.perf_counter()
-    for seed in (11, 12):
-        m = M.vortex_mesh(256, True, jitter=0.2, seed=seed)
-        s = Solver(m, cfg, device=dev, precision=1)
-        s.set_u(G.isentropic_vortex(m))
-        s.vr_to_tolerance(tol, 2000)
-        X, T, _ = harvest(s, 8, 0.5, tol, 2000)
-        Xs.append(X)
-        Ts.append(T)
-        s.close()
-    X, T = torch.cat(Xs), torch.cat(Ts)
-    torch.cuda.synchronize()
-    t_harvest = time.perf_counter() - t0
-    net = WarmStartNet(dev, seed=7)
-    t0 = time.perf_counter()
-    _, val = train(net, X, T, epochs=20)
-    torch.cuda.synchronize()
-    t_train = time.perf_counter() - t0
-    out = {"pairs": int(X.shape[0]), "harvest_s": t_harvest, "train_s": t_train,
-           "train_samples_per_s": 20 * X.shape[0] / t_train, "val_loss": val,
-           "target_mean_square": float((T ** 2).mean()), "tolerance_rms_increment": tol}
-    del X, T, Xs, Ts
-    # inference throughput of the tensor-core forward (tcgen05): 4,194,304 rows of 64 features
-    rows = 4_194_304
-    Xf = torch.randn((rows, 64), device=dev, dtype=torch.float32)
-    Yf = net.forward(Xf)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(5):
-        Yf = net.forward(Xf)
-    e1.record()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / 5
-    flop = 2 * (64 * 64 * 3 + 64 * 20) * rows
-    out["forward_tc"] = {"rows": rows, "ms": ms, "rows_per_s": rows / (ms * 1e-3), "tflops": flop / (ms * 1e-3) / 1e12,
-                         "gbs": rows * (64 * 4 + 20 * 4) / (ms * 1e-3) / 1e9,
-                         "note": "tcgen05.mma kind::f16, BF16 operands, FP32 accumulator in tensor memory; "
-                                 "bytes are the FP32 features read and outputs written"}
-    del Xf, Yf
-    m = M.vortex_mesh(grid, True, jitter=0.2, seed=9999)
-    for name, use in (("plain", None), ("learned", net)):
-        s = Solver(m, cfg, device=dev, precision=1)
-        s.set_u(G.isentropic_vortex(m))
-        s.vr_to_tolerance(tol, 2000)
-        s.ssprk3_step_tol(0.5, tol, 2000, use)
-        torch.cuda.synchronize()
+    out = {"tolerance_rms_increment": tol, "evaluation_grid": 1448}
+    for design in (0, 1):
         t0 = time.perf_counter()
-        sw = [s.ssprk3_step_tol(0.5, tol, 2000, use) for _ in range(3)]
+        X, T = training_set(tol, steps=8, n=256, features=design)
         torch.cuda.synchronize()
-        out[name] = {"sweeps_per_step": sw, "ms_per_step": (time.perf_counter() - t0) / 3 * 1e3}
-        s.close()
-    out["sweeps_saved_per_step"] = float(np.mean(out["plain"]["sweeps_per_step"]) -
-                                         np.mean(out["learned"]["sweeps_per_step"]))
-    if log:
-        log(out)
+        t_harvest = time.perf_counter() - t0
+        net = WarmStartNet(dev, seed=7, features=design)
+        t0 = time.perf_counter()
+        _, val = train(net, X, T, epochs=20)
+        torch.cuda.synchronize()
+        t_train = time.perf_counter() - t0
+        r = {"pairs": int(X.shape[0]), "harvest_s": t_harvest, "train_s": t_train,
+             "train_samples_per_s": 20 * X.shape[0] / t_train, "val_loss": val,
+             "target_mean_square": float((T ** 2).mean())}
+        del X, T
+        r.update(evaluate(net, tol, grid=1448, steps=3, seed=9999))
+        out[f"design{design}"] = r
+        if log:
+            log(design, r)
+        if design == 0:
+            # inference throughput of the tensor-core forward: 4,194,304 rows of 64 features
+            rows = 4_194_304
+            Xf = torch.randn((rows, 64), device=dev, dtype=torch.float32)
+            Yf = net.forward(Xf)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(5):
+                Yf = net.forward(Xf)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / 5
+            flop = 2 * (64 * 64 * 3 + 64 * 20) * rows
+            out["forward_tc"] = {"rows": rows, "ms": ms, "rows_per_s": rows / (ms * 1e-3),
+                                 "tflops": flop / (ms * 1e-3) / 1e12, "gbs": rows * (64 * 4 + 20 * 4) / (ms * 1e-3) / 1e9,
+                                 "note": "tcgen05.mma kind::f16, BF16 operands, FP32 accumulator in tensor memory; "
+                                         "bytes are the FP32 features read and outputs written"}
+            del Xf, Yf
+        net.close()
     return out
 
 
@@ -537,6 +573,8 @@ def main():
     ap.add_argument("--riemann-grid", type=int, default=2048, help="grid size of the Riemann / CWBAP report")
     ap.add_argument("--riemann-end-grid", type=int, default=512,
                     help="grid size of the Riemann run to t = 0.3 in the default bench")
+    ap.add_argument("--steady-full", action="store_true",
+                    help="only the steady RANS-SA NACA 0012 runs to the 1e-8 drop (about 10 minutes); one JSON line")
     ap.add_argument("--riemann-full", action="store_true",
                     help="only the Riemann problem to t = 0.3 on the configured 2048 x 2048 mesh (both precisions, "
                          "about 17 minutes); prints one JSON line")
@@ -547,6 +585,14 @@ def main():
 
     import torch
 
+    if args.steady_full:
+        torch.cuda.set_device(0)
+        clk = ClockSampler(0)
+        r = steady_full(0, log=lambda *a: print(*a, file=sys.stderr, flush=True))
+        r["clocks"] = clk.stop()
+        r["command"] = "python bench.py --steady-full"
+        print(json.dumps(r))
+        return
     if args.riemann_full:
         torch.cuda.set_device(0)
         clk = ClockSampler(0)
@@ -714,6 +760,10 @@ def main():
         out["cpu_baseline"] = cpu_baseline()
     if rank == 0 and ws == 1 and not args.no_steady:
         out["steady_naca0012_sa"] = steady_leg(dev)
+        rec = os.path.join(ROOT, "profiles", "steady_naca0012_sa_full.json")
+        if os.path.exists(rec):  # the runs to the 1e-8 drop, recorded by --steady-full (too long for here)
+            with open(rec) as fh:
+                out["steady_naca0012_sa_full_recorded"] = json.load(fh)
     if rank == 0 and ws == 1 and not args.no_riemann:
         out["small_mesh_c1"] = small_mesh_leg(dev)
     if rank == 0 and ws == 1 and not args.no_riemann:

@@ -18,7 +18,8 @@ EXPORTS = [
     "dndsg_residual", "dndsg_face_values", "dndsg_get_status", "dndsg_eval_rhs_noalloc",
     "dndsg_mlp_create", "dndsg_mlp_destroy", "dndsg_mlp_last_error", "dndsg_mlp_set_params",
     "dndsg_mlp_get_params", "dndsg_mlp_forward", "dndsg_mlp_gradient", "dndsg_mlp_train_step",
-    "dndsg_mlp_features", "dndsg_vr_to_tolerance", "dndsg_ssprk3_step_tol",
+    "dndsg_mlp_features", "dndsg_vr_to_tolerance", "dndsg_ssprk3_step_tol", "dndsg_mlp_set_features",
+    "dndsg_set_warm_start_features",
     "dndsg_lusgs_colours", "dndsg_lusgs_set_order", "dndsg_lusgs_matrix_init", "dndsg_lusgs_forward", "dndsg_lusgs_backward",
     "dndsg_bdf_begin", "dndsg_implicit_iteration", "dndsg_dual_reset", "dndsg_dual_step", "dndsg_lusgs_matvec", "dndsg_gmres_lusgs",
     "dndsg_set_owned", "dndsg_rk_dt", "dndsg_rk_set_dt", "dndsg_rk_vr", "dndsg_rk_limit", "dndsg_rk_stage",
@@ -105,6 +106,8 @@ def lib():
     L.dndsg_mlp_gradient.argtypes = [vp, vp, vp, i64, C.POINTER(dbl), vp, vp]
     L.dndsg_mlp_train_step.argtypes = [vp, vp, vp, i64, C.c_float, C.POINTER(dbl), vp]
     L.dndsg_mlp_features.argtypes = [vp, vp, vp, vp]
+    L.dndsg_mlp_set_features.argtypes = [vp, i32]
+    L.dndsg_set_warm_start_features.argtypes = [vp, i32]
     L.dndsg_vr_to_tolerance.argtypes = [vp, vp, dbl, i32, C.POINTER(i32), C.POINTER(i64), vp, vp, vp]
     L.dndsg_ssprk3_step_tol.argtypes = [vp, vp, dbl, dbl, dbl, i32, C.POINTER(i32), vp, vp, vp]
     L.dndsg_lusgs_colours.argtypes = [vp, vp, C.POINTER(i32)]

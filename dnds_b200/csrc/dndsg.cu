@@ -73,6 +73,7 @@ struct dndsg_ctx {
   float* mlpGeom = nullptr;  // [N][8] slot face centres in each cell's polynomial frame
   void *mlpM = nullptr, *mlpA = nullptr, *mlpB = nullptr, *mlpH = nullptr;  // learned warm start work (T)
   float* mlpSc = nullptr;                                                     // [N][4] output scales
+  int mlpFeatureMode = 0;  // warm-start features: 0 Jacobi extrapolation, 1 previous coefficients
   unsigned long long* accCount = nullptr;
   int64_t nWallCells = 0;
   // implicit path: the sweep order as a rank per cell (a neighbour of lower rank is "before"),
@@ -1698,6 +1699,7 @@ struct dndsg_mlp {
   unsigned* flags = nullptr;  // kFlagTimeout from the tensor-core forward
   int64_t step = 0;
   bool attrFwd = false, attrTrain = false;
+  int featureMode = 0;  // the feature design the network is trained for (dndsg_mlp_set_features)
   std::string err;
 };
 
@@ -1716,11 +1718,12 @@ static_assert(kIn == DNDSG_MLP_IN && kOut == DNDSG_MLP_OUT && kNParam == DNDSG_M
 MlpDev mlp_dev(const dndsg_mlp* m) { return MlpDev{m->P, m->W}; }
 
 template <class T>
-__global__ void k_mlp_features(HotView<T> h, MlpIters<T> it, float* X, float* Sc) {
+__global__ void k_mlp_features(HotView<T> h, MlpIters<T> it, int mode, float* X, float* Sc) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= h.N) return;
   float x[kInP], sc[4];
-  mlp_cell_features<T>(i, h, it, x, sc);
+  if (mode == 0) mlp_cell_features<T>(i, h, it, x, sc);
+  else mlp_cell_features_prev<T>(i, h, it.x0, it.geom, x, sc);
   if (X)
     for (int k = 0; k < kIn; k++) X[i * kIn + k] = x[k];
   for (int v = 0; v < 4; v++) Sc[i * 4 + v] = sc[v];
@@ -1802,7 +1805,9 @@ int ensure_mlp_buffers(dndsg_ctx* c) {
       (rc = dalloc(c, c->mlpH, bytes)) || (rc = dalloc(c, c->mlpSc, sizeof(float) * 4 * c->N)) ||
       (rc = dalloc(c, c->accCount, sizeof(unsigned long long))))
     return rc;
-  DG_CUDA(c, cudaFuncSetAttribute(k_mlp_tc<TcCellFeatures<T>, TcWarmStart<T>>,
+  DG_CUDA(c, cudaFuncSetAttribute(k_mlp_tc<TcCellFeatures<T, 0>, TcWarmStart<T>>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TcSmem)));
+  DG_CUDA(c, cudaFuncSetAttribute(k_mlp_tc<TcCellFeatures<T, 1>, TcWarmStart<T>>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TcSmem)));
   return 0;
 }
@@ -1826,14 +1831,13 @@ int vr_to_tol(dndsg_ctx* c, const dndsg_mlp* m, double tol, int maxSweeps, int* 
   if (m && harvest) return fail(c, DNDSG_BAD_ARGUMENT, "harvesting runs without a network");
   if (accOut) *accOut = 0;
   auto converged = [&]() { return sweeps > 0 && std::sqrt(inc / double(c->N)) <= tol; };
-  if ((m || harvest) && maxSweeps >= (m ? 4 : 2)) {
+  const int mode = c->mlpFeatureMode;
+  if (m && m->featureMode != mode)
+    return fail(c, DNDSG_BAD_ARGUMENT, "the network's feature design differs from the context's");
+  if (mode == 1 && (m || harvest) && maxSweeps >= (m ? 2 : 1)) {
+    // the configured input: features of the start x0 itself (neighbour mean differences, x0)
     if ((rc = ensure_mlp_buffers<T>(c))) return rc;
-    // x1 = J(x0) into A, x2 = J(x1) into B (with its increment)
-    launch_vr_from<T>(c, c->urec, c->mlpA, false, s);
-    k_zero_scalar<<<1, 1, 0, s>>>(c->scal + S_INC);
-    launch_vr_from<T>(c, c->mlpA, c->mlpB, true, s);
-    sweeps = 2;
-    k_mlp_features<T><<<grid_for(c->N), kBlock, 0, s>>>(view<T>(c), iters<T>(c, c->urec, c->mlpA, c->mlpB), hX,
+    k_mlp_features<T><<<grid_for(c->N), kBlock, 0, s>>>(view<T>(c), iters<T>(c, c->urec, nullptr, nullptr), 1, hX,
                                                          c->mlpSc);
     if ((rc = check_launch(c))) return rc;
     if (m) {
@@ -1842,7 +1846,44 @@ int vr_to_tol(dndsg_ctx* c, const dndsg_mlp* m, double tol, int maxSweeps, int* 
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
       const int64_t tiles = (c->N + kTcRows - 1) / kTcRows;
       k_mlp_tc<<<(unsigned)std::min<int64_t>(tiles, 4 * sms), kTcRows, sizeof(TcSmem), s>>>(
-          mlp_dev(m), TcCellFeatures<T>{view<T>(c), iters<T>(c, c->urec, c->mlpA, c->mlpB)},
+          mlp_dev(m), TcCellFeatures<T, 1>{view<T>(c), iters<T>(c, c->urec, nullptr, nullptr)},
+          TcWarmStart<T>{(const T*)c->urec, (T*)c->mlpM}, c->N, c->flags);
+      launch_vr_from<T>(c, c->urec, c->mlpA, false, s);  // J(x0)
+      launch_vr_from<T>(c, c->mlpM, c->mlpH, false, s);  // J(xm)
+      k_zero_scalar<<<1, 1, 0, s>>>(c->scal + S_INC);
+      k_vr_gate<T><<<grid_for(c->N), kBlock, 0, s>>>(c->N, (const T*)c->urec, (const T*)c->mlpA,
+                                                     (const T*)c->mlpM, (const T*)c->mlpH, (T*)c->mlpB,
+                                                     c->scal + S_INC, c->accCount);
+      std::swap(c->urec, c->mlpB);
+      sweeps = 2;
+      if ((rc = check_launch(c))) return rc;
+      if (accOut) {
+        unsigned long long a = 0;
+        DG_CUDA(c, cudaMemcpyAsync(&a, c->accCount, sizeof(a), cudaMemcpyDeviceToHost, s));
+        DG_CUDA(c, cudaStreamSynchronize(s));
+        *accOut = (int64_t)a;
+      }
+      if ((rc = read_scalar(c, c->scal + S_INC, &inc, s))) return rc;
+    } else if (hT) {
+      DG_CUDA(c, cudaMemcpyAsync(c->mlpH, c->urec, sizeof(T) * 20 * c->N, cudaMemcpyDeviceToDevice, s));
+    }
+  } else if (mode == 0 && (m || harvest) && maxSweeps >= (m ? 4 : 2)) {
+    if ((rc = ensure_mlp_buffers<T>(c))) return rc;
+    // x1 = J(x0) into A, x2 = J(x1) into B (with its increment)
+    launch_vr_from<T>(c, c->urec, c->mlpA, false, s);
+    k_zero_scalar<<<1, 1, 0, s>>>(c->scal + S_INC);
+    launch_vr_from<T>(c, c->mlpA, c->mlpB, true, s);
+    sweeps = 2;
+    k_mlp_features<T><<<grid_for(c->N), kBlock, 0, s>>>(view<T>(c), iters<T>(c, c->urec, c->mlpA, c->mlpB), 0, hX,
+                                                         c->mlpSc);
+    if ((rc = check_launch(c))) return rc;
+    if (m) {
+      DG_CUDA(c, cudaMemsetAsync(c->accCount, 0, sizeof(unsigned long long), s));
+      int sms = 148;
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+      const int64_t tiles = (c->N + kTcRows - 1) / kTcRows;
+      k_mlp_tc<<<(unsigned)std::min<int64_t>(tiles, 4 * sms), kTcRows, sizeof(TcSmem), s>>>(
+          mlp_dev(m), TcCellFeatures<T, 0>{view<T>(c), iters<T>(c, c->urec, c->mlpA, c->mlpB)},
           TcWarmStart<T>{(const T*)c->mlpB, (T*)c->mlpM}, c->N, c->flags);
       launch_vr_from<T>(c, c->mlpB, c->urecNew, false, s);  // J(x2)
       launch_vr_from<T>(c, c->mlpM, c->mlpH, false, s);     // J(xm)
@@ -2062,23 +2103,46 @@ int dndsg_mlp_train_step(dndsg_mlp* m, const float* X, const float* Tg, int64_t 
   return 0;
 }
 
+int dndsg_mlp_set_features(dndsg_mlp* m, int mode) {
+  if (!m || (mode != 0 && mode != 1)) return DNDSG_BAD_ARGUMENT;
+  m->featureMode = mode;
+  return 0;
+}
+
+int dndsg_set_warm_start_features(dndsg_ctx* c, int mode) {
+  if (!c || (mode != 0 && mode != 1)) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
+  c->mlpFeatureMode = mode;
+  return 0;
+}
+
 int dndsg_mlp_features(dndsg_ctx* c, float* X, float* scales, void* s) {
   if (!c || !X || !scales) return DNDSG_BAD_ARGUMENT;
   if (c->dead) return refuse_dead(c);
   if (c->sa) return fail(c, DNDSG_UNSUPPORTED, "the learned warm start is for 4-variable contexts");
   int rc = c->fp32 ? ensure_mlp_buffers<float>(c) : ensure_mlp_buffers<double>(c);
   if (rc) return rc;
+  // design 1: the features of the current coefficients themselves
+  if (c->mlpFeatureMode == 1) {
+    if (c->fp32)
+      k_mlp_features<float><<<grid_for(c->N), kBlock, 0, st(s)>>>(
+          view<float>(c), iters<float>(c, c->urec, nullptr, nullptr), 1, X, scales);
+    else
+      k_mlp_features<double><<<grid_for(c->N), kBlock, 0, st(s)>>>(
+          view<double>(c), iters<double>(c, c->urec, nullptr, nullptr), 1, X, scales);
+    return check_launch(c);
+  }
   // x1 = J(x0), x2 = J(x1) into work buffers; the context's coefficients are left as they are
   if (c->fp32) {
     launch_vr_from<float>(c, c->urec, c->mlpA, false, st(s));
     launch_vr_from<float>(c, c->mlpA, c->mlpB, false, st(s));
     k_mlp_features<float><<<grid_for(c->N), kBlock, 0, st(s)>>>(view<float>(c), iters<float>(c, c->urec, c->mlpA, c->mlpB),
-                                                                 X, scales);
+                                                                 0, X, scales);
   } else {
     launch_vr_from<double>(c, c->urec, c->mlpA, false, st(s));
     launch_vr_from<double>(c, c->mlpA, c->mlpB, false, st(s));
     k_mlp_features<double><<<grid_for(c->N), kBlock, 0, st(s)>>>(view<double>(c),
-                                                                  iters<double>(c, c->urec, c->mlpA, c->mlpB), X, scales);
+                                                                  iters<double>(c, c->urec, c->mlpA, c->mlpB), 0, X, scales);
   }
   return check_launch(c);
 }

@@ -95,6 +95,39 @@ DG_HD void mlp_cell_features(int64_t i, const HotView<T>& h, const MlpIters<T>& 
   for (int k = 0; k < 8; k++) x[56 + k] = it.geom[i * 8 + k];
 }
 
+// The second input design, the one the configuration names: the neighbour mean differences to up to 4
+// neighbours and the previous-step coefficients x0 (the coefficients the reconstruction starts from:
+// those the previous stage or step left), before any sweep:
+//   x[4k + v]      = du_k[v] / s_v   as above
+//   x[16 + 4q + v] = x0[q][v] / s_v  (coefficients are mean differences over lengths: the same scale)
+//   x[36 .. 55]    = 0
+//   x[56 + 2k + d] = slot k's face centre in the cell's own polynomial frame
+// Output y[4q + v] = (x* - x0)[q][v] / s_v, returned scales r = s.
+template <class T>
+DG_HD void mlp_cell_features_prev(int64_t i, const HotView<T>& h, const T* x0, const float* geom, float x[kInP],
+                                  float r[4]) {
+  double du[4][4], ui[4];
+  for (int v = 0; v < 4; v++) ui[v] = h.u[i * 4 + v];
+  for (int k = 0; k < 4; k++)
+    for (int v = 0; v < 4; v++) du[k][v] = 0.0;
+  for (int k = 0; k < h.nfmax && k < 4; k++) {
+    if (h.vrMode[aos(i, k, h.nfmax)] != VR_INNER) continue;
+    const int64_t j = h.vrNbr[aos(i, k, h.nfmax)];
+    for (int v = 0; v < 4; v++) du[k][v] = h.u[j * 4 + v] - ui[v];
+  }
+  auto clampf = [](double a) { return (float)(a > 1e3 ? 1e3 : (a < -1e3 ? -1e3 : a)); };
+  for (int v = 0; v < 4; v++) {
+    double m = 0;
+    for (int k = 0; k < 4; k++) m = dmax(m, fabs(du[k][v]));
+    const double sv = dmax(m, dmax(1e-12 * fabs(ui[v]), 1e-30));
+    r[v] = (float)sv;
+    for (int k = 0; k < 4; k++) x[4 * k + v] = clampf(du[k][v] / sv);
+    for (int q = 0; q < 5; q++) x[16 + 4 * q + v] = clampf((double)x0[i * 20 + 4 * q + v] / sv);
+  }
+  for (int k = 36; k < 56; k++) x[k] = 0.f;
+  for (int k = 0; k < 8; k++) x[56 + k] = geom[i * 8 + k];
+}
+
 }  // namespace dg
 
 #if defined(__CUDACC__)
@@ -234,14 +267,16 @@ struct TcOutY {  // Y [n][20] = the network output
   }
   __device__ void store(int64_t, int64_t, const float*, const float*) const {}
 };
-template <class T>
-struct TcCellFeatures {  // the warm-start features of cell r
+template <class T, int MODE>
+struct TcCellFeatures {  // the warm-start features of cell r (MODE 0: Jacobi extrapolation, 1: previous coefficients)
   static constexpr bool kTile = false;
   HotView<T> h;
   MlpIters<T> it;
   __device__ void load(int64_t r, int64_t n, float x[kInP], float sc[4]) const {
-    if (r < n) mlp_cell_features<T>(r, h, it, x, sc);
-    else {
+    if (r < n) {
+      if (MODE == 0) mlp_cell_features<T>(r, h, it, x, sc);
+      else mlp_cell_features_prev<T>(r, h, it.x0, it.geom, x, sc);
+    } else {
       for (int k = 0; k < kInP; k++) x[k] = 0.f;
       for (int v = 0; v < 4; v++) sc[v] = 0.f;
     }
@@ -249,7 +284,7 @@ struct TcCellFeatures {  // the warm-start features of cell r
   __device__ void load_tile(int64_t, int64_t, unsigned char*) const {}
 };
 template <class T>
-struct TcWarmStart {  // dst = x2 + y r
+struct TcWarmStart {  // dst = base + y r (base: x2 for MODE 0, x0 for MODE 1)
   static constexpr bool kTile = false;
   const T* x2;
   T* dst;

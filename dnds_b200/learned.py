@@ -51,7 +51,7 @@ def _stream_ptr():
 class WarmStartNet:
     """One network on one GPU; parameters are FP32 masters with a BF16 copy for the MMAs."""
 
-    def __init__(self, device: int = 0, seed: int = 0, params: np.ndarray | None = None):
+    def __init__(self, device: int = 0, seed: int = 0, params: np.ndarray | None = None, features: int = 0):
         self.L = _lib.lib()
         self.device = device
         h = C.c_void_p()
@@ -59,6 +59,8 @@ class WarmStartNet:
         if rc != 0:
             raise DndsgError(rc, "dndsg_mlp_create failed")
         self.h = h
+        self.features = int(features)
+        self._check(self.L.dndsg_mlp_set_features(self.h, self.features))
         if params is not None:
             self.params = params
 
@@ -175,10 +177,11 @@ def sweep_counts(solver: Solver, steps: int, cfl: float, tol: float, net=None, m
     return [solver.ssprk3_step_tol(cfl, tol, max_sweeps, net, t_end) for _ in range(steps)]
 
 
-def training_set(tol: float = 1e-7, steps: int = 8, n: int = 256, seeds=(11, 12), log=None):
+def training_set(tol: float = 1e-7, steps: int = 8, n: int = 256, seeds=(11, 12), log=None, features: int = 0):
     """(X, T) harvested from tolerance-mode runs of the three explicit workloads on small meshes:
     the isentropic vortex on 40x40 quads, on jittered n x n x 2 triangles (one run per seed), and
-    the four-quadrant Riemann problem with the limiter on jittered n x n x 2 triangles."""
+    the four-quadrant Riemann problem with the limiter on jittered n x n x 2 triangles; features of
+    the given design (0 Jacobi extrapolation, 1 previous-step coefficients)."""
     import torch
 
     from .geometry import isentropic_vortex, quadrant_states
@@ -194,6 +197,7 @@ def training_set(tol: float = 1e-7, steps: int = 8, n: int = 256, seeds=(11, 12)
     Xs, Ts = [], []
     for name, m, pre, cfl, init in runs:
         s = Solver(m, preset(pre), precision=1)
+        s.set_warm_start_features(features)
         s.set_u(init(m, 0.0))
         s.vr_to_tolerance(tol, 2000)
         X, T, sw = harvest(s, steps, cfl, tol, 2000)
@@ -203,6 +207,51 @@ def training_set(tol: float = 1e-7, steps: int = 8, n: int = 256, seeds=(11, 12)
             log(f"{name}: {X.shape[0]} pairs, sweeps per step {sw}")
         s.close()
     return torch.cat(Xs), torch.cat(Ts)
+
+
+def evaluate(net, tol: float = 1e-7, grid: int = 1448, steps: int = 3, seed: int = 9999, log=None):
+    """Jacobi sweeps per SSP-RK3 step to the same rms-increment tolerance, without and with the
+    network, on fresh-seed jittered grid x grid x 2 meshes of the vortex and of the Riemann problem
+    (with the CWBAP limiter), FP32 bulk: sweeps per step, ms per step (wall time of the steps), and the
+    density difference of the two runs after the steps (L2 relative to the density's L2)."""
+    import time
+
+    import torch
+
+    from .geometry import cell_quadrature, isentropic_vortex, quadrant_states
+    from .mesh import riemann_mesh, vortex_mesh
+    from .settings import RIEMANN_2D_STATES, preset
+
+    out = {}
+    cases = (("vortex", lambda: vortex_mesh(grid, True, jitter=0.2, seed=seed), "vortex", 0.5,
+              lambda m: isentropic_vortex(m)),
+             ("riemann", lambda: riemann_mesh(grid, seed=seed), "riemann", 0.4,
+              lambda m: quadrant_states(m, RIEMANN_2D_STATES)))
+    for name, mk, pre, cfl, init in cases:
+        m = mk()
+        vol = cell_quadrature(m)[1].sum(1)
+        r, us = {"cells": m.n_cells}, {}
+        for label, use in (("plain", None), ("learned", net)):
+            s = Solver(m, preset(pre), precision=1)
+            s.set_warm_start_features(net.features)
+            s.set_u(init(m))
+            s.vr_to_tolerance(tol, 2000)
+            s.ssprk3_step_tol(cfl, tol, 2000, use)  # warm-up step
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            sw = [s.ssprk3_step_tol(cfl, tol, 2000, use) for _ in range(steps)]
+            torch.cuda.synchronize()
+            r[label] = {"sweeps_per_step": sw, "ms_per_step": (time.perf_counter() - t0) / steps * 1e3}
+            us[label] = s.get_u()
+            s.close()
+        d = us["learned"][:, 0] - us["plain"][:, 0]
+        r["rho_l2_learned_vs_plain"] = float(np.sqrt((d * d * vol).sum() / (us["plain"][:, 0] ** 2 * vol).sum()))
+        r["sweeps_saved_per_step"] = float(np.mean(r["plain"]["sweeps_per_step"]) -
+                                           np.mean(r["learned"]["sweeps_per_step"]))
+        out[name] = r
+        if log:
+            log(name, r)
+    return out
 
 
 def time_forward(rows_list=(1 << 20, 1 << 22), reps: int = 5, seed: int = 7):

@@ -283,6 +283,11 @@ class Solver:
         return it, rel, wf
 
     # ------------------------------------------------------------------ learned warm start
+    def set_warm_start_features(self, mode: int):
+        """The warm start's input design: 0 Jacobi extrapolation, 1 the previous-step coefficients and
+        the neighbour mean differences (dndsg_set_warm_start_features)."""
+        self._check(self.L.dndsg_set_warm_start_features(self.h, int(mode)))
+
     def mlp_features(self, X_ptr: int, scales_ptr: int):
         """Features [N][64] and scales [N][4] of the current state into device arrays."""
         self._check(self.L.dndsg_mlp_features(self.h, C.c_void_p(X_ptr), C.c_void_p(scales_ptr), self.stream))

@@ -417,17 +417,30 @@ int dndsg_mlp_gradient(dndsg_mlp* mlp, const float* X, const float* T, int64_t n
  * loss (host, may be NULL) is the batch loss before the step */
 int dndsg_mlp_train_step(dndsg_mlp* mlp, const float* X, const float* T, int64_t n, float lr, double* loss,
                          void* stream);
+/* The warm start's input design, per context (for harvesting and use) and per
+ * network (the design it is trained for; a mismatch is an error):
+ *   0  Jacobi extrapolation (default): the neighbour mean differences, the
+ *      increments of two plain sweeps from the start x0 and the slot geometry;
+ *      output (x* - x2) / r, the learned start x2 + y r, gated against J(x2)
+ *   1  the previous-step coefficients: the neighbour mean differences to up to
+ *      4 neighbours and x0 itself (the coefficients the previous stage or step
+ *      left), before any sweep; output (x* - x0) / s with s the per-variable
+ *      mean-difference scale, the learned start x0 + y s gated against J(x0)
+ *      (the two gate sweeps count), needs max_sweeps >= 2 */
+int dndsg_mlp_set_features(dndsg_mlp* mlp, int mode);
+int dndsg_set_warm_start_features(dndsg_ctx* ctx, int mode);
 /* features of the context's current coefficients, X [n_cells][64], and the
- * output scales r [n_cells][4] (device); runs two sweeps into work buffers
- * and leaves the context's coefficients unchanged */
+ * output scales r [n_cells][4] (device); design 0 runs two sweeps into work
+ * buffers; the context's coefficients are left unchanged */
 int dndsg_mlp_features(dndsg_ctx* ctx, float* X, float* scales, void* stream);
 /* Jacobi sweeps on the context's coefficients until the rms increment
- * sqrt(sum |dx|^2 / n_cells) <= tol or max_sweeps.  With mlp (may be NULL,
- * needs max_sweeps >= 4): sweeps x0 -> x1 -> x2, the learned start xm, then
- * J(x2) and J(xm) gated per cell (accepted_out: cells that kept the learned
- * start); the four count as sweeps.  harvest_x [n_cells][64], harvest_t
- * [n_cells][20] (device, may be NULL; only without mlp) receive the features
- * after the first two sweeps and the targets (converged - x2) / r_v. */
+ * sqrt(sum |dx|^2 / n_cells) <= tol or max_sweeps.  With mlp (may be NULL;
+ * design 0 needs max_sweeps >= 4): sweeps x0 -> x1 -> x2, the learned start
+ * xm, then J(x2) and J(xm) gated per cell (accepted_out: cells that kept the
+ * learned start); the four count as sweeps (design 1: see above).  harvest_x
+ * [n_cells][64], harvest_t [n_cells][20] (device, may be NULL; only without
+ * mlp) receive the features and the training targets of the context's
+ * design. */
 int dndsg_vr_to_tolerance(dndsg_ctx* ctx, const dndsg_mlp* mlp, double tol, int max_sweeps, int* sweeps_out,
                           int64_t* accepted_out, float* harvest_x, float* harvest_t, void* stream);
 /* dndsg_ssprk3_step with the reconstruction of every stage iterated to tol

@@ -252,3 +252,48 @@ def test_learned_start_sweeps_report(capsys):
     with capsys.disabled():
         print(f"\nJacobi sweeps per step to rms increment {tol:g} (vortex 96x96x2, fresh seed): "
               f"plain {res['plain']}, learned start {res['learned']}")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [1, 0])
+def test_previous_coefficient_design_keeps_the_tolerance(precision):
+    """Input design 1 (neighbour mean differences and the previous-step coefficients, before any
+    sweep): harvested targets are (converged - x0) / s with finite features, a network of the other
+    design is refused, and with a random or absurd network the iteration still stops only at the
+    plain Jacobi tolerance."""
+    torch, dev = _torch()
+    from dnds_b200.learned import WarmStartNet, harvest
+    from dnds_b200.solver import DndsgError
+
+    tol = 1e-7
+    s = _vortex(48, 22, precision)
+    s.set_warm_start_features(1)
+    s.vr_to_tolerance(tol, 2000)
+    X, T, sweeps = harvest(s, 1, 0.5, tol, 2000)
+    X, T = X.cpu().numpy(), T.cpu().numpy()
+    assert np.isfinite(X).all() and np.isfinite(T).all()
+    assert np.all(X[:, 36:56] == 0)
+    # the mean-difference block is scaled per variable by its own largest entry
+    du = X[:, :16].reshape(-1, 4, 4)
+    m = np.abs(du).max(axis=1)
+    live = m > 0
+    assert np.allclose(m[live], 1.0, atol=1e-6)
+    ref = _vortex(48, 22, precision)
+    ref.ssprk3_step(0.5)
+    ref.vr_to_tolerance(tol, 2000)
+    x_ref = ref.get_urec()
+    with pytest.raises(DndsgError, match="feature design"):
+        t = _vortex(48, 22, precision)
+        t.set_warm_start_features(1)
+        t.vr_to_tolerance(tol, 2000, WarmStartNet(0, params=mo.random_params(5), features=0))
+    for scale in (1.0, 1e3):
+        net = WarmStartNet(0, params=mo.random_params(23, scale=scale), features=1)
+        t = _vortex(48, 22, precision)
+        t.set_warm_start_features(1)
+        t.ssprk3_step(0.5)
+        n1, acc = t.vr_to_tolerance(tol, 2000, net)
+        assert n1 < 2000 and 0 <= acc <= t.N
+        x = t.get_urec()
+        assert np.sqrt(np.mean(np.sum((x - x_ref) ** 2, axis=(1, 2)))) < 200 * tol
+        flags, _ = t.status()
+        assert flags == 0
