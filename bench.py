@@ -515,6 +515,7 @@ def learned_leg(dev, grid, tol=1e-7, log=None):
     from dnds_b200.learned import WarmStartNet, evaluate, train, training_set
 
     out = {"tolerance_rms_increment": tol, "evaluation_grid": 1448}
+    nets = {}
     for design in (0, 1):
         t0 = time.perf_counter()
         X, T = training_set(tol, steps=8, n=256, features=design)
@@ -525,33 +526,32 @@ def learned_leg(dev, grid, tol=1e-7, log=None):
         _, val = train(net, X, T, epochs=20)
         torch.cuda.synchronize()
         t_train = time.perf_counter() - t0
-        r = {"pairs": int(X.shape[0]), "harvest_s": t_harvest, "train_s": t_train,
-             "train_samples_per_s": 20 * X.shape[0] / t_train, "val_loss": val,
-             "target_mean_square": float((T ** 2).mean())}
+        out[f"design{design}_training"] = {"pairs": int(X.shape[0]), "harvest_s": t_harvest, "train_s": t_train,
+                                           "train_samples_per_s": 20 * X.shape[0] / t_train, "val_loss": val,
+                                           "target_mean_square": float((T ** 2).mean())}
         del X, T
-        r.update(evaluate(net, tol, grid=1448, steps=3, seed=9999))
-        out[f"design{design}"] = r
-        if log:
-            log(design, r)
-        if design == 0:
-            # inference throughput of the tensor-core forward: 4,194,304 rows of 64 features
-            rows = 4_194_304
-            Xf = torch.randn((rows, 64), device=dev, dtype=torch.float32)
-            Yf = net.forward(Xf)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            for _ in range(5):
-                Yf = net.forward(Xf)
-            e1.record()
-            torch.cuda.synchronize()
-            ms = e0.elapsed_time(e1) / 5
-            flop = 2 * (64 * 64 * 3 + 64 * 20) * rows
-            out["forward_tc"] = {"rows": rows, "ms": ms, "rows_per_s": rows / (ms * 1e-3),
-                                 "tflops": flop / (ms * 1e-3) / 1e12, "gbs": rows * (64 * 4 + 20 * 4) / (ms * 1e-3) / 1e9,
-                                 "note": "tcgen05.mma kind::f16, BF16 operands, FP32 accumulator in tensor memory; "
-                                         "bytes are the FP32 features read and outputs written"}
-            del Xf, Yf
-        net.close()
+        nets[f"design{design}"] = net
+    out["evaluation"] = evaluate(nets, tol, grid=1448, steps=3, seed=9999, log=log)
+    # inference throughput of the tensor-core forward: 4,194,304 rows of 64 features
+    rows = 4_194_304
+    net = nets["design0"]
+    Xf = torch.randn((rows, 64), device=dev, dtype=torch.float32)
+    Yf = net.forward(Xf)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        Yf = net.forward(Xf)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / 5
+    flop = 2 * (64 * 64 * 3 + 64 * 20) * rows
+    out["forward_tc"] = {"rows": rows, "ms": ms, "rows_per_s": rows / (ms * 1e-3),
+                         "tflops": flop / (ms * 1e-3) / 1e12, "gbs": rows * (64 * 4 + 20 * 4) / (ms * 1e-3) / 1e9,
+                         "note": "tcgen05.mma kind::f16, BF16 operands, FP32 accumulator in tensor memory; "
+                                 "bytes are the FP32 features read and outputs written"}
+    del Xf, Yf
+    for n in nets.values():
+        n.close()
     return out
 
 

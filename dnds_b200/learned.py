@@ -209,11 +209,12 @@ def training_set(tol: float = 1e-7, steps: int = 8, n: int = 256, seeds=(11, 12)
     return torch.cat(Xs), torch.cat(Ts)
 
 
-def evaluate(net, tol: float = 1e-7, grid: int = 1448, steps: int = 3, seed: int = 9999, log=None):
-    """Jacobi sweeps per SSP-RK3 step to the same rms-increment tolerance, without and with the
-    network, on fresh-seed jittered grid x grid x 2 meshes of the vortex and of the Riemann problem
-    (with the CWBAP limiter), FP32 bulk: sweeps per step, ms per step (wall time of the steps), and the
-    density difference of the two runs after the steps (L2 relative to the density's L2)."""
+def evaluate(nets: dict, tol: float = 1e-7, grid: int = 1448, steps: int = 3, seed: int = 9999, log=None):
+    """Jacobi sweeps per SSP-RK3 step to the same rms-increment tolerance, without a network and with
+    each network of `nets` (name -> WarmStartNet), on fresh-seed jittered grid x grid x 2 meshes of the
+    vortex and of the Riemann problem (with the CWBAP limiter), FP32 bulk: sweeps per step, ms per step
+    (wall time of the steps), and the density difference to the plain run after the steps (L2 relative
+    to the density's L2)."""
     import time
 
     import torch
@@ -231,23 +232,23 @@ def evaluate(net, tol: float = 1e-7, grid: int = 1448, steps: int = 3, seed: int
         m = mk()
         vol = cell_quadrature(m)[1].sum(1)
         r, us = {"cells": m.n_cells}, {}
-        for label, use in (("plain", None), ("learned", net)):
+        for label, net in [("plain", None)] + list(nets.items()):
             s = Solver(m, preset(pre), precision=1)
-            s.set_warm_start_features(net.features)
+            s.set_warm_start_features(net.features if net is not None else 0)
             s.set_u(init(m))
             s.vr_to_tolerance(tol, 2000)
-            s.ssprk3_step_tol(cfl, tol, 2000, use)  # warm-up step
+            s.ssprk3_step_tol(cfl, tol, 2000, net)  # warm-up step
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            sw = [s.ssprk3_step_tol(cfl, tol, 2000, use) for _ in range(steps)]
+            sw = [s.ssprk3_step_tol(cfl, tol, 2000, net) for _ in range(steps)]
             torch.cuda.synchronize()
             r[label] = {"sweeps_per_step": sw, "ms_per_step": (time.perf_counter() - t0) / steps * 1e3}
             us[label] = s.get_u()
             s.close()
-        d = us["learned"][:, 0] - us["plain"][:, 0]
-        r["rho_l2_learned_vs_plain"] = float(np.sqrt((d * d * vol).sum() / (us["plain"][:, 0] ** 2 * vol).sum()))
-        r["sweeps_saved_per_step"] = float(np.mean(r["plain"]["sweeps_per_step"]) -
-                                           np.mean(r["learned"]["sweeps_per_step"]))
+            if label != "plain":
+                d = us[label][:, 0] - us["plain"][:, 0]
+                r[label]["rho_l2_vs_plain"] = float(np.sqrt((d * d * vol).sum() / (us["plain"][:, 0] ** 2 * vol).sum()))
+                r[label]["sweeps_saved_per_step"] = float(np.mean(r["plain"]["sweeps_per_step"]) - np.mean(sw))
         out[name] = r
         if log:
             log(name, r)

@@ -3,6 +3,7 @@
 //
 //   VRFiniteVolume2DGPU::ReconstructionJacobiStep      VRFiniteVolume2D, DNDS_FV_VR.hpp:1474-1479
 //   VRFiniteVolume2DGPU::ReconstructionWBAPLimitFacialV3  DNDS_FV_VR.hpp:2055-2061
+//   VRFiniteVolume2DGPU::ReconstructionWBAPLimitFacialV2  DNDS_FV_VR.hpp:1751-1757
 //   EulerEvaluatorGPU::EvaluateDt                       EulerEvaluator, DNDS_FV_EulerEvaluator.hpp:1408-1411
 //   EulerEvaluatorGPU::EvaluateRHS                      DNDS_FV_EulerEvaluator.hpp:1412-1418
 //   EulerEvaluatorGPU::EvaluateResidual                 DNDS_FV_EulerEvaluator.hpp:1455-1461
@@ -11,6 +12,8 @@
 //   ImplicitSteadyGPU::Step                             ImplicitBDFDualTimeStep::Step (order 1) with the
 //                                                       EulerSolver lambdas, DNDS_ODE.hpp:444-486 and
 //                                                       DNDS_FV_EulerSolver.hpp:713-994
+//   ImplicitSteadyGPU::Run                              the same internal loop in one call, with the fstop
+//                                                       CFL ramp and fsolve per gmresCode (:984-1061)
 //   ImplicitDualTimeStepGPU::Step                       ImplicitSDIRK4DualTimeStep / ImplicitBDFDualTimeStep
 //                                                       ::Step, DNDS_ODE.hpp:269-497, with the EulerSolver
 //                                                       lambdas (odeCode, gmresCode), :594-1226
@@ -88,6 +91,11 @@ class VRFiniteVolume2DGPU {
   void ReconstructionWBAPLimitFacialV3(bool ifAll, std::vector<double>* ifUseLimiter = nullptr, void* stream = nullptr) {
     if (ifUseLimiter) ifUseLimiter->resize(c_.nCells());
     c_.check(dndsg_limiter_wbap(c_.get(), ifAll ? 1 : 0, ifUseLimiter ? ifUseLimiter->data() : nullptr, stream));
+  }
+  // 3WBAP limiting (limiterProcedure 0) in place
+  void ReconstructionWBAPLimitFacialV2(bool ifAll, std::vector<double>* ifUseLimiter = nullptr, void* stream = nullptr) {
+    if (ifUseLimiter) ifUseLimiter->resize(c_.nCells());
+    c_.check(dndsg_limiter_wbap_v2(c_.get(), ifAll ? 1 : 0, ifUseLimiter ? ifUseLimiter->data() : nullptr, stream));
   }
 
  private:
@@ -175,6 +183,17 @@ class ImplicitSteadyGPU {
     }
     if (wallFlux) wallFlux->assign(wf, wf + 4);
     return iter > nTimeStepInternal ? nTimeStepInternal : iter;
+  }
+  // the whole steady internal loop in one call (dndsg_steady_solve); returns the iterations taken
+  int Run(const dndsg_steady_settings& settings, std::vector<double>* wallFlux = nullptr,
+          std::vector<double>* history = nullptr, void* stream = nullptr) {
+    int it = 0;
+    double res[5], wf[5];
+    if (history) history->assign(settings.max_iter, 0.0);
+    c_.check(dndsg_steady_solve(c_.get(), &settings, &it, res, wf, history ? history->data() : nullptr, stream));
+    if (wallFlux) wallFlux->assign(wf, wf + 4);
+    if (history) history->resize(it);
+    return it;
   }
 
  private:

@@ -39,7 +39,8 @@ def test_shim_header_compiles(tmp_path):
                    "    st.Step(100.0, 1e-8, 10, 1e100, 1, false, &r); ev.LUSGSMatrixVec(1.0, nullptr, nullptr);\n"
                    "    dndsg::ImplicitDualTimeStepGPU ode(c, 1, 2); ode.Step(0.1, 0.0, 100.0, 10, 1e-3, 1, false, 2, 10, 2);\n"
                    "    dndsg::GMRES_LeftPreconditionedGPU g(c, 10); g.solve(1.0, nullptr, nullptr, 2);\n"
-                   "    dndsg::ExplicitSSPRK3GPU rk(c); rk.Step(0.5); rk.Steps(0.5, 10, 2.0); } return 0; }\n")
+                   "    dndsg::ExplicitSSPRK3GPU rk(c); rk.Step(0.5); rk.Steps(0.5, 10, 2.0);\n"
+                   "    vr.ReconstructionWBAPLimitFacialV2(true); dndsg_steady_settings ss{}; st.Run(ss, &r, &r); } return 0; }\n")
     _compile(src, tmp_path / "a.out")
 
 
