@@ -20,7 +20,7 @@ EXPORTS = [
     "dndsg_mlp_get_params", "dndsg_mlp_forward", "dndsg_mlp_gradient", "dndsg_mlp_train_step",
     "dndsg_mlp_features", "dndsg_vr_to_tolerance", "dndsg_ssprk3_step_tol", "dndsg_mlp_set_features",
     "dndsg_set_warm_start_features",
-    "dndsg_lusgs_colours", "dndsg_lusgs_set_order", "dndsg_lusgs_matrix_init", "dndsg_lusgs_forward", "dndsg_lusgs_backward",
+    "dndsg_lusgs_colours", "dndsg_lusgs_set_order", "dndsg_lusgs_set_parts", "dndsg_lusgs_matrix_init", "dndsg_lusgs_forward", "dndsg_lusgs_backward",
     "dndsg_bdf_begin", "dndsg_implicit_iteration", "dndsg_dual_reset", "dndsg_dual_step", "dndsg_lusgs_matvec", "dndsg_gmres_lusgs",
     "dndsg_set_owned", "dndsg_rk_dt", "dndsg_rk_set_dt", "dndsg_rk_vr", "dndsg_rk_limit", "dndsg_rk_stage",
     "dndsg_rk_finish", "dndsg_halo_pack", "dndsg_halo_unpack", "dndsg_steady_solve",
@@ -112,6 +112,7 @@ def lib():
     L.dndsg_ssprk3_step_tol.argtypes = [vp, vp, dbl, dbl, dbl, i32, C.POINTER(i32), vp, vp, vp]
     L.dndsg_lusgs_colours.argtypes = [vp, vp, C.POINTER(i32)]
     L.dndsg_lusgs_set_order.argtypes = [vp, i32, vp, C.POINTER(i32)]
+    L.dndsg_lusgs_set_parts.argtypes = [vp, vp, i32, C.POINTER(i32)]
     L.dndsg_lusgs_matrix_init.argtypes = [vp, dbl, dbl, vp]
     L.dndsg_lusgs_forward.argtypes = [vp, dbl, vp, vp, vp]
     L.dndsg_lusgs_backward.argtypes = [vp, dbl, vp, vp, vp]

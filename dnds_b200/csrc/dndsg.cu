@@ -88,6 +88,14 @@ struct dndsg_ctx {
   int64_t maxLevelWidth = 0;
   std::vector<int32_t> colourHost;  // greedy colouring, kept for dndsg_lusgs_colours
   int lusgsOrder = 0;               // 0 colour batches, 1 level-scheduled scan order
+  // partitioned scan-order sweeps (the reference on several ranks): the part of every cell (empty:
+  // one part), and per sweep the index of every part's first level in fwdOff / bwdOff ([parts + 1],
+  // device) with the most levels of one part
+  std::vector<int32_t> lusgsPart;
+  int lusgsParts = 1;
+  int32_t *fwdPartLev = nullptr, *bwdPartLev = nullptr;
+  int fwdPartMax = 0, bwdPartMax = 0;
+  std::vector<int64_t> scanHost;  // the scan order last set (empty: natural cell order)
   double *Dinv = nullptr, *inc = nullptr, *resAcc = nullptr;
   double* Dmat = nullptr;  // the LU-SGS diagonal itself (GMRES matrix-vector product)
   // dual time stepping: BDF history (earlier steps' states) or the SDIRK stage right-hand sides,
@@ -2348,7 +2356,26 @@ __device__ __forceinline__ LuMatF& mat_flow(LuMatS& r) { return r.f; }
 __device__ __forceinline__ const LuMatF& mat_flow(const LuMatF& r) { return r; }
 __device__ __forceinline__ const LuMatF& mat_flow(const LuMatS& r) { return r.f; }
 
-// writes the record of every schedule position of one sweep, all positions in parallel
+// the neighbour term w dF - wl dU of one record slot (fields as in LuSlot) added to buf, and its U5
+// row c a + (w vn - wl) dS added to bufS when SA
+template <bool SA>
+__device__ __forceinline__ void lu_term(double vx, double vy, double vn, double H, double kq, double wl, double nx,
+                                        double ny, double w, double c, const double d[4], double dS, double g1,
+                                        double buf[4], double& bufS) {
+  const double dmn = nx * d[1] + ny * d[2];
+  const double a = dmn - vn * d[0];
+  const double dp = g1 * (d[3] - vx * d[1] - vy * d[2] + kq * d[0]);
+  const double dF[4] = {dmn, vn * d[1] + vx * a + nx * dp, vn * d[2] + vy * a + ny * dp, H * a + vn * (d[3] + dp)};
+  for (int v = 0; v < 4; v++) buf[v] += w * dF[v] - wl * d[v];
+  if constexpr (SA) bufS += c * a + (w * vn - wl) * dS;
+}
+
+// writes the record of every schedule position of one sweep, all positions in parallel.  In a
+// partitioned backward sweep a neighbour in another part (position kGhostPos) is a ghost: its
+// increment is the one after the forward sweep, which is what inc holds while this kernel runs, so
+// its term is summed here and folded into x0 (x0 = dU_fwd + di * ghost terms) instead of taking a
+// slot of the walk
+constexpr int32_t kGhostPos = -2;
 template <class T, bool FWD, bool SA>
 __global__ void __launch_bounds__(kBlock) k_lusgs_pack_mat(HotView<T> h, SaView<T> sa, const int32_t* cells,
                                                            const int32_t* nbF, const int32_t* nbJ, const int32_t* nbP,
@@ -2367,13 +2394,15 @@ __global__ void __launch_bounds__(kBlock) k_lusgs_pack_mat(HotView<T> h, SaView<
     f.j[k] = p.i;
     f.p[k] = 0;
   }
+  double ghost[4] = {0, 0, 0, 0}, ghostS = 0.0;
+  bool anyGhost = false;
   for (int k = 0; k < 4; k++) {
     if (!p.use[k]) continue;
     const double* U = p.U[k];
     const double ir = 1.0 / U[0];
     const double vx = U[1] * ir, vy = U[2] * ir, q2 = vx * vx + vy * vy;
     const double pr = g1 * (U[3] - 0.5 * U[0] * q2);
-    LuSlot& q = f.s[nu];
+    LuSlot q;
     q.vx = vx;
     q.vy = vy;
     q.vn = vx * p.nx[k] + vy * p.ny[k];
@@ -2384,6 +2413,15 @@ __global__ void __launch_bounds__(kBlock) k_lusgs_pack_mat(HotView<T> h, SaView<
     q.ny = p.ny[k];
     q.w = p.w[k];
     q.c = SA ? p.w[k] * sa.u[p.j[k]] * ir : 0.0;
+    if (!FWD && pa[k] == kGhostPos) {
+      double d[4];
+      load4<double>(&inc[(int64_t)p.j[k] * 4], d);
+      lu_term<SA>(q.vx, q.vy, q.vn, q.H, q.kq, q.wl, q.nx, q.ny, q.w, q.c, d, SA ? sa.inc[p.j[k]] : 0.0, g1, ghost,
+                  ghostS);
+      anyGhost = true;
+      continue;
+    }
+    f.s[nu] = q;
     f.j[nu] = p.j[k];
     f.p[nu] = pa[k];
     nu++;
@@ -2391,14 +2429,17 @@ __global__ void __launch_bounds__(kBlock) k_lusgs_pack_mat(HotView<T> h, SaView<
   for (int k = nu; k < 4; k++) f.s[k] = LuSlot{};
   double add[4] = {0, 0, 0, 0};
   if (!FWD) load4<double>(&inc[p.i * 4], add);
+  if (anyGhost)
+    for (int v = 0; v < 4; v++) add[v] += p.di * ghost[v];
   for (int v = 0; v < 4; v++) f.x0[v] = FWD ? p.base[v] : add[v];
   f.di = p.di;
   f.i = (int32_t)p.i;
   f.nu = nu;
   if constexpr (SA) {
     LuMatS& r = rec[t];
-    r.x0S = FWD ? sa.rhs[p.i] : sa.inc[p.i];
-    r.diS = sa.Dinv[p.i];
+    const double diS = sa.Dinv[p.i];
+    r.diS = diS;
+    r.x0S = FWD ? sa.rhs[p.i] : sa.inc[p.i] + (anyGhost ? diS * ghostS : 0.0);
     r.pad[0] = r.pad[1] = 0.0;
   }
 }
@@ -2466,14 +2507,7 @@ __device__ __forceinline__ void lusgs_mat_cell(const SaView<T>& sa, const LuMat<
     if (q >= nu) break;
     const double* sl = &f.s[q].vx;
     const double2 vxy = ld2(sl), vnH = ld2(sl + 2), kwl = ld2(sl + 4), nxy = ld2(sl + 6), wc = ld2(sl + 8);
-    const double* d = dU[q];
-    const double dmn = nxy.x * d[1] + nxy.y * d[2];
-    const double a = dmn - vnH.x * d[0];
-    const double dp = g1 * (d[3] - vxy.x * d[1] - vxy.y * d[2] + kwl.x * d[0]);
-    const double dF[4] = {dmn, vnH.x * d[1] + vxy.x * a + nxy.x * dp, vnH.x * d[2] + vxy.y * a + nxy.y * dp,
-                          vnH.y * a + vnH.x * (d[3] + dp)};
-    for (int v = 0; v < 4; v++) buf[v] += wc.x * dF[v] - kwl.y * d[v];
-    if constexpr (SA) bufS += wc.y * a + (wc.x * vnH.x - kwl.y) * dS[q];
+    lu_term<SA>(vxy.x, vxy.y, vnH.x, vnH.y, kwl.x, kwl.y, nxy.x, nxy.y, wc.x, wc.y, dU[q], dS[q], g1, buf, bufS);
   }
   double o[4];
   for (int v = 0; v < 4; v++) o[v] = FWD ? f.di * buf[v] : x0[v] + f.di * buf[v];
@@ -2492,12 +2526,15 @@ __device__ __forceinline__ void lusgs_mat_cell(const SaView<T>& sa, const LuMat<
 // of a shared-memory double buffer on an mbarrier while the other warps finish the current level;
 // the block barrier per level publishes the increments (global memory and the ring).  Positions of
 // a level beyond kRecBlock read their records from global memory.  A bulk copy that does not land
-// in time sets kFlagTimeout and ends the walk.
+// in time sets kFlagTimeout and ends the walk.  Partitioned sweeps (partLev non-null) launch one
+// block per part, each walking its own levels (partLev[b] to partLev[b + 1] of off) with its own
+// ring: the parts share no dependency inside a sweep, so the blocks never wait on one another.
 template <bool SA>
 constexpr int mat_threads() { return kRecBlock + 32; }
 template <class T, bool FWD, bool SA>
 __global__ void __launch_bounds__(mat_threads<SA>()) k_lusgs_levels_mat(SaView<T> sa, const LuMat<SA>* rec,
-                                                                        const int64_t* off, int nlev, double* inc,
+                                                                        const int64_t* off, int nlev,
+                                                                        const int32_t* partLev, double* inc,
                                                                         double g1, unsigned* flags) {
   using R = LuMat<SA>;
   constexpr int NT = kRecBlock;
@@ -2509,6 +2546,11 @@ __global__ void __launch_bounds__(mat_threads<SA>()) k_lusgs_levels_mat(SaView<T
   R* buf = reinterpret_cast<R*>(ringS + (SA ? kMatRing : 0));
   const int tid = threadIdx.x;
   const bool producer = tid == NT;
+  if (partLev) {  // one block per part: this part's levels
+    const int32_t l0 = partLev[blockIdx.x];
+    nlev = partLev[blockIdx.x + 1] - l0;
+    off += l0;
+  }
   for (int l = tid; l <= nlev; l += blockDim.x) so[l] = (int32_t)off[l];
   if (tid == 0) {
     for (int k = 0; k < kRecStages; k++) mbar_init(smem_u32(&bars[k]), 1);
@@ -2690,7 +2732,11 @@ int ensure_lusgs(dndsg_ctx* c) {
 
 // the reference's sequential sweep in a given scan order, level-scheduled: the forward level of a
 // cell is one more than the largest forward level of its neighbours earlier in the scan (the
-// backward level likewise over the later ones), and each level is one batch
+// backward level likewise over the later ones), and each level is one batch.  With parts (the
+// reference on several ranks, DNDS_FV_EulerEvaluator.cpp:1177-1181, 1313-1317) every part sweeps its
+// own cells in the scan order: levels count only neighbours of the same part, the schedule holds
+// part after part (each part's levels contiguous), and a neighbour in another part enters the
+// backward sweep only, as a ghost (kGhostPos) with its post-forward increment
 int set_scan_order(dndsg_ctx* c, const int64_t* scan2cell) {
   int rc;
   if ((rc = ensure_lusgs(c))) return rc;
@@ -2702,30 +2748,65 @@ int set_scan_order(dndsg_ctx* c, const int64_t* scan2cell) {
     pos[i] = (int32_t)s;
     order[s] = (int32_t)i;
   }
+  if (scan2cell) c->scanHost.assign(scan2cell, scan2cell + N);
+  else c->scanHost.clear();
+  const int P = c->lusgsParts;
+  std::vector<int32_t> part(N, 0);
+  if (P > 1) part = c->lusgsPart;
   std::vector<int64_t> deg;
   std::vector<int32_t> adj;
   if ((rc = lusgs_adjacency(c, deg, adj))) return rc;
-  std::vector<int32_t> lf(N, 0), lb(N, 0);
-  int nf = 0, nb = 0;
+  std::vector<int32_t> lf(N, 0), lb(N, 0), nlf(P, 0), nlb(P, 0);
   for (int64_t s = 0; s < N; s++) {
     const int32_t i = order[s];
     int l = 0;
     for (int64_t k = deg[i]; k < deg[i + 1]; k++)
-      if (pos[adj[k]] < s) l = std::max(l, lf[adj[k]] + 1);
+      if (pos[adj[k]] < s && part[adj[k]] == part[i]) l = std::max(l, lf[adj[k]] + 1);
     lf[i] = l;
-    nf = std::max(nf, l + 1);
+    nlf[part[i]] = std::max(nlf[part[i]], l + 1);
   }
   for (int64_t s = N - 1; s >= 0; s--) {
     const int32_t i = order[s];
     int l = 0;
     for (int64_t k = deg[i]; k < deg[i + 1]; k++)
-      if (pos[adj[k]] > s) l = std::max(l, lb[adj[k]] + 1);
+      if (pos[adj[k]] > s && part[adj[k]] == part[i]) l = std::max(l, lb[adj[k]] + 1);
     lb[i] = l;
-    nb = std::max(nb, l + 1);
+    nlb[part[i]] = std::max(nlb[part[i]], l + 1);
+  }
+  // schedule keys: the part's first level plus the level within the part
+  std::vector<int32_t> baseF(P + 1, 0), baseB(P + 1, 0);
+  for (int p = 0; p < P; p++) {
+    baseF[p + 1] = baseF[p] + nlf[p];
+    baseB[p + 1] = baseB[p] + nlb[p];
+  }
+  const int fMax = *std::max_element(nlf.begin(), nlf.end()), bMax = *std::max_element(nlb.begin(), nlb.end());
+  if (P > 1 && (std::max(fMax, bMax) > kRecMaxLevels || c->nfmax > 4))  // checked before anything changes
+    return fail(c, DNDSG_UNSUPPORTED, "partitioned sweeps need at most 4 faces per cell and " +
+                                          std::to_string(kRecMaxLevels) + " levels per part");
+  c->fwdPartMax = fMax;
+  c->bwdPartMax = bMax;
+  const int nf = baseF[P], nb = baseB[P];
+  for (int64_t i = 0; i < N; i++) {
+    lf[i] += baseF[part[i]];
+    lb[i] += baseB[part[i]];
   }
   std::vector<int32_t> fwd, bwd;
   group_by(lf, nf, fwd, c->fwdOff);
   group_by(lb, nb, bwd, c->bwdOff);
+  for (int32_t** d : {&c->fwdPartLev, &c->bwdPartLev}) {
+    if (*d) {
+      auto it = std::find(c->allocs.begin(), c->allocs.end(), (void*)*d);
+      if (it != c->allocs.end()) c->allocs.erase(it);
+      cudaFree(*d);
+      *d = nullptr;
+    }
+  }
+  if (P > 1) {
+    if ((rc = dalloc(c, c->fwdPartLev, sizeof(int32_t) * (P + 1))) || (rc = dalloc(c, c->bwdPartLev, sizeof(int32_t) * (P + 1))))
+      return rc;
+    DG_CUDA(c, cudaMemcpy(c->fwdPartLev, baseF.data(), sizeof(int32_t) * (P + 1), cudaMemcpyHostToDevice));
+    DG_CUDA(c, cudaMemcpy(c->bwdPartLev, baseB.data(), sizeof(int32_t) * (P + 1), cudaMemcpyHostToDevice));
+  }
   c->maxLevelWidth = 0;
   for (int k = 0; k < nf; k++) c->maxLevelWidth = std::max(c->maxLevelWidth, c->fwdOff[k + 1] - c->fwdOff[k]);
   for (int k = 0; k < nb; k++) c->maxLevelWidth = std::max(c->maxLevelWidth, c->bwdOff[k + 1] - c->bwdOff[k]);
@@ -2762,7 +2843,12 @@ int set_scan_order(dndsg_ctx* c, const int64_t* scan2cell) {
         const int32_t f = sf >= 0 ? sf : ~sf;
         const int32_t j = sf >= 0 ? R[f] : L[f];
         if (j < 0) continue;
-        if (forward ? pos[j] < pos[i] : pos[j] > pos[i]) {
+        if (part[j] != part[i]) {
+          if (!forward) {
+            nj[4 * t + k] = j;
+            np[4 * t + k] = kGhostPos;
+          }
+        } else if (forward ? pos[j] < pos[i] : pos[j] > pos[i]) {
           nj[4 * t + k] = j;
           np[4 * t + k] = at[j];
         }
@@ -2813,21 +2899,25 @@ void launch_lusgs_sweep(dndsg_ctx* c, bool forward, double alpha, const double* 
   const int nb = (int)off.size() - 1;
   // many narrow levels: one block walks them all over records packed in parallel beforehand
   // (a launch per level would cost more than the work)
-  if (c->lusgsOrder == 1 && nb <= kRecMaxLevels && c->nfmax <= 4) {
+  if (c->lusgsOrder == 1 && (forward ? c->fwdPartMax : c->bwdPartMax) <= kRecMaxLevels && c->nfmax <= 4) {
     const int64_t* od = forward ? c->fwdOffDev : c->bwdOffDev;
     const int32_t* nf = forward ? c->fwdNbF : c->bwdNbF;
     const int32_t* nj = forward ? c->fwdNbJ : c->bwdNbJ;
     const int32_t* np = forward ? c->fwdNbP : c->bwdNbP;
+    const int32_t* pl = c->lusgsParts > 1 ? (forward ? c->fwdPartLev : c->bwdPartLev) : nullptr;
+    const int nblk = c->lusgsParts > 1 ? c->lusgsParts : 1;
     SaView<T> none{};
     LuMatF* rec = (LuMatF*)c->lusgsMat;
     if (forward) {
       k_lusgs_pack_mat<T, true, false><<<grid_for(c->N), kBlock, 0, s>>>(h, none, cells, nf, nj, np, c->N, alpha, c->Dinv,
                                                                           rhs, inc, rec);
-      k_lusgs_levels_mat<T, true, false><<<1, mat_threads<false>(), mat_smem<false>(), s>>>(none, rec, od, nb, inc, h.gamma - 1, c->flags);
+      k_lusgs_levels_mat<T, true, false><<<nblk, mat_threads<false>(), mat_smem<false>(), s>>>(none, rec, od, nb, pl, inc,
+                                                                                              h.gamma - 1, c->flags);
     } else {
       k_lusgs_pack_mat<T, false, false><<<grid_for(c->N), kBlock, 0, s>>>(h, none, cells, nf, nj, np, c->N, alpha, c->Dinv,
                                                                            rhs, inc, rec);
-      k_lusgs_levels_mat<T, false, false><<<1, mat_threads<false>(), mat_smem<false>(), s>>>(none, rec, od, nb, inc, h.gamma - 1, c->flags);
+      k_lusgs_levels_mat<T, false, false><<<nblk, mat_threads<false>(), mat_smem<false>(), s>>>(none, rec, od, nb, pl, inc,
+                                                                                               h.gamma - 1, c->flags);
     }
     return;
   }
@@ -2905,7 +2995,31 @@ int dndsg_lusgs_set_order(dndsg_ctx* c, int mode, const int64_t* scan2cell, int*
     c->lusgsOrder = 0;
     if ((rc = upload_schedule(c, col, fwd, bwd))) return rc;
   }
-  if (n_batches) *n_batches = (int)(c->fwdOff.size() - 1 + c->bwdOff.size() - 1);
+  if (n_batches)
+    *n_batches = c->lusgsOrder == 1 ? c->fwdPartMax + c->bwdPartMax : (int)(c->fwdOff.size() - 1 + c->bwdOff.size() - 1);
+  return 0;
+}
+
+int dndsg_lusgs_set_parts(dndsg_ctx* c, const int32_t* part, int n_parts, int* n_batches) {
+  if (!c || (part && (n_parts < 1 || n_parts > 65535))) return DNDSG_BAD_ARGUMENT;
+  if (c->dead) return refuse_dead(c);
+  int rc;
+  if ((rc = set_device(c)) || (rc = ensure_lusgs(c))) return rc;
+  if (part && n_parts > 1) {
+    for (int64_t i = 0; i < c->N; i++)
+      if (part[i] < 0 || part[i] >= n_parts) return fail(c, DNDSG_BAD_ARGUMENT, "part index out of range");
+    c->lusgsPart.assign(part, part + c->N);
+    c->lusgsParts = n_parts;
+  } else {
+    c->lusgsPart.clear();
+    c->lusgsParts = 1;
+  }
+  if ((rc = set_scan_order(c, c->scanHost.empty() ? nullptr : c->scanHost.data()))) {
+    c->lusgsPart.clear();
+    c->lusgsParts = 1;
+    return rc;
+  }
+  if (n_batches) *n_batches = c->fwdPartMax + c->bwdPartMax;
   return 0;
 }
 
@@ -3156,20 +3270,24 @@ void launch_lusgs_sweep_sa(dndsg_ctx* c, bool forward, double alpha, const doubl
   const std::vector<int64_t>& off = forward ? c->fwdOff : c->bwdOff;
   const int32_t* cells = forward ? c->fwdCells : c->bwdCells;
   const int nb = (int)off.size() - 1;
-  if (c->lusgsOrder == 1 && nb <= kRecMaxLevels && c->nfmax <= 4) {
+  if (c->lusgsOrder == 1 && (forward ? c->fwdPartMax : c->bwdPartMax) <= kRecMaxLevels && c->nfmax <= 4) {
     const int64_t* od = forward ? c->fwdOffDev : c->bwdOffDev;
     const int32_t* nf = forward ? c->fwdNbF : c->bwdNbF;
     const int32_t* nj = forward ? c->fwdNbJ : c->bwdNbJ;
     const int32_t* np = forward ? c->fwdNbP : c->bwdNbP;
+    const int32_t* pl = c->lusgsParts > 1 ? (forward ? c->fwdPartLev : c->bwdPartLev) : nullptr;
+    const int nblk = c->lusgsParts > 1 ? c->lusgsParts : 1;
     LuMatS* rec = (LuMatS*)c->lusgsMat;
     if (forward) {
       k_lusgs_pack_mat<T, true, true><<<grid_for(c->N), kBlock, 0, s>>>(h, sa, cells, nf, nj, np, c->N, alpha, c->Dinv,
                                                                          rhs4, inc4, rec);
-      k_lusgs_levels_mat<T, true, true><<<1, mat_threads<true>(), mat_smem<true>(), s>>>(sa, rec, od, nb, inc4, h.gamma - 1, c->flags);
+      k_lusgs_levels_mat<T, true, true><<<nblk, mat_threads<true>(), mat_smem<true>(), s>>>(sa, rec, od, nb, pl, inc4,
+                                                                                           h.gamma - 1, c->flags);
     } else {
       k_lusgs_pack_mat<T, false, true><<<grid_for(c->N), kBlock, 0, s>>>(h, sa, cells, nf, nj, np, c->N, alpha, c->Dinv,
                                                                           rhs4, inc4, rec);
-      k_lusgs_levels_mat<T, false, true><<<1, mat_threads<true>(), mat_smem<true>(), s>>>(sa, rec, od, nb, inc4, h.gamma - 1, c->flags);
+      k_lusgs_levels_mat<T, false, true><<<nblk, mat_threads<true>(), mat_smem<true>(), s>>>(sa, rec, od, nb, pl, inc4,
+                                                                                            h.gamma - 1, c->flags);
     }
     return;
   }

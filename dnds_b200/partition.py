@@ -47,9 +47,14 @@ def _neighbours(mesh: M.Mesh):
     return start, b
 
 
+def block_owner(n_cells: int, nparts: int) -> np.ndarray:
+    """The part of every cell: nparts contiguous blocks of the cell order (int32)."""
+    return ((np.arange(n_cells, dtype=np.int64) * nparts) // n_cells).astype(np.int32)
+
+
 def partition_mesh(mesh: M.Mesh, nparts: int) -> list[Part]:
     n = mesh.n_cells
-    owner = (np.arange(n, dtype=np.int64) * nparts) // n
+    owner = block_owner(n, nparts).astype(np.int64)
     start, nb = _neighbours(mesh)
     parts = []
     for p in range(nparts):

@@ -179,6 +179,16 @@ class Solver:
         self._check(self.L.dndsg_lusgs_set_order(self.h, int(mode), _p(o) if o is not None else None, C.byref(nb)))
         return nb.value
 
+    def lusgs_set_parts(self, part=None, n_parts: int = 1) -> int:
+        """Partitioned scan-order sweeps, as the reference on n_parts ranks: part [N] in [0, n_parts)
+        (None: one part).  Switches to the scan-order schedule (the order last given to
+        lusgs_set_order, natural if none).  Returns the most levels of one part, forward plus backward."""
+        nb = C.c_int()
+        self._parts = None if part is None else np.ascontiguousarray(part, dtype=np.int32)
+        self._check(self.L.dndsg_lusgs_set_parts(self.h, _p(self._parts) if self._parts is not None else None,
+                                                 int(n_parts), C.byref(nb)))
+        return nb.value
+
     def LUSGSMatrixInit(self, dt: float = 1e100, alpha_diag: float = 1.0):
         """LUSGSMatrixInit (DNDS_FV_EulerEvaluator.cpp:995-1047) from the last EvaluateDt."""
         self._check(self.L.dndsg_lusgs_matrix_init(self.h, float(dt), float(alpha_diag), self.stream))

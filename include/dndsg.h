@@ -234,8 +234,23 @@ int dndsg_lusgs_colours(dndsg_ctx* ctx, int32_t* colour_out, int* n_colours);
  * the scan order scan2cell [n_cells] (host; NULL = natural cell order, the
  * reference's SOR_iScan2iCell default), run as dependency levels (one batch
  * per level) so that it computes what the sequential sweep computes.
- * n_batches (may be NULL): forward plus backward batches per iteration. */
+ * n_batches (may be NULL): forward plus backward batches per iteration (mode 1
+ * with parts: the most levels of one part, forward plus backward). */
 int dndsg_lusgs_set_order(dndsg_ctx* ctx, int mode, const int64_t* scan2cell, int* n_batches);
+/* partitioned sweeps: the mode-1 sweep as the reference runs it on n_parts MPI
+ * ranks (DNDS_FV_EulerEvaluator.cpp:1177-1181, 1313-1317; replaces the ranks'
+ * UpdateLUSGSForward / pull / UpdateLUSGSBackward sequence).  Every part sweeps
+ * its own cells in the scan order; a neighbour in another part is a ghost that
+ * enters only the backward sweep, with its increment as it stood after the
+ * forward sweep (the pull between the two).  part [n_cells] (host) in
+ * [0, n_parts); NULL or n_parts == 1: one part.  Rebuilds the mode-1 schedule
+ * with the scan order last given to dndsg_lusgs_set_order (natural order if
+ * none) and switches to it; each sweep then runs the parts' level walks
+ * concurrently, one thread block per part.  Parts apply to mode 1 only; a later
+ * dndsg_lusgs_set_order(mode 1) keeps them.  DNDSG_UNSUPPORTED (nothing
+ * changed) when a cell has more than 4 faces or a part more than 4095 levels.
+ * n_batches (may be NULL): the most levels of one part, forward plus backward. */
+int dndsg_lusgs_set_parts(dndsg_ctx* ctx, const int32_t* part, int n_parts, int* n_batches);
 /* LUSGSMatrixInit (DNDS_FV_EulerEvaluator.cpp:995-1047): D_i = 1/dTau_i + 1/dt
  * + sum_f (alpha/2) lambda_f A_f / V_i with dTau = (the DNDSG_BUF_DT of the last
  * dndsg_eval_dt) / alpha, and lambda_f from that same call */

@@ -133,13 +133,19 @@ class EulerEvaluatorGPU {
   void UpdateLUSGSBackward(double alphaDiag, const double* rhs, double* uInc, void* stream = nullptr) {
     c_.check(dndsg_lusgs_backward(c_.get(), alphaDiag, rhs, uInc, stream));
   }
-  // sweep order: mode 0 colour batches, 1 the sequential order scan2cell (nullptr: natural), level-scheduled
   void LUSGSMatrixVec(double alphaDiag, const double* x, double* Ax, void* stream = nullptr) {
     c_.check(dndsg_lusgs_matvec(c_.get(), alphaDiag, x, Ax, stream));
   }
+  // sweep order: mode 0 colour batches, 1 the sequential order scan2cell (nullptr: natural), level-scheduled
   int SetLUSGSOrder(int mode, const int64_t* scan2cell = nullptr) {
     int nb = 0;
     c_.check(dndsg_lusgs_set_order(c_.get(), mode, scan2cell, &nb));
+    return nb;
+  }
+  // the mode-1 sweep partitioned as on nParts ranks (part of every cell; nullptr: one part)
+  int SetLUSGSParts(const int32_t* part, int nParts) {
+    int nb = 0;
+    c_.check(dndsg_lusgs_set_parts(c_.get(), part, nParts, &nb));
     return nb;
   }
 

@@ -145,6 +145,7 @@ struct orc_ctx {
   std::vector<double> dtCell;
   std::vector<double> Dinv;      // LU-SGS diagonal inverse [N][nv] (diagonal per variable)
   std::vector<double> Dmat;      // the diagonal itself (jacobianCell, for LUSGSMatrixVec)
+  std::vector<int32_t> lusgsPart;  // partition of every cell for the partitioned sweeps (empty: none)
   // dual time stepping: BDF history (prevStart / cnPrev as ImplicitBDFDualTimeStep) or SDIRK
   // stage right-hand sides
   std::vector<std::vector<double>> odeVec;
@@ -1646,22 +1647,28 @@ void lusgs_matrix_init(orc_ctx& c, const double* dTau, double dt, double alpha) 
 }
 
 // the off-diagonal sum of UpdateLUSGSForward / Backward (DNDS_FV_EulerEvaluator.cpp:1149-1357)
-// over the neighbours j with scan position before (forward) or after (backward) cell i
+// over the neighbours j with scan position before (forward) or after (backward) cell i.  With a
+// partition (the reference run on several MPI ranks): a neighbour in another part is a ghost, whose
+// scan position counts as after every local cell (iScanOther = iScan + 1, :1177-1181, 1313-1317): it
+// enters the backward sweep only, with its value as pulled after the forward sweep (ghostInc)
 void lusgs_offdiag(const orc_ctx& c, int64_t i, int64_t si, const std::vector<int64_t>& pos, bool forward,
-                   double alpha, const double* inc, double* buf) {
+                   double alpha, const double* inc, double* buf, const double* ghostInc = nullptr) {
   const CellGeo& g = c.cg[i];
+  const bool parts = !c.lusgsPart.empty();
   for (int k = 0; k < g.nface; k++) {
     const int f = g.faces[k];
     const FaceGeo& fg = c.fg[f];
     const int64_t j = fg.L == i ? fg.R : fg.L;
     if (j < 0) continue;
-    if (forward ? !(pos[j] < si) : !(pos[j] > si)) continue;
+    const bool ghost = parts && c.lusgsPart[j] != c.lusgsPart[i];
+    if (ghost ? forward : (forward ? !(pos[j] < si) : !(pos[j] > si))) continue;
     const double nn = std::sqrt(sqr(fg.ncenter[0]) + sqr(fg.ncenter[1]));
     const double sg = fg.L == i ? 1.0 : -1.0;  // faces out of i
     const double n[2] = {sg * fg.ncenter[0] / nn, sg * fg.ncenter[1] / nn};
     const int nv = c.nv;
     double dF[kMaxV];
-    flux_jac_times_du(&c.u[j * nv], n, &inc[j * nv], c.lambdaFace[f], c.s.gamma, dF, nv);
+    flux_jac_times_du(&c.u[j * nv], n, ghost ? &ghostInc[j * nv] : &inc[j * nv], c.lambdaFace[f], c.s.gamma, dF,
+                      nv);
     for (int v = 0; v < nv; v++) buf[v] -= (0.5 * alpha) * fg.area / g.vol * dF[v];
   }
 }
@@ -1688,14 +1695,17 @@ void lusgs_sweeps(const orc_ctx& c, double alpha, const double* rhs, double* inc
       lusgs_offdiag(c, i, s, pos, true, alpha, inc, buf);
       for (int v = 0; v < nv; v++) inc[i * nv + v] = c.Dinv[i * nv + v] * buf[v];
     }
-  if (doBackward)
+  if (doBackward) {
+    std::vector<double> ghostInc;  // the ghosts' increments as pulled after the forward sweep
+    if (!c.lusgsPart.empty()) ghostInc.assign(inc, inc + c.N * c.nv);
     for (int64_t s = c.N - 1; s >= 0; s--) {
       const int64_t i = order[s];
       const int nv = c.nv;
       double buf[kMaxV] = {0};
-      lusgs_offdiag(c, i, s, pos, false, alpha, inc, buf);
+      lusgs_offdiag(c, i, s, pos, false, alpha, inc, buf, ghostInc.data());
       for (int v = 0; v < nv; v++) inc[i * nv + v] += c.Dinv[i * nv + v] * buf[v];
     }
+  }
 }
 
 
@@ -2025,6 +2035,12 @@ int orc_implicit_iteration(orc_ctx* c, double cfl, double dt, double alpha, cons
   for (int64_t i = 0; i < c->N; i++) compress_inc(*c, &c->u[i * nv], &inc[i * nv]);
   for (int64_t k = 0; k < n; k++) c->u[k] += inc[k];
   if (inc_out) std::memcpy(inc_out, inc.data(), sizeof(double) * n);
+  return 0;
+}
+
+int orc_set_lusgs_parts(orc_ctx* c, const int32_t* part) {
+  if (!part) c->lusgsPart.clear();
+  else c->lusgsPart.assign(part, part + c->N);
   return 0;
 }
 

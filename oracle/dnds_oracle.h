@@ -139,6 +139,9 @@ int orc_lusgs_matrix_init(orc_ctx* c, const double* dtau, double dt, double alph
  * on inc [n][nvars]; scan2cell [n] is the sweep order (NULL: natural order) */
 int orc_lusgs_forward(orc_ctx* c, double alpha, const double* rhs, double* inc, const int64_t* scan2cell);
 int orc_lusgs_backward(orc_ctx* c, double alpha, const double* rhs, double* inc, const int64_t* scan2cell);
+/* partitioned sweeps, the reference run on several ranks: part [n] of every cell (NULL: one part);
+ * a neighbour in another part enters only the backward sweep, with its post-forward increment */
+int orc_set_lusgs_parts(orc_ctx* c, const int32_t* part);
 /* one BDF pseudo-time iteration (ImplicitBDFDualTimeStep::Step, DNDS_ODE.hpp:444-486,
  * first order) with the EulerSolver fdtau/frhs/fsolve lambdas; x_last [n][nvars]
  * is the state at the start of the physical step; inc_out [n][nvars] may be NULL */

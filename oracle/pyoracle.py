@@ -103,6 +103,7 @@ def lib():
         L.orc_lusgs_backward.argtypes = [vp, dbl, vp, vp, vp]
         L.orc_implicit_iteration.argtypes = [vp, dbl, dbl, dbl, vp, vp, dbl, i32, vp]
         L.orc_lusgs_matvec.argtypes = [vp, dbl, vp, vp]
+        L.orc_set_lusgs_parts.argtypes = [vp, vp]
         L.orc_gmres_lusgs.argtypes = [vp, dbl, i32, i32, vp, vp, vp]
         L.orc_dual_reset.argtypes = [vp]
         L.orc_dual_step.argtypes = [vp, C.POINTER(OrcDual), dbl, dbl, vp, vp, vp]
@@ -260,6 +261,11 @@ class Oracle:
             return None, None
         o = np.ascontiguousarray(scan2cell, dtype=np.int64)
         return o, _p(o)
+
+    def set_lusgs_parts(self, part=None):
+        """Partitioned LU-SGS sweeps (the reference on several MPI ranks); None: one part."""
+        self._parts = None if part is None else np.ascontiguousarray(part, dtype=np.int32)
+        lib().orc_set_lusgs_parts(self.h, _p(self._parts) if self._parts is not None else None)
 
     def lusgs_matrix_init(self, dt, alpha=1.0, dtau=None):
         d = None if dtau is None else np.ascontiguousarray(dtau, dtype=np.float64)

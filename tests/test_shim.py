@@ -34,7 +34,7 @@ def test_shim_header_compiles(tmp_path):
                    "int main(){ dndsg_mesh_desc m{}; dndsg_settings s{}; (void)m; (void)s;\n"
                    "  if (false) { dndsg::Context c(m, s); dndsg::VRFiniteVolume2DGPU vr(c); dndsg::EulerEvaluatorGPU ev(c);\n"
                    "    std::vector<double> r; vr.ReconstructionJacobiStep(); ev.EvaluateRHS(r, 0.0);\n"
-                   "    ev.SetLUSGSOrder(1); ev.LUSGSMatrixInit(1e100, 1.0); ev.UpdateLUSGSForward(1.0, nullptr, nullptr);\n"
+                   "    ev.SetLUSGSOrder(1); ev.SetLUSGSParts(nullptr, 1); ev.LUSGSMatrixInit(1e100, 1.0); ev.UpdateLUSGSForward(1.0, nullptr, nullptr);\n"
                    "    ev.UpdateLUSGSBackward(1.0, nullptr, nullptr); dndsg::ImplicitSteadyGPU st(c);\n"
                    "    st.Step(100.0, 1e-8, 10, 1e100, 1, false, &r); ev.LUSGSMatrixVec(1.0, nullptr, nullptr);\n"
                    "    dndsg::ImplicitDualTimeStepGPU ode(c, 1, 2); ode.Step(0.1, 0.0, 100.0, 10, 1e-3, 1, false, 2, 10, 2);\n"
