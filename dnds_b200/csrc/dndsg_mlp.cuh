@@ -401,41 +401,38 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_tc(MlpDev m, Src src, Dst dst, 
 // 128 rows per tile, one per thread; one CTA per SM holding all 512 tensor-memory columns:
 //   cols   0-191  the pre-activations z1, z2, z3 of the tile (FP32, kept for the backward pass)
 //   cols 192-255  the layer-4 output, then each backward product dH = dz W
-//   cols 256-511  dW1 .. dW4, accumulated over all of the CTA's tiles (rows = output units)
-// Every product is M = 128, K-major, BF16 x BF16 -> FP32.  The weight-gradient product
-// dW = dz^T h runs over the 128 rows of the tile as its K dimension: dz^T and h^T are written
-// transposed into shared memory (128-wide K, stride byte offset 2048), dz^T padded to 128 rows with
-// zeros (the unused accumulator rows stay zero).  dH = dz W uses the transposed weights W^T.
+//   cols 256-511  dW1 .. dW4, accumulated over all of the CTA's tiles (M = 64: output unit u in
+//                 tensor-memory lane (u & 15) + 32 (u >> 4), the half-subpartition layout of M = 64)
+// Every operand stays in the one layout it is written in, the K-major core-matrix layout of the forward
+// products ([rows][64 units], cm_off); the products that need an operand transposed read it as an
+// MN-major operand instead (the same bytes: MN-blocks of 8 units 128 B apart, K-blocks of 8 rows 1024 B
+// apart), so nothing is copied transposed:
+//   forward       z_l  = h_{l-1} W_l^T       A h_{l-1} K-major, B W_l K-major         M 128, N 64 | 32, K 64
+//   input grad    dH   = dz_l W_l            A dz_l K-major,    B W_l MN-major         M 128, N 64, K 64 | 32
+//   weight grad   dW_l += dz_l^T h_{l-1}     A dz_l MN-major,   B h_{l-1} MN-major     M 64, N 64, K 128
 constexpr int kTrCols = 512;
 struct TrTcSmem {
   alignas(128) unsigned char Wf[3 * kHid * 128 + kOutP * 128];  // W_l [N][64], core-matrix layout
-  alignas(128) unsigned char Wt[4][64 * 128];                    // W_l^T [64][64] (W4^T: columns >= 32 zero)
-  alignas(128) unsigned char A[kTcRows * 128];                   // x, h1, h2, h3, then dz, [128][64]
-  alignas(128) unsigned char XT[64 * 256];                       // x^T [64][128]
-  alignas(128) unsigned char HT[3][64 * 256];                    // h_l^T [64][128]
-  alignas(128) unsigned char DZT[kTcRows * 256];                 // dz^T [128][128], rows >= N zero
+  alignas(128) unsigned char X[kTcRows * 128];                   // the tile's features [128][64]
+  alignas(128) unsigned char H[3][kTcRows * 128];                // h1, h2, h3 [128][64]
+  alignas(128) unsigned char DZ[kTcRows * 128];                  // dz_l [128][64] (dz4: units >= 32 zero)
   float gb[3 * kHid + kOutP];                                    // bias gradients of the CTA
   uint64_t bar;
   uint32_t tmem;
+  unsigned char pad[8192];  // more than half of an SM's shared memory: one CTA per SM
 };
 static_assert(sizeof(TrTcSmem) > 233472 / 2, "one CTA per SM: it holds all 512 tensor-memory columns");
 
-// byte offset of element (row, k) of a 128-wide K-major operand
-__device__ __forceinline__ uint32_t cm_off128(int row, int k) {
-  return (uint32_t)((row >> 3) * 2048 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
-}
-__device__ __forceinline__ uint64_t umma_desc_sbo(uint32_t saddr, uint32_t sbo) {
-  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(sbo >> 4) << 32) |
+// MN-major shared-memory descriptor of the same core-matrix layout: leading byte offset (K-blocks of 8 rows)
+// 1024, stride byte offset (MN-blocks of 8 units) 128, descriptor version 1, no swizzle
+__device__ __forceinline__ uint64_t umma_desc_mn(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(1024 >> 4) << 16) | ((uint64_t)(128 >> 4) << 32) |
          (1ull << 46);
 }
-// one thread issues D (+)= A B for K = 16 ksteps (A and B K-major with the given stride byte offsets)
-__device__ __forceinline__ void umma_chain(uint32_t d, uint32_t a, uint32_t sboA, uint32_t b, uint32_t sboB,
-                                           uint32_t idesc, int ksteps, bool accumulate) {
-  for (int ks = 0; ks < ksteps; ks++)
-    umma_bf16(d, umma_desc_sbo(a + 256 * ks, sboA), umma_desc_sbo(b + 256 * ks, sboB), idesc, accumulate || ks > 0);
-}
-__device__ __forceinline__ void st_bf16(unsigned char* base, uint32_t off, float v) {
-  *reinterpret_cast<__nv_bfloat16*>(base + off) = __float2bfloat16(v);
+// instruction descriptor of kind::f16 with the operands' majors (a_major bit 15, b_major bit 16) and M
+__host__ __device__ constexpr uint32_t umma_idesc_mk(int m, int n, bool aMN, bool bMN) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | (aMN ? (1u << 15) : 0u) | (bMN ? (1u << 16) : 0u) |
+         ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
 }
 // sum over the 128 rows (threads) of column values v[16], added into gb[c0 .. c0 + 15]
 __device__ __forceinline__ void tr_bias_sum(const float* v, float* gb, int c0) {
@@ -451,18 +448,14 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_train_tc(MlpDev m, const float*
   extern __shared__ __align__(128) unsigned char raw[];
   TrTcSmem& S = *reinterpret_cast<TrTcSmem*>(raw);
   const int tid = threadIdx.x, warp = tid >> 5;
-  // weights: W_l in the forward layout and W_l^T for dH = dz W
-  for (int e = tid; e < (3 * kHid + kOutP) * 64; e += blockDim.x) {
-    const int row = e >> 6, k = e & 63;
+  // the weights (row-major [N][64] BF16 in global memory) into the core-matrix layout, 16 B at a time
+  for (int e = tid; e < (3 * kHid + kOutP) * 8; e += blockDim.x) {
+    const int row = e >> 3, kc = e & 7;
     const int layer = row < 3 * kHid ? row / kHid : 3, rl = row - layer * kHid;
     const int woff = layer == 0 ? kWOff1 : layer == 1 ? kWOff2 : layer == 2 ? kWOff3 : kWOff4;
-    const bf16 w = m.W[woff + rl * 64 + k];
-    *reinterpret_cast<bf16*>(S.Wf + layer * kHid * 128 + cm_off(rl, k)) = w;
-    *reinterpret_cast<bf16*>(S.Wt[layer] + cm_off(k, rl)) = w;
+    *reinterpret_cast<uint4*>(S.Wf + layer * kHid * 128 + cm_off(rl, 8 * kc)) =
+        *reinterpret_cast<const uint4*>(m.W + woff + rl * 64 + 8 * kc);
   }
-  for (int e = tid; e < 64 * kOutP; e += blockDim.x)  // W4^T columns 32..63
-    *reinterpret_cast<bf16*>(S.Wt[3] + cm_off(e >> 5, kOutP + (e & 31))) = __float2bfloat16(0.f);
-  for (int e = tid; e < kTcRows * 128; e += blockDim.x) S.DZT[e * 2] = 0, S.DZT[e * 2 + 1] = 0;
   for (int e = tid; e < 3 * kHid + kOutP; e += blockDim.x) S.gb[e] = 0.f;
   const uint32_t bar = smem_u32(&S.bar);
   if (warp == 0) {
@@ -479,8 +472,12 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_train_tc(MlpDev m, const float*
   __syncthreads();
   tc_fence_after();
   const uint32_t tb = S.tmem, lane0 = (uint32_t)(warp * 32) << 16;
-  const uint32_t aA = smem_u32(S.A), aXT = smem_u32(S.XT), aDZT = smem_u32(S.DZT);
-  const uint32_t idesc64 = umma_idesc(kHid), idesc32 = umma_idesc(kOutP);
+  const uint32_t aX = smem_u32(S.X), aDZ = smem_u32(S.DZ), aW = smem_u32(S.Wf);
+  const uint32_t aH[3] = {smem_u32(S.H[0]), smem_u32(S.H[1]), smem_u32(S.H[2])};
+  constexpr uint32_t idFwd64 = umma_idesc_mk(kTcRows, kHid, false, false);
+  constexpr uint32_t idFwd32 = umma_idesc_mk(kTcRows, kOutP, false, false);
+  constexpr uint32_t idDH = umma_idesc_mk(kTcRows, kHid, false, true);
+  constexpr uint32_t idDW = umma_idesc_mk(64, kHid, true, true);
   uint32_t phase = 0;
   bool failed = false, first = true;
   double lossLocal = 0.0;
@@ -502,7 +499,7 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_train_tc(MlpDev m, const float*
   };
   for (int64_t tile = blockIdx.x; tile * kTcRows < n && !failed; tile += gridDim.x) {
     const int64_t r0 = tile * kTcRows, r = r0 + tid;
-    // x: coalesced 32-B pieces into A (K-major) and x^T
+    // x: coalesced 32-B pieces into the K-major operand
     for (int e = tid; e < kTcRows * 8; e += blockDim.x) {
       const int row = e >> 3, kc = e & 7;
       float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -513,35 +510,32 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_train_tc(MlpDev m, const float*
       }
       __nv_bfloat162 p[4];
       for (int j = 0; j < 4; j++) p[j] = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
-      *reinterpret_cast<uint4*>(S.A + cm_off(row, 8 * kc)) = *reinterpret_cast<uint4*>(p);
-      for (int j = 0; j < 8; j++) st_bf16(S.XT, cm_off128(8 * kc + j, row), v[j]);
+      *reinterpret_cast<uint4*>(S.X + cm_off(row, 8 * kc)) = *reinterpret_cast<uint4*>(p);
     }
-    // ---- forward: z_l into tensor memory, h_l = SiLU(z_l + b_l) into A and h_l^T
+    // ---- forward: z_l into tensor memory, h_l = SiLU(z_l + b_l) into H[l]
     for (int l = 0; l < 4 && !failed; l++) {
       const uint32_t dcol = l < 3 ? 64u * l : 192u;
+      const uint32_t aIn = l == 0 ? aX : aH[l - 1], aWl = aW + (uint32_t)l * kHid * 128;
       if (!run([&] {
-            umma_chain(tb + dcol, aA, 1024, smem_u32(S.Wf + l * kHid * 128), 1024, l < 3 ? idesc64 : idesc32, 4, false);
+            for (int ks = 0; ks < 4; ks++)
+              umma_bf16(tb + dcol, umma_desc(aIn + 256 * ks), umma_desc(aWl + 256 * ks), l < 3 ? idFwd64 : idFwd32,
+                        ks > 0);
           })) {
         failed = true;
         break;
       }
       if (l < 3) {
-        for (int c0 = 0; c0 < 64; c0 += 16) {
-          float z[16];
-          tmem_ld16(tb + lane0 + dcol + c0, z);
-          tmem_wait_ld();
-          for (int k = 0; k < 16; k++) {
-            const float h = silu(z[k] + tc_bias_s(m.P, l, c0 + k));
-            st_bf16(S.A, cm_off(tid, c0 + k), h);
-            st_bf16(S.HT[l], cm_off128(c0 + k, tid), h);
-          }
-        }
+        float h[64];
+        for (int c0 = 0; c0 < 64; c0 += 16) tmem_ld16(tb + lane0 + dcol + c0, h + c0);
+        tmem_wait_ld();
+        for (int k = 0; k < 64; k++) h[k] = silu(h[k] + tc_bias_s(m.P, l, k));
+        tc_store_row(S.H[l], tid, h);
       } else {  // y = z4 + b4, dz4 = 2 (y - t) / count on the 20 outputs
-        float z[32], dz[32];
+        float z[32], dz[64];
         tmem_ld16(tb + lane0 + 192, z);
         tmem_ld16(tb + lane0 + 208, z + 16);
         tmem_wait_ld();
-        for (int o = 0; o < 32; o++) {
+        for (int o = 0; o < 64; o++) {
           float d = 0.f;
           if (o < kOut && r < n) {
             const float y = z[o] + tc_bias_s(m.P, 3, o);
@@ -551,36 +545,38 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_train_tc(MlpDev m, const float*
           }
           dz[o] = d;
         }
-        for (int o = 0; o < 64; o++) st_bf16(S.A, cm_off(tid, o), o < 32 ? dz[o] : 0.f);
-        for (int o = 0; o < 32; o++) st_bf16(S.DZT, cm_off128(o, tid), dz[o]);
+        tc_store_row(S.DZ, tid, dz);
         tr_bias_sum(dz, S.gb + 3 * kHid, 0);
         tr_bias_sum(dz + 16, S.gb + 3 * kHid, 16);
       }
     }
     // ---- backward: dW_l += dz_l^T h_{l-1}; dH = dz_l W_l; dz_{l-1} = dH SiLU'(z_{l-1} + b_{l-1})
     for (int l = 3; l >= 0 && !failed; l--) {
-      const uint32_t hT = l > 0 ? smem_u32(S.HT[l - 1]) : aXT;
+      const uint32_t aPrev = l > 0 ? aH[l - 1] : aX, aWl = aW + (uint32_t)l * kHid * 128;
       const bool acc = !first;
       if (!run([&] {
-            umma_chain(tb + 256 + 64u * l, aDZT, 2048, hT, 2048, idesc64, 8, acc);
-            if (l > 0) umma_chain(tb + 192, aA, 1024, smem_u32(S.Wt[l]), 1024, idesc64, 4, false);
+            for (int ks = 0; ks < kTcRows / 16; ks++)
+              umma_bf16(tb + 256 + 64u * l, umma_desc_mn(aDZ + 2048 * ks), umma_desc_mn(aPrev + 2048 * ks), idDW,
+                        acc || ks > 0);
+            if (l > 0) {
+              const int kst = l == 3 ? kOutP / 16 : kHid / 16;  // K = the layer's output units
+              for (int ks = 0; ks < kst; ks++)
+                umma_bf16(tb + 192, umma_desc(aDZ + 256 * ks), umma_desc_mn(aWl + 2048 * ks), idDH, ks > 0);
+            }
           })) {
         failed = true;
         break;
       }
       if (l > 0) {
+        float dh[64], z[64];
         for (int c0 = 0; c0 < 64; c0 += 16) {
-          float dh[16], z[16], dz[16];
-          tmem_ld16(tb + lane0 + 192 + c0, dh);
-          tmem_ld16(tb + lane0 + 64u * (l - 1) + c0, z);
-          tmem_wait_ld();
-          for (int k = 0; k < 16; k++) {
-            dz[k] = r < n ? dh[k] * silu_grad(z[k] + tc_bias_s(m.P, l - 1, c0 + k)) : 0.f;
-            st_bf16(S.A, cm_off(tid, c0 + k), dz[k]);
-            st_bf16(S.DZT, cm_off128(c0 + k, tid), dz[k]);
-          }
-          tr_bias_sum(dz, S.gb + (l - 1) * kHid, c0);
+          tmem_ld16(tb + lane0 + 192 + c0, dh + c0);
+          tmem_ld16(tb + lane0 + 64u * (l - 1) + c0, z + c0);
         }
+        tmem_wait_ld();
+        for (int k = 0; k < 64; k++) dh[k] = r < n ? dh[k] * silu_grad(z[k] + tc_bias_s(m.P, l - 1, k)) : 0.f;
+        tc_store_row(S.DZ, tid, dh);
+        for (int c0 = 0; c0 < 64; c0 += 16) tr_bias_sum(dh + c0, S.gb + (l - 1) * kHid, c0);
       }
     }
     first = false;
@@ -592,8 +588,10 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_train_tc(MlpDev m, const float*
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  // the CTA's weight gradients (rows < N of each accumulator) and bias gradients into G
+  // the CTA's weight gradients and bias gradients into G: dW_l unit u = 16 w + t in lane t < 16 of warp w
   if (!failed && !first) {
+    const int u = 16 * warp + (tid & 31);
+    const bool mine = (tid & 31) < 16;
     for (int l = 0; l < 4; l++) {
       const int N = l < 3 ? kHid : kOutP;
       const int woff = l == 0 ? kOffW1 : l == 1 ? kOffW2 : l == 2 ? kOffW3 : kOffW4;
@@ -601,9 +599,9 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_train_tc(MlpDev m, const float*
         float g[16];
         tmem_ld16(tb + lane0 + 256 + 64u * l + c0, g);
         tmem_wait_ld();
-        if (tid < N)
+        if (mine && u < N)
           for (int k = 0; k < 16; k++)
-            if (g[k] != 0.f) atomicAdd(&G[woff + tid * 64 + c0 + k], g[k]);
+            if (g[k] != 0.f) atomicAdd(&G[woff + u * 64 + c0 + k], g[k]);
       }
     }
     for (int e = tid; e < 3 * kHid + kOutP; e += blockDim.x) {
