@@ -461,7 +461,7 @@ def riemann_to_end_leg(dev, grid=512, t_end=0.3, log=None):
     HLLC) in FP32 bulk and in FP64 on a grid x grid jittered mesh (2 grid^2 triangles): steps, device
     time of the whole run, cell-RK-stage updates/s over it, and the density difference of the two
     precisions at t = 0.3 (L2 volume-weighted and Linf, absolute and relative to the density's own L2).
-    The configured 2048 x 2048 mesh takes about 39,000 steps per precision (python bench.py
+    The configured 2048 x 2048 mesh takes about 47,000 steps per precision (python bench.py
     --riemann-full); the default run uses a coarser grid so that the bench ends within minutes."""
     import torch
 

@@ -2065,7 +2065,7 @@ int mlp_grad(dndsg_mlp* m, const float* X, const float* Tg, int64_t n, cudaStrea
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m->device);
   const int64_t tiles = (n + kTcRows - 1) / kTcRows;
   const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(tiles, sms));  // one CTA per SM
-  k_mlp_train_tc<<<grid, kTcRows, sizeof(TrTcSmem), s>>>(mlp_dev(m), X, Tg, n, 1.0f / (float)(n * kOut), m->G,
+  k_mlp_train_tc<<<grid, kTrThreads, sizeof(TrTcSmem), s>>>(mlp_dev(m), X, Tg, n, 1.0f / (float)(n * kOut), m->G,
                                                          m->loss, m->flags);
   DG_MCUDA(m, cudaGetLastError());
   return 0;

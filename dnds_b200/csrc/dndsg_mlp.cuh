@@ -398,7 +398,8 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_tc(MlpDev m, Src src, Dst dst, 
 
 // loss = mean over rows and the 20 outputs of (y - t)^2; gradients accumulate into G
 // ---------------------------------------------------------------- training on the tensor cores (tcgen05)
-// 128 rows per tile, one per thread; one CTA per SM holding all 512 tensor-memory columns:
+// 128 rows per tile, 512 threads (16 columns of one row each); one CTA per SM holding all 512
+// tensor-memory columns:
 //   cols   0-191  the pre-activations z1, z2, z3 of the tile (FP32, kept for the backward pass)
 //   cols 192-255  the layer-4 output, then each backward product dH = dz W
 //   cols 256-511  dW1 .. dW4, accumulated over all of the CTA's tiles (M = 64: output unit u in
@@ -434,20 +435,51 @@ __host__ __device__ constexpr uint32_t umma_idesc_mk(int m, int n, bool aMN, boo
   return (1u << 4) | (1u << 7) | (1u << 10) | (aMN ? (1u << 15) : 0u) | (bMN ? (1u << 16) : 0u) |
          ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
 }
-// sum over the 128 rows (threads) of column values v[16], added into gb[c0 .. c0 + 15]
-__device__ __forceinline__ void tr_bias_sum(const float* v, float* gb, int c0) {
-  for (int k = 0; k < 16; k++) {
-    float a = v[k];
-    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-    if ((threadIdx.x & 31) == 0) atomicAdd(&gb[c0 + k], a);
+// one butterfly round of a 16-column warp sum: lanes L and L ^ O trade halves of their W columns, each
+// keeping the half its bit O selects, summed with the partner's copy of the same columns
+template <int W, int O>
+__device__ __forceinline__ void tr_bfly(float* v, int lane) {
+  const bool up = (lane & O) != 0;
+#pragma unroll
+  for (int k = 0; k < W; k++) {
+    const float send = up ? v[k] : v[k + W], keep = up ? v[k + W] : v[k];
+    v[k] = keep + __shfl_xor_sync(0xffffffffu, send, O);
+  }
+}
+// the sums over the warp's 32 rows of 16 column values v (destroyed), added into gb[0 .. 15]: four
+// butterfly rounds halve the columns a lane holds (8 + 4 + 2 + 1 shuffles, against 5 per column for
+// 16 separate reductions), a last one completes the sum, and 16 lanes add one column each
+__device__ __forceinline__ void tr_bias_sum16(float* v, float* gb) {
+  const int lane = threadIdx.x & 31;
+  tr_bfly<8, 16>(v, lane);
+  tr_bfly<4, 8>(v, lane);
+  tr_bfly<2, 4>(v, lane);
+  tr_bfly<1, 2>(v, lane);
+  const float sum = v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
+  const int c = ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
+  if ((lane & 1) == 0) atomicAdd(&gb[c], sum);
+}
+// 16 values of a row, as BF16, into columns c0 .. c0 + 15 of a 64-wide K-major operand (c0 % 8 == 0)
+__device__ __forceinline__ void tc_store16(unsigned char* A, int row, int c0, const float* x) {
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    __nv_bfloat162 p[4];
+    for (int e = 0; e < 4; e++) p[e] = __floats2bfloat162_rn(x[8 * h + 2 * e], x[8 * h + 2 * e + 1]);
+    *reinterpret_cast<uint4*>(A + cm_off(row, c0 + 8 * h)) = *reinterpret_cast<uint4*>(p);
   }
 }
 
-__global__ void __launch_bounds__(kTcRows) k_mlp_train_tc(MlpDev m, const float* X, const float* Tg, int64_t n,
-                                                          float invCount, float* G, double* lossAcc, unsigned* flags) {
+// 512 threads: warp w reads tensor-memory lanes 32 (w % 4) .. + 31, i.e. tile rows 32 q + lane (q = w % 4),
+// and handles columns 16 g .. 16 g + 15 (g = w / 4) of every 64-wide layer, so the epilogues of a
+// tile (bias, activation, operand store, bias-gradient sums) are spread over 16 warps
+constexpr int kTrThreads = 512;
+__global__ void __launch_bounds__(kTrThreads, 1) k_mlp_train_tc(MlpDev m, const float* X, const float* Tg, int64_t n,
+                                                                float invCount, float* G, double* lossAcc,
+                                                                unsigned* flags) {
   extern __shared__ __align__(128) unsigned char raw[];
   TrTcSmem& S = *reinterpret_cast<TrTcSmem*>(raw);
-  const int tid = threadIdx.x, warp = tid >> 5;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int q = warp & 3, g = warp >> 2, row = 32 * q + lane;
   // the weights (row-major [N][64] BF16 in global memory) into the core-matrix layout, 16 B at a time
   for (int e = tid; e < (3 * kHid + kOutP) * 8; e += blockDim.x) {
     const int row = e >> 3, kc = e & 7;
@@ -471,7 +503,7 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_train_tc(MlpDev m, const float*
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  const uint32_t tb = S.tmem, lane0 = (uint32_t)(warp * 32) << 16;
+  const uint32_t tb = S.tmem, lane0 = (uint32_t)(q * 32) << 16, col0 = 16u * g;
   const uint32_t aX = smem_u32(S.X), aDZ = smem_u32(S.DZ), aW = smem_u32(S.Wf);
   const uint32_t aH[3] = {smem_u32(S.H[0]), smem_u32(S.H[1]), smem_u32(S.H[2])};
   constexpr uint32_t idFwd64 = umma_idesc_mk(kTcRows, kHid, false, false);
@@ -498,7 +530,7 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_train_tc(MlpDev m, const float*
     return true;
   };
   for (int64_t tile = blockIdx.x; tile * kTcRows < n && !failed; tile += gridDim.x) {
-    const int64_t r0 = tile * kTcRows, r = r0 + tid;
+    const int64_t r0 = tile * kTcRows, r = r0 + row;
     // x: coalesced 32-B pieces into the K-major operand
     for (int e = tid; e < kTcRows * 8; e += blockDim.x) {
       const int row = e >> 3, kc = e & 7;
@@ -525,29 +557,29 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_train_tc(MlpDev m, const float*
         break;
       }
       if (l < 3) {
-        float h[64];
-        for (int c0 = 0; c0 < 64; c0 += 16) tmem_ld16(tb + lane0 + dcol + c0, h + c0);
+        float h[16];
+        tmem_ld16(tb + lane0 + dcol + col0, h);
         tmem_wait_ld();
-        for (int k = 0; k < 64; k++) h[k] = silu(h[k] + tc_bias_s(m.P, l, k));
-        tc_store_row(S.H[l], tid, h);
-      } else {  // y = z4 + b4, dz4 = 2 (y - t) / count on the 20 outputs
-        float z[32], dz[64];
-        tmem_ld16(tb + lane0 + 192, z);
-        tmem_ld16(tb + lane0 + 208, z + 16);
-        tmem_wait_ld();
-        for (int o = 0; o < 64; o++) {
-          float d = 0.f;
-          if (o < kOut && r < n) {
-            const float y = z[o] + tc_bias_s(m.P, 3, o);
-            const float dd = y - Tg[r * kOut + o];
-            lossLocal += (double)dd * dd;
-            d = 2.f * dd * invCount;
+        for (int k = 0; k < 16; k++) h[k] = silu(h[k] + tc_bias_s(m.P, l, col0 + k));
+        tc_store16(S.H[l], row, col0, h);
+      } else {  // y = z4 + b4, dz4 = 2 (y - t) / count on the 20 outputs (column groups 0 and 1)
+        float dz[16];
+        for (int k = 0; k < 16; k++) dz[k] = 0.f;
+        if (g < 2) {
+          float z[16];
+          tmem_ld16(tb + lane0 + 192 + col0, z);
+          tmem_wait_ld();
+          for (int k = 0; k < 16; k++) {
+            const int o = col0 + k;
+            if (o < kOut && r < n) {
+              const float dd = z[k] + tc_bias_s(m.P, 3, o) - Tg[r * kOut + o];
+              lossLocal += (double)dd * dd;
+              dz[k] = 2.f * dd * invCount;
+            }
           }
-          dz[o] = d;
         }
-        tc_store_row(S.DZ, tid, dz);
-        tr_bias_sum(dz, S.gb + 3 * kHid, 0);
-        tr_bias_sum(dz + 16, S.gb + 3 * kHid, 16);
+        tc_store16(S.DZ, row, col0, dz);  // units 32 .. 63 stay zero
+        if (g < 2) tr_bias_sum16(dz, S.gb + 3 * kHid + col0);
       }
     }
     // ---- backward: dW_l += dz_l^T h_{l-1}; dH = dz_l W_l; dz_{l-1} = dH SiLU'(z_{l-1} + b_{l-1})
@@ -568,15 +600,14 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_train_tc(MlpDev m, const float*
         break;
       }
       if (l > 0) {
-        float dh[64], z[64];
-        for (int c0 = 0; c0 < 64; c0 += 16) {
-          tmem_ld16(tb + lane0 + 192 + c0, dh + c0);
-          tmem_ld16(tb + lane0 + 64u * (l - 1) + c0, z + c0);
-        }
+        float dh[16], z[16];
+        tmem_ld16(tb + lane0 + 192 + col0, dh);
+        tmem_ld16(tb + lane0 + 64u * (l - 1) + col0, z);
         tmem_wait_ld();
-        for (int k = 0; k < 64; k++) dh[k] = r < n ? dh[k] * silu_grad(z[k] + tc_bias_s(m.P, l - 1, k)) : 0.f;
-        tc_store_row(S.DZ, tid, dh);
-        for (int c0 = 0; c0 < 64; c0 += 16) tr_bias_sum(dh + c0, S.gb + (l - 1) * kHid, c0);
+        for (int k = 0; k < 16; k++)
+          dh[k] = r < n ? dh[k] * silu_grad(z[k] + tc_bias_s(m.P, l - 1, col0 + k)) : 0.f;
+        tc_store16(S.DZ, row, col0, dh);
+        tr_bias_sum16(dh, S.gb + (l - 1) * kHid + col0);
       }
     }
     first = false;
@@ -588,21 +619,20 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_train_tc(MlpDev m, const float*
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  // the CTA's weight gradients and bias gradients into G: dW_l unit u = 16 w + t in lane t < 16 of warp w
+  // the CTA's weight gradients and bias gradients into G: dW_l unit u = 16 q + t in lane t < 16 of the
+  // warps of lane quarter q, columns 16 g .. 16 g + 15
   if (!failed && !first) {
-    const int u = 16 * warp + (tid & 31);
-    const bool mine = (tid & 31) < 16;
+    const int u = 16 * q + lane;
+    const bool mine = lane < 16;
     for (int l = 0; l < 4; l++) {
       const int N = l < 3 ? kHid : kOutP;
       const int woff = l == 0 ? kOffW1 : l == 1 ? kOffW2 : l == 2 ? kOffW3 : kOffW4;
-      for (int c0 = 0; c0 < 64; c0 += 16) {
-        float g[16];
-        tmem_ld16(tb + lane0 + 256 + 64u * l + c0, g);
-        tmem_wait_ld();
-        if (mine && u < N)
-          for (int k = 0; k < 16; k++)
-            if (g[k] != 0.f) atomicAdd(&G[woff + u * 64 + c0 + k], g[k]);
-      }
+      float gv[16];
+      tmem_ld16(tb + lane0 + 256 + 64u * l + col0, gv);
+      tmem_wait_ld();
+      if (mine && u < N)
+        for (int k = 0; k < 16; k++)
+          if (gv[k] != 0.f) atomicAdd(&G[woff + u * 64 + col0 + k], gv[k]);
     }
     for (int e = tid; e < 3 * kHid + kOutP; e += blockDim.x) {
       const int off = e < kHid ? kOffB1 + e : e < 2 * kHid ? kOffB2 + e - kHid : e < 3 * kHid ? kOffB3 + e - 2 * kHid
