@@ -1,6 +1,7 @@
 """Steady NACA 0012 runs on the implicit path (the role of the reference's EulerSolver run with
 `ifSteadyQuit`, DNDS_FV_EulerSolver.hpp:609-615 and :984-1061): first-order BDF pseudo time with
-colour-batched or scan-order LU-SGS, stopping on the relative density increment (fstop).
+colour-batched or scan-order LU-SGS (optionally partitioned, --parts), stopping on the relative
+density increment (fstop).
 
     python -m dnds_b200.steady --case sa --iters 2000 --cfl 100
 
@@ -42,6 +43,8 @@ def main(argv=None):
     ap.add_argument("--cfl", type=float, default=100.0)
     ap.add_argument("--threshold", type=float, default=1e-8, help="relative density increment to stop at")
     ap.add_argument("--order", choices=["natural", "colour", "lines"], default="natural")
+    ap.add_argument("--parts", type=int, default=1,
+                    help="sweep the scan order in this many parts, as the reference on that many ranks")
     ap.add_argument("--precision", type=int, default=0, help="0 FP64, 1 FP32 bulk")
     ap.add_argument("--every", type=int, default=100)
     ap.add_argument("--plt", default=None, help="write the final state as a Tecplot binary file (PrintData)")
@@ -52,6 +55,10 @@ def main(argv=None):
     s = Solver(m, cfg, precision=a.precision)
     nb = s.lusgs_set_order(0) if a.order == "colour" else s.lusgs_set_order(
         1, M.line_scan_order(m) if a.order == "lines" else None)
+    if a.parts > 1 and a.order != "colour":
+        from .partition import block_owner
+
+        nb = s.lusgs_set_parts(block_owner(m.n_cells, a.parts), a.parts)
     s.set_u(np.tile(np.array(cfg["eulerSetting"]["farFieldStaticValue"]), (m.n_cells, 1)))
     s.bdf_begin()
     print(f"{m.name}: {m.n_cells} cells, case {a.case}, {nb} LU-SGS batches per iteration")
