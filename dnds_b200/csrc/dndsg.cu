@@ -154,6 +154,20 @@ __device__ __forceinline__ double warp_max(double v) {
   for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
 }
+// the sum of v over a block of kBlock threads (all of them call this) added to *acc by one thread:
+// one atomic per block instead of one per warp (many warps adding to one address serialise in L2)
+__device__ __forceinline__ void block_add(double v, double* acc) {
+  __shared__ double part[kBlock / 32];
+  v = warp_sum(v);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double t = threadIdx.x < kBlock / 32 ? part[threadIdx.x] : 0.0;
+    t = warp_sum(t);
+    if (threadIdx.x == 0 && t != 0.0) atomicAdd(acc, t);
+  }
+  __syncthreads();  // part is reused by the next call
+}
 
 // ------------------------------------------------------------------ setup kernels
 __global__ void k_setup_cell(MeshView m, SetupParams p, CellSetup* cells, double* vol, double* bary, int* bad) {
@@ -2631,10 +2645,7 @@ __global__ void __launch_bounds__(kBlock) k_add_inc(int64_t N, double* u, const 
       a[v] = fabs(d) * w;
     }
   }
-  for (int v = 0; v < 4; v++) {
-    const double r = warp_sum(a[v]);
-    if ((threadIdx.x & 31) == 0 && r != 0.0) atomicAdd(&acc[v], r);
-  }
+  for (int v = 0; v < 4; v++) block_add(a[v], &acc[v]);
 }
 
 // the wall force: minus the sum of the Riemann fluxes of the Wall_Euler / Wall_NoSlip faces
@@ -3216,8 +3227,7 @@ __global__ void __launch_bounds__(kBlock) k_sa_add_inc(int64_t N, double* u, dou
     u[i] += d;
     a = fabs(d) * (volWise ? vol[i] : 1.0);
   }
-  a = warp_sum(a);
-  if ((threadIdx.x & 31) == 0 && a != 0.0) atomicAdd(acc, a);
+  block_add(a, acc);
 }
 
 __global__ void __launch_bounds__(kBlock) k_sa_wall_flux(int64_t Fi, int64_t F, const int32_t* faceBC,

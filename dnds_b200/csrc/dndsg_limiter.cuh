@@ -190,6 +190,27 @@ DG_HD double limiter_cell_indicator(int64_t i, const LimView& v) {
 DG_HD double signE(double x) { return x > 0 ? 1.0 : (x < 0 ? -1.0 : 0.0); }
 DG_HD float signE(float x) { return x > 0 ? 1.0f : (x < 0 ? -1.0f : 0.0f); }
 
+// Quotients and square roots of the limiting pass.  FP64 contexts keep exact operations; in FP32-bulk
+// contexts the pass is bound by instruction issue, and the hardware approximations serve: __fdividef
+// (2 ulp for divisors in [2^-126, 2^126], which every divisor it is given here lies in) and x rsqrt(x)
+// (about 2 ulp), far below the FP32 tolerance of the limited coefficients
+DG_HD double lim_div(double a, double b) { return a / b; }
+DG_HD double lim_sqrt(double x) { return sqrt(x); }
+DG_HD float lim_div(float a, float b) {
+#if defined(__CUDA_ARCH__)
+  return __fdividef(a, b);
+#else
+  return a / b;
+#endif
+}
+DG_HD float lim_sqrt(float x) {
+#if defined(__CUDA_ARCH__)
+  return x > 0.f ? x * rsqrtf(x) : 0.f;
+#else
+  return sqrtf(x);
+#endif
+}
+
 // FWBAP_L2_Biway(u1, u2, out, n) (DNDS_FV_Limiters.hpp:410-449), p = 4
 DG_HD double wbap_biway(double u1, double u2, double n) {
   double frac = u1 / (fabs(u2) + 1e-12) * signE(u2);
@@ -199,10 +220,10 @@ DG_HD double wbap_biway(double u1, double u2, double n) {
 // the same in FP32: |frac| is capped at 1e9 so that frac^4 stays finite (above the cap the
 // FP64 result is below 1e-9 |u1|, under FP32 resolution of u1, and the capped one is as small)
 DG_HD float wbap_biway(float u1, float u2, float n) {
-  float frac = u1 / (fabsf(u2) + 1e-12f) * signE(u2);
+  float frac = lim_div(u1, fabsf(u2) + 1e-12f) * signE(u2);  // divisor in [1e-12, FLT_MAX]
   frac = copysignf(fminf(fabsf(frac), 1e9f), frac);
   const float th1 = frac * frac * frac, th2 = (frac * frac) * (frac * frac);
-  return u1 * (n + th1) / (n + th2);
+  return u1 * lim_div(n + th1, n + th2);  // divisor in [n, n + 1e36], n >= 1
 }
 // one term of FWBAP_L2_Multiway (DNDS_FV_Limiters.hpp:341-405): theta = u0 / (|s| + verySmall^(1/4))
 // * sign(s), accumulated as theta^4 (down) and theta^3 (up); in FP32 capped at 1e9 as above
@@ -226,16 +247,33 @@ DG_HD void char_rows(int a, C gamma, const double* UL, const double* UR, C nx, C
   C UC[4], r[4];
   for (int k = 0; k < 4; k++) UC[k] = (C)((UL[k] + UR[k]) * 0.5);
   to_normal_frame(UC, nx, ny, r);
-  const C ir = C(1) / r[0];
+  const C ir = lim_div(C(1), r[0]);
   const C vx = r[1] * ir, vy = r[2] * ir, vs = vx * vx + vy * vy;
-  C p, a2, H;
-  thermal(r[3], r[0], vs, gamma, p, a2, H);
-  const C as = sqrt(a2), gb = gamma - C(1), sc = gb / (C(2) * as * as);
+  C p, a2, H, as, sc, asg, a2g, a4g;  // as / (gamma - 1), as^2 / (gamma - 1), 4 as^2 / (gamma - 1)
+  const C gb = gamma - C(1);
+  if constexpr (sizeof(C) == 4) {  // FP32: one reciprocal each of rho, a^2 and gamma - 1
+    const C igb = lim_div(C(1), gb);
+    p = gb * (r[3] - r[0] * C(0.5) * vs);
+    a2 = gamma * p * ir;
+    H = (r[3] + p) * ir;
+    as = lim_sqrt(a2);
+    sc = gb * lim_div(C(0.5), a2);
+    asg = as * igb;
+    a2g = a2 * igb;
+    a4g = C(4) * a2g;
+  } else {  // FP64: the operations in the order of the reference's expressions
+    thermal(r[3], r[0], vs, gamma, p, a2, H);
+    as = sqrt(a2);
+    sc = gb / (C(2) * as * as);
+    asg = as / gb;
+    a2g = (as * as) / gb;
+    a4g = C(4) / gb * (as * as);
+  }
   C L0[4];
-  if (a == 0) { L0[0] = H + as / gb * (vx - as); L0[1] = -vx - as / gb; L0[2] = -vy; L0[3] = C(1); }
-  else if (a == 1) { L0[0] = -C(2) * H + C(4) / gb * (as * as); L0[1] = vx * 2; L0[2] = vy * 2; L0[3] = -C(2); }
-  else if (a == 2) { L0[0] = vy * (-C(2) * (as * as) / gb); L0[1] = C(0); L0[2] = C(2) * (as * as) / gb; L0[3] = C(0); }
-  else { L0[0] = H - as / gb * (vx + as); L0[1] = -vx + as / gb; L0[2] = -vy; L0[3] = C(1); }
+  if (a == 0) { L0[0] = H + asg * (vx - as); L0[1] = -vx - asg; L0[2] = -vy; L0[3] = C(1); }
+  else if (a == 1) { L0[0] = -C(2) * H + a4g; L0[1] = vx * 2; L0[2] = vy * 2; L0[3] = -C(2); }
+  else if (a == 2) { L0[0] = vy * (-C(2) * a2g); L0[1] = C(0); L0[2] = C(2) * a2g; L0[3] = C(0); }
+  else { L0[0] = H - asg * (vx + as); L0[1] = -vx + asg; L0[2] = -vy; L0[3] = C(1); }
   // L = L0 * diag(1, base^T) in the momentum block: columns 1, 2 times [[nx, ny], [-ny, nx]]
   const C c1 = L0[1] * sc, c2 = L0[2] * sc;
   Lrow[0] = L0[0] * sc; Lrow[1] = c1 * nx - c2 * ny; Lrow[2] = c1 * ny + c2 * nx; Lrow[3] = L0[3] * sc;
@@ -336,7 +374,7 @@ __device__ __forceinline__ void limiter_cell4(bool valid, int64_t i, int c, cons
   C res[5];
   for (int q = 0; q < 5; q++) res[q] = ri[q];
   if (V3) {
-    for (int q = 0; q < 5; q++) res[q] = ri[q] * (up[q] + nStd) / (down[q] + nStd);
+    for (int q = 0; q < 5; q++) res[q] = ri[q] * lim_div(up[q] + nStd, down[q] + nStd);
   } else if (nO > 0) {
     constexpr int ls = PASS == 0 ? 2 : 0, nr = PASS == 0 ? 3 : 2;
     for (int r = 0; r < nr; r++) res[ls + r] = first[ls + r] * (up[ls + r] + C(1)) / (down[ls + r] + C(1));
