@@ -547,20 +547,23 @@ def learned_leg(dev, grid, tol=1e-7, log=None):
     """The learned VR warm start (BF16 MLP on tcgen05), both input designs: each is harvested from
     tolerance-mode runs of the three explicit workloads (the vortex on 40 x 40 quads and on two
     256 x 256 x 2 jittered triangle meshes, the Riemann problem with the limiter on 256 x 256 x 2), trained
-    on the GPU, and evaluated as Jacobi sweeps per SSP-RK3 step to the same rms-increment tolerance,
+    on the GPU (pairs whose targets exceed +-10 left out: learned.bounded_pairs), and evaluated as
+    Jacobi sweeps per SSP-RK3 step to the same rms-increment tolerance,
     with and without the network, on fresh-seed (9999) 1448 x 1448 x 2 = 4,193,408-triangle vortex and
     Riemann meshes.  Design 0 extrapolates two plain sweeps; design 1 is the configured input (neighbour
     mean differences and the previous-step coefficients).  Plus the tensor-core forward's throughput.
     Timed outside the headline."""
     import torch
 
-    from dnds_b200.learned import WarmStartNet, evaluate, train, training_set
+    from dnds_b200.learned import WarmStartNet, bounded_pairs, evaluate, train, training_set
 
     out = {"tolerance_rms_increment": tol, "evaluation_grid": 1448}
     nets = {}
     for design in (0, 1):
         t0 = time.perf_counter()
         X, T = training_set(tol, steps=8, n=256, features=design)
+        n_harvested = int(X.shape[0])
+        X, T, kept = bounded_pairs(X, T)
         torch.cuda.synchronize()
         t_harvest = time.perf_counter() - t0
         net = WarmStartNet(dev, seed=7, features=design)
@@ -568,7 +571,8 @@ def learned_leg(dev, grid, tol=1e-7, log=None):
         _, val = train(net, X, T, epochs=20)
         torch.cuda.synchronize()
         t_train = time.perf_counter() - t0
-        out[f"design{design}_training"] = {"pairs": int(X.shape[0]), "harvest_s": t_harvest, "train_s": t_train,
+        out[f"design{design}_training"] = {"pairs_harvested": n_harvested, "pairs": int(X.shape[0]),
+                                           "kept_fraction": kept, "harvest_s": t_harvest, "train_s": t_train,
                                            "train_samples_per_s": 20 * X.shape[0] / t_train, "val_loss": val,
                                            "target_mean_square": float((T ** 2).mean())}
         del X, T

@@ -137,6 +137,16 @@ def harvest(solver: Solver, steps: int, cfl: float, tol: float, max_sweeps: int 
     return torch.cat(Xs), torch.cat(Ts), sweeps
 
 
+def bounded_pairs(X, T, bound: float = 10.0):
+    """The pairs whose targets all lie within +-bound, and the fraction kept.  Targets are coefficient
+    changes in units of the cell's own feature scale; where that scale sits at its floor (a nearly
+    uniform neighbourhood) a rounding-level change becomes a huge target, yet the network's output is
+    multiplied by that same tiny scale when it is applied, so such pairs carry nothing for inference
+    and would only dominate the mean-square loss."""
+    keep = T.abs().amax(dim=1) <= bound
+    return X[keep].contiguous(), T[keep].contiguous(), float(keep.float().mean())
+
+
 def train(net: WarmStartNet, X, T, epochs: int = 20, batch: int = 65536, lr: float = 2e-3,
           lr_end: float = 5e-5, seed: int = 0, val_frac: float = 0.05, log=None):
     """Minibatch Adam with a cosine learning-rate decay; returns (train losses per epoch, validation loss)."""

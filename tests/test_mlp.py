@@ -64,6 +64,18 @@ def _rel(a, b):
     return float(np.linalg.norm(np.asarray(a, np.float64) - b) / np.linalg.norm(b))
 
 
+def test_bounded_pairs_drops_only_unbounded_targets():
+    import torch
+
+    from dnds_b200.learned import bounded_pairs
+
+    X = torch.arange(12, dtype=torch.float32).reshape(4, 3)
+    T = torch.tensor([[0.5, -2.0], [11.0, 0.0], [-10.0, 10.0], [0.0, -10.5]])
+    Xk, Tk, kept = bounded_pairs(X, T, bound=10.0)
+    assert kept == 0.5
+    assert torch.equal(Xk, X[[0, 2]]) and torch.equal(Tk, T[[0, 2]])
+
+
 @pytest.mark.gpu
 def test_forward_matches_oracle():
     torch, dev = _torch()
