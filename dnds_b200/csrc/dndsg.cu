@@ -329,9 +329,10 @@ __global__ void k_setup_lim_compact(MeshView m, const CellSetup* cells, const do
   const int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   setup_limiter_compact<T>(f, m, cells, faceW, g, cellFr);
 }
-// FP64: 2 blocks per SM.  FP32 (FP32 arithmetic, 95 registers at 2 blocks): 3 blocks per SM
+// FP64: 2 blocks per SM.  FP32: 4 blocks per SM (64 registers; the pass waits on its gathers, and the
+// fourth block took the 8,388,608-triangle Riemann step from 8.61 to 8.44 ms against three)
 template <class T>
-__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 3 : 2) k_lim_face(LimView v, const T* urec, int32_t* count) {
+__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 4 : 2) k_lim_face(LimView v, const T* urec, int32_t* count) {
   int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (f == 0) *count = 0;  // the list of cells to limit, filled by the next launch
   if (f < v.F) limiter_face_indicator<T>(f, v, urec);

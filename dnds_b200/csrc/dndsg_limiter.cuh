@@ -34,10 +34,11 @@ DG_HD int64_t lim_at(int64_t f, int e) { return f * kLimStride + e; }
 constexpr int kMsR2L = 0, kMsL2R = 25;
 // the indicator's compact data, in the context's precision: per face (AoSoA E = kLimG) the frame
 // coordinates (xi, eta) of gauss point 0 in the left and the right cell and the 6 face weights; per
-// cell ([N][kLimCell]) the frame's Pinv (row-major) and basis moments.  D at the point follows from
-// these (p2_diffs_at), a fifth of the bytes of storing it.
+// cell ([N][kLimCell]) the frame's Pinv (row-major) and basis moments, padded to 12 so that a cell's
+// row is read in 16-byte vectors.  D at the point follows from these (p2_diffs_at), a fifth of the bytes
+// of storing it.
 constexpr int kLimG = 10;
-constexpr int kLimCell = 9;
+constexpr int kLimCell = 12;
 
 struct LimView {
   int64_t N, F, Fi;
@@ -108,6 +109,7 @@ DG_HD void setup_limiter_compact(int64_t f, const MeshView& m, const CellSetup* 
     T* o = cellFr + f * kLimCell;
     o[0] = (T)fr.Pinv[0][0]; o[1] = (T)fr.Pinv[0][1]; o[2] = (T)fr.Pinv[1][0]; o[3] = (T)fr.Pinv[1][1];
     for (int k = 0; k < 5; k++) o[4 + k] = (T)fr.moment[k];
+    for (int k = 9; k < kLimCell; k++) o[k] = T(0);
   }
 }
 
@@ -127,14 +129,17 @@ DG_HD void limiter_face_indicator(int64_t f, const LimView& v, const T* urec) {
   C sv[2][6][2];
   for (int side = 0; side < 2; side++) {
     const int64_t cell = side ? R : L;
-    const T* c = cf + cell * kLimCell;
+    // the cell's frame row and its 5 x 4 coefficients in 16-byte vectors (rho and E are used)
+    T c[kLimCell], rows[5][4];
+    for (int k = 0; k < kLimCell; k += 4) load_row(cf + cell * kLimCell + k, &c[k]);
+    for (int q = 0; q < 5; q++) load_row(urec + cell * 20 + 4 * q, rows[q]);
     const C Q[2][2] = {{c[0], c[1]}, {c[2], c[3]}};
     const C mo[5] = {c[4], c[5], c[6], c[7], c[8]};
     C D[6][5];
     p2_diffs_at<C>(Q, mo, g[aos(f, 2 * side, kLimG)], g[aos(f, 2 * side + 1, kLimG)], D);
     for (int k = 0; k < 2; k++) {
       C r[5];
-      for (int q = 0; q < 5; q++) r[q] = urec[cell * 20 + q * 4 + var[k]];
+      for (int q = 0; q < 5; q++) r[q] = rows[q][k == 0 ? 0 : 3];
       for (int d = 0; d < 6; d++) {
         C a = C(0);
         for (int q = 0; q < 5; q++) a += D[d][q] * r[q];
