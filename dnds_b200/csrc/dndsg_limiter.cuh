@@ -129,10 +129,20 @@ DG_HD void limiter_face_indicator(int64_t f, const LimView& v, const T* urec) {
   C sv[2][6][2];
   for (int side = 0; side < 2; side++) {
     const int64_t cell = side ? R : L;
-    // the cell's frame row and its 5 x 4 coefficients in 16-byte vectors (rho and E are used)
+    // the cell's frame row and its 5 x 4 coefficients (rho and E are used): in FP32 as 16-byte vectors
+    // (a fourth of the load instructions of the issue-bound pass); in FP64, whose pass runs at two
+    // blocks per SM with 128 registers, the nine frame values and ten coefficients one by one
     T c[kLimCell], rows[5][4];
-    for (int k = 0; k < kLimCell; k += 4) load_row(cf + cell * kLimCell + k, &c[k]);
-    for (int q = 0; q < 5; q++) load_row(urec + cell * 20 + 4 * q, rows[q]);
+    if constexpr (sizeof(T) == 4) {
+      for (int k = 0; k < kLimCell; k += 4) load_row(cf + cell * kLimCell + k, &c[k]);
+      for (int q = 0; q < 5; q++) load_row(urec + cell * 20 + 4 * q, rows[q]);
+    } else {
+      for (int k = 0; k < 9; k++) c[k] = cf[cell * kLimCell + k];
+      for (int q = 0; q < 5; q++) {
+        rows[q][0] = urec[cell * 20 + 4 * q];
+        rows[q][3] = urec[cell * 20 + 4 * q + 3];
+      }
+    }
     const C Q[2][2] = {{c[0], c[1]}, {c[2], c[3]}};
     const C mo[5] = {c[4], c[5], c[6], c[7], c[8]};
     C D[6][5];
