@@ -313,9 +313,9 @@ __global__ void __launch_bounds__(TILE * 4) k_vr_tma4(HotView<T> h, unsigned* fl
 }
 
 template <class T>
-__global__ void k_vr_wall_fixup(HotView<T> h, const int32_t* cells, int64_t n) {
+__global__ void k_vr_wall_fixup(HotView<T> h, const int32_t* cells, int64_t n) {  // 4 threads per wall cell
   int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (k < n) vr_wall_fixup<T>(cells[k], h);
+  if (k < 4 * n) vr_wall_fixup<T>(cells[k >> 2], (int)(k & 3), h);
 }
 // ---- CWBAP limiter: face indicator integrals, cell indicator, limiting pass
 template <class T>
@@ -626,7 +626,7 @@ int run_vr(dndsg_ctx* c, bool inc, cudaStream_t s) {
       k_vr_tma4<T, TILE, 3><<<(unsigned)((c->N + TILE - 1) / TILE), TILE * 4, smem, s>>>(h, c->flags);
     else
       k_vr_tma4<T, TILE, 4><<<(unsigned)((c->N + TILE - 1) / TILE), TILE * 4, smem, s>>>(h, c->flags);
-    if (c->nWallCells > 0) k_vr_wall_fixup<T><<<grid_for(c->nWallCells), kBlock, 0, s>>>(h, c->wallCells, c->nWallCells);
+    if (c->nWallCells > 0) k_vr_wall_fixup<T><<<grid_for(4 * c->nWallCells), kBlock, 0, s>>>(h, c->wallCells, c->nWallCells);
   } else {
     k_vr<T, false, false><<<grid_for(c->N), kBlock, 0, s>>>(h, nullptr);
   }
@@ -1807,7 +1807,7 @@ void launch_vr_from(dndsg_ctx* c, const void* src, void* dst, bool inc, cudaStre
     const unsigned grid = (unsigned)((c->N + TILE - 1) / TILE);
     if (c->nfmax == 3) k_vr_tma4<T, TILE, 3><<<grid, TILE * 4, (size_t)TILE * 3 * 30 * sizeof(T), s>>>(h, c->flags);
     else k_vr_tma4<T, TILE, 4><<<grid, TILE * 4, (size_t)TILE * 4 * 30 * sizeof(T), s>>>(h, c->flags);
-    if (c->nWallCells > 0) k_vr_wall_fixup<T><<<grid_for(c->nWallCells), kBlock, 0, s>>>(h, c->wallCells, c->nWallCells);
+    if (c->nWallCells > 0) k_vr_wall_fixup<T><<<grid_for(4 * c->nWallCells), kBlock, 0, s>>>(h, c->wallCells, c->nWallCells);
   } else {
     k_vr<T, false, false><<<grid_for(c->N), kBlock, 0, s>>>(h, nullptr);
   }

@@ -1128,50 +1128,48 @@ DG_HD void vr_cell_var(int64_t i, int v, const HotView<T>& h, const Op& opk) {
   }
 }
 
-// Wall_Euler / Wall_NoSlip slots of cell i (DNDS_FV_VR.hpp:1577-1665): adds
-// relax * A^-1 * (integral of the weighted jump to the wall state) to urecNew
+// Wall_Euler / Wall_NoSlip slots of cell i (DNDS_FV_VR.hpp:1577-1665): adds relax * A^-1 * (integral of
+// the weighted jump to the wall state) to urecNew, for conservative component c only (the wall state of
+// an Euler wall couples the momentum components, so every component's face value is formed, but the
+// jump, its integral and the A^-1 product of component c are independent of the others)
 template <class T>
-DG_HD void vr_wall_fixup(int64_t i, const HotView<T>& h) {
+DG_HD void vr_wall_fixup(int64_t i, int c, const HotView<T>& h) {
   double ui[4];
-  for (int c = 0; c < 4; c++) ui[c] = h.u[i * 4 + c];
-  double add[5][4];
-  for (int r = 0; r < 5; r++) for (int c = 0; c < 4; c++) add[r][c] = 0;
+  for (int v = 0; v < 4; v++) ui[v] = h.u[i * 4 + v];
+  double add[5] = {0, 0, 0, 0, 0};
   for (int k = 0; k < h.nfmax; k++) {
     if (h.vrMode[aos(i, k, h.nfmax)] != VR_WALLCORR) continue;
     int32_t f = h.vrFace[aos(i, k, h.nfmax)];
     double nx = h.faceNormal[2 * f], ny = h.faceNormal[2 * f + 1];
     double w0 = h.faceW0[f], area = h.faceArea[f];
     int bc = h.faceBC[f];
-    double corr[5][4];
-    for (int q = 0; q < 5; q++) for (int c = 0; c < 4; c++) corr[q][c] = 0;
+    double corr[5] = {0, 0, 0, 0, 0};
     for (int g = 0; g < 3; g++) {
-      double phi[5], uBL[4], uBV[4];
+      double phi[5], uBL[4];
       for (int q = 0; q < 5; q++) phi[q] = (double)h.faceBasis[aos(f, g * 5 + q, 30)];
-      for (int c = 0; c < 4; c++) {
+      for (int v = 0; v < 4; v++) {
         double s = 0;
-        for (int q = 0; q < 5; q++) s += phi[q] * (double)h.urec[i * 20 + q * 4 + c];
-        uBL[c] = s + ui[c];
+        for (int q = 0; q < 5; q++) s += phi[q] * (double)h.urec[i * 20 + q * 4 + v];
+        uBL[v] = s + ui[v];
       }
+      double uBVc;
       if (bc == BC_WALL_EULER) {
-        double d = nx * uBL[1] + ny * uBL[2];
-        uBV[0] = uBL[0]; uBV[1] = uBL[1] - nx * d; uBV[2] = uBL[2] - ny * d; uBV[3] = uBL[3];
+        const double d = nx * uBL[1] + ny * uBL[2];
+        uBVc = c == 1 ? uBL[1] - nx * d : (c == 2 ? uBL[2] - ny * d : uBL[c]);
       } else {
-        uBV[0] = uBL[0]; uBV[1] = -uBL[1]; uBV[2] = -uBL[2]; uBV[3] = uBL[3];
+        uBVc = (c == 1 || c == 2) ? -uBL[c] : uBL[c];
       }
       double jw = 0.5 * area * l3_weight(g);
-      for (int q = 0; q < 5; q++)
-        for (int c = 0; c < 4; c++) corr[q][c] += phi[q] * w0 * w0 * (uBV[c] - ui[c]) * jw;
+      for (int q = 0; q < 5; q++) corr[q] += phi[q] * w0 * w0 * (uBVc - ui[c]) * jw;
     }
     const double* Ai = &h.Ainv[i * 25];
-    for (int r = 0; r < 5; r++)
-      for (int c = 0; c < 4; c++) {
-        double s = 0;
-        for (int q = 0; q < 5; q++) s += Ai[r * 5 + q] * corr[q][c];
-        add[r][c] += s;
-      }
+    for (int r = 0; r < 5; r++) {
+      double s = 0;
+      for (int q = 0; q < 5; q++) s += Ai[r * 5 + q] * corr[q];
+      add[r] += s;
+    }
   }
-  for (int r = 0; r < 5; r++)
-    for (int c = 0; c < 4; c++) h.urecNew[i * 20 + r * 4 + c] += T(h.relax * add[r][c]);
+  for (int r = 0; r < 5; r++) h.urecNew[i * 20 + r * 4 + c] += T(h.relax * add[r]);
 }
 
 }  // namespace dg
