@@ -232,3 +232,58 @@ def test_bad_parts_are_refused_and_change_nothing():
         s.lusgs_set_parts(bad, 4)
     assert s.lusgs_set_order(1) == nb
     s.close()
+
+
+@pytest.mark.gpu
+def test_partitioned_sweeps_on_mixed_cells_match_oracle(oracle_lib):
+    """Ragged face slots (quadrilaterals and triangles side by side, far field all round) in 3 parts."""
+    import importlib.util
+    import os
+
+    spec = importlib.util.spec_from_file_location(
+        "edge_cases", os.path.join(os.path.dirname(os.path.abspath(__file__)), "test_edge_cases.py"))
+    ec = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(ec)
+    m = ec._mixed_mesh(12)
+    cfg = _cfg()
+    far = np.array(cfg["eulerSetting"]["farFieldStaticValue"])
+    x = m.node_xy[m.cell_nodes.clip(0)].mean(1)
+    u0 = far[None, :] * (1 + 0.05 * np.sin(6.0 * x[:, :1]) * np.cos(5.0 * x[:, 1:]))
+    parts = block_owner(m.n_cells, 3)
+    s = _gpu(m, cfg)
+    s.lusgs_set_order(1)
+    s.lusgs_set_parts(parts, 3)
+    s.set_u(u0)
+    s.bdf_begin()
+    o = oracle_lib.Oracle(m, cfg, n_threads=4)
+    o.set_lusgs_parts(parts)
+    o.set_u(u0)
+    for _ in range(10):
+        res, _ = s.implicit_iteration(50.0)
+        inc = o.implicit_iteration(50.0, u0)
+        assert abs(res[0] - np.abs(inc[:, 0]).sum()) < 1e-9 * res[0]
+    assert _rel(s.get_u(), o.get_u()) < 1e-10
+    s.close()
+
+
+@pytest.mark.gpu
+def test_an_empty_part_is_walked_as_nothing(oracle_lib):
+    """Parts 0 and 2 of 3 (part 1 holds no cell): its block has no level and returns at once."""
+    m, cfg = _naca_small(), _cfg()
+    u0 = _free_stream(m, cfg) * (1 + 0.01 * np.sin(np.arange(m.n_cells))[:, None])
+    parts = 2 * block_owner(m.n_cells, 2)
+    s = _gpu(m, cfg)
+    s.lusgs_set_order(1)
+    s.lusgs_set_parts(parts, 3)
+    s.set_u(u0)
+    s.bdf_begin()
+    o = oracle_lib.Oracle(m, cfg, n_threads=4)
+    o.set_lusgs_parts(parts)
+    o.set_u(u0)
+    for _ in range(5):
+        s.implicit_iteration(100.0)
+        o.implicit_iteration(100.0, u0)
+    assert _rel(s.get_u(), o.get_u()) < 1e-10
+    flags, _ = s.status()
+    assert flags == 0
+    s.close()
