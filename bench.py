@@ -504,6 +504,53 @@ def riemann_to_end_leg(dev, grid=512, t_end=0.3, log=None):
     return out
 
 
+def renumber_leg(dev, grid=N_GRID, steps=20, log=None):
+    """The METIS-free renumbering on the headline workload (FP32 bulk): the VR sweep, the RHS and the
+    SSP-RK3 step on the generator's cell order, on a random permutation of it (a mesh file whose
+    element order carries no locality), and on that permutation renumbered along a Hilbert curve
+    (mesh.renumber).  CUDA-event times; the results of all three are the same, permuted."""
+    import torch
+
+    from dnds_b200 import geometry as G
+    from dnds_b200 import mesh as M
+    from dnds_b200 import settings as S
+    from dnds_b200.solver import Solver
+
+    m0 = M.vortex_mesh(grid, True, jitter=0.2, seed=1234)
+    u0 = G.isentropic_vortex(m0)
+    shuffled, sh = M.renumber(m0, np.random.default_rng(7).permutation(m0.n_cells))
+    t0 = time.perf_counter()
+    hil, order = M.renumber(shuffled)
+    t_renumber = time.perf_counter() - t0
+    out = {"workload": f"isentropic vortex, {grid}x{grid}x2 = {m0.n_cells:,} triangles, FP32 bulk",
+           "renumber_host_s": t_renumber}
+    ev = lambda: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))  # noqa: E731
+    for key, m, u in (("generator_order", m0, u0), ("random_order", shuffled, u0[sh]),
+                      ("random_then_hilbert", hil, u0[sh][order])):
+        L, R = m.face_cells[:, 0], m.face_cells[:, 1]
+        inner = R >= 0
+        s = Solver(m, S.preset("vortex"), device=dev, precision=1)
+        s.set_u(u)
+        for _ in range(3):
+            s.ssprk3_step(0.5)
+        r = {"mean_face_index_gap": float(np.abs(L[inner] - R[inner]).mean())}
+        for name, fn in (("vr_ms", lambda: s.ReconstructionJacobiStep(1)), ("rhs_ms", lambda: s.EvaluateRHS(0.0, copy=False)),
+                         ("step_ms", lambda: s.ssprk3_step(0.5))):
+            e0, e1 = ev()
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(steps):
+                fn()
+            e1.record()
+            torch.cuda.synchronize()
+            r[name] = e0.elapsed_time(e1) / steps
+        s.close()
+        out[key] = r
+        if log:
+            log(key, r)
+    return out
+
+
 def small_mesh_leg(dev, steps=2000):
     """The launch-bound small case: the isentropic vortex on 40 x 40 periodic quads (1,600 cells), P2 VR +
     Roe, SSP-RK3 CFL 0.5: ms per step with one kernel launch per kernel (dndsg_ssprk3_step) and with
@@ -615,6 +662,7 @@ def main():
     ap.add_argument("--precisions", default="fp32,fp64")
     ap.add_argument("--no-steady", action="store_true", help="skip the implicit steady RANS-SA NACA 0012 report")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start report")
+    ap.add_argument("--no-renumber", action="store_true", help="skip the cell-renumbering (locality) report")
     ap.add_argument("--no-riemann", action="store_true", help="skip the 8.4M-triangle Riemann / CWBAP report")
     ap.add_argument("--riemann-grid", type=int, default=2048, help="grid size of the Riemann / CWBAP report")
     ap.add_argument("--riemann-end-grid", type=int, default=512,
@@ -819,6 +867,8 @@ def main():
         if os.path.exists(rec):  # the configured mesh to t = 0.3, recorded by --riemann-full (too long for here)
             with open(rec) as fh:
                 out["riemann_to_t03_2048_recorded"] = json.load(fh)
+    if rank == 0 and ws == 1 and not args.no_renumber:
+        out["renumber_locality"] = renumber_leg(dev, args.grid)
     if rank == 0 and ws == 1 and not args.no_learned:
         out["learned_vr"] = learned_leg(dev, args.grid)
     if rank == 0:

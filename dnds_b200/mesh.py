@@ -370,6 +370,58 @@ def naca0012_cmesh(n_airfoil: int = 256, n_wake: int = 128, nj: int = 128, first
     return _as_mesh(xy, cells, faces, f"naca0012_c{ni}x{nj}", meta)
 
 
+def hilbert_order(points: np.ndarray, bits: int = 16) -> np.ndarray:
+    """The indices that sort points [n, 2] along a Hilbert curve through their bounding square, quantised
+    to a 2^bits x 2^bits grid (the iterative index of the curve: per bit level, the quadrant's
+    contribution s^2 ((3 rx) xor ry), then the quadrant's rotation).  Consecutive points of the order
+    are close in space."""
+    pts = np.asarray(points, dtype=np.float64)
+    lo = pts.min(0)
+    span = max(float(np.ptp(pts[:, 0])), float(np.ptp(pts[:, 1])), 1e-300)
+    n = 1 << bits
+    q = np.clip(((pts - lo) / span * (n - 1)).astype(np.int64), 0, n - 1)
+    x, y = q[:, 0].copy(), q[:, 1].copy()
+    d = np.zeros(len(pts), dtype=np.int64)
+    s = n >> 1
+    while s > 0:
+        rx = ((x & s) > 0).astype(np.int64)
+        ry = ((y & s) > 0).astype(np.int64)
+        d += s * s * ((3 * rx) ^ ry)
+        flip = (ry == 0) & (rx == 1)
+        x = np.where(flip, n - 1 - x, x)
+        y = np.where(flip, n - 1 - y, y)
+        swap = ry == 0
+        x, y = np.where(swap, y, x), np.where(swap, x, y)
+        s >>= 1
+    return np.argsort(d, kind="stable")
+
+
+def renumber(m: Mesh, order: np.ndarray | None = None) -> tuple[Mesh, np.ndarray]:
+    """A METIS-free renumbering for locality: the mesh with its cells in `order` (new cell k is old cell
+    order[k]; default the Hilbert order of the cell centroids) and its faces sorted by the lower new
+    index of their cells, so that the cells and faces a kernel gathers together sit close in memory.
+    Every cell keeps its nodes (hence its element-local face order) and every face its nodes, cells
+    (renumbered), boundary type and periodic shift, so the discretisation is unchanged: results on the
+    new mesh are those of the old one, permuted.  Returns (mesh, order); a state of the old mesh maps
+    to the new one as u[order]."""
+    n = m.n_cells
+    cn = m.cell_nodes
+    valid = cn >= 0
+    cent = (m.node_xy[np.maximum(cn, 0)] * valid[:, :, None]).sum(1) / valid.sum(1)[:, None]
+    order = hilbert_order(cent) if order is None else np.asarray(order, dtype=np.int64)
+    if order.shape != (n,) or not np.array_equal(np.sort(order), np.arange(n)):
+        raise ValueError("order is not a permutation of the cells")
+    new_of_old = np.empty(n, dtype=np.int64)
+    new_of_old[order] = np.arange(n)
+    L = new_of_old[m.face_cells[:, 0]]
+    R = np.where(m.face_cells[:, 1] >= 0, new_of_old[np.maximum(m.face_cells[:, 1], 0)], -1)
+    lo = np.where(R >= 0, np.minimum(L, R), L)
+    fperm = np.lexsort((np.maximum(L, R), lo))
+    faces = (m.face_nodes[fperm], np.stack([L, R], 1)[fperm], m.face_bc[fperm], m.face_shift[fperm])
+    meta = {"renumbered_from": m.name}
+    return _as_mesh(m.node_xy, cn[order], faces, f"{m.name}_renumbered", meta), order
+
+
 def line_scan_order(m: Mesh) -> np.ndarray:
     """LU-SGS scan order for a C-mesh from naca0012_cmesh: the wall-normal grid lines, even ones
     first, then odd ones, each from the wall outwards.  Like the natural cell order (which also runs
