@@ -504,6 +504,118 @@ def riemann_to_end_leg(dev, grid=512, t_end=0.3, log=None):
     return out
 
 
+def dual_time_leg(dev, grid=N_GRID, steps=10, dt=0.05, log=None):
+    """The reference's implicit unsteady driver on the headline vortex (2,097,152 triangles): SDIRK4 and
+    BDF2 dual time (ImplicitSDIRK4DualTimeStep / ImplicitBDFDualTimeStep, DNDS_ODE.hpp:269-497) with
+    LU-SGS in colour batches, pseudo-time CFL 100, at most 20 internal iterations per stage to a density
+    increment ratio of 1e-4, physical dt 0.05 (about 12 times the explicit step at CFL 0.5), `steps`
+    steps to t = 0.5; and SDIRK4 with GMRES(LU-SGS) (5 Krylov vectors, one restart).  ms per physical step, internal iterations per
+    stage, and the density L2 error against the exact advected vortex at the end, FP64 and FP32 bulk.
+    The oracle's SDIRK4 step on the 128 x 128 x 2 version on the host cores gives the CPU figure."""
+    import torch
+
+    from dnds_b200 import geometry as G
+    from dnds_b200 import mesh as M
+    from dnds_b200 import settings as S
+    from dnds_b200.solver import Solver
+
+    m = M.vortex_mesh(grid, True, jitter=0.2, seed=1234)
+    u0 = G.isentropic_vortex(m)
+    vol = G.cell_quadrature(m)[1].sum(1)
+    exact = G.isentropic_vortex(m, t=steps * dt)[:, 0]
+    out = {"workload": f"isentropic vortex, {grid}x{grid}x2 = {m.n_cells:,} triangles, physical dt {dt}, "
+                       f"{steps} steps to t = {steps * dt:g}, pseudo-time CFL 100, LU-SGS colour batches, "
+                       "internal iterations <= 20 to 1e-4"}
+    variants = (("sdirk4", dict(scheme="sdirk4"), 1), ("sdirk4", dict(scheme="sdirk4"), 0),
+                ("bdf2", dict(scheme="bdf", bdf_order=2), 1),
+                ("sdirk4_gmres", dict(scheme="sdirk4", gmres_code=1, n_gmres_space=5, n_gmres_iter=1), 1))
+    for name, kw, prec in variants:
+        s = Solver(m, S.preset("vortex"), device=dev, precision=prec)
+        s.set_u(u0)
+        its = []
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for k in range(steps):
+            it, _ = s.dual_step(dt, k * dt, cfl=100.0, max_iter=20, threshold=1e-4, **kw)
+            its.append([int(x) for x in it])
+        e1.record()
+        torch.cuda.synchronize()
+        d = s.get_u()[:, 0] - exact
+        key = f"{name}_{'fp32' if prec else 'fp64'}"
+        out[key] = {"ms_per_step": e0.elapsed_time(e1) / steps, "iterations_per_stage": its,
+                    "l2_rho_vs_exact": float(np.sqrt((d * d * vol).sum() / vol.sum()))}
+        s.close()
+        if log:
+            log(key, out[key])
+    try:  # the oracle's SDIRK4 step on a bounded sample of the workload, host cores
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle
+
+        pyoracle.build()
+        mc = M.vortex_mesh(128, True, jitter=0.2, seed=1234)
+        o = pyoracle.Oracle(mc, S.preset("vortex"), n_threads=0)
+        o.set_u(G.isentropic_vortex(mc))
+        t0 = time.perf_counter()
+        o.dual_step(dt, 0.0, scheme="sdirk4", cfl=100.0, max_iter=20, threshold=1e-4)
+        sec = time.perf_counter() - t0
+        out["cpu_oracle"] = {"ms_per_step": sec * 1e3, "cells": mc.n_cells, "cores": os.cpu_count(), "kind": "port",
+                             "cell_steps_per_s": mc.n_cells / sec, "sample": "one SDIRK4 step, 128x128x2 triangles"}
+    except Exception as e:  # the CPU figure is a side report
+        out["cpu_oracle"] = {"error": str(e)[:200]}
+    return out
+
+
+def partition_leg(dev, grid=512, steps=20, log=None):
+    """Partitioned runs on one GPU (dnds_b200.partition.PartitionedRun: one context per part with its
+    ghost layer, halo pack / unpack after every VR sweep and stage update, dt reduced over the parts on
+    the host) against the whole mesh, FP32 bulk, the vortex on grid x grid x 2 triangles: ms per
+    SSP-RK3 step (wall time over `steps` steps; the partitioned step synchronises once for dt) and the
+    largest difference of the owned means from the whole-mesh run.  On several GPUs the pack / unpack
+    pairs become NCCL send / receive; that run is not available on one GPU."""
+    import torch
+
+    from dnds_b200 import geometry as G
+    from dnds_b200 import mesh as M
+    from dnds_b200 import settings as S
+    from dnds_b200.partition import PartitionedRun
+    from dnds_b200.solver import Solver
+
+    m = M.vortex_mesh(grid, True, jitter=0.2, seed=1234)
+    u0 = G.isentropic_vortex(m)
+    cfg = S.preset("vortex")
+    out = {"workload": f"isentropic vortex, {grid}x{grid}x2 = {m.n_cells:,} triangles, FP32 bulk, SSP-RK3 CFL 0.5"}
+    s = Solver(m, cfg, device=dev, precision=1)
+    s.set_u(u0)
+    s.ssprk3_step(0.5)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        s.ssprk3_step(0.5)
+    torch.cuda.synchronize()
+    out["whole_mesh_ms_per_step"] = (time.perf_counter() - t0) / steps * 1e3
+    ref = s.get_u()
+    s.close()
+    for nparts in (2, 4):
+        t0 = time.perf_counter()
+        pr = PartitionedRun(m, cfg, nparts, precision=1, device=dev)
+        t_setup = time.perf_counter() - t0
+        pr.set_u(u0)
+        pr.ssprk3_step(0.5)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            pr.ssprk3_step(0.5)
+        torch.cuda.synchronize()
+        ms = (time.perf_counter() - t0) / steps * 1e3
+        diff = float(np.abs(pr.get_u() - ref).max() / np.abs(ref).max())
+        pr.close()
+        out[f"parts{nparts}"] = {"ms_per_step": ms, "max_rel_diff_vs_whole": diff, "setup_s": t_setup}
+        if log:
+            log(f"parts{nparts}", out[f"parts{nparts}"])
+    return out
+
+
 def renumber_leg(dev, grid=N_GRID, steps=20, log=None):
     """The METIS-free renumbering on the headline workload (FP32 bulk): the VR sweep, the RHS and the
     SSP-RK3 step on the generator's cell order, on a random permutation of it (a mesh file whose
@@ -663,6 +775,7 @@ def main():
     ap.add_argument("--no-steady", action="store_true", help="skip the implicit steady RANS-SA NACA 0012 report")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start report")
     ap.add_argument("--no-renumber", action="store_true", help="skip the cell-renumbering (locality) report")
+    ap.add_argument("--no-dual", action="store_true", help="skip the implicit unsteady (dual time) report")
     ap.add_argument("--no-riemann", action="store_true", help="skip the 8.4M-triangle Riemann / CWBAP report")
     ap.add_argument("--riemann-grid", type=int, default=2048, help="grid size of the Riemann / CWBAP report")
     ap.add_argument("--riemann-end-grid", type=int, default=512,
@@ -867,8 +980,11 @@ def main():
         if os.path.exists(rec):  # the configured mesh to t = 0.3, recorded by --riemann-full (too long for here)
             with open(rec) as fh:
                 out["riemann_to_t03_2048_recorded"] = json.load(fh)
+    if rank == 0 and ws == 1 and not args.no_dual:
+        out["dual_time_vortex"] = dual_time_leg(dev, args.grid)
     if rank == 0 and ws == 1 and not args.no_renumber:
         out["renumber_locality"] = renumber_leg(dev, args.grid)
+        out["partitioned_one_gpu"] = partition_leg(dev)
     if rank == 0 and ws == 1 and not args.no_learned:
         out["learned_vr"] = learned_leg(dev, args.grid)
     if rank == 0:
