@@ -217,13 +217,16 @@ int dndsg_eval_rhs_noalloc(dndsg_ctx* ctx, const double* u, const void* urec, do
 int dndsg_get_status(dndsg_ctx* ctx, uint32_t* flags, uint64_t* n_reduced, void* stream);
 
 /* ---------------------------------------------------------------------------
- * Implicit steady path: colour-batched LU-SGS and first-order BDF pseudo time.
+ * Implicit steady path: LU-SGS and first-order BDF pseudo time.
  * The reference sweeps cells one at a time in a scan order
- * (UpdateLUSGSForward / Backward, DNDS_FV_EulerEvaluator.cpp:1149-1357).  Here
- * the cells get a greedy distance-1 colouring and each colour is one parallel
- * step; that is exactly the reference's sweep in the colour-sorted scan order
- * (a neighbour is "before" a cell when its colour is smaller).  The diagonal
- * is one scalar per cell, as in the reference without source terms.
+ * (UpdateLUSGSForward / Backward, DNDS_FV_EulerEvaluator.cpp:1149-1357).  By
+ * default the cells get a greedy distance-1 colouring and each colour is one
+ * parallel step; that is exactly the reference's sweep in the colour-sorted
+ * scan order (a neighbour is "before" a cell when its colour is smaller).
+ * dndsg_lusgs_set_order runs a given scan order (the reference's natural order
+ * by default) as dependency levels, and dndsg_lusgs_set_parts that sweep as on
+ * several ranks.  The diagonal is one scalar per cell, as in the reference
+ * without source terms (the SA variable adds its source Jacobian).
  * ------------------------------------------------------------------------ */
 /* the colouring: colour_out [n_cells] (host, may be NULL), n_colours */
 int dndsg_lusgs_colours(dndsg_ctx* ctx, int32_t* colour_out, int* n_colours);
