@@ -1,8 +1,9 @@
 /*
  * dndsg.h -- C ABI of the B200 (sm_100a) implementation of the DNDS
  * residual-evaluation hot path: the variational-reconstruction (VR) Jacobi
- * sweep, the CWBAP limiter and the face Gauss-point Riemann flux with scatter
- * to cells, plus the SSP-RK3 stage composition that drives them.
+ * sweep, the WBAP limiters (CWBAP and 3WBAP) and the face Gauss-point Riemann
+ * flux with scatter to cells, the SSP-RK3 stage composition that drives them,
+ * and the implicit path (EvaluateDt, LU-SGS, BDF / SDIRK4 dual time, GMRES).
  *
  * Every entry point returns 0 on success and a non-zero dndsg_status code on
  * failure; nothing throws or aborts.  dndsg_last_error() gives the message.
