@@ -1315,7 +1315,7 @@ void face_flux(const orc_ctx& c, int64_t f, double t, double fl[3][kMaxV], doubl
   for (int ig = 0; ig < 3; ig++) {
     double nn = std::sqrt(sqr(fg.n[ig][0]) + sqr(fg.n[ig][1]));
     double un[2] = {fg.n[ig][0] / nn, fg.n[ig][1] / nn};
-    double inc[kMaxV], ULxy[kMaxV], URxy[kMaxV], ULm[kMaxV], URm[kMaxV];
+    double inc[kMaxV] = {}, ULxy[kMaxV] = {}, URxy[kMaxV] = {}, ULm[kMaxV] = {}, URm[kMaxV] = {};
     bool redL = false, redR = false;
     for (int v = 0; v < nv; v++) {
       double s = 0;
@@ -1541,7 +1541,7 @@ void eval_rhs(orc_ctx& c, double t, double* rhs, double* wallFlux, int* nreduced
         const double wdet = q.w[ig] * (J[0][0] * J[1][1] - J[0][1] * J[1][0]);
         double D[kND][kND];
         diff_base_value(c, g, x, y, g.moment, D);
-        double inc[kMaxV], U[kMaxV], G[2][kMaxV];
+        double inc[kMaxV] = {}, U[kMaxV] = {}, G[2][kMaxV] = {};
         for (int v = 0; v < nv; v++) {
           double s0 = 0, s1 = 0, s2 = 0;
           for (int r = 0; r < 5; r++) {
@@ -2107,7 +2107,7 @@ int orc_dual_step(orc_ctx* c, const orc_dual_settings* d, double dt, double t, c
     compose(rhs);
     lusgs_matrix_init(*c, dTau.data(), dt, alphaDiag);
     for (int64_t i = 0; i < c->N; i++) {
-      double r[kMaxV];
+      double r[kMaxV] = {};
       for (int v = 0; v < nv; v++) r[v] = rhs[i * nv + v] * dTau[i];
       compress_inc(*c, &c->u[i * nv], r);
       for (int v = 0; v < nv; v++) rhs[i * nv + v] = r[v] / dTau[i];
