@@ -57,7 +57,8 @@ struct dndsg_ctx {
   void *saUrec = nullptr, *saUrecNew = nullptr;  // T [N][5]
   double* Ainv = nullptr;
   void* limFace = nullptr;                                 // T: the limiting pass's per-face matrices
-  double *faceInd = nullptr, *indicator = nullptr;         // the indicator's integrals and values
+  void* faceInd = nullptr;                                  // the indicator's face integrals (precision T)
+  double* indicator = nullptr;                              // the indicator's values
   int32_t *limList = nullptr, *limCount = nullptr;  // cells the limiter pass limits, and their number
   void *limG = nullptr, *limCell = nullptr;         // the indicator's compact face and cell data (T)
   int sms = 0;                                      // multiprocessors of the device
@@ -339,11 +340,12 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 4 : 2) k_lim_face(Lim
 }
 // the indicator of every cell; a cell with si >= scale (or every cell, ifAll) is appended to the
 // list (order of the list is immaterial: each cell's result depends on the unlimited data only)
+template <class T>
 __global__ void __launch_bounds__(kBlock) k_lim_cell_indicator(LimView v, int32_t* list, int32_t* count) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   bool lim = false;
   if (i < v.N) {
-    const double ind = limiter_cell_indicator(i, v);
+    const double ind = limiter_cell_indicator<T>(i, v);
     v.indicator[i] = ind;
     lim = !(ind < v.scale) || v.ifAll;
   }
@@ -652,7 +654,7 @@ template <class T>
 void run_limiter_v3(dndsg_ctx* c, int ifAll, cudaStream_t s) {
   LimView v = lim_view(c, ifAll);
   k_lim_face<T><<<grid_for(c->F), kBlock, 0, s>>>(v, (const T*)c->urec, c->limCount);
-  k_lim_cell_indicator<<<grid_for(c->N), kBlock, 0, s>>>(v, c->limList, c->limCount);
+  k_lim_cell_indicator<T><<<grid_for(c->N), kBlock, 0, s>>>(v, c->limList, c->limCount);
   // urecNew (the previous sweep's coefficients, free until the next sweep) holds the limited ones
   if (!c->sms && cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess) c->sms = 148;
   const unsigned g = (unsigned)std::min<int64_t>(grid_for(c->N), 4 * c->sms);
@@ -668,7 +670,7 @@ template <class T>
 void run_limiter_v2(dndsg_ctx* c, int ifAll, cudaStream_t s) {
   LimView v = lim_view(c, ifAll);
   k_lim_face<T><<<grid_for(c->F), kBlock, 0, s>>>(v, (const T*)c->urec, c->limCount);
-  k_lim_cell_indicator<<<grid_for(c->N), kBlock, 0, s>>>(v, c->limList, c->limCount);
+  k_lim_cell_indicator<T><<<grid_for(c->N), kBlock, 0, s>>>(v, c->limList, c->limCount);
   if (!c->sms && cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess) c->sms = 148;
   const unsigned g = (unsigned)std::min<int64_t>(grid_for(c->N), 4 * c->sms);
   if (c->nfmax == 3) k_lim_apply4<T, false, 0, 3><<<g, kBlock, 0, s>>>(v, (const T*)c->urec, (T*)c->urecNew, c->limList, c->limCount);
@@ -1005,7 +1007,7 @@ int setup_run(dndsg_ctx* c, const dndsg_mesh_desc* md) {
   if ((rc = check_launch(c))) return rc;
   if (c->s.limiter) {
     if ((rc = dalloc(c, c->limFace, sizeof(T) * kLimStride * F))) return rc;
-    if ((rc = dalloc(c, c->faceInd, sizeof(double) * 4 * F))) return rc;
+    if ((rc = dalloc(c, c->faceInd, sizeof(T) * 4 * F))) return rc;
     if ((rc = dalloc(c, c->indicator, sizeof(double) * N))) return rc;
     if ((rc = dalloc(c, c->limList, sizeof(int32_t) * N)) || (rc = dalloc(c, c->limCount, sizeof(int32_t)))) return rc;
     k_setup_limiter<T><<<grid_for(F), kBlock>>>(m, p, cells, faceW, (T*)c->limFace, dBad);

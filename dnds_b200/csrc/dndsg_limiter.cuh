@@ -52,7 +52,7 @@ struct LimView {
   const void* limG;        // T [F] AoSoA kLimG (T = the context's precision)
   const void* limCell;     // T [N][kLimCell]
   const double* u;
-  double* faceInd;         // [F][4]: IJI_rho, IJI_E, ISI_rho, ISI_E
+  void* faceInd;           // T [F][4]: IJI_rho, IJI_E, ISI_rho, ISI_E
   double* indicator;       // [N]
   double gamma;
   double tangWeight, tangModMin, tangModPower;
@@ -114,13 +114,17 @@ DG_HD void setup_limiter_compact(int64_t f, const MeshView& m, const CellSetup* 
 }
 
 // the indicator integrals of one face, in the storage precision T: FP64 in FP64 contexts, FP32 in
-// FP32-bulk contexts (the four integrals are stored in FP64 for the cell pass)
+// FP32-bulk contexts (computed in T, scaled by the FP64 face area and stored in T for the cell pass)
 template <class T>
 DG_HD void limiter_face_indicator(int64_t f, const LimView& v, const T* urec) {
   using C = T;
   int32_t L = v.faceL[f], R = v.faceR[f];
-  double* out = &v.faceInd[f * 4];
-  if (R < 0) { out[0] = out[1] = out[2] = out[3] = 0; return; }
+  T* out = static_cast<T*>(v.faceInd) + f * 4;
+  if (R < 0) {
+    const T zero[4] = {T(0), T(0), T(0), T(0)};
+    store_row(out, zero);
+    return;
+  }
   // per side: the rows of the cell's basis derivatives at gauss point 0 (from the cell's frame) times
   // its rho and E coefficients, the mean added to the value row; one side's derivatives live at a time
   const T* g = static_cast<const T*>(v.limG);
@@ -184,19 +188,23 @@ DG_HD void limiter_face_indicator(int64_t f, const LimView& v, const T* urec) {
       is[c] += ps * ps;
     }
   // |n| of gauss point 0 is area/2, times the LINE_1 weight 2
-  out[0] = (double)ij[0] * area; out[1] = (double)ij[1] * area; out[2] = (double)is[0] * area;
-  out[3] = (double)is[1] * area;
+  const T rec[4] = {(T)((double)ij[0] * area), (T)((double)ij[1] * area), (T)((double)is[0] * area),
+                    (T)((double)is[1] * area)};
+  store_row(out, rec);
 }
 
-// cell pass of the indicator: si = sqrt(max |IJI/ISI|) * P^2
+// cell pass of the indicator: si = sqrt(max |IJI/ISI|) * P^2, the face integrals (precision T) summed
+// in FP64
+template <class T>
 DG_HD double limiter_cell_indicator(int64_t i, const LimView& v) {
   double sj[2] = {0, 0}, ss[2] = {0, 0};
   for (int k = 0; k < v.nfmax; k++) {
     int32_t sf = v.cellFace[aos(i, k, v.nfmax)];
     if (sf == kEmptySlot) continue;
     int32_t f = sf >= 0 ? sf : ~sf;
-    const double* d = &v.faceInd[(int64_t)f * 4];
-    sj[0] += d[0]; sj[1] += d[1]; ss[0] += d[2]; ss[1] += d[3];
+    T d[4];
+    load_row(static_cast<const T*>(v.faceInd) + (int64_t)f * 4, d);
+    sj[0] += (double)d[0]; sj[1] += (double)d[1]; ss[0] += (double)d[2]; ss[1] += (double)d[3];
   }
   double s0 = sj[0] / (ss[0] + kVerySmall), s1 = sj[1] / (ss[1] + kVerySmall);
   return sqrt(dmax(fabs(s0), fabs(s1))) * v.porder2;
