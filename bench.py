@@ -41,11 +41,11 @@ N_GRID = 1024
 VR_BYTES_PER_CELL = {4: 130 * 4 + 32 + 12, 8: 130 * 8 + 32 + 12}
 KERNELS_PER_STEP = 14  # init, dt face, dt cell, dt finalize, 3 x (VR, flux, update), time advance
 # algorithmic bytes per triangle cell of one whole SSP-RK3 step: 3 stages x (VR sweep, face flux with
-# 1.5 faces per cell (basis 30s, normal / length / dLambda / indices ~40 B, flux out 32 B) plus the
-# cell's coefficients 20s and means 32 B once, cell update 136 B) + EvaluateDt ~74 B.  FP32 bulk
-# 3 x (564 + 412 + 136) + 74 = 3410 B, FP64 3 x (1084 + 660 + 136) + 74 = 5714 B: at equal HBM
-# efficiency the FP32-bulk step can be at most 5714 / 3410 = 1.68 times faster
-STEP_BYTES_PER_CELL = {4: 3 * (564 + 412 + 136) + 74, 8: 3 * (1084 + 660 + 136) + 74}
+# 1.5 faces per cell (the compact basis record 18s, normal / length / dLambda / indices ~40 B, flux out
+# 32 B) plus the cell's coefficients 20s and means 32 B once, cell update 136 B) + EvaluateDt ~74 B.
+# FP32 bulk 3 x (564 + 328 + 136) + 74 = 3158 B, FP64 3 x (1084 + 516 + 136) + 74 = 5282 B: at equal
+# HBM efficiency the FP32-bulk step can be at most 5282 / 3158 = 1.67 times faster
+STEP_BYTES_PER_CELL = {4: 3 * (564 + 328 + 136) + 74, 8: 3 * (1084 + 516 + 136) + 74}
 # DRAM bytes (read + write) per launch of the FP32 VR sweep: ncu --metrics dram__bytes_read.sum,
 # dram__bytes_write.sum --clock-control none on one k_vr_tma4<float,32,3> launch over the 512x512 version of
 # this mesh (524,288 cells; 291.23 MB read + written, 555 B per cell against the 564 B algorithmic), scaled by

@@ -187,7 +187,7 @@ __global__ void k_setup_face(MeshView m, SetupParams p, const CellSetup* cells, 
                              double* area, double* center, double* w0, T* basis) {
   int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (f >= m.F) return;
-  setup_face<T>(f, m, p, cells, faceW, normal, area, center, w0, basis, nullptr);
+  setup_face<T>(f, m, p, cells, faceW, normal, area, center, w0, basis);
 }
 
 __global__ void k_setup_sa_cells(int64_t N, const CellSetup* cells, const double* seg, int64_t nw, double* gp,
@@ -949,7 +949,7 @@ int setup_run(dndsg_ctx* c, const dndsg_mesh_desc* md) {
   if ((rc = dalloc(c, c->faceArea, sizeof(double) * F))) return rc;
   if ((rc = dalloc(c, c->faceCenter, sizeof(double) * 2 * F))) return rc;
   if ((rc = dalloc(c, c->faceW0, sizeof(double) * F))) return rc;
-  if ((rc = dalloc(c, c->faceBasis, sizeof(T) * aos_size(F, 30)))) return rc;
+  if ((rc = dalloc(c, c->faceBasis, sizeof(T) * aos_size(F, kFaceBasisE)))) return rc;
   k_setup_face<T><<<grid_for(F), kBlock>>>(m, p, cells, faceW, c->faceNormal, c->faceArea, c->faceCenter, c->faceW0,
                                            (T*)c->faceBasis);
   if ((rc = check_launch(c))) return rc;

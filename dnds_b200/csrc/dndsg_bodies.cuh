@@ -24,6 +24,33 @@ constexpr int32_t kEmptySlot = INT32_MIN;  // cellFace slot without a face
 DG_HD double l3_point(int g) { return g == 0 ? -0.7745966692414834 : (g == 1 ? 0.0 : 0.7745966692414834); }
 DG_HD double l3_weight(int g) { return g == 1 ? 8.0 / 9.0 : 5.0 / 9.0; }
 
+// The value-row basis of a face's two cells at its 3 gauss points, stored compactly (AoSoA, E = 18):
+// per side 9 values, the 5 basis values v1 at the face centre (gauss point 1), the centre's frame
+// coordinates (xi, eta) and the frame offset (dxi, deta) from the centre to gauss point 2 (gauss
+// point 0 is at the opposite offset).  The quadratic monomials m = (xi, eta, xi^2, xi eta, eta^2)
+// give the other points exactly: the basis at gauss points 0 and 2 is v1 + C -+ B, where
+// B = (dxi, deta, 2 xi dxi, xi deta + eta dxi, 2 eta deta) and C = (0, 0, dxi^2, dxi deta, deta^2)
+// are the odd and even parts of m(xi + s dxi, eta + s deta) - m(xi, eta) at s = +-1.  18 values per
+// face instead of the 30 of a table of the basis at every point.
+constexpr int kFaceBasisSide = 9, kFaceBasisE = 18;
+
+template <class T>
+struct FaceBasisSide {
+  T v1[5], B[5], C[5];
+  DG_HD FaceBasisSide(const T* fb, int64_t f, int side) {
+    const int o = side * kFaceBasisSide;
+    for (int k = 0; k < 5; k++) v1[k] = fb[aos(f, o + k, kFaceBasisE)];
+    const T xi = fb[aos(f, o + 5, kFaceBasisE)], eta = fb[aos(f, o + 6, kFaceBasisE)];
+    const T dxi = fb[aos(f, o + 7, kFaceBasisE)], det = fb[aos(f, o + 8, kFaceBasisE)];
+    B[0] = dxi; B[1] = det; B[2] = T(2) * xi * dxi; B[3] = xi * det + eta * dxi; B[4] = T(2) * eta * det;
+    C[0] = T(0); C[1] = T(0); C[2] = dxi * dxi; C[3] = dxi * det; C[4] = det * det;
+  }
+  // the basis values at gauss point g
+  DG_HD void at(int g, T phi[5]) const {
+    for (int k = 0; k < 5; k++) phi[k] = g == 1 ? v1[k] : (g == 0 ? (v1[k] + C[k]) - B[k] : (v1[k] + C[k]) + B[k]);
+  }
+};
+
 // ---------------------------------------------------------------- setup
 struct SetupParams {
   int use_local_coord, anisotropic_lengths, base_center_type;
@@ -250,7 +277,7 @@ struct HotView {
   const int32_t* faceL;
   const int32_t* faceR;
   const int32_t* faceBC;
-  const T* faceBasis;       // AoSoA E = 30: [side][gp][5] value-row basis at face gauss points
+  const T* faceBasis;       // AoSoA E = kFaceBasisE: per side the compact record of face_phi below
   const double* faceNormal; // [F][2] unit, out of L
   const double* faceArea;   // [F]
   const double* faceCenter; // [F][2]
@@ -378,9 +405,12 @@ DG_HD void vr_cell_op(int64_t i, const HotView<T>& h, const Op& opk) {
       load_rec(&h.urec[i * 20], ri);
       double corr[5][4];
       for (int q = 0; q < 5; q++) for (int v = 0; v < 4; v++) corr[q][v] = 0;
+      const FaceBasisSide<T> fb(h.faceBasis, f, 0);
       for (int g = 0; g < 3; g++) {
         double phi[5];
-        for (int q = 0; q < 5; q++) phi[q] = (double)h.faceBasis[aos(f, g * 5 + q, 30)];
+        T pg[5];
+        fb.at(g, pg);
+        for (int q = 0; q < 5; q++) phi[q] = (double)pg[q];
         double uBL[4], uBV[4];
         for (int v = 0; v < 4; v++) {
           double s = 0;
@@ -414,33 +444,34 @@ DG_HD void vr_cell(int64_t i, const HotView<T>& h) {
   vr_cell_op<T, RELAX1>(i, h, VrOpGlobal<T>{h.vrOp, i, h.nfmax * 30});
 }
 
+// reconstruction increments phi(gp) . urec of one cell at the 3 gauss points of a face, from the
+// side's compact basis: the dot products of the coefficient rows with v1, B and C (rows 2..4 only),
+// combined per point as phi . r = v1.r + C.r -+ B.r; gauss point 1 is the plain sum v1.r
+template <class T>
+DG_HD void side_increments(const FaceBasisSide<T>& b, const T* rec, T inc[3][4]) {
+  T a[4] = {T(0), T(0), T(0), T(0)}, o[4] = {T(0), T(0), T(0), T(0)}, e[4] = {T(0), T(0), T(0), T(0)};
+  for (int q = 0; q < 5; q++) {
+    T row[4];
+    load_row(rec + 4 * q, row);
+    for (int v = 0; v < 4; v++) {
+      a[v] += b.v1[q] * row[v];
+      o[v] += b.B[q] * row[v];
+      if (q >= 2) e[v] += b.C[q] * row[v];
+    }
+  }
+  for (int v = 0; v < 4; v++) {
+    const T p = a[v] + e[v];
+    inc[0][v] = p - o[v]; inc[1][v] = a[v]; inc[2][v] = p + o[v];
+  }
+}
+
 // reconstruction increments phi(gp) . urec of both cells at the 3 gauss points of
 // face f; the coefficient rows are streamed once (EvaluateRHS, DNDS_FV_EulerEvaluator.cpp:250-360)
 template <class T>
 DG_HD void face_increments(int64_t f, int32_t L, int32_t R, const HotView<T>& h, T incL[3][4], T incR[3][4]) {
-  T phi[3][5];
-  for (int g = 0; g < 3; g++)
-    for (int q = 0; q < 5; q++) phi[g][q] = h.faceBasis[aos(f, g * 5 + q, 30)];
-  for (int g = 0; g < 3; g++) for (int v = 0; v < 4; v++) incL[g][v] = T(0);
-  const T* rl = &h.urec[(int64_t)L * 20];
-  for (int q = 0; q < 5; q++) {
-    T row[4];
-    load_row(rl + 4 * q, row);
-    for (int g = 0; g < 3; g++)
-      for (int v = 0; v < 4; v++) incL[g][v] += phi[g][q] * row[v];
-  }
-  for (int g = 0; g < 3; g++) for (int v = 0; v < 4; v++) incR[g][v] = T(0);
-  if (R >= 0) {
-    for (int g = 0; g < 3; g++)
-      for (int q = 0; q < 5; q++) phi[g][q] = h.faceBasis[aos(f, 15 + g * 5 + q, 30)];
-    const T* rr = &h.urec[(int64_t)R * 20];
-    for (int q = 0; q < 5; q++) {
-      T row[4];
-      load_row(rr + 4 * q, row);
-      for (int g = 0; g < 3; g++)
-        for (int v = 0; v < 4; v++) incR[g][v] += phi[g][q] * row[v];
-    }
-  }
+  side_increments(FaceBasisSide<T>(h.faceBasis, f, 0), &h.urec[(int64_t)L * 20], incL);
+  if (R >= 0) side_increments(FaceBasisSide<T>(h.faceBasis, f, 1), &h.urec[(int64_t)R * 20], incR);
+  else for (int g = 0; g < 3; g++) for (int v = 0; v < 4; v++) incR[g][v] = T(0);
 }
 
 // positivity-compressed states at gauss point g (CompressRecPart, boundary state on a boundary face)
@@ -946,7 +977,7 @@ DG_HD void setup_face_grad(int64_t f, const MeshView& m, const CellSetup* cells,
 
 template <class T>
 DG_HD void setup_face(int64_t f, const MeshView& m, const SetupParams& p, const CellSetup* cells, double* faceW,
-                      double* normal, double* area, double* center, double* w0, T* basis, double* basisD) {
+                      double* normal, double* area, double* center, double* w0, T* basis) {
   FaceGeom g = face_geom(f, m);
   double W[6];
   face_weights(f, m, p, g, cells, W);
@@ -957,19 +988,21 @@ DG_HD void setup_face(int64_t f, const MeshView& m, const SetupParams& p, const 
   w0[f] = W[0];
   int32_t L = m.face_cells[2 * f], R = m.face_cells[2 * f + 1];
   double sx = m.face_shift ? m.face_shift[2 * f] : 0.0, sy = m.face_shift ? m.face_shift[2 * f + 1] : 0.0;
-  for (int q = 0; q < 3; q++) {
-    double v[5];
-    p2_values(cells[L].fr, g.gx[q], g.gy[q], v);
-    for (int k = 0; k < 5; k++) {
-      basis[aos(f, q * 5 + k, 30)] = (T)v[k];
-      if (basisD) basisD[aos(f, q * 5 + k, 30)] = v[k];
+  // gauss point 2 minus the face centre (gauss point 1): s_2 (x1 - x0) / 2
+  const int32_t a = m.face_nodes[2 * f], b = m.face_nodes[2 * f + 1];
+  const double hx = l3_point(2) * 0.5 * (m.node_xy[2 * b] - m.node_xy[2 * a]);
+  const double hy = l3_point(2) * 0.5 * (m.node_xy[2 * b + 1] - m.node_xy[2 * a + 1]);
+  for (int side = 0; side < 2; side++) {
+    double rec[kFaceBasisSide] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (side == 0 || R >= 0) {
+      const CellFrame& fr = cells[side ? R : L].fr;
+      const double ox = side ? sx : 0.0, oy = side ? sy : 0.0;
+      p2_values(fr, g.gx[1] - ox, g.gy[1] - oy, rec);
+      p2_frame_coords(fr, g.gx[1] - ox, g.gy[1] - oy, rec[5], rec[6]);
+      rec[7] = fr.Pinv[0][0] * hx + fr.Pinv[0][1] * hy;
+      rec[8] = fr.Pinv[1][0] * hx + fr.Pinv[1][1] * hy;
     }
-    if (R >= 0) p2_values(cells[R].fr, g.gx[q] - sx, g.gy[q] - sy, v);
-    else for (int k = 0; k < 5; k++) v[k] = 0;
-    for (int k = 0; k < 5; k++) {
-      basis[aos(f, 15 + q * 5 + k, 30)] = (T)v[k];
-      if (basisD) basisD[aos(f, 15 + q * 5 + k, 30)] = v[k];
-    }
+    for (int k = 0; k < kFaceBasisSide; k++) basis[aos(f, side * kFaceBasisSide + k, kFaceBasisE)] = (T)rec[k];
   }
 }
 
@@ -1144,9 +1177,12 @@ DG_HD void vr_wall_fixup(int64_t i, int c, const HotView<T>& h) {
     double w0 = h.faceW0[f], area = h.faceArea[f];
     int bc = h.faceBC[f];
     double corr[5] = {0, 0, 0, 0, 0};
+    const FaceBasisSide<T> fb(h.faceBasis, f, 0);
     for (int g = 0; g < 3; g++) {
       double phi[5], uBL[4];
-      for (int q = 0; q < 5; q++) phi[q] = (double)h.faceBasis[aos(f, g * 5 + q, 30)];
+      T pg[5];
+      fb.at(g, pg);
+      for (int q = 0; q < 5; q++) phi[q] = (double)pg[q];
       for (int v = 0; v < 4; v++) {
         double s = 0;
         for (int q = 0; q < 5; q++) s += phi[q] * (double)h.urec[i * 20 + q * 4 + v];

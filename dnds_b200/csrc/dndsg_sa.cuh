@@ -146,10 +146,13 @@ DG_HD void sa_vr_cell(int64_t i, const HotView<T>& h, const SaView<T>& sa) {
       const double w0 = h.faceW0[f], area = h.faceArea[f];
       const bool noslip = h.faceBC[f] == BC_WALL_NOSLIP;
       double corr[5] = {0, 0, 0, 0, 0};
+      const FaceBasisSide<T> fb(h.faceBasis, f, 0);
       for (int g = 0; g < 3; g++) {
         double phi[5], uBL = ui;
+        T pg[5];
+        fb.at(g, pg);
         for (int q = 0; q < 5; q++) {
-          phi[q] = (double)h.faceBasis[aos(f, g * 5 + q, 30)];
+          phi[q] = (double)pg[q];
           uBL += phi[q] * (double)ri[q];
         }
         const double uBV = noslip ? 0.0 : uBL;
@@ -175,7 +178,9 @@ DG_HD void sa_point(const HotView<T>& h, const SaView<T>& sa, int64_t f, int g, 
                     double UR[4], double& sL, double& sR, int& nred) {
   const double sLm = sa.u[L];
   double incS = 0;
-  for (int q = 0; q < 5; q++) incS += (double)h.faceBasis[aos(f, g * 5 + q, 30)] * (double)sa.urec[(int64_t)L * 5 + q];
+  T pg[5];
+  FaceBasisSide<T>(h.faceBasis, f, 0).at(g, pg);
+  for (int q = 0; q < 5; q++) incS += (double)pg[q] * (double)sa.urec[(int64_t)L * 5 + q];
   double inc[4];
   for (int v = 0; v < 4; v++) inc[v] = (double)incL[v];
   bool cL = compress_rec_part(uL, inc, UL);
@@ -183,8 +188,8 @@ DG_HD void sa_point(const HotView<T>& h, const SaView<T>& sa, int64_t f, int g, 
   nred += cL ? 1 : 0;
   if (inner) {
     double incSR = 0;
-    for (int q = 0; q < 5; q++)
-      incSR += (double)h.faceBasis[aos(f, 15 + g * 5 + q, 30)] * (double)sa.urec[(int64_t)R * 5 + q];
+    FaceBasisSide<T>(h.faceBasis, f, 1).at(g, pg);
+    for (int q = 0; q < 5; q++) incSR += (double)pg[q] * (double)sa.urec[(int64_t)R * 5 + q];
     for (int v = 0; v < 4; v++) inc[v] = (double)incR[v];
     bool cR = compress_rec_part(uR, inc, UR);
     sR = cR ? sa.u[R] : sa.u[R] + incSR;
@@ -214,20 +219,21 @@ DG_HD void sa_point(const HotView<T>& h, const SaView<T>& sa, int64_t f, int g, 
 template <class T>
 DG_HD void face_increment_point(int64_t f, int g, int32_t L, int32_t R, const HotView<T>& h, T incL[4], T incR[4]) {
   for (int v = 0; v < 4; v++) incL[v] = incR[v] = T(0);
+  T phi[5];
+  FaceBasisSide<T>(h.faceBasis, f, 0).at(g, phi);
   const T* rl = &h.urec[(int64_t)L * 20];
   for (int q = 0; q < 5; q++) {
-    const T phi = h.faceBasis[aos(f, g * 5 + q, 30)];
     T row[4];
     load_row(rl + 4 * q, row);
-    for (int v = 0; v < 4; v++) incL[v] += phi * row[v];
+    for (int v = 0; v < 4; v++) incL[v] += phi[q] * row[v];
   }
   if (R >= 0) {
+    FaceBasisSide<T>(h.faceBasis, f, 1).at(g, phi);
     const T* rr = &h.urec[(int64_t)R * 20];
     for (int q = 0; q < 5; q++) {
-      const T phi = h.faceBasis[aos(f, 15 + g * 5 + q, 30)];
       T row[4];
       load_row(rr + 4 * q, row);
-      for (int v = 0; v < 4; v++) incR[v] += phi * row[v];
+      for (int v = 0; v < 4; v++) incR[v] += phi[q] * row[v];
     }
   }
 }
