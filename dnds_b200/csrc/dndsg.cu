@@ -393,8 +393,9 @@ __device__ __forceinline__ double stage_time(const double* scal, int useDev, dou
 // faces [f0, f1): interior faces first (BND = false), then boundary faces.  The FP32 Roe interior
 // kernel runs 4 blocks per SM (64 registers, a few spilled words): the gathers want the occupancy
 // more than the registers (measured: 2 blocks 0.296 ms, 3: 0.283, 4: 0.243, 5: 0.318 per RHS on
-// 2,097,152 triangles).  The FP32 HLLC interior kernel (FP64 algebra) runs 3 (measured per SSP-RK3
-// step of the 8,388,608-triangle Riemann problem: 2 blocks 11.77 ms, 3: 11.36, 4: 11.58)
+// 2,097,152 triangles).  The FP32 HLLC interior kernel (flux-difference form) runs 3 (measured per
+// SSP-RK3 step of the 8,388,608-triangle Riemann problem: 3 blocks 7.79-7.81 ms, 4 blocks with 64
+// registers and 172 B spilled 8.02-8.04 ms)
 template <class T, int RIEMANN, bool BND>
 __global__ void __launch_bounds__(kBlock, (sizeof(T) == 4 && RIEMANN == 1 && !BND) ? 4 : ((sizeof(T) == 4 && !BND) ? 3 : 2)) k_face_flux(HotView<T> h, int64_t f0, int64_t f1, const double* scal,
                                                          int useDev, double tHost, double c, unsigned* flags,
