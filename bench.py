@@ -39,7 +39,7 @@ N_GRID = 1024
 # algorithmic bytes per triangle cell of one VR Jacobi sweep: read urec 20s, A^-1B 75s, A^-1b 15s,
 # write urec 20s (s = bytes per real), cell means 4x8, 3 neighbour indices 3x4
 VR_BYTES_PER_CELL = {4: 130 * 4 + 32 + 12, 8: 130 * 8 + 32 + 12}
-KERNELS_PER_STEP = 14  # init, dt face, dt cell, dt finalize, 3 x (VR, flux, update), time advance
+KERNELS_PER_STEP = 13  # init, 3 x (VR, flux, update) with dt cell and dt finalize after the first flux, time advance
 # algorithmic bytes per triangle cell of one whole SSP-RK3 step: 3 stages x (VR sweep, face flux with
 # 1.5 faces per cell (the compact basis record 18s, normal / length / dLambda / indices ~40 B, flux out
 # 32 B) plus the cell's coefficients 20s and means 32 B once, cell update 136 B) + EvaluateDt ~74 B.

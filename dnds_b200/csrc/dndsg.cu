@@ -387,7 +387,7 @@ __global__ void __launch_bounds__(kBlock) k_lim_scatter(T* urec, const T* buf, c
 }
 
 __device__ __forceinline__ double stage_time(const double* scal, int useDev, double tHost, double c) {
-  return useDev ? scal[S_T] + c * scal[S_DT] : tHost;
+  return useDev ? (c == 0.0 ? scal[S_T] : scal[S_T] + c * scal[S_DT]) : tHost;
 }
 
 // faces [f0, f1): interior faces first (BND = false), then boundary faces.  The FP32 Roe interior
@@ -396,7 +396,10 @@ __device__ __forceinline__ double stage_time(const double* scal, int useDev, dou
 // 2,097,152 triangles).  The FP32 HLLC interior kernel (flux-difference form) runs 3 (measured per
 // SSP-RK3 step of the 8,388,608-triangle Riemann problem: 3 blocks 7.79-7.81 ms, 4 blocks with 64
 // registers and 172 B spilled 8.02-8.04 ms)
-template <class T, int RIEMANN, bool BND>
+// DT = true (the first stage of an SSP-RK3 step): each thread first writes its face's EvaluateDt terms
+// (dt_face: lambda A and the entropy-fix dLambda, from the same means this stage reads), which the
+// flux then reads back, so the step needs no separate face pass for dt
+template <class T, int RIEMANN, bool BND, bool DT = false>
 __global__ void __launch_bounds__(kBlock, (sizeof(T) == 4 && RIEMANN == 1 && !BND) ? 4 : ((sizeof(T) == 4 && !BND) ? 3 : 2)) k_face_flux(HotView<T> h, int64_t f0, int64_t f1, const double* scal,
                                                          int useDev, double tHost, double c, unsigned* flags,
                                                          unsigned long long* nred) {
@@ -404,6 +407,7 @@ __global__ void __launch_bounds__(kBlock, (sizeof(T) == 4 && RIEMANN == 1 && !BN
   int r = 0;
   bool bad = false;
   if (f < f1) {
+    if constexpr (DT) dt_face<T>(f, h);
     double out[4];
     double t = stage_time(scal, useDev, tHost, c);
     if constexpr (sizeof(T) == 4 && RIEMANN == 1 && !BND)
@@ -689,9 +693,29 @@ void run_limiter(dndsg_ctx* c, int ifAll, cudaStream_t s) {
   else run_limiter_v3<T>(c, ifAll, s);
 }
 
-// the face-flux launches of EvaluateRHS over the arrays of h (interior faces, then boundary faces)
+// the inviscid face-flux launches (interior faces, then boundary faces); DT: with the faces' dt terms
+template <class T, bool DT>
+void launch_flux_inviscid(dndsg_ctx* c, const HotView<T>& h, int useDev, double tHost, double cst, cudaStream_t s) {
+  const int64_t Fi = c->Fi, F = c->F;
+  if (c->s.riemann == 2) {
+    if (Fi > 0)
+      k_face_flux<T, 2, false, DT><<<grid_for(Fi), kBlock, 0, s>>>(h, 0, Fi, c->scal, useDev, tHost, cst, c->flags, c->nreduced);
+    if (F > Fi)
+      k_face_flux<T, 2, true, DT><<<grid_for(F - Fi), kBlock, 0, s>>>(h, Fi, F, c->scal, useDev, tHost, cst, c->flags, c->nreduced);
+  } else {
+    if (Fi > 0)
+      k_face_flux<T, 1, false, DT><<<grid_for(Fi), kBlock, 0, s>>>(h, 0, Fi, c->scal, useDev, tHost, cst, c->flags, c->nreduced);
+    if (F > Fi)
+      k_face_flux<T, 1, true, DT><<<grid_for(F - Fi), kBlock, 0, s>>>(h, Fi, F, c->scal, useDev, tHost, cst, c->flags, c->nreduced);
+  }
+}
+
+// the face-flux launches of EvaluateRHS over the arrays of h (interior faces, then boundary faces).
+// dt = true (inviscid contexts only, the caller checks): the launches also write the faces' EvaluateDt
+// terms (k_face_flux with DT)
 template <class T>
-void launch_flux_h(dndsg_ctx* c, const HotView<T>& h, int useDev, double tHost, double cst, cudaStream_t s) {
+void launch_flux_h(dndsg_ctx* c, const HotView<T>& h, int useDev, double tHost, double cst, cudaStream_t s,
+                   bool dt = false) {
   const int64_t Fi = c->Fi, F = c->F;
   if (c->s.mu_gas > 0) {
     if (c->s.riemann == 2) {
@@ -707,22 +731,16 @@ void launch_flux_h(dndsg_ctx* c, const HotView<T>& h, int useDev, double tHost, 
     }
     return;
   }
-  if (c->s.riemann == 2) {
-    if (Fi > 0)
-      k_face_flux<T, 2, false><<<grid_for(Fi), kBlock, 0, s>>>(h, 0, Fi, c->scal, useDev, tHost, cst, c->flags, c->nreduced);
-    if (F > Fi)
-      k_face_flux<T, 2, true><<<grid_for(F - Fi), kBlock, 0, s>>>(h, Fi, F, c->scal, useDev, tHost, cst, c->flags, c->nreduced);
-  } else {
-    if (Fi > 0)
-      k_face_flux<T, 1, false><<<grid_for(Fi), kBlock, 0, s>>>(h, 0, Fi, c->scal, useDev, tHost, cst, c->flags, c->nreduced);
-    if (F > Fi)
-      k_face_flux<T, 1, true><<<grid_for(F - Fi), kBlock, 0, s>>>(h, Fi, F, c->scal, useDev, tHost, cst, c->flags, c->nreduced);
+  if (dt) {
+    launch_flux_inviscid<T, true>(c, h, useDev, tHost, cst, s);
+    return;
   }
+  launch_flux_inviscid<T, false>(c, h, useDev, tHost, cst, s);
 }
 
 template <class T>
-void launch_flux(dndsg_ctx* c, int useDev, double tHost, double cst, cudaStream_t s) {
-  launch_flux_h<T>(c, view<T>(c), useDev, tHost, cst, s);
+void launch_flux(dndsg_ctx* c, int useDev, double tHost, double cst, cudaStream_t s, bool dt = false) {
+  launch_flux_h<T>(c, view<T>(c), useDev, tHost, cst, s, dt);
 }
 
 template <class T>
@@ -735,16 +753,31 @@ int run_dt(dndsg_ctx* c, double cfl, double maxDt, bool copyLast, cudaStream_t s
   return 0;
 }
 
+// one SSP-RK3 step.  Inviscid contexts take EvaluateDt's face terms from the first stage's face-flux
+// launches (the same means, the same dt_face arithmetic): the VR sweep and the limiter of stage 1 do
+// not depend on dt, so dt_cell and the minimum follow the first face pass and precede the first update.
+// Viscous contexts (whose dt_face adds the viscous term) run the dt pass first.
 template <class T>
 int run_step(dndsg_ctx* c, double cfl, double tEnd, cudaStream_t s) {
-  run_dt<T>(c, cfl, 1e100, true, s);
-  k_dt_finalize<<<1, 1, 0, s>>>(c->scal, tEnd);
+  const bool fuseDt = !(c->s.mu_gas > 0);
+  if (fuseDt) {
+    k_init_dtmin<<<1, 1, 0, s>>>(c->scal);
+  } else {
+    run_dt<T>(c, cfl, 1e100, true, s);
+    k_dt_finalize<<<1, 1, 0, s>>>(c->scal, tEnd);
+  }
   const double cst[3] = {0.0, 1.0, 0.5};
   for (int stg = 0; stg < 3; stg++) {
     run_vr<T>(c, false, s);
     if (c->s.limiter) run_limiter<T>(c, 0, s);
-    launch_flux<T>(c, 1, 0.0, cst[stg], s);
     HotView<T> h = view<T>(c);
+    if (stg == 0 && fuseDt) {
+      launch_flux<T>(c, 1, 0.0, cst[stg], s, true);
+      k_dt_cell<T, true><<<grid_for(c->N), kBlock, 0, s>>>(h, cfl, 1e100, c->scal);
+      k_dt_finalize<<<1, 1, 0, s>>>(c->scal, tEnd);
+    } else {
+      launch_flux<T>(c, 1, 0.0, cst[stg], s);
+    }
     if (stg == 0) k_cell_update<T, 0><<<grid_for(c->N), kBlock, 0, s>>>(h, c->scal);
     else if (stg == 1) k_cell_update<T, 1><<<grid_for(c->N), kBlock, 0, s>>>(h, c->scal);
     else k_cell_update<T, 2><<<grid_for(c->N), kBlock, 0, s>>>(h, c->scal);
