@@ -165,13 +165,17 @@ int dndsg_eval_rhs(dndsg_ctx* ctx, double t, double* rhs_out, void* stream);
  * with the EulerSolver stage body frhs (DNDS_FV_EulerSolver.hpp:713-837):
  * EvaluateDt (global dt, clipped so that t does not pass t_end), then per
  * stage one VR Jacobi sweep, the limiter when enabled, EvaluateRHS and the
- * stage update.  Time lives on the device and advances by the step's dt, so
- * the call is asynchronous and can be captured in a CUDA graph. */
+ * stage update.  In inviscid contexts EvaluateDt's face terms are written by
+ * the first stage's face-flux launch (from the same means; the first sweep and
+ * limiter do not depend on dt), and its cell pass runs before the first
+ * update.  Time lives on the device and advances by the step's dt, so the
+ * call is asynchronous and can be captured in a CUDA graph. */
 int dndsg_ssprk3_step(dndsg_ctx* ctx, double cfl, double t_end, void* stream);
 
 /* n calls of dndsg_ssprk3_step, with the same results: pairs of steps are
  * replayed from a CUDA graph captured on first use for this cfl / t_end (one
- * graph launch instead of 28 kernel launches; small meshes are launch-bound).
+ * graph launch instead of 26 kernel launches, 28 with a viscous flux; small
+ * meshes are launch-bound).
  * Same arguments as dndsg_ssprk3_step plus the step count n >= 0. */
 int dndsg_ssprk3_steps(dndsg_ctx* ctx, double cfl, double t_end, int64_t n, void* stream);
 
